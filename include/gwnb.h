@@ -1,0 +1,282 @@
+/*
+ * gwnb.h -- C ABI of the B200-native generalized-winding-number library (libgwnb.so).
+ *
+ * Every entry point takes plain pointers, sizes and a CUDA stream, and returns an int status code
+ * (GWNB_OK, GWNB_INVALID_ARGUMENT, GWNB_CUDA_RUNTIME_ERROR, GWNB_INTERNAL_ERROR). The message for
+ * the last failure on the calling host thread is returned by gwnb_last_error_message().
+ *
+ * The entry points replace the public C++ template API of smallgwn (namespace gwn, headers under
+ * include/gwn/ of that project); the citation beside each declaration names the interface it
+ * replaces. The C++ drop-in headers in include/gwn/ of this repository are thin inline wrappers
+ * over these symbols, so existing smallgwn callers keep their source code.
+ *
+ * Supported instantiation: Width = 4, Real = float, Index = uint32_t, MortonCode in {uint32_t,
+ * uint64_t}, Taylor Order in {0, 1, 2}.
+ *
+ * Memory layouts that cross this boundary are identical to smallgwn's:
+ *   - gwnb_child_f32        == gwn::gwn_bvh_child<float>      (32 B, include/gwn/gwn_bvh.cuh:55-103)
+ *   - gwnb_node4_f32        == gwn::gwn_bvh_node<4, float>    (128 B, :108-124)
+ *   - gwnb_triangle_f32     == gwn::gwn_bvh_triangle<float>   (36 B, :39-49)
+ *   - moment nodes          == gwn::gwn_bvh_moment_node<4, Order, float> field-SoA (:144-202)
+ * Objects own device memory allocated with cudaMallocAsync on the stream passed to the call that
+ * created them; gwnb_*_release frees it with cudaFreeAsync on the stream given to the release.
+ */
+#ifndef GWNB_H
+#define GWNB_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define GWNB_API __attribute__((visibility("default")))
+#else
+#define GWNB_API
+#endif
+
+/* cudaStream_t without pulling in the CUDA headers. */
+typedef struct CUstream_st *gwnb_stream_t;
+
+enum {
+    GWNB_OK = 0,
+    GWNB_INVALID_ARGUMENT = 1,
+    GWNB_CUDA_RUNTIME_ERROR = 2,
+    GWNB_INTERNAL_ERROR = 3,
+};
+
+enum { GWNB_METHOD_HPLOC = 0, GWNB_METHOD_LBVH = 1 };
+
+/* Precision of the exact near-field solid angle inside the Taylor traversal. */
+enum {
+    GWNB_NEAR_PLAIN = 0,       /* FP32 Van Oosterom-Strackee, as smallgwn evaluates it        */
+    GWNB_NEAR_COMPENSATED = 1, /* two-product compensated FP32, FP64 on flagged triangles    */
+};
+
+typedef struct gwnb_aabb_f32 {
+    float min_x, min_y, min_z, max_x, max_y, max_z;
+} gwnb_aabb_f32;
+
+typedef struct gwnb_child_f32 {
+    gwnb_aabb_f32 bounds;
+    uint64_t reference; /* bits 0-46 offset, bit 47 valid, bits 48-63 primitive count */
+} gwnb_child_f32;
+
+typedef struct gwnb_node4_f32 {
+    gwnb_child_f32 children[4];
+} gwnb_node4_f32;
+
+typedef struct gwnb_triangle_f32 {
+    float v0_x, v0_y, v0_z, e1_x, e1_y, e1_z, e2_x, e2_y, e2_z;
+} gwnb_triangle_f32;
+
+/* Device geometry view; mirrors gwn::gwn_geometry_accessor<float, uint32_t>
+ * (include/gwn/gwn_geometry.cuh:19-49). */
+typedef struct gwnb_geometry_f32 {
+    float *vertex_x, *vertex_y, *vertex_z;
+    uint64_t vertex_count;
+    uint32_t *tri_i0, *tri_i1, *tri_i2;
+    uint64_t triangle_count;
+} gwnb_geometry_f32;
+
+/* Library-owned derived state of a BVH (parent links, arrival counters, padded triangle records,
+ * device error word). Opaque to callers. */
+typedef struct gwnb_bvh_aux gwnb_bvh_aux;
+
+/* Device BVH view; field meaning mirrors gwn::gwn_bvh_accessor<4, float, uint32_t>
+ * (include/gwn/gwn_bvh.cuh:208-258). `node_capacity` is the allocated node count (>= node_count). */
+typedef struct gwnb_bvh4_f32 {
+    gwnb_node4_f32 *nodes;
+    uint64_t node_count;
+    uint64_t node_capacity;
+    uint32_t *primitive_indices;
+    gwnb_triangle_f32 *triangles;
+    uint64_t primitive_count;
+    gwnb_child_f32 root;
+    uint32_t internal_stack_bound;
+    uint32_t packed_stack_bound;
+    uint64_t revision;
+    gwnb_bvh_aux *aux;
+} gwnb_bvh4_f32;
+
+typedef struct gwnb_moment_aux gwnb_moment_aux;
+
+/* Device Taylor-moment view; mirrors gwn::gwn_bvh_moment_accessor<4, Order, float, uint32_t>
+ * (include/gwn/gwn_bvh.cuh:265-294). `nodes` holds gwn_bvh_moment_node<4, Order, float>. */
+typedef struct gwnb_moment4_f32 {
+    int order;
+    void *nodes;
+    uint64_t node_count;
+    uint64_t bvh_revision;
+    gwnb_moment_aux *aux;
+} gwnb_moment4_f32;
+
+/* Options of the Taylor batch beyond smallgwn's template parameters. */
+typedef struct gwnb_taylor_options {
+    int block_size;     /* smallgwn gwn_query_batch_config::block_size (0 = default 256)        */
+    int stack_capacity; /* smallgwn gwn_query_batch_config::stack_capacity (0 = default 64)     */
+    int sort_queries;   /* 1: Morton-order the batch internally for traversal coherence          */
+    int near_precision; /* GWNB_NEAR_PLAIN or GWNB_NEAR_COMPENSATED                               */
+    float fp64_threshold; /* compensated mode: |den| < threshold * |a||b||c| takes the FP64 path */
+} gwnb_taylor_options;
+
+/* ---- status ------------------------------------------------------------------------------ */
+
+/* Message of the most recent failing call on this host thread (smallgwn gwn_status::message,
+ * include/gwn/gwn_utils.cuh:212-283). */
+GWNB_API const char *gwnb_last_error_message(void);
+/* CUDA error code of the most recent GWNB_CUDA_RUNTIME_ERROR on this host thread. */
+GWNB_API int gwnb_last_cuda_error(void);
+/* Library version string. */
+GWNB_API const char *gwnb_version(void);
+
+/* ---- geometry (include/gwn/gwn_geometry.cuh:66-90) ---------------------------------------- */
+
+/* Replaces gwn::gwn_upload_geometry (include/gwn/gwn_geometry.cuh:66-72,
+ * detail/gwn_geometry_impl.cuh:183-206). Allocates a new view in *out; the caller releases any
+ * previous view (staging-and-swap keeps the previous object intact on failure). Synchronizes
+ * `stream` to validate indices, as smallgwn does. */
+GWNB_API int gwnb_geometry_upload_f32(gwnb_geometry_f32 *out, const float *x, const float *y, const float *z,
+                             uint64_t vertex_count, const uint32_t *i0, const uint32_t *i1,
+                             const uint32_t *i2, uint64_t triangle_count, gwnb_stream_t stream);
+
+/* Replaces gwn::gwn_update_geometry (include/gwn/gwn_geometry.cuh:85-90). Host positions,
+ * asynchronous. */
+GWNB_API int gwnb_geometry_update_f32(gwnb_geometry_f32 *geometry, const float *x, const float *y,
+                             const float *z, uint64_t vertex_count, gwnb_stream_t stream);
+
+/* Same as gwnb_geometry_update_f32 but the positions already live in device memory. */
+GWNB_API int gwnb_geometry_update_device_f32(gwnb_geometry_f32 *geometry, const float *x, const float *y,
+                                    const float *z, uint64_t vertex_count, gwnb_stream_t stream);
+
+/* Replaces gwn::detail::gwn_release_accessor (detail/gwn_geometry_impl.cuh:16-26). */
+GWNB_API void gwnb_geometry_release_f32(gwnb_geometry_f32 *geometry, gwnb_stream_t stream);
+
+/* ---- BVH build (include/gwn/gwn_bvh_build.cuh:15-39) ------------------------------------- */
+
+/* Replaces gwn::gwn_build_bvh<4, float, uint32_t, MortonCode> (include/gwn/gwn_bvh_build.cuh:34-39,
+ * detail/gwn_bvh_build_impl.cuh:44-274). method: GWNB_METHOD_HPLOC or GWNB_METHOD_LBVH;
+ * hploc_search_radius in [1, 8]; morton_bits 32 or 64. Writes a new view into *out. */
+GWNB_API int gwnb_bvh4_build_f32(const gwnb_geometry_f32 *geometry, int method, uint32_t hploc_search_radius,
+                        int morton_bits, gwnb_bvh4_f32 *out, gwnb_stream_t stream);
+
+/* Replaces gwn::detail::gwn_release_bvh_accessor (include/gwn/gwn_bvh.cuh:301-313). */
+GWNB_API void gwnb_bvh4_release_f32(gwnb_bvh4_f32 *bvh, gwnb_stream_t stream);
+
+/* Build stages exposed for parity checks. Output buffers are caller-owned device memory sized
+ * for triangle_count elements (binary arrays: triangle_count - 1).
+ * Replaces gwn::detail::gwn_bvh_build_preprocess (detail/gwn_bvh_build_common.cuh:371-381):
+ * sorted Morton codes (uint32 or uint64 per morton_bits), sorted primitive ids, sorted AABBs. */
+GWNB_API int gwnb_build_preprocess_f32(const gwnb_geometry_f32 *geometry, int morton_bits,
+                              void *sorted_codes, uint32_t *sorted_ids, gwnb_aabb_f32 *sorted_aabbs,
+                              gwnb_stream_t stream);
+
+/* Binary node as produced by the binary builders: (left index, left kind, right index, right
+ * kind), kind 1 = internal, 2 = leaf (detail/gwn_bvh_build_binary.cuh:13-28). */
+typedef struct gwnb_binary_node {
+    uint32_t left_index;
+    uint32_t left_kind;
+    uint32_t right_index;
+    uint32_t right_kind;
+} gwnb_binary_node;
+
+/* Replaces gwn::detail::gwn_bvh_build_binary_lbvh (detail/gwn_bvh_build_lbvh.cuh:19-99). */
+GWNB_API int gwnb_build_binary_lbvh(const void *sorted_codes, int morton_bits, uint64_t count,
+                           const gwnb_aabb_f32 *sorted_aabbs, gwnb_binary_node *nodes,
+                           uint32_t *internal_parent, gwnb_aabb_f32 *internal_bounds,
+                           gwnb_stream_t stream);
+
+/* Replaces gwn::detail::gwn_bvh_build_binary_hploc_impl (detail/gwn_bvh_build_hploc.cuh:480-622).
+ * Writes the root internal index to *root (device-to-host copy, synchronizes). */
+GWNB_API int gwnb_build_binary_hploc(const void *sorted_codes, int morton_bits, uint64_t count,
+                            const gwnb_aabb_f32 *sorted_aabbs, uint32_t search_radius,
+                            gwnb_binary_node *nodes, uint32_t *internal_parent,
+                            gwnb_aabb_f32 *internal_bounds, uint32_t *root, gwnb_stream_t stream);
+
+/* Stable LSD radix sort of (key, value) pairs over key bits [0, key_bits); onesweep passes.
+ * Stands in for cub::DeviceRadixSort::SortPairs at detail/gwn_bvh_build_common.cuh:332-347.
+ * keys are uint32 (key_bytes 4) or uint64 (key_bytes 8). values may be NULL (identity ids).
+ * Results go to keys_out / values_out. */
+GWNB_API int gwnb_radix_sort_pairs(const void *keys_in, void *keys_out, const uint32_t *values_in,
+                          uint32_t *values_out, uint64_t count, int key_bytes, int key_bits,
+                          gwnb_stream_t stream);
+
+/* ---- refit (include/gwn/gwn_bvh_refit.cuh:25-51) ----------------------------------------- */
+
+/* Replaces gwn::gwn_refit_bvh (include/gwn/gwn_bvh_refit.cuh:25-29,
+ * detail/gwn_bvh_refit_impl.cuh:194-352). Synchronizes to publish root bounds and errors, as
+ * smallgwn does. */
+GWNB_API int gwnb_bvh4_refit_f32(const gwnb_geometry_f32 *geometry, gwnb_bvh4_f32 *bvh, gwnb_stream_t stream);
+
+/* Stream-ordered refit with no host synchronization and no allocation after the first call on a
+ * BVH (capturable in a CUDA graph). Root bounds and errors stay on the device; read them with
+ * gwnb_bvh4_sync_status_f32. Has no smallgwn counterpart (smallgwn's refit always synchronizes). */
+GWNB_API int gwnb_bvh4_refit_async_f32(const gwnb_geometry_f32 *geometry, gwnb_bvh4_f32 *bvh,
+                              gwnb_stream_t stream);
+
+/* Synchronizes `stream`, copies the device-side root bounds into bvh->root.bounds and turns the
+ * device error word into a status. */
+GWNB_API int gwnb_bvh4_sync_status_f32(gwnb_bvh4_f32 *bvh, gwnb_stream_t stream);
+
+/* Replaces gwn::gwn_refit_bvh_moment<Order> (include/gwn/gwn_bvh_refit.cuh:36-51,
+ * detail/gwn_bvh_refit_moment_impl.cuh:137-279). Writes a new view into *out. */
+GWNB_API int gwnb_moment4_refit_f32(const gwnb_bvh4_f32 *bvh, int order, gwnb_moment4_f32 *out,
+                           gwnb_stream_t stream);
+
+/* Refit moments into an existing moment view (same BVH topology, new geometry) without
+ * allocation or host synchronization. Has no smallgwn counterpart. */
+GWNB_API int gwnb_moment4_refit_async_f32(const gwnb_bvh4_f32 *bvh, gwnb_moment4_f32 *moment,
+                                 gwnb_stream_t stream);
+
+/* Replaces gwn::detail::gwn_release_bvh_moment_accessor (include/gwn/gwn_bvh.cuh:316-322). */
+GWNB_API void gwnb_moment4_release_f32(gwnb_moment4_f32 *moment, gwnb_stream_t stream);
+
+/* Size in bytes of one gwn_bvh_moment_node<4, order, float>. */
+GWNB_API uint64_t gwnb_moment_node_bytes(int order);
+
+/* ---- queries (include/gwn/gwn_query.cuh) -------------------------------------------------- */
+
+/* Replaces gwn::gwn_compute_winding_number_exact_batch<Config> (include/gwn/gwn_query.cuh:308-346).
+ * query_* and output are device pointers of `count` floats. Asynchronous. */
+GWNB_API int gwnb_winding_exact_batch_f32(const gwnb_bvh4_f32 *bvh, const float *query_x,
+                                 const float *query_y, const float *query_z, float *output,
+                                 uint64_t count, int block_size, gwnb_stream_t stream);
+
+/* Replaces gwn::gwn_compute_winding_number_taylor_batch<Order, Config>
+ * (include/gwn/gwn_query.cuh:384-445). `options` may be NULL (defaults: block 256, stack 64,
+ * sorted queries, plain near field). Asynchronous. A traversal that would overflow its stack
+ * writes NaN and sets the BVH's device error word instead of trapping. */
+GWNB_API int gwnb_winding_taylor_batch_f32(const gwnb_bvh4_f32 *bvh, const gwnb_moment4_f32 *moment,
+                                  const float *query_x, const float *query_y, const float *query_z,
+                                  float *output, uint64_t count, float accuracy_scale,
+                                  const gwnb_taylor_options *options, gwnb_stream_t stream);
+
+/* Replaces gwn::gwn_compute_winding_gradient_taylor_batch<Order, Config>
+ * (include/gwn/gwn_query.cuh:688-756): dw/dq of the Taylor winding number. */
+GWNB_API int gwnb_winding_gradient_taylor_batch_f32(const gwnb_bvh4_f32 *bvh,
+                                           const gwnb_moment4_f32 *moment, const float *query_x,
+                                           const float *query_y, const float *query_z,
+                                           float *grad_x, float *grad_y, float *grad_z,
+                                           uint64_t count, float accuracy_scale,
+                                           const gwnb_taylor_options *options,
+                                           gwnb_stream_t stream);
+
+/* Per-query traversal statistics of the Taylor batch (diagnostics; nodes entered, far-field
+ * child evaluations, exact near-field triangles). Writes three uint32 arrays of `count`. */
+GWNB_API int gwnb_winding_taylor_stats_f32(const gwnb_bvh4_f32 *bvh, const gwnb_moment4_f32 *moment,
+                                  const float *query_x, const float *query_y, const float *query_z,
+                                  uint64_t count, float accuracy_scale, uint32_t *nodes_entered,
+                                  uint32_t *far_evaluations, uint32_t *near_triangles,
+                                  gwnb_stream_t stream);
+
+/* Number of FP64 fallbacks taken by the last compensated Taylor batch on this BVH (device
+ * counter read back with a synchronization). */
+GWNB_API int gwnb_bvh4_fp64_fallback_count(const gwnb_bvh4_f32 *bvh, uint64_t *count, gwnb_stream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GWNB_H */

@@ -1,0 +1,417 @@
+"""The oracle: CPU restatement of smallgwn's winding-number path, plus smallgwn's own kernels.
+
+TEST INFRASTRUCTURE ONLY -- imported by tests/, __graft_entry__.smoke() and bench.py's CPU
+baseline, never by the product (smallgwn_b200/). Two libraries back it:
+  * _build/liboracle.so   gwn_oracle.c (C, OpenMP): exact winding FP32/FP64, Morton codes, stable
+                          sort, Karras LBVH, H-PLOC, BVH4 collapse, triangle records, Taylor
+                          moments and Taylor traversal with per-query counts;
+  * _ref/libgwnref.so     smallgwn's CUDA implementation compiled from its headers (ref_shim.cu),
+                          present when the reference project was available at build time.
+Parity pins: tests/test_oracle.py checks the C restatement against analytic known answers and
+against golden vectors recorded from smallgwn's own kernels (tests/golden/).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+_ORACLE = None
+_REF = None
+
+NODE_DTYPE = np.dtype([("bounds", np.float32, (6,)), ("reference", np.uint64)])
+BNODE_DTYPE = np.dtype((np.uint32, 4))
+
+
+def _p(a: np.ndarray | None):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def lib() -> C.CDLL:
+    global _ORACLE
+    if _ORACLE is None:
+        from .build import build_oracle
+
+        path = build_oracle()
+        _ORACLE = C.CDLL(str(path))
+        _ORACLE.oracle_max_threads.restype = C.c_int
+        _ORACLE.oracle_hploc.restype = C.c_int
+        _ORACLE.oracle_collapse.restype = C.c_int
+        _ORACLE.oracle_triangles.restype = C.c_int
+    return _ORACLE
+
+
+def ref_lib() -> C.CDLL | None:
+    """smallgwn's own kernels (oracle/_ref/libgwnref.so) or None when not built."""
+    global _REF
+    if _REF is None:
+        path = HERE / "_ref" / "libgwnref.so"
+        if not path.exists():
+            return None
+        _REF = C.CDLL(str(path))
+        _REF.ref_last_message.restype = C.c_char_p
+    return _REF
+
+
+def max_threads() -> int:
+    return int(lib().oracle_max_threads())
+
+
+def _f32(a):
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+def _u32(a):
+    return np.ascontiguousarray(a, dtype=np.uint32)
+
+
+def exact_winding(mesh: dict, qx, qy, qz, threads: int = 0, fp64: bool = False) -> np.ndarray:
+    """tests/reference_cpu.cuh:84-114 restated: brute-force exact winding, FP32 or FP64."""
+    threads = threads or max_threads()
+    i0, i1, i2 = _u32(mesh["i0"]), _u32(mesh["i1"]), _u32(mesh["i2"])
+    n = len(qx)
+    if fp64:
+        x, y, z = (np.ascontiguousarray(mesh[k], dtype=np.float64) for k in "xyz")
+        q = [np.ascontiguousarray(v, dtype=np.float64) for v in (qx, qy, qz)]
+        out = np.empty(n, np.float64)
+        lib().oracle_exact_winding_f64(_p(x), _p(y), _p(z), C.c_uint64(x.size), _p(i0), _p(i1), _p(i2),
+                                       C.c_uint64(i0.size), _p(q[0]), _p(q[1]), _p(q[2]), _p(out),
+                                       C.c_uint64(n), C.c_int(threads))
+        return out
+    x, y, z = (_f32(mesh[k]) for k in "xyz")
+    q = [_f32(v) for v in (qx, qy, qz)]
+    out = np.empty(n, np.float32)
+    lib().oracle_exact_winding_f32(_p(x), _p(y), _p(z), C.c_uint64(x.size), _p(i0), _p(i1), _p(i2),
+                                   C.c_uint64(i0.size), _p(q[0]), _p(q[1]), _p(q[2]), _p(out), C.c_uint64(n),
+                                   C.c_int(threads))
+    return out
+
+
+def exact_records(tris: np.ndarray, qx, qy, qz, threads: int = 0) -> np.ndarray:
+    """Exact winding over leaf-ordered records (gwn_query_winding_impl.cuh:377-389)."""
+    threads = threads or max_threads()
+    t = np.ascontiguousarray(tris, dtype=np.float32)
+    q = [_f32(v) for v in (qx, qy, qz)]
+    out = np.empty(len(q[0]), np.float32)
+    lib().oracle_exact_records(_p(t), C.c_uint64(t.shape[0]), _p(q[0]), _p(q[1]), _p(q[2]), C.c_uint64(len(out)),
+                               _p(out), C.c_int(threads))
+    return out
+
+
+def morton(mesh: dict, bits: int = 64) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
+    """Triangle AABBs (nt, 6), Morton codes (uint64 storage) and scene (min, max, inv)."""
+    x, y, z = (_f32(mesh[k]) for k in "xyz")
+    i0, i1, i2 = _u32(mesh["i0"]), _u32(mesh["i1"]), _u32(mesh["i2"])
+    nt = i0.size
+    aabbs = np.empty((nt, 6), np.float32)
+    codes = np.empty(nt, np.uint64)
+    scene = np.empty(9, np.float32)
+    lib().oracle_scene_and_morton(_p(x), _p(y), _p(z), C.c_uint64(x.size), _p(i0), _p(i1), _p(i2), C.c_uint64(nt),
+                                  C.c_int(bits), _p(aabbs), _p(codes), _p(scene))
+    return aabbs, codes, scene
+
+
+def sort_pairs(codes: np.ndarray) -> tuple[np.ndarray, np.ndarray]:
+    c = np.ascontiguousarray(codes, dtype=np.uint64)
+    out = np.empty_like(c)
+    ids = np.empty(c.size, np.uint32)
+    lib().oracle_sort_pairs(_p(c), C.c_uint64(c.size), _p(out), _p(ids))
+    return out, ids
+
+
+def karras(sorted_codes: np.ndarray, bits: int) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
+    c = np.ascontiguousarray(sorted_codes, dtype=np.uint64)
+    n = c.size
+    nodes = np.zeros((max(n - 1, 0), 4), np.uint32)
+    ip = np.empty(max(n - 1, 0), np.uint32)
+    lp = np.empty(n, np.uint32)
+    lib().oracle_karras(_p(c), C.c_int(bits), C.c_uint64(n), _p(nodes), _p(ip), _p(lp))
+    return nodes, ip, lp
+
+
+def binary_bounds(nodes: np.ndarray, leaf_aabbs: np.ndarray, root: int) -> np.ndarray:
+    n = leaf_aabbs.shape[0]
+    out = np.zeros((max(n - 1, 0), 6), np.float32)
+    lib().oracle_binary_bounds(_p(np.ascontiguousarray(nodes, np.uint32)), C.c_uint64(n),
+                               _p(np.ascontiguousarray(leaf_aabbs, np.float32)), C.c_uint32(root), _p(out))
+    return out
+
+
+def hploc(sorted_codes: np.ndarray, bits: int, leaf_aabbs: np.ndarray, radius: int):
+    c = np.ascontiguousarray(sorted_codes, dtype=np.uint64)
+    n = c.size
+    nodes = np.zeros((max(n - 1, 0), 4), np.uint32)
+    bounds = np.zeros((max(n - 1, 0), 6), np.float32)
+    root = C.c_uint32(0)
+    rc = lib().oracle_hploc(_p(c), C.c_int(bits), C.c_uint64(n), _p(np.ascontiguousarray(leaf_aabbs, np.float32)),
+                            C.c_uint32(radius), _p(nodes), _p(bounds), C.byref(root))
+    if rc != 0:
+        raise RuntimeError("oracle H-PLOC did not converge")
+    return nodes, bounds, int(root.value)
+
+
+def collapse(bin_nodes: np.ndarray, bin_bounds: np.ndarray, leaf_aabbs: np.ndarray, root: int):
+    n = leaf_aabbs.shape[0]
+    out = np.zeros((max(n - 1, 1), 4), NODE_DTYPE)
+    cnt = C.c_uint64(0)
+    ib = C.c_uint32(0)
+    pb = C.c_uint32(0)
+    lib().oracle_collapse(_p(np.ascontiguousarray(bin_nodes, np.uint32)),
+                          _p(np.ascontiguousarray(bin_bounds, np.float32)),
+                          _p(np.ascontiguousarray(leaf_aabbs, np.float32)), C.c_uint64(n), C.c_uint32(root), _p(out),
+                          C.byref(cnt), C.byref(ib), C.byref(pb))
+    return out[: cnt.value], int(ib.value), int(pb.value)
+
+
+def triangles(mesh: dict, ids: np.ndarray) -> np.ndarray:
+    x, y, z = (_f32(mesh[k]) for k in "xyz")
+    i0, i1, i2 = _u32(mesh["i0"]), _u32(mesh["i1"]), _u32(mesh["i2"])
+    ids = _u32(ids)
+    out = np.zeros((ids.size, 9), np.float32)
+    bad = lib().oracle_triangles(_p(x), _p(y), _p(z), C.c_uint64(x.size), _p(i0), _p(i1), _p(i2), C.c_uint64(i0.size),
+                                 _p(ids), _p(out))
+    if bad:
+        raise ValueError("invalid triangle index")
+    return out
+
+
+def moments(order: int, nodes: np.ndarray, tris: np.ndarray) -> np.ndarray:
+    """smallgwn-layout moment nodes, shape (nodes, fields, 4)."""
+    F = {0: 7, 1: 13, 2: 23}[order]
+    nd = np.ascontiguousarray(nodes.reshape(-1, 4), dtype=NODE_DTYPE)
+    out = np.zeros((nd.shape[0], F, 4), np.float32)
+    t = np.ascontiguousarray(tris, np.float32)
+    lib().oracle_moments(C.c_int(order), _p(nd), C.c_uint64(nd.shape[0]), _p(t), C.c_uint64(t.shape[0]), _p(out))
+    return out
+
+
+def taylor(order: int, nodes: np.ndarray, mom: np.ndarray, tris: np.ndarray, root_ref: int, qx, qy, qz,
+           beta: float = 2.0, stack_capacity: int = 256, threads: int = 0, stats: bool = False):
+    """gwn_winding_taylor_impl restated; with stats also (nodes entered, far children, exact tris)."""
+    threads = threads or max_threads()
+    nd = np.ascontiguousarray(nodes.reshape(-1, 4), dtype=NODE_DTYPE)
+    m = np.ascontiguousarray(mom, np.float32)
+    t = np.ascontiguousarray(tris, np.float32)
+    q = [_f32(v) for v in (qx, qy, qz)]
+    n = q[0].size
+    out = np.empty(n, np.float32)
+    st = np.zeros((n, 3), np.uint32) if stats else None
+    lib().oracle_taylor(C.c_int(order), _p(nd), C.c_uint64(nd.shape[0]), _p(m), _p(t), C.c_uint64(t.shape[0]),
+                        C.c_uint64(root_ref), _p(q[0]), _p(q[1]), _p(q[2]), C.c_uint64(n), C.c_float(beta),
+                        C.c_int(stack_capacity), _p(out), _p(st), C.c_int(threads))
+    return (out, st) if stats else out
+
+
+def build_lbvh(mesh: dict, bits: int = 64) -> dict:
+    """Full CPU pipeline: Morton, stable sort, Karras, bounds, BVH4 collapse, triangle records."""
+    aabbs, codes, scene = morton(mesh, bits)
+    sc, ids = sort_pairs(codes)
+    saabb = aabbs[ids]
+    n = ids.size
+    out = {"sorted_codes": sc, "sorted_ids": ids, "sorted_aabbs": saabb, "scene": scene}
+    if n == 1:
+        out.update(nodes=np.zeros((0, 4), NODE_DTYPE), internal_stack_bound=0, packed_stack_bound=0,
+                   root_reference=(1 << 47) | (1 << 48))
+    else:
+        bn, ip, lp = karras(sc, bits)
+        bb = binary_bounds(bn, saabb, 0)
+        nodes, ib, pb = collapse(bn, bb, saabb, 0)
+        out.update(binary_nodes=bn, binary_bounds=bb, nodes=nodes, internal_stack_bound=ib, packed_stack_bound=pb,
+                   root_reference=(1 << 47))
+    out["triangles"] = triangles(mesh, ids)
+    return out
+
+
+# ---- smallgwn's own kernels (oracle/_ref) -------------------------------------------------------
+
+
+class Reference:
+    """Handle on smallgwn's CUDA implementation for one mesh (needs a GPU and oracle/_ref)."""
+
+    def __init__(self, mesh: dict):
+        self.lib = ref_lib()
+        if self.lib is None:
+            raise RuntimeError("oracle/_ref/libgwnref.so is not built")
+        self.mesh = mesh
+        x, y, z = (_f32(mesh[k]) for k in "xyz")
+        i0, i1, i2 = _u32(mesh["i0"]), _u32(mesh["i1"]), _u32(mesh["i2"])
+        self._keep = (x, y, z, i0, i1, i2)
+        h = C.c_void_p()
+        self._check(self.lib.ref_create(_p(x), _p(y), _p(z), C.c_uint64(x.size), _p(i0), _p(i1), _p(i2),
+                                        C.c_uint64(i0.size), C.byref(h)))
+        self.h = h
+
+    def _check(self, rc: int) -> None:
+        if rc != 0:
+            raise RuntimeError(f"reference call failed ({rc}): {self.lib.ref_last_message().decode()}")
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.ref_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def build(self, method: int = 1, radius: int = 8, bits: int = 64) -> None:
+        self._check(self.lib.ref_build(self.h, C.c_int(method), C.c_uint32(radius), C.c_int(bits)))
+
+    def bvh(self) -> dict:
+        nn = C.c_uint64()
+        ib = C.c_uint32()
+        pb = C.c_uint32()
+        rr = C.c_uint64()
+        rb = np.zeros(6, np.float32)
+        self._check(self.lib.ref_bvh_info(self.h, C.byref(nn), C.byref(ib), C.byref(pb), C.byref(rr), _p(rb)))
+        nt = self._keep[3].size
+        nodes = np.zeros((nn.value, 4), NODE_DTYPE)
+        prims = np.zeros(nt, np.uint32)
+        tris = np.zeros((nt, 9), np.float32)
+        self._check(self.lib.ref_bvh_copy(self.h, _p(nodes), _p(prims), _p(tris)))
+        return {"nodes": nodes, "primitive_indices": prims, "triangles": tris, "root_reference": rr.value,
+                "root_bounds": rb, "internal_stack_bound": ib.value, "packed_stack_bound": pb.value}
+
+    def moments(self, order: int) -> np.ndarray:
+        self._check(self.lib.ref_moment(self.h, C.c_int(order)))
+        F = {0: 7, 1: 13, 2: 23}[order]
+        nn = C.c_uint64()
+        dummy = C.c_uint32()
+        rr = C.c_uint64()
+        rb = np.zeros(6, np.float32)
+        self._check(self.lib.ref_bvh_info(self.h, C.byref(nn), C.byref(dummy), C.byref(dummy), C.byref(rr), _p(rb)))
+        out = np.zeros((nn.value, F, 4), np.float32)
+        self._check(self.lib.ref_moment_copy(self.h, C.c_int(order), _p(out)))
+        return out
+
+    def exact(self, qx, qy, qz) -> np.ndarray:
+        q = [_f32(v) for v in (qx, qy, qz)]
+        out = np.empty(q[0].size, np.float32)
+        self._check(self.lib.ref_exact(self.h, _p(q[0]), _p(q[1]), _p(q[2]), _p(out), C.c_uint64(out.size)))
+        return out
+
+    def taylor(self, order: int, qx, qy, qz, beta: float = 2.0) -> np.ndarray:
+        q = [_f32(v) for v in (qx, qy, qz)]
+        out = np.empty(q[0].size, np.float32)
+        self._check(self.lib.ref_taylor(self.h, C.c_int(order), _p(q[0]), _p(q[1]), _p(q[2]), _p(out),
+                                        C.c_uint64(out.size), C.c_float(beta)))
+        return out
+
+    def time_taylor(self, order: int, qx, qy, qz, beta: float, warmup: int, iters: int) -> float:
+        q = [_f32(v) for v in (qx, qy, qz)]
+        ms = C.c_float()
+        self._check(self.lib.ref_time_taylor(self.h, C.c_int(order), _p(q[0]), _p(q[1]), _p(q[2]),
+                                             C.c_uint64(q[0].size), C.c_float(beta), C.c_int(warmup), C.c_int(iters),
+                                             C.byref(ms)))
+        return float(ms.value)
+
+    def time_exact(self, qx, qy, qz, warmup: int, iters: int) -> float:
+        q = [_f32(v) for v in (qx, qy, qz)]
+        ms = C.c_float()
+        self._check(self.lib.ref_time_exact(self.h, _p(q[0]), _p(q[1]), _p(q[2]), C.c_uint64(q[0].size),
+                                            C.c_int(warmup), C.c_int(iters), C.byref(ms)))
+        return float(ms.value)
+
+    def time_build(self, method: int, radius: int, bits: int, iters: int) -> float:
+        ms = C.c_float()
+        self._check(self.lib.ref_time_build(self.h, C.c_int(method), C.c_uint32(radius), C.c_int(bits),
+                                            C.c_int(iters), C.byref(ms)))
+        return float(ms.value)
+
+    def update_refit(self, x, y, z) -> None:
+        xs, ys, zs = (_f32(v) for v in (x, y, z))
+        self._check(self.lib.ref_update_refit(self.h, _p(xs), _p(ys), _p(zs), C.c_uint64(xs.size)))
+
+    def preprocess(self, bits: int = 64):
+        nt = self._keep[3].size
+        codes = np.zeros(nt, np.uint64)
+        ids = np.zeros(nt, np.uint32)
+        aabbs = np.zeros((nt, 6), np.float32)
+        self._check(self.lib.ref_preprocess(self.h, C.c_int(bits), _p(codes), _p(ids), _p(aabbs)))
+        return codes, ids, aabbs
+
+
+def ref_binary(method: int, bits: int, sorted_codes: np.ndarray, sorted_aabbs: np.ndarray, radius: int = 8):
+    lib_ = ref_lib()
+    if lib_ is None:
+        raise RuntimeError("oracle/_ref/libgwnref.so is not built")
+    c = np.ascontiguousarray(sorted_codes, np.uint64)
+    a = np.ascontiguousarray(sorted_aabbs, np.float32)
+    n = c.size
+    nodes = np.zeros((n - 1, 4), np.uint32)
+    bounds = np.zeros((n - 1, 6), np.float32)
+    root = C.c_uint32()
+    rc = lib_.ref_binary(C.c_int(method), C.c_int(bits), C.c_uint64(n), _p(c), _p(a), C.c_uint32(radius), _p(nodes),
+                         _p(bounds), C.byref(root))
+    if rc != 0:
+        raise RuntimeError(f"reference binary build failed: {lib_.ref_last_message().decode()}")
+    return nodes, bounds, int(root.value)
+
+
+def ref_exact_f64(mesh: dict, qx, qy, qz) -> np.ndarray:
+    lib_ = ref_lib()
+    if lib_ is None:
+        raise RuntimeError("oracle/_ref/libgwnref.so is not built")
+    x, y, z = (np.ascontiguousarray(mesh[k], dtype=np.float64) for k in "xyz")
+    i0, i1, i2 = _u32(mesh["i0"]), _u32(mesh["i1"]), _u32(mesh["i2"])
+    q = [np.ascontiguousarray(v, dtype=np.float64) for v in (qx, qy, qz)]
+    out = np.empty(q[0].size, np.float64)
+    rc = lib_.ref_exact_f64(_p(x), _p(y), _p(z), C.c_uint64(x.size), _p(i0), _p(i1), _p(i2), C.c_uint64(i0.size),
+                            _p(q[0]), _p(q[1]), _p(q[2]), _p(out), C.c_uint64(out.size))
+    if rc != 0:
+        raise RuntimeError(f"reference FP64 exact failed: {lib_.ref_last_message().decode()}")
+    return out
+
+
+# ---- canonical forms for comparisons up to node numbering -----------------------------------------
+
+
+def canonical_wide(nodes: np.ndarray, root_ref: int) -> list:
+    """Nested tuple of (child kind, primitive offset/count or subtree) per slot, depth first."""
+    import sys
+
+    sys.setrecursionlimit(100000)
+    nd = nodes.reshape(-1, 4)
+
+    def walk(i: int):
+        res = []
+        for s in range(4):
+            r = int(nd[i, s]["reference"])
+            if not (r >> 47) & 1:
+                res.append(None)
+            elif (r >> 48) == 0:
+                res.append(walk(r & ((1 << 47) - 1)))
+            else:
+                res.append(("L", r & ((1 << 47) - 1), r >> 48))
+        return tuple(res)
+
+    if (root_ref >> 48) != 0:
+        return [("L", root_ref & ((1 << 47) - 1), root_ref >> 48)]
+    return [walk(root_ref & ((1 << 47) - 1))]
+
+
+def binary_leaf_sets(nodes: np.ndarray, root: int) -> set:
+    """Set of frozensets of leaf ids under every internal node (numbering independent)."""
+    nd = np.asarray(nodes, np.uint32).reshape(-1, 4)
+    n = nd.shape[0]
+    order = []
+    stack = [root]
+    while stack:
+        v = stack.pop()
+        order.append(v)
+        if nd[v, 1] == 1:
+            stack.append(int(nd[v, 0]))
+        if nd[v, 3] == 1:
+            stack.append(int(nd[v, 2]))
+    leaves = {}
+    for v in reversed(order):
+        s = []
+        for idx, kind in ((nd[v, 0], nd[v, 1]), (nd[v, 2], nd[v, 3])):
+            s += [int(idx)] if kind == 2 else leaves[int(idx)]
+        leaves[v] = s
+    assert len(order) == n, "binary tree does not reach every internal node"
+    return {frozenset(v) for v in leaves.values()}

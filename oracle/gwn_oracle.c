@@ -1,0 +1,990 @@
+/*
+ * gwn_oracle.c -- CPU restatement of smallgwn's winding-number path.
+ *
+ * TEST INFRASTRUCTURE ONLY. This file is the parity checker for the CUDA library: only tests/,
+ * __graft_entry__.smoke() and the CPU-baseline leg of bench.py may load it. Nothing in the
+ * product path (smallgwn_b200/, include/) calls it.
+ *
+ * Every function cites the smallgwn file:line it restates (paths relative to that project).
+ * Compiled with -ffp-contract=off so float arithmetic is plain IEEE single precision; the
+ * topology-deciding arithmetic (Morton quantisation, half areas) therefore matches the CUDA
+ * library bit for bit.
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+typedef struct {
+    float min_x, min_y, min_z, max_x, max_y, max_z;
+} o_aabb;
+
+typedef struct {
+    o_aabb bounds;
+    uint64_t reference;
+} o_child;
+
+typedef struct {
+    o_child c[4];
+} o_node4;
+
+typedef struct {
+    float v0_x, v0_y, v0_z, e1_x, e1_y, e1_z, e2_x, e2_y, e2_z;
+} o_tri;
+
+typedef struct {
+    uint32_t li, lk, ri, rk; /* kind 1 = internal, 2 = leaf */
+} o_bnode;
+
+#define K_INTERNAL 1u
+#define K_LEAF 2u
+#define INV32 0xffffffffu
+#define OFFSET_MASK ((((uint64_t)1) << 47) - 1)
+#define VALID_BIT (((uint64_t)1) << 47)
+
+static inline int ref_valid(uint64_t r) { return (r & VALID_BIT) != 0; }
+static inline uint32_t ref_count(uint64_t r) { return (uint32_t)(r >> 48); }
+static inline int ref_internal(uint64_t r) { return ref_valid(r) && ref_count(r) == 0; }
+static inline int ref_leaf(uint64_t r) { return ref_valid(r) && ref_count(r) != 0; }
+static inline uint64_t ref_offset(uint64_t r) { return r & OFFSET_MASK; }
+static inline uint64_t make_ref(uint64_t off, uint64_t cnt) { return VALID_BIT | off | (cnt << 48); }
+
+/* std::min / std::max operand order (include/gwn/detail/gwn_bvh_build_common.cuh:90-96). */
+static inline float fmin_r(float a, float b) { return (b < a) ? b : a; }
+static inline float fmax_r(float a, float b) { return (a < b) ? b : a; }
+
+static o_aabb aabb_union(o_aabb l, o_aabb r) {
+    o_aabb u = {fmin_r(l.min_x, r.min_x), fmin_r(l.min_y, r.min_y), fmin_r(l.min_z, r.min_z),
+                fmax_r(l.max_x, r.max_x), fmax_r(l.max_y, r.max_y), fmax_r(l.max_z, r.max_z)};
+    return u;
+}
+
+/* gwn_aabb_half_area, detail/gwn_bvh_build_common.cuh:98-104 (products, then left-to-right sum). */
+static float half_area(o_aabb b) {
+    float dx = fmax_r(b.max_x - b.min_x, 0.0f);
+    float dy = fmax_r(b.max_y - b.min_y, 0.0f);
+    float dz = fmax_r(b.max_z - b.min_z, 0.0f);
+    float p0 = dx * dy, p1 = dy * dz, p2 = dz * dx;
+    float s = p0 + p1;
+    return s + p2;
+}
+
+/* ---------------------------------------------------------------------------------------------- */
+/* Exact winding: tests/reference_cpu.cuh:22-82 (normalise, Van Oosterom-Strackee, zero for a     */
+/* vertex hit or a vanishing numerator), summed over every triangle, divided by 4 pi.             */
+
+#define DEFINE_EXACT(T, SUFFIX, SQRT, ATAN2)                                                      \
+    static T solid_angle_##SUFFIX(T ax, T ay, T az, T bx, T by, T bz, T cx, T cy, T cz, T qx, T qy, \
+                                  T qz) {                                                          \
+        T qax = ax - qx, qay = ay - qy, qaz = az - qz;                                            \
+        T qbx = bx - qx, qby = by - qy, qbz = bz - qz;                                            \
+        T qcx = cx - qx, qcy = cy - qy, qcz = cz - qz;                                            \
+        T la = SQRT(qax * qax + qay * qay + qaz * qaz);                                           \
+        T lb = SQRT(qbx * qbx + qby * qby + qbz * qbz);                                           \
+        T lc = SQRT(qcx * qcx + qcy * qcy + qcz * qcz);                                           \
+        if (la == (T)0 || lb == (T)0 || lc == (T)0)                                               \
+            return (T)0;                                                                          \
+        qax /= la; qay /= la; qaz /= la;                                                          \
+        qbx /= lb; qby /= lb; qbz /= lb;                                                          \
+        qcx /= lc; qcy /= lc; qcz /= lc;                                                          \
+        T ux = qbx - qax, uy = qby - qay, uz = qbz - qaz;                                         \
+        T vx = qcx - qax, vy = qcy - qay, vz = qcz - qaz;                                         \
+        T crx = uy * vz - uz * vy, cry = uz * vx - ux * vz, crz = ux * vy - uy * vx;              \
+        T num = qax * crx + qay * cry + qaz * crz;                                                \
+        if (num == (T)0)                                                                          \
+            return (T)0;                                                                          \
+        T den = (T)1 + (qax * qbx + qay * qby + qaz * qbz) + (qax * qcx + qay * qcy + qaz * qcz) + \
+                (qbx * qcx + qby * qcy + qbz * qcz);                                              \
+        return (T)2 * ATAN2(num, den);                                                            \
+    }                                                                                             \
+    void oracle_exact_winding_##SUFFIX(const T *vx, const T *vy, const T *vz, uint64_t nv,         \
+                                       const uint32_t *i0, const uint32_t *i1, const uint32_t *i2, \
+                                       uint64_t nt, const T *qx, const T *qy, const T *qz, T *out, \
+                                       uint64_t nq, int threads) {                                 \
+        const T k_pi = (T)3.141592653589793238462643383279502884L;                                 \
+        (void)threads;                                                                            \
+        _Pragma("omp parallel for schedule(dynamic, 64) num_threads(threads > 0 ? threads : 1)")   \
+        for (int64_t q = 0; q < (int64_t)nq; ++q) {                                               \
+            T sum = (T)0;                                                                         \
+            for (uint64_t t = 0; t < nt; ++t) {                                                   \
+                uint32_t a = i0[t], b = i1[t], c = i2[t];                                         \
+                if (a >= nv || b >= nv || c >= nv)                                                \
+                    continue;                                                                     \
+                sum += solid_angle_##SUFFIX(vx[a], vy[a], vz[a], vx[b], vy[b], vz[b], vx[c], vy[c], \
+                                            vz[c], qx[q], qy[q], qz[q]);                          \
+            }                                                                                     \
+            out[q] = sum / ((T)4 * k_pi);                                                         \
+        }                                                                                         \
+    }
+
+DEFINE_EXACT(float, f32, sqrtf, atan2f)
+DEFINE_EXACT(double, f64, sqrt, atan2)
+
+/* Exact winding over leaf-ordered triangle records, gwn_winding_number_exact_impl
+ * (detail/gwn_query_winding_impl.cuh:377-389): vertices b = v0 + e1, c = v0 + e2. */
+static float record_solid_angle(const o_tri *t, float qx, float qy, float qz) {
+    return solid_angle_f32(t->v0_x, t->v0_y, t->v0_z, t->v0_x + t->e1_x, t->v0_y + t->e1_y,
+                           t->v0_z + t->e1_z, t->v0_x + t->e2_x, t->v0_y + t->e2_y, t->v0_z + t->e2_z,
+                           qx, qy, qz);
+}
+
+/* ---------------------------------------------------------------------------------------------- */
+/* Scene bounds, triangle AABBs and Morton codes: detail/gwn_bvh_build_common.cuh:22-88 (traits,  */
+/* clamp, quantise, interleave), :157-214 (per-triangle functor), :243-274 (scene inverse).        */
+
+static uint32_t expand10(uint32_t v) {
+    uint32_t x = v & 0x000003ffu;
+    x = (x | (x << 16)) & 0x030000ffu;
+    x = (x | (x << 8)) & 0x0300f00fu;
+    x = (x | (x << 4)) & 0x030c30c3u;
+    x = (x | (x << 2)) & 0x09249249u;
+    return x;
+}
+static uint64_t expand21(uint64_t v) {
+    uint64_t x = v & 0x1fffffu;
+    x = (x | (x << 32)) & 0x1f00000000ffffull;
+    x = (x | (x << 16)) & 0x1f0000ff0000ffull;
+    x = (x | (x << 8)) & 0x100f00f00f00f00full;
+    x = (x | (x << 4)) & 0x10c30c30c30c30c3ull;
+    x = (x | (x << 2)) & 0x1249249249249249ull;
+    return x;
+}
+static float clamp01(float v) {
+    if (v < 0.0f)
+        return 0.0f;
+    if (v > 1.0f)
+        return 1.0f;
+    return v;
+}
+
+/* bits = 32 or 64; codes are written as uint64 either way. scene_out (9 floats) = min, max, inv. */
+void oracle_scene_and_morton(const float *vx, const float *vy, const float *vz, uint64_t nv,
+                             const uint32_t *i0, const uint32_t *i1, const uint32_t *i2, uint64_t nt,
+                             int bits, o_aabb *aabbs, uint64_t *codes, float *scene_out) {
+    float mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (uint64_t i = 0; i < nv; ++i) {
+        float v[3] = {vx[i], vy[i], vz[i]};
+        for (int a = 0; a < 3; ++a) {
+            mn[a] = fmin_r(mn[a], v[a]);
+            mx[a] = fmax_r(mx[a], v[a]);
+        }
+    }
+    float inv[3];
+    for (int a = 0; a < 3; ++a)
+        inv[a] = (mx[a] == mn[a]) ? 1.0f : 1.0f / (mx[a] - mn[a]);
+    if (scene_out) {
+        for (int a = 0; a < 3; ++a) {
+            scene_out[a] = mn[a];
+            scene_out[3 + a] = mx[a];
+            scene_out[6 + a] = inv[a];
+        }
+    }
+    for (uint64_t t = 0; t < nt; ++t) {
+        uint32_t a = i0[t], b = i1[t], c = i2[t];
+        if (a >= nv || b >= nv || c >= nv) {
+            memset(&aabbs[t], 0, sizeof(o_aabb));
+            codes[t] = 0;
+            continue;
+        }
+        o_aabb bb = {fmin_r(vx[a], fmin_r(vx[b], vx[c])), fmin_r(vy[a], fmin_r(vy[b], vy[c])),
+                     fmin_r(vz[a], fmin_r(vz[b], vz[c])), fmax_r(vx[a], fmax_r(vx[b], vx[c])),
+                     fmax_r(vy[a], fmax_r(vy[b], vy[c])), fmax_r(vz[a], fmax_r(vz[b], vz[c]))};
+        aabbs[t] = bb;
+        float ctr[3] = {(bb.min_x + bb.max_x) * 0.5f, (bb.min_y + bb.max_y) * 0.5f,
+                        (bb.min_z + bb.max_z) * 0.5f};
+        if (bits == 32) {
+            uint32_t q[3];
+            for (int k = 0; k < 3; ++k)
+                q[k] = (uint32_t)(clamp01((ctr[k] - mn[k]) * inv[k]) * 1023.0f);
+            codes[t] = (expand10(q[0]) << 2) | (expand10(q[1]) << 1) | expand10(q[2]);
+        } else {
+            uint64_t q[3];
+            for (int k = 0; k < 3; ++k)
+                q[k] = (uint64_t)(clamp01((ctr[k] - mn[k]) * inv[k]) * 2097151.0f);
+            codes[t] = (expand21(q[0]) << 2) | (expand21(q[1]) << 1) | expand21(q[2]);
+        }
+    }
+}
+
+/* Stable sort of (code, id) pairs -- the permutation cub::DeviceRadixSort::SortPairs produces
+ * for keys over bits [0, 64) at detail/gwn_bvh_build_common.cuh:332-347. LSD radix, 16-bit digits. */
+void oracle_sort_pairs(const uint64_t *codes, uint64_t n, uint64_t *sorted, uint32_t *ids) {
+    uint64_t *k0 = (uint64_t *)malloc(n * sizeof(uint64_t)), *k1 = (uint64_t *)malloc(n * sizeof(uint64_t));
+    uint32_t *v0 = (uint32_t *)malloc(n * sizeof(uint32_t)), *v1 = (uint32_t *)malloc(n * sizeof(uint32_t));
+    uint64_t *cnt = (uint64_t *)malloc(65536 * sizeof(uint64_t));
+    for (uint64_t i = 0; i < n; ++i) {
+        k0[i] = codes[i];
+        v0[i] = (uint32_t)i;
+    }
+    for (int pass = 0; pass < 4; ++pass) {
+        int sh = 16 * pass;
+        memset(cnt, 0, 65536 * sizeof(uint64_t));
+        for (uint64_t i = 0; i < n; ++i)
+            cnt[(k0[i] >> sh) & 0xffffu]++;
+        uint64_t acc = 0;
+        for (int d = 0; d < 65536; ++d) {
+            uint64_t c = cnt[d];
+            cnt[d] = acc;
+            acc += c;
+        }
+        for (uint64_t i = 0; i < n; ++i) {
+            uint64_t pos = cnt[(k0[i] >> sh) & 0xffffu]++;
+            k1[pos] = k0[i];
+            v1[pos] = v0[i];
+        }
+        uint64_t *tk = k0; k0 = k1; k1 = tk;
+        uint32_t *tv = v0; v0 = v1; v1 = tv;
+    }
+    memcpy(sorted, k0, n * sizeof(uint64_t));
+    memcpy(ids, v0, n * sizeof(uint32_t));
+    free(k0); free(k1); free(v0); free(v1); free(cnt);
+}
+
+/* ---------------------------------------------------------------------------------------------- */
+/* Karras LBVH: detail/gwn_bvh_build_binary.cuh:29-129 (delta with index tie-break),             */
+/* bounds: :131-192 (union of the two children, bottom up).                                        */
+
+static int clz64(uint64_t v) { return v == 0 ? 64 : __builtin_clzll(v); }
+static int clz32(uint32_t v) { return v == 0 ? 32 : __builtin_clz(v); }
+
+static int k_delta(const uint64_t *codes, int bits, int64_t n, int64_t i, int64_t j) {
+    if (j < 0 || j >= n)
+        return -1;
+    uint64_t ci = codes[i], cj = codes[j];
+    if (ci == cj) {
+        uint64_t diff = (uint64_t)i ^ (uint64_t)j;
+        if (diff == 0)
+            return bits + 64;
+        return bits + clz64(diff);
+    }
+    if (bits == 32)
+        return clz32((uint32_t)(ci ^ cj));
+    return clz64(ci ^ cj);
+}
+
+/* parents: (parent << 1) | slot for internal nodes (n-1) and leaves (n); INV for the root. */
+void oracle_karras(const uint64_t *codes, int bits, uint64_t n, o_bnode *nodes, uint32_t *internal_parent,
+                   uint32_t *leaf_parent) {
+    for (uint64_t i = 0; i + 1 < n; ++i)
+        internal_parent[i] = INV32;
+    for (uint64_t i = 0; i < n; ++i)
+        leaf_parent[i] = INV32;
+    for (int64_t i = 0; i + 1 < (int64_t)n; ++i) {
+        int dir = (k_delta(codes, bits, n, i, i + 1) - k_delta(codes, bits, n, i, i - 1) >= 0) ? 1 : -1;
+        int dmin = k_delta(codes, bits, n, i, i - dir);
+        int64_t lmax = 2;
+        while (k_delta(codes, bits, n, i, i + lmax * dir) > dmin)
+            lmax <<= 1;
+        int64_t l = 0;
+        for (int64_t t = lmax >> 1; t > 0; t >>= 1)
+            if (k_delta(codes, bits, n, i, i + (l + t) * dir) > dmin)
+                l += t;
+        int64_t j = i + l * dir;
+        int64_t first = i < j ? i : j, last = i < j ? j : i;
+        int dnode = k_delta(codes, bits, n, first, last);
+        int64_t split = first, step = last - first;
+        do {
+            step = (step + 1) >> 1;
+            int64_t cand = split + step;
+            if (cand < last && k_delta(codes, bits, n, first, cand) > dnode)
+                split = cand;
+        } while (step > 1);
+        o_bnode nd;
+        nd.li = (uint32_t)split;
+        nd.lk = (split == first) ? K_LEAF : K_INTERNAL;
+        nd.ri = (uint32_t)(split + 1);
+        nd.rk = (split + 1 == last) ? K_LEAF : K_INTERNAL;
+        nodes[i] = nd;
+        uint32_t me2 = (uint32_t)i << 1;
+        if (nd.lk == K_INTERNAL) internal_parent[nd.li] = me2; else leaf_parent[nd.li] = me2;
+        if (nd.rk == K_INTERNAL) internal_parent[nd.ri] = me2 | 1u; else leaf_parent[nd.ri] = me2 | 1u;
+    }
+}
+
+static o_aabb binary_bounds_rec(const o_bnode *nodes, const o_aabb *leaf, o_aabb *out, uint32_t idx,
+                                uint32_t kind) {
+    if (kind == K_LEAF)
+        return leaf[idx];
+    /* iterative post-order to avoid deep recursion on degenerate trees */
+    (void)nodes; (void)out;
+    return leaf[0];
+}
+
+/* Bottom-up bounds for any binary hierarchy (children before parents not assumed). */
+void oracle_binary_bounds(const o_bnode *nodes, uint64_t n, const o_aabb *leaf, uint32_t root, o_aabb *out) {
+    (void)binary_bounds_rec;
+    if (n < 2)
+        return;
+    uint32_t *stack = (uint32_t *)malloc(2 * n * sizeof(uint32_t));
+    uint8_t *state = (uint8_t *)calloc(n, 1);
+    int64_t sp = 0;
+    stack[sp++] = root;
+    while (sp > 0) {
+        uint32_t v = stack[sp - 1];
+        o_bnode nd = nodes[v];
+        if (!state[v]) {
+            state[v] = 1;
+            if (nd.rk == K_INTERNAL) stack[sp++] = nd.ri;
+            if (nd.lk == K_INTERNAL) stack[sp++] = nd.li;
+            continue;
+        }
+        --sp;
+        o_aabb l = nd.lk == K_LEAF ? leaf[nd.li] : out[nd.li];
+        o_aabb r = nd.rk == K_LEAF ? leaf[nd.ri] : out[nd.ri];
+        out[v] = aabb_union(l, r);
+    }
+    free(stack);
+    free(state);
+}
+
+/* ---------------------------------------------------------------------------------------------- */
+/* H-PLOC: detail/gwn_bvh_build_hploc.cuh:104-478, simulated one leaf path at a time. Each range */
+/* is merged from the cluster lists of its two halves, so the tree does not depend on the order  */
+/* the paths run in; internal ids are assigned sequentially here.                                  */
+
+static uint64_t h_delta(const uint64_t *codes, int bits, uint32_t a, uint32_t b) {
+    if (bits == 32) {
+        uint64_t ca = (codes[a] << 32) | a, cb = (codes[b] << 32) | b;
+        return ca ^ cb;
+    }
+    uint64_t d = codes[a] ^ codes[b];
+    return d == 0 ? (uint64_t)(a ^ b) : d;
+}
+
+typedef struct {
+    const uint64_t *codes;
+    int bits;
+    uint32_t n;
+    uint32_t radius;
+    const o_aabb *leaf;
+    o_bnode *nodes;
+    o_aabb *ib;
+    uint32_t *cluster;
+    uint32_t next_id;
+    int failed;
+} hploc_state;
+
+static uint32_t f_bits(float f) {
+    uint32_t u;
+    memcpy(&u, &f, 4);
+    return u;
+}
+
+static void hploc_merge_range(hploc_state *st, uint32_t left, uint32_t right, uint32_t split, int fin) {
+    uint32_t cid[32];
+    o_aabb b[32];
+    uint32_t r_end = right + 1;
+    for (int l = 0; l < 32; ++l)
+        cid[l] = INV32;
+    /* left list (up to 16) then right list */
+    uint32_t nl = 0, nr = 0;
+    uint32_t cntl = (split - left) < 16 ? (split - left) : 16;
+    for (uint32_t k = 0; k < cntl; ++k)
+        cid[k] = st->cluster[left + k];
+    for (uint32_t k = 0; k < cntl; ++k)
+        nl += cid[k] != INV32;
+    uint32_t cntr = (r_end - split) < 16 ? (r_end - split) : 16;
+    for (uint32_t k = 0; k < cntr; ++k)
+        cid[nl + k] = st->cluster[split + k];
+    for (uint32_t k = 0; k < cntr; ++k)
+        nr += cid[nl + k] != INV32;
+    uint32_t num = nl + nr;
+    for (uint32_t l = 0; l < 32; ++l) {
+        if (l < num)
+            b[l] = cid[l] < st->n ? st->leaf[cid[l]] : st->ib[cid[l] - st->n];
+        else
+            memset(&b[l], 0, sizeof(o_aabb));
+    }
+    uint32_t threshold = fin ? 1u : 16u;
+    int guard = 0;
+    while (num > threshold) {
+        uint32_t prev = num;
+        /* nearest neighbour with packed keys (:195-241) */
+        uint32_t best[32], nk[32], nn[32];
+        for (int l = 0; l < 32; ++l)
+            best[l] = 0xffffffffu;
+        for (uint32_t r = 1; r <= 8 && r <= st->radius; ++r) {
+            uint32_t right_key[32];
+            int nvalid[32];
+            for (uint32_t l = 0; l < 32; ++l) {
+                uint32_t nlane = l + r;
+                nvalid[l] = nlane < num;
+                right_key[l] = 0xffffffffu;
+                if (nvalid[l]) {
+                    float area = half_area(aabb_union(b[l], b[nlane]));
+                    uint32_t akey = (f_bits(area) << 1) & ~0xfu;
+                    uint32_t rel = (r - 1u) << 1;
+                    right_key[l] = akey | rel | ((nlane & 1u) ^ 1u);
+                    uint32_t lk = akey | rel | (l & 1u);
+                    if (lk < best[l])
+                        best[l] = lk;
+                }
+            }
+            for (uint32_t l = 0; l < 32; ++l) {
+                uint32_t src = nvalid[l] ? l + r : l;
+                nk[l] = best[src];
+                if (nvalid[l] && right_key[l] < nk[l])
+                    nk[l] = right_key[l];
+            }
+            for (uint32_t l = 0; l < 32; ++l)
+                if ((int)l - (int)r >= 0)
+                    best[l] = nk[l - r];
+        }
+        for (uint32_t l = 0; l < 32; ++l) {
+            uint32_t off = ((best[l] & 0xfu) >> 1) + 1u;
+            int rightward = ((best[l] ^ l) & 1u) == 0u;
+            nn[l] = rightward ? l + off : l - off;
+        }
+        /* merge mutual pairs (:300-399) */
+        uint32_t safe[32];
+        int mutual[32], domerge[32];
+        for (uint32_t l = 0; l < 32; ++l) {
+            int active = l < num;
+            int nv = nn[l] < num && nn[l] != l;
+            if (active && !nv)
+                st->failed = 1;
+            safe[l] = nv ? nn[l] : l;
+        }
+        uint32_t mcount = 0;
+        for (uint32_t l = 0; l < 32; ++l) {
+            int active = l < num;
+            int nv = nn[l] < num && nn[l] != l;
+            mutual[l] = active && nv && l == safe[safe[l]];
+            domerge[l] = mutual[l] && l < safe[l];
+            mcount += domerge[l];
+        }
+        uint32_t base = st->next_id;
+        st->next_id += mcount;
+        uint32_t rel = 0;
+        uint32_t ncid[32];
+        o_aabb nb[32];
+        for (uint32_t l = 0; l < 32; ++l) {
+            ncid[l] = cid[safe[l]];
+            nb[l] = b[safe[l]];
+        }
+        for (uint32_t l = 0; l < 32; ++l) {
+            if (!domerge[l])
+                continue;
+            uint32_t merged = base + rel++;
+            if (merged < st->n || merged >= 2 * st->n - 1) {
+                st->failed = 1;
+                continue;
+            }
+            o_aabb mb = aabb_union(b[l], nb[l]);
+            uint32_t iid = merged - st->n;
+            o_bnode nd;
+            nd.li = cid[l] < st->n ? cid[l] : cid[l] - st->n;
+            nd.lk = cid[l] < st->n ? K_LEAF : K_INTERNAL;
+            nd.ri = ncid[l] < st->n ? ncid[l] : ncid[l] - st->n;
+            nd.rk = ncid[l] < st->n ? K_LEAF : K_INTERNAL;
+            st->nodes[iid] = nd;
+            st->ib[iid] = mb;
+            cid[l] = merged;
+            b[l] = mb;
+        }
+        /* compaction: keep merged lanes and non-mutual lanes, in lane order */
+        uint32_t kc[32];
+        o_aabb kb[32];
+        uint32_t kept = 0;
+        for (uint32_t l = 0; l < 32; ++l) {
+            if (domerge[l] || !mutual[l]) {
+                kc[kept] = cid[l];
+                kb[kept] = b[l];
+                ++kept;
+            }
+        }
+        for (uint32_t l = 0; l < 32; ++l) {
+            if (l < kept) {
+                cid[l] = kc[l];
+                b[l] = kb[l];
+            } else {
+                cid[l] = INV32;
+            }
+        }
+        num -= mcount;
+        if (num == prev || ++guard > 64) {
+            st->failed = 1;
+            break;
+        }
+    }
+    for (uint32_t l = 0; l < nl + nr; ++l)
+        st->cluster[left + l] = cid[l];
+}
+
+/* Returns 0 on success; *root = n - 2. codes are uint64 holding 32- or 64-bit Morton codes. */
+int oracle_hploc(const uint64_t *codes, int bits, uint64_t n64, const o_aabb *leaf, uint32_t radius,
+                 o_bnode *nodes, o_aabb *ib, uint32_t *root) {
+    uint32_t n = (uint32_t)n64;
+    *root = INV32;
+    if (n < 2)
+        return 0;
+    hploc_state st = {codes, bits, n, radius, leaf, nodes, ib, NULL, n, 0};
+    st.cluster = (uint32_t *)malloc(n * sizeof(uint32_t));
+    uint32_t *bp = (uint32_t *)malloc(n * sizeof(uint32_t));
+    for (uint32_t i = 0; i < n; ++i) {
+        st.cluster[i] = i;
+        bp[i] = INV32;
+    }
+    for (uint32_t i = 0; i < n; ++i) {
+        uint32_t left = i, right = i, split = 0;
+        for (;;) {
+            uint32_t prev;
+            int is_right = left == 0 ||
+                           (right != n - 1 && h_delta(codes, bits, right, right + 1) < h_delta(codes, bits, left - 1, left));
+            if (is_right) {
+                prev = bp[right];
+                bp[right] = left;
+                if (prev != INV32) {
+                    split = right + 1;
+                    right = prev;
+                }
+            } else {
+                prev = bp[left - 1];
+                bp[left - 1] = right;
+                if (prev != INV32) {
+                    split = left;
+                    left = prev;
+                }
+            }
+            if (prev == INV32)
+                break;
+            uint32_t size = right - left + 1;
+            int fin = size == n;
+            if (size > 16 || fin)
+                hploc_merge_range(&st, left, right, split, fin);
+        }
+    }
+    free(st.cluster);
+    free(bp);
+    if (st.failed || st.next_id != 2 * n - 1)
+        return 1;
+    *root = n - 2;
+    return 0;
+}
+
+/* ---------------------------------------------------------------------------------------------- */
+/* BVH4 collapse, rule of detail/gwn_bvh_build_collapse.cuh:163-199 (expand the internal candidate */
+/* with the largest half area; equal areas keep the lower binary index; the expanded candidate's   */
+/* left child takes its slot and the right child is appended). Nodes are numbered breadth first,   */
+/* children of a node consecutively in slot order. Stack bounds follow :266-296.                   */
+
+int oracle_collapse(const o_bnode *bin, const o_aabb *bb, const o_aabb *leaf, uint64_t n, uint32_t root,
+                    o_node4 *nodes, uint64_t *node_count, uint32_t *internal_bound, uint32_t *packed_bound) {
+    if (n < 2) {
+        *node_count = 0;
+        *internal_bound = 0;
+        *packed_bound = 0;
+        return 0;
+    }
+    typedef struct {
+        uint32_t b, pi, pp;
+    } item;
+    item *q = (item *)malloc((n - 1) * sizeof(item));
+    uint64_t head = 0, tail = 0;
+    q[tail++] = (item){root, 0, 0};
+    uint32_t ib_max = 0, pb_max = 0;
+    while (head < tail) {
+        item it = q[head];
+        uint64_t w = head++;
+        uint32_t ci[4], ck[4];
+        o_bnode r = bin[it.b];
+        ci[0] = r.li; ck[0] = r.lk; ci[1] = r.ri; ck[1] = r.rk;
+        int k = 2;
+        while (k < 4) {
+            int best = -1;
+            float best_area = -INFINITY;
+            uint32_t best_index = INV32;
+            for (int c = 0; c < k; ++c) {
+                if (ck[c] != K_INTERNAL)
+                    continue;
+                float area = half_area(bb[ci[c]]);
+                if (best >= 0 && area < best_area)
+                    continue;
+                if (best >= 0 && area == best_area && ci[c] >= best_index)
+                    continue;
+                best = c;
+                best_area = area;
+                best_index = ci[c];
+            }
+            if (best < 0)
+                break;
+            o_bnode e = bin[ci[best]];
+            ci[best] = e.li; ck[best] = e.lk;
+            ci[k] = e.ri; ck[k] = e.rk;
+            ++k;
+        }
+        uint32_t kint = 0;
+        for (int c = 0; c < k; ++c)
+            kint += ck[c] == K_INTERNAL;
+        uint32_t nib = it.pi + (kint > 0 ? kint - 1 : 0);
+        uint32_t npb = it.pp + (uint32_t)(k - 1);
+        if (nib > ib_max) ib_max = nib;
+        if (npb > pb_max) pb_max = npb;
+        o_node4 nd;
+        memset(&nd, 0, sizeof(nd));
+        for (int c = 0; c < k; ++c) {
+            if (ck[c] == K_LEAF) {
+                nd.c[c].bounds = leaf[ci[c]];
+                nd.c[c].reference = make_ref(ci[c], 1);
+            } else {
+                nd.c[c].bounds = bb[ci[c]];
+                nd.c[c].reference = make_ref(tail, 0);
+                q[tail++] = (item){ci[c], nib, npb};
+            }
+        }
+        nodes[w] = nd;
+    }
+    *node_count = tail;
+    *internal_bound = ib_max;
+    *packed_bound = pb_max;
+    free(q);
+    return 0;
+}
+
+/* Leaf-ordered triangle records, detail/gwn_bvh_triangle_impl.cuh:24-67. Returns nonzero on an
+ * invalid index. */
+int oracle_triangles(const float *vx, const float *vy, const float *vz, uint64_t nv, const uint32_t *i0,
+                     const uint32_t *i1, const uint32_t *i2, uint64_t nt, const uint32_t *ids, o_tri *out) {
+    int bad = 0;
+    for (uint64_t s = 0; s < nt; ++s) {
+        uint32_t t = ids[s];
+        if (t >= nt) {
+            bad = 1;
+            continue;
+        }
+        uint32_t a = i0[t], b = i1[t], c = i2[t];
+        if (a >= nv || b >= nv || c >= nv) {
+            bad = 1;
+            continue;
+        }
+        o_tri r = {vx[a], vy[a], vz[a], vx[b] - vx[a], vy[b] - vy[a], vz[b] - vz[a],
+                   vx[c] - vx[a], vy[c] - vy[a], vz[c] - vz[a]};
+        out[s] = r;
+    }
+    return bad;
+}
+
+/* ---------------------------------------------------------------------------------------------- */
+/* Taylor moments: detail/gwn_bvh_refit_common.cuh:123-387 (per-triangle raw moments including     */
+/* the HDK split integrals for order 2), :67-111 (accumulation), :514-608 (recentring, packing),   */
+/* :113-121 (far-field radius). Output: gwn_bvh_moment_node<4, order, float> field-SoA.            */
+
+typedef struct {
+    float area, apx, apy, apz, nx, ny, nz;
+    float F[3][3];  /* n_i * centroid_j */
+    float R[3][6];  /* raw second moments */
+} o_payload;
+
+static void pay_acc(o_payload *d, const o_payload *s) {
+    d->area += s->area; d->apx += s->apx; d->apy += s->apy; d->apz += s->apz;
+    d->nx += s->nx; d->ny += s->ny; d->nz += s->nz;
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j)
+            d->F[i][j] += s->F[i][j];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 6; ++j)
+            d->R[i][j] += s->R[i][j];
+}
+
+static void split_int(float vs[3][3], int va, int vb, int vc, int i, const float P[3], float *oii, float *oij,
+                      float *oik) {
+    int j = (i == 2) ? 0 : i + 1;
+    int k = (j == 2) ? 0 : j + 1;
+    float oab_i = vs[vb][i] - vs[va][i], oab_j = vs[vb][j] - vs[va][j], oab_k = vs[vb][k] - vs[va][k];
+    float oac_i = vs[vc][i] - vs[va][i], oac_j = vs[vc][j] - vs[va][j], oac_k = vs[vc][k] - vs[va][k];
+    float ocb_i = vs[vb][i] - vs[vc][i], ocb_j = vs[vb][j] - vs[vc][j], ocb_k = vs[vb][k] - vs[vc][k];
+    float t = (oac_i > 0.0f) ? (oab_i / oac_i) : 0.0f;
+    float jd = t * oac_j - oab_j, kd = t * oac_k - oab_k;
+    float ca0 = jd * oab_k - kd * oab_j, ca1 = kd * oab_i, ca2 = jd * oab_i;
+    float cc0 = jd * ocb_k - kd * ocb_j, cc1 = kd * ocb_i, cc2 = jd * ocb_i;
+    float sa = sqrtf(fmax_r(ca0 * ca0 + ca1 * ca1 + ca2 * ca2, 0.0f));
+    float sc = sqrtf(fmax_r(cc0 * cc0 + cc1 * cc1 + cc2 * cc2, 0.0f));
+    float pai = vs[va][i] - P[i], pci = vs[vc][i] - P[i];
+    *oii = sa * (0.5f * pai * pai + (2.0f / 3.0f) * pai * oab_i + 0.25f * oab_i * oab_i) +
+           sc * (0.5f * pci * pci + (2.0f / 3.0f) * pci * ocb_i + 0.25f * ocb_i * ocb_i);
+    for (int w = 0; w < 2; ++w) {
+        float *out = w == 0 ? oij : oik;
+        int jk = w == 0 ? j : k;
+        float diff = w == 0 ? jd : kd;
+        if (!out)
+            continue;
+        float mid = vs[vb][jk] + 0.5f * diff;
+        float amid = mid - vs[va][jk], cmid = mid - vs[vc][jk];
+        float paj = vs[va][jk] - P[jk], pcj = vs[vc][jk] - P[jk];
+        *out = sa * (0.5f * pai * paj + (1.0f / 3.0f) * pai * amid + (1.0f / 3.0f) * paj * oab_i +
+                     0.25f * oab_i * amid) +
+               sc * (0.5f * pci * pcj + (1.0f / 3.0f) * pci * cmid + (1.0f / 3.0f) * pcj * ocb_i +
+                     0.25f * ocb_i * cmid);
+    }
+}
+
+static void tri_moment(const o_tri *t, int order, o_payload *m) {
+    memset(m, 0, sizeof(*m));
+    float ax = t->v0_x, ay = t->v0_y, az = t->v0_z;
+    float bx = ax + t->e1_x, by = ay + t->e1_y, bz = az + t->e1_z;
+    float cx = ax + t->e2_x, cy = ay + t->e2_y, cz = az + t->e2_z;
+    float px = (ax + bx + cx) / 3.0f, py = (ay + by + cy) / 3.0f, pz = (az + bz + cz) / 3.0f;
+    float abx = bx - ax, aby = by - ay, abz = bz - az, acx = cx - ax, acy = cy - ay, acz = cz - az;
+    float nx = 0.5f * (aby * acz - abz * acy), ny = 0.5f * (abz * acx - abx * acz), nz = 0.5f * (abx * acy - aby * acx);
+    float area = sqrtf(fmax_r(nx * nx + ny * ny + nz * nz, 0.0f));
+    m->area = area;
+    m->apx = px * area; m->apy = py * area; m->apz = pz * area;
+    m->nx = nx; m->ny = ny; m->nz = nz;
+    float N[3] = {nx, ny, nz}, P[3] = {px, py, pz};
+    if (order >= 1)
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j)
+                m->F[i][j] = N[i] * P[j];
+    if (order >= 2 && area != 0.0f) {
+        float inv_area = 1.0f / area;
+        float nh[3] = {nx * inv_area, ny * inv_area, nz * inv_area};
+        float vs[3][3] = {{ax, ay, az}, {bx, by, bz}, {cx, cy, cz}};
+        int ord[3][3];
+        float span[3];
+        for (int a = 0; a < 3; ++a) {
+            int o0 = 0, o1 = 1, o2 = 2, tmp;
+            if (vs[0][a] > vs[1][a]) { tmp = o0; o0 = o1; o1 = tmp; }
+            if (vs[o0][a] > vs[2][a]) { tmp = o0; o0 = o2; o2 = tmp; }
+            if (vs[o1][a] > vs[o2][a]) { tmp = o1; o1 = o2; o2 = tmp; }
+            ord[a][0] = o0; ord[a][1] = o1; ord[a][2] = o2;
+            span[a] = vs[o2][a] - vs[o0][a];
+        }
+        float ixx = 0, iyy = 0, izz = 0, ixy = 0, iyz = 0, izx = 0;
+        float dx = span[0], dy = span[1], dz = span[2];
+        if (dx > 0.0f)
+            split_int(vs, ord[0][0], ord[0][1], ord[0][2], 0, P, &ixx, (dx >= dy && dy > 0.0f) ? &ixy : NULL,
+                      (dx >= dz && dz > 0.0f) ? &izx : NULL);
+        if (dy > 0.0f)
+            split_int(vs, ord[1][0], ord[1][1], ord[1][2], 1, P, &iyy, (dy >= dz && dz > 0.0f) ? &iyz : NULL,
+                      (dx < dy && dx > 0.0f) ? &ixy : NULL);
+        if (dz > 0.0f)
+            split_int(vs, ord[2][0], ord[2][1], ord[2][2], 2, P, &izz, (dx < dz && dx > 0.0f) ? &izx : NULL,
+                      (dy < dz && dy > 0.0f) ? &iyz : NULL);
+        float ig[6] = {ixx, iyy, izz, ixy, iyz, izx};
+        float pp[6] = {px * px, py * py, pz * pz, px * py, py * pz, pz * px};
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 6; ++j)
+                m->R[i][j] = nh[i] * ig[j] + N[i] * pp[j];
+    }
+}
+
+static void finalize_slot(o_aabb b, const o_payload *m, int order, float *f) {
+    float ax, ay, az;
+    if (m->area > 0.0f) {
+        ax = m->apx / m->area; ay = m->apy / m->area; az = m->apz / m->area;
+    } else {
+        ax = (b.min_x + b.max_x) * 0.5f; ay = (b.min_y + b.max_y) * 0.5f; az = (b.min_z + b.max_z) * 0.5f;
+    }
+    float dx = fmax_r(ax - b.min_x, b.max_x - ax), dy = fmax_r(ay - b.min_y, b.max_y - ay),
+          dz = fmax_r(az - b.min_z, b.max_z - az);
+    f[0] = dx * dx + dy * dy + dz * dz;
+    f[1] = ax; f[2] = ay; f[3] = az;
+    f[4] = m->nx; f[5] = m->ny; f[6] = m->nz;
+    if (order >= 1) {
+        float xx = m->F[0][0] - ax * m->nx, yy = m->F[1][1] - ay * m->ny, zz = m->F[2][2] - az * m->nz;
+        float xy = m->F[0][1] - ay * m->nx, yx = m->F[1][0] - ax * m->ny;
+        float yz = m->F[1][2] - az * m->ny, zy = m->F[2][1] - ay * m->nz;
+        float zx = m->F[2][0] - ax * m->nz, xz = m->F[0][2] - az * m->nx;
+        f[7] = xx; f[8] = yy; f[9] = zz; f[10] = xy + yx; f[11] = yz + zy; f[12] = zx + xz;
+    }
+    if (order >= 2) {
+        float P[3] = {ax, ay, az}, N[3] = {m->nx, m->ny, m->nz};
+        float c[3][6];
+        for (int i = 0; i < 3; ++i) {
+            c[i][0] = m->R[i][0] - 2.0f * P[0] * m->F[i][0] + P[0] * P[0] * N[i];
+            c[i][1] = m->R[i][1] - 2.0f * P[1] * m->F[i][1] + P[1] * P[1] * N[i];
+            c[i][2] = m->R[i][2] - 2.0f * P[2] * m->F[i][2] + P[2] * P[2] * N[i];
+            c[i][3] = m->R[i][3] - P[0] * m->F[i][1] - P[1] * m->F[i][0] + P[0] * P[1] * N[i];
+            c[i][4] = m->R[i][4] - P[1] * m->F[i][2] - P[2] * m->F[i][1] + P[1] * P[2] * N[i];
+            c[i][5] = m->R[i][5] - P[2] * m->F[i][0] - P[0] * m->F[i][2] + P[2] * P[0] * N[i];
+        }
+        f[13] = c[0][0]; f[14] = c[1][1]; f[15] = c[2][2];
+        f[16] = 2.0f * (c[0][4] + c[1][5] + c[2][3]);
+        f[17] = 2.0f * c[0][3] + c[1][0];
+        f[18] = 2.0f * c[0][5] + c[2][0];
+        f[19] = 2.0f * c[1][4] + c[2][1];
+        f[20] = 2.0f * c[1][3] + c[0][1];
+        f[21] = 2.0f * c[2][5] + c[0][2];
+        f[22] = 2.0f * c[2][4] + c[1][2];
+    }
+}
+
+static int field_count(int order) { return order == 0 ? 7 : (order == 1 ? 13 : 23); }
+
+/* out: nn * field_count(order) * 4 floats. Children must have larger indices than parents. */
+void oracle_moments(int order, const o_node4 *nodes, uint64_t nn, const o_tri *tris, uint64_t nt, float *out) {
+    int F = field_count(order);
+    o_payload *pend = (o_payload *)calloc(nn ? nn : 1, sizeof(o_payload));
+    for (int64_t n = (int64_t)nn - 1; n >= 0; --n) {
+        o_payload total;
+        memset(&total, 0, sizeof(total));
+        int init = 0;
+        float *ref = out + (uint64_t)n * F * 4;
+        for (int s = 0; s < 4; ++s) {
+            uint64_t r = nodes[n].c[s].reference;
+            if (!ref_valid(r)) {
+                for (int f = 0; f < F; ++f)
+                    ref[f * 4 + s] = 0.0f;
+                continue;
+            }
+            o_payload m;
+            memset(&m, 0, sizeof(m));
+            if (ref_internal(r)) {
+                m = pend[ref_offset(r)];
+            } else {
+                uint64_t first = ref_offset(r);
+                uint32_t cnt = ref_count(r);
+                for (uint32_t k = 0; k < cnt && first + k < nt; ++k) {
+                    o_payload tm;
+                    tri_moment(&tris[first + k], order, &tm);
+                    if (k == 0) m = tm; else pay_acc(&m, &tm);
+                }
+            }
+            float f[23];
+            finalize_slot(nodes[n].c[s].bounds, &m, order, f);
+            for (int q = 0; q < F; ++q)
+                ref[q * 4 + s] = f[q];
+            if (init) pay_acc(&total, &m); else total = m;
+            init = 1;
+        }
+        pend[n] = total;
+    }
+    free(pend);
+}
+
+/* ---------------------------------------------------------------------------------------------- */
+/* Taylor traversal: gwn_winding_taylor_impl (detail/gwn_query_winding_impl.cuh:101-374), with    */
+/* per-query counts of nodes entered, accepted far-field children and exact triangles.             */
+
+static float taylor_one(int order, const o_node4 *nodes, uint64_t nn, const float *mom, const o_tri *tris,
+                        uint64_t nt, uint64_t root_ref, float qx, float qy, float qz, float beta2, int cap,
+                        uint32_t *st_nodes, uint32_t *st_far, uint32_t *st_near) {
+    const float k_pi = 3.14159265358979323846f;
+    int F = field_count(order);
+    float omega = 0.0f;
+    uint32_t sn = 0, sf = 0, snear = 0;
+    uint32_t stack[256];
+    int sp = 0;
+    if (cap > 256) cap = 256;
+    if (ref_leaf(root_ref)) {
+        uint64_t first = ref_offset(root_ref);
+        for (uint32_t k = 0; k < ref_count(root_ref) && first + k < nt; ++k) {
+            omega += record_solid_angle(&tris[first + k], qx, qy, qz);
+            ++snear;
+        }
+    } else {
+        uint32_t node = (uint32_t)ref_offset(root_ref);
+        for (;;) {
+            if (node >= nn)
+                break;
+            ++sn;
+            const float *T = mom + (uint64_t)node * F * 4;
+            uint32_t next = INV32;
+            for (int s = 0; s < 4; ++s) {
+                uint64_t r = nodes[node].c[s].reference;
+                if (!ref_valid(r))
+                    continue;
+                float rx = qx - T[1 * 4 + s], ry = qy - T[2 * 4 + s], rz = qz - T[3 * 4 + s];
+                float q2 = rx * rx + ry * ry + rz * rz;
+                int descend = !(q2 > 0.0f);
+                if (!descend)
+                    descend = q2 <= T[0 * 4 + s] * beta2;
+                if (!descend) {
+                    float m1 = 1.0f / sqrtf(q2);
+                    float m2 = m1 * m1, m3 = m2 * m1;
+                    float nx = rx * m1, ny = ry * m1, nz = rz * m1;
+                    float Nx = T[4 * 4 + s], Ny = T[5 * 4 + s], Nz = T[6 * 4 + s];
+                    float rdn = nx * Nx + ny * Ny + nz * Nz;
+                    float w = -m2 * rdn;
+                    if (order >= 1) {
+                        float xx = T[7 * 4 + s], yy = T[8 * 4 + s], zz = T[9 * 4 + s];
+                        float xy = T[10 * 4 + s], yz = T[11 * 4 + s], zx = T[12 * 4 + s];
+                        float Tt = xx + yy + zz;
+                        float S = nx * nx * xx + ny * ny * yy + nz * nz * zz + nx * ny * xy + nx * nz * zx + ny * nz * yz;
+                        w += m3 * (Tt - 3.0f * S);
+                    }
+                    if (order >= 2) {
+                        float m4 = m2 * m2;
+                        float nx2 = nx * nx, ny2 = ny * ny, nz2 = nz * nz;
+                        float nx3 = nx2 * nx, ny3 = ny2 * ny, nz3 = nz2 * nz;
+                        float xxx = T[13 * 4 + s], yyy = T[14 * 4 + s], zzz = T[15 * 4 + s], spn = T[16 * 4 + s];
+                        float Axy = T[17 * 4 + s], Axz = T[18 * 4 + s], Ayz = T[19 * 4 + s];
+                        float Ayx = T[20 * 4 + s], Azx = T[21 * 4 + s], Azy = T[22 * 4 + s];
+                        float t0x = Ayx + Azx, t0y = Azy + Axy, t0z = Axz + Ayz;
+                        float t1x = ny * Axy + nz * Axz, t1y = nz * Ayz + nx * Ayx, t1z = nx * Azx + ny * Azy;
+                        w += m4 * (1.5f * (nx * (3.0f * xxx + t0x) + ny * (3.0f * yyy + t0y) + nz * (3.0f * zzz + t0z)) -
+                                   7.5f * (nx3 * xxx + ny3 * yyy + nz3 * zzz + nx * ny * nz * spn + nx2 * t1x +
+                                           ny2 * t1y + nz2 * t1z));
+                    }
+                    if (isfinite(w)) {
+                        omega += w;
+                        ++sf;
+                        continue;
+                    }
+                }
+                if (ref_internal(r)) {
+                    if (next != INV32) {
+                        if (sp >= cap)
+                            return NAN;
+                        stack[sp++] = next;
+                    }
+                    next = (uint32_t)ref_offset(r);
+                    continue;
+                }
+                uint64_t first = ref_offset(r);
+                for (uint32_t k = 0; k < ref_count(r) && first + k < nt; ++k) {
+                    omega += record_solid_angle(&tris[first + k], qx, qy, qz);
+                    ++snear;
+                }
+            }
+            if (next != INV32) {
+                node = next;
+                continue;
+            }
+            if (sp == 0)
+                break;
+            node = stack[--sp];
+        }
+    }
+    if (st_nodes) { *st_nodes = sn; *st_far = sf; *st_near = snear; }
+    return omega / (4.0f * k_pi);
+}
+
+void oracle_taylor(int order, const o_node4 *nodes, uint64_t nn, const float *mom, const o_tri *tris, uint64_t nt,
+                   uint64_t root_ref, const float *qx, const float *qy, const float *qz, uint64_t nq, float beta,
+                   int stack_capacity, float *out, uint32_t *stats, int threads) {
+    float beta2 = beta * beta;
+    (void)threads;
+#pragma omp parallel for schedule(dynamic, 64) num_threads(threads > 0 ? threads : 1)
+    for (int64_t q = 0; q < (int64_t)nq; ++q) {
+        uint32_t *st = stats ? stats + 3 * q : NULL;
+        out[q] = taylor_one(order, nodes, nn, mom, tris, nt, root_ref, qx[q], qy[q], qz[q], beta2, stack_capacity,
+                            st, st ? st + 1 : NULL, st ? st + 2 : NULL);
+    }
+}
+
+/* Exact winding from leaf-ordered records (linear scan), for parity with the exact batch. */
+void oracle_exact_records(const o_tri *tris, uint64_t nt, const float *qx, const float *qy, const float *qz,
+                          uint64_t nq, float *out, int threads) {
+    const float k_pi = 3.14159265358979323846f;
+    (void)threads;
+#pragma omp parallel for schedule(dynamic, 64) num_threads(threads > 0 ? threads : 1)
+    for (int64_t q = 0; q < (int64_t)nq; ++q) {
+        float s = 0.0f;
+        for (uint64_t t = 0; t < nt; ++t)
+            s += record_solid_angle(&tris[t], qx[q], qy[q], qz[q]);
+        out[q] = s / (4.0f * k_pi);
+    }
+}
+
+int oracle_max_threads(void) {
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}

@@ -1,0 +1,156 @@
+"""ctypes binding of libgwnb.so (include/gwnb.h).
+
+The structures below mirror the C declarations field by field. Loading fails loudly when the
+library has not been built: there is no CPU fallback for any entry point.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+_LIB_PATH = Path(__file__).resolve().parent / "libgwnb.so"
+
+GWNB_OK = 0
+GWNB_INVALID_ARGUMENT = 1
+GWNB_CUDA_RUNTIME_ERROR = 2
+GWNB_INTERNAL_ERROR = 3
+
+GWNB_METHOD_HPLOC = 0
+GWNB_METHOD_LBVH = 1
+
+GWNB_NEAR_PLAIN = 0
+GWNB_NEAR_COMPENSATED = 1
+
+
+class aabb_f32(C.Structure):
+    _fields_ = [(n, C.c_float) for n in ("min_x", "min_y", "min_z", "max_x", "max_y", "max_z")]
+
+
+class child_f32(C.Structure):
+    _fields_ = [("bounds", aabb_f32), ("reference", C.c_uint64)]
+
+
+class node4_f32(C.Structure):
+    _fields_ = [("children", child_f32 * 4)]
+
+
+class triangle_f32(C.Structure):
+    _fields_ = [(n, C.c_float) for n in ("v0_x", "v0_y", "v0_z", "e1_x", "e1_y", "e1_z", "e2_x", "e2_y", "e2_z")]
+
+
+class geometry_f32(C.Structure):
+    _fields_ = [
+        ("vertex_x", C.c_void_p), ("vertex_y", C.c_void_p), ("vertex_z", C.c_void_p),
+        ("vertex_count", C.c_uint64),
+        ("tri_i0", C.c_void_p), ("tri_i1", C.c_void_p), ("tri_i2", C.c_void_p),
+        ("triangle_count", C.c_uint64),
+    ]
+
+
+class bvh4_f32(C.Structure):
+    _fields_ = [
+        ("nodes", C.c_void_p),
+        ("node_count", C.c_uint64),
+        ("node_capacity", C.c_uint64),
+        ("primitive_indices", C.c_void_p),
+        ("triangles", C.c_void_p),
+        ("primitive_count", C.c_uint64),
+        ("root", child_f32),
+        ("internal_stack_bound", C.c_uint32),
+        ("packed_stack_bound", C.c_uint32),
+        ("revision", C.c_uint64),
+        ("aux", C.c_void_p),
+    ]
+
+
+class moment4_f32(C.Structure):
+    _fields_ = [
+        ("order", C.c_int),
+        ("nodes", C.c_void_p),
+        ("node_count", C.c_uint64),
+        ("bvh_revision", C.c_uint64),
+        ("aux", C.c_void_p),
+    ]
+
+
+class taylor_options(C.Structure):
+    _fields_ = [
+        ("block_size", C.c_int),
+        ("stack_capacity", C.c_int),
+        ("sort_queries", C.c_int),
+        ("near_precision", C.c_int),
+        ("fp64_threshold", C.c_float),
+    ]
+
+
+class binary_node(C.Structure):
+    _fields_ = [(n, C.c_uint32) for n in ("left_index", "left_kind", "right_index", "right_kind")]
+
+
+assert C.sizeof(child_f32) == 32 and C.sizeof(node4_f32) == 128 and C.sizeof(triangle_f32) == 36
+
+P = C.c_void_p
+U64 = C.c_uint64
+U32 = C.c_uint32
+I = C.c_int
+F = C.c_float
+
+# name -> (restype, argtypes)
+SIGNATURES: dict[str, tuple] = {
+    "gwnb_last_error_message": (C.c_char_p, []),
+    "gwnb_last_cuda_error": (I, []),
+    "gwnb_version": (C.c_char_p, []),
+    "gwnb_geometry_upload_f32": (I, [C.POINTER(geometry_f32), P, P, P, U64, P, P, P, U64, P]),
+    "gwnb_geometry_update_f32": (I, [C.POINTER(geometry_f32), P, P, P, U64, P]),
+    "gwnb_geometry_update_device_f32": (I, [C.POINTER(geometry_f32), P, P, P, U64, P]),
+    "gwnb_geometry_release_f32": (None, [C.POINTER(geometry_f32), P]),
+    "gwnb_bvh4_build_f32": (I, [C.POINTER(geometry_f32), I, U32, I, C.POINTER(bvh4_f32), P]),
+    "gwnb_bvh4_release_f32": (None, [C.POINTER(bvh4_f32), P]),
+    "gwnb_build_preprocess_f32": (I, [C.POINTER(geometry_f32), I, P, P, P, P]),
+    "gwnb_build_binary_lbvh": (I, [P, I, U64, P, P, P, P, P]),
+    "gwnb_build_binary_hploc": (I, [P, I, U64, P, U32, P, P, P, C.POINTER(U32), P]),
+    "gwnb_radix_sort_pairs": (I, [P, P, P, P, U64, I, I, P]),
+    "gwnb_bvh4_refit_f32": (I, [C.POINTER(geometry_f32), C.POINTER(bvh4_f32), P]),
+    "gwnb_bvh4_refit_async_f32": (I, [C.POINTER(geometry_f32), C.POINTER(bvh4_f32), P]),
+    "gwnb_bvh4_sync_status_f32": (I, [C.POINTER(bvh4_f32), P]),
+    "gwnb_moment4_refit_f32": (I, [C.POINTER(bvh4_f32), I, C.POINTER(moment4_f32), P]),
+    "gwnb_moment4_refit_async_f32": (I, [C.POINTER(bvh4_f32), C.POINTER(moment4_f32), P]),
+    "gwnb_moment4_release_f32": (None, [C.POINTER(moment4_f32), P]),
+    "gwnb_moment_node_bytes": (U64, [I]),
+    "gwnb_winding_exact_batch_f32": (I, [C.POINTER(bvh4_f32), P, P, P, P, U64, I, P]),
+    "gwnb_winding_taylor_batch_f32": (
+        I, [C.POINTER(bvh4_f32), C.POINTER(moment4_f32), P, P, P, P, U64, F, C.POINTER(taylor_options), P]),
+    "gwnb_winding_gradient_taylor_batch_f32": (
+        I, [C.POINTER(bvh4_f32), C.POINTER(moment4_f32), P, P, P, P, P, P, U64, F, C.POINTER(taylor_options), P]),
+    "gwnb_winding_taylor_stats_f32": (
+        I, [C.POINTER(bvh4_f32), C.POINTER(moment4_f32), P, P, P, U64, F, P, P, P, P]),
+    "gwnb_bvh4_fp64_fallback_count": (I, [C.POINTER(bvh4_f32), C.POINTER(U64), P]),
+}
+
+_lib: C.CDLL | None = None
+
+
+def library_path() -> Path:
+    return _LIB_PATH
+
+
+def load() -> C.CDLL:
+    """Load libgwnb.so and bind every entry point of include/gwnb.h. Raises if it is missing."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not _LIB_PATH.exists():
+        raise RuntimeError(
+            f"{_LIB_PATH} is missing: build it with `python -m smallgwn_b200.build` "
+            "(nvcc, sm_100a). There is no CPU fallback.")
+    lib = C.CDLL(str(_LIB_PATH))
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def last_error() -> str:
+    return load().gwnb_last_error_message().decode(errors="replace")

@@ -1,0 +1,459 @@
+"""Python mirror of smallgwn's public API over libgwnb.so.
+
+Names, argument meaning and error behaviour follow smallgwn's C++ API
+(include/gwn/gwn_geometry.cuh, gwn_bvh.cuh, gwn_bvh_build.cuh, gwn_bvh_refit.cuh, gwn_query.cuh):
+every call returns a ``gwn_status``; objects own device storage, are rebound to the stream of the
+last successful mutating call and are replaced atomically (staging and swap) so a failed call
+leaves the previous state intact. Device buffers are torch CUDA tensors (or raw device pointers).
+Only width 4, float32 positions and uint32 indices are provided, as in the C ABI.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import enum
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _lib
+
+
+class gwn_error(enum.IntEnum):
+    success = 0
+    invalid_argument = 1
+    cuda_runtime_error = 2
+    internal_error = 3
+
+
+@dataclass
+class gwn_status:
+    """Mirror of gwn::gwn_status (include/gwn/gwn_utils.cuh:223-283)."""
+    error: gwn_error = gwn_error.success
+    message: str = ""
+
+    def is_ok(self) -> bool:
+        return self.error == gwn_error.success
+
+    @staticmethod
+    def ok() -> "gwn_status":
+        return gwn_status()
+
+    def __bool__(self) -> bool:  # truthiness = success, for terse checks
+        return self.is_ok()
+
+
+def _status(rc: int) -> gwn_status:
+    if rc == _lib.GWNB_OK:
+        return gwn_status()
+    return gwn_status(gwn_error(rc), _lib.last_error())
+
+
+class gwn_bvh_build_method(enum.IntEnum):
+    """Mirror of gwn::gwn_bvh_build_method (include/gwn/gwn_bvh_build.cuh:15-20)."""
+    k_hploc = 0
+    k_lbvh = 1
+
+
+@dataclass
+class gwn_bvh_build_options:
+    """Mirror of gwn::gwn_bvh_build_options (include/gwn/gwn_bvh_build.cuh:22-28)."""
+    method: int = gwn_bvh_build_method.k_hploc
+    hploc_search_radius: int = 8
+
+
+@dataclass(frozen=True)
+class gwn_query_batch_config:
+    """Mirror of gwn::gwn_query_batch_config (include/gwn/gwn_query.cuh:48-61)."""
+    block_size: int = 256
+    stack_capacity: int = 64
+
+
+class near_precision(enum.IntEnum):
+    plain = _lib.GWNB_NEAR_PLAIN
+    compensated = _lib.GWNB_NEAR_COMPENSATED
+
+
+def _stream(stream) -> int | None:
+    if stream is None:
+        return None  # cudaStreamLegacy / stream 0
+    if isinstance(stream, int):
+        return stream or None
+    handle = getattr(stream, "cuda_stream", None)
+    if handle is not None:
+        return int(handle) or None
+    raise TypeError(f"unsupported stream object {stream!r}")
+
+
+def _ptr(buf) -> int | None:
+    if buf is None:
+        return None
+    if isinstance(buf, int):
+        return buf or None
+    dp = getattr(buf, "data_ptr", None)
+    if dp is not None:
+        if not buf.is_cuda:
+            raise ValueError("device buffers must be CUDA tensors")
+        if not buf.is_contiguous():
+            raise ValueError("device buffers must be contiguous")
+        return int(dp()) or None
+    raise TypeError(f"unsupported device buffer {type(buf)!r}")
+
+
+def _numel(buf) -> int:
+    if buf is None:
+        return 0
+    return int(buf.numel())
+
+
+def _host(arr, dtype) -> np.ndarray:
+    a = np.ascontiguousarray(np.asarray(arr), dtype=dtype)
+    return a
+
+
+class _stream_mixin:
+    def __init__(self) -> None:
+        self._stream = None
+
+    def stream(self):
+        return self._stream
+
+    def set_stream(self, stream) -> None:
+        self._stream = stream
+
+
+class gwn_geometry_object(_stream_mixin):
+    """Mirror of gwn::gwn_geometry_object<float, uint32_t> (include/gwn/gwn_geometry.cuh:98-149)."""
+
+    def __init__(self) -> None:
+        super().__init__()
+        self._view = _lib.geometry_f32()
+
+    def accessor(self) -> _lib.geometry_f32:
+        return self._view
+
+    def vertex_count(self) -> int:
+        return int(self._view.vertex_count)
+
+    def triangle_count(self) -> int:
+        return int(self._view.triangle_count)
+
+    def has_data(self) -> bool:
+        return self.vertex_count() != 0 or self.triangle_count() != 0
+
+    def clear(self) -> None:
+        if self.has_data():
+            _lib.load().gwnb_geometry_release_f32(C.byref(self._view), _stream(self._stream))
+        self._view = _lib.geometry_f32()
+
+    def __del__(self) -> None:
+        try:
+            self.clear()
+        except Exception:
+            pass
+
+
+def gwn_upload_geometry(obj: gwn_geometry_object, x, y, z, i0, i1, i2, stream=None) -> gwn_status:
+    """Upload host SoA positions and indices; replaces ``obj`` only on success."""
+    lib = _lib.load()
+    xs, ys, zs = (_host(a, np.float32) for a in (x, y, z))
+    a0, a1, a2 = (_host(a, np.uint32) for a in (i0, i1, i2))
+    if not (xs.size == ys.size == zs.size):
+        return gwn_status(gwn_error.invalid_argument, "Vertex SoA spans must have identical lengths.")
+    if not (a0.size == a1.size == a2.size):
+        return gwn_status(gwn_error.invalid_argument, "Triangle SoA spans must have identical lengths.")
+    staging = _lib.geometry_f32()
+    rc = lib.gwnb_geometry_upload_f32(
+        C.byref(staging), xs.ctypes.data or None, ys.ctypes.data or None, zs.ctypes.data or None, xs.size,
+        a0.ctypes.data or None, a1.ctypes.data or None, a2.ctypes.data or None, a0.size, _stream(stream))
+    if rc != _lib.GWNB_OK:
+        return _status(rc)
+    obj.clear()
+    obj._view = staging
+    obj.set_stream(stream)
+    return gwn_status()
+
+
+def gwn_update_geometry(obj: gwn_geometry_object, x, y, z, stream=None) -> gwn_status:
+    """Copy new host (numpy) or device (torch CUDA) positions into an uploaded geometry."""
+    lib = _lib.load()
+    if hasattr(x, "is_cuda") and x.is_cuda:
+        n = _numel(x)
+        if not (_numel(y) == n == _numel(z)):
+            return gwn_status(gwn_error.invalid_argument, "Vertex SoA spans must have identical lengths.")
+        rc = lib.gwnb_geometry_update_device_f32(C.byref(obj._view), _ptr(x), _ptr(y), _ptr(z), n, _stream(stream))
+    else:
+        xs, ys, zs = (_host(a, np.float32) for a in (x, y, z))
+        if not (xs.size == ys.size == zs.size):
+            return gwn_status(gwn_error.invalid_argument, "Vertex SoA spans must have identical lengths.")
+        rc = lib.gwnb_geometry_update_f32(C.byref(obj._view), xs.ctypes.data or None, ys.ctypes.data or None,
+                                          zs.ctypes.data or None, xs.size, _stream(stream))
+        obj._keepalive = (xs, ys, zs)  # host memory must outlive the asynchronous copy
+    if rc == _lib.GWNB_OK:
+        obj.set_stream(stream)
+    return _status(rc)
+
+
+class gwn_bvh4_object(_stream_mixin):
+    """Mirror of gwn::gwn_bvh4_object<float, uint32_t> (include/gwn/gwn_bvh.cuh:329-381)."""
+
+    def __init__(self) -> None:
+        super().__init__()
+        self._view = _lib.bvh4_f32()
+
+    def accessor(self) -> _lib.bvh4_f32:
+        return self._view
+
+    def has_data(self) -> bool:
+        v = self._view
+        if v.revision == 0 or not (v.root.reference >> 47) & 1 or v.primitive_count == 0:
+            return False
+        return True
+
+    def clear(self) -> None:
+        if self._view.primitive_count or self._view.aux:
+            _lib.load().gwnb_bvh4_release_f32(C.byref(self._view), _stream(self._stream))
+        self._view = _lib.bvh4_f32()
+
+    def __del__(self) -> None:
+        try:
+            self.clear()
+        except Exception:
+            pass
+
+
+def gwn_build_bvh(geometry: gwn_geometry_object, bvh: gwn_bvh4_object,
+                  options: gwn_bvh_build_options | None = None, stream=None, morton_bits: int = 64) -> gwn_status:
+    """Build a BVH4 (LBVH or H-PLOC binary builder + wide collapse). Strong guarantee."""
+    opt = options or gwn_bvh_build_options()
+    staging = _lib.bvh4_f32()
+    rc = _lib.load().gwnb_bvh4_build_f32(C.byref(geometry._view), int(opt.method), int(opt.hploc_search_radius),
+                                         int(morton_bits), C.byref(staging), _stream(stream))
+    if rc != _lib.GWNB_OK:
+        return _status(rc)
+    bvh.clear()
+    bvh._view = staging
+    bvh.set_stream(stream)
+    return gwn_status()
+
+
+def gwn_refit_bvh(geometry: gwn_geometry_object, bvh: gwn_bvh4_object, stream=None) -> gwn_status:
+    """Refit bounds and triangle records in place (synchronizes, publishes a new revision)."""
+    before = bvh._view.revision
+    rc = _lib.load().gwnb_bvh4_refit_f32(C.byref(geometry._view), C.byref(bvh._view), _stream(stream))
+    if rc == _lib.GWNB_OK or (before != 0 and bvh._view.revision == 0):
+        bvh.set_stream(stream)
+    return _status(rc)
+
+
+class gwn_bvh4_moment_object(_stream_mixin):
+    """Mirror of gwn::gwn_bvh4_moment_object<Order, float, uint32_t> (include/gwn/gwn_bvh.cuh:387-430)."""
+
+    def __init__(self, order: int) -> None:
+        super().__init__()
+        if order not in (0, 1, 2):
+            raise ValueError("Taylor order must be 0, 1, or 2.")
+        self.order = order
+        self._view = _lib.moment4_f32(order=order)
+
+    def accessor(self) -> _lib.moment4_f32:
+        return self._view
+
+    def has_data(self) -> bool:
+        return self._view.bvh_revision != 0
+
+    def is_valid_for(self, bvh: gwn_bvh4_object) -> bool:
+        return bvh.has_data() and self._view.bvh_revision == bvh._view.revision
+
+    def clear(self) -> None:
+        if self._view.nodes or self._view.aux:
+            _lib.load().gwnb_moment4_release_f32(C.byref(self._view), _stream(self._stream))
+        self._view = _lib.moment4_f32(order=self.order)
+
+    def __del__(self) -> None:
+        try:
+            self.clear()
+        except Exception:
+            pass
+
+
+def gwn_refit_bvh_moment(order: int, bvh: gwn_bvh4_object, moment: gwn_bvh4_moment_object, stream=None) -> gwn_status:
+    """Compute Taylor moments of ``order`` aligned to ``bvh``; replaces ``moment`` on success."""
+    if moment.order != order:
+        return gwn_status(gwn_error.invalid_argument, "Moment object order does not match the requested order.")
+    staging = _lib.moment4_f32(order=order)
+    rc = _lib.load().gwnb_moment4_refit_f32(C.byref(bvh._view), order, C.byref(staging), _stream(stream))
+    if rc != _lib.GWNB_OK:
+        return _status(rc)
+    moment.clear()
+    moment._view = staging
+    moment.set_stream(stream)
+    return gwn_status()
+
+
+def _check_spans(qx, qy, qz, out) -> gwn_status | None:
+    n = _numel(qx)
+    if not (_numel(qy) == n == _numel(qz)):
+        return gwn_status(gwn_error.invalid_argument, "Query SoA spans must have identical lengths.")
+    if _numel(out) != n:
+        return gwn_status(gwn_error.invalid_argument, "Output span size must match query count.")
+    return None
+
+
+def gwn_compute_winding_number_exact_batch(bvh: gwn_bvh4_object, qx, qy, qz, out, stream=None,
+                                           config: gwn_query_batch_config = gwn_query_batch_config()) -> gwn_status:
+    """Exact winding numbers of a device batch (asynchronous)."""
+    lib = _lib.load()
+    if not bvh.has_data():
+        return gwn_status(gwn_error.invalid_argument, "BVH object contains no queryable data.")
+    bad = _check_spans(qx, qy, qz, out)
+    if bad is not None:
+        return bad
+    rc = lib.gwnb_winding_exact_batch_f32(C.byref(bvh._view), _ptr(qx), _ptr(qy), _ptr(qz), _ptr(out),
+                                          _numel(out), int(config.block_size), _stream(stream))
+    return _status(rc)
+
+
+def _options(config: gwn_query_batch_config, sort_queries: bool, precision: int, fp64_threshold: float):
+    return _lib.taylor_options(int(config.block_size), int(config.stack_capacity), 1 if sort_queries else 0,
+                               int(precision), float(fp64_threshold))
+
+
+def gwn_compute_winding_number_taylor_batch(order: int, bvh: gwn_bvh4_object, moment: gwn_bvh4_moment_object,
+                                            qx, qy, qz, out, accuracy_scale: float = 2.0, stream=None,
+                                            config: gwn_query_batch_config = gwn_query_batch_config(),
+                                            sort_queries: bool = True, precision: int = near_precision.plain,
+                                            fp64_threshold: float = 1e-3) -> gwn_status:
+    """Taylor-approximated winding numbers of a device batch (asynchronous)."""
+    if moment.order != order:
+        return gwn_status(gwn_error.invalid_argument, "Moment object order does not match the requested order.")
+    bad = _check_spans(qx, qy, qz, out)
+    if bad is not None:
+        return bad
+    opt = _options(config, sort_queries, precision, fp64_threshold)
+    rc = _lib.load().gwnb_winding_taylor_batch_f32(
+        C.byref(bvh._view), C.byref(moment._view), _ptr(qx), _ptr(qy), _ptr(qz), _ptr(out), _numel(out),
+        float(accuracy_scale), C.byref(opt), _stream(stream))
+    return _status(rc)
+
+
+def gwn_compute_winding_gradient_taylor_batch(order: int, bvh: gwn_bvh4_object, moment: gwn_bvh4_moment_object,
+                                              qx, qy, qz, gx, gy, gz, accuracy_scale: float = 2.0, stream=None,
+                                              config: gwn_query_batch_config = gwn_query_batch_config(),
+                                              sort_queries: bool = True) -> gwn_status:
+    """Gradient of the Taylor winding number with respect to the query point."""
+    if moment.order != order:
+        return gwn_status(gwn_error.invalid_argument, "Moment object order does not match the requested order.")
+    for g in (gx, gy, gz):
+        bad = _check_spans(qx, qy, qz, g)
+        if bad is not None:
+            return bad
+    opt = _options(config, sort_queries, near_precision.plain, 1e-3)
+    rc = _lib.load().gwnb_winding_gradient_taylor_batch_f32(
+        C.byref(bvh._view), C.byref(moment._view), _ptr(qx), _ptr(qy), _ptr(qz), _ptr(gx), _ptr(gy), _ptr(gz),
+        _numel(qx), float(accuracy_scale), C.byref(opt), _stream(stream))
+    return _status(rc)
+
+
+def taylor_traversal_stats(bvh: gwn_bvh4_object, moment: gwn_bvh4_moment_object, qx, qy, qz, nodes, far, near,
+                           accuracy_scale: float = 2.0, stream=None) -> gwn_status:
+    """Per-query counts of nodes entered, far-field children accepted and exact triangles."""
+    rc = _lib.load().gwnb_winding_taylor_stats_f32(
+        C.byref(bvh._view), C.byref(moment._view), _ptr(qx), _ptr(qy), _ptr(qz), _numel(qx), float(accuracy_scale),
+        _ptr(nodes), _ptr(far), _ptr(near), _stream(stream))
+    return _status(rc)
+
+
+def fp64_fallback_count(bvh: gwn_bvh4_object, stream=None) -> int:
+    n = C.c_uint64(0)
+    rc = _lib.load().gwnb_bvh4_fp64_fallback_count(C.byref(bvh._view), C.byref(n), _stream(stream))
+    if rc != _lib.GWNB_OK:
+        raise RuntimeError(_lib.last_error())
+    return int(n.value)
+
+
+def refit_bvh_async(geometry: gwn_geometry_object, bvh: gwn_bvh4_object, stream=None) -> gwn_status:
+    """Stream-ordered refit without host synchronization (graph capturable)."""
+    return _status(_lib.load().gwnb_bvh4_refit_async_f32(C.byref(geometry._view), C.byref(bvh._view),
+                                                        _stream(stream)))
+
+
+def refit_bvh_moment_async(bvh: gwn_bvh4_object, moment: gwn_bvh4_moment_object, stream=None) -> gwn_status:
+    """Refit an existing moment object for the BVH's current geometry without synchronization."""
+    return _status(_lib.load().gwnb_moment4_refit_async_f32(C.byref(bvh._view), C.byref(moment._view),
+                                                           _stream(stream)))
+
+
+def sync_bvh_status(bvh: gwn_bvh4_object, stream=None) -> gwn_status:
+    """Synchronize, publish device-side root bounds and turn device error bits into a status."""
+    return _status(_lib.load().gwnb_bvh4_sync_status_f32(C.byref(bvh._view), _stream(stream)))
+
+
+# ---- host views of device state (tests, diagnostics) ------------------------------------------------
+
+NODE_DTYPE = np.dtype([("bounds", np.float32, (6,)), ("reference", np.uint64)])
+TRI_DTYPE = np.dtype((np.float32, 9))
+
+
+def _copy_to_host(ptr: int, nbytes: int) -> bytes:
+    import torch
+
+    if nbytes == 0:
+        return b""
+    buf = torch.empty(nbytes, dtype=torch.uint8)
+    torch.cuda.synchronize()
+    cudart = _cudart()
+    rc = cudart.cudaMemcpy(C.c_void_p(buf.data_ptr()), C.c_void_p(ptr), C.c_size_t(nbytes), 2)
+    if rc != 0:
+        raise RuntimeError(f"cudaMemcpy failed ({rc})")
+    return buf.numpy().tobytes()
+
+
+_cudart_lib = None
+
+
+def _cudart():
+    global _cudart_lib
+    if _cudart_lib is None:
+        import glob
+        import os
+
+        cands = []
+        try:
+            import torch
+
+            cands += glob.glob(os.path.join(os.path.dirname(torch.__file__), "lib", "libcudart*.so*"))
+        except Exception:
+            pass
+        cands += glob.glob("/usr/local/cuda/lib64/libcudart.so*")
+        for c in cands:
+            try:
+                _cudart_lib = C.CDLL(c)
+                break
+            except OSError:
+                continue
+        if _cudart_lib is None:
+            raise RuntimeError("libcudart not found")
+        _cudart_lib.cudaMemcpy.restype = C.c_int
+        _cudart_lib.cudaMemcpy.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t, C.c_int]
+    return _cudart_lib
+
+
+def bvh_host_arrays(bvh: gwn_bvh4_object) -> dict:
+    """Copy nodes, primitive order and triangle records of a BVH to host numpy arrays."""
+    v = bvh._view
+    nodes = np.frombuffer(_copy_to_host(v.nodes, int(v.node_count) * 128), dtype=NODE_DTYPE).reshape(-1, 4)
+    prims = np.frombuffer(_copy_to_host(v.primitive_indices, int(v.primitive_count) * 4), dtype=np.uint32)
+    tris = np.frombuffer(_copy_to_host(v.triangles, int(v.primitive_count) * 36), dtype=np.float32).reshape(-1, 9)
+    return {"nodes": nodes, "primitive_indices": prims, "triangles": tris,
+            "root_reference": int(v.root.reference),
+            "root_bounds": np.array([getattr(v.root.bounds, f) for f, _ in _lib.aabb_f32._fields_], np.float32),
+            "internal_stack_bound": int(v.internal_stack_bound), "packed_stack_bound": int(v.packed_stack_bound),
+            "revision": int(v.revision)}
+
+
+def moment_host_array(moment: gwn_bvh4_moment_object) -> np.ndarray:
+    """Copy smallgwn-layout moment nodes to host: shape (nodes, fields, 4)."""
+    v = moment._view
+    fields = {0: 7, 1: 13, 2: 23}[moment.order]
+    raw = _copy_to_host(v.nodes, int(v.node_count) * fields * 16)
+    return np.frombuffer(raw, dtype=np.float32).reshape(-1, fields, 4)

@@ -1,0 +1,200 @@
+// Internal declarations shared by the libgwnb CUDA translation units.
+//
+// Layout contract with smallgwn (include/gwn/gwn_bvh.cuh of that project):
+//   child = 24 B bounds + 8 B packed reference (bits 0-46 offset, bit 47 valid, 48-63 count),
+//   node  = 4 children (128 B), triangle record = {v0, v1 - v0, v2 - v0} (36 B),
+//   moment node = field-SoA, one float[4] per field.
+// Library-private layouts (query sidecar, padded triangles) are defined here too.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+#include <string>
+
+#include "../../include/gwnb.h"
+
+namespace gwnb {
+
+constexpr std::uint64_t k_offset_mask = (std::uint64_t(1) << 47) - 1;
+constexpr std::uint64_t k_valid_bit = std::uint64_t(1) << 47;
+constexpr int k_count_shift = 48;
+constexpr std::uint32_t k_invalid_u32 = 0xffffffffu;
+
+// Error bits of the device status word that every BVH carries.
+enum : unsigned int {
+    k_err_index = 1u << 0,        // triangle index out of range
+    k_err_topology = 1u << 1,     // inconsistent child references / arrival counts
+    k_err_wait_timeout = 1u << 2, // a bounded spin gave up
+    k_err_stack_overflow = 1u << 3,
+    k_err_collapse = 1u << 4,
+    k_err_hploc = 1u << 5,
+};
+
+struct aabb {
+    float min_x, min_y, min_z, max_x, max_y, max_z;
+};
+static_assert(sizeof(aabb) == 24);
+
+struct child {
+    aabb bounds;
+    std::uint64_t reference;
+};
+static_assert(sizeof(child) == 32);
+
+struct node4 {
+    child c[4];
+};
+static_assert(sizeof(node4) == 128);
+
+struct triangle {
+    float v0_x, v0_y, v0_z, e1_x, e1_y, e1_z, e2_x, e2_y, e2_z;
+};
+static_assert(sizeof(triangle) == 36);
+
+// Padded triangle record for 128-bit loads in traversal: (v0.xyz, e1.x) (e1.yz, e2.xy)
+// (e2.z, n.xyz) with n = e1 x e2.
+struct alignas(16) triangle48 {
+    float4 a, b, c;
+};
+
+struct binary_node {
+    std::uint32_t left_index, left_kind, right_index, right_kind;
+};
+constexpr std::uint32_t k_kind_internal = 1u;
+constexpr std::uint32_t k_kind_leaf = 2u;
+
+__host__ __device__ inline bool ref_valid(std::uint64_t r) { return (r & k_valid_bit) != 0; }
+__host__ __device__ inline std::uint32_t ref_count(std::uint64_t r) {
+    return static_cast<std::uint32_t>(r >> k_count_shift);
+}
+__host__ __device__ inline bool ref_internal(std::uint64_t r) {
+    return ref_valid(r) && ref_count(r) == 0u;
+}
+__host__ __device__ inline bool ref_leaf(std::uint64_t r) {
+    return ref_valid(r) && ref_count(r) != 0u;
+}
+__host__ __device__ inline std::uint64_t ref_offset(std::uint64_t r) { return r & k_offset_mask; }
+__host__ __device__ inline std::uint64_t make_ref(std::uint64_t offset, std::uint64_t count) {
+    return k_valid_bit | offset | (count << k_count_shift);
+}
+
+// Query sidecar (one record per wide node, written by the moment refit). Per child slot the
+// record holds float4 blocks: a = (P.xyz, r2) with r2 < 0 marking an invalid slot,
+// b = (N.xyz, ref bits), then the order-1/2 coefficients. ref bits: internal child -> node index;
+// leaf -> 0x80000000 | first sorted triangle; bit 30 set when the leaf holds more than one
+// triangle (its count is then read from the per-node count table).
+constexpr std::uint32_t k_qref_leaf = 0x80000000u;
+constexpr std::uint32_t k_qref_multi = 0x40000000u;
+constexpr std::uint32_t k_qref_index_mask = 0x3fffffffu;
+
+template <int Order> struct qnode_traits;
+template <> struct qnode_traits<0> { static constexpr int k_f4_per_child = 2; };
+template <> struct qnode_traits<1> { static constexpr int k_f4_per_child = 4; };
+template <> struct qnode_traits<2> { static constexpr int k_f4_per_child = 6; };
+inline int qnode_f4_per_child(int order) { return order == 0 ? 2 : (order == 1 ? 4 : 6); }
+
+// Field counts of smallgwn's moment node (floats per child slot).
+inline int moment_field_count(int order) { return order == 0 ? 7 : (order == 1 ? 13 : 23); }
+
+// Host-side state that travels with a BVH view (gwnb_bvh_aux).
+struct bvh_aux_impl {
+    bool derived = false;            // parent links / padded triangles are valid for the fields below
+    std::uint64_t revision = 0;      // BVH revision this state was derived for
+    void *triangles_ptr = nullptr;
+    std::uint64_t node_count = 0;
+    std::uint64_t primitive_count = 0;
+    void *nodes_ptr = nullptr;       // nodes pointer this state was derived for
+    // device arrays
+    std::uint32_t *parent_slot = nullptr; // (parent << 2) | slot, k_invalid_u32 for the root
+    std::uint32_t *expected = nullptr;    // arrivals expected per node
+    std::uint32_t *arrivals = nullptr;    // arrival counters (left at zero between calls)
+    std::uint32_t *leaf_nodes = nullptr;  // nodes with at least one leaf child
+    std::uint64_t leaf_node_count = 0;
+    triangle48 *tri48 = nullptr;          // padded triangle records
+    aabb *root_bounds = nullptr;          // device copy of the root bounds
+    unsigned int *status = nullptr;       // device error word
+    unsigned long long *fp64_count = nullptr; // FP64 fallback counter of the compensated path
+    void *scratch = nullptr;              // per-BVH reusable scratch for batched queries
+    std::size_t scratch_bytes = 0;
+    cudaStream_t stream = nullptr;        // stream the arrays were allocated on
+};
+
+struct moment_aux_impl {
+    float4 *qnodes = nullptr;   // query sidecar, node_count * 4 * f4_per_child float4
+    std::uint32_t *qcounts = nullptr; // per node: 4 leaf counts (only read for multi-triangle leaves)
+    void *payload = nullptr;    // per-node additive raw-moment payload used by the climb
+    std::size_t payload_stride = 0;
+};
+
+// ---- status helpers (host) -------------------------------------------------------------------
+int set_error(int code, std::string const &message);
+int set_cuda_error(cudaError_t err, char const *what);
+#define GWNB_CUDA_TRY(expr)                                                                        \
+    do {                                                                                           \
+        cudaError_t gwnb_err_ = (expr);                                                            \
+        if (gwnb_err_ != cudaSuccess)                                                              \
+            return ::gwnb::set_cuda_error(gwnb_err_, #expr);                                       \
+    } while (0)
+#define GWNB_TRY(expr)                                                                             \
+    do {                                                                                           \
+        int gwnb_rc_ = (expr);                                                                     \
+        if (gwnb_rc_ != GWNB_OK)                                                                   \
+            return gwnb_rc_;                                                                       \
+    } while (0)
+
+std::uint64_t reserve_revision();
+int device_sm_count();
+
+// ---- allocation (stream ordered) ---------------------------------------------------------------
+template <class T> int alloc(T **ptr, std::size_t count, cudaStream_t s) {
+    *ptr = nullptr;
+    if (count == 0)
+        return GWNB_OK;
+    void *p = nullptr;
+    cudaError_t e = cudaMallocAsync(&p, count * sizeof(T), s);
+    if (e != cudaSuccess)
+        return set_cuda_error(e, "cudaMallocAsync");
+    *ptr = static_cast<T *>(p);
+    return GWNB_OK;
+}
+template <class T> void release(T *&ptr, cudaStream_t s) {
+    if (ptr != nullptr)
+        (void)cudaFreeAsync(ptr, s);
+    ptr = nullptr;
+}
+
+// ---- cross-TU kernels / launchers ---------------------------------------------------------------
+int radix_sort_pairs(void const *keys_in, void *keys_out, std::uint32_t const *values_in,
+                     std::uint32_t *values_out, std::uint64_t n, int key_bytes, int key_bits,
+                     cudaStream_t s, unsigned int *status);
+
+int create_bvh_aux(gwnb_bvh4_f32 *bvh, cudaStream_t s);
+int ensure_bvh_aux(gwnb_bvh4_f32 *bvh, cudaStream_t s);
+int write_tri48(gwnb_bvh4_f32 const *bvh, cudaStream_t s);
+
+__device__ inline unsigned int lane_id() { return threadIdx.x & 31u; }
+
+// min/max with the operand order of std::min / std::max (keeps signed-zero choices identical).
+__host__ __device__ inline float rmin(float a, float b) { return (b < a) ? b : a; }
+__host__ __device__ inline float rmax(float a, float b) { return (a < b) ? b : a; }
+
+__device__ inline aabb aabb_union(aabb const &l, aabb const &r) {
+    return aabb{rmin(l.min_x, r.min_x), rmin(l.min_y, r.min_y), rmin(l.min_z, r.min_z),
+                rmax(l.max_x, r.max_x), rmax(l.max_y, r.max_y), rmax(l.max_z, r.max_z)};
+}
+
+// Half surface area with explicit round-to-nearest operations so that the result does not
+// depend on floating-point contraction choices.
+__device__ inline float aabb_half_area(aabb const &b) {
+    float const dx = rmax(__fsub_rn(b.max_x, b.min_x), 0.0f);
+    float const dy = rmax(__fsub_rn(b.max_y, b.min_y), 0.0f);
+    float const dz = rmax(__fsub_rn(b.max_z, b.min_z), 0.0f);
+    return __fadd_rn(__fadd_rn(__fmul_rn(dx, dy), __fmul_rn(dy, dz)), __fmul_rn(dz, dx));
+}
+
+// Loads that bypass L1: data written by other SMs during the same kernel.
+__device__ inline float4 ldcg4(float4 const *p) { return __ldcg(p); }
+
+} // namespace gwnb

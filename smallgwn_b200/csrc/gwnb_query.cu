@@ -1,0 +1,610 @@
+// Winding-number queries.
+//
+// Exact batch (replaces gwn_compute_winding_number_exact_batch, gwn_query.cuh:308-346): every CTA
+// stages tiles of triangle records in shared memory, each thread evaluates its queries against
+// the tile with broadcast shared loads. The solid angle is the Van Oosterom-Strackee formula in
+// unnormalised form, tan(Omega/2) = a.(e1 x e2) / (|a||b||c| + (a.b)|c| + (a.c)|b| + (b.c)|a|),
+// which equals smallgwn's unit-vector form (detail/gwn_query_geometry_impl.cuh:16-45) and keeps
+// its conventions: zero when the query sits on a vertex or the numerator vanishes.
+//
+// Taylor batch (replaces gwn_compute_winding_number_taylor_batch, gwn_query.cuh:384-445): the
+// traversal order, acceptance test and far-field terms follow detail/gwn_query_winding_impl.cuh
+// :101-374 (accept a child iff |q-P|^2 > 0, |q-P|^2 > r^2 beta^2 and the expansion is finite;
+// otherwise enter internal children, the last directly and the others through the stack, and sum
+// leaf triangles exactly). Differences: the batch is Morton-ordered internally for coherence, node
+// data comes from a per-node query sidecar with 128-bit loads, the stack lives in shared memory,
+// and stack overflow writes NaN and raises a device error bit instead of trapping.
+#include "gwnb_internal.cuh"
+
+#include <algorithm>
+
+namespace gwnb {
+namespace {
+
+constexpr float k_pi_f = 3.14159265358979323846f;
+
+// ---- exact solid angle ---------------------------------------------------------------------------
+
+// a = v0 - q, e1, e2 edges, n = e1 x e2.
+__device__ __forceinline__ float solid_angle_plain(float ax, float ay, float az, float e1x, float e1y,
+                                                   float e1z, float e2x, float e2y, float e2z,
+                                                   float nx, float ny, float nz) {
+    float const bx = ax + e1x, by = ay + e1y, bz = az + e1z;
+    float const cx = ax + e2x, cy = ay + e2y, cz = az + e2z;
+    float const a2 = ax * ax + ay * ay + az * az;
+    float const b2 = bx * bx + by * by + bz * bz;
+    float const c2 = cx * cx + cy * cy + cz * cz;
+    float const la = sqrtf(a2), lb = sqrtf(b2), lc = sqrtf(c2);
+    if (la == 0.0f || lb == 0.0f || lc == 0.0f)
+        return 0.0f;
+    float const num = ax * nx + ay * ny + az * nz;
+    if (num == 0.0f)
+        return 0.0f;
+    float const ab = ax * bx + ay * by + az * bz;
+    float const ac = ax * cx + ay * cy + az * cz;
+    float const bc = bx * cx + by * cy + bz * cz;
+    float const den = la * lb * lc + ab * lc + ac * lb + bc * la;
+    return 2.0f * atan2f(num, den);
+}
+
+// Error-free transformations (Dekker / Ogita-Rump-Oishi "Accurate sum and dot product", 2005).
+__device__ __forceinline__ void two_prod(float a, float b, float &p, float &e) {
+    p = a * b;
+    e = fmaf(a, b, -p);
+}
+__device__ __forceinline__ void two_sum(float a, float b, float &s, float &e) {
+    s = a + b;
+    float const z = s - a;
+    e = (a - (s - z)) + (b - z);
+}
+// Compensated dot product of length 3 (Dot2).
+__device__ __forceinline__ float dot3_comp(float a0, float a1, float a2, float b0, float b1, float b2) {
+    float p, s, h, r, q;
+    two_prod(a0, b0, p, s);
+    two_prod(a1, b1, h, r);
+    two_sum(p, h, p, q);
+    s += q + r;
+    two_prod(a2, b2, h, r);
+    two_sum(p, h, p, q);
+    s += q + r;
+    return p + s;
+}
+
+// Compensated near field: numerator a.(e1 x e2) with compensated cross and dot products, the
+// denominator from compensated dots; triangles whose denominator and numerator are both small
+// relative to |a||b||c| (query close to an edge or vertex line) take an FP64 evaluation.
+__device__ __forceinline__ float solid_angle_comp(float ax, float ay, float az, float e1x, float e1y,
+                                                  float e1z, float e2x, float e2y, float e2z,
+                                                  float threshold, unsigned long long *fp64_count) {
+    float const bx = ax + e1x, by = ay + e1y, bz = az + e1z;
+    float const cx = ax + e2x, cy = ay + e2y, cz = az + e2z;
+    float const a2 = dot3_comp(ax, ay, az, ax, ay, az);
+    float const b2 = dot3_comp(bx, by, bz, bx, by, bz);
+    float const c2 = dot3_comp(cx, cy, cz, cx, cy, cz);
+    float const la = sqrtf(a2), lb = sqrtf(b2), lc = sqrtf(c2);
+    if (la == 0.0f || lb == 0.0f || lc == 0.0f)
+        return 0.0f;
+    // n = e1 x e2, each component a compensated 2-term difference of products
+    float const nx = dot3_comp(e1y, -e1z, 0.0f, e2z, e2y, 0.0f);
+    float const ny = dot3_comp(e1z, -e1x, 0.0f, e2x, e2z, 0.0f);
+    float const nz = dot3_comp(e1x, -e1y, 0.0f, e2y, e2x, 0.0f);
+    float const num = dot3_comp(ax, ay, az, nx, ny, nz);
+    float const ab = dot3_comp(ax, ay, az, bx, by, bz);
+    float const ac = dot3_comp(ax, ay, az, cx, cy, cz);
+    float const bc = dot3_comp(bx, by, bz, cx, cy, cz);
+    float const labc = la * lb * lc;
+    float const den = labc + dot3_comp(ab, ac, bc, lc, lb, la);
+    float const scale = labc;
+    if (fabsf(den) < threshold * scale && fabsf(num) < threshold * scale) {
+        if (fp64_count != nullptr)
+            atomicAdd(fp64_count, 1ull);
+        double const dax = ax, day = ay, daz = az;
+        double const dbx = dax + e1x, dby = day + e1y, dbz = daz + e1z;
+        double const dcx = dax + e2x, dcy = day + e2y, dcz = daz + e2z;
+        double const dla = sqrt(dax * dax + day * day + daz * daz);
+        double const dlb = sqrt(dbx * dbx + dby * dby + dbz * dbz);
+        double const dlc = sqrt(dcx * dcx + dcy * dcy + dcz * dcz);
+        double const dnx = static_cast<double>(e1y) * e2z - static_cast<double>(e1z) * e2y;
+        double const dny = static_cast<double>(e1z) * e2x - static_cast<double>(e1x) * e2z;
+        double const dnz = static_cast<double>(e1x) * e2y - static_cast<double>(e1y) * e2x;
+        double const dnum = dax * dnx + day * dny + daz * dnz;
+        if (dnum == 0.0)
+            return 0.0f;
+        double const dden = dla * dlb * dlc + (dax * dbx + day * dby + daz * dbz) * dlc +
+                            (dax * dcx + day * dcy + daz * dcz) * dlb +
+                            (dbx * dcx + dby * dcy + dbz * dcz) * dla;
+        return static_cast<float>(2.0 * atan2(dnum, dden));
+    }
+    if (num == 0.0f)
+        return 0.0f;
+    return 2.0f * atan2f(num, den);
+}
+
+// Gradient of the solid angle w.r.t. the query (Biot-Savart form), as smallgwn's
+// gwn_gradient_solid_angle_triangle_impl (detail/gwn_query_winding_impl.cuh:21-60).
+__device__ __forceinline__ float3 solid_angle_grad(float ax, float ay, float az, float e1x, float e1y,
+                                                   float e1z, float e2x, float e2y, float e2z) {
+    float3 const g[3] = {make_float3(ax, ay, az), make_float3(ax + e1x, ay + e1y, az + e1z),
+                         make_float3(ax + e2x, ay + e2y, az + e2z)};
+    float l[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+        l[i] = sqrtf(g[i].x * g[i].x + g[i].y * g[i].y + g[i].z * g[i].z);
+    if (l[0] == 0.0f || l[1] == 0.0f || l[2] == 0.0f)
+        return make_float3(0.0f, 0.0f, 0.0f);
+    float3 h[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+        h[i] = make_float3(g[i].x / l[i], g[i].y / l[i], g[i].z / l[i]);
+    float3 r = make_float3(0.0f, 0.0f, 0.0f);
+#pragma unroll
+    for (int e = 0; e < 3; ++e) {
+        int const i = e, j = (e + 1) % 3;
+        float3 const cr = make_float3(g[i].y * g[j].z - g[i].z * g[j].y, g[i].z * g[j].x - g[i].x * g[j].z,
+                                      g[i].x * g[j].y - g[i].y * g[j].x);
+        float const cs = cr.x * cr.x + cr.y * cr.y + cr.z * cr.z;
+        if (cs == 0.0f)
+            continue;
+        float const sc = ((g[i].x - g[j].x) * (h[i].x - h[j].x) + (g[i].y - g[j].y) * (h[i].y - h[j].y) +
+                          (g[i].z - g[j].z) * (h[i].z - h[j].z)) /
+                         cs;
+        r.x += sc * cr.x;
+        r.y += sc * cr.y;
+        r.z += sc * cr.z;
+    }
+    return r;
+}
+
+// ---- exact batch --------------------------------------------------------------------------------
+
+constexpr int k_exact_block = 256;
+constexpr int k_exact_tile = 256;
+constexpr int k_exact_q = 2; // queries per thread
+
+__global__ void __launch_bounds__(k_exact_block)
+    k_exact(triangle const *__restrict__ tris, std::uint64_t nt, float const *__restrict__ qx,
+            float const *__restrict__ qy, float const *__restrict__ qz, float *__restrict__ out,
+            std::uint64_t nq) {
+    __shared__ float4 s_tri[k_exact_tile][3];
+    std::uint64_t const base = static_cast<std::uint64_t>(blockIdx.x) * (k_exact_block * k_exact_q);
+    float px[k_exact_q], py[k_exact_q], pz[k_exact_q], acc[k_exact_q];
+#pragma unroll
+    for (int k = 0; k < k_exact_q; ++k) {
+        std::uint64_t const i = base + threadIdx.x + static_cast<std::uint64_t>(k) * k_exact_block;
+        bool const v = i < nq;
+        px[k] = v ? qx[i] : 0.0f;
+        py[k] = v ? qy[i] : 0.0f;
+        pz[k] = v ? qz[i] : 0.0f;
+        acc[k] = 0.0f;
+    }
+    for (std::uint64_t t0 = 0; t0 < nt; t0 += k_exact_tile) {
+        __syncthreads();
+        std::uint64_t const t = t0 + threadIdx.x;
+        if (threadIdx.x < k_exact_tile) {
+            if (t < nt) {
+                triangle const r = tris[t];
+                float const nx = r.e1_y * r.e2_z - r.e1_z * r.e2_y;
+                float const ny = r.e1_z * r.e2_x - r.e1_x * r.e2_z;
+                float const nz = r.e1_x * r.e2_y - r.e1_y * r.e2_x;
+                s_tri[threadIdx.x][0] = make_float4(r.v0_x, r.v0_y, r.v0_z, r.e1_x);
+                s_tri[threadIdx.x][1] = make_float4(r.e1_y, r.e1_z, r.e2_x, r.e2_y);
+                s_tri[threadIdx.x][2] = make_float4(r.e2_z, nx, ny, nz);
+            } else {
+                // padding triangle at infinity-free origin with zero edges contributes 0
+                s_tri[threadIdx.x][0] = make_float4(0, 0, 0, 0);
+                s_tri[threadIdx.x][1] = make_float4(0, 0, 0, 0);
+                s_tri[threadIdx.x][2] = make_float4(0, 0, 0, 0);
+            }
+        }
+        __syncthreads();
+        std::uint64_t const rem = nt - t0;
+        int const cnt = rem < static_cast<std::uint64_t>(k_exact_tile) ? static_cast<int>(rem) : k_exact_tile;
+#pragma unroll 2
+        for (int j = 0; j < cnt; ++j) {
+            float4 const A = s_tri[j][0];
+            float4 const B = s_tri[j][1];
+            float4 const C = s_tri[j][2];
+#pragma unroll
+            for (int k = 0; k < k_exact_q; ++k)
+                acc[k] += solid_angle_plain(A.x - px[k], A.y - py[k], A.z - pz[k], A.w, B.x, B.y, B.z,
+                                            B.w, C.x, C.y, C.z, C.w);
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < k_exact_q; ++k) {
+        std::uint64_t const i = base + threadIdx.x + static_cast<std::uint64_t>(k) * k_exact_block;
+        if (i < nq)
+            out[i] = acc[k] / (4.0f * k_pi_f);
+    }
+}
+
+// ---- query ordering -----------------------------------------------------------------------------
+
+__device__ inline std::uint32_t expand10(std::uint32_t v) {
+    std::uint32_t x = v & 0x3ffu;
+    x = (x | (x << 16)) & 0x030000ffu;
+    x = (x | (x << 8)) & 0x0300f00fu;
+    x = (x | (x << 4)) & 0x030c30c3u;
+    x = (x | (x << 2)) & 0x09249249u;
+    return x;
+}
+
+__global__ void __launch_bounds__(256)
+    k_query_codes(float const *__restrict__ qx, float const *__restrict__ qy,
+                  float const *__restrict__ qz, std::uint64_t n, aabb const *__restrict__ root,
+                  std::uint32_t *__restrict__ codes) {
+    std::uint64_t const i = static_cast<std::uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    aabb const b = *root;
+    float const ex = fmaxf(b.max_x - b.min_x, 1e-30f);
+    float const ey = fmaxf(b.max_y - b.min_y, 1e-30f);
+    float const ez = fmaxf(b.max_z - b.min_z, 1e-30f);
+    // a margin around the box keeps far queries spread as well
+    float const fx = (qx[i] - b.min_x) / ex * 0.5f + 0.25f;
+    float const fy = (qy[i] - b.min_y) / ey * 0.5f + 0.25f;
+    float const fz = (qz[i] - b.min_z) / ez * 0.5f + 0.25f;
+    auto q = [](float f) -> std::uint32_t {
+        f = fminf(fmaxf(f, 0.0f), 1.0f); // NaN -> 0
+        return static_cast<std::uint32_t>(f * 1023.0f);
+    };
+    codes[i] = (expand10(q(fx)) << 2) | (expand10(q(fy)) << 1) | expand10(q(fz));
+}
+
+// ---- Taylor traversal ---------------------------------------------------------------------------
+
+struct taylor_params {
+    float4 const *qnodes;
+    std::uint32_t const *qcounts;
+    triangle48 const *tri48;
+    std::uint64_t primitive_count;
+    std::uint64_t node_count;
+    std::uint64_t root_ref; // packed reference of the root
+    float const *qx;
+    float const *qy;
+    float const *qz;
+    std::uint32_t const *order; // sorted position -> query index (nullptr: identity)
+    float *out;
+    float *grad_x;
+    float *grad_y;
+    float *grad_z;
+    std::uint32_t *stat_nodes;
+    std::uint32_t *stat_far;
+    std::uint32_t *stat_near;
+    std::uint64_t n;
+    float beta2;
+    float fp64_threshold;
+    unsigned long long *fp64_count;
+    unsigned int *status;
+};
+
+template <int Order, int Cap, int Mode, bool Grad, bool Stats>
+__global__ void __launch_bounds__(256) k_taylor(taylor_params p) {
+    constexpr int Q = qnode_traits<Order>::k_f4_per_child;
+    extern __shared__ std::uint32_t s_stack[]; // [Cap][blockDim.x]
+    std::uint64_t const idx = static_cast<std::uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (idx >= p.n)
+        return;
+    std::uint32_t const qi = p.order != nullptr ? p.order[idx] : static_cast<std::uint32_t>(idx);
+    float const qx = p.qx[qi], qy = p.qy[qi], qz = p.qz[qi];
+    float omega = 0.0f;
+    float gx = 0.0f, gy = 0.0f, gz = 0.0f;
+    std::uint32_t st_nodes = 0, st_far = 0, st_near = 0;
+    unsigned const stride = blockDim.x;
+    std::uint32_t *const stack = s_stack + threadIdx.x;
+    int sp = 0;
+    bool overflow = false;
+
+    auto leaf = [&](std::uint32_t first, std::uint32_t cnt) {
+        for (std::uint32_t k = 0; k < cnt; ++k) {
+            std::uint64_t const t = static_cast<std::uint64_t>(first) + k;
+            if (t >= p.primitive_count)
+                break;
+            float4 const A = __ldg(&p.tri48[t].a);
+            float4 const B = __ldg(&p.tri48[t].b);
+            float4 const C = __ldg(&p.tri48[t].c);
+            float const ax = A.x - qx, ay = A.y - qy, az = A.z - qz;
+            if constexpr (Mode == GWNB_NEAR_COMPENSATED)
+                omega += solid_angle_comp(ax, ay, az, A.w, B.x, B.y, B.z, B.w, C.x, p.fp64_threshold,
+                                          p.fp64_count);
+            else
+                omega += solid_angle_plain(ax, ay, az, A.w, B.x, B.y, B.z, B.w, C.x, C.y, C.z, C.w);
+            if constexpr (Grad) {
+                float3 const g = solid_angle_grad(ax, ay, az, A.w, B.x, B.y, B.z, B.w, C.x);
+                gx += g.x;
+                gy += g.y;
+                gz += g.z;
+            }
+            if constexpr (Stats)
+                ++st_near;
+        }
+    };
+
+    if (ref_leaf(p.root_ref)) {
+        leaf(static_cast<std::uint32_t>(ref_offset(p.root_ref)), ref_count(p.root_ref));
+    } else {
+        std::uint32_t node = static_cast<std::uint32_t>(ref_offset(p.root_ref));
+        for (;;) {
+            if (node >= p.node_count)
+                break;
+            if constexpr (Stats)
+                ++st_nodes;
+            float4 const *nd = p.qnodes + static_cast<std::uint64_t>(node) * (4 * Q);
+            std::uint32_t next = k_invalid_u32;
+#pragma unroll
+            for (int s = 0; s < 4; ++s) {
+                float4 const a = __ldg(nd + s * Q);
+                if (a.w < 0.0f)
+                    continue;
+                float4 const b = __ldg(nd + s * Q + 1);
+                float const rx = qx - a.x, ry = qy - a.y, rz = qz - a.z;
+                float const q2 = rx * rx + ry * ry + rz * rz;
+                bool descend = !(q2 > 0.0f);
+                if (!descend)
+                    descend = q2 <= a.w * p.beta2;
+                if (!descend) {
+                    float const m1 = rsqrtf(q2);
+                    float const m2 = m1 * m1;
+                    float const m3 = m2 * m1;
+                    float const nx = rx * m1, ny = ry * m1, nz = rz * m1;
+                    float const rdn = nx * b.x + ny * b.y + nz * b.z;
+                    float w = -m2 * rdn;
+                    float g0 = 0.0f, g1 = 0.0f, g2 = 0.0f;
+                    if constexpr (Grad) {
+                        g0 = m3 * (3.0f * nx * rdn - b.x);
+                        g1 = m3 * (3.0f * ny * rdn - b.y);
+                        g2 = m3 * (3.0f * nz * rdn - b.z);
+                    }
+                    if constexpr (Order >= 1) {
+                        float4 const c = __ldg(nd + s * Q + 2);
+                        float4 const d = __ldg(nd + s * Q + 3);
+                        // c = (Nxx, Nyy, Nzz, Nxy+Nyx), d = (Nyz+Nzy, Nzx+Nxz, [Order 2 ...])
+                        float const T = c.x + c.y + c.z;
+                        float const S = nx * nx * c.x + ny * ny * c.y + nz * nz * c.z + nx * ny * c.w +
+                                        nx * nz * d.y + ny * nz * d.x;
+                        w += m3 * (T - 3.0f * S);
+                        if constexpr (Grad) {
+                            float const m4 = m2 * m2;
+                            float const vx = 2.0f * c.x * nx + c.w * ny + d.y * nz;
+                            float const vy = c.w * nx + 2.0f * c.y * ny + d.x * nz;
+                            float const vz = d.y * nx + d.x * ny + 2.0f * c.z * nz;
+                            float const co = 15.0f * S - 3.0f * T;
+                            g0 += m4 * (co * nx - 3.0f * vx);
+                            g1 += m4 * (co * ny - 3.0f * vy);
+                            g2 += m4 * (co * nz - 3.0f * vz);
+                        }
+                        if constexpr (Order >= 2) {
+                            float4 const e = __ldg(nd + s * Q + 4);
+                            float4 const f = __ldg(nd + s * Q + 5);
+                            // d.z = Nxxx, d.w = Nyyy, e = (Nzzz, spn, Axy, Axz), f = (Ayz, Ayx, Azx, Azy)
+                            float const xxx = d.z, yyy = d.w, zzz = e.x, spn = e.y;
+                            float const Axy = e.z, Axz = e.w, Ayz = f.x, Ayx = f.y, Azx = f.z, Azy = f.w;
+                            float const m4 = m2 * m2;
+                            float const nx2 = nx * nx, ny2 = ny * ny, nz2 = nz * nz;
+                            float const nx3 = nx2 * nx, ny3 = ny2 * ny, nz3 = nz2 * nz;
+                            float const t0x = Ayx + Azx, t0y = Azy + Axy, t0z = Axz + Ayz;
+                            float const t1x = ny * Axy + nz * Axz;
+                            float const t1y = nz * Ayz + nx * Ayx;
+                            float const t1z = nx * Azx + ny * Azy;
+                            w += m4 * (1.5f * (nx * (3.0f * xxx + t0x) + ny * (3.0f * yyy + t0y) +
+                                               nz * (3.0f * zzz + t0z)) -
+                                       7.5f * (nx3 * xxx + ny3 * yyy + nz3 * zzz + nx * ny * nz * spn +
+                                               nx2 * t1x + ny2 * t1y + nz2 * t1z));
+                            if constexpr (Grad) {
+                                float const m5 = m4 * m1;
+                                float const Px = 3.0f * xxx + Ayx + Azx;
+                                float const Py = 3.0f * yyy + Azy + Axy;
+                                float const Pz = 3.0f * zzz + Axz + Ayz;
+                                float const L2 = nx * Px + ny * Py + nz * Pz;
+                                float const C2 = nx3 * xxx + ny3 * yyy + nz3 * zzz + nx * ny * nz * spn +
+                                                 nx2 * (ny * Axy + nz * Axz) + ny2 * (nz * Ayz + nx * Ayx) +
+                                                 nz2 * (nx * Azx + ny * Azy);
+                                float const Rx = 3.0f * xxx * nx2 + 2.0f * Axy * nx * ny + 2.0f * Axz * nx * nz +
+                                                 Ayx * ny2 + Azx * nz2 + spn * ny * nz;
+                                float const Ry = 3.0f * yyy * ny2 + 2.0f * Ayx * nx * ny + 2.0f * Ayz * ny * nz +
+                                                 Axy * nx2 + Azy * nz2 + spn * nx * nz;
+                                float const Rz = 3.0f * zzz * nz2 + 2.0f * Azx * nx * nz + 2.0f * Azy * ny * nz +
+                                                 Axz * nx2 + Ayz * ny2 + spn * nx * ny;
+                                float const h = 52.5f * C2;
+                                g0 += m5 * (1.5f * Px - 7.5f * (nx * L2 + Rx) + nx * h);
+                                g1 += m5 * (1.5f * Py - 7.5f * (ny * L2 + Ry) + ny * h);
+                                g2 += m5 * (1.5f * Pz - 7.5f * (nz * L2 + Rz) + nz * h);
+                            }
+                        }
+                    }
+                    if (isfinite(w)) {
+                        omega += w;
+                        if constexpr (Grad) {
+                            gx += g0;
+                            gy += g1;
+                            gz += g2;
+                        }
+                        if constexpr (Stats)
+                            ++st_far;
+                        continue;
+                    }
+                }
+                std::uint32_t const ref = __float_as_uint(b.w);
+                if ((ref & k_qref_leaf) == 0u) {
+                    if (next != k_invalid_u32) {
+                        if (sp >= Cap) {
+                            overflow = true;
+                            break;
+                        }
+                        stack[static_cast<unsigned>(sp) * stride] = next;
+                        ++sp;
+                    }
+                    next = ref;
+                } else {
+                    std::uint32_t const cnt = (ref & k_qref_multi) ? p.qcounts[static_cast<std::uint64_t>(node) * 4 + s] : 1u;
+                    leaf(ref & k_qref_index_mask, cnt);
+                }
+            }
+            if (overflow)
+                break;
+            if (next != k_invalid_u32) {
+                node = next;
+                continue;
+            }
+            if (sp == 0)
+                break;
+            --sp;
+            node = stack[static_cast<unsigned>(sp) * stride];
+        }
+    }
+    float const inv4pi = 1.0f / (4.0f * k_pi_f);
+    if (overflow) {
+        atomicOr(p.status, k_err_stack_overflow);
+        float const nan = __int_as_float(0x7fc00000);
+        if (p.out != nullptr)
+            p.out[qi] = nan;
+        if constexpr (Grad) {
+            p.grad_x[qi] = nan;
+            p.grad_y[qi] = nan;
+            p.grad_z[qi] = nan;
+        }
+        return;
+    }
+    if (p.out != nullptr)
+        p.out[qi] = omega / (4.0f * k_pi_f);
+    if constexpr (Grad) {
+        p.grad_x[qi] = gx * inv4pi;
+        p.grad_y[qi] = gy * inv4pi;
+        p.grad_z[qi] = gz * inv4pi;
+    }
+    if constexpr (Stats) {
+        p.stat_nodes[qi] = st_nodes;
+        p.stat_far[qi] = st_far;
+        p.stat_near[qi] = st_near;
+    }
+}
+
+template <int Order, int Cap, int Mode, bool Grad, bool Stats>
+int launch_taylor_cap(taylor_params const &p, int block, cudaStream_t s) {
+    std::size_t const smem = static_cast<std::size_t>(Cap) * block * sizeof(std::uint32_t);
+    auto kern = k_taylor<Order, Cap, Mode, Grad, Stats>;
+    if (smem > 48 * 1024)
+        GWNB_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           static_cast<int>(smem)));
+    unsigned const grid = static_cast<unsigned>((p.n + block - 1) / block);
+    kern<<<grid, block, smem, s>>>(p);
+    GWNB_CUDA_TRY(cudaGetLastError());
+    return GWNB_OK;
+}
+
+template <int Order, int Mode, bool Grad, bool Stats>
+int launch_taylor_mode(taylor_params const &p, int block, int cap, cudaStream_t s) {
+    if (cap <= 16)
+        return launch_taylor_cap<Order, 16, Mode, Grad, Stats>(p, block, s);
+    if (cap <= 32)
+        return launch_taylor_cap<Order, 32, Mode, Grad, Stats>(p, block, s);
+    if (cap <= 64)
+        return launch_taylor_cap<Order, 64, Mode, Grad, Stats>(p, block, s);
+    return launch_taylor_cap<Order, 128, Mode, Grad, Stats>(p, block, s);
+}
+
+template <int Order, bool Grad, bool Stats>
+int launch_taylor_order(taylor_params const &p, int block, int cap, int mode, cudaStream_t s) {
+    if (mode == GWNB_NEAR_COMPENSATED)
+        return launch_taylor_mode<Order, GWNB_NEAR_COMPENSATED, Grad, Stats>(p, block, cap, s);
+    return launch_taylor_mode<Order, GWNB_NEAR_PLAIN, Grad, Stats>(p, block, cap, s);
+}
+
+} // namespace
+
+int exact_batch(triangle const *tris, std::uint64_t nt, float const *qx, float const *qy,
+                float const *qz, float *out, std::uint64_t nq, cudaStream_t s) {
+    if (nq == 0)
+        return GWNB_OK;
+    unsigned const grid = static_cast<unsigned>((nq + k_exact_block * k_exact_q - 1) / (k_exact_block * k_exact_q));
+    k_exact<<<grid, k_exact_block, 0, s>>>(tris, nt, qx, qy, qz, out, nq);
+    GWNB_CUDA_TRY(cudaGetLastError());
+    return GWNB_OK;
+}
+
+struct taylor_request {
+    int order;
+    float4 const *qnodes;
+    std::uint32_t const *qcounts;
+    triangle48 const *tri48;
+    std::uint64_t primitive_count;
+    std::uint64_t node_count;
+    std::uint64_t root_ref;
+    aabb const *root_bounds; // device
+    float const *qx, *qy, *qz;
+    float *out, *gx, *gy, *gz;
+    std::uint32_t *stat_nodes, *stat_far, *stat_near;
+    std::uint64_t n;
+    float accuracy_scale;
+    int block;
+    int stack_capacity; // must already be >= the BVH's internal stack bound
+    int sort_queries;
+    int near_mode;
+    float fp64_threshold;
+    unsigned long long *fp64_count;
+    unsigned int *status;
+};
+
+int taylor_batch(taylor_request const &r, cudaStream_t s) {
+    if (r.n == 0)
+        return GWNB_OK;
+    taylor_params p{};
+    p.qnodes = r.qnodes;
+    p.qcounts = r.qcounts;
+    p.tri48 = r.tri48;
+    p.primitive_count = r.primitive_count;
+    p.node_count = r.node_count;
+    p.root_ref = r.root_ref;
+    p.qx = r.qx;
+    p.qy = r.qy;
+    p.qz = r.qz;
+    p.out = r.out;
+    p.grad_x = r.gx;
+    p.grad_y = r.gy;
+    p.grad_z = r.gz;
+    p.stat_nodes = r.stat_nodes;
+    p.stat_far = r.stat_far;
+    p.stat_near = r.stat_near;
+    p.n = r.n;
+    p.beta2 = r.accuracy_scale * r.accuracy_scale;
+    p.fp64_threshold = r.fp64_threshold;
+    p.fp64_count = r.fp64_count;
+    p.status = r.status;
+    std::uint32_t *codes = nullptr, *sorted_codes = nullptr, *order = nullptr;
+    bool const sorted = r.sort_queries != 0 && r.n > 1 && r.root_bounds != nullptr;
+    if (sorted) {
+        GWNB_TRY(alloc(&codes, r.n, s));
+        GWNB_TRY(alloc(&sorted_codes, r.n, s));
+        GWNB_TRY(alloc(&order, r.n, s));
+        k_query_codes<<<static_cast<unsigned>((r.n + 255) / 256), 256, 0, s>>>(r.qx, r.qy, r.qz, r.n,
+                                                                            r.root_bounds, codes);
+        GWNB_TRY(radix_sort_pairs(codes, sorted_codes, nullptr, order, r.n, 4, 30, s, r.status));
+        p.order = order;
+    }
+    bool const grad = r.gx != nullptr;
+    bool const stats = r.stat_nodes != nullptr;
+    int rc = GWNB_OK;
+    int const block = r.block > 0 ? r.block : 256;
+    int const cap = r.stack_capacity;
+#define GWNB_DISPATCH(O)                                                                           \
+    if (grad)                                                                                      \
+        rc = launch_taylor_order<O, true, false>(p, block, cap, r.near_mode, s);                   \
+    else if (stats)                                                                                \
+        rc = launch_taylor_order<O, false, true>(p, block, cap, r.near_mode, s);                   \
+    else                                                                                           \
+        rc = launch_taylor_order<O, false, false>(p, block, cap, r.near_mode, s);
+    if (r.order == 0) {
+        GWNB_DISPATCH(0)
+    } else if (r.order == 1) {
+        GWNB_DISPATCH(1)
+    } else {
+        GWNB_DISPATCH(2)
+    }
+#undef GWNB_DISPATCH
+    release(codes, s);
+    release(sorted_codes, s);
+    release(order, s);
+    return rc;
+}
+
+} // namespace gwnb
