@@ -1,0 +1,151 @@
+#pragma once
+
+/// \file gwn_query.cuh
+/// \brief Batch winding-number queries: exact, Taylor and Taylor gradient.
+///
+/// Template signatures follow smallgwn's include/gwn/gwn_query.cuh:41-61, :308-445 and :688-756.
+/// Batches validate their objects and spans, enqueue work on \p stream and return without
+/// synchronizing. Deliberate difference: the traversal never traps. A query that would overflow
+/// its stack writes NaN and raises a device error bit (read with gwnb_bvh4_sync_status_f32); the
+/// overflow-callback parameter is accepted for source compatibility and is not invoked, because
+/// device functors cannot cross the C ABI.
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+#include <type_traits>
+
+#include "gwn_bvh.cuh"
+#include "gwn_geometry.cuh"
+
+namespace gwn {
+
+inline constexpr int k_gwn_default_query_batch_block_size = 256;
+inline constexpr int k_gwn_default_traversal_stack_capacity = 64;
+
+struct gwn_query_batch_config {
+    int block_size = k_gwn_default_query_batch_block_size;
+    int stack_capacity = k_gwn_default_traversal_stack_capacity;
+};
+
+template <gwn_query_batch_config Config>
+concept gwn_query_batch_config_value = Config.block_size > 0 && Config.block_size <= 1024;
+
+template <gwn_query_batch_config Config>
+concept gwn_traversal_batch_config_value = gwn_query_batch_config_value<Config> && Config.stack_capacity > 0;
+
+/// Accepted for source compatibility; see the file comment.
+struct gwn_traversal_overflow_ignore {};
+
+/// Library-specific Taylor options (query ordering and near-field precision).
+struct gwn_taylor_batch_options {
+    bool sort_queries = true;
+    int near_precision = GWNB_NEAR_PLAIN;
+    float fp64_threshold = 1e-3f;
+};
+
+namespace detail {
+
+template <int Width, gwn_real_type Real, gwn_index_type Index>
+[[nodiscard]] inline gwnb_bvh4_f32 query_view(gwn_bvh_object<Width, Real, Index> const &bvh) noexcept {
+    auto &b = const_cast<gwn_bvh_object<Width, Real, Index> &>(bvh);
+    return to_gwnb(bvh.accessor(), object_access::aux(b), object_access::capacity(b));
+}
+
+template <int Width, gwn_real_type Real, gwn_index_type Index>
+inline void store_aux(gwn_bvh_object<Width, Real, Index> const &bvh, gwnb_bvh4_f32 const &v) noexcept {
+    object_access::aux(const_cast<gwn_bvh_object<Width, Real, Index> &>(bvh)) = v.aux;
+}
+
+template <class T>
+[[nodiscard]] inline gwn_status check_batch_spans(gwn_device_span<T const> x, gwn_device_span<T const> y,
+                                                  gwn_device_span<T const> z, std::size_t out_size) noexcept {
+    if (x.size() != y.size() || x.size() != z.size())
+        return gwn_status::invalid_argument("Query SoA spans must have identical lengths.");
+    if (x.size() != out_size)
+        return gwn_status::invalid_argument("Output span size must match query count.");
+    return gwn_status::ok();
+}
+
+} // namespace detail
+
+template <gwn_query_batch_config Config = gwn_query_batch_config{}, int Width, gwn_real_type Real,
+          gwn_index_type Index = std::uint32_t>
+    requires gwn_query_batch_config_value<Config>
+[[nodiscard]] gwn_status gwn_compute_winding_number_exact_batch(
+    gwn_bvh_object<Width, Real, Index> const &bvh, gwn_device_span<std::type_identity_t<Real> const> const qx,
+    gwn_device_span<std::type_identity_t<Real> const> const qy,
+    gwn_device_span<std::type_identity_t<Real> const> const qz, gwn_device_span<Real> const output,
+    cudaStream_t const stream = gwn_default_stream()
+) noexcept {
+    if constexpr (Width != 4 || !detail::k_supported<Real, Index>) {
+        return detail::unsupported_instantiation();
+    } else {
+        if (!bvh.accessor().is_valid())
+            return gwn_status::invalid_argument("BVH object contains no queryable data.");
+        GWN_RETURN_ON_ERROR(detail::check_batch_spans(qx, qy, qz, output.size()));
+        gwnb_bvh4_f32 v = detail::query_view(bvh);
+        int const rc = gwnb_winding_exact_batch_f32(&v, qx.data(), qy.data(), qz.data(), output.data(), output.size(),
+                                                    Config.block_size, detail::gwnb_stream(stream));
+        detail::store_aux(bvh, v);
+        return detail::gwnb_to_status(rc);
+    }
+}
+
+template <int Order, gwn_query_batch_config Config = gwn_query_batch_config{}, int Width, gwn_real_type Real,
+          gwn_index_type Index = std::uint32_t, typename OverflowCallback = gwn_traversal_overflow_ignore>
+    requires gwn_traversal_batch_config_value<Config>
+[[nodiscard]] gwn_status gwn_compute_winding_number_taylor_batch(
+    gwn_bvh_object<Width, Real, Index> const &bvh, gwn_bvh_moment_object<Width, Order, Real, Index> const &moment,
+    gwn_device_span<std::type_identity_t<Real> const> const qx,
+    gwn_device_span<std::type_identity_t<Real> const> const qy,
+    gwn_device_span<std::type_identity_t<Real> const> const qz, gwn_device_span<Real> const output,
+    Real const accuracy_scale = Real(2), cudaStream_t const stream = gwn_default_stream(),
+    OverflowCallback const & = {}, gwn_taylor_batch_options const options = {}
+) noexcept {
+    static_assert(Order == 0 || Order == 1 || Order == 2, "Taylor order must be 0, 1, or 2.");
+    if constexpr (Width != 4 || !detail::k_supported<Real, Index>) {
+        return detail::unsupported_instantiation();
+    } else {
+        GWN_RETURN_ON_ERROR(detail::check_batch_spans(qx, qy, qz, output.size()));
+        gwnb_bvh4_f32 v = detail::query_view(bvh);
+        gwnb_moment4_f32 m = moment.view();
+        gwnb_taylor_options o{Config.block_size, Config.stack_capacity, options.sort_queries ? 1 : 0,
+                              options.near_precision, options.fp64_threshold};
+        int const rc = gwnb_winding_taylor_batch_f32(&v, &m, qx.data(), qy.data(), qz.data(), output.data(),
+                                                     output.size(), accuracy_scale, &o, detail::gwnb_stream(stream));
+        detail::store_aux(bvh, v);
+        return detail::gwnb_to_status(rc);
+    }
+}
+
+template <int Order, gwn_query_batch_config Config = gwn_query_batch_config{}, int Width, gwn_real_type Real,
+          gwn_index_type Index = std::uint32_t, typename OverflowCallback = gwn_traversal_overflow_ignore>
+    requires gwn_traversal_batch_config_value<Config>
+[[nodiscard]] gwn_status gwn_compute_winding_gradient_taylor_batch(
+    gwn_bvh_object<Width, Real, Index> const &bvh, gwn_bvh_moment_object<Width, Order, Real, Index> const &moment,
+    gwn_device_span<std::type_identity_t<Real> const> const qx,
+    gwn_device_span<std::type_identity_t<Real> const> const qy,
+    gwn_device_span<std::type_identity_t<Real> const> const qz, gwn_device_span<Real> const gx,
+    gwn_device_span<Real> const gy, gwn_device_span<Real> const gz, Real const accuracy_scale = Real(2),
+    cudaStream_t const stream = gwn_default_stream(), OverflowCallback const & = {}
+) noexcept {
+    if constexpr (Width != 4 || !detail::k_supported<Real, Index>) {
+        return detail::unsupported_instantiation();
+    } else {
+        GWN_RETURN_ON_ERROR(detail::check_batch_spans(qx, qy, qz, gx.size()));
+        if (gy.size() != gx.size() || gz.size() != gx.size())
+            return gwn_status::invalid_argument("Output span size must match query count.");
+        gwnb_bvh4_f32 v = detail::query_view(bvh);
+        gwnb_moment4_f32 m = moment.view();
+        gwnb_taylor_options o{Config.block_size, Config.stack_capacity, 1, GWNB_NEAR_PLAIN, 1e-3f};
+        int const rc = gwnb_winding_gradient_taylor_batch_f32(&v, &m, qx.data(), qy.data(), qz.data(), gx.data(),
+                                                              gy.data(), gz.data(), gx.size(), accuracy_scale, &o,
+                                                              detail::gwnb_stream(stream));
+        detail::store_aux(bvh, v);
+        return detail::gwnb_to_status(rc);
+    }
+}
+
+} // namespace gwn

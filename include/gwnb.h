@@ -271,6 +271,20 @@ GWNB_API int gwnb_winding_taylor_stats_f32(const gwnb_bvh4_f32 *bvh, const gwnb_
                                   uint32_t *far_evaluations, uint32_t *near_triangles,
                                   gwnb_stream_t stream);
 
+/* Exact winding numbers of the float mesh evaluated in FP64 (brute force over the geometry's
+ * triangles, double-precision Van Oosterom-Strackee). Counterpart of smallgwn's Real = double
+ * instantiation of gwn_compute_winding_number_exact_batch (tests/reference_cpu.cuh:84-114 is its
+ * CPU form); used as the FP64 error reference. query_* are float, output is double. */
+GWNB_API int gwnb_winding_exact_geometry_fp64(const gwnb_geometry_f32 *geometry, const float *query_x,
+                                              const float *query_y, const float *query_z, double *output,
+                                              uint64_t count, gwnb_stream_t stream);
+
+/* Morton order of a query batch relative to the BVH root bounds: order[i] is the index of the
+ * i-th query in traversal-coherent order (the permutation the Taylor batch applies internally when
+ * sort_queries is set). No smallgwn counterpart. */
+GWNB_API int gwnb_query_order_f32(const gwnb_bvh4_f32 *bvh, const float *query_x, const float *query_y,
+                                  const float *query_z, uint64_t count, uint32_t *order, gwnb_stream_t stream);
+
 /* Number of FP64 fallbacks taken by the last compensated Taylor batch on this BVH (device
  * counter read back with a synchronization). */
 GWNB_API int gwnb_bvh4_fp64_fallback_count(const gwnb_bvh4_f32 *bvh, uint64_t *count, gwnb_stream_t stream);

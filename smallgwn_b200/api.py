@@ -363,6 +363,23 @@ def taylor_traversal_stats(bvh: gwn_bvh4_object, moment: gwn_bvh4_moment_object,
     return _status(rc)
 
 
+def exact_winding_fp64(geometry: gwn_geometry_object, qx, qy, qz, out, stream=None) -> gwn_status:
+    """FP64 exact winding numbers of the float mesh (float32 queries, float64 output tensor)."""
+    bad = _check_spans(qx, qy, qz, out)
+    if bad is not None:
+        return bad
+    rc = _lib.load().gwnb_winding_exact_geometry_fp64(C.byref(geometry._view), _ptr(qx), _ptr(qy), _ptr(qz),
+                                                      _ptr(out), _numel(out), _stream(stream))
+    return _status(rc)
+
+
+def query_order(bvh: gwn_bvh4_object, qx, qy, qz, order, stream=None) -> gwn_status:
+    """Traversal-coherent (Morton) order of a query batch; `order` is an int32 CUDA tensor."""
+    rc = _lib.load().gwnb_query_order_f32(C.byref(bvh._view), _ptr(qx), _ptr(qy), _ptr(qz), _numel(qx), _ptr(order),
+                                          _stream(stream))
+    return _status(rc)
+
+
 def fp64_fallback_count(bvh: gwn_bvh4_object, stream=None) -> int:
     n = C.c_uint64(0)
     rc = _lib.load().gwnb_bvh4_fp64_fallback_count(C.byref(bvh._view), C.byref(n), _stream(stream))

@@ -75,6 +75,10 @@ int refit_moments_async(gwnb_bvh4_f32 const *bvh, gwnb_moment4_f32 *m, cudaStrea
 std::size_t moment_payload_bytes(int order);
 int exact_batch(triangle const *tris, std::uint64_t nt, float const *qx, float const *qy, float const *qz,
                 float *out, std::uint64_t nq, cudaStream_t s);
+int exact_batch_f64(gwnb_geometry_f32 const &g, float const *qx, float const *qy, float const *qz, double *out,
+                    std::uint64_t nq, cudaStream_t s);
+int query_order(aabb const *root_bounds, float const *qx, float const *qy, float const *qz, std::uint64_t n,
+                std::uint32_t *order, cudaStream_t s, unsigned int *status);
 struct taylor_request {
     int order;
     float4 const *qnodes;
@@ -762,6 +766,28 @@ int gwnb_winding_taylor_stats_f32(const gwnb_bvh4_f32 *b, const gwnb_moment4_f32
     gwnb_taylor_options o{256, 0, 1, GWNB_NEAR_PLAIN, 1e-3f};
     return taylor_common(b, m, qx, qy, qz, nullptr, nullptr, nullptr, nullptr, nodes, far_evals, near_tris, n, beta,
                          &o, stream);
+}
+
+int gwnb_winding_exact_geometry_fp64(const gwnb_geometry_f32 *g, const float *qx, const float *qy, const float *qz,
+                                     double *out, uint64_t n, gwnb_stream_t stream) {
+    if (!geometry_valid(g))
+        return set_error(GWNB_INVALID_ARGUMENT, "Geometry accessor is invalid.");
+    if (!has_storage(qx, n) || !has_storage(qy, n) || !has_storage(qz, n) || !has_storage(out, n))
+        return set_error(GWNB_INVALID_ARGUMENT, "Query/output spans must use non-null storage when non-empty.");
+    return exact_batch_f64(*g, qx, qy, qz, out, n, as_cuda(stream));
+}
+
+int gwnb_query_order_f32(const gwnb_bvh4_f32 *b_in, const float *qx, const float *qy, const float *qz, uint64_t n,
+                         uint32_t *order, gwnb_stream_t stream) {
+    if (!bvh_valid(b_in))
+        return set_error(GWNB_INVALID_ARGUMENT, "BVH object contains no queryable data.");
+    if (!has_storage(qx, n) || !has_storage(qy, n) || !has_storage(qz, n) || !has_storage(order, n))
+        return set_error(GWNB_INVALID_ARGUMENT, "Query/output spans must use non-null storage when non-empty.");
+    cudaStream_t const s = as_cuda(stream);
+    auto *b = const_cast<gwnb_bvh4_f32 *>(b_in);
+    GWNB_TRY(ensure_bvh_aux(b, s));
+    auto *a = reinterpret_cast<bvh_aux_impl *>(b->aux);
+    return query_order(a->root_bounds, qx, qy, qz, n, order, s, a->status);
 }
 
 int gwnb_bvh4_fp64_fallback_count(const gwnb_bvh4_f32 *b, uint64_t *count, gwnb_stream_t stream) {

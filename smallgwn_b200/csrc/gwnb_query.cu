@@ -218,6 +218,69 @@ __global__ void __launch_bounds__(k_exact_block)
     }
 }
 
+// ---- FP64 exact over the float geometry ---------------------------------------------------------
+
+constexpr int k_f64_tile = 128;
+
+__global__ void __launch_bounds__(k_exact_block)
+    k_exact_f64(gwnb_geometry_f32 g, float const *__restrict__ qx, float const *__restrict__ qy,
+                float const *__restrict__ qz, double *__restrict__ out, std::uint64_t nq) {
+    __shared__ double s_v[k_f64_tile][9];
+    std::uint64_t const i = static_cast<std::uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    double const px = i < nq ? qx[i] : 0.0, py = i < nq ? qy[i] : 0.0, pz = i < nq ? qz[i] : 0.0;
+    double acc = 0.0;
+    std::uint64_t const nt = g.triangle_count, nv = g.vertex_count;
+    for (std::uint64_t t0 = 0; t0 < nt; t0 += k_f64_tile) {
+        __syncthreads();
+        if (threadIdx.x < k_f64_tile) {
+            std::uint64_t const t = t0 + threadIdx.x;
+            bool ok = t < nt;
+            std::uint32_t a = 0, b = 0, c = 0;
+            if (ok) {
+                a = g.tri_i0[t];
+                b = g.tri_i1[t];
+                c = g.tri_i2[t];
+                ok = a < nv && b < nv && c < nv;
+            }
+            if (ok) {
+                s_v[threadIdx.x][0] = g.vertex_x[a];
+                s_v[threadIdx.x][1] = g.vertex_y[a];
+                s_v[threadIdx.x][2] = g.vertex_z[a];
+                s_v[threadIdx.x][3] = g.vertex_x[b];
+                s_v[threadIdx.x][4] = g.vertex_y[b];
+                s_v[threadIdx.x][5] = g.vertex_z[b];
+                s_v[threadIdx.x][6] = g.vertex_x[c];
+                s_v[threadIdx.x][7] = g.vertex_y[c];
+                s_v[threadIdx.x][8] = g.vertex_z[c];
+            } else {
+                for (int k = 0; k < 9; ++k)
+                    s_v[threadIdx.x][k] = 0.0; // degenerate point triangle contributes 0
+            }
+        }
+        __syncthreads();
+        std::uint64_t const rem = nt - t0;
+        int const cnt = rem < static_cast<std::uint64_t>(k_f64_tile) ? static_cast<int>(rem) : k_f64_tile;
+        for (int j = 0; j < cnt; ++j) {
+            double const ax = s_v[j][0] - px, ay = s_v[j][1] - py, az = s_v[j][2] - pz;
+            double const bx = s_v[j][3] - px, by = s_v[j][4] - py, bz = s_v[j][5] - pz;
+            double const cx = s_v[j][6] - px, cy = s_v[j][7] - py, cz = s_v[j][8] - pz;
+            double const la = sqrt(ax * ax + ay * ay + az * az);
+            double const lb = sqrt(bx * bx + by * by + bz * bz);
+            double const lc = sqrt(cx * cx + cy * cy + cz * cz);
+            if (la == 0.0 || lb == 0.0 || lc == 0.0)
+                continue;
+            double const num = ax * (by * cz - bz * cy) + ay * (bz * cx - bx * cz) + az * (bx * cy - by * cx);
+            if (num == 0.0)
+                continue;
+            double const den = la * lb * lc + (ax * bx + ay * by + az * bz) * lc + (ax * cx + ay * cy + az * cz) * lb +
+                               (bx * cx + by * cy + bz * cz) * la;
+            acc += 2.0 * atan2(num, den);
+        }
+    }
+    if (i < nq)
+        out[i] = acc / (4.0 * 3.141592653589793238462643383279502884);
+}
+
 // ---- query ordering -----------------------------------------------------------------------------
 
 __device__ inline std::uint32_t expand10(std::uint32_t v) {
@@ -520,6 +583,30 @@ int exact_batch(triangle const *tris, std::uint64_t nt, float const *qx, float c
     k_exact<<<grid, k_exact_block, 0, s>>>(tris, nt, qx, qy, qz, out, nq);
     GWNB_CUDA_TRY(cudaGetLastError());
     return GWNB_OK;
+}
+
+int exact_batch_f64(gwnb_geometry_f32 const &g, float const *qx, float const *qy, float const *qz, double *out,
+                    std::uint64_t nq, cudaStream_t s) {
+    if (nq == 0)
+        return GWNB_OK;
+    k_exact_f64<<<static_cast<unsigned>((nq + k_exact_block - 1) / k_exact_block), k_exact_block, 0, s>>>(
+        g, qx, qy, qz, out, nq);
+    GWNB_CUDA_TRY(cudaGetLastError());
+    return GWNB_OK;
+}
+
+int query_order(aabb const *root_bounds, float const *qx, float const *qy, float const *qz, std::uint64_t n,
+                std::uint32_t *order, cudaStream_t s, unsigned int *status) {
+    if (n == 0)
+        return GWNB_OK;
+    std::uint32_t *codes = nullptr, *sorted = nullptr;
+    GWNB_TRY(alloc(&codes, n, s));
+    GWNB_TRY(alloc(&sorted, n, s));
+    k_query_codes<<<static_cast<unsigned>((n + 255) / 256), 256, 0, s>>>(qx, qy, qz, n, root_bounds, codes);
+    int const rc = radix_sort_pairs(codes, sorted, nullptr, order, n, 4, 30, s, status);
+    release(codes, s);
+    release(sorted, s);
+    return rc;
 }
 
 struct taylor_request {

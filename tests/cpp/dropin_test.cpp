@@ -1,0 +1,203 @@
+// Drop-in API test: smallgwn-style C++ code (include/gwn/gwn.cuh) compiled by a plain C++20 host
+// compiler and linked against libgwnb.so. Each case restates one of smallgwn's unit tests:
+//   leaf-root build record          tests/unit_gwn_bvh.cu:93-139
+//   two-triangle query records      tests/unit_gwn_bvh.cu:141-218
+//   refit bounds and primitive order tests/unit_gwn_bvh.cu:220-287
+//   rejected options keep the BVH   tests/unit_gwn_bvh.cu:289-358
+//   exact vs CPU, asymmetric octahedron  tests/unit_gwn_query_winding.cu:193-215
+//   full-descent Taylor == exact    tests/unit_gwn_bvh_moment.cu:42-114
+//   stale moments are rejected      tests/unit_gwn_bvh_moment.cu:116-156
+// Exit code 0 when every check passes; `--compile-only` exits before touching the GPU.
+#include <gwn/gwn.cuh>
+
+#include <array>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+namespace {
+
+int g_failures = 0;
+
+#define CHECK(cond)                                                                                \
+    do {                                                                                           \
+        if (!(cond)) {                                                                             \
+            std::fprintf(stderr, "%s:%d: CHECK failed: %s\n", __FILE__, __LINE__, #cond);          \
+            ++g_failures;                                                                          \
+        }                                                                                          \
+    } while (0)
+
+using Real = float;
+using Index = std::uint32_t;
+
+template <class T> gwn::gwn_host_span<T const> hs(std::vector<T> const &v) { return {v.data(), v.size()}; }
+template <class T, std::size_t N> gwn::gwn_host_span<T const> hs(std::array<T, N> const &v) {
+    return {v.data(), v.size()};
+}
+
+struct dbuf {
+    float *p = nullptr;
+    std::size_t n = 0;
+    explicit dbuf(std::vector<float> const &h) : n(h.size()) {
+        cudaMalloc(&p, n * sizeof(float));
+        cudaMemcpy(p, h.data(), n * sizeof(float), cudaMemcpyHostToDevice);
+    }
+    explicit dbuf(std::size_t count) : n(count) { cudaMalloc(&p, n * sizeof(float)); }
+    ~dbuf() { cudaFree(p); }
+    std::vector<float> host() const {
+        std::vector<float> h(n);
+        cudaDeviceSynchronize();
+        cudaMemcpy(h.data(), p, n * sizeof(float), cudaMemcpyDeviceToHost);
+        return h;
+    }
+    gwn::gwn_device_span<float const> in() const { return {p, n}; }
+    gwn::gwn_device_span<float> out() { return {p, n}; }
+};
+
+template <class T> std::vector<T> to_host(cuda::std::span<T> s) {
+    std::vector<T> h(s.size());
+    cudaDeviceSynchronize();
+    cudaMemcpy(h.data(), s.data(), s.size_bytes(), cudaMemcpyDeviceToHost);
+    return h;
+}
+
+double cpu_winding(std::vector<float> const &x, std::vector<float> const &y, std::vector<float> const &z,
+                   std::vector<Index> const &i0, std::vector<Index> const &i1, std::vector<Index> const &i2,
+                   double qx, double qy, double qz) {
+    double sum = 0;
+    for (std::size_t t = 0; t < i0.size(); ++t) {
+        double a[3] = {x[i0[t]] - qx, y[i0[t]] - qy, z[i0[t]] - qz};
+        double b[3] = {x[i1[t]] - qx, y[i1[t]] - qy, z[i1[t]] - qz};
+        double c[3] = {x[i2[t]] - qx, y[i2[t]] - qy, z[i2[t]] - qz};
+        double la = std::sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]);
+        double lb = std::sqrt(b[0] * b[0] + b[1] * b[1] + b[2] * b[2]);
+        double lc = std::sqrt(c[0] * c[0] + c[1] * c[1] + c[2] * c[2]);
+        double num = a[0] * (b[1] * c[2] - b[2] * c[1]) + a[1] * (b[2] * c[0] - b[0] * c[2]) +
+                     a[2] * (b[0] * c[1] - b[1] * c[0]);
+        double den = la * lb * lc + (a[0] * b[0] + a[1] * b[1] + a[2] * b[2]) * lc +
+                     (a[0] * c[0] + a[1] * c[1] + a[2] * c[2]) * lb + (b[0] * c[0] + b[1] * c[1] + b[2] * c[2]) * la;
+        sum += 2 * std::atan2(num, den);
+    }
+    return sum / (4 * M_PI);
+}
+
+void leaf_root_build() {
+    std::vector<float> x{0, 1, 0}, y{0, 0, 1}, z{0, 0, 0};
+    std::vector<Index> i0{0}, i1{1}, i2{2};
+    gwn::gwn_geometry_object<Real, Index> geometry;
+    CHECK(gwn::gwn_upload_geometry(geometry, hs(x), hs(y), hs(z), hs(i0), hs(i1), hs(i2)).is_ok());
+    gwn::gwn_bvh4_object<Real, Index> bvh;
+    CHECK(gwn::gwn_build_bvh(geometry, bvh).is_ok());
+    auto const &a = bvh.accessor();
+    CHECK(a.is_valid() && a.has_leaf_root() && a.nodes.empty());
+    CHECK(a.root.offset() == 0 && a.root.primitive_count() == 1);
+    CHECK(a.root.bounds.min_x == 0 && a.root.bounds.max_x == 1 && a.root.bounds.max_y == 1 && a.root.bounds.max_z == 0);
+    auto tris = to_host(a.triangles);
+    CHECK(tris.size() == 1 && tris[0].e1_x == 1 && tris[0].e2_y == 1 && tris[0].v0_z == 0);
+}
+
+void two_triangle_records_and_refit() {
+    std::vector<float> x{0, 1, 0, 4, 6, 4}, y{0, 0, 2, 0, 0, 3}, z{1, 1, 1, -2, -2, -2};
+    std::vector<Index> i0{0, 3}, i1{1, 4}, i2{2, 5};
+    gwn::gwn_geometry_object<Real, Index> geometry;
+    CHECK(gwn::gwn_upload_geometry(geometry, hs(x), hs(y), hs(z), hs(i0), hs(i1), hs(i2)).is_ok());
+    gwn::gwn_bvh4_object<Real, Index> bvh;
+    CHECK(gwn::gwn_build_bvh(geometry, bvh, gwn::gwn_bvh_build_options{.method = gwn::gwn_bvh_build_method::k_lbvh})
+              .is_ok());
+    CHECK(bvh.accessor().nodes.size() == 1 && bvh.accessor().root.is_internal());
+    auto nodes = to_host(bvh.accessor().nodes);
+    int leaves = 0;
+    for (int s = 0; s < 4; ++s)
+        leaves += nodes[0].child(s).is_leaf() ? 1 : 0;
+    CHECK(leaves == 2);
+    auto order = to_host(bvh.accessor().primitive_indices);
+
+    x = {-7, -2, -7, 8, 11, 8};
+    y = {5, 5, 9, -4, -4, 2};
+    z = {3, 3, 3, -6, -6, -6};
+    CHECK(gwn::gwn_update_geometry(geometry, hs(x), hs(y), hs(z)).is_ok());
+    CHECK(gwn::gwn_refit_bvh(geometry, bvh).is_ok());
+    auto const &a = bvh.accessor();
+    CHECK(to_host(a.primitive_indices) == order);
+    CHECK(a.root.bounds.min_x == -7 && a.root.bounds.min_y == -4 && a.root.bounds.min_z == -6);
+    CHECK(a.root.bounds.max_x == 11 && a.root.bounds.max_y == 9 && a.root.bounds.max_z == 3);
+    auto tris = to_host(a.triangles);
+    for (std::size_t s = 0; s < tris.size(); ++s) {
+        Index const p = order[s];
+        CHECK(tris[s].v0_x == x[i0[p]] && tris[s].e1_y == y[i1[p]] - y[i0[p]] && tris[s].e2_z == z[i2[p]] - z[i0[p]]);
+    }
+}
+
+void rejected_options_keep_bvh() {
+    std::vector<float> x{0, 1, 0}, y{0, 0, 1}, z{0, 0, 0};
+    std::vector<Index> i0{0}, i1{1}, i2{2};
+    gwn::gwn_geometry_object<Real, Index> geometry;
+    CHECK(gwn::gwn_upload_geometry(geometry, hs(x), hs(y), hs(z), hs(i0), hs(i1), hs(i2)).is_ok());
+    gwn::gwn_bvh4_object<Real, Index> bvh;
+    CHECK(gwn::gwn_build_bvh(geometry, bvh).is_ok());
+    auto *prims = bvh.accessor().primitive_indices.data();
+    for (std::uint32_t r : {0u, 9u}) {
+        auto st = gwn::gwn_build_bvh(geometry, bvh, gwn::gwn_bvh_build_options{gwn::gwn_bvh_build_method::k_hploc, r});
+        CHECK(st.error() == gwn::gwn_error::invalid_argument);
+        CHECK(bvh.accessor().primitive_indices.data() == prims && bvh.has_data());
+    }
+    gwn::gwn_geometry_object<double, Index> dgeo;
+    std::vector<double> dx{0, 1, 0};
+    auto st = gwn::gwn_upload_geometry(dgeo, hs(dx), hs(dx), hs(dx), hs(i0), hs(i1), hs(i2));
+    CHECK(st.error() == gwn::gwn_error::invalid_argument);
+}
+
+void queries_match_cpu() {
+    std::vector<float> x{1.7f, -0.8f, 0.15f, -0.1f, 0.2f, -0.2f}, y{0.1f, -0.2f, 1.2f, -0.7f, 0.1f, -0.1f},
+        z{0, 0.1f, -0.1f, 0.15f, 1.5f, -0.9f};
+    std::vector<Index> i0{0, 2, 1, 3, 2, 1, 3, 0}, i1{2, 1, 3, 0, 0, 2, 1, 3}, i2{4, 4, 4, 4, 5, 5, 5, 5};
+    gwn::gwn_geometry_object<Real, Index> geometry;
+    CHECK(gwn::gwn_upload_geometry(geometry, hs(x), hs(y), hs(z), hs(i0), hs(i1), hs(i2)).is_ok());
+    gwn::gwn_bvh4_object<Real, Index> bvh;
+    CHECK(gwn::gwn_build_bvh(geometry, bvh).is_ok());
+    std::vector<float> qx{0, 4, -2, 0.2f, 1.5f}, qy{0, 3, 1, -1.4f, 0.2f}, qz{0, 2, -3, 2.2f, -1.8f};
+    dbuf dx(qx), dy(qy), dz(qz), exact(qx.size()), taylor(qx.size());
+    CHECK(gwn::gwn_compute_winding_number_exact_batch(bvh, dx.in(), dy.in(), dz.in(), exact.out()).is_ok());
+    gwn::gwn_bvh4_moment_object<1, Real, Index> moment;
+    CHECK(gwn::gwn_refit_bvh_moment<1>(bvh, moment).is_ok());
+    CHECK(moment.accessor().is_valid_for(bvh.accessor()));
+    CHECK(gwn::gwn_compute_winding_number_taylor_batch<1>(bvh, moment, dx.in(), dy.in(), dz.in(), taylor.out(),
+                                                          Real(1e6))
+              .is_ok());
+    auto he = exact.host();
+    auto ht = taylor.host();
+    for (std::size_t i = 0; i < qx.size(); ++i) {
+        double const ref = cpu_winding(x, y, z, i0, i1, i2, qx[i], qy[i], qz[i]);
+        CHECK(std::abs(he[i] - ref) <= 1e-5);
+        CHECK(std::abs(ht[i] - he[i]) <= 1e-6);
+    }
+    // a refit publishes a new revision: the old moments are stale
+    CHECK(gwn::gwn_refit_bvh(geometry, bvh).is_ok());
+    CHECK(!moment.accessor().is_valid_for(bvh.accessor()));
+    auto st = gwn::gwn_compute_winding_number_taylor_batch<1>(bvh, moment, dx.in(), dy.in(), dz.in(), taylor.out());
+    CHECK(st.error() == gwn::gwn_error::invalid_argument);
+    // stack capacity below the BVH's bound is rejected up front
+    constexpr gwn::gwn_query_batch_config k_tiny{256, 1};
+    CHECK(gwn::gwn_refit_bvh_moment<1>(bvh, moment).is_ok());
+    if (bvh.accessor().internal_stack_bound > 1) {
+        st = gwn::gwn_compute_winding_number_taylor_batch<1, k_tiny>(bvh, moment, dx.in(), dy.in(), dz.in(),
+                                                                     taylor.out());
+        CHECK(st.error() == gwn::gwn_error::invalid_argument);
+        CHECK(st.message().find("Traversal stack capacity") != std::string::npos);
+    }
+}
+
+} // namespace
+
+int main(int argc, char **argv) {
+    if (argc > 1 && std::strcmp(argv[1], "--compile-only") == 0)
+        return 0;
+    leaf_root_build();
+    two_triangle_records_and_refit();
+    rejected_options_keep_bvh();
+    queries_match_cpu();
+    if (g_failures == 0)
+        std::printf("dropin_test: all checks passed\n");
+    return g_failures == 0 ? 0 : 1;
+}

@@ -1,0 +1,125 @@
+"""The C ABI library loads, exports every symbol include/gwnb.h declares, and rejects invalid
+arguments before touching the GPU (CPU only: no kernel is launched here).
+
+Argument checks restate smallgwn's contract tests: invalid build method and H-PLOC radius 0 / 9
+(tests/unit_gwn_bvh.cu:289-358), empty BVH / stale moment / negative or NaN accuracy scale and span
+mismatches (tests/unit_gwn_query_winding.cu:245-313).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import re
+import subprocess
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from smallgwn_b200 import _lib, api
+
+HEADER = Path(__file__).resolve().parents[1] / "include" / "gwnb.h"
+
+
+def declared_symbols() -> set[str]:
+    text = HEADER.read_text()
+    return set(re.findall(r"GWNB_API[^;(]*?\b(gwnb_\w+)\s*\(", text))
+
+
+def test_every_declared_symbol_is_exported():
+    lib = _lib.load()
+    names = declared_symbols()
+    assert len(names) >= 20
+    for n in names:
+        assert hasattr(lib, n), n
+    out = subprocess.run(["nm", "-D", "--defined-only", str(_lib.library_path())], capture_output=True, text=True)
+    exported = set(re.findall(r" T (gwnb_\w+)", out.stdout))
+    assert names <= exported
+    assert set(_lib.SIGNATURES) == names
+
+
+def test_library_reports_version():
+    assert b"sm_100a" in _lib.load().gwnb_version()
+
+
+def test_structure_sizes_match_the_reference_layout():
+    assert C.sizeof(_lib.child_f32) == 32
+    assert C.sizeof(_lib.node4_f32) == 128
+    assert C.sizeof(_lib.triangle_f32) == 36
+    for order, fields in ((0, 7), (1, 13), (2, 23)):
+        assert _lib.load().gwnb_moment_node_bytes(order) == fields * 16
+
+
+def test_build_rejects_bad_options_without_gpu():
+    lib = _lib.load()
+    g = _lib.geometry_f32()
+    out = _lib.bvh4_f32()
+    assert lib.gwnb_bvh4_build_f32(C.byref(g), 7, 8, 64, C.byref(out), None) == _lib.GWNB_INVALID_ARGUMENT
+    assert "method" in _lib.last_error()
+    for radius in (0, 9):
+        assert lib.gwnb_bvh4_build_f32(C.byref(g), 0, radius, 64, C.byref(out), None) == _lib.GWNB_INVALID_ARGUMENT
+        assert "radius" in _lib.last_error()
+    assert lib.gwnb_bvh4_build_f32(C.byref(g), 1, 8, 16, C.byref(out), None) == _lib.GWNB_INVALID_ARGUMENT
+
+
+def test_python_mirror_rejects_bad_options_and_keeps_object():
+    geo = api.gwn_geometry_object()
+    bvh = api.gwn_bvh4_object()
+    st = api.gwn_build_bvh(geo, bvh, api.gwn_bvh_build_options(method=0, hploc_search_radius=9))
+    assert st.error == api.gwn_error.invalid_argument and not bvh.has_data()
+    st = api.gwn_upload_geometry(geo, [0, 1], [0, 1, 2], [0, 1], [0], [1], [2])
+    assert st.error == api.gwn_error.invalid_argument and not geo.has_data()
+
+
+def test_queries_reject_invalid_state_without_gpu():
+    lib = _lib.load()
+    empty = _lib.bvh4_f32()
+    mom = _lib.moment4_f32()
+    assert lib.gwnb_winding_exact_batch_f32(C.byref(empty), None, None, None, None, 0, 256, None) == \
+        _lib.GWNB_INVALID_ARGUMENT
+    assert "no queryable data" in _lib.last_error()
+    assert lib.gwnb_winding_taylor_batch_f32(C.byref(empty), C.byref(mom), None, None, None, None, 0, 2.0, None,
+                                             None) == _lib.GWNB_INVALID_ARGUMENT
+    # a syntactically valid leaf-root view (host pointers never dereferenced) with a stale moment
+    fake = _lib.bvh4_f32()
+    fake.primitive_count = 1
+    fake.primitive_indices = 8
+    fake.triangles = 8
+    fake.revision = 5
+    fake.root.reference = (1 << 47) | (1 << 48)
+    stale = _lib.moment4_f32(order=0, bvh_revision=4)
+    assert lib.gwnb_winding_taylor_batch_f32(C.byref(fake), C.byref(stale), None, None, None, None, 0, 2.0, None,
+                                             None) == _lib.GWNB_INVALID_ARGUMENT
+    assert "not aligned" in _lib.last_error()
+    fresh = _lib.moment4_f32(order=0, bvh_revision=5)
+    for beta in (-1.0, float("nan")):
+        assert lib.gwnb_winding_taylor_batch_f32(C.byref(fake), C.byref(fresh), None, None, None, None, 0, beta,
+                                                 None, None) == _lib.GWNB_INVALID_ARGUMENT
+        assert "accuracy scale" in _lib.last_error()
+    # non-empty batch with null storage
+    assert lib.gwnb_winding_exact_batch_f32(C.byref(fake), None, None, None, None, 3, 256, None) == \
+        _lib.GWNB_INVALID_ARGUMENT
+    assert "non-null storage" in _lib.last_error()
+
+
+def test_stack_capacity_below_bound_is_rejected():
+    lib = _lib.load()
+    fake = _lib.bvh4_f32()
+    fake.nodes = 8
+    fake.node_count = 3
+    fake.primitive_count = 9
+    fake.primitive_indices = 8
+    fake.triangles = 8
+    fake.revision = 5
+    fake.internal_stack_bound = 2
+    fake.root.reference = 1 << 47
+    mom = _lib.moment4_f32(order=1, bvh_revision=5, node_count=3, nodes=8, aux=8)
+    opt = _lib.taylor_options(256, 1, 1, 0, 1e-3)
+    rc = lib.gwnb_winding_taylor_batch_f32(C.byref(fake), C.byref(mom), None, None, None, None, 0, 2.0,
+                                           C.byref(opt), None)
+    assert rc == _lib.GWNB_INVALID_ARGUMENT
+    assert "Traversal stack capacity" in _lib.last_error()
+
+
+def test_status_mirror():
+    assert api.gwn_status().is_ok()
+    assert not api.gwn_status(api.gwn_error.internal_error, "x").is_ok()

@@ -1,0 +1,270 @@
+"""GPU parity of the winding-number queries against the oracle and smallgwn's own kernels.
+
+Tolerances: exact path 1e-5 absolute against the oracle's FP32 brute force (reference tolerance
+2e-6 against its CPU reference at tests/unit_gwn_query_winding.cu:193-215; the two FP32 formulas
+round differently); Taylor with beta = 1e6 equals exact within 1e-6
+(tests/unit_gwn_bvh_moment.cu:42-114); Taylor at beta = 2 against the oracle's traversal of the same
+tree and moments within 1e-5 (summation order differs). Contract checks restate
+tests/unit_gwn_query_winding.cu:222-313, tests/unit_gwn_bvh_moment.cu:116-268 and
+tests/unit_gwn_query_stack.cu:246-345; the gradient is checked against central differences as in
+tests/unit_gwn_query_gradient.cu:211-267.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import oracle
+import smallgwn_b200 as g
+from conftest import asym_octahedron, octahedron, single_triangle
+from smallgwn_b200 import api, meshes
+from test_gpu_build import WORKLOADS, build, upload
+
+pytestmark = pytest.mark.gpu
+
+EXACT_TOL = 1e-5
+
+
+def within(a, b, atol=EXACT_TOL, rtol=2e-5) -> bool:
+    """FP32-vs-FP32 agreement: atol + rtol * |w| (smallgwn's builder tests use 2e-5 + 2e-5 |w|,
+    tests/integration_gwn_builder.cu:228-233)."""
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return bool(np.all(np.abs(a - b) <= atol + rtol * np.maximum(np.abs(a), np.abs(b))))
+
+
+def dev(cuda, *arrs):
+    return [cuda.from_numpy(np.ascontiguousarray(a, np.float32)).cuda() for a in arrs]
+
+
+def run_exact(cuda, bvh, q):
+    d = dev(cuda, *q)
+    out = cuda.empty_like(d[0])
+    st = g.gwn_compute_winding_number_exact_batch(bvh, *d, out)
+    assert st.is_ok(), st.message
+    cuda.cuda.synchronize()
+    return out.cpu().numpy()
+
+
+def run_taylor(cuda, order, bvh, mom, q, beta, **kw):
+    d = dev(cuda, *q)
+    out = cuda.empty_like(d[0])
+    st = g.gwn_compute_winding_number_taylor_batch(order, bvh, mom, *d, out, accuracy_scale=beta, **kw)
+    assert st.is_ok(), st.message
+    cuda.cuda.synchronize()
+    return out.cpu().numpy()
+
+
+def moments_of(bvh, order):
+    m = g.gwn_bvh4_moment_object(order)
+    st = g.gwn_refit_bvh_moment(order, bvh, m)
+    assert st.is_ok(), st.message
+    return m
+
+
+@pytest.mark.parametrize("name", list(WORKLOADS))
+def test_exact_batch_matches_oracle(cuda, name):
+    mesh = WORKLOADS[name]()
+    bvh = build(upload(mesh))
+    q = meshes.mixed_queries(mesh, 3000, seed=4) if mesh["i0"].size > 100 else meshes.small_queries(3000)
+    out = run_exact(cuda, bvh, q)
+    ref = oracle.exact_winding(mesh, *q)
+    assert within(out, ref)
+    # where the two FP32 evaluations differ most, ours is no further from FP64 than the oracle's
+    ref64 = oracle.exact_winding(mesh, *q, fp64=True)
+    assert np.max(np.abs(out - ref64)) <= np.max(np.abs(ref - ref64)) + EXACT_TOL
+
+
+def test_exact_batch_small_workload_full(cuda):
+    mesh = meshes.small_mesh()
+    bvh = build(upload(mesh))
+    q = meshes.small_queries(100_000)
+    out = run_exact(cuda, bvh, q)
+    ref = oracle.exact_winding(mesh, *q)
+    err = np.abs(out - ref)
+    assert err.max() <= EXACT_TOL, err.max()
+
+
+@pytest.mark.parametrize("order", [0, 1, 2])
+@pytest.mark.parametrize("method", [g.gwn_bvh_build_method.k_lbvh, g.gwn_bvh_build_method.k_hploc])
+@pytest.mark.parametrize("name", ["icosphere4", "uv64x32", "soup40"])
+def test_taylor_matches_oracle_traversal(cuda, name, method, order):
+    mesh = WORKLOADS[name]()
+    bvh = build(upload(mesh), method)
+    mom = moments_of(bvh, order)
+    h = api.bvh_host_arrays(bvh)
+    mh = api.moment_host_array(mom)
+    q = meshes.mixed_queries(mesh, 4000, seed=6)
+    ref_mom = oracle.moments(order, h["nodes"], h["triangles"])
+    scale = np.abs(ref_mom).max(axis=(0, 2), keepdims=True) + 1e-12
+    assert np.max(np.abs(mh - ref_mom) / scale) < 1e-4
+    for sort in (True, False):
+        out = run_taylor(cuda, order, bvh, mom, q, 2.0, sort_queries=sort)
+        ref = oracle.taylor(order, h["nodes"], mh, h["triangles"], h["root_reference"], *q, beta=2.0)
+        assert within(out, ref)
+    full = run_taylor(cuda, order, bvh, mom, q, 1e6)
+    exact = run_exact(cuda, bvh, q)
+    assert within(full, exact, atol=1e-6, rtol=2e-6)
+
+
+@pytest.mark.parametrize("order", [0, 1, 2])
+def test_traversal_statistics_match_oracle(cuda, order):
+    mesh = WORKLOADS["uv64x32"]()
+    bvh = build(upload(mesh), g.gwn_bvh_build_method.k_hploc)
+    mom = moments_of(bvh, order)
+    h = api.bvh_host_arrays(bvh)
+    mh = api.moment_host_array(mom)
+    q = meshes.mixed_queries(mesh, 2000, seed=8)
+    d = dev(cuda, *q)
+    stats = [cuda.empty(2000, dtype=cuda.int32, device="cuda") for _ in range(3)]
+    assert api.taylor_traversal_stats(bvh, mom, *d, *stats, accuracy_scale=2.0).is_ok()
+    got = np.stack([s.cpu().numpy() for s in stats], -1)
+    _, ref = oracle.taylor(order, h["nodes"], mh, h["triangles"], h["root_reference"], *q, beta=2.0, stats=True)
+    # identical decisions except where an acceptance test sits within rounding of its threshold
+    assert np.mean(np.all(got == ref, axis=1)) > 0.995
+
+
+@pytest.mark.parametrize("method", [g.gwn_bvh_build_method.k_lbvh, g.gwn_bvh_build_method.k_hploc])
+def test_far_field_orders_reduce_error(cuda, method):
+    mesh = asym_octahedron()
+    bvh = build(upload(mesh), method)
+    q = [np.array(v, np.float32) for v in ([2.9, -2.7, 0.4, -0.6, 3.2, -2.8, 1.8, -2.1],
+                                          [0.4, -0.8, 3.1, -2.9, 2.2, 1.7, -2.6, 2.4],
+                                          [1.1, -0.5, 0.8, -1.2, -2.3, 2.5, 2.8, -2.5])]
+    ref = oracle.exact_winding(mesh, *q)
+    errs = [float(np.mean(np.abs(run_taylor(cuda, o, bvh, moments_of(bvh, o), q, 0.0) - ref))) for o in (0, 1, 2)]
+    assert errs[1] < errs[0] and errs[2] < errs[1] and errs[2] < 2e-3
+
+
+def test_nan_query_propagates(cuda):
+    mesh = asym_octahedron()
+    bvh = build(upload(mesh))
+    mom = moments_of(bvh, 2)
+    q = [np.array([np.nan], np.float32), np.array([0.25], np.float32), np.array([3.0], np.float32)]
+    assert np.isnan(run_exact(cuda, bvh, q)[0])
+    assert np.isnan(run_taylor(cuda, 2, bvh, mom, q, 0.0)[0])
+
+
+def test_leaf_root_taylor_equals_exact(cuda):
+    bvh = build(upload(single_triangle()))
+    mom = moments_of(bvh, 2)
+    q = [np.array([2.0], np.float32)] * 3
+    t = run_taylor(cuda, 2, bvh, mom, q, 0.0)
+    e = run_exact(cuda, bvh, q)
+    assert t[0] == pytest.approx(e[0], rel=1e-6)
+
+
+def test_batch_contract(cuda):
+    empty_bvh = g.gwn_bvh4_object()
+    empty_mom = g.gwn_bvh4_moment_object(0)
+    e = cuda.empty(0, device="cuda")
+    assert g.gwn_compute_winding_number_taylor_batch(0, empty_bvh, empty_mom, e, e, e, e).error == \
+        g.gwn_error.invalid_argument
+    assert g.gwn_compute_winding_number_exact_batch(empty_bvh, e, e, e, e).error == g.gwn_error.invalid_argument
+    bvh = build(upload(asym_octahedron()))
+    mom = moments_of(bvh, 0)
+    assert g.gwn_compute_winding_number_taylor_batch(0, bvh, mom, e, e, e, e).is_ok()
+    for beta in (-1.0, float("nan")):
+        assert g.gwn_compute_winding_number_taylor_batch(0, bvh, mom, e, e, e, e, accuracy_scale=beta).error == \
+            g.gwn_error.invalid_argument
+    assert g.gwn_compute_winding_number_exact_batch(bvh, e, e, e, e).is_ok()
+    one = cuda.empty(1, device="cuda")
+    assert g.gwn_compute_winding_number_taylor_batch(0, bvh, mom, e, e, e, one).error == g.gwn_error.invalid_argument
+    assert g.gwn_compute_winding_number_exact_batch(bvh, e, e, e, one).error == g.gwn_error.invalid_argument
+
+
+def test_stale_moments_rejected_after_rebuild_and_refit(cuda):
+    geo = upload(octahedron())
+    bvh = build(geo)
+    mom = moments_of(bvh, 1)
+    e = cuda.empty(0, device="cuda")
+    assert g.gwn_build_bvh(geo, bvh).is_ok()
+    assert not mom.is_valid_for(bvh)
+    assert g.gwn_compute_winding_number_taylor_batch(1, bvh, mom, e, e, e, e).error == g.gwn_error.invalid_argument
+    assert g.gwn_refit_bvh_moment(1, bvh, mom).is_ok() and mom.is_valid_for(bvh)
+    assert g.gwn_refit_bvh(geo, bvh).is_ok()
+    assert not mom.is_valid_for(bvh)
+    assert g.gwn_compute_winding_number_taylor_batch(1, bvh, mom, e, e, e, e).error == g.gwn_error.invalid_argument
+
+
+def test_stack_capacity_below_bound_rejected(cuda):
+    bvh = build(upload(octahedron()))
+    assert bvh.accessor().internal_stack_bound > 1
+    mom = moments_of(bvh, 1)
+    q = dev(cuda, [0.25], [0.25], [2.0])
+    out = cuda.empty(1, device="cuda")
+    st = g.gwn_compute_winding_number_taylor_batch(1, bvh, mom, *q, out,
+                                                   config=g.gwn_query_batch_config(stack_capacity=1))
+    assert st.error == g.gwn_error.invalid_argument and "Traversal stack capacity" in st.message
+
+
+def test_moment_replacement_on_other_stream(cuda):
+    s_a, s_b = cuda.cuda.Stream(), cuda.cuda.Stream()
+    geo = upload(octahedron(), s_a)
+    bvh = g.gwn_bvh4_object()
+    assert g.gwn_build_bvh(geo, bvh, stream=s_a).is_ok()
+    mom = g.gwn_bvh4_moment_object(0)
+    assert g.gwn_refit_bvh_moment(0, bvh, mom, s_a).is_ok()
+    n = 1 << 20
+    q = [cuda.zeros(n, device="cuda") for _ in range(3)]
+    out = cuda.empty(n, device="cuda")
+    s_a.synchronize()
+    assert g.gwn_compute_winding_number_taylor_batch(0, bvh, mom, *q, out, stream=s_a).is_ok()
+    assert g.gwn_refit_bvh_moment(0, bvh, mom, s_b).is_ok()
+    assert mom.stream() is s_b and mom.is_valid_for(bvh)
+    s_b.synchronize()
+    s_a.synchronize()
+
+
+@pytest.mark.parametrize("order", [1, 2])
+def test_gradient_matches_central_differences(cuda, order):
+    mesh = meshes.to_soa(*meshes.uv_sphere(48, 24, seed=31))
+    bvh = build(upload(mesh), g.gwn_bvh_build_method.k_hploc)
+    mom = moments_of(bvh, order)
+    rng = np.random.default_rng(3)
+    p = rng.uniform(-0.6, 0.6, size=(64, 3)).astype(np.float32)
+    p[32:] *= 3.0
+    q = [p[:, k].copy() for k in range(3)]
+    d = dev(cuda, *q)
+    gr = [cuda.empty(64, device="cuda") for _ in range(3)]
+    st = g.gwn_compute_winding_gradient_taylor_batch(order, bvh, mom, *d, *gr, accuracy_scale=1e6)
+    assert st.is_ok(), st.message
+    cuda.cuda.synchronize()
+    grad = np.stack([x.cpu().numpy() for x in gr], -1)
+    h = 1e-3
+    fd = np.zeros_like(grad)
+    for k in range(3):
+        qp = [c.astype(np.float64) for c in q]
+        qm = [c.astype(np.float64) for c in q]
+        qp[k] = qp[k] + h
+        qm[k] = qm[k] - h
+        wp = oracle.exact_winding(mesh, *qp, fp64=True)
+        wm = oracle.exact_winding(mesh, *qm, fp64=True)
+        fd[:, k] = (wp - wm) / (2 * h)
+    scale = np.abs(fd).max() + 1e-6
+    assert np.max(np.abs(grad - fd)) / scale < 3e-3
+
+
+@pytest.mark.skipif(oracle.ref_lib() is None, reason="smallgwn's own kernels (oracle/_ref) not built")
+@pytest.mark.parametrize("name", ["icosphere4", "uv64x32", "soup40"])
+def test_queries_match_reference_kernels(cuda, name):
+    mesh = WORKLOADS[name]()
+    bvh = build(upload(mesh))
+    R = oracle.Reference(mesh)
+    R.build(1, 8, 64)
+    q = meshes.mixed_queries(mesh, 4000, seed=12)
+    assert within(run_exact(cuda, bvh, q), R.exact(*q))
+    for order in (0, 1, 2):
+        mom = moments_of(bvh, order)
+        ref_m = R.moments(order)
+        mh = api.moment_host_array(mom)
+        scale = np.abs(ref_m).max(axis=(0, 2), keepdims=True) + 1e-12
+        assert np.max(np.abs(mh - ref_m) / scale) < 1e-4
+        ours = run_taylor(cuda, order, bvh, mom, q, 2.0)
+        theirs = R.taylor(order, *q, beta=2.0)
+        diff = np.abs(ours - theirs)
+        # identical trees and moments up to rounding: agreement is at summation-order level except
+        # for queries whose acceptance test sits at its threshold
+        assert np.quantile(diff, 0.999) <= EXACT_TOL
+        assert within(run_taylor(cuda, order, bvh, mom, q, 1e6), R.taylor(order, *q, beta=1e6))
+    R.close()
