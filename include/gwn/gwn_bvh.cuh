@@ -212,7 +212,7 @@ template <int Width, gwn_real_type Real, gwn_index_type Index>
         v.triangles = reinterpret_cast<gwnb_triangle_f32 *>(a.triangles.data());
         v.primitive_count = a.primitive_indices.size();
         static_assert(sizeof(v.root) == sizeof(a.root));
-        __builtin_memcpy(&v.root, &a.root, sizeof(v.root));
+        __builtin_memcpy(static_cast<void *>(&v.root), static_cast<void const *>(&a.root), sizeof(v.root));
         v.internal_stack_bound = a.internal_stack_bound;
         v.packed_stack_bound = a.packed_stack_bound;
         v.revision = a.revision;
@@ -229,7 +229,7 @@ inline void from_gwnb(gwnb_bvh4_f32 const &v, gwn_bvh_accessor<Width, Real, Inde
         a.primitive_indices = cuda::std::span<Index>(v.primitive_indices, v.primitive_count);
         a.triangles = cuda::std::span<gwn_bvh_triangle<Real>>(
             reinterpret_cast<gwn_bvh_triangle<Real> *>(v.triangles), v.primitive_count);
-        __builtin_memcpy(&a.root, &v.root, sizeof(a.root));
+        __builtin_memcpy(static_cast<void *>(&a.root), &v.root, sizeof(a.root));
         a.internal_stack_bound = v.internal_stack_bound;
         a.packed_stack_bound = v.packed_stack_bound;
         a.revision = v.revision;

@@ -120,6 +120,7 @@ typedef struct gwnb_taylor_options {
     int sort_queries;   /* 1: Morton-order the batch internally for traversal coherence          */
     int near_precision; /* GWNB_NEAR_PLAIN or GWNB_NEAR_COMPENSATED                               */
     float fp64_threshold; /* compensated mode: |den| < threshold * |a||b||c| takes the FP64 path */
+    int per_thread;       /* 0: warp-cooperative traversal (default); 1: one traversal per thread  */
 } gwnb_taylor_options;
 
 /* ---- status ------------------------------------------------------------------------------ */

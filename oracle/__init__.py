@@ -415,3 +415,32 @@ def binary_leaf_sets(nodes: np.ndarray, root: int) -> set:
         leaves[v] = s
     assert len(order) == n, "binary tree does not reach every internal node"
     return {frozenset(v) for v in leaves.values()}
+
+
+def match_wide_nodes(nodes_a: np.ndarray, root_a: int, nodes_b: np.ndarray, root_b: int) -> np.ndarray:
+    """Pair the nodes of two structurally identical BVH4s by walking both from the root in slot
+    order. Returns idx with nodes_b[idx[i]] corresponding to nodes_a[i]; raises if the trees differ."""
+    na = nodes_a.reshape(-1, 4)
+    nb = nodes_b.reshape(-1, 4)
+    if na.shape[0] != nb.shape[0]:
+        raise AssertionError("node counts differ")
+    idx = np.full(na.shape[0], -1, np.int64)
+    if na.shape[0] == 0:
+        return idx
+    off = (1 << 47) - 1
+    stack = [(int(root_a) & off, int(root_b) & off)]
+    while stack:
+        i, j = stack.pop()
+        idx[i] = j
+        for s in range(4):
+            ra, rb = int(na[i, s]["reference"]), int(nb[j, s]["reference"])
+            va, vb = (ra >> 47) & 1, (rb >> 47) & 1
+            if va != vb or (ra >> 48) != (rb >> 48):
+                raise AssertionError(f"trees differ at node {i}/{j} slot {s}")
+            if va and (ra >> 48) == 0:
+                stack.append((ra & off, rb & off))
+            elif va and (ra & off) != (rb & off):
+                raise AssertionError(f"leaf ranges differ at node {i}/{j} slot {s}")
+    if (idx < 0).any():
+        raise AssertionError("unreachable nodes")
+    return idx

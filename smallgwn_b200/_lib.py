@@ -80,6 +80,7 @@ class taylor_options(C.Structure):
         ("sort_queries", C.c_int),
         ("near_precision", C.c_int),
         ("fp64_threshold", C.c_float),
+        ("per_thread", C.c_int),
     ]
 
 

@@ -313,23 +313,25 @@ def gwn_compute_winding_number_exact_batch(bvh: gwn_bvh4_object, qx, qy, qz, out
     return _status(rc)
 
 
-def _options(config: gwn_query_batch_config, sort_queries: bool, precision: int, fp64_threshold: float):
+def _options(config: gwn_query_batch_config, sort_queries: bool, precision: int, fp64_threshold: float,
+             per_thread: bool = False):
     return _lib.taylor_options(int(config.block_size), int(config.stack_capacity), 1 if sort_queries else 0,
-                               int(precision), float(fp64_threshold))
+                               int(precision), float(fp64_threshold), 1 if per_thread else 0)
 
 
 def gwn_compute_winding_number_taylor_batch(order: int, bvh: gwn_bvh4_object, moment: gwn_bvh4_moment_object,
                                             qx, qy, qz, out, accuracy_scale: float = 2.0, stream=None,
                                             config: gwn_query_batch_config = gwn_query_batch_config(),
                                             sort_queries: bool = True, precision: int = near_precision.plain,
-                                            fp64_threshold: float = 1e-3) -> gwn_status:
-    """Taylor-approximated winding numbers of a device batch (asynchronous)."""
+                                            fp64_threshold: float = 1e-3, per_thread: bool = False) -> gwn_status:
+    """Taylor-approximated winding numbers of a device batch (asynchronous). ``per_thread``
+    selects one independent traversal per thread instead of the warp-cooperative traversal."""
     if moment.order != order:
         return gwn_status(gwn_error.invalid_argument, "Moment object order does not match the requested order.")
     bad = _check_spans(qx, qy, qz, out)
     if bad is not None:
         return bad
-    opt = _options(config, sort_queries, precision, fp64_threshold)
+    opt = _options(config, sort_queries, precision, fp64_threshold, per_thread)
     rc = _lib.load().gwnb_winding_taylor_batch_f32(
         C.byref(bvh._view), C.byref(moment._view), _ptr(qx), _ptr(qy), _ptr(qz), _ptr(out), _numel(out),
         float(accuracy_scale), C.byref(opt), _stream(stream))

@@ -79,29 +79,7 @@ int exact_batch_f64(gwnb_geometry_f32 const &g, float const *qx, float const *qy
                     std::uint64_t nq, cudaStream_t s);
 int query_order(aabb const *root_bounds, float const *qx, float const *qy, float const *qz, std::uint64_t n,
                 std::uint32_t *order, cudaStream_t s, unsigned int *status);
-struct taylor_request {
-    int order;
-    float4 const *qnodes;
-    std::uint32_t const *qcounts;
-    triangle48 const *tri48;
-    std::uint64_t primitive_count;
-    std::uint64_t node_count;
-    std::uint64_t root_ref;
-    aabb const *root_bounds;
-    float const *qx, *qy, *qz;
-    float *out, *gx, *gy, *gz;
-    std::uint32_t *stat_nodes, *stat_far, *stat_near;
-    std::uint64_t n;
-    float accuracy_scale;
-    int block;
-    int stack_capacity;
-    int sort_queries;
-    int near_mode;
-    float fp64_threshold;
-    unsigned long long *fp64_count;
-    unsigned int *status;
-};
-int taylor_batch(taylor_request const &r, cudaStream_t s);
+
 
 namespace {
 
@@ -734,6 +712,7 @@ static int taylor_common(const gwnb_bvh4_f32 *b_in, const gwnb_moment4_f32 *m, c
     r.stack_capacity = std::max<int>(static_cast<int>(b->internal_stack_bound), 1);
     r.sort_queries = o.sort_queries;
     r.near_mode = o.near_precision;
+    r.per_thread = o.per_thread;
     r.fp64_threshold = o.fp64_threshold;
     r.fp64_count = a->fp64_count;
     r.status = a->status;

@@ -170,6 +170,32 @@ int radix_sort_pairs(void const *keys_in, void *keys_out, std::uint32_t const *v
                      std::uint32_t *values_out, std::uint64_t n, int key_bytes, int key_bits,
                      cudaStream_t s, unsigned int *status);
 
+// One Taylor / gradient / statistics batch as the C ABI hands it to the query kernels.
+struct taylor_request {
+    int order;
+    float4 const *qnodes;
+    std::uint32_t const *qcounts;
+    triangle48 const *tri48;
+    std::uint64_t primitive_count;
+    std::uint64_t node_count;
+    std::uint64_t root_ref;
+    aabb const *root_bounds; // device
+    float const *qx, *qy, *qz;
+    float *out, *gx, *gy, *gz;
+    std::uint32_t *stat_nodes, *stat_far, *stat_near;
+    std::uint64_t n;
+    float accuracy_scale;
+    int block;
+    int stack_capacity; // already >= the BVH's internal stack bound
+    int sort_queries;
+    int near_mode;
+    int per_thread; // 1: one independent traversal per thread; 0: warp-cooperative
+    float fp64_threshold;
+    unsigned long long *fp64_count;
+    unsigned int *status;
+};
+int taylor_batch(taylor_request const &r, cudaStream_t s);
+
 int create_bvh_aux(gwnb_bvh4_f32 *bvh, cudaStream_t s);
 int ensure_bvh_aux(gwnb_bvh4_f32 *bvh, cudaStream_t s);
 int write_tri48(gwnb_bvh4_f32 const *bvh, cudaStream_t s);

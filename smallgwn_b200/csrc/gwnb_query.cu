@@ -316,6 +316,10 @@ __global__ void __launch_bounds__(256)
 
 // ---- Taylor traversal ---------------------------------------------------------------------------
 
+template <int Order, bool Grad>
+__device__ __forceinline__ float far_field(float rx, float ry, float rz, float q2, float4 const &b,
+                                           float4 const *__restrict__ cd, float &g0, float &g1, float &g2);
+
 struct taylor_params {
     float4 const *qnodes;
     std::uint32_t const *qcounts;
@@ -406,75 +410,8 @@ __global__ void __launch_bounds__(256) k_taylor(taylor_params p) {
                 if (!descend)
                     descend = q2 <= a.w * p.beta2;
                 if (!descend) {
-                    float const m1 = rsqrtf(q2);
-                    float const m2 = m1 * m1;
-                    float const m3 = m2 * m1;
-                    float const nx = rx * m1, ny = ry * m1, nz = rz * m1;
-                    float const rdn = nx * b.x + ny * b.y + nz * b.z;
-                    float w = -m2 * rdn;
                     float g0 = 0.0f, g1 = 0.0f, g2 = 0.0f;
-                    if constexpr (Grad) {
-                        g0 = m3 * (3.0f * nx * rdn - b.x);
-                        g1 = m3 * (3.0f * ny * rdn - b.y);
-                        g2 = m3 * (3.0f * nz * rdn - b.z);
-                    }
-                    if constexpr (Order >= 1) {
-                        float4 const c = __ldg(nd + s * Q + 2);
-                        float4 const d = __ldg(nd + s * Q + 3);
-                        // c = (Nxx, Nyy, Nzz, Nxy+Nyx), d = (Nyz+Nzy, Nzx+Nxz, [Order 2 ...])
-                        float const T = c.x + c.y + c.z;
-                        float const S = nx * nx * c.x + ny * ny * c.y + nz * nz * c.z + nx * ny * c.w +
-                                        nx * nz * d.y + ny * nz * d.x;
-                        w += m3 * (T - 3.0f * S);
-                        if constexpr (Grad) {
-                            float const m4 = m2 * m2;
-                            float const vx = 2.0f * c.x * nx + c.w * ny + d.y * nz;
-                            float const vy = c.w * nx + 2.0f * c.y * ny + d.x * nz;
-                            float const vz = d.y * nx + d.x * ny + 2.0f * c.z * nz;
-                            float const co = 15.0f * S - 3.0f * T;
-                            g0 += m4 * (co * nx - 3.0f * vx);
-                            g1 += m4 * (co * ny - 3.0f * vy);
-                            g2 += m4 * (co * nz - 3.0f * vz);
-                        }
-                        if constexpr (Order >= 2) {
-                            float4 const e = __ldg(nd + s * Q + 4);
-                            float4 const f = __ldg(nd + s * Q + 5);
-                            // d.z = Nxxx, d.w = Nyyy, e = (Nzzz, spn, Axy, Axz), f = (Ayz, Ayx, Azx, Azy)
-                            float const xxx = d.z, yyy = d.w, zzz = e.x, spn = e.y;
-                            float const Axy = e.z, Axz = e.w, Ayz = f.x, Ayx = f.y, Azx = f.z, Azy = f.w;
-                            float const m4 = m2 * m2;
-                            float const nx2 = nx * nx, ny2 = ny * ny, nz2 = nz * nz;
-                            float const nx3 = nx2 * nx, ny3 = ny2 * ny, nz3 = nz2 * nz;
-                            float const t0x = Ayx + Azx, t0y = Azy + Axy, t0z = Axz + Ayz;
-                            float const t1x = ny * Axy + nz * Axz;
-                            float const t1y = nz * Ayz + nx * Ayx;
-                            float const t1z = nx * Azx + ny * Azy;
-                            w += m4 * (1.5f * (nx * (3.0f * xxx + t0x) + ny * (3.0f * yyy + t0y) +
-                                               nz * (3.0f * zzz + t0z)) -
-                                       7.5f * (nx3 * xxx + ny3 * yyy + nz3 * zzz + nx * ny * nz * spn +
-                                               nx2 * t1x + ny2 * t1y + nz2 * t1z));
-                            if constexpr (Grad) {
-                                float const m5 = m4 * m1;
-                                float const Px = 3.0f * xxx + Ayx + Azx;
-                                float const Py = 3.0f * yyy + Azy + Axy;
-                                float const Pz = 3.0f * zzz + Axz + Ayz;
-                                float const L2 = nx * Px + ny * Py + nz * Pz;
-                                float const C2 = nx3 * xxx + ny3 * yyy + nz3 * zzz + nx * ny * nz * spn +
-                                                 nx2 * (ny * Axy + nz * Axz) + ny2 * (nz * Ayz + nx * Ayx) +
-                                                 nz2 * (nx * Azx + ny * Azy);
-                                float const Rx = 3.0f * xxx * nx2 + 2.0f * Axy * nx * ny + 2.0f * Axz * nx * nz +
-                                                 Ayx * ny2 + Azx * nz2 + spn * ny * nz;
-                                float const Ry = 3.0f * yyy * ny2 + 2.0f * Ayx * nx * ny + 2.0f * Ayz * ny * nz +
-                                                 Axy * nx2 + Azy * nz2 + spn * nx * nz;
-                                float const Rz = 3.0f * zzz * nz2 + 2.0f * Azx * nx * nz + 2.0f * Azy * ny * nz +
-                                                 Axz * nx2 + Ayz * ny2 + spn * nx * ny;
-                                float const h = 52.5f * C2;
-                                g0 += m5 * (1.5f * Px - 7.5f * (nx * L2 + Rx) + nx * h);
-                                g1 += m5 * (1.5f * Py - 7.5f * (ny * L2 + Ry) + ny * h);
-                                g2 += m5 * (1.5f * Pz - 7.5f * (nz * L2 + Rz) + nz * h);
-                            }
-                        }
-                    }
+                    float const w = far_field<Order, Grad>(rx, ry, rz, q2, b, nd + s * Q + 2, g0, g1, g2);
                     if (isfinite(w)) {
                         omega += w;
                         if constexpr (Grad) {
@@ -542,6 +479,262 @@ __global__ void __launch_bounds__(256) k_taylor(taylor_params p) {
     }
 }
 
+// Far-field Taylor terms of one accepted child (smallgwn gwn_query_winding_impl.cuh:193-327).
+// a = (P, r2), b = (N, ref); c.. = packed order-1/2 coefficients at nd[1..].
+template <int Order, bool Grad>
+__device__ __forceinline__ float far_field(float rx, float ry, float rz, float q2, float4 const &b,
+                                           float4 const *__restrict__ cd, float &g0, float &g1, float &g2) {
+    float const m1 = rsqrtf(q2);
+    float const m2 = m1 * m1;
+    float const m3 = m2 * m1;
+    float const nx = rx * m1, ny = ry * m1, nz = rz * m1;
+    float const rdn = nx * b.x + ny * b.y + nz * b.z;
+    float w = -m2 * rdn;
+    if constexpr (Grad) {
+        g0 = m3 * (3.0f * nx * rdn - b.x);
+        g1 = m3 * (3.0f * ny * rdn - b.y);
+        g2 = m3 * (3.0f * nz * rdn - b.z);
+    }
+    if constexpr (Order >= 1) {
+        float4 const c = __ldg(cd);
+        float4 const d = __ldg(cd + 1);
+        float const T = c.x + c.y + c.z;
+        float const S = nx * nx * c.x + ny * ny * c.y + nz * nz * c.z + nx * ny * c.w + nx * nz * d.y + ny * nz * d.x;
+        w += m3 * (T - 3.0f * S);
+        if constexpr (Grad) {
+            float const m4 = m2 * m2;
+            float const vx = 2.0f * c.x * nx + c.w * ny + d.y * nz;
+            float const vy = c.w * nx + 2.0f * c.y * ny + d.x * nz;
+            float const vz = d.y * nx + d.x * ny + 2.0f * c.z * nz;
+            float const co = 15.0f * S - 3.0f * T;
+            g0 += m4 * (co * nx - 3.0f * vx);
+            g1 += m4 * (co * ny - 3.0f * vy);
+            g2 += m4 * (co * nz - 3.0f * vz);
+        }
+        if constexpr (Order >= 2) {
+            float4 const e = __ldg(cd + 2);
+            float4 const f = __ldg(cd + 3);
+            float const xxx = d.z, yyy = d.w, zzz = e.x, spn = e.y;
+            float const Axy = e.z, Axz = e.w, Ayz = f.x, Ayx = f.y, Azx = f.z, Azy = f.w;
+            float const m4 = m2 * m2;
+            float const nx2 = nx * nx, ny2 = ny * ny, nz2 = nz * nz;
+            float const nx3 = nx2 * nx, ny3 = ny2 * ny, nz3 = nz2 * nz;
+            float const t0x = Ayx + Azx, t0y = Azy + Axy, t0z = Axz + Ayz;
+            float const t1x = ny * Axy + nz * Axz;
+            float const t1y = nz * Ayz + nx * Ayx;
+            float const t1z = nx * Azx + ny * Azy;
+            w += m4 * (1.5f * (nx * (3.0f * xxx + t0x) + ny * (3.0f * yyy + t0y) + nz * (3.0f * zzz + t0z)) -
+                       7.5f * (nx3 * xxx + ny3 * yyy + nz3 * zzz + nx * ny * nz * spn + nx2 * t1x + ny2 * t1y +
+                               nz2 * t1z));
+            if constexpr (Grad) {
+                float const m5 = m4 * m1;
+                float const Px = 3.0f * xxx + Ayx + Azx;
+                float const Py = 3.0f * yyy + Azy + Axy;
+                float const Pz = 3.0f * zzz + Axz + Ayz;
+                float const L2 = nx * Px + ny * Py + nz * Pz;
+                float const C2 = nx3 * xxx + ny3 * yyy + nz3 * zzz + nx * ny * nz * spn + nx2 * (ny * Axy + nz * Axz) +
+                                 ny2 * (nz * Ayz + nx * Ayx) + nz2 * (nx * Azx + ny * Azy);
+                float const Rx = 3.0f * xxx * nx2 + 2.0f * Axy * nx * ny + 2.0f * Axz * nx * nz + Ayx * ny2 + Azx * nz2 +
+                                 spn * ny * nz;
+                float const Ry = 3.0f * yyy * ny2 + 2.0f * Ayx * nx * ny + 2.0f * Ayz * ny * nz + Axy * nx2 + Azy * nz2 +
+                                 spn * nx * nz;
+                float const Rz = 3.0f * zzz * nz2 + 2.0f * Azx * nx * nz + 2.0f * Azy * ny * nz + Axz * nx2 + Ayz * ny2 +
+                                 spn * nx * ny;
+                float const h = 52.5f * C2;
+                g0 += m5 * (1.5f * Px - 7.5f * (nx * L2 + Rx) + nx * h);
+                g1 += m5 * (1.5f * Py - 7.5f * (ny * L2 + Ry) + ny * h);
+                g2 += m5 * (1.5f * Pz - 7.5f * (nz * L2 + Rz) + nz * h);
+            }
+        }
+    }
+    return w;
+}
+
+// Warp-cooperative traversal: the 32 lanes of a warp (32 Morton-adjacent queries) walk one
+// depth-first traversal together. Every stack entry carries the mask of lanes that still need the
+// subtree; a lane leaves a subtree as soon as it accepts the child's far field. Node records are
+// loaded with warp-uniform addresses and the stack lives in the lanes' registers (lane k holds
+// entries k and k + 32), so control flow stays uniform. For every lane the nodes it needs are
+// visited in the same order as in an independent depth-first traversal (children in decreasing
+// slot order, contributions added in slot order), so the per-lane sums equal those of k_taylor.
+template <int Order, int Cap, int Mode, bool Grad, bool Stats>
+__global__ void __launch_bounds__(256) k_taylor_warp(taylor_params p) {
+    static_assert(Cap <= 64, "warp stack holds at most 64 entries");
+    constexpr int Q = qnode_traits<Order>::k_f4_per_child;
+    unsigned const lane = threadIdx.x & 31u;
+    std::uint64_t const idx = static_cast<std::uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    bool const valid = idx < p.n;
+    unsigned const full = __ballot_sync(0xffffffffu, valid);
+    if (full == 0u)
+        return;
+    std::uint32_t const qi = valid ? (p.order != nullptr ? p.order[idx] : static_cast<std::uint32_t>(idx)) : 0u;
+    float const qx = valid ? p.qx[qi] : 0.0f;
+    float const qy = valid ? p.qy[qi] : 0.0f;
+    float const qz = valid ? p.qz[qi] : 0.0f;
+    float omega = 0.0f;
+    float gx = 0.0f, gy = 0.0f, gz = 0.0f;
+    std::uint32_t st_nodes = 0, st_far = 0, st_near = 0;
+
+    auto leaf = [&](std::uint32_t first, std::uint32_t cnt) {
+        for (std::uint32_t k = 0; k < cnt; ++k) {
+            std::uint64_t const t = static_cast<std::uint64_t>(first) + k;
+            if (t >= p.primitive_count)
+                break;
+            float4 const A = __ldg(&p.tri48[t].a);
+            float4 const B = __ldg(&p.tri48[t].b);
+            float4 const C = __ldg(&p.tri48[t].c);
+            float const ax = A.x - qx, ay = A.y - qy, az = A.z - qz;
+            if constexpr (Mode == GWNB_NEAR_COMPENSATED)
+                omega += solid_angle_comp(ax, ay, az, A.w, B.x, B.y, B.z, B.w, C.x, p.fp64_threshold, p.fp64_count);
+            else
+                omega += solid_angle_plain(ax, ay, az, A.w, B.x, B.y, B.z, B.w, C.x, C.y, C.z, C.w);
+            if constexpr (Grad) {
+                float3 const g = solid_angle_grad(ax, ay, az, A.w, B.x, B.y, B.z, B.w, C.x);
+                gx += g.x;
+                gy += g.y;
+                gz += g.z;
+            }
+            if constexpr (Stats)
+                ++st_near;
+        }
+    };
+
+    bool overflow = false;
+    if (ref_leaf(p.root_ref)) {
+        if (valid)
+            leaf(static_cast<std::uint32_t>(ref_offset(p.root_ref)), ref_count(p.root_ref));
+    } else {
+        std::uint32_t node = static_cast<std::uint32_t>(ref_offset(p.root_ref));
+        unsigned mask = full;
+        // distributed stack: entry e lives in lane e & 31, bank e >> 5
+        std::uint32_t st_node0 = 0, st_node1 = 0;
+        unsigned st_mask0 = 0, st_mask1 = 0;
+        int sp = 0;
+        for (;;) {
+            if (node >= p.node_count)
+                break;
+            bool const active = ((mask >> lane) & 1u) != 0u;
+            if constexpr (Stats)
+                st_nodes += active ? 1u : 0u;
+            float4 const *nd = p.qnodes + static_cast<std::uint64_t>(node) * (4 * Q);
+            std::uint32_t next = k_invalid_u32;
+            unsigned next_mask = 0u;
+#pragma unroll
+            for (int s = 0; s < 4; ++s) {
+                float4 const a = __ldg(nd + s * Q);
+                if (a.w < 0.0f)
+                    continue;
+                float4 const b = __ldg(nd + s * Q + 1);
+                bool desc = false;
+                if (active) {
+                    float const rx = qx - a.x, ry = qy - a.y, rz = qz - a.z;
+                    float const q2 = rx * rx + ry * ry + rz * rz;
+                    desc = !(q2 > 0.0f);
+                    if (!desc)
+                        desc = q2 <= a.w * p.beta2;
+                    if (!desc) {
+                        float g0 = 0.0f, g1 = 0.0f, g2 = 0.0f;
+                        float const w = far_field<Order, Grad>(rx, ry, rz, q2, b, nd + s * Q + 2, g0, g1, g2);
+                        if (isfinite(w)) {
+                            omega += w;
+                            if constexpr (Grad) {
+                                gx += g0;
+                                gy += g1;
+                                gz += g2;
+                            }
+                            if constexpr (Stats)
+                                ++st_far;
+                        } else {
+                            desc = true;
+                        }
+                    }
+                }
+                unsigned const dmask = __ballot_sync(0xffffffffu, desc);
+                if (dmask == 0u)
+                    continue;
+                std::uint32_t const ref = __float_as_uint(b.w);
+                if ((ref & k_qref_leaf) == 0u) {
+                    if (next != k_invalid_u32) {
+                        if (sp >= Cap) {
+                            overflow = true;
+                            break;
+                        }
+                        if (static_cast<unsigned>(sp & 31) == lane) {
+                            if (sp < 32) {
+                                st_node0 = next;
+                                st_mask0 = next_mask;
+                            } else {
+                                st_node1 = next;
+                                st_mask1 = next_mask;
+                            }
+                        }
+                        ++sp;
+                    }
+                    next = ref;
+                    next_mask = dmask;
+                } else if (desc) {
+                    std::uint32_t const cnt =
+                        (ref & k_qref_multi) ? p.qcounts[static_cast<std::uint64_t>(node) * 4 + s] : 1u;
+                    leaf(ref & k_qref_index_mask, cnt);
+                }
+            }
+            if (overflow)
+                break;
+            if (next != k_invalid_u32) {
+                node = next;
+                mask = next_mask;
+                continue;
+            }
+            if (sp == 0)
+                break;
+            --sp;
+            int const src = sp & 31;
+            if (sp < 32) {
+                node = __shfl_sync(0xffffffffu, st_node0, src);
+                mask = __shfl_sync(0xffffffffu, st_mask0, src);
+            } else {
+                node = __shfl_sync(0xffffffffu, st_node1, src);
+                mask = __shfl_sync(0xffffffffu, st_mask1, src);
+            }
+        }
+    }
+    if (!valid)
+        return;
+    float const inv4pi = 1.0f / (4.0f * k_pi_f);
+    if (overflow) {
+        atomicOr(p.status, k_err_stack_overflow);
+        float const nan = __int_as_float(0x7fc00000);
+        if (p.out != nullptr)
+            p.out[qi] = nan;
+        if constexpr (Grad) {
+            p.grad_x[qi] = nan;
+            p.grad_y[qi] = nan;
+            p.grad_z[qi] = nan;
+        }
+        return;
+    }
+    if (p.out != nullptr)
+        p.out[qi] = omega / (4.0f * k_pi_f);
+    if constexpr (Grad) {
+        p.grad_x[qi] = gx * inv4pi;
+        p.grad_y[qi] = gy * inv4pi;
+        p.grad_z[qi] = gz * inv4pi;
+    }
+    if constexpr (Stats) {
+        p.stat_nodes[qi] = st_nodes;
+        p.stat_far[qi] = st_far;
+        p.stat_near[qi] = st_near;
+    }
+}
+
+template <int Order, int Cap, int Mode, bool Grad, bool Stats>
+int launch_taylor_warp(taylor_params const &p, int block, cudaStream_t s) {
+    unsigned const grid = static_cast<unsigned>((p.n + block - 1) / block);
+    k_taylor_warp<Order, Cap, Mode, Grad, Stats><<<grid, block, 0, s>>>(p);
+    GWNB_CUDA_TRY(cudaGetLastError());
+    return GWNB_OK;
+}
+
 template <int Order, int Cap, int Mode, bool Grad, bool Stats>
 int launch_taylor_cap(taylor_params const &p, int block, cudaStream_t s) {
     std::size_t const smem = static_cast<std::size_t>(Cap) * block * sizeof(std::uint32_t);
@@ -556,7 +749,11 @@ int launch_taylor_cap(taylor_params const &p, int block, cudaStream_t s) {
 }
 
 template <int Order, int Mode, bool Grad, bool Stats>
-int launch_taylor_mode(taylor_params const &p, int block, int cap, cudaStream_t s) {
+int launch_taylor_mode(taylor_params const &p, int block, int cap, bool per_thread, cudaStream_t s) {
+    if (!per_thread && cap <= 32)
+        return launch_taylor_warp<Order, 32, Mode, Grad, Stats>(p, block, s);
+    if (!per_thread && cap <= 64)
+        return launch_taylor_warp<Order, 64, Mode, Grad, Stats>(p, block, s);
     if (cap <= 16)
         return launch_taylor_cap<Order, 16, Mode, Grad, Stats>(p, block, s);
     if (cap <= 32)
@@ -567,10 +764,10 @@ int launch_taylor_mode(taylor_params const &p, int block, int cap, cudaStream_t 
 }
 
 template <int Order, bool Grad, bool Stats>
-int launch_taylor_order(taylor_params const &p, int block, int cap, int mode, cudaStream_t s) {
+int launch_taylor_order(taylor_params const &p, int block, int cap, int mode, bool per_thread, cudaStream_t s) {
     if (mode == GWNB_NEAR_COMPENSATED)
-        return launch_taylor_mode<Order, GWNB_NEAR_COMPENSATED, Grad, Stats>(p, block, cap, s);
-    return launch_taylor_mode<Order, GWNB_NEAR_PLAIN, Grad, Stats>(p, block, cap, s);
+        return launch_taylor_mode<Order, GWNB_NEAR_COMPENSATED, Grad, Stats>(p, block, cap, per_thread, s);
+    return launch_taylor_mode<Order, GWNB_NEAR_PLAIN, Grad, Stats>(p, block, cap, per_thread, s);
 }
 
 } // namespace
@@ -609,28 +806,7 @@ int query_order(aabb const *root_bounds, float const *qx, float const *qy, float
     return rc;
 }
 
-struct taylor_request {
-    int order;
-    float4 const *qnodes;
-    std::uint32_t const *qcounts;
-    triangle48 const *tri48;
-    std::uint64_t primitive_count;
-    std::uint64_t node_count;
-    std::uint64_t root_ref;
-    aabb const *root_bounds; // device
-    float const *qx, *qy, *qz;
-    float *out, *gx, *gy, *gz;
-    std::uint32_t *stat_nodes, *stat_far, *stat_near;
-    std::uint64_t n;
-    float accuracy_scale;
-    int block;
-    int stack_capacity; // must already be >= the BVH's internal stack bound
-    int sort_queries;
-    int near_mode;
-    float fp64_threshold;
-    unsigned long long *fp64_count;
-    unsigned int *status;
-};
+
 
 int taylor_batch(taylor_request const &r, cudaStream_t s) {
     if (r.n == 0)
@@ -673,13 +849,14 @@ int taylor_batch(taylor_request const &r, cudaStream_t s) {
     int rc = GWNB_OK;
     int const block = r.block > 0 ? r.block : 256;
     int const cap = r.stack_capacity;
+    bool const per_thread = r.per_thread != 0;
 #define GWNB_DISPATCH(O)                                                                           \
     if (grad)                                                                                      \
-        rc = launch_taylor_order<O, true, false>(p, block, cap, r.near_mode, s);                   \
+        rc = launch_taylor_order<O, true, false>(p, block, cap, r.near_mode, per_thread, s);       \
     else if (stats)                                                                                \
-        rc = launch_taylor_order<O, false, true>(p, block, cap, r.near_mode, s);                   \
+        rc = launch_taylor_order<O, false, true>(p, block, cap, r.near_mode, per_thread, s);       \
     else                                                                                           \
-        rc = launch_taylor_order<O, false, false>(p, block, cap, r.near_mode, s);
+        rc = launch_taylor_order<O, false, false>(p, block, cap, r.near_mode, per_thread, s);
     if (r.order == 0) {
         GWNB_DISPATCH(0)
     } else if (r.order == 1) {
