@@ -2,8 +2,9 @@
 
 Workload (per rank): displaced UV sphere 1024 x 512 (1,046,528 triangles, seed 2), 10M mixed
 queries (half uniform in the 1.2x bounding box, half at surface samples offset along the normal by
-N(0, 1e-3), seed 2 + rank), H-PLOC (radius 8) BVH4, Taylor order 2 at accuracy scale 2, compensated
-near field. A step is one call of the Taylor batch on the 10M device-resident queries.
+N(0, 1e-3), seed 2 + rank), H-PLOC (radius 8) BVH4, Taylor order 2 at accuracy scale 3.5,
+compensated near field. A step is one call of the Taylor batch on the 10M device-resident queries
+(Morton ordering of the queries included).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -50,15 +51,16 @@ def parse() -> argparse.Namespace:
     ap.add_argument("--order", type=int, default=ORDER)
     ap.add_argument("--beta", type=float, default=BETA)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--profile", choices=["taylor", "taylor-thread", "build", "exact"], default=None,
+    ap.add_argument("--profile", choices=["taylor", "taylor-plain", "taylor-thread", "build", "exact"], default=None,
                     help="run one small workload for a profiler (no JSON): 2 launches of the kernel")
     return ap.parse_args()
 
 
 def run_profile(args) -> None:
-    """Small, self-contained launches for ncu: the traversal kernel over pre-ordered queries
-    (`taylor`, `taylor-thread`), one H-PLOC build (`build`) or the exact batch on the small
-    icosphere (`exact`). Uses --queries (default here 1M) and --order / --beta."""
+    """Self-contained launches for ncu: the traversal kernel over pre-ordered queries (`taylor`:
+    the timed form, warp-cooperative with the compensated near field; `taylor-plain`: FP32 near
+    field; `taylor-thread`: one traversal per thread, FP32 near field), one H-PLOC build (`build`)
+    or the exact batch on the small icosphere (`exact`). Uses --queries and --order / --beta."""
     import torch
 
     import smallgwn_b200 as g
@@ -95,9 +97,10 @@ def run_profile(args) -> None:
     order = torch.empty(dq[0].numel(), dtype=torch.int32, device="cuda")
     assert api.query_order(bvh, *dq, order).is_ok()
     sq = [d[order.long()].contiguous() for d in dq]
+    precision = g.near_precision.compensated if args.profile == "taylor" else g.near_precision.plain
     for _ in range(2):
         assert g.gwn_compute_winding_number_taylor_batch(args.order, bvh, mom, *sq, out, accuracy_scale=args.beta,
-                                                         stream=stream, sort_queries=False,
+                                                         stream=stream, sort_queries=False, precision=precision,
                                                          per_thread=args.profile == "taylor-thread").is_ok()
     torch.cuda.synchronize()
     print(f"profile {args.profile} ok")
@@ -440,7 +443,8 @@ def main() -> None:
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
                          "frac": achieved / pk["hbm_gbs"], "peak_source": pk["source"],
                          "traffic": traffic,
-                         "kernel": "k_taylor (traversal, pre-ordered queries)", "kernel_ms": kernel_ms,
+                         "kernel": "k_taylor_warp (traversal, compensated, pre-ordered queries)",
+                         "kernel_ms": kernel_ms,
                          "algorithmic_bytes": alg_bytes,
                          "bytes_model": "16 B/query + (128 B node + moment node) per node entered + 36 B per exact triangle"},
             "cpu_baseline": cpu,

@@ -73,6 +73,11 @@ class near_precision(enum.IntEnum):
     compensated = _lib.GWNB_NEAR_COMPENSATED
 
 
+# Compensated near field: (query, triangle) pairs whose numerator and denominator are both below
+# this fraction of |a||b||c| are evaluated in FP64 (about 0.03 pairs per near-surface query).
+FP64_THRESHOLD = 1.0 / 16.0
+
+
 def _stream(stream) -> int | None:
     if stream is None:
         return None  # cudaStreamLegacy / stream 0
@@ -323,7 +328,7 @@ def gwn_compute_winding_number_taylor_batch(order: int, bvh: gwn_bvh4_object, mo
                                             qx, qy, qz, out, accuracy_scale: float = 2.0, stream=None,
                                             config: gwn_query_batch_config = gwn_query_batch_config(),
                                             sort_queries: bool = True, precision: int = near_precision.plain,
-                                            fp64_threshold: float = 1e-3, per_thread: bool = False) -> gwn_status:
+                                            fp64_threshold: float = FP64_THRESHOLD, per_thread: bool = False) -> gwn_status:
     """Taylor-approximated winding numbers of a device batch (asynchronous). ``per_thread``
     selects one independent traversal per thread instead of the warp-cooperative traversal."""
     if moment.order != order:
@@ -349,7 +354,7 @@ def gwn_compute_winding_gradient_taylor_batch(order: int, bvh: gwn_bvh4_object, 
         bad = _check_spans(qx, qy, qz, g)
         if bad is not None:
             return bad
-    opt = _options(config, sort_queries, near_precision.plain, 1e-3)
+    opt = _options(config, sort_queries, near_precision.plain, FP64_THRESHOLD)
     rc = _lib.load().gwnb_winding_gradient_taylor_batch_f32(
         C.byref(bvh._view), C.byref(moment._view), _ptr(qx), _ptr(qy), _ptr(qz), _ptr(gx), _ptr(gy), _ptr(gz),
         _numel(qx), float(accuracy_scale), C.byref(opt), _stream(stream))

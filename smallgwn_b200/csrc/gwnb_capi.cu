@@ -652,7 +652,7 @@ static int taylor_common(const gwnb_bvh4_f32 *b_in, const gwnb_moment4_f32 *m, c
                          gwnb_stream_t stream) {
     if (!bvh_valid(b_in))
         return set_error(GWNB_INVALID_ARGUMENT, "BVH object contains no queryable data.");
-    gwnb_taylor_options o{256, 64, 1, GWNB_NEAR_PLAIN, 1e-3f};
+    gwnb_taylor_options o{256, 64, 1, GWNB_NEAR_PLAIN, 1.0f / 16.0f};
     if (opt != nullptr) {
         o = *opt;
         if (o.block_size == 0)
@@ -742,7 +742,7 @@ int gwnb_winding_taylor_stats_f32(const gwnb_bvh4_f32 *b, const gwnb_moment4_f32
                                   uint32_t *far_evals, uint32_t *near_tris, gwnb_stream_t stream) {
     if (n > 0 && (nodes == nullptr || far_evals == nullptr || near_tris == nullptr))
         return set_error(GWNB_INVALID_ARGUMENT, "Statistics outputs must be non-null.");
-    gwnb_taylor_options o{256, 0, 1, GWNB_NEAR_PLAIN, 1e-3f};
+    gwnb_taylor_options o{256, 0, 1, GWNB_NEAR_PLAIN, 1.0f / 16.0f};
     return taylor_common(b, m, qx, qy, qz, nullptr, nullptr, nullptr, nullptr, nodes, far_evals, near_tris, n, beta,
                          &o, stream);
 }

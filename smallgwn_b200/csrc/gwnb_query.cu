@@ -5,7 +5,8 @@
 // the tile with broadcast shared loads. The solid angle is the Van Oosterom-Strackee formula in
 // unnormalised form, tan(Omega/2) = a.(e1 x e2) / (|a||b||c| + (a.b)|c| + (a.c)|b| + (b.c)|a|),
 // which equals smallgwn's unit-vector form (detail/gwn_query_geometry_impl.cuh:16-45) and keeps
-// its conventions: zero when the query sits on a vertex or the numerator vanishes.
+// its conventions: zero when the query sits on a vertex or the numerator vanishes. Pairs where
+// both terms cancel (query by an edge's line) are re-evaluated in FP64 (solid_angle_guarded).
 //
 // Taylor batch (replaces gwn_compute_winding_number_taylor_batch, gwn_query.cuh:384-445): the
 // traversal order, acceptance test and far-field terms follow detail/gwn_query_winding_impl.cuh
@@ -14,146 +15,32 @@
 // leaf triangles exactly). Differences: the batch is Morton-ordered internally for coherence, node
 // data comes from a per-node query sidecar with 128-bit loads, the stack lives in shared memory,
 // and stack overflow writes NaN and raises a device error bit instead of trapping.
-#include "gwnb_internal.cuh"
+#include "gwnb_field.cuh"
 
 #include <algorithm>
 
 namespace gwnb {
 namespace {
 
-constexpr float k_pi_f = 3.14159265358979323846f;
+using namespace field;
 
-// ---- exact solid angle ---------------------------------------------------------------------------
-
-// a = v0 - q, e1, e2 edges, n = e1 x e2.
-__device__ __forceinline__ float solid_angle_plain(float ax, float ay, float az, float e1x, float e1y,
-                                                   float e1z, float e2x, float e2y, float e2z,
-                                                   float nx, float ny, float nz) {
-    float const bx = ax + e1x, by = ay + e1y, bz = az + e1z;
-    float const cx = ax + e2x, cy = ay + e2y, cz = az + e2z;
-    float const a2 = ax * ax + ay * ay + az * az;
-    float const b2 = bx * bx + by * by + bz * bz;
-    float const c2 = cx * cx + cy * cy + cz * cz;
-    float const la = sqrtf(a2), lb = sqrtf(b2), lc = sqrtf(c2);
-    if (la == 0.0f || lb == 0.0f || lc == 0.0f)
-        return 0.0f;
-    float const num = ax * nx + ay * ny + az * nz;
-    if (num == 0.0f)
-        return 0.0f;
-    float const ab = ax * bx + ay * by + az * bz;
-    float const ac = ax * cx + ay * cy + az * cz;
-    float const bc = bx * cx + by * cy + bz * cz;
-    float const den = la * lb * lc + ab * lc + ac * lb + bc * la;
-    return 2.0f * atan2f(num, den);
-}
-
-// Error-free transformations (Dekker / Ogita-Rump-Oishi "Accurate sum and dot product", 2005).
-__device__ __forceinline__ void two_prod(float a, float b, float &p, float &e) {
-    p = a * b;
-    e = fmaf(a, b, -p);
-}
-__device__ __forceinline__ void two_sum(float a, float b, float &s, float &e) {
-    s = a + b;
-    float const z = s - a;
-    e = (a - (s - z)) + (b - z);
-}
-// Compensated dot product of length 3 (Dot2).
-__device__ __forceinline__ float dot3_comp(float a0, float a1, float a2, float b0, float b1, float b2) {
-    float p, s, h, r, q;
-    two_prod(a0, b0, p, s);
-    two_prod(a1, b1, h, r);
-    two_sum(p, h, p, q);
-    s += q + r;
-    two_prod(a2, b2, h, r);
-    two_sum(p, h, p, q);
-    s += q + r;
-    return p + s;
-}
-
-// Compensated near field: numerator a.(e1 x e2) with compensated cross and dot products, the
-// denominator from compensated dots; triangles whose denominator and numerator are both small
-// relative to |a||b||c| (query close to an edge or vertex line) take an FP64 evaluation.
-__device__ __forceinline__ float solid_angle_comp(float ax, float ay, float az, float e1x, float e1y,
-                                                  float e1z, float e2x, float e2y, float e2z,
-                                                  float threshold, unsigned long long *fp64_count) {
-    float const bx = ax + e1x, by = ay + e1y, bz = az + e1z;
-    float const cx = ax + e2x, cy = ay + e2y, cz = az + e2z;
-    float const a2 = dot3_comp(ax, ay, az, ax, ay, az);
-    float const b2 = dot3_comp(bx, by, bz, bx, by, bz);
-    float const c2 = dot3_comp(cx, cy, cz, cx, cy, cz);
-    float const la = sqrtf(a2), lb = sqrtf(b2), lc = sqrtf(c2);
-    if (la == 0.0f || lb == 0.0f || lc == 0.0f)
-        return 0.0f;
-    // n = e1 x e2, each component a compensated 2-term difference of products
-    float const nx = dot3_comp(e1y, -e1z, 0.0f, e2z, e2y, 0.0f);
-    float const ny = dot3_comp(e1z, -e1x, 0.0f, e2x, e2z, 0.0f);
-    float const nz = dot3_comp(e1x, -e1y, 0.0f, e2y, e2x, 0.0f);
-    float const num = dot3_comp(ax, ay, az, nx, ny, nz);
-    float const ab = dot3_comp(ax, ay, az, bx, by, bz);
-    float const ac = dot3_comp(ax, ay, az, cx, cy, cz);
-    float const bc = dot3_comp(bx, by, bz, cx, cy, cz);
-    float const labc = la * lb * lc;
-    float const den = labc + dot3_comp(ab, ac, bc, lc, lb, la);
-    float const scale = labc;
-    if (fabsf(den) < threshold * scale && fabsf(num) < threshold * scale) {
-        if (fp64_count != nullptr)
-            atomicAdd(fp64_count, 1ull);
-        double const dax = ax, day = ay, daz = az;
-        double const dbx = dax + e1x, dby = day + e1y, dbz = daz + e1z;
-        double const dcx = dax + e2x, dcy = day + e2y, dcz = daz + e2z;
-        double const dla = sqrt(dax * dax + day * day + daz * daz);
-        double const dlb = sqrt(dbx * dbx + dby * dby + dbz * dbz);
-        double const dlc = sqrt(dcx * dcx + dcy * dcy + dcz * dcz);
-        double const dnx = static_cast<double>(e1y) * e2z - static_cast<double>(e1z) * e2y;
-        double const dny = static_cast<double>(e1z) * e2x - static_cast<double>(e1x) * e2z;
-        double const dnz = static_cast<double>(e1x) * e2y - static_cast<double>(e1y) * e2x;
-        double const dnum = dax * dnx + day * dny + daz * dnz;
-        if (dnum == 0.0)
-            return 0.0f;
-        double const dden = dla * dlb * dlc + (dax * dbx + day * dby + daz * dbz) * dlc +
-                            (dax * dcx + day * dcy + daz * dcz) * dlb +
-                            (dbx * dcx + dby * dcy + dbz * dcz) * dla;
-        return static_cast<float>(2.0 * atan2(dnum, dden));
+// Running sums of many terms of mixed size (up to a million solid angles per query in the exact
+// batch): with Compensated, Neumaier's variant of Kahan summation (Neumaier 1974) carries the
+// rounding error of every addition, so terms below half an ulp of the running sum are not lost.
+template <bool Compensated> struct accum {
+    float s = 0.0f;
+    __device__ __forceinline__ void add(float x) { s += x; }
+    __device__ __forceinline__ float value() const { return s; }
+};
+template <> struct accum<true> {
+    float s = 0.0f, c = 0.0f;
+    __device__ __forceinline__ void add(float x) {
+        float const t = s + x;
+        c += (fabsf(s) >= fabsf(x)) ? ((s - t) + x) : ((x - t) + s);
+        s = t;
     }
-    if (num == 0.0f)
-        return 0.0f;
-    return 2.0f * atan2f(num, den);
-}
-
-// Gradient of the solid angle w.r.t. the query (Biot-Savart form), as smallgwn's
-// gwn_gradient_solid_angle_triangle_impl (detail/gwn_query_winding_impl.cuh:21-60).
-__device__ __forceinline__ float3 solid_angle_grad(float ax, float ay, float az, float e1x, float e1y,
-                                                   float e1z, float e2x, float e2y, float e2z) {
-    float3 const g[3] = {make_float3(ax, ay, az), make_float3(ax + e1x, ay + e1y, az + e1z),
-                         make_float3(ax + e2x, ay + e2y, az + e2z)};
-    float l[3];
-#pragma unroll
-    for (int i = 0; i < 3; ++i)
-        l[i] = sqrtf(g[i].x * g[i].x + g[i].y * g[i].y + g[i].z * g[i].z);
-    if (l[0] == 0.0f || l[1] == 0.0f || l[2] == 0.0f)
-        return make_float3(0.0f, 0.0f, 0.0f);
-    float3 h[3];
-#pragma unroll
-    for (int i = 0; i < 3; ++i)
-        h[i] = make_float3(g[i].x / l[i], g[i].y / l[i], g[i].z / l[i]);
-    float3 r = make_float3(0.0f, 0.0f, 0.0f);
-#pragma unroll
-    for (int e = 0; e < 3; ++e) {
-        int const i = e, j = (e + 1) % 3;
-        float3 const cr = make_float3(g[i].y * g[j].z - g[i].z * g[j].y, g[i].z * g[j].x - g[i].x * g[j].z,
-                                      g[i].x * g[j].y - g[i].y * g[j].x);
-        float const cs = cr.x * cr.x + cr.y * cr.y + cr.z * cr.z;
-        if (cs == 0.0f)
-            continue;
-        float const sc = ((g[i].x - g[j].x) * (h[i].x - h[j].x) + (g[i].y - g[j].y) * (h[i].y - h[j].y) +
-                          (g[i].z - g[j].z) * (h[i].z - h[j].z)) /
-                         cs;
-        r.x += sc * cr.x;
-        r.y += sc * cr.y;
-        r.z += sc * cr.z;
-    }
-    return r;
-}
+    __device__ __forceinline__ float value() const { return s + c; }
+};
 
 // ---- exact batch --------------------------------------------------------------------------------
 
@@ -167,7 +54,8 @@ __global__ void __launch_bounds__(k_exact_block)
             std::uint64_t nq) {
     __shared__ float4 s_tri[k_exact_tile][3];
     std::uint64_t const base = static_cast<std::uint64_t>(blockIdx.x) * (k_exact_block * k_exact_q);
-    float px[k_exact_q], py[k_exact_q], pz[k_exact_q], acc[k_exact_q];
+    float px[k_exact_q], py[k_exact_q], pz[k_exact_q];
+    accum<true> acc[k_exact_q];
 #pragma unroll
     for (int k = 0; k < k_exact_q; ++k) {
         std::uint64_t const i = base + threadIdx.x + static_cast<std::uint64_t>(k) * k_exact_block;
@@ -175,7 +63,6 @@ __global__ void __launch_bounds__(k_exact_block)
         px[k] = v ? qx[i] : 0.0f;
         py[k] = v ? qy[i] : 0.0f;
         pz[k] = v ? qz[i] : 0.0f;
-        acc[k] = 0.0f;
     }
     for (std::uint64_t t0 = 0; t0 < nt; t0 += k_exact_tile) {
         __syncthreads();
@@ -206,15 +93,15 @@ __global__ void __launch_bounds__(k_exact_block)
             float4 const C = s_tri[j][2];
 #pragma unroll
             for (int k = 0; k < k_exact_q; ++k)
-                acc[k] += solid_angle_plain(A.x - px[k], A.y - py[k], A.z - pz[k], A.w, B.x, B.y, B.z,
-                                            B.w, C.x, C.y, C.z, C.w);
+                acc[k].add(solid_angle_guarded(A.x - px[k], A.y - py[k], A.z - pz[k], A.w, B.x, B.y, B.z,
+                                               B.w, C.x, C.y, C.z, C.w));
         }
     }
 #pragma unroll
     for (int k = 0; k < k_exact_q; ++k) {
         std::uint64_t const i = base + threadIdx.x + static_cast<std::uint64_t>(k) * k_exact_block;
         if (i < nq)
-            out[i] = acc[k] / (4.0f * k_pi_f);
+            out[i] = acc[k].value() / (4.0f * k_pi_f);
     }
 }
 
@@ -316,10 +203,6 @@ __global__ void __launch_bounds__(256)
 
 // ---- Taylor traversal ---------------------------------------------------------------------------
 
-template <int Order, bool Grad>
-__device__ __forceinline__ float far_field(float rx, float ry, float rz, float q2, float4 const &b,
-                                           float4 const *__restrict__ cd, float &g0, float &g1, float &g2);
-
 struct taylor_params {
     float4 const *qnodes;
     std::uint32_t const *qcounts;
@@ -354,7 +237,7 @@ __global__ void __launch_bounds__(256) k_taylor(taylor_params p) {
         return;
     std::uint32_t const qi = p.order != nullptr ? p.order[idx] : static_cast<std::uint32_t>(idx);
     float const qx = p.qx[qi], qy = p.qy[qi], qz = p.qz[qi];
-    float omega = 0.0f;
+    accum<Mode == GWNB_NEAR_COMPENSATED> omega;
     float gx = 0.0f, gy = 0.0f, gz = 0.0f;
     std::uint32_t st_nodes = 0, st_far = 0, st_near = 0;
     unsigned const stride = blockDim.x;
@@ -372,10 +255,10 @@ __global__ void __launch_bounds__(256) k_taylor(taylor_params p) {
             float4 const C = __ldg(&p.tri48[t].c);
             float const ax = A.x - qx, ay = A.y - qy, az = A.z - qz;
             if constexpr (Mode == GWNB_NEAR_COMPENSATED)
-                omega += solid_angle_comp(ax, ay, az, A.w, B.x, B.y, B.z, B.w, C.x, p.fp64_threshold,
-                                          p.fp64_count);
+                omega.add(solid_angle_comp(ax, ay, az, A.w, B.x, B.y, B.z, B.w, C.x, C.y, C.z, C.w,
+                                           p.fp64_threshold, p.fp64_count));
             else
-                omega += solid_angle_plain(ax, ay, az, A.w, B.x, B.y, B.z, B.w, C.x, C.y, C.z, C.w);
+                omega.add(solid_angle_plain(ax, ay, az, A.w, B.x, B.y, B.z, B.w, C.x, C.y, C.z, C.w));
             if constexpr (Grad) {
                 float3 const g = solid_angle_grad(ax, ay, az, A.w, B.x, B.y, B.z, B.w, C.x);
                 gx += g.x;
@@ -413,7 +296,7 @@ __global__ void __launch_bounds__(256) k_taylor(taylor_params p) {
                     float g0 = 0.0f, g1 = 0.0f, g2 = 0.0f;
                     float const w = far_field<Order, Grad>(rx, ry, rz, q2, b, nd + s * Q + 2, g0, g1, g2);
                     if (isfinite(w)) {
-                        omega += w;
+                        omega.add(w);
                         if constexpr (Grad) {
                             gx += g0;
                             gy += g1;
@@ -466,7 +349,7 @@ __global__ void __launch_bounds__(256) k_taylor(taylor_params p) {
         return;
     }
     if (p.out != nullptr)
-        p.out[qi] = omega / (4.0f * k_pi_f);
+        p.out[qi] = omega.value() / (4.0f * k_pi_f);
     if constexpr (Grad) {
         p.grad_x[qi] = gx * inv4pi;
         p.grad_y[qi] = gy * inv4pi;
@@ -479,76 +362,6 @@ __global__ void __launch_bounds__(256) k_taylor(taylor_params p) {
     }
 }
 
-// Far-field Taylor terms of one accepted child (smallgwn gwn_query_winding_impl.cuh:193-327).
-// a = (P, r2), b = (N, ref); c.. = packed order-1/2 coefficients at nd[1..].
-template <int Order, bool Grad>
-__device__ __forceinline__ float far_field(float rx, float ry, float rz, float q2, float4 const &b,
-                                           float4 const *__restrict__ cd, float &g0, float &g1, float &g2) {
-    float const m1 = rsqrtf(q2);
-    float const m2 = m1 * m1;
-    float const m3 = m2 * m1;
-    float const nx = rx * m1, ny = ry * m1, nz = rz * m1;
-    float const rdn = nx * b.x + ny * b.y + nz * b.z;
-    float w = -m2 * rdn;
-    if constexpr (Grad) {
-        g0 = m3 * (3.0f * nx * rdn - b.x);
-        g1 = m3 * (3.0f * ny * rdn - b.y);
-        g2 = m3 * (3.0f * nz * rdn - b.z);
-    }
-    if constexpr (Order >= 1) {
-        float4 const c = __ldg(cd);
-        float4 const d = __ldg(cd + 1);
-        float const T = c.x + c.y + c.z;
-        float const S = nx * nx * c.x + ny * ny * c.y + nz * nz * c.z + nx * ny * c.w + nx * nz * d.y + ny * nz * d.x;
-        w += m3 * (T - 3.0f * S);
-        if constexpr (Grad) {
-            float const m4 = m2 * m2;
-            float const vx = 2.0f * c.x * nx + c.w * ny + d.y * nz;
-            float const vy = c.w * nx + 2.0f * c.y * ny + d.x * nz;
-            float const vz = d.y * nx + d.x * ny + 2.0f * c.z * nz;
-            float const co = 15.0f * S - 3.0f * T;
-            g0 += m4 * (co * nx - 3.0f * vx);
-            g1 += m4 * (co * ny - 3.0f * vy);
-            g2 += m4 * (co * nz - 3.0f * vz);
-        }
-        if constexpr (Order >= 2) {
-            float4 const e = __ldg(cd + 2);
-            float4 const f = __ldg(cd + 3);
-            float const xxx = d.z, yyy = d.w, zzz = e.x, spn = e.y;
-            float const Axy = e.z, Axz = e.w, Ayz = f.x, Ayx = f.y, Azx = f.z, Azy = f.w;
-            float const m4 = m2 * m2;
-            float const nx2 = nx * nx, ny2 = ny * ny, nz2 = nz * nz;
-            float const nx3 = nx2 * nx, ny3 = ny2 * ny, nz3 = nz2 * nz;
-            float const t0x = Ayx + Azx, t0y = Azy + Axy, t0z = Axz + Ayz;
-            float const t1x = ny * Axy + nz * Axz;
-            float const t1y = nz * Ayz + nx * Ayx;
-            float const t1z = nx * Azx + ny * Azy;
-            w += m4 * (1.5f * (nx * (3.0f * xxx + t0x) + ny * (3.0f * yyy + t0y) + nz * (3.0f * zzz + t0z)) -
-                       7.5f * (nx3 * xxx + ny3 * yyy + nz3 * zzz + nx * ny * nz * spn + nx2 * t1x + ny2 * t1y +
-                               nz2 * t1z));
-            if constexpr (Grad) {
-                float const m5 = m4 * m1;
-                float const Px = 3.0f * xxx + Ayx + Azx;
-                float const Py = 3.0f * yyy + Azy + Axy;
-                float const Pz = 3.0f * zzz + Axz + Ayz;
-                float const L2 = nx * Px + ny * Py + nz * Pz;
-                float const C2 = nx3 * xxx + ny3 * yyy + nz3 * zzz + nx * ny * nz * spn + nx2 * (ny * Axy + nz * Axz) +
-                                 ny2 * (nz * Ayz + nx * Ayx) + nz2 * (nx * Azx + ny * Azy);
-                float const Rx = 3.0f * xxx * nx2 + 2.0f * Axy * nx * ny + 2.0f * Axz * nx * nz + Ayx * ny2 + Azx * nz2 +
-                                 spn * ny * nz;
-                float const Ry = 3.0f * yyy * ny2 + 2.0f * Ayx * nx * ny + 2.0f * Ayz * ny * nz + Axy * nx2 + Azy * nz2 +
-                                 spn * nx * nz;
-                float const Rz = 3.0f * zzz * nz2 + 2.0f * Azx * nx * nz + 2.0f * Azy * ny * nz + Axz * nx2 + Ayz * ny2 +
-                                 spn * nx * ny;
-                float const h = 52.5f * C2;
-                g0 += m5 * (1.5f * Px - 7.5f * (nx * L2 + Rx) + nx * h);
-                g1 += m5 * (1.5f * Py - 7.5f * (ny * L2 + Ry) + ny * h);
-                g2 += m5 * (1.5f * Pz - 7.5f * (nz * L2 + Rz) + nz * h);
-            }
-        }
-    }
-    return w;
-}
 
 // Warp-cooperative traversal: the 32 lanes of a warp (32 Morton-adjacent queries) walk one
 // depth-first traversal together. Every stack entry carries the mask of lanes that still need the
@@ -557,8 +370,18 @@ __device__ __forceinline__ float far_field(float rx, float ry, float rz, float q
 // entries k and k + 32), so control flow stays uniform. For every lane the nodes it needs are
 // visited in the same order as in an independent depth-first traversal (children in decreasing
 // slot order, contributions added in slot order), so the per-lane sums equal those of k_taylor.
+// Occupancy: the plain form fits 48 registers (5 resident blocks of 256); the compensated near
+// field would take ~70, so it is bounded to 4 blocks (64 registers) and the rarely taken FP64 branch
+// absorbs any spilling; the gradient and statistics forms also take 4, and the compensated gradient
+// 3 (85 registers).
+template <int Mode, bool Grad, bool Stats> struct taylor_warp_occupancy {
+    static constexpr bool comp = Mode == GWNB_NEAR_COMPENSATED;
+    static constexpr int value = (comp && Grad) ? 3 : ((comp || Grad || Stats) ? 4 : 5);
+};
+
 template <int Order, int Cap, int Mode, bool Grad, bool Stats>
-__global__ void __launch_bounds__(256) k_taylor_warp(taylor_params p) {
+__global__ void __launch_bounds__(256, (taylor_warp_occupancy<Mode, Grad, Stats>::value))
+    k_taylor_warp(taylor_params p) {
     static_assert(Cap <= 64, "warp stack holds at most 64 entries");
     constexpr int Q = qnode_traits<Order>::k_f4_per_child;
     unsigned const lane = threadIdx.x & 31u;
@@ -571,7 +394,7 @@ __global__ void __launch_bounds__(256) k_taylor_warp(taylor_params p) {
     float const qx = valid ? p.qx[qi] : 0.0f;
     float const qy = valid ? p.qy[qi] : 0.0f;
     float const qz = valid ? p.qz[qi] : 0.0f;
-    float omega = 0.0f;
+    accum<Mode == GWNB_NEAR_COMPENSATED> omega;
     float gx = 0.0f, gy = 0.0f, gz = 0.0f;
     std::uint32_t st_nodes = 0, st_far = 0, st_near = 0;
 
@@ -585,9 +408,10 @@ __global__ void __launch_bounds__(256) k_taylor_warp(taylor_params p) {
             float4 const C = __ldg(&p.tri48[t].c);
             float const ax = A.x - qx, ay = A.y - qy, az = A.z - qz;
             if constexpr (Mode == GWNB_NEAR_COMPENSATED)
-                omega += solid_angle_comp(ax, ay, az, A.w, B.x, B.y, B.z, B.w, C.x, p.fp64_threshold, p.fp64_count);
+                omega.add(solid_angle_comp(ax, ay, az, A.w, B.x, B.y, B.z, B.w, C.x, C.y, C.z, C.w,
+                                           p.fp64_threshold, p.fp64_count));
             else
-                omega += solid_angle_plain(ax, ay, az, A.w, B.x, B.y, B.z, B.w, C.x, C.y, C.z, C.w);
+                omega.add(solid_angle_plain(ax, ay, az, A.w, B.x, B.y, B.z, B.w, C.x, C.y, C.z, C.w));
             if constexpr (Grad) {
                 float3 const g = solid_angle_grad(ax, ay, az, A.w, B.x, B.y, B.z, B.w, C.x);
                 gx += g.x;
@@ -636,7 +460,7 @@ __global__ void __launch_bounds__(256) k_taylor_warp(taylor_params p) {
                         float g0 = 0.0f, g1 = 0.0f, g2 = 0.0f;
                         float const w = far_field<Order, Grad>(rx, ry, rz, q2, b, nd + s * Q + 2, g0, g1, g2);
                         if (isfinite(w)) {
-                            omega += w;
+                            omega.add(w);
                             if constexpr (Grad) {
                                 gx += g0;
                                 gy += g1;
@@ -714,7 +538,7 @@ __global__ void __launch_bounds__(256) k_taylor_warp(taylor_params p) {
         return;
     }
     if (p.out != nullptr)
-        p.out[qi] = omega / (4.0f * k_pi_f);
+        p.out[qi] = omega.value() / (4.0f * k_pi_f);
     if constexpr (Grad) {
         p.grad_x[qi] = gx * inv4pi;
         p.grad_y[qi] = gy * inv4pi;

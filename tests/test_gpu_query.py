@@ -49,9 +49,12 @@ def within(a, b, atol=EXACT_TOL, rtol=2e-5) -> Agreement:
 
 
 def within_except_flips(a, b, atol=EXACT_TOL, rtol=2e-5, frac=1e-3) -> Agreement:
-    """Taylor against an independent traversal: acceptance tests that land within rounding of their
-    threshold may decide differently (FMA contraction, rsqrt), which moves that query by the
-    local truncation error; allow that for at most `frac` of the queries."""
+    """Agreement up to at most `frac` of the queries. Taylor against an independent traversal:
+    acceptance tests that land within rounding of their threshold may decide differently (FMA
+    contraction, rsqrt), which moves that query by the local truncation error. Exact sums: a query
+    by an edge's line leaves FP32 errors up to ~1e-3 in the solid angle formula, which the guarded
+    exact batch re-evaluates in FP64 and a plain FP32 evaluation does not. Callers pair this with
+    a check against FP64."""
     r = Agreement(a, b, atol, rtol)
     r.bad_count = 0 if r.bad_count <= max(1, int(frac * r.n)) else r.bad_count
     return r
@@ -95,11 +98,15 @@ def test_exact_batch_matches_oracle(cuda, name):
     ref = oracle.exact_winding(mesh, *q)
     # 513 coincident triangles sum 513 equal solid angles: FP32 rounding grows with the count
     rtol = 1e-4 if name.startswith("equal") else 2e-5
-    agree = within(out, ref, rtol=rtol)
+    agree = within_except_flips(out, ref, rtol=rtol)
     assert agree, agree
-    # ours is no further from FP64 than the oracle's FP32 brute force (up to rounding)
+    # ours is no further from FP64 than the oracle's FP32 brute force (up to rounding), and with
+    # the FP64 re-evaluation of cancelling pairs it stays within a few FP32 ulps of the sum
     ref64 = oracle.exact_winding(mesh, *q, fp64=True)
-    assert np.max(np.abs(out - ref64)) <= 2 * np.max(np.abs(ref - ref64)) + EXACT_TOL
+    err = np.abs(out - ref64)
+    assert err.max() <= 2 * np.max(np.abs(ref - ref64)) + EXACT_TOL
+    if not name.startswith("equal"):
+        assert err.max() <= 5e-6, err.max()
 
 
 def test_exact_batch_small_workload_full(cuda):
@@ -131,9 +138,10 @@ def test_taylor_matches_oracle_traversal(cuda, name, method, order):
         agree = within_except_flips(out, ref)
         assert agree, agree
     # full descent evaluates every triangle exactly: equal to the exact batch up to summation order
+    # and to the pairs the exact batch re-evaluates in FP64
     full = run_taylor(cuda, order, bvh, mom, q, 1e6)
     exact = run_exact(cuda, bvh, q)
-    agree = within(full, exact)
+    agree = within_except_flips(full, exact)
     assert agree, agree
 
 
@@ -287,8 +295,13 @@ def test_queries_match_reference_kernels(cuda, name):
     R = oracle.Reference(mesh)
     R.build(1, 8, 64)
     q = meshes.mixed_queries(mesh, 4000, seed=12)
-    agree = within(run_exact(cuda, bvh, q), R.exact(*q))
+    ours, theirs = run_exact(cuda, bvh, q), R.exact(*q)
+    # near-surface queries are ill-conditioned in FP32: the two may differ there, where ours
+    # re-evaluates in FP64 and stays within a few ulps of the FP64 sum
+    agree = within_except_flips(ours, theirs)
     assert agree, agree
+    ref64 = oracle.exact_winding(mesh, *q, fp64=True)
+    assert np.max(np.abs(ours - ref64)) <= min(5e-6, 2 * np.max(np.abs(theirs - ref64)) + EXACT_TOL)
     # the two BVH4s are the same tree with differently numbered nodes: pair them up
     h = api.bvh_host_arrays(bvh)
     rb = R.bvh()
@@ -303,8 +316,20 @@ def test_queries_match_reference_kernels(cuda, name):
         # queries whose acceptance test sits at its threshold
         agree = within_except_flips(run_taylor(cuda, order, bvh, mom, q, 2.0), R.taylor(order, *q, beta=2.0))
         assert agree, agree
-        agree = within(run_taylor(cuda, order, bvh, mom, q, 1e6), R.taylor(order, *q, beta=1e6))
+        # full descent: every triangle exactly, with the plain FP32 near field on both sides. Both
+        # FP32 forms lose digits to cancellation for a query on or by an edge's line (up to ~6e-4
+        # for either, and either's worst case can be a few times the other's): typical errors
+        # alike, worst cases of the same order.
+        full, full_ref = run_taylor(cuda, order, bvh, mom, q, 1e6), R.taylor(order, *q, beta=1e6)
+        agree = within_except_flips(full, full_ref)
         assert agree, agree
+        e_ours, e_ref = np.abs(full - ref64), np.abs(full_ref - ref64)
+        assert np.quantile(e_ours, 0.99) <= 2 * np.quantile(e_ref, 0.99) + 1e-6
+        assert e_ours.max() <= 4 * e_ref.max() + EXACT_TOL
+        # the compensated near field with FP64 for cancelling pairs is within a few ulps of FP64
+        comp = run_taylor(cuda, order, bvh, mom, q, 1e6, precision=g.near_precision.compensated,
+                          fp64_threshold=1.0 / 16.0)
+        assert np.abs(comp - ref64).max() <= 5e-6
     R.close()
 
 
