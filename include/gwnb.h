@@ -286,6 +286,25 @@ GWNB_API int gwnb_winding_exact_geometry_fp64(const gwnb_geometry_f32 *geometry,
 GWNB_API int gwnb_query_order_f32(const gwnb_bvh4_f32 *bvh, const float *query_x, const float *query_y,
                                   const float *query_z, uint64_t count, uint32_t *order, gwnb_stream_t stream);
 
+/* Largest batch gwnb_winding_taylor_batch_noalloc_f32 accepts. */
+#define GWNB_NOALLOC_MAX_QUERIES 262144u
+
+/* Taylor batch that allocates no device memory (no smallgwn counterpart: smallgwn's batches need
+ * no scratch, this library's allocate their query-ordering scratch per call). For callers that
+ * cannot let a library allocate -- fixed device-memory budgets owned by a host engine, real-time
+ * loops where an allocation would stall, replayed work that forbids new allocations. Same
+ * arguments and results as gwnb_winding_taylor_batch_f32; at most GWNB_NOALLOC_MAX_QUERIES
+ * queries per call (larger batches return GWNB_INVALID_ARGUMENT). Scratch is one file-scope
+ * device array (about 5.5 MB) that every GPU loading the library holds until exit; calls whose
+ * work overlaps on the GPU race on it. The BVH must already carry derived state (built or refit
+ * by this library). The first call on a device looks up the array's address; make it before any
+ * stream capture. */
+GWNB_API int gwnb_winding_taylor_batch_noalloc_f32(const gwnb_bvh4_f32 *bvh, const gwnb_moment4_f32 *moment,
+                                                   const float *query_x, const float *query_y,
+                                                   const float *query_z, float *output, uint64_t count,
+                                                   float accuracy_scale, const gwnb_taylor_options *options,
+                                                   gwnb_stream_t stream);
+
 /* Number of FP64 fallbacks taken by the last compensated Taylor batch on this BVH (device
  * counter read back with a synchronization). */
 GWNB_API int gwnb_bvh4_fp64_fallback_count(const gwnb_bvh4_f32 *bvh, uint64_t *count, gwnb_stream_t stream);

@@ -695,4 +695,57 @@ int taylor_batch(taylor_request const &r, cudaStream_t s) {
     return rc;
 }
 
+std::size_t radix_sort_u32_scratch_words(std::uint64_t n, int key_bits);
+int radix_sort_pairs_u32_in_scratch(std::uint32_t const *keys_in, std::uint32_t *keys_out,
+                                    std::uint32_t const *values_in, std::uint32_t *values_out, std::uint64_t n,
+                                    int key_bits, std::uint32_t *keys_tmp, std::uint32_t *vals_tmp,
+                                    std::uint32_t *words, cudaStream_t s, unsigned int *status);
+
+// The Taylor batch of taylor_batch() with every temporary in caller-provided scratch (query Morton
+// codes, sorted codes, the order, the sort's ping-pong buffers and its words); allocates nothing.
+int taylor_batch_in_scratch(taylor_request const &r, std::uint32_t *scratch, std::uint64_t capacity,
+                            cudaStream_t s) {
+    if (r.n == 0)
+        return GWNB_OK;
+    if (r.n > capacity)
+        return set_error(GWNB_INVALID_ARGUMENT, "query batch exceeds the scratch capacity");
+    taylor_params p{};
+    p.qnodes = r.qnodes;
+    p.qcounts = r.qcounts;
+    p.tri48 = r.tri48;
+    p.primitive_count = r.primitive_count;
+    p.node_count = r.node_count;
+    p.root_ref = r.root_ref;
+    p.qx = r.qx;
+    p.qy = r.qy;
+    p.qz = r.qz;
+    p.out = r.out;
+    p.n = r.n;
+    p.beta2 = r.accuracy_scale * r.accuracy_scale;
+    p.fp64_threshold = r.fp64_threshold;
+    p.fp64_count = r.fp64_count;
+    p.status = r.status;
+    if (r.sort_queries != 0 && r.n > 1 && r.root_bounds != nullptr) {
+        // five regions of `capacity` words each, then the sort's words
+        std::uint32_t *codes = scratch;
+        std::uint32_t *sorted_codes = scratch + capacity;
+        std::uint32_t *order = scratch + 2 * capacity;
+        std::uint32_t *keys_tmp = scratch + 3 * capacity;
+        std::uint32_t *vals_tmp = scratch + 4 * capacity;
+        std::uint32_t *words = scratch + 5 * capacity;
+        k_query_codes<<<static_cast<unsigned>((r.n + 255) / 256), 256, 0, s>>>(r.qx, r.qy, r.qz, r.n,
+                                                                            r.root_bounds, codes);
+        GWNB_TRY(radix_sort_pairs_u32_in_scratch(codes, sorted_codes, nullptr, order, r.n, 30, keys_tmp, vals_tmp,
+                                                 words, s, r.status));
+        p.order = order;
+    }
+    int const block = r.block > 0 ? r.block : 256;
+    bool const per_thread = r.per_thread != 0;
+    if (r.order == 0)
+        return launch_taylor_order<0, false, false>(p, block, r.stack_capacity, r.near_mode, per_thread, s);
+    if (r.order == 1)
+        return launch_taylor_order<1, false, false>(p, block, r.stack_capacity, r.near_mode, per_thread, s);
+    return launch_taylor_order<2, false, false>(p, block, r.stack_capacity, r.near_mode, per_thread, s);
+}
+
 } // namespace gwnb

@@ -280,7 +280,62 @@ int sort_impl(K const *keys_in, K *keys_out, std::uint32_t const *vals_in,
     return GWNB_OK;
 }
 
+// The same passes as sort_impl over caller-provided scratch: keys_tmp (n keys), vals_tmp (n
+// words) and `words` (histograms, tile counters, tile status), which is cleared here.
+template <class K>
+int sort_in_scratch(K const *keys_in, K *keys_out, std::uint32_t const *vals_in, std::uint32_t *vals_out,
+                    std::uint64_t n, int key_bits, K *keys_tmp, std::uint32_t *vals_tmp, std::uint32_t *words,
+                    cudaStream_t s, unsigned int *status) {
+    constexpr int k_items = sort_items<K>::value;
+    constexpr std::uint64_t k_tile = static_cast<std::uint64_t>(k_threads) * k_items;
+    if (n == 0)
+        return GWNB_OK;
+    int const passes = (key_bits + 7) / 8;
+    std::uint64_t const tiles = (n + k_tile - 1) / k_tile;
+    std::size_t const word_count = passes * 256 + passes + passes * tiles * 256;
+    GWNB_CUDA_TRY(cudaMemsetAsync(words, 0, word_count * sizeof(std::uint32_t), s));
+    std::uint32_t *hist = words;
+    std::uint32_t *counters = words + passes * 256;
+    std::uint32_t *tile_status = counters + passes;
+    int const sms = device_sm_count();
+    unsigned const hist_grid = static_cast<unsigned>(
+        std::min<std::uint64_t>((n + k_threads - 1) / k_threads, static_cast<std::uint64_t>(sms) * 8));
+    k_sort_histogram<K><<<hist_grid, k_threads, 0, s>>>(keys_in, n, passes, key_bits, hist);
+    bool to_out = (passes % 2) == 1;
+    K const *src_k = keys_in;
+    std::uint32_t const *src_v = vals_in;
+    for (int p = 0; p < passes; ++p) {
+        K *dst_k = to_out ? keys_out : keys_tmp;
+        std::uint32_t *dst_v = to_out ? vals_out : vals_tmp;
+        int const bits = std::min(8, key_bits - 8 * p);
+        std::uint32_t const mask = (1u << bits) - 1u;
+        k_onesweep<K, k_items><<<static_cast<unsigned>(tiles), k_threads, 0, s>>>(
+            src_k, src_v, dst_k, dst_v, n, 8 * p, mask, hist + p * 256,
+            tile_status + static_cast<std::size_t>(p) * tiles * 256, counters + p, status);
+        src_k = dst_k;
+        src_v = dst_v;
+        to_out = !to_out;
+    }
+    GWNB_CUDA_TRY(cudaGetLastError());
+    return GWNB_OK;
+}
+
 } // namespace
+
+std::size_t radix_sort_u32_scratch_words(std::uint64_t n, int key_bits) {
+    constexpr std::uint64_t k_tile = static_cast<std::uint64_t>(k_threads) * sort_items<std::uint32_t>::value;
+    int const passes = (key_bits + 7) / 8;
+    std::uint64_t const tiles = (n + k_tile - 1) / k_tile;
+    return static_cast<std::size_t>(passes * 256 + passes + passes * tiles * 256);
+}
+
+int radix_sort_pairs_u32_in_scratch(std::uint32_t const *keys_in, std::uint32_t *keys_out,
+                                    std::uint32_t const *values_in, std::uint32_t *values_out, std::uint64_t n,
+                                    int key_bits, std::uint32_t *keys_tmp, std::uint32_t *vals_tmp,
+                                    std::uint32_t *words, cudaStream_t s, unsigned int *status) {
+    return sort_in_scratch<std::uint32_t>(keys_in, keys_out, values_in, values_out, n, key_bits, keys_tmp, vals_tmp,
+                                          words, s, status);
+}
 
 int radix_sort_pairs(void const *keys_in, void *keys_out, std::uint32_t const *values_in,
                      std::uint32_t *values_out, std::uint64_t n, int key_bytes, int key_bits,
