@@ -309,6 +309,44 @@ GWNB_API int gwnb_winding_taylor_batch_noalloc_f32(const gwnb_bvh4_f32 *bvh, con
  * counter read back with a synchronization). */
 GWNB_API int gwnb_bvh4_fp64_fallback_count(const gwnb_bvh4_f32 *bvh, uint64_t *count, gwnb_stream_t stream);
 
+/* ---- adjoint of the Taylor batch (no smallgwn counterpart) --------------------------------- */
+
+/* What a forward pass keeps for its backward pass -- the save-for-backward contract a
+ * torch.autograd.Function wraps: the query arrays by reference (the caller keeps them alive and
+ * unchanged until the backward call) and the BVH revision the result was computed at. No
+ * traversal state is kept; the backward pass recomputes the traversal. */
+typedef struct gwnb_taylor_saved_f32 {
+    const float *query_x;
+    const float *query_y;
+    const float *query_z;
+    uint64_t count;
+    float accuracy_scale;
+    int order;
+    uint64_t bvh_revision;
+    gwnb_taylor_options options;
+} gwnb_taylor_saved_f32;
+
+/* Forward: the Taylor batch of gwnb_winding_taylor_batch_f32 (orders 0 and 1 only), filling
+ * `saved` for gwnb_winding_taylor_backward_f32. */
+GWNB_API int gwnb_winding_taylor_forward_f32(const gwnb_bvh4_f32 *bvh, const gwnb_moment4_f32 *moment,
+                                             const float *query_x, const float *query_y, const float *query_z,
+                                             float *output, uint64_t count, float accuracy_scale,
+                                             const gwnb_taylor_options *options, gwnb_taylor_saved_f32 *saved,
+                                             gwnb_stream_t stream);
+
+/* Backward: given grad_output g (count floats), the gradients of L = sum_q g_q w(q) with respect to
+ * the geometry's vertex positions (grad_vertex_*: vertex_count floats each, overwritten) and the
+ * query points (grad_query_*: count floats each). Either triple may be all NULL to skip it. The
+ * BVH must be the one of the forward pass at the same revision, built from `geometry` (one
+ * primitive per geometry triangle), with `moment` refit for it. Acceptance decisions are held
+ * fixed (they carry no derivative); slots of zero area pass no gradient through their centre.
+ * Asynchronous on `stream`. */
+GWNB_API int gwnb_winding_taylor_backward_f32(const gwnb_taylor_saved_f32 *saved, const gwnb_geometry_f32 *geometry,
+                                              const gwnb_bvh4_f32 *bvh, const gwnb_moment4_f32 *moment,
+                                              const float *grad_output, float *grad_vertex_x,
+                                              float *grad_vertex_y, float *grad_vertex_z, float *grad_query_x,
+                                              float *grad_query_y, float *grad_query_z, gwnb_stream_t stream);
+
 #ifdef __cplusplus
 }
 #endif

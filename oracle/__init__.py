@@ -204,6 +204,30 @@ def taylor(order: int, nodes: np.ndarray, mom: np.ndarray, tris: np.ndarray, roo
     return (out, st) if stats else out
 
 
+def taylor_frozen_f64(order: int, nodes: np.ndarray, mom: np.ndarray, root_ref: int, vertices: np.ndarray,
+                      mesh: dict, primitive_indices: np.ndarray, decide, evaluate, beta: float = 2.0,
+                      threads: int = 0) -> np.ndarray:
+    """FP64 Taylor winding numbers (orders 0, 1) with the float traversal's acceptance decisions
+    frozen: decisions from the float moment nodes `mom` at the float points `decide`, the sum in
+    FP64 at the points `evaluate` with moments recomputed from the FP64 `vertices` (V, 3). Central
+    differences of it are the checker of the adjoint."""
+    threads = threads or max_threads()
+    nd = np.ascontiguousarray(nodes.reshape(-1, 4), dtype=NODE_DTYPE)
+    m = np.ascontiguousarray(mom, np.float32)
+    v = [np.ascontiguousarray(vertices[:, k], np.float64) for k in range(3)]
+    i0, i1, i2 = _u32(mesh["i0"]), _u32(mesh["i1"]), _u32(mesh["i2"])
+    prim = _u32(primitive_indices)
+    d = [_f32(x) for x in decide]
+    e = [np.ascontiguousarray(x, np.float64) for x in evaluate]
+    n = d[0].size
+    out = np.empty(n, np.float64)
+    lib().oracle_taylor_frozen_f64(C.c_int(order), _p(nd), C.c_uint64(nd.shape[0]), C.c_uint64(root_ref), _p(m),
+                                   _p(v[0]), _p(v[1]), _p(v[2]), _p(i0), _p(i1), _p(i2), _p(prim),
+                                   C.c_uint64(prim.size), _p(d[0]), _p(d[1]), _p(d[2]), _p(e[0]), _p(e[1]), _p(e[2]),
+                                   C.c_uint64(n), C.c_float(beta), _p(out), C.c_int(threads))
+    return out
+
+
 def build_lbvh(mesh: dict, bits: int = 64) -> dict:
     """Full CPU pipeline: Morton, stable sort, Karras, bounds, BVH4 collapse, triangle records."""
     aabbs, codes, scene = morton(mesh, bits)
@@ -300,6 +324,14 @@ class Reference:
         self._check(self.lib.ref_taylor(self.h, C.c_int(order), _p(q[0]), _p(q[1]), _p(q[2]), _p(out),
                                         C.c_uint64(out.size), C.c_float(beta)))
         return out
+
+    def taylor_gradient(self, order: int, qx, qy, qz, beta: float = 2.0) -> np.ndarray:
+        """smallgwn's Taylor query gradient, shape (n, 3)."""
+        q = [_f32(v) for v in (qx, qy, qz)]
+        g = [np.empty(q[0].size, np.float32) for _ in range(3)]
+        self._check(self.lib.ref_taylor_gradient(self.h, C.c_int(order), _p(q[0]), _p(q[1]), _p(q[2]), _p(g[0]),
+                                                 _p(g[1]), _p(g[2]), C.c_uint64(q[0].size), C.c_float(beta)))
+        return np.stack(g, -1)
 
     def time_taylor(self, order: int, qx, qy, qz, beta: float, warmup: int, iters: int) -> float:
         q = [_f32(v) for v in (qx, qy, qz)]

@@ -988,3 +988,203 @@ int oracle_max_threads(void) {
     return 1;
 #endif
 }
+
+/* ---------------------------------------------------------------------------------------------- */
+/* FP64 Taylor winding numbers (orders 0 and 1) with frozen acceptance decisions: the checker of   */
+/* the adjoint. The decisions are those of the float traversal of taylor_one (the test of          */
+/* detail/gwn_query_winding_impl.cuh:168-240 on the float moment nodes at the float decision       */
+/* point); the sum is then evaluated in FP64 at an FP64 evaluation point, with every slot's         */
+/* moments recomputed in FP64 from FP64 vertex positions by the formulas of                         */
+/* detail/gwn_bvh_refit_common.cuh:67-121 (N = sum n, P = sum A c / sum A or the box centre,        */
+/* M_ij = sum n_i c_j - N_i P_j) and triangles reached in the near field evaluated exactly.          */
+/* Central differences of this piecewise-smooth function are what the adjoint must reproduce.      */
+
+typedef struct {
+    double area, ac[3], n[3], nc[3][3];
+} o_pay64;
+
+typedef struct {
+    double P[3], N[3], M[3][3];
+} o_slot64;
+
+static void tri_pay64(const double *vx, const double *vy, const double *vz, uint32_t a, uint32_t b, uint32_t c,
+                      o_pay64 *m) {
+    double v0[3] = {vx[a], vy[a], vz[a]}, v1[3] = {vx[b], vy[b], vz[b]}, v2[3] = {vx[c], vy[c], vz[c]};
+    double e1[3], e2[3], ce[3], n[3];
+    for (int k = 0; k < 3; ++k) {
+        e1[k] = v1[k] - v0[k];
+        e2[k] = v2[k] - v0[k];
+        ce[k] = (v0[k] + v1[k] + v2[k]) / 3.0;
+    }
+    n[0] = 0.5 * (e1[1] * e2[2] - e1[2] * e2[1]);
+    n[1] = 0.5 * (e1[2] * e2[0] - e1[0] * e2[2]);
+    n[2] = 0.5 * (e1[0] * e2[1] - e1[1] * e2[0]);
+    m->area = sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+    for (int i = 0; i < 3; ++i) {
+        m->ac[i] = m->area * ce[i];
+        m->n[i] = n[i];
+        for (int j = 0; j < 3; ++j)
+            m->nc[i][j] = n[i] * ce[j];
+    }
+}
+
+static void pay64_acc(o_pay64 *d, const o_pay64 *s) {
+    d->area += s->area;
+    for (int i = 0; i < 3; ++i) {
+        d->ac[i] += s->ac[i];
+        d->n[i] += s->n[i];
+        for (int j = 0; j < 3; ++j)
+            d->nc[i][j] += s->nc[i][j];
+    }
+}
+
+static double solid_angle_d(const double a[3], const double b[3], const double c[3]) {
+    double la = sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]);
+    double lb = sqrt(b[0] * b[0] + b[1] * b[1] + b[2] * b[2]);
+    double lc = sqrt(c[0] * c[0] + c[1] * c[1] + c[2] * c[2]);
+    if (la == 0.0 || lb == 0.0 || lc == 0.0)
+        return 0.0;
+    double num = a[0] * (b[1] * c[2] - b[2] * c[1]) + a[1] * (b[2] * c[0] - b[0] * c[2]) +
+                 a[2] * (b[0] * c[1] - b[1] * c[0]);
+    if (num == 0.0)
+        return 0.0;
+    double den = la * lb * lc + (a[0] * b[0] + a[1] * b[1] + a[2] * b[2]) * lc +
+                 (a[0] * c[0] + a[1] * c[1] + a[2] * c[2]) * lb + (b[0] * c[0] + b[1] * c[1] + b[2] * c[2]) * la;
+    return 2.0 * atan2(num, den);
+}
+
+/* nodes: the BVH4 (children after parents); mom: the float moment nodes the decisions use;
+ * vx/vy/vz: FP64 vertex positions; i0/i1/i2: geometry triangles; prim: sorted -> geometry triangle;
+ * d*: float decision points; e*: FP64 evaluation points. out: winding numbers (FP64). */
+void oracle_taylor_frozen_f64(int order, const o_node4 *nodes, uint64_t nn, uint64_t root_ref, const float *mom,
+                              const double *vx, const double *vy, const double *vz, const uint32_t *i0,
+                              const uint32_t *i1, const uint32_t *i2, const uint32_t *prim, uint64_t nt,
+                              const float *dx, const float *dy, const float *dz, const double *ex, const double *ey,
+                              const double *ez, uint64_t nq, float beta, double *out, int threads) {
+    const double k_pi = 3.141592653589793238462643383279502884;
+    int F = field_count(order);
+    float beta2 = beta * beta;
+    o_slot64 *slots = (o_slot64 *)calloc(nn ? nn * 4 : 1, sizeof(o_slot64));
+    o_pay64 *pend = (o_pay64 *)calloc(nn ? nn : 1, sizeof(o_pay64));
+    for (int64_t n = (int64_t)nn - 1; n >= 0; --n) {
+        o_pay64 total;
+        memset(&total, 0, sizeof(total));
+        for (int s = 0; s < 4; ++s) {
+            uint64_t r = nodes[n].c[s].reference;
+            if (!ref_valid(r))
+                continue;
+            o_pay64 m;
+            memset(&m, 0, sizeof(m));
+            if (ref_internal(r)) {
+                m = pend[ref_offset(r)];
+            } else {
+                for (uint32_t k = 0; k < ref_count(r) && ref_offset(r) + k < nt; ++k) {
+                    uint32_t t = prim[ref_offset(r) + k];
+                    o_pay64 tm;
+                    tri_pay64(vx, vy, vz, i0[t], i1[t], i2[t], &tm);
+                    pay64_acc(&m, &tm);
+                }
+            }
+            o_slot64 *sl = &slots[(uint64_t)n * 4 + s];
+            o_aabb b = nodes[n].c[s].bounds;
+            double P[3];
+            if (m.area > 0.0) {
+                for (int i = 0; i < 3; ++i)
+                    P[i] = m.ac[i] / m.area;
+            } else {
+                P[0] = 0.5 * ((double)b.min_x + b.max_x);
+                P[1] = 0.5 * ((double)b.min_y + b.max_y);
+                P[2] = 0.5 * ((double)b.min_z + b.max_z);
+            }
+            for (int i = 0; i < 3; ++i) {
+                sl->P[i] = P[i];
+                sl->N[i] = m.n[i];
+                for (int j = 0; j < 3; ++j)
+                    sl->M[i][j] = m.nc[i][j] - m.n[i] * P[j];
+            }
+            pay64_acc(&total, &m);
+        }
+        pend[n] = total;
+    }
+    (void)threads;
+#pragma omp parallel for schedule(dynamic, 16) num_threads(threads > 0 ? threads : 1)
+    for (int64_t q = 0; q < (int64_t)nq; ++q) {
+        double e[3] = {ex[q], ey[q], ez[q]};
+        double omega = 0.0;
+        uint32_t stack[256];
+        int sp = 0;
+        if (ref_leaf(root_ref)) {
+            for (uint32_t k = 0; k < ref_count(root_ref) && ref_offset(root_ref) + k < nt; ++k) {
+                uint32_t t = prim[ref_offset(root_ref) + k];
+                double a[3] = {vx[i0[t]] - e[0], vy[i0[t]] - e[1], vz[i0[t]] - e[2]};
+                double b[3] = {vx[i1[t]] - e[0], vy[i1[t]] - e[1], vz[i1[t]] - e[2]};
+                double c[3] = {vx[i2[t]] - e[0], vy[i2[t]] - e[1], vz[i2[t]] - e[2]};
+                omega += solid_angle_d(a, b, c);
+            }
+        } else {
+            uint32_t node = (uint32_t)ref_offset(root_ref);
+            for (;;) {
+                if (node >= nn)
+                    break;
+                const float *T = mom + (uint64_t)node * F * 4;
+                uint32_t next = INV32;
+                for (int s = 0; s < 4; ++s) {
+                    uint64_t r = nodes[node].c[s].reference;
+                    if (!ref_valid(r))
+                        continue;
+                    float rx = dx[q] - T[1 * 4 + s], ry = dy[q] - T[2 * 4 + s], rz = dz[q] - T[3 * 4 + s];
+                    float q2 = rx * rx + ry * ry + rz * rz;
+                    int descend = !(q2 > 0.0f);
+                    if (!descend)
+                        descend = q2 <= T[0 * 4 + s] * beta2;
+                    if (!descend) {
+                        const o_slot64 *sl = &slots[(uint64_t)node * 4 + s];
+                        double d[3] = {e[0] - sl->P[0], e[1] - sl->P[1], e[2] - sl->P[2]};
+                        double r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+                        double m1 = 1.0 / sqrt(r2), m2 = m1 * m1, m3 = m2 * m1;
+                        double u[3] = {d[0] * m1, d[1] * m1, d[2] * m1};
+                        double w = -m2 * (u[0] * sl->N[0] + u[1] * sl->N[1] + u[2] * sl->N[2]);
+                        if (order >= 1) {
+                            double tr = sl->M[0][0] + sl->M[1][1] + sl->M[2][2];
+                            double S = 0.0;
+                            for (int i = 0; i < 3; ++i)
+                                for (int j = 0; j < 3; ++j)
+                                    S += u[i] * sl->M[i][j] * u[j];
+                            w += m3 * (tr - 3.0 * S);
+                        }
+                        omega += w;
+                        continue;
+                    }
+                    if (ref_internal(r)) {
+                        if (next != INV32) {
+                            if (sp >= 256) {
+                                omega = NAN;
+                                break;
+                            }
+                            stack[sp++] = next;
+                        }
+                        next = (uint32_t)ref_offset(r);
+                        continue;
+                    }
+                    for (uint32_t k = 0; k < ref_count(r) && ref_offset(r) + k < nt; ++k) {
+                        uint32_t t = prim[ref_offset(r) + k];
+                        double a[3] = {vx[i0[t]] - e[0], vy[i0[t]] - e[1], vz[i0[t]] - e[2]};
+                        double b[3] = {vx[i1[t]] - e[0], vy[i1[t]] - e[1], vz[i1[t]] - e[2]};
+                        double c[3] = {vx[i2[t]] - e[0], vy[i2[t]] - e[1], vz[i2[t]] - e[2]};
+                        omega += solid_angle_d(a, b, c);
+                    }
+                }
+                if (next != INV32) {
+                    node = next;
+                    continue;
+                }
+                if (sp == 0)
+                    break;
+                node = stack[--sp];
+            }
+        }
+        out[q] = omega / (4.0 * k_pi);
+    }
+    free(slots);
+    free(pend);
+}

@@ -81,6 +81,18 @@ gwn::gwn_status taylor_any(ctx &c, gwn::gwn_bvh4_moment_object<Order, Real, Inde
     return taylor_cfg<Order, gwn::gwn_query_batch_config{256, 256}>(c, m, x, y, z, o, beta);
 }
 
+template <int Order>
+gwn::gwn_status gradient_any(ctx &c, gwn::gwn_bvh4_moment_object<Order, Real, Index> const &m, dbuf<float> &x,
+                             dbuf<float> &y, dbuf<float> &z, dbuf<float> &gx, dbuf<float> &gy, dbuf<float> &gz,
+                             float beta) {
+    constexpr gwn::gwn_query_batch_config cfg{256, 64};
+    return gwn::gwn_compute_winding_gradient_taylor_batch<Order, cfg, 4, Real, Index, no_trap>(
+        c.bvh, m, gwn::gwn_device_span<float const>(x.p, x.n), gwn::gwn_device_span<float const>(y.p, y.n),
+        gwn::gwn_device_span<float const>(z.p, z.n), gwn::gwn_device_span<float>(gx.p, gx.n),
+        gwn::gwn_device_span<float>(gy.p, gy.n), gwn::gwn_device_span<float>(gz.p, gz.n), beta,
+        gwn::gwn_default_stream(), no_trap{});
+}
+
 gwn::gwn_status taylor_order(ctx &c, int order, dbuf<float> &x, dbuf<float> &y, dbuf<float> &z, dbuf<float> &o,
                              float beta) {
     if (order == 0)
@@ -189,6 +201,27 @@ int ref_taylor(void *p, int order, const float *qx, const float *qy, const float
         return fail(s);
     cudaDeviceSynchronize();
     o.to_host(out);
+    return static_cast<int>(cudaGetLastError());
+}
+
+// smallgwn's Taylor query gradient (gwn_compute_winding_gradient_taylor_batch) of a host batch.
+int ref_taylor_gradient(void *p, int order, const float *qx, const float *qy, const float *qz, float *gx, float *gy,
+                        float *gz, uint64_t n, float beta) {
+    auto &c = *static_cast<ctx *>(p);
+    if (c.bvh.accessor().internal_stack_bound > 64) {
+        g_msg = "stack bound above 64";
+        return -1;
+    }
+    dbuf<float> x(qx, n), y(qy, n), z(qz, n), ox(n), oy(n), oz(n);
+    gwn::gwn_status s = order == 0   ? gradient_any<0>(c, c.m0, x, y, z, ox, oy, oz, beta)
+                        : order == 1 ? gradient_any<1>(c, c.m1, x, y, z, ox, oy, oz, beta)
+                                     : gradient_any<2>(c, c.m2, x, y, z, ox, oy, oz, beta);
+    if (!s.is_ok())
+        return fail(s);
+    cudaDeviceSynchronize();
+    ox.to_host(gx);
+    oy.to_host(gy);
+    oz.to_host(gz);
     return static_cast<int>(cudaGetLastError());
 }
 

@@ -19,7 +19,10 @@ from .api import (  # noqa: F401
     gwn_refit_bvh,
     gwn_refit_bvh_moment,
     gwn_status,
+    gwn_taylor_saved,
     gwn_update_geometry,
     gwn_upload_geometry,
+    gwn_winding_taylor_backward,
+    gwn_winding_taylor_forward,
     near_precision,
 )

@@ -84,6 +84,19 @@ class taylor_options(C.Structure):
     ]
 
 
+class taylor_saved_f32(C.Structure):
+    _fields_ = [
+        ("query_x", C.c_void_p),
+        ("query_y", C.c_void_p),
+        ("query_z", C.c_void_p),
+        ("count", C.c_uint64),
+        ("accuracy_scale", C.c_float),
+        ("order", C.c_int),
+        ("bvh_revision", C.c_uint64),
+        ("options", taylor_options),
+    ]
+
+
 class binary_node(C.Structure):
     _fields_ = [(n, C.c_uint32) for n in ("left_index", "left_kind", "right_index", "right_kind")]
 
@@ -130,6 +143,12 @@ SIGNATURES: dict[str, tuple] = {
     "gwnb_query_order_f32": (I, [C.POINTER(bvh4_f32), P, P, P, U64, P, P]),
     "gwnb_winding_taylor_batch_noalloc_f32": (
         I, [C.POINTER(bvh4_f32), C.POINTER(moment4_f32), P, P, P, P, U64, F, C.POINTER(taylor_options), P]),
+    "gwnb_winding_taylor_forward_f32": (
+        I, [C.POINTER(bvh4_f32), C.POINTER(moment4_f32), P, P, P, P, U64, F, C.POINTER(taylor_options),
+            C.POINTER(taylor_saved_f32), P]),
+    "gwnb_winding_taylor_backward_f32": (
+        I, [C.POINTER(taylor_saved_f32), C.POINTER(geometry_f32), C.POINTER(bvh4_f32), C.POINTER(moment4_f32), P,
+            P, P, P, P, P, P, P]),
 }
 
 _lib: C.CDLL | None = None

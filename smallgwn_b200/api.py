@@ -412,6 +412,53 @@ def sync_bvh_status(bvh: gwn_bvh4_object, stream=None) -> gwn_status:
     return _status(_lib.load().gwnb_bvh4_sync_status_f32(C.byref(bvh._view), _stream(stream)))
 
 
+# ---- adjoint of the Taylor batch ------------------------------------------------------------------
+
+class gwn_taylor_saved:
+    """What a forward pass keeps for its backward pass: the query buffers (held here, so they stay
+    alive) and the BVH revision; the backward pass recomputes the traversal."""
+
+    def __init__(self, queries) -> None:
+        self._view = _lib.taylor_saved_f32()
+        self._queries = queries
+
+
+def gwn_winding_taylor_forward(order: int, bvh: gwn_bvh4_object, moment: gwn_bvh4_moment_object, qx, qy, qz, out,
+                               accuracy_scale: float = 2.0, stream=None,
+                               config: gwn_query_batch_config = gwn_query_batch_config(),
+                               sort_queries: bool = True, precision: int = near_precision.plain,
+                               fp64_threshold: float = FP64_THRESHOLD) -> tuple[gwn_status, gwn_taylor_saved | None]:
+    """Taylor winding numbers (orders 0 and 1) plus the saved state of their backward pass."""
+    if moment.order != order:
+        return gwn_status(gwn_error.invalid_argument, "Moment object order does not match the requested order."), None
+    bad = _check_spans(qx, qy, qz, out)
+    if bad is not None:
+        return bad, None
+    saved = gwn_taylor_saved((qx, qy, qz))
+    opt = _options(config, sort_queries, precision, fp64_threshold, False)
+    rc = _lib.load().gwnb_winding_taylor_forward_f32(
+        C.byref(bvh._view), C.byref(moment._view), _ptr(qx), _ptr(qy), _ptr(qz), _ptr(out), _numel(out),
+        float(accuracy_scale), C.byref(opt), C.byref(saved._view), _stream(stream))
+    st = _status(rc)
+    return st, (saved if st.is_ok() else None)
+
+
+def gwn_winding_taylor_backward(saved: gwn_taylor_saved, geometry: gwn_geometry_object | None, bvh: gwn_bvh4_object,
+                                moment: gwn_bvh4_moment_object, grad_out, dvx=None, dvy=None, dvz=None, dqx=None,
+                                dqy=None, dqz=None, stream=None) -> gwn_status:
+    """dL/dV (vertex_count floats per axis, overwritten) and dL/dq (query count per axis) of
+    L = sum_q grad_out[q] * w(q); pass None for a triple to skip it."""
+    if saved is None:
+        return gwn_status(gwn_error.invalid_argument, "Taylor backward: saved state must be non-null.")
+    if _numel(grad_out) != int(saved._view.count):
+        return gwn_status(gwn_error.invalid_argument, "Upstream gradient size must match the query count.")
+    geo = C.byref(geometry._view) if geometry is not None else None
+    rc = _lib.load().gwnb_winding_taylor_backward_f32(
+        C.byref(saved._view), geo, C.byref(bvh._view), C.byref(moment._view), _ptr(grad_out), _ptr(dvx), _ptr(dvy),
+        _ptr(dvz), _ptr(dqx), _ptr(dqy), _ptr(dqz), _stream(stream))
+    return _status(rc)
+
+
 # ---- host views of device state (tests, diagnostics) ------------------------------------------------
 
 NODE_DTYPE = np.dtype([("bounds", np.float32, (6,)), ("reference", np.uint64)])

@@ -781,4 +781,107 @@ int gwnb_bvh4_fp64_fallback_count(const gwnb_bvh4_f32 *b, uint64_t *count, gwnb_
     return GWNB_OK;
 }
 
+int gwnb_winding_taylor_forward_f32(const gwnb_bvh4_f32 *b, const gwnb_moment4_f32 *m, const float *qx,
+                                    const float *qy, const float *qz, float *out, uint64_t n, float beta,
+                                    const gwnb_taylor_options *opt, gwnb_taylor_saved_f32 *saved,
+                                    gwnb_stream_t stream) {
+    if (saved == nullptr)
+        return set_error(GWNB_INVALID_ARGUMENT, "Taylor forward: saved state must be non-null.");
+    if (m == nullptr || (m->order != 0 && m->order != 1))
+        return set_error(GWNB_INVALID_ARGUMENT, "The Taylor adjoint supports orders 0 and 1.");
+    GWNB_TRY(taylor_common(b, m, qx, qy, qz, out, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, n, beta, opt,
+                           stream));
+    gwnb_taylor_options o{256, 64, 1, GWNB_NEAR_PLAIN, 1.0f / 16.0f, 0};
+    if (opt != nullptr)
+        o = *opt;
+    if (o.block_size == 0)
+        o.block_size = 256;
+    if (o.stack_capacity == 0)
+        o.stack_capacity = 64;
+    saved->query_x = qx;
+    saved->query_y = qy;
+    saved->query_z = qz;
+    saved->count = n;
+    saved->accuracy_scale = beta;
+    saved->order = m->order;
+    saved->bvh_revision = b->revision;
+    saved->options = o;
+    return GWNB_OK;
+}
+
+int gwnb_winding_taylor_backward_f32(const gwnb_taylor_saved_f32 *saved, const gwnb_geometry_f32 *g,
+                                     const gwnb_bvh4_f32 *b_in, const gwnb_moment4_f32 *m, const float *gout,
+                                     float *dvx, float *dvy, float *dvz, float *dqx, float *dqy, float *dqz,
+                                     gwnb_stream_t stream) {
+    if (saved == nullptr)
+        return set_error(GWNB_INVALID_ARGUMENT, "Taylor backward: saved state must be non-null.");
+    if (saved->order != 0 && saved->order != 1)
+        return set_error(GWNB_INVALID_ARGUMENT, "The Taylor adjoint supports orders 0 and 1.");
+    if (!bvh_valid(b_in))
+        return set_error(GWNB_INVALID_ARGUMENT, "BVH object contains no queryable data.");
+    if (b_in->revision != saved->bvh_revision)
+        return set_error(GWNB_INVALID_ARGUMENT, "Taylor backward: the BVH changed since the forward pass.");
+    if (!moment_valid_for(m, b_in) || m->order != saved->order)
+        return set_error(GWNB_INVALID_ARGUMENT, "Moment object is not aligned with the BVH.");
+    bool const want_v = dvx != nullptr || dvy != nullptr || dvz != nullptr;
+    bool const want_q = dqx != nullptr || dqy != nullptr || dqz != nullptr;
+    if (want_v && (dvx == nullptr || dvy == nullptr || dvz == nullptr))
+        return set_error(GWNB_INVALID_ARGUMENT, "Vertex gradient outputs must be all null or all non-null.");
+    if (want_q && (dqx == nullptr || dqy == nullptr || dqz == nullptr))
+        return set_error(GWNB_INVALID_ARGUMENT, "Query gradient outputs must be all null or all non-null.");
+    if (want_v) {
+        if (!geometry_valid(g))
+            return set_error(GWNB_INVALID_ARGUMENT, "Geometry accessor is invalid.");
+        if (g->triangle_count != b_in->primitive_count)
+            return set_error(GWNB_INVALID_ARGUMENT, "Taylor backward: geometry does not match the BVH.");
+    }
+    std::uint64_t const n = saved->count;
+    if (!has_storage(gout, n) || !has_storage(saved->query_x, n) || !has_storage(saved->query_y, n) ||
+        !has_storage(saved->query_z, n))
+        return set_error(GWNB_INVALID_ARGUMENT, "Query/output spans must use non-null storage when non-empty.");
+    if (ref_internal(b_in->root.reference) && b_in->internal_stack_bound > 64)
+        return set_error(GWNB_INVALID_ARGUMENT, "Taylor backward: stack bounds above 64 are not supported.");
+    if (!want_v && !want_q)
+        return GWNB_OK;
+    cudaStream_t const s = as_cuda(stream);
+    auto *b = const_cast<gwnb_bvh4_f32 *>(b_in);
+    GWNB_TRY(ensure_bvh_aux(b, s));
+    auto *a = reinterpret_cast<bvh_aux_impl *>(b->aux);
+    auto *ma = reinterpret_cast<moment_aux_impl *>(m->aux);
+    adjoint_request r{};
+    r.order = saved->order;
+    r.qnodes = ma != nullptr ? ma->qnodes : nullptr;
+    r.qcounts = ma != nullptr ? ma->qcounts : nullptr;
+    r.tri48 = a->tri48;
+    r.triangles = reinterpret_cast<triangle const *>(b->triangles);
+    r.nodes = reinterpret_cast<node4 const *>(b->nodes);
+    r.primitive_count = b->primitive_count;
+    r.node_count = b->node_count;
+    r.root_ref = b->root.reference;
+    r.root_bounds = a->root_bounds;
+    r.parent_slot = a->parent_slot;
+    r.primitive_indices = b->primitive_indices;
+    r.payload = ma != nullptr ? static_cast<float const *>(ma->payload) : nullptr;
+    r.payload_floats = ma != nullptr ? ma->payload_stride / sizeof(float) : 0;
+    if (want_v)
+        r.g = *g;
+    r.qx = saved->query_x;
+    r.qy = saved->query_y;
+    r.qz = saved->query_z;
+    r.grad_out = gout;
+    r.dvx = want_v ? dvx : nullptr;
+    r.dvy = want_v ? dvy : nullptr;
+    r.dvz = want_v ? dvz : nullptr;
+    r.dqx = want_q ? dqx : nullptr;
+    r.dqy = want_q ? dqy : nullptr;
+    r.dqz = want_q ? dqz : nullptr;
+    r.n = n;
+    r.accuracy_scale = saved->accuracy_scale;
+    r.block = 256; // the backward traversal's own launch shape (its kernels are bounded to 256 threads)
+    r.stack_capacity = std::max<int>(static_cast<int>(b->internal_stack_bound), 1);
+    r.sort_queries = saved->options.sort_queries;
+    r.status = a->status;
+    return taylor_adjoint(r, s);
+}
+
 } // extern "C"

@@ -196,6 +196,36 @@ struct taylor_request {
 };
 int taylor_batch(taylor_request const &r, cudaStream_t s);
 
+// One backward pass of the Taylor batch (orders 0 and 1) as the C ABI hands it to the adjoint.
+struct adjoint_request {
+    int order;
+    float4 const *qnodes;
+    std::uint32_t const *qcounts;
+    triangle48 const *tri48;
+    triangle const *triangles;
+    node4 const *nodes;
+    std::uint64_t primitive_count;
+    std::uint64_t node_count;
+    std::uint64_t root_ref;
+    aabb const *root_bounds;           // device
+    std::uint32_t const *parent_slot;  // per node: (parent << 2) | slot
+    std::uint32_t const *primitive_indices;
+    float const *payload;              // per-node moment payload (area first)
+    std::uint64_t payload_floats;
+    gwnb_geometry_f32 g;
+    float const *qx, *qy, *qz;
+    float const *grad_out;
+    float *dvx, *dvy, *dvz; // nullptr: no vertex gradients
+    float *dqx, *dqy, *dqz; // nullptr: no query gradients
+    std::uint64_t n;
+    float accuracy_scale;
+    int block;
+    int stack_capacity;
+    int sort_queries;
+    unsigned int *status;
+};
+int taylor_adjoint(adjoint_request const &r, cudaStream_t s);
+
 int create_bvh_aux(gwnb_bvh4_f32 *bvh, cudaStream_t s);
 int ensure_bvh_aux(gwnb_bvh4_f32 *bvh, cudaStream_t s);
 int write_tri48(gwnb_bvh4_f32 const *bvh, cudaStream_t s);

@@ -120,6 +120,48 @@ def test_stack_capacity_below_bound_is_rejected():
     assert "Traversal stack capacity" in _lib.last_error()
 
 
+def test_adjoint_pair_validation():
+    """The Taylor forward / backward pair refuses bad calls on the host, before any device work."""
+    lib = _lib.load()
+    fake = _lib.bvh4_f32()
+    fake.nodes = 8
+    fake.node_count = 3
+    fake.primitive_count = 9
+    fake.primitive_indices = 8
+    fake.triangles = 8
+    fake.revision = 5
+    fake.internal_stack_bound = 2
+    fake.root.reference = 1 << 47
+    mom1 = _lib.moment4_f32(order=1, bvh_revision=5, node_count=3, nodes=8, aux=8)
+    mom2 = _lib.moment4_f32(order=2, bvh_revision=5, node_count=3, nodes=8, aux=8)
+    saved = _lib.taylor_saved_f32()
+    # no saved state
+    assert lib.gwnb_winding_taylor_forward_f32(C.byref(fake), C.byref(mom1), None, None, None, None, 0, 2.0, None,
+                                               None, None) == _lib.GWNB_INVALID_ARGUMENT
+    assert "saved state" in _lib.last_error()
+    # order 2 has no adjoint
+    assert lib.gwnb_winding_taylor_forward_f32(C.byref(fake), C.byref(mom2), None, None, None, None, 0, 2.0, None,
+                                               C.byref(saved), None) == _lib.GWNB_INVALID_ARGUMENT
+    assert "orders 0 and 1" in _lib.last_error()
+    assert lib.gwnb_winding_taylor_backward_f32(None, None, C.byref(fake), C.byref(mom1), None, None, None, None,
+                                                None, None, None, None) == _lib.GWNB_INVALID_ARGUMENT
+    saved.order = 2
+    assert lib.gwnb_winding_taylor_backward_f32(C.byref(saved), None, C.byref(fake), C.byref(mom1), None, None,
+                                                None, None, None, None, None, None) == _lib.GWNB_INVALID_ARGUMENT
+    assert "orders 0 and 1" in _lib.last_error()
+    # the BVH must be at the forward pass's revision
+    saved.order = 1
+    saved.bvh_revision = 4
+    assert lib.gwnb_winding_taylor_backward_f32(C.byref(saved), None, C.byref(fake), C.byref(mom1), None, None,
+                                                None, None, None, None, None, None) == _lib.GWNB_INVALID_ARGUMENT
+    assert "changed since the forward pass" in _lib.last_error()
+    # partial output triples are refused
+    saved.bvh_revision = 5
+    assert lib.gwnb_winding_taylor_backward_f32(C.byref(saved), None, C.byref(fake), C.byref(mom1), None, 8, None,
+                                                None, None, None, None, None) == _lib.GWNB_INVALID_ARGUMENT
+    assert "all null or all non-null" in _lib.last_error()
+
+
 def test_status_mirror():
     assert api.gwn_status().is_ok()
     assert not api.gwn_status(api.gwn_error.internal_error, "x").is_ok()

@@ -1,0 +1,244 @@
+"""GPU checks of the Taylor adjoint (gwnb_winding_taylor_forward_f32 / _backward_f32).
+
+The backward pass gives dL/dV and dL/dq of L = sum_q g_q w(q). Checked against:
+  * FP64 central differences (h = 1e-4, Richardson-extrapolated with h / 2) of the oracle's FP64
+    Taylor sum with the float traversal's acceptance decisions frozen -- the piecewise-smooth
+    function the adjoint differentiates -- on an open, inconsistently oriented soup (20 % of the
+    triangles deleted, 5 % flipped), 64 random vertices and 64 random queries;
+  * FP64 central differences of the exact winding number when every slot is descended;
+  * the library's Taylor gradient batch and smallgwn's own Taylor query gradient
+    (include/gwn/gwn_query.cuh:688-756) for dL/dq = g grad w.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import oracle
+import smallgwn_b200 as g
+from smallgwn_b200 import api, meshes
+
+pytestmark = pytest.mark.gpu
+
+H = 1e-4
+
+
+def setup(cuda, mesh, order, nq, seed, method=g.gwn_bvh_build_method.k_hploc):
+    geo = g.gwn_geometry_object()
+    assert g.gwn_upload_geometry(geo, mesh["x"], mesh["y"], mesh["z"], mesh["i0"], mesh["i1"], mesh["i2"]).is_ok()
+    bvh = g.gwn_bvh4_object()
+    assert g.gwn_build_bvh(geo, bvh, g.gwn_bvh_build_options(method=method)).is_ok()
+    mom = g.gwn_bvh4_moment_object(order)
+    assert g.gwn_refit_bvh_moment(order, bvh, mom).is_ok()
+    q = meshes.mixed_queries(mesh, nq, seed=seed)
+    w = np.random.default_rng(seed + 1).normal(size=nq).astype(np.float32)
+    return geo, bvh, mom, q, w
+
+
+def run_adjoint(cuda, order, geo, bvh, mom, q, w, beta, **kw):
+    d = [cuda.from_numpy(np.ascontiguousarray(v, np.float32)).cuda() for v in q]
+    out = cuda.empty_like(d[0])
+    st, saved = g.gwn_winding_taylor_forward(order, bvh, mom, *d, out, accuracy_scale=beta, **kw)
+    assert st.is_ok(), st.message
+    gout = cuda.from_numpy(w).cuda()
+    nv = geo.vertex_count()
+    dv =[cuda.empty(nv, device="cuda") for _ in range(3)]
+    dq = [cuda.empty(len(w), device="cuda") for _ in range(3)]
+    st = g.gwn_winding_taylor_backward(saved, geo, bvh, mom, gout, *dv, *dq)
+    assert st.is_ok(), st.message
+    assert api.sync_bvh_status(bvh).is_ok()
+    cuda.cuda.synchronize()
+    return (out.cpu().numpy(), np.stack([x.cpu().numpy() for x in dv], -1),
+            np.stack([x.cpu().numpy() for x in dq], -1), d)
+
+
+def richardson(f, h=H):
+    """Central difference with Richardson extrapolation: (4 D(h/2) - D(h)) / 3."""
+    d1 = (f(h) - f(-h)) / (2 * h)
+    d2 = (f(h / 2) - f(-h / 2)) / h
+    return (4 * d2 - d1) / 3
+
+
+def mesh_distance(mesh, q, chunk=128):
+    """Unsigned distance of each query to the mesh (closest point on a triangle by the Voronoi
+    region tests of Ericson, Real-Time Collision Detection, 5.1.5), brute force."""
+    V = np.stack([mesh["x"], mesh["y"], mesh["z"]], -1).astype(np.float64)
+    a, b, c = V[mesh["i0"]], V[mesh["i1"]], V[mesh["i2"]]
+    ab, ac = b - a, c - a
+    P = np.stack(q, -1).astype(np.float64)
+    out = np.empty(len(P))
+    dot = lambda u, v: np.einsum("...k,...k->...", u, v)  # noqa: E731
+    for s in range(0, len(P), chunk):
+        p = P[s:s + chunk, None, :]
+        ap, bp, cp = p - a, p - b, p - c
+        d1, d2, d3, d4, d5, d6 = dot(ab, ap), dot(ac, ap), dot(ab, bp), dot(ac, bp), dot(ab, cp), dot(ac, cp)
+        va, vb, vc = d3 * d6 - d5 * d4, d5 * d2 - d1 * d6, d1 * d4 - d3 * d2
+        with np.errstate(divide="ignore", invalid="ignore"):
+            t_ab = d1 / (d1 - d3)
+            t_ac = d2 / (d2 - d6)
+            t_bc = (d4 - d3) / ((d4 - d3) + (d5 - d6))
+            den = 1.0 / (va + vb + vc)
+        inner = a + ab * (vb * den)[..., None] + ac * (vc * den)[..., None]
+        conds = [(d1 <= 0) & (d2 <= 0), (d3 >= 0) & (d4 <= d3), (vc <= 0) & (d1 >= 0) & (d3 <= 0),
+                 (d6 >= 0) & (d5 <= d6), (vb <= 0) & (d2 >= 0) & (d6 <= 0),
+                 (va <= 0) & (d4 - d3 >= 0) & (d5 - d6 >= 0)]
+        choices = [np.broadcast_to(a, inner.shape), np.broadcast_to(b, inner.shape), a + ab * t_ab[..., None],
+                   np.broadcast_to(c, inner.shape), a + ac * t_ac[..., None], b + (c - b) * t_bc[..., None]]
+        closest = inner.copy()
+        for cond, ch in reversed(list(zip(conds, choices))):
+            closest = np.where(cond[..., None], ch, closest)
+        out[s:s + chunk] = np.sqrt(np.nanmin(dot(p - closest, p - closest), axis=1))
+    return out
+
+
+def rel_error(adj, fd):
+    """Per-sample relative error with a floor of 1 % of the largest derivative of the set."""
+    floor = 1e-2 * np.max(np.abs(fd))
+    return np.abs(adj - fd) / np.maximum(np.abs(fd), floor)
+
+
+@pytest.mark.parametrize("order", [0, 1])
+def test_adjoint_matches_fp64_central_differences(cuda, order):
+    mesh = meshes.soup_mesh(40, seed=13)
+    geo, bvh, mom, q, w = setup(cuda, mesh, order, 2000, seed=21)
+    # The winding number jumps by 1 across a triangle: a query within the stencil's reach of the
+    # surface (a vertex or the query moving by h) has no central difference there. Such queries
+    # keep g = 0 (vertex differences) and are not sampled (query differences).
+    far = mesh_distance(mesh, q) > 3 * H
+    w = np.where(far, w, 0.0).astype(np.float32)
+    beta = 2.0
+    _, dv, dq, _ = run_adjoint(cuda, order, geo, bvh, mom, q, w, beta)
+    h = api.bvh_host_arrays(bvh)
+    mh = api.moment_host_array(mom)
+    V = np.stack([mesh["x"], mesh["y"], mesh["z"]], -1).astype(np.float64)
+    q64 = [v.astype(np.float64) for v in q]
+    w64 = w.astype(np.float64)
+
+    def L(Vp, ev=q64, dec=q, gg=w64):
+        return float(gg @ oracle.taylor_frozen_f64(order, h["nodes"], mh, h["root_reference"], Vp, mesh,
+                                                   h["primitive_indices"], dec, ev, beta=beta))
+
+    rng = np.random.default_rng(5)
+    used = np.unique(np.concatenate([mesh["i0"], mesh["i1"], mesh["i2"]]))
+    verts = rng.choice(used, 64, replace=False)
+    fd_v = np.zeros((64, 3))
+    for i, v in enumerate(verts):
+        for k in range(3):
+            def f(step):
+                Vp = V.copy()
+                Vp[v, k] += step
+                return L(Vp)
+            fd_v[i, k] = richardson(f)
+    err_v = rel_error(dv[verts], fd_v)
+    assert err_v.max() <= 1e-3, (err_v.max(), np.abs(fd_v).max())
+
+    sel = rng.choice(np.flatnonzero(far), 64, replace=False)
+    dec = [x[sel] for x in q]
+    fd_q = np.zeros((64, 3))
+    for k in range(3):
+        def f(step):
+            ev = [x[sel].astype(np.float64) for x in q]
+            ev[k] = ev[k] + step
+            return w64[sel] * oracle.taylor_frozen_f64(order, h["nodes"], mh, h["root_reference"], V, mesh,
+                                                       h["primitive_indices"], dec, ev, beta=beta)
+        fd_q[:, k] = richardson(f)
+    err_q = rel_error(dq[sel], fd_q)
+    assert err_q.max() <= 1e-3, (err_q.max(), np.abs(fd_q).max())
+
+
+def test_adjoint_exact_limit_matches_exact_winding_differences(cuda):
+    """With every slot descended the function is the exact winding number: its FP64 central
+    differences (oracle brute force, no traversal involved) are an independent check."""
+    mesh = meshes.soup_mesh(16, seed=3)
+    geo, bvh, mom, q, w = setup(cuda, mesh, 1, 256, seed=31)
+    _, dv, dq, _ = run_adjoint(cuda, 1, geo, bvh, mom, q, w, 1e6)
+    q64 = [v.astype(np.float64) for v in q]
+    w64 = w.astype(np.float64)
+    rng = np.random.default_rng(8)
+    used = np.unique(np.concatenate([mesh["i0"], mesh["i1"], mesh["i2"]]))
+    verts = rng.choice(used, 16, replace=False)
+    fd = np.zeros((16, 3))
+    for i, v in enumerate(verts):
+        for k in range(3):
+            def f(step):
+                m = dict(mesh)
+                key = "xyz"[k]
+                m[key] = mesh[key].astype(np.float64).copy()
+                m[key][v] += step
+                return float(w64 @ oracle.exact_winding(m, *q64, fp64=True))
+            fd[i, k] = richardson(f)
+    assert rel_error(dv[verts], fd).max() <= 1e-3
+
+
+@pytest.mark.parametrize("order", [0, 1])
+def test_adjoint_query_gradient_is_the_taylor_gradient(cuda, order):
+    mesh = meshes.soup_mesh(40, seed=13)
+    geo, bvh, mom, q, w = setup(cuda, mesh, order, 4000, seed=41)
+    _, _, dq, d = run_adjoint(cuda, order, geo, bvh, mom, q, w, 2.0)
+    gr = [cuda.empty(len(w), device="cuda") for _ in range(3)]
+    assert g.gwn_compute_winding_gradient_taylor_batch(order, bvh, mom, *d, *gr, accuracy_scale=2.0).is_ok()
+    cuda.cuda.synchronize()
+    grad = np.stack([x.cpu().numpy() for x in gr], -1)
+    ref = w[:, None] * grad
+    # the same traversal and far field; the near field differentiates the atan2 form instead of
+    # the Biot-Savart form
+    scale = np.abs(ref).max()
+    assert np.quantile(np.abs(dq - ref), 0.999) <= 1e-4 * scale
+    if oracle.ref_lib() is not None:
+        R = oracle.Reference(mesh)
+        R.build(0, 8, 64)  # H-PLOC, radius 8, 64-bit codes: the tree of setup()
+        R.moments(order)
+        rg = R.taylor_gradient(order, *q, beta=2.0)
+        R.close()
+        # smallgwn's BVH is the same tree up to node numbering: same decisions up to rounding
+        diff = np.abs(dq - w[:, None] * rg)
+        assert np.mean(diff.max(axis=1) <= 1e-4 * scale) >= 0.999
+
+
+def test_adjoint_contract(cuda):
+    mesh = meshes.soup_mesh(16, seed=3)
+    geo, bvh, mom, q, w = setup(cuda, mesh, 1, 64, seed=2)
+    d = [cuda.from_numpy(np.ascontiguousarray(v, np.float32)).cuda() for v in q]
+    out = cuda.empty_like(d[0])
+    gout = cuda.from_numpy(w).cuda()
+    # order 2 has no adjoint
+    m2 = g.gwn_bvh4_moment_object(2)
+    assert g.gwn_refit_bvh_moment(2, bvh, m2).is_ok()
+    st, saved = g.gwn_winding_taylor_forward(2, bvh, m2, *d, out)
+    assert st.error == g.gwn_error.invalid_argument and saved is None
+    st, saved = g.gwn_winding_taylor_forward(1, bvh, mom, *d, out)
+    assert st.is_ok()
+    # skipping both outputs, or either, is allowed
+    assert g.gwn_winding_taylor_backward(saved, geo, bvh, mom, gout).is_ok()
+    dq = [cuda.empty(64, device="cuda") for _ in range(3)]
+    assert g.gwn_winding_taylor_backward(saved, None, bvh, mom, gout, None, None, None, *dq).is_ok()
+    # a partial output triple is refused
+    st = g.gwn_winding_taylor_backward(saved, geo, bvh, mom, gout, dq[0], None, None)
+    assert st.error == g.gwn_error.invalid_argument
+    # a refit after the forward pass invalidates its saved state
+    assert g.gwn_refit_bvh(geo, bvh).is_ok()
+    assert g.gwn_refit_bvh_moment(1, bvh, mom).is_ok()
+    st = g.gwn_winding_taylor_backward(saved, geo, bvh, mom, gout, None, None, None, *dq)
+    assert st.error == g.gwn_error.invalid_argument and "changed" in st.message
+    cuda.cuda.synchronize()
+
+
+def test_autograd_function_matches_the_c_abi_pair(cuda):
+    from smallgwn_b200.autograd import WindingField, winding_number
+
+    mesh = meshes.soup_mesh(24, seed=5)
+    faces = np.stack([mesh["i0"], mesh["i1"], mesh["i2"]], -1)
+    V = cuda.from_numpy(np.stack([mesh["x"], mesh["y"], mesh["z"]], -1).astype(np.float32)).cuda()
+    field = WindingField(V, faces, order=1, accuracy_scale=2.0)
+    q = meshes.mixed_queries(mesh, 1000, seed=6)
+    Q = cuda.from_numpy(np.stack(q, -1).astype(np.float32)).cuda()
+    wts = cuda.from_numpy(np.random.default_rng(1).normal(size=1000).astype(np.float32)).cuda()
+    Vp = V.clone().requires_grad_(True)
+    Qp = Q.clone().requires_grad_(True)
+    out = winding_number(Vp, Qp, field)
+    (wts * out).sum().backward()
+    ref_out, dv, dq, _ = run_adjoint(cuda, 1, field.geometry, field.bvh, field.moment, q, wts.cpu().numpy(), 2.0)
+    np.testing.assert_allclose(out.detach().cpu().numpy(), ref_out, atol=1e-6)
+    scale_v = np.abs(dv).max()
+    assert np.abs(Vp.grad.cpu().numpy() - dv).max() <= 1e-4 * scale_v
+    assert np.abs(Qp.grad.cpu().numpy() - dq).max() <= 1e-4 * np.abs(dq).max()

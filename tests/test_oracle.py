@@ -210,6 +210,27 @@ def test_far_field_order_progression(method):
     assert errs[1] < errs[0] and errs[2] < errs[1] and errs[2] < 2e-3
 
 
+@pytest.mark.parametrize("order", [0, 1])
+def test_frozen_fp64_taylor_is_the_float_traversal_in_fp64(order):
+    """The adjoint's checker: the FP64 Taylor sum with the float traversal's decisions equals the
+    float traversal up to FP32 rounding (the float near field loses up to ~1e-4 at a query by an
+    edge's line), and with every slot descended equals the FP64 exact sum."""
+    m = meshes.soup_mesh(24, seed=7)
+    b = oracle.build_lbvh(m)
+    mom = oracle.moments(order, b["nodes"], b["triangles"])
+    q = meshes.mixed_queries(m, 400, seed=9)
+    V = np.stack([m["x"], m["y"], m["z"]], -1).astype(np.float64)
+    q64 = [v.astype(np.float64) for v in q]
+    w32 = oracle.taylor(order, b["nodes"], mom, b["triangles"], b["root_reference"], *q, beta=2.0)
+    w64 = oracle.taylor_frozen_f64(order, b["nodes"], mom, b["root_reference"], V, m, b["sorted_ids"], q, q64,
+                                   beta=2.0)
+    d = np.abs(w64 - w32)
+    assert np.quantile(d, 0.99) < 2e-6 and d.max() < 5e-4, (np.quantile(d, 0.99), d.max())
+    full = oracle.taylor_frozen_f64(order, b["nodes"], mom, b["root_reference"], V, m, b["sorted_ids"], q, q64,
+                                    beta=1e6)
+    np.testing.assert_allclose(full, oracle.exact_winding(m, *q64, fp64=True), atol=1e-12)
+
+
 def test_leaf_root_build_record():
     b = oracle.build_lbvh(single_triangle())
     assert b["root_reference"] == VALID | (1 << 48)
