@@ -47,11 +47,16 @@ def parse() -> argparse.Namespace:
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="taylor", choices=["taylor", "adjoint", "precision", "exact"],
+                    help="taylor: the headline (1M-triangle sphere, 10M queries); adjoint: forward + backward "
+                         "on the 159k-triangle soup; precision: 8.4M-triangle sphere, 100M near-surface queries "
+                         "in 16M chunks; exact: brute-force exact batch on the small icosphere")
     ap.add_argument("--queries", type=int, default=N_QUERIES)
     ap.add_argument("--order", type=int, default=ORDER)
     ap.add_argument("--beta", type=float, default=BETA)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--profile", choices=["taylor", "taylor-plain", "taylor-thread", "build", "exact"], default=None,
+    ap.add_argument("--profile", choices=["taylor", "taylor-plain", "taylor-thread", "build", "exact", "adjoint"],
+                    default=None,
                     help="run one small workload for a profiler (no JSON): 2 launches of the kernel")
     return ap.parse_args()
 
@@ -67,6 +72,28 @@ def run_profile(args) -> None:
     from smallgwn_b200 import api, meshes
 
     stream = torch.cuda.current_stream()
+    if args.profile == "adjoint":
+        # forward + backward (order 1) on the 159k-triangle soup, twice
+        mesh = meshes.soup_mesh(316, seed=3)
+        q = meshes.mixed_queries(mesh, args.queries, seed=3)
+        geo = g.gwn_geometry_object()
+        assert g.gwn_upload_geometry(geo, mesh["x"], mesh["y"], mesh["z"], mesh["i0"], mesh["i1"], mesh["i2"]).is_ok()
+        bvh = g.gwn_bvh4_object()
+        assert g.gwn_build_bvh(geo, bvh, g.gwn_bvh_build_options(method=0, hploc_search_radius=8)).is_ok()
+        mom = g.gwn_bvh4_moment_object(1)
+        assert g.gwn_refit_bvh_moment(1, bvh, mom).is_ok()
+        dq = [torch.from_numpy(v).to("cuda") for v in q]
+        gout = torch.from_numpy(np.random.default_rng(3).normal(size=len(q[0])).astype(np.float32)).cuda()
+        out = torch.empty_like(dq[0])
+        dV = [torch.empty(geo.vertex_count(), device="cuda") for _ in range(3)]
+        dQ = [torch.empty_like(dq[0]) for _ in range(3)]
+        for _ in range(2):
+            st, saved = g.gwn_winding_taylor_forward(1, bvh, mom, *dq, out, accuracy_scale=2.0, stream=stream)
+            assert st.is_ok(), st.message
+            assert g.gwn_winding_taylor_backward(saved, geo, bvh, mom, gout, *dV, *dQ, stream=stream).is_ok()
+        torch.cuda.synchronize()
+        print("profile adjoint ok")
+        return
     if args.profile == "exact":
         mesh = meshes.small_mesh()
         q = meshes.small_queries(100_000)
@@ -274,6 +301,320 @@ def config_dict(args, mesh) -> dict:
             "l2": "flushed (256 MiB write) between timed steps", "parallelism": f"replicas x{args.gpus}"}
 
 
+def timed_steps(fn, steps: int, warmup: int, stream, flush) -> list[float]:
+    """Per-step device times (ms) of fn() on `stream` after `warmup` untimed calls; L2 flushed
+    before every timed step."""
+    import torch
+
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    for e0, e1 in ev:
+        flush.fill_(1)
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+    torch.cuda.synchronize()
+    return [a.elapsed_time(b) for a, b in ev]
+
+
+def run_adjoint_workload(args) -> None:
+    """Differentiation workload: UV 316 x 316 displaced sphere with 20 % of the triangles deleted
+    and 5 % flipped (seed 3), 1M mixed queries, upstream weights N(0, 1), Taylor order 1, accuracy
+    scale 2. A step is the forward pass plus the backward pass (dL/dV and dL/dq) on device-resident
+    data. The adjoint is checked against FP64 central differences (Richardson) of the oracle's
+    frozen-decision FP64 Taylor sum on 64 vertices and 64 queries, for losses restricted to 4096
+    queries away from the surface: h = 1e-4 with queries farther than 30 h, and h = 1e-6 with
+    queries farther than 100 h (which keeps most near-surface queries)."""
+    import torch
+
+    import oracle
+    import smallgwn_b200 as g
+    from smallgwn_b200 import api, meshes
+
+    n = args.queries if args.queries != N_QUERIES else 1_000_000
+    order, beta, h = 1, 2.0, 1e-4
+    mesh = meshes.soup_mesh(316, seed=3)
+    q = meshes.mixed_queries(mesh, n, seed=3)
+    w = np.random.default_rng(3).normal(size=n).astype(np.float32)
+    stream = torch.cuda.current_stream()
+    geo = g.gwn_geometry_object()
+    assert g.gwn_upload_geometry(geo, mesh["x"], mesh["y"], mesh["z"], mesh["i0"], mesh["i1"], mesh["i2"]).is_ok()
+    bvh = g.gwn_bvh4_object()
+    assert g.gwn_build_bvh(geo, bvh, g.gwn_bvh_build_options(method=0, hploc_search_radius=8)).is_ok()
+    mom = g.gwn_bvh4_moment_object(order)
+    assert g.gwn_refit_bvh_moment(order, bvh, mom).is_ok()
+    nv = geo.vertex_count()
+    dq = [torch.from_numpy(v).cuda() for v in q]
+    gout = torch.from_numpy(w).cuda()
+    out = torch.empty(n, device="cuda")
+    dV = [torch.empty(nv, device="cuda") for _ in range(3)]
+    dQ = [torch.empty(n, device="cuda") for _ in range(3)]
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    state = {}
+
+    def fwd():
+        st, state["saved"] = g.gwn_winding_taylor_forward(order, bvh, mom, *dq, out, accuracy_scale=beta, stream=stream)
+        assert st.is_ok(), st.message
+
+    def bwd():
+        st = g.gwn_winding_taylor_backward(state["saved"], geo, bvh, mom, gout, *dV, *dQ, stream=stream)
+        assert st.is_ok(), st.message
+
+    def step():
+        fwd()
+        bwd()
+
+    t_step = timed_steps(step, args.steps, args.warmup, stream, flush)
+    t_fwd = timed_steps(fwd, 3, 1, stream, flush)
+    t_bwd = timed_steps(bwd, 3, 1, stream, flush)
+    assert api.sync_bvh_status(bvh).is_ok()
+
+    # ---- FD checks on losses restricted to 4096 queries away from the surface (untimed) ----
+    dist = oracle.mesh_distance(mesh, *[x[:8000] for x in q])
+    hb, mh = api.bvh_host_arrays(bvh), api.moment_host_array(mom)
+    V = np.stack([mesh["x"], mesh["y"], mesh["z"]], -1).astype(np.float64)
+    used = np.unique(np.concatenate([mesh["i0"], mesh["i1"], mesh["i2"]]))
+
+    def fd_check(step: float, clearance: float) -> dict:
+        """Central differences (Richardson with step and step / 2) of the oracle's frozen-decision
+        FP64 sum for the loss over queries farther than clearance * step from the surface (the
+        extrapolation error grows like 120 (step / distance)^4), against the adjoint of that loss."""
+        far = np.flatnonzero(dist > clearance * step)[:4096]
+        ws = np.zeros(n, np.float32)
+        ws[far] = w[far]
+        st = g.gwn_winding_taylor_backward(state["saved"], geo, bvh, mom, torch.from_numpy(ws).cuda(), *dV, *dQ,
+                                           stream=stream)
+        assert st.is_ok(), st.message
+        torch.cuda.synchronize()
+        adj_v = torch.stack(dV, -1).cpu().numpy()
+        adj_q = torch.stack(dQ, -1).cpu().numpy()
+        dec = [x[far] for x in q]
+        ev0 = [x[far].astype(np.float64) for x in q]
+        wf = w[far].astype(np.float64)
+
+        def frozen(Vp, ev, d=dec):
+            return oracle.taylor_frozen_f64(order, hb["nodes"], mh, hb["root_reference"], Vp, mesh,
+                                            hb["primitive_indices"], d, ev, beta=beta)
+
+        def richardson(f):
+            return (4 * (f(step / 2) - f(-step / 2)) / step - (f(step) - f(-step)) / (2 * step)) / 3
+
+        rng = np.random.default_rng(5)
+        verts = rng.choice(used, 64, replace=False)
+        fd_v = np.zeros((64, 3))
+        for i, v in enumerate(verts):
+            for k in range(3):
+                def fv(s, v=v, k=k):
+                    Vp = V.copy()
+                    Vp[v, k] += s
+                    return float(wf @ frozen(Vp, ev0))
+                fd_v[i, k] = richardson(fv)
+        sel = rng.choice(far.size, 64, replace=False)
+        fd_q = np.zeros((64, 3))
+        for k in range(3):
+            def fq(s, k=k):
+                ev = [x[sel].copy() for x in ev0]
+                ev[k] += s
+                return wf[sel] * frozen(V, ev, [x[sel] for x in dec])
+            fd_q[:, k] = richardson(fq)
+
+        def errs(a, f):
+            return {"norm_rel": float(np.linalg.norm(a - f) / np.linalg.norm(f)),
+                    "max_rel_floor_1pct": float(np.max(np.abs(a - f) / np.maximum(np.abs(f), 1e-2 * np.abs(f).max())))}
+
+        near = int(np.count_nonzero(dist[far] < 1e-2))
+        return {"h": step, "clearance": clearance * step, "richardson": True, "vertices": 64, "queries": 64,
+                "loss_queries": int(far.size), "loss_queries_within_1e-2": near,
+                "dV": errs(adj_v[verts], fd_v), "dq": errs(adj_q[far][sel], fd_q)}
+
+    checks = [fd_check(h, 30.0), fd_check(1e-6, 100.0)]
+    ms = float(np.mean(t_step))
+    line = {
+        "metric": "Adjoint (forward + backward) queries/s, order 1, 159k-triangle open soup",
+        "value": n / (ms / 1e3), "unit": "queries/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": "UV 316x316 displaced sphere, 20% of triangles deleted, 5% flipped (seed 3), "
+                               f"{n} mixed queries, g ~ N(0,1)", "triangles": int(mesh["i0"].size),
+                   "vertices": int(nv), "taylor_order": order, "accuracy_scale": beta,
+                   "forward_ms": float(np.mean(t_fwd)), "backward_ms": float(np.mean(t_bwd)),
+                   "l2": "flushed (256 MiB write) between timed steps"},
+        "fd_checks": checks,
+        "gpu_launches": None,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_precision_workload(args) -> None:
+    """Precision stress: UV 2896 x 1448 displaced sphere (8,381,024 triangles, seed 5), 100M
+    queries at surface samples offset along the normal by a log-uniform magnitude in [1e-6, 1e-1]
+    of random sign, streamed in 16M chunks (sampled on the device), Taylor order 2 at accuracy
+    scale 3.5 with the compensated near field. Errors on a 20k-query subset of the first chunk
+    against the FP64 exact winding number, beside the plain FP32 Taylor form, the plain FP32 sum
+    over every triangle (full descent) and the exact batch."""
+    import torch
+
+    import smallgwn_b200 as g
+    from smallgwn_b200 import api, meshes
+
+    total = args.queries if args.queries != N_QUERIES else 100_000_000
+    chunk = 16_000_000
+    order, beta, sub = 2, BETA, 20_000
+    mesh = meshes.sphere_mesh(2896, 1448, seed=5)
+    geo = g.gwn_geometry_object()
+    assert g.gwn_upload_geometry(geo, mesh["x"], mesh["y"], mesh["z"], mesh["i0"], mesh["i1"], mesh["i2"]).is_ok()
+    bvh = g.gwn_bvh4_object()
+    opts = g.gwn_bvh_build_options(method=0, hploc_search_radius=8)
+    build_ms = []
+    for _ in range(3):
+        t0 = time.perf_counter()
+        assert g.gwn_build_bvh(geo, bvh, opts).is_ok()
+        torch.cuda.synchronize()
+        build_ms.append((time.perf_counter() - t0) * 1e3)
+    mom = g.gwn_bvh4_moment_object(order)
+    assert g.gwn_refit_bvh_moment(order, bvh, mom).is_ok()
+    stream = torch.cuda.current_stream()
+
+    # device sampler: uniform non-degenerate triangle, uniform barycentric point, signed log offset
+    a, b, c, nrm, area2 = meshes.triangle_normals(mesh)
+    good = np.flatnonzero(area2 > 0)
+    A = torch.from_numpy(a[good].astype(np.float32)).cuda()
+    AB = torch.from_numpy((b - a)[good].astype(np.float32)).cuda()
+    AC = torch.from_numpy((c - a)[good].astype(np.float32)).cuda()
+    U = torch.from_numpy((nrm[good] / area2[good, None]).astype(np.float32)).cuda()
+    gen = torch.Generator(device="cuda")
+
+    def sample(k: int, m: int):
+        gen.manual_seed(5_000 + k)
+        t = torch.randint(0, A.shape[0], (m,), device="cuda", generator=gen)
+        uv = torch.rand(m, 2, device="cuda", generator=gen)
+        flip = uv.sum(1) > 1
+        uv[flip] = 1 - uv[flip]
+        mag = torch.exp(torch.empty(m, device="cuda").uniform_(np.log(1e-6), np.log(1e-1), generator=gen))
+        off = mag * torch.where(torch.rand(m, device="cuda", generator=gen) < 0.5, -1.0, 1.0)
+        p = A[t] + uv[:, :1] * AB[t] + uv[:, 1:] * AC[t] + off[:, None] * U[t]
+        return [p[:, k].contiguous() for k in range(3)], off
+
+    out = torch.empty(chunk, device="cuda")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    comp = g.near_precision.compensated
+    times, fp64_pairs, done = [], 0, 0
+    first = None
+    k = 0
+    while done < total:
+        m = min(chunk, total - done)
+        qs, off = sample(k, m)
+        if first is None:
+            first = ([x[:sub].clone() for x in qs], off[:sub].clone())
+        o = out[:m]
+
+        def run(qs=qs, o=o):
+            st = g.gwn_compute_winding_number_taylor_batch(order, bvh, mom, *qs, o, accuracy_scale=beta,
+                                                           stream=stream, precision=comp)
+            assert st.is_ok(), st.message
+
+        times += timed_steps(run, 1, 1 if k == 0 else 0, stream, flush)
+        fp64_pairs += api.fp64_fallback_count(bvh, stream)
+        done += m
+        k += 1
+    qsub, osub = first
+    ref64 = torch.empty(sub, dtype=torch.float64, device="cuda")
+    assert api.exact_winding_fp64(geo, *qsub, ref64, stream).is_ok()
+    res = {}
+    forms = {"taylor_compensated": (beta, comp), "taylor_plain": (beta, g.near_precision.plain),
+             "full_descent_plain_fp32": (1e6, g.near_precision.plain),
+             "full_descent_compensated": (1e6, comp)}
+    osub_np = osub.cpu().numpy()
+    bins = [1e-6, 1e-5, 1e-4, 1e-3, 1e-2, 1e-1]
+    o2 = torch.empty(sub, device="cuda")
+    for name, (bt, prec) in forms.items():
+        assert g.gwn_compute_winding_number_taylor_batch(order, bvh, mom, *qsub, o2, accuracy_scale=bt,
+                                                         stream=stream, precision=prec).is_ok()
+        torch.cuda.synchronize()
+        err = (o2.double() - ref64).abs().cpu().numpy()
+        per = {}
+        for lo, hi in zip(bins[:-1], bins[1:]):
+            msk = (np.abs(osub_np) >= lo) & (np.abs(osub_np) < hi)
+            per[f"{lo:g}-{hi:g}"] = {"max": float(err[msk].max()), "p99": float(np.quantile(err[msk], 0.99))}
+        res[name] = {"max": float(err.max()), "p99": float(np.quantile(err, 0.99)), "by_offset": per}
+    assert g.gwn_compute_winding_number_exact_batch(bvh, *qsub, o2, stream).is_ok()
+    torch.cuda.synchronize()
+    err = (o2.double() - ref64).abs().cpu().numpy()
+    res["exact_batch"] = {"max": float(err.max()), "p99": float(np.quantile(err, 0.99))}
+    stats = [torch.empty(sub, dtype=torch.int32, device="cuda") for _ in range(3)]
+    assert api.taylor_traversal_stats(bvh, mom, *qsub, *stats, accuracy_scale=beta, stream=stream).is_ok()
+    assert g.gwn_compute_winding_number_taylor_batch(order, bvh, mom, *qsub, o2, accuracy_scale=beta, stream=stream,
+                                                     precision=comp).is_ok()
+    sub_fp64 = api.fp64_fallback_count(bvh, stream)
+    near_pairs = float(stats[2].double().sum().item())
+    ms = float(np.sum(times))
+    line = {
+        "metric": "Precision stress: Taylor winding queries/s at 8.4M tris (compensated FP32, FP64 on flagged pairs)",
+        "value": total / (ms / 1e3), "unit": "queries/s", "n_gpus": 1, "steps": k, "warmup": 1,
+        "ms_per_step": ms / k, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": "UV 2896x1448 displaced sphere (seed 5), near-surface queries with offsets "
+                               "log-uniform in [1e-6, 1e-1] of either sign", "triangles": int(mesh["i0"].size),
+                   "queries": total, "chunk": chunk, "taylor_order": order, "accuracy_scale": beta,
+                   "bvh_nodes": int(bvh.accessor().node_count), "build_ms_hploc": build_ms,
+                   "l2": "flushed (256 MiB write) before every chunk"},
+        "errors_vs_fp64": res, "error_subset": sub,
+        "fp64_pairs": {"all_chunks": int(fp64_pairs), "subset": int(sub_fp64),
+                       "subset_near_field_pairs": near_pairs,
+                       "subset_fraction": sub_fp64 / max(near_pairs, 1.0)},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_exact_workload(args) -> None:
+    """Plain exact winding number, small: icosphere level 4 (5,120 triangles, radial noise seed 0),
+    100k queries uniform in [-1.5, 1.5]^3 (seed 1), LBVH, exact batch; the oracle's FP32 brute force
+    on the host threads beside it (a restatement of smallgwn's CPU reference)."""
+    import torch
+
+    import oracle
+    import smallgwn_b200 as g
+    from smallgwn_b200 import meshes
+
+    mesh = meshes.small_mesh()
+    q = meshes.small_queries(100_000)
+    geo = g.gwn_geometry_object()
+    assert g.gwn_upload_geometry(geo, mesh["x"], mesh["y"], mesh["z"], mesh["i0"], mesh["i1"], mesh["i2"]).is_ok()
+    bvh = g.gwn_bvh4_object()
+    assert g.gwn_build_bvh(geo, bvh, g.gwn_bvh_build_options(method=1)).is_ok()
+    stream = torch.cuda.current_stream()
+    dq = [torch.from_numpy(v).cuda() for v in q]
+    out = torch.empty(dq[0].numel(), device="cuda")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+    def run():
+        assert g.gwn_compute_winding_number_exact_batch(bvh, *dq, out, stream).is_ok()
+
+    t = timed_steps(run, args.steps, args.warmup, stream, flush)
+    ms = float(np.mean(t))
+    nq, nt = dq[0].numel(), int(mesh["i0"].size)
+    ref = oracle.exact_winding(mesh, *q)
+    err = float(np.abs(out.cpu().numpy() - ref).max())
+    threads = oracle.max_threads()
+    t0 = time.perf_counter()
+    m = 10_000
+    oracle.exact_winding(mesh, *[x[:m] for x in q], threads=threads)
+    cpu_s = time.perf_counter() - t0
+    line = {
+        "metric": "Exact winding evaluations/s (query x triangle), small icosphere",
+        "value": nq * nt / (ms / 1e3), "unit": "evaluations/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "icosphere L4 (5,120 tris), 100k queries in [-1.5,1.5]^3", "builder": "lbvh",
+                   "max_abs_diff_vs_oracle_fp32": err},
+        "cpu_baseline": {"value": m * nt / cpu_s, "unit": "evaluations/s", "cores": threads, "kind": "port",
+                         "sample": f"{m} of the queries against all triangles"},
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main() -> None:
     args = parse()
     if args.profile is not None:
@@ -281,6 +622,10 @@ def main() -> None:
         return
     if args.impl == "reference":
         run_reference_arm(args)
+        return
+    if args.workload != "taylor":
+        {"adjoint": run_adjoint_workload, "precision": run_precision_workload,
+         "exact": run_exact_workload}[args.workload](args)
         return
     import torch
 

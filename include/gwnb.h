@@ -347,6 +347,51 @@ GWNB_API int gwnb_winding_taylor_backward_f32(const gwnb_taylor_saved_f32 *saved
                                               float *grad_vertex_y, float *grad_vertex_z, float *grad_query_x,
                                               float *grad_query_y, float *grad_query_z, gwnb_stream_t stream);
 
+/* ---- batched dynamic meshes (no smallgwn counterpart) ----------------------------------------- */
+
+/* Many meshes whose vertices move every frame (topology fixed): one frame refits every BVH and its
+ * moments and evaluates every mesh's Taylor queries in three persistent launches, with no host
+ * synchronization, so a frame can be captured in a CUDA graph. */
+typedef struct gwnb_batch gwnb_batch;
+
+typedef struct gwnb_batch_mesh_f32 {
+    gwnb_geometry_f32 geometry; /* view of the mesh (positions read by every frame's refit)      */
+    gwnb_bvh4_f32 *bvh;         /* built by this library from `geometry`; refit in place          */
+    gwnb_moment4_f32 *moment;   /* moments of `bvh`; refit in place (all meshes share one order)  */
+    const float *query_x;       /* this mesh's queries (fixed for the batch; read every frame)    */
+    const float *query_y;
+    const float *query_z;
+    float *output;              /* winding numbers, query_count floats                            */
+    uint64_t query_count;
+} gwnb_batch_mesh_f32;
+
+/* Launch shape of a frame, as chosen by gwnb_batch_tune_f32. */
+typedef struct gwnb_batch_tuning {
+    int refit_block;  /* threads per block of the refit launches                                  */
+    int query_block;  /* threads per block of the query launch (multiple of 32, at most 256)      */
+    int per_thread;   /* 0: 32 queries per warp walk one traversal; 1: one traversal per thread   */
+    int sorted;       /* 1: traverse each mesh's queries in Morton order (computed at creation)   */
+    int grid_scale;   /* persistent grids of SMs x grid_scale blocks                              */
+    float frame_ms;   /* measured frame time of this shape (output of tuning)                     */
+} gwnb_batch_tuning;
+
+/* Creates a batch over `mesh_count` meshes (copies the descriptors; the pointed-to objects must
+ * outlive the batch). Computes each mesh's query order. While the batch exists its frames refit the
+ * BVHs and moments in place and leave their revisions unchanged. */
+GWNB_API int gwnb_batch_create_f32(const gwnb_batch_mesh_f32 *meshes, uint32_t mesh_count, float accuracy_scale,
+                                   const gwnb_taylor_options *options, gwnb_batch **batch, gwnb_stream_t stream);
+/* Times `repetitions` frames of every candidate launch shape on `stream` and keeps the fastest
+ * (written to `chosen` when non-NULL). Frames run: the meshes are refit and queried. */
+GWNB_API int gwnb_batch_tune_f32(gwnb_batch *batch, int repetitions, gwnb_batch_tuning *chosen, gwnb_stream_t stream);
+GWNB_API int gwnb_batch_set_tuning_f32(gwnb_batch *batch, const gwnb_batch_tuning *tuning);
+/* Enqueues one frame (refit, moment refit, queries) on `stream`; asynchronous and capturable once
+ * a frame or a tuning has run outside capture. */
+GWNB_API int gwnb_batch_frame_f32(gwnb_batch *batch, gwnb_stream_t stream);
+/* Synchronizes `stream` and reports device-side errors of any mesh (index or topology faults,
+ * stack overflow) as GWNB_INTERNAL_ERROR. */
+GWNB_API int gwnb_batch_sync_f32(gwnb_batch *batch, gwnb_stream_t stream);
+GWNB_API int gwnb_batch_release_f32(gwnb_batch *batch, gwnb_stream_t stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -228,6 +228,19 @@ def taylor_frozen_f64(order: int, nodes: np.ndarray, mom: np.ndarray, root_ref: 
     return out
 
 
+def mesh_distance(mesh: dict, qx, qy, qz, threads: int = 0) -> np.ndarray:
+    """Unsigned distance of each point to the mesh (FP64 brute force)."""
+    threads = threads or max_threads()
+    v = [np.ascontiguousarray(mesh[k], np.float64) for k in "xyz"]
+    i0, i1, i2 = _u32(mesh["i0"]), _u32(mesh["i1"]), _u32(mesh["i2"])
+    q = [np.ascontiguousarray(x, np.float64) for x in (qx, qy, qz)]
+    out = np.empty(q[0].size, np.float64)
+    lib().oracle_mesh_distance_f64(_p(v[0]), _p(v[1]), _p(v[2]), C.c_uint64(v[0].size), _p(i0), _p(i1), _p(i2),
+                                   C.c_uint64(i0.size), _p(q[0]), _p(q[1]), _p(q[2]), C.c_uint64(q[0].size), _p(out),
+                                   C.c_int(threads))
+    return out
+
+
 def build_lbvh(mesh: dict, bits: int = 64) -> dict:
     """Full CPU pipeline: Morton, stable sort, Karras, bounds, BVH4 collapse, triangle records."""
     aabbs, codes, scene = morton(mesh, bits)

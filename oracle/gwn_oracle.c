@@ -990,6 +990,83 @@ int oracle_max_threads(void) {
 }
 
 /* ---------------------------------------------------------------------------------------------- */
+/* Unsigned point-to-mesh distance (brute force, FP64): the closest point on each triangle by the  */
+/* Voronoi-region tests of Ericson, Real-Time Collision Detection (2005), section 5.1.5. Used by   */
+/* the adjoint checks to keep central-difference stencils away from the surface, where the winding */
+/* number jumps.                                                                                  */
+
+static double point_triangle_dist2(const double p[3], const double a[3], const double b[3], const double c[3]) {
+    double ab[3], ac[3], ap[3], bp[3], cp[3], q[3];
+    for (int k = 0; k < 3; ++k) {
+        ab[k] = b[k] - a[k];
+        ac[k] = c[k] - a[k];
+        ap[k] = p[k] - a[k];
+        bp[k] = p[k] - b[k];
+        cp[k] = p[k] - c[k];
+    }
+#define DOT3(u, v) ((u)[0] * (v)[0] + (u)[1] * (v)[1] + (u)[2] * (v)[2])
+    double d1 = DOT3(ab, ap), d2 = DOT3(ac, ap);
+    if (d1 <= 0.0 && d2 <= 0.0)
+        return DOT3(ap, ap);
+    double d3 = DOT3(ab, bp), d4 = DOT3(ac, bp);
+    if (d3 >= 0.0 && d4 <= d3)
+        return DOT3(bp, bp);
+    double vc = d1 * d4 - d3 * d2;
+    if (vc <= 0.0 && d1 >= 0.0 && d3 <= 0.0) {
+        double v = d1 / (d1 - d3);
+        for (int k = 0; k < 3; ++k)
+            q[k] = p[k] - (a[k] + v * ab[k]);
+        return DOT3(q, q);
+    }
+    double d5 = DOT3(ab, cp), d6 = DOT3(ac, cp);
+    if (d6 >= 0.0 && d5 <= d6)
+        return DOT3(cp, cp);
+    double vb = d5 * d2 - d1 * d6;
+    if (vb <= 0.0 && d2 >= 0.0 && d6 <= 0.0) {
+        double w = d2 / (d2 - d6);
+        for (int k = 0; k < 3; ++k)
+            q[k] = p[k] - (a[k] + w * ac[k]);
+        return DOT3(q, q);
+    }
+    double va = d3 * d6 - d5 * d4;
+    if (va <= 0.0 && (d4 - d3) >= 0.0 && (d5 - d6) >= 0.0) {
+        double w = (d4 - d3) / ((d4 - d3) + (d5 - d6));
+        for (int k = 0; k < 3; ++k)
+            q[k] = p[k] - (b[k] + w * (c[k] - b[k]));
+        return DOT3(q, q);
+    }
+    double den = va + vb + vc;
+    if (!(den != 0.0)) /* degenerate triangle: nearest of its vertices */
+        return fmin(DOT3(ap, ap), fmin(DOT3(bp, bp), DOT3(cp, cp)));
+    double v = vb / den, w = vc / den;
+    for (int k = 0; k < 3; ++k)
+        q[k] = p[k] - (a[k] + ab[k] * v + ac[k] * w);
+    return DOT3(q, q);
+#undef DOT3
+}
+
+void oracle_mesh_distance_f64(const double *vx, const double *vy, const double *vz, uint64_t nv, const uint32_t *i0,
+                              const uint32_t *i1, const uint32_t *i2, uint64_t nt, const double *qx, const double *qy,
+                              const double *qz, uint64_t nq, double *out, int threads) {
+    (void)threads;
+#pragma omp parallel for schedule(dynamic, 16) num_threads(threads > 0 ? threads : 1)
+    for (int64_t q = 0; q < (int64_t)nq; ++q) {
+        double p[3] = {qx[q], qy[q], qz[q]};
+        double best = INFINITY;
+        for (uint64_t t = 0; t < nt; ++t) {
+            uint32_t ia = i0[t], ib = i1[t], ic = i2[t];
+            if (ia >= nv || ib >= nv || ic >= nv)
+                continue;
+            double a[3] = {vx[ia], vy[ia], vz[ia]}, b[3] = {vx[ib], vy[ib], vz[ib]}, c[3] = {vx[ic], vy[ic], vz[ic]};
+            double d2 = point_triangle_dist2(p, a, b, c);
+            if (d2 < best)
+                best = d2;
+        }
+        out[q] = sqrt(best);
+    }
+}
+
+/* ---------------------------------------------------------------------------------------------- */
 /* FP64 Taylor winding numbers (orders 0 and 1) with frozen acceptance decisions: the checker of   */
 /* the adjoint. The decisions are those of the float traversal of taylor_one (the test of          */
 /* detail/gwn_query_winding_impl.cuh:168-240 on the float moment nodes at the float decision       */

@@ -5,6 +5,7 @@ The product is libgwnb.so (CUDA kernels + the C ABI of include/gwnb.h). This pac
 (`api.py`) for tests and benchmarks. `meshes.py` generates the seeded synthetic workloads.
 """
 from .api import (  # noqa: F401
+    gwn_batch,
     gwn_bvh4_moment_object,
     gwn_bvh4_object,
     gwn_bvh_build_method,
@@ -15,6 +16,7 @@ from .api import (  # noqa: F401
     gwn_compute_winding_number_taylor_batch,
     gwn_error,
     gwn_geometry_object,
+    gwn_geometry_view,
     gwn_query_batch_config,
     gwn_refit_bvh,
     gwn_refit_bvh_moment,

@@ -97,6 +97,30 @@ class taylor_saved_f32(C.Structure):
     ]
 
 
+class batch_mesh_f32(C.Structure):
+    _fields_ = [
+        ("geometry", geometry_f32),
+        ("bvh", C.POINTER(bvh4_f32)),
+        ("moment", C.POINTER(moment4_f32)),
+        ("query_x", C.c_void_p),
+        ("query_y", C.c_void_p),
+        ("query_z", C.c_void_p),
+        ("output", C.c_void_p),
+        ("query_count", C.c_uint64),
+    ]
+
+
+class batch_tuning(C.Structure):
+    _fields_ = [
+        ("refit_block", C.c_int),
+        ("query_block", C.c_int),
+        ("per_thread", C.c_int),
+        ("sorted", C.c_int),
+        ("grid_scale", C.c_int),
+        ("frame_ms", C.c_float),
+    ]
+
+
 class binary_node(C.Structure):
     _fields_ = [(n, C.c_uint32) for n in ("left_index", "left_kind", "right_index", "right_kind")]
 
@@ -149,6 +173,13 @@ SIGNATURES: dict[str, tuple] = {
     "gwnb_winding_taylor_backward_f32": (
         I, [C.POINTER(taylor_saved_f32), C.POINTER(geometry_f32), C.POINTER(bvh4_f32), C.POINTER(moment4_f32), P,
             P, P, P, P, P, P, P]),
+    "gwnb_batch_create_f32": (
+        I, [C.POINTER(batch_mesh_f32), C.c_uint32, F, C.POINTER(taylor_options), C.POINTER(P), P]),
+    "gwnb_batch_tune_f32": (I, [P, I, C.POINTER(batch_tuning), P]),
+    "gwnb_batch_set_tuning_f32": (I, [P, C.POINTER(batch_tuning)]),
+    "gwnb_batch_frame_f32": (I, [P, P]),
+    "gwnb_batch_sync_f32": (I, [P, P]),
+    "gwnb_batch_release_f32": (I, [P, P]),
 }
 
 _lib: C.CDLL | None = None

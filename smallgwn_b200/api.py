@@ -157,6 +157,28 @@ class gwn_geometry_object(_stream_mixin):
             pass
 
 
+class gwn_geometry_view:
+    """Non-owning geometry over caller device buffers (torch CUDA tensors: float32 x, y, z and
+    int32/uint32 i0, i1, i2), e.g. slices of one shared vertex buffer; accepted wherever a
+    gwn_geometry_object is. The tensors are held, so they outlive the view."""
+
+    def __init__(self, x, y, z, i0, i1, i2) -> None:
+        n, t = _numel(x), _numel(i0)
+        if not (_numel(y) == n == _numel(z)) or not (_numel(i1) == t == _numel(i2)):
+            raise ValueError("geometry view: SoA spans must have identical lengths")
+        self._keep = (x, y, z, i0, i1, i2)
+        self._view = _lib.geometry_f32(_ptr(x), _ptr(y), _ptr(z), n, _ptr(i0), _ptr(i1), _ptr(i2), t)
+
+    def accessor(self) -> _lib.geometry_f32:
+        return self._view
+
+    def vertex_count(self) -> int:
+        return int(self._view.vertex_count)
+
+    def triangle_count(self) -> int:
+        return int(self._view.triangle_count)
+
+
 def gwn_upload_geometry(obj: gwn_geometry_object, x, y, z, i0, i1, i2, stream=None) -> gwn_status:
     """Upload host SoA positions and indices; replaces ``obj`` only on success."""
     lib = _lib.load()
@@ -457,6 +479,64 @@ def gwn_winding_taylor_backward(saved: gwn_taylor_saved, geometry: gwn_geometry_
         C.byref(saved._view), geo, C.byref(bvh._view), C.byref(moment._view), _ptr(grad_out), _ptr(dvx), _ptr(dvy),
         _ptr(dvz), _ptr(dqx), _ptr(dqy), _ptr(dqz), _stream(stream))
     return _status(rc)
+
+
+# ---- batched dynamic meshes ---------------------------------------------------------------------------
+
+class gwn_batch:
+    """Many meshes refit and queried per frame in three persistent launches (gwnb_batch_*).
+
+    ``meshes`` is a list of (geometry, bvh, moment, qx, qy, qz, out): each BVH built from its
+    geometry, each moment object refit for it (one Taylor order for all), queries and outputs CUDA
+    tensors. The objects and tensors must outlive the batch; frames refit the BVHs and moments in
+    place. ``frame()`` is asynchronous and capturable in a CUDA graph once a frame or a tuning has
+    run outside capture."""
+
+    def __init__(self, meshes, accuracy_scale: float = 2.0, stream=None, precision: int = near_precision.plain,
+                 fp64_threshold: float = FP64_THRESHOLD) -> None:
+        self._handle = C.c_void_p()
+        self._keep = list(meshes)
+        arr = (_lib.batch_mesh_f32 * len(meshes))()
+        for i, (geo, bvh, mom, qx, qy, qz, out) in enumerate(meshes):
+            if _numel(out) != _numel(qx) or _numel(qy) != _numel(qx) or _numel(qz) != _numel(qx):
+                raise ValueError(f"batch mesh {i}: query/output spans must have identical lengths")
+            arr[i] = _lib.batch_mesh_f32(geo._view, C.pointer(bvh._view), C.pointer(mom._view), _ptr(qx), _ptr(qy),
+                                         _ptr(qz), _ptr(out), _numel(qx))
+        opt = _options(gwn_query_batch_config(), True, precision, fp64_threshold, False)
+        rc = _lib.load().gwnb_batch_create_f32(arr, len(meshes), float(accuracy_scale), C.byref(opt),
+                                               C.byref(self._handle), _stream(stream))
+        self.status = _status(rc)
+        self._stream = stream
+
+    def ok(self) -> bool:
+        return self.status.is_ok() and bool(self._handle)
+
+    def tune(self, repetitions: int = 3, stream=None) -> tuple[gwn_status, dict]:
+        t = _lib.batch_tuning()
+        rc = _lib.load().gwnb_batch_tune_f32(self._handle, int(repetitions), C.byref(t), _stream(stream))
+        return _status(rc), {f: getattr(t, f) for f, _ in _lib.batch_tuning._fields_}
+
+    def set_tuning(self, refit_block: int, query_block: int, per_thread: int, sorted_queries: int,
+                   grid_scale: int) -> gwn_status:
+        t = _lib.batch_tuning(refit_block, query_block, per_thread, sorted_queries, grid_scale, 0.0)
+        return _status(_lib.load().gwnb_batch_set_tuning_f32(self._handle, C.byref(t)))
+
+    def frame(self, stream=None) -> gwn_status:
+        return _status(_lib.load().gwnb_batch_frame_f32(self._handle, _stream(stream)))
+
+    def sync(self, stream=None) -> gwn_status:
+        return _status(_lib.load().gwnb_batch_sync_f32(self._handle, _stream(stream)))
+
+    def release(self, stream=None) -> None:
+        if self._handle:
+            _lib.load().gwnb_batch_release_f32(self._handle, _stream(stream if stream is not None else self._stream))
+            self._handle = C.c_void_p()
+
+    def __del__(self) -> None:
+        try:
+            self.release()
+        except Exception:
+            pass
 
 
 # ---- host views of device state (tests, diagnostics) ------------------------------------------------

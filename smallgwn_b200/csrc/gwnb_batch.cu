@@ -1,0 +1,262 @@
+// Batched dynamic meshes: many BVHs refit and queried per frame in three persistent launches.
+//
+// smallgwn serves one mesh per call, and every refit synchronizes with the host
+// (detail/gwn_bvh_refit_impl.cuh:324, detail/gwn_bvh_refit_moment_impl.cuh:260). Here a batch holds
+// the device descriptors of all its meshes: a frame is the batched bounds refit (one work item per
+// leaf-bearing node of every BVH), the batched moment refit, and one traversal launch over every
+// mesh's queries (warp-aligned ranges of a common slot space). Nothing in a frame allocates or
+// synchronizes, so applications capture frames (with their own vertex updates) in a CUDA graph.
+//
+// The autotuner times candidate launch shapes -- refit block size; query block size, traversal
+// form (a warp of 32 Morton-adjacent queries walking one traversal, or one traversal per thread),
+// Morton-ordered or input order, persistent grid size -- on the batch itself and keeps the fastest.
+#include "gwnb_internal.cuh"
+
+#include <algorithm>
+#include <cstdio>
+#include <new>
+#include <string>
+#include <vector>
+
+struct gwnb_batch {
+    std::vector<gwnb_bvh4_f32 *> bvhs;
+    std::vector<unsigned int *> status_words;
+    gwnb::batch_refit_state refit{};
+    gwnb::batch_query_state query{};
+    gwnb_batch_tuning tuning{128, 256, 0, 1, 8, 0.0f};
+    unsigned int **d_status = nullptr; // device copy of status_words
+    unsigned int *d_flags = nullptr;   // OR of every mesh's status word
+    cudaStream_t stream = nullptr;     // stream the batch's arrays were allocated on
+};
+
+namespace gwnb {
+namespace {
+
+__global__ void k_gather_status(unsigned int *const *__restrict__ words, std::uint32_t n, unsigned int *out) {
+    unsigned int v = 0;
+    for (std::uint32_t i = threadIdx.x; i < n; i += blockDim.x)
+        v |= *words[i];
+    if (v != 0u)
+        atomicOr(out, v);
+}
+
+void release_batch(gwnb_batch *b, cudaStream_t s) {
+    batch_refit_release(b->refit, s);
+    batch_query_release(b->query, s);
+    release(b->d_status, s);
+    release(b->d_flags, s);
+}
+
+int frame(gwnb_batch *b, gwnb_batch_tuning const &t, cudaStream_t s) {
+    GWNB_TRY(batch_refit_launch(b->refit, t.refit_block, s));
+    batch_query_config const c{t.query_block, t.per_thread, t.sorted, t.grid_scale};
+    return batch_query_launch(b->query, c, s);
+}
+
+bool tuning_valid(gwnb_batch_tuning const &t) {
+    return t.refit_block >= 32 && t.refit_block <= 256 && (t.refit_block % 32) == 0 && t.query_block >= 32 &&
+           t.query_block <= 256 && (t.query_block % 32) == 0 && (t.per_thread == 0 || t.per_thread == 1) &&
+           (t.sorted == 0 || t.sorted == 1) && t.grid_scale >= 1 && t.grid_scale <= 64;
+}
+
+} // namespace
+} // namespace gwnb
+
+using namespace gwnb;
+
+extern "C" {
+
+int gwnb_batch_create_f32(const gwnb_batch_mesh_f32 *meshes, uint32_t mesh_count, float beta,
+                          const gwnb_taylor_options *opt, gwnb_batch **out, gwnb_stream_t stream) {
+    if (out == nullptr)
+        return set_error(GWNB_INVALID_ARGUMENT, "batch: output handle must be non-null.");
+    *out = nullptr;
+    if (mesh_count == 0 || meshes == nullptr)
+        return set_error(GWNB_INVALID_ARGUMENT, "batch: at least one mesh is required.");
+    if (!(beta >= 0.0f))
+        return set_error(GWNB_INVALID_ARGUMENT, "Taylor accuracy scale must be nonnegative.");
+    gwnb_taylor_options o{256, 64, 1, GWNB_NEAR_PLAIN, 1.0f / 16.0f, 0};
+    if (opt != nullptr)
+        o = *opt;
+    if (o.near_precision != GWNB_NEAR_PLAIN && o.near_precision != GWNB_NEAR_COMPENSATED)
+        return set_error(GWNB_INVALID_ARGUMENT, "Unknown near-field precision mode.");
+    int const order = meshes[0].moment != nullptr ? meshes[0].moment->order : -1;
+    for (uint32_t i = 0; i < mesh_count; ++i) {
+        gwnb_batch_mesh_f32 const &m = meshes[i];
+        if (!geometry_valid(&m.geometry))
+            return set_error(GWNB_INVALID_ARGUMENT, "batch: mesh " + std::to_string(i) + " has an invalid geometry.");
+        if (!bvh_valid(m.bvh))
+            return set_error(GWNB_INVALID_ARGUMENT, "batch: mesh " + std::to_string(i) + " has no queryable BVH.");
+        if (m.geometry.triangle_count != m.bvh->primitive_count)
+            return set_error(GWNB_INVALID_ARGUMENT,
+                             "batch: mesh " + std::to_string(i) + " geometry does not match its BVH.");
+        if (!moment_valid_for(m.moment, m.bvh) || m.moment->order != order)
+            return set_error(GWNB_INVALID_ARGUMENT,
+                             "batch: mesh " + std::to_string(i) + " moments are stale or of another order.");
+        if (!has_storage(m.query_x, m.query_count) || !has_storage(m.query_y, m.query_count) ||
+            !has_storage(m.query_z, m.query_count) || !has_storage(m.output, m.query_count))
+            return set_error(GWNB_INVALID_ARGUMENT,
+                             "batch: mesh " + std::to_string(i) + " query/output spans must be non-null.");
+        if (m.query_count > 0xffffffffull)
+            return set_error(GWNB_INVALID_ARGUMENT, "Query batch exceeds 2^32 - 1 queries.");
+        if (ref_internal(m.bvh->root.reference) && m.bvh->internal_stack_bound > 64)
+            return set_error(GWNB_INVALID_ARGUMENT, "Batched traversal supports stack bounds up to 64.");
+    }
+    cudaStream_t const s = as_cuda(stream);
+    auto *b = new (std::nothrow) gwnb_batch{};
+    if (b == nullptr)
+        return set_error(GWNB_INTERNAL_ERROR, "out of host memory");
+    b->stream = s;
+    std::vector<gwnb_geometry_f32> geoms(mesh_count);
+    std::vector<gwnb_moment4_f32 *> moms(mesh_count);
+    std::vector<taylor_request> reqs(mesh_count);
+    b->bvhs.resize(mesh_count);
+    b->status_words.resize(mesh_count);
+    auto fail = [&](int rc) {
+        release_batch(b, s);
+        delete b;
+        return rc;
+    };
+    int rc = GWNB_OK;
+    for (uint32_t i = 0; i < mesh_count; ++i) {
+        gwnb_batch_mesh_f32 const &m = meshes[i];
+        if ((rc = ensure_bvh_aux(m.bvh, s)) != GWNB_OK)
+            return fail(rc);
+        auto *a = reinterpret_cast<bvh_aux_impl *>(m.bvh->aux);
+        auto *ma = reinterpret_cast<moment_aux_impl *>(m.moment->aux);
+        geoms[i] = m.geometry;
+        moms[i] = m.moment;
+        b->bvhs[i] = m.bvh;
+        b->status_words[i] = a->status;
+        taylor_request &r = reqs[i];
+        r.order = order;
+        r.qnodes = ma != nullptr ? ma->qnodes : nullptr;
+        r.qcounts = ma != nullptr ? ma->qcounts : nullptr;
+        r.tri48 = a->tri48;
+        r.primitive_count = m.bvh->primitive_count;
+        r.node_count = m.bvh->node_count;
+        r.root_ref = m.bvh->root.reference;
+        r.root_bounds = a->root_bounds;
+        r.qx = m.query_x;
+        r.qy = m.query_y;
+        r.qz = m.query_z;
+        r.out = m.output;
+        r.n = m.query_count;
+        r.accuracy_scale = beta;
+        r.stack_capacity = std::max<int>(static_cast<int>(m.bvh->internal_stack_bound), 1);
+        r.sort_queries = 1;
+        r.near_mode = o.near_precision;
+        r.fp64_threshold = o.fp64_threshold;
+        r.fp64_count = a->fp64_count;
+        r.status = a->status;
+    }
+    if ((rc = batch_refit_prepare(geoms.data(), b->bvhs.data(), moms.data(), mesh_count, order, &b->refit, s)) !=
+        GWNB_OK)
+        return fail(rc);
+    if ((rc = batch_query_prepare(reqs.data(), mesh_count, &b->query, s)) != GWNB_OK)
+        return fail(rc);
+    if ((rc = alloc(&b->d_status, mesh_count, s)) != GWNB_OK || (rc = alloc(&b->d_flags, 1, s)) != GWNB_OK)
+        return fail(rc);
+    if (cudaMemcpyAsync(b->d_status, b->status_words.data(), mesh_count * sizeof(unsigned int *),
+                        cudaMemcpyHostToDevice, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess)
+        return fail(set_cuda_error(cudaGetLastError(), "batch descriptors"));
+    *out = b;
+    return GWNB_OK;
+}
+
+int gwnb_batch_set_tuning_f32(gwnb_batch *b, const gwnb_batch_tuning *t) {
+    if (b == nullptr || t == nullptr || !tuning_valid(*t))
+        return set_error(GWNB_INVALID_ARGUMENT, "batch: invalid tuning.");
+    b->tuning = *t;
+    return GWNB_OK;
+}
+
+int gwnb_batch_frame_f32(gwnb_batch *b, gwnb_stream_t stream) {
+    if (b == nullptr)
+        return set_error(GWNB_INVALID_ARGUMENT, "batch: null handle.");
+    return frame(b, b->tuning, as_cuda(stream));
+}
+
+int gwnb_batch_tune_f32(gwnb_batch *b, int reps, gwnb_batch_tuning *chosen, gwnb_stream_t stream) {
+    if (b == nullptr || reps <= 0)
+        return set_error(GWNB_INVALID_ARGUMENT, "batch: tuning needs a handle and a positive repetition count.");
+    cudaStream_t const s = as_cuda(stream);
+    std::vector<gwnb_batch_tuning> cand;
+    for (int refit_block : {128, 256})
+        for (int per_thread : {0, 1})
+            for (int sorted : {1, 0})
+                for (int block : {128, 256})
+                    for (int scale : {4, 8, 16})
+                        cand.push_back(gwnb_batch_tuning{refit_block, block, per_thread, sorted, scale, 0.0f});
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    GWNB_CUDA_TRY(cudaEventCreate(&e0));
+    GWNB_CUDA_TRY(cudaEventCreate(&e1));
+    int rc = GWNB_OK;
+    gwnb_batch_tuning best{};
+    float best_ms = -1.0f;
+    for (gwnb_batch_tuning &t : cand) {
+        if ((rc = frame(b, t, s)) != GWNB_OK) // warm-up (and one-time attribute setup)
+            break;
+        if (cudaEventRecord(e0, s) != cudaSuccess) {
+            rc = set_cuda_error(cudaGetLastError(), "batch tuning");
+            break;
+        }
+        for (int r = 0; r < reps && rc == GWNB_OK; ++r)
+            rc = frame(b, t, s);
+        if (rc != GWNB_OK)
+            break;
+        float ms = 0.0f;
+        if (cudaEventRecord(e1, s) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+            cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) {
+            rc = set_cuda_error(cudaGetLastError(), "batch tuning");
+            break;
+        }
+        t.frame_ms = ms / static_cast<float>(reps);
+        if (best_ms < 0.0f || t.frame_ms < best_ms) {
+            best_ms = t.frame_ms;
+            best = t;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc != GWNB_OK)
+        return rc;
+    b->tuning = best;
+    // leave the chosen shape's one-time setup done, so the next frame can be captured
+    GWNB_TRY(frame(b, best, s));
+    GWNB_CUDA_TRY(cudaStreamSynchronize(s));
+    if (chosen != nullptr)
+        *chosen = best;
+    return GWNB_OK;
+}
+
+int gwnb_batch_sync_f32(gwnb_batch *b, gwnb_stream_t stream) {
+    if (b == nullptr)
+        return set_error(GWNB_INVALID_ARGUMENT, "batch: null handle.");
+    cudaStream_t const s = as_cuda(stream);
+    GWNB_CUDA_TRY(cudaMemsetAsync(b->d_flags, 0, sizeof(unsigned int), s));
+    k_gather_status<<<1, 256, 0, s>>>(b->d_status, static_cast<std::uint32_t>(b->status_words.size()), b->d_flags);
+    GWNB_CUDA_TRY(cudaGetLastError());
+    unsigned int flags = 0;
+    GWNB_CUDA_TRY(cudaMemcpyAsync(&flags, b->d_flags, sizeof(flags), cudaMemcpyDeviceToHost, s));
+    GWNB_CUDA_TRY(cudaStreamSynchronize(s));
+    if (flags != 0u)
+        return set_error(GWNB_INTERNAL_ERROR, "batch: device error bits 0x" + [&] {
+            char buf[16];
+            std::snprintf(buf, sizeof(buf), "%x", flags);
+            return std::string(buf);
+        }() + " (index, topology, wait timeout, stack overflow) on at least one mesh.");
+    return GWNB_OK;
+}
+
+int gwnb_batch_release_f32(gwnb_batch *b, gwnb_stream_t stream) {
+    if (b == nullptr)
+        return GWNB_OK;
+    cudaStream_t const s = stream != nullptr ? as_cuda(stream) : b->stream;
+    release_batch(b, s);
+    delete b;
+    return GWNB_OK;
+}
+
+} // extern "C"

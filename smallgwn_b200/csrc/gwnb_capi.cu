@@ -83,37 +83,6 @@ int query_order(aabb const *root_bounds, float const *qx, float const *qy, float
 
 namespace {
 
-cudaStream_t as_cuda(gwnb_stream_t s) { return reinterpret_cast<cudaStream_t>(s); }
-
-bool has_storage(void const *p, std::uint64_t n) { return n == 0 || p != nullptr; }
-
-bool geometry_valid(gwnb_geometry_f32 const *g) {
-    return g != nullptr && has_storage(g->vertex_x, g->vertex_count) &&
-           has_storage(g->vertex_y, g->vertex_count) && has_storage(g->vertex_z, g->vertex_count) &&
-           has_storage(g->tri_i0, g->triangle_count) && has_storage(g->tri_i1, g->triangle_count) &&
-           has_storage(g->tri_i2, g->triangle_count);
-}
-
-bool bvh_valid(gwnb_bvh4_f32 const *b) {
-    if (b == nullptr || b->revision == 0 || !ref_valid(b->root.reference) || b->primitive_count == 0)
-        return false;
-    if (!has_storage(b->nodes, b->node_count) || b->primitive_indices == nullptr || b->triangles == nullptr)
-        return false;
-    std::uint64_t const off = ref_offset(b->root.reference);
-    if (ref_internal(b->root.reference))
-        return off < b->node_count;
-    std::uint64_t const cnt = ref_count(b->root.reference);
-    return off <= b->primitive_count && cnt <= b->primitive_count - off;
-}
-
-bool moment_valid_for(gwnb_moment4_f32 const *m, gwnb_bvh4_f32 const *b) {
-    if (m == nullptr || !bvh_valid(b) || m->bvh_revision != b->revision)
-        return false;
-    if (ref_leaf(b->root.reference))
-        return m->node_count == 0;
-    return m->nodes != nullptr && m->node_count == b->node_count && m->aux != nullptr;
-}
-
 __global__ void k_validate_indices(std::uint32_t const *i0, std::uint32_t const *i1, std::uint32_t const *i2,
                                    std::uint64_t nt, std::uint64_t nv, unsigned int *flag) {
     std::uint64_t const t = static_cast<std::uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;

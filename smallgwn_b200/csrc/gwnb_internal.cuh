@@ -128,6 +128,41 @@ struct moment_aux_impl {
     std::size_t payload_stride = 0;
 };
 
+// ---- host-side validation of C ABI views ----------------------------------------------------------
+
+inline cudaStream_t as_cuda(gwnb_stream_t s) { return reinterpret_cast<cudaStream_t>(s); }
+
+inline bool has_storage(void const *p, std::uint64_t n) { return n == 0 || p != nullptr; }
+
+inline bool geometry_valid(gwnb_geometry_f32 const *g) {
+    return g != nullptr && has_storage(g->vertex_x, g->vertex_count) &&
+           has_storage(g->vertex_y, g->vertex_count) && has_storage(g->vertex_z, g->vertex_count) &&
+           has_storage(g->tri_i0, g->triangle_count) && has_storage(g->tri_i1, g->triangle_count) &&
+           has_storage(g->tri_i2, g->triangle_count);
+}
+
+// A queryable BVH: a revision, a valid root reference and the arrays it implies.
+inline bool bvh_valid(gwnb_bvh4_f32 const *b) {
+    if (b == nullptr || b->revision == 0 || !ref_valid(b->root.reference) || b->primitive_count == 0)
+        return false;
+    if (!has_storage(b->nodes, b->node_count) || b->primitive_indices == nullptr || b->triangles == nullptr)
+        return false;
+    std::uint64_t const off = ref_offset(b->root.reference);
+    if (ref_internal(b->root.reference))
+        return off < b->node_count;
+    std::uint64_t const cnt = ref_count(b->root.reference);
+    return off <= b->primitive_count && cnt <= b->primitive_count - off;
+}
+
+// Moments refit for exactly this revision of the BVH (smallgwn gwn_bvh_moment_accessor::is_valid_for).
+inline bool moment_valid_for(gwnb_moment4_f32 const *m, gwnb_bvh4_f32 const *b) {
+    if (m == nullptr || !bvh_valid(b) || m->bvh_revision != b->revision)
+        return false;
+    if (ref_leaf(b->root.reference))
+        return m->node_count == 0;
+    return m->nodes != nullptr && m->node_count == b->node_count && m->aux != nullptr;
+}
+
 // ---- status helpers (host) -------------------------------------------------------------------
 int set_error(int code, std::string const &message);
 int set_cuda_error(cudaError_t err, char const *what);
@@ -225,6 +260,46 @@ struct adjoint_request {
     unsigned int *status;
 };
 int taylor_adjoint(adjoint_request const &r, cudaStream_t s);
+
+// Batched refit of many BVHs (bounds, then moments) in one persistent launch each. The device
+// descriptor arrays are of types private to the refit translation unit.
+struct batch_refit_state {
+    std::uint32_t mesh_count = 0;
+    int order = 0;
+    std::uint64_t bounds_items = 0;
+    std::uint64_t moment_items = 0;
+    void *bounds_meshes = nullptr;
+    void *moment_meshes = nullptr;
+    std::uint64_t *bounds_begin = nullptr; // mesh_count + 1 work offsets
+    std::uint64_t *moment_begin = nullptr;
+};
+int batch_refit_prepare(gwnb_geometry_f32 const *geoms, gwnb_bvh4_f32 *const *bvhs, gwnb_moment4_f32 *const *moms,
+                        std::uint32_t n, int order, batch_refit_state *st, cudaStream_t s);
+int batch_refit_launch(batch_refit_state const &st, int block, cudaStream_t s);
+void batch_refit_release(batch_refit_state &st, cudaStream_t s);
+
+// Batched Taylor queries of many BVHs in one persistent launch: each mesh's queries occupy a
+// range of warp slots (padded to whole warps) of a global slot space.
+struct batch_query_state {
+    std::uint32_t mesh_count = 0;
+    int order = 0;
+    int near_mode = GWNB_NEAR_PLAIN;
+    std::uint64_t warps = 0;               // total warps of the slot space
+    void *meshes = nullptr;                // device per-mesh traversal descriptors (Morton order)
+    void *meshes_unsorted = nullptr;       // the same in input order
+    std::uint64_t *warp_begin = nullptr;   // mesh_count + 1 warp offsets
+    std::uint32_t *orders = nullptr;       // per-mesh Morton orders, concatenated
+    int max_stack_bound = 0;
+};
+struct batch_query_config {
+    int block;      // threads per block (multiple of 32)
+    int per_thread; // 0: warp-cooperative traversal, 1: one traversal per thread
+    int sorted;     // 1: traverse in each mesh's Morton order
+    int grid_scale; // persistent grid = SMs x grid_scale blocks
+};
+int batch_query_prepare(taylor_request const *meshes, std::uint32_t n, batch_query_state *st, cudaStream_t s);
+int batch_query_launch(batch_query_state const &st, batch_query_config const &c, cudaStream_t s);
+void batch_query_release(batch_query_state &st, cudaStream_t s);
 
 int create_bvh_aux(gwnb_bvh4_f32 *bvh, cudaStream_t s);
 int ensure_bvh_aux(gwnb_bvh4_f32 *bvh, cudaStream_t s);

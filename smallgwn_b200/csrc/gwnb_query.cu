@@ -18,28 +18,27 @@
 #include "gwnb_field.cuh"
 
 #include <algorithm>
+#include <vector>
 
 namespace gwnb {
 namespace {
 
 using namespace field;
 
-// Running sums of many terms of mixed size (up to a million solid angles per query in the exact
-// batch): with Compensated, Neumaier's variant of Kahan summation (Neumaier 1974) carries the
-// rounding error of every addition, so terms below half an ulp of the running sum are not lost.
+// Running sums of many terms of mixed size (up to millions of solid angles per query in the exact
+// batch, most of them below an ulp of a running sum near 4 pi). With Compensated the sum is kept in
+// FP64: the same two registers as a Kahan/Neumaier pair, one DADD per term instead of six FP32
+// operations, and no order dependence -- a float Neumaier sum of the 8.4M-triangle sphere still
+// loses up to 3e-5 because its correction term itself grows to ~0.15.
 template <bool Compensated> struct accum {
     float s = 0.0f;
     __device__ __forceinline__ void add(float x) { s += x; }
     __device__ __forceinline__ float value() const { return s; }
 };
 template <> struct accum<true> {
-    float s = 0.0f, c = 0.0f;
-    __device__ __forceinline__ void add(float x) {
-        float const t = s + x;
-        c += (fabsf(s) >= fabsf(x)) ? ((s - t) + x) : ((x - t) + s);
-        s = t;
-    }
-    __device__ __forceinline__ float value() const { return s + c; }
+    double s = 0.0;
+    __device__ __forceinline__ void add(float x) { s += static_cast<double>(x); }
+    __device__ __forceinline__ float value() const { return static_cast<float>(s); }
 };
 
 // ---- exact batch --------------------------------------------------------------------------------
@@ -228,11 +227,12 @@ struct taylor_params {
     unsigned int *status;
 };
 
+// One query of the per-thread traversal: sorted position idx of the batch described by p, with
+// s_stack pointing at this thread's column of a [Cap][blockDim.x] shared-memory stack.
 template <int Order, int Cap, int Mode, bool Grad, bool Stats>
-__global__ void __launch_bounds__(256) k_taylor(taylor_params p) {
+__device__ __forceinline__ void taylor_thread_item(taylor_params const &p, std::uint64_t idx,
+                                                   std::uint32_t *s_stack) {
     constexpr int Q = qnode_traits<Order>::k_f4_per_child;
-    extern __shared__ std::uint32_t s_stack[]; // [Cap][blockDim.x]
-    std::uint64_t const idx = static_cast<std::uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (idx >= p.n)
         return;
     std::uint32_t const qi = p.order != nullptr ? p.order[idx] : static_cast<std::uint32_t>(idx);
@@ -241,7 +241,7 @@ __global__ void __launch_bounds__(256) k_taylor(taylor_params p) {
     float gx = 0.0f, gy = 0.0f, gz = 0.0f;
     std::uint32_t st_nodes = 0, st_far = 0, st_near = 0;
     unsigned const stride = blockDim.x;
-    std::uint32_t *const stack = s_stack + threadIdx.x;
+    std::uint32_t *const stack = s_stack; // this thread's column; entries are blockDim.x apart
     int sp = 0;
     bool overflow = false;
 
@@ -362,6 +362,12 @@ __global__ void __launch_bounds__(256) k_taylor(taylor_params p) {
     }
 }
 
+template <int Order, int Cap, int Mode, bool Grad, bool Stats>
+__global__ void __launch_bounds__(256) k_taylor(taylor_params p) {
+    extern __shared__ std::uint32_t s_stack[]; // [Cap][blockDim.x]
+    taylor_thread_item<Order, Cap, Mode, Grad, Stats>(
+        p, static_cast<std::uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x, s_stack + threadIdx.x);
+}
 
 // Warp-cooperative traversal: the 32 lanes of a warp (32 Morton-adjacent queries) walk one
 // depth-first traversal together. Every stack entry carries the mask of lanes that still need the
@@ -379,13 +385,13 @@ template <int Mode, bool Grad, bool Stats> struct taylor_warp_occupancy {
     static constexpr int value = (comp && Grad) ? 3 : ((comp || Grad || Stats) ? 4 : 5);
 };
 
+// One warp of the warp-cooperative traversal: lane k takes sorted position idx (idx - lane is the
+// warp's first position). Every lane of the warp must call it with the same p.
 template <int Order, int Cap, int Mode, bool Grad, bool Stats>
-__global__ void __launch_bounds__(256, (taylor_warp_occupancy<Mode, Grad, Stats>::value))
-    k_taylor_warp(taylor_params p) {
+__device__ __forceinline__ void taylor_warp_item(taylor_params const &p, std::uint64_t idx) {
     static_assert(Cap <= 64, "warp stack holds at most 64 entries");
     constexpr int Q = qnode_traits<Order>::k_f4_per_child;
     unsigned const lane = threadIdx.x & 31u;
-    std::uint64_t const idx = static_cast<std::uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     bool const valid = idx < p.n;
     unsigned const full = __ballot_sync(0xffffffffu, valid);
     if (full == 0u)
@@ -552,6 +558,57 @@ __global__ void __launch_bounds__(256, (taylor_warp_occupancy<Mode, Grad, Stats>
 }
 
 template <int Order, int Cap, int Mode, bool Grad, bool Stats>
+__global__ void __launch_bounds__(256, (taylor_warp_occupancy<Mode, Grad, Stats>::value))
+    k_taylor_warp(taylor_params p) {
+    taylor_warp_item<Order, Cap, Mode, Grad, Stats>(p, static_cast<std::uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x);
+}
+
+// ---- batched traversal (many BVHs, one persistent launch) -----------------------------------------
+//
+// Mesh m owns warps [warp_begin[m], warp_begin[m + 1]) of a global slot space (its queries padded
+// to whole warps, so no warp spans two BVHs). The grid strides over warps; a warp finds its mesh by
+// binary search (a warp-uniform result) and runs the single-BVH traversal on its 32 slots.
+
+__device__ __forceinline__ std::uint32_t find_mesh_warp(std::uint64_t const *begin, std::uint32_t mesh_count,
+                                                        std::uint64_t w) {
+    std::uint32_t lo = 0, hi = mesh_count;
+    while (hi - lo > 1) {
+        std::uint32_t const mid = (lo + hi) >> 1;
+        if (__ldg(begin + mid) <= w)
+            lo = mid;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
+template <int Order, int Cap, int Mode>
+__global__ void __launch_bounds__(256, (taylor_warp_occupancy<Mode, false, false>::value))
+    k_batch_taylor_warp(taylor_params const *__restrict__ meshes, std::uint64_t const *__restrict__ warp_begin,
+                        std::uint32_t mesh_count, std::uint64_t warps) {
+    std::uint64_t const warps_per_grid = static_cast<std::uint64_t>(gridDim.x) * (blockDim.x >> 5);
+    for (std::uint64_t w = static_cast<std::uint64_t>(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5); w < warps;
+         w += warps_per_grid) {
+        std::uint32_t const m = find_mesh_warp(warp_begin, mesh_count, w);
+        taylor_warp_item<Order, Cap, Mode, false, false>(meshes[m], (w - warp_begin[m]) * 32 + (threadIdx.x & 31u));
+    }
+}
+
+template <int Order, int Cap, int Mode>
+__global__ void __launch_bounds__(256)
+    k_batch_taylor_thread(taylor_params const *__restrict__ meshes, std::uint64_t const *__restrict__ warp_begin,
+                          std::uint32_t mesh_count, std::uint64_t warps) {
+    extern __shared__ std::uint32_t s_stack[]; // [Cap][blockDim.x]
+    std::uint64_t const warps_per_grid = static_cast<std::uint64_t>(gridDim.x) * (blockDim.x >> 5);
+    for (std::uint64_t w = static_cast<std::uint64_t>(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5); w < warps;
+         w += warps_per_grid) {
+        std::uint32_t const m = find_mesh_warp(warp_begin, mesh_count, w);
+        taylor_thread_item<Order, Cap, Mode, false, false>(meshes[m], (w - warp_begin[m]) * 32 + (threadIdx.x & 31u),
+                                                           s_stack + threadIdx.x);
+    }
+}
+
+template <int Order, int Cap, int Mode, bool Grad, bool Stats>
 int launch_taylor_warp(taylor_params const &p, int block, cudaStream_t s) {
     unsigned const grid = static_cast<unsigned>((p.n + block - 1) / block);
     k_taylor_warp<Order, Cap, Mode, Grad, Stats><<<grid, block, 0, s>>>(p);
@@ -632,9 +689,8 @@ int query_order(aabb const *root_bounds, float const *qx, float const *qy, float
 
 
 
-int taylor_batch(taylor_request const &r, cudaStream_t s) {
-    if (r.n == 0)
-        return GWNB_OK;
+namespace {
+taylor_params make_taylor_params(taylor_request const &r) {
     taylor_params p{};
     p.qnodes = r.qnodes;
     p.qcounts = r.qcounts;
@@ -657,6 +713,14 @@ int taylor_batch(taylor_request const &r, cudaStream_t s) {
     p.fp64_threshold = r.fp64_threshold;
     p.fp64_count = r.fp64_count;
     p.status = r.status;
+    return p;
+}
+} // namespace
+
+int taylor_batch(taylor_request const &r, cudaStream_t s) {
+    if (r.n == 0)
+        return GWNB_OK;
+    taylor_params p = make_taylor_params(r);
     std::uint32_t *codes = nullptr, *sorted_codes = nullptr, *order = nullptr;
     bool const sorted = r.sort_queries != 0 && r.n > 1 && r.root_bounds != nullptr;
     if (sorted) {
@@ -693,6 +757,110 @@ int taylor_batch(taylor_request const &r, cudaStream_t s) {
     release(sorted_codes, s);
     release(order, s);
     return rc;
+}
+
+// ---- batched traversal (host) -----------------------------------------------------------------------
+
+int batch_query_prepare(taylor_request const *reqs, std::uint32_t n, batch_query_state *st, cudaStream_t s) {
+    std::vector<taylor_params> sorted(n), unsorted(n);
+    std::vector<std::uint64_t> wb(n + 1, 0);
+    std::uint64_t total = 0;
+    int max_bound = 1;
+    for (std::uint32_t i = 0; i < n; ++i) {
+        total += reqs[i].n;
+        wb[i + 1] = wb[i] + (reqs[i].n + 31) / 32;
+        max_bound = std::max(max_bound, reqs[i].stack_capacity);
+    }
+    GWNB_TRY(alloc(&st->orders, std::max<std::uint64_t>(total, 1), s));
+    std::uint64_t off = 0;
+    for (std::uint32_t i = 0; i < n; ++i) {
+        taylor_params p = make_taylor_params(reqs[i]);
+        unsorted[i] = p;
+        if (reqs[i].n > 1 && reqs[i].root_bounds != nullptr) {
+            GWNB_TRY(query_order(reqs[i].root_bounds, reqs[i].qx, reqs[i].qy, reqs[i].qz, reqs[i].n, st->orders + off, s,
+                                 reqs[i].status));
+            p.order = st->orders + off;
+        }
+        sorted[i] = p;
+        off += reqs[i].n;
+    }
+    taylor_params *ds = nullptr, *du = nullptr;
+    GWNB_TRY(alloc(&ds, n, s));
+    GWNB_TRY(alloc(&du, n, s));
+    GWNB_TRY(alloc(&st->warp_begin, n + 1, s));
+    st->meshes = ds;
+    st->meshes_unsorted = du;
+    GWNB_CUDA_TRY(cudaMemcpyAsync(ds, sorted.data(), n * sizeof(taylor_params), cudaMemcpyHostToDevice, s));
+    GWNB_CUDA_TRY(cudaMemcpyAsync(du, unsorted.data(), n * sizeof(taylor_params), cudaMemcpyHostToDevice, s));
+    GWNB_CUDA_TRY(cudaMemcpyAsync(st->warp_begin, wb.data(), (n + 1) * sizeof(std::uint64_t), cudaMemcpyHostToDevice, s));
+    GWNB_CUDA_TRY(cudaStreamSynchronize(s)); // the host vectors go out of scope
+    st->mesh_count = n;
+    st->order = n > 0 ? reqs[0].order : 0;
+    st->near_mode = n > 0 ? reqs[0].near_mode : GWNB_NEAR_PLAIN;
+    st->warps = wb[n];
+    st->max_stack_bound = max_bound;
+    return GWNB_OK;
+}
+
+namespace {
+template <int Order, int Cap, int Mode>
+int launch_batch_cap(batch_query_state const &st, batch_query_config const &c, cudaStream_t s) {
+    auto const *meshes = static_cast<taylor_params const *>(c.sorted ? st.meshes : st.meshes_unsorted);
+    int const block = c.block;
+    std::uint64_t const need = (st.warps * 32 + block - 1) / block;
+    std::uint64_t const cap = static_cast<std::uint64_t>(device_sm_count()) * std::max(c.grid_scale, 1);
+    unsigned const grid = static_cast<unsigned>(std::max<std::uint64_t>(std::min(need, cap), 1));
+    if (c.per_thread == 0) {
+        k_batch_taylor_warp<Order, Cap, Mode><<<grid, block, 0, s>>>(meshes, st.warp_begin, st.mesh_count, st.warps);
+    } else {
+        std::size_t const smem = static_cast<std::size_t>(Cap) * block * sizeof(std::uint32_t);
+        auto kern = k_batch_taylor_thread<Order, Cap, Mode>;
+        if (smem > 48 * 1024)
+            GWNB_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+        kern<<<grid, block, smem, s>>>(meshes, st.warp_begin, st.mesh_count, st.warps);
+    }
+    GWNB_CUDA_TRY(cudaGetLastError());
+    return GWNB_OK;
+}
+
+template <int Order, int Mode>
+int launch_batch_mode(batch_query_state const &st, batch_query_config const &c, cudaStream_t s) {
+    if (st.max_stack_bound <= 32)
+        return launch_batch_cap<Order, 32, Mode>(st, c, s);
+    return launch_batch_cap<Order, 64, Mode>(st, c, s);
+}
+
+template <int Order>
+int launch_batch_order(batch_query_state const &st, batch_query_config const &c, cudaStream_t s) {
+    if (st.near_mode == GWNB_NEAR_COMPENSATED)
+        return launch_batch_mode<Order, GWNB_NEAR_COMPENSATED>(st, c, s);
+    return launch_batch_mode<Order, GWNB_NEAR_PLAIN>(st, c, s);
+}
+} // namespace
+
+int batch_query_launch(batch_query_state const &st, batch_query_config const &c, cudaStream_t s) {
+    if (st.warps == 0)
+        return GWNB_OK;
+    if (c.block < 32 || c.block > 256 || (c.block % 32) != 0)
+        return set_error(GWNB_INVALID_ARGUMENT, "Batch query block size must be a multiple of 32 in [32, 256].");
+    if (st.max_stack_bound > 64)
+        return set_error(GWNB_INVALID_ARGUMENT, "Batched traversal supports stack bounds up to 64.");
+    if (st.order == 0)
+        return launch_batch_order<0>(st, c, s);
+    if (st.order == 1)
+        return launch_batch_order<1>(st, c, s);
+    return launch_batch_order<2>(st, c, s);
+}
+
+void batch_query_release(batch_query_state &st, cudaStream_t s) {
+    auto *ds = static_cast<taylor_params *>(st.meshes);
+    auto *du = static_cast<taylor_params *>(st.meshes_unsorted);
+    release(ds, s);
+    release(du, s);
+    release(st.warp_begin, s);
+    release(st.orders, s);
+    st.meshes = nullptr;
+    st.meshes_unsorted = nullptr;
 }
 
 std::size_t radix_sort_u32_scratch_words(std::uint64_t n, int key_bits);

@@ -16,6 +16,7 @@
 #include "gwnb_internal.cuh"
 
 #include <new>
+#include <vector>
 
 namespace gwnb {
 namespace {
@@ -126,10 +127,9 @@ struct refit_params {
     unsigned int *status;
 };
 
-__global__ void __launch_bounds__(k_block) k_refit_bounds(refit_params p) {
-    std::uint64_t const t = static_cast<std::uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (t >= p.leaf_node_count)
-        return;
+// One work item of the bounds refit: leaf-bearing node t of the BVH refreshes its triangles, then
+// climbs while it is the last arrival.
+__device__ __forceinline__ void refit_bounds_item(refit_params const &p, std::uint64_t t) {
     std::uint32_t cur = p.leaf_nodes[t];
     // Refresh the leaf children of this node.
 #pragma unroll
@@ -198,7 +198,14 @@ __global__ void __launch_bounds__(k_block) k_refit_bounds(refit_params p) {
     }
 }
 
-__global__ void k_refit_leaf_root(refit_params p, std::uint64_t first, std::uint32_t cnt) {
+__global__ void __launch_bounds__(k_block) k_refit_bounds(refit_params p) {
+    std::uint64_t const t = static_cast<std::uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t < p.leaf_node_count)
+        refit_bounds_item(p, t);
+}
+
+// The whole refit of a BVH whose root is a leaf (one work item).
+__device__ __forceinline__ void refit_leaf_root_item(refit_params const &p, std::uint64_t first, std::uint32_t cnt) {
     aabb u{0, 0, 0, 0, 0, 0};
     bool init = false;
     for (std::uint32_t k = 0; k < cnt; ++k) {
@@ -217,6 +224,10 @@ __global__ void k_refit_leaf_root(refit_params p, std::uint64_t first, std::uint
         init = true;
     }
     *p.root_bounds = u;
+}
+
+__global__ void k_refit_leaf_root(refit_params p, std::uint64_t first, std::uint32_t cnt) {
+    refit_leaf_root_item(p, first, cnt);
 }
 
 // ---- moments -----------------------------------------------------------------------------------
@@ -586,10 +597,9 @@ __device__ inline void finish_node(moment_params const &p, std::uint32_t n) {
     store_payload_cg(pend + n, total);
 }
 
-template <int Order> __global__ void __launch_bounds__(k_block) k_refit_moments(moment_params p) {
-    std::uint64_t const t = static_cast<std::uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (t >= p.leaf_node_count)
-        return;
+// One work item of the moment refit: from leaf-bearing node t, finish every node this thread is
+// the last arrival at, climbing to the root.
+template <int Order> __device__ __forceinline__ void refit_moments_item(moment_params const &p, std::uint64_t t) {
     std::uint32_t cur = p.leaf_nodes[t];
     std::uint64_t guard = 0;
     for (;;) {
@@ -614,6 +624,67 @@ template <int Order> __global__ void __launch_bounds__(k_block) k_refit_moments(
             return;
         }
         cur = parent;
+    }
+}
+
+template <int Order> __global__ void __launch_bounds__(k_block) k_refit_moments(moment_params p) {
+    std::uint64_t const t = static_cast<std::uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t < p.leaf_node_count)
+        refit_moments_item<Order>(p, t);
+}
+
+// ---- batched refit (many BVHs, one launch) -------------------------------------------------------
+//
+// Mesh m owns work items [begin[m], begin[m + 1]) of a global index space: its leaf-bearing nodes,
+// or a single item when its root is a leaf. A persistent grid strides over the items; each finds its
+// mesh by binary search over `begin` (mesh_count + 1 ascending offsets) and runs the single-BVH item.
+// The climbs never wait on one another (the last arrival continues), so any grid size is safe.
+
+__device__ __forceinline__ std::uint32_t find_mesh(std::uint64_t const *begin, std::uint32_t mesh_count,
+                                                   std::uint64_t item) {
+    std::uint32_t lo = 0, hi = mesh_count; // begin[lo] <= item < begin[hi]
+    while (hi - lo > 1) {
+        std::uint32_t const mid = (lo + hi) >> 1;
+        if (__ldg(begin + mid) <= item)
+            lo = mid;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
+struct batch_bounds_mesh {
+    refit_params p;
+    std::uint64_t leaf_root_first; // root is a leaf: its triangle range (leaf_root_count > 0)
+    std::uint32_t leaf_root_count;
+};
+
+constexpr int k_batch_block_max = 256; // batched refit launches take 32..256 threads per block
+
+__global__ void __launch_bounds__(k_batch_block_max)
+    k_batch_refit_bounds(batch_bounds_mesh const *__restrict__ meshes, std::uint64_t const *__restrict__ begin,
+                         std::uint32_t mesh_count) {
+    std::uint64_t const total = begin[mesh_count];
+    for (std::uint64_t i = static_cast<std::uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < total;
+         i += static_cast<std::uint64_t>(gridDim.x) * blockDim.x) {
+        std::uint32_t const m = find_mesh(begin, mesh_count, i);
+        batch_bounds_mesh const &d = meshes[m];
+        if (d.leaf_root_count > 0)
+            refit_leaf_root_item(d.p, d.leaf_root_first, d.leaf_root_count);
+        else
+            refit_bounds_item(d.p, i - begin[m]);
+    }
+}
+
+template <int Order>
+__global__ void __launch_bounds__(k_batch_block_max)
+    k_batch_refit_moments(moment_params const *__restrict__ meshes, std::uint64_t const *__restrict__ begin,
+                          std::uint32_t mesh_count) {
+    std::uint64_t const total = begin[mesh_count];
+    for (std::uint64_t i = static_cast<std::uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < total;
+         i += static_cast<std::uint64_t>(gridDim.x) * blockDim.x) {
+        std::uint32_t const m = find_mesh(begin, mesh_count, i);
+        refit_moments_item<Order>(meshes[m], i - begin[m]);
     }
 }
 
@@ -701,6 +772,123 @@ int write_tri48(gwnb_bvh4_f32 const *bvh, cudaStream_t s) {
         reinterpret_cast<triangle const *>(bvh->triangles), a->tri48, bvh->primitive_count);
     GWNB_CUDA_TRY(cudaGetLastError());
     return GWNB_OK;
+}
+
+namespace {
+refit_params make_refit_params(gwnb_geometry_f32 const &g, gwnb_bvh4_f32 const *bvh) {
+    auto *a = reinterpret_cast<bvh_aux_impl *>(bvh->aux);
+    refit_params p{};
+    p.g = g;
+    p.nodes = reinterpret_cast<node4 *>(bvh->nodes);
+    p.node_count = bvh->node_count;
+    p.primitive_indices = bvh->primitive_indices;
+    p.triangles = reinterpret_cast<triangle *>(bvh->triangles);
+    p.tri48 = a->tri48;
+    p.primitive_count = bvh->primitive_count;
+    p.parent_slot = a->parent_slot;
+    p.expected = a->expected;
+    p.arrivals = a->arrivals;
+    p.leaf_nodes = a->leaf_nodes;
+    p.leaf_node_count = a->leaf_node_count;
+    p.root_bounds = a->root_bounds;
+    p.status = a->status;
+    return p;
+}
+
+moment_params make_moment_params(gwnb_bvh4_f32 const *bvh, gwnb_moment4_f32 const *m) {
+    auto *a = reinterpret_cast<bvh_aux_impl *>(bvh->aux);
+    auto *ma = reinterpret_cast<moment_aux_impl *>(m->aux);
+    moment_params p{};
+    p.nodes = reinterpret_cast<node4 const *>(bvh->nodes);
+    p.node_count = bvh->node_count;
+    p.triangles = reinterpret_cast<triangle const *>(bvh->triangles);
+    p.primitive_count = bvh->primitive_count;
+    p.parent_slot = a->parent_slot;
+    p.expected = a->expected;
+    p.arrivals = a->arrivals + bvh->node_count;
+    p.leaf_nodes = a->leaf_nodes;
+    p.leaf_node_count = a->leaf_node_count;
+    p.ref_nodes = static_cast<float *>(m->nodes);
+    p.qnodes = ma->qnodes;
+    p.qcounts = ma->qcounts;
+    p.pending = ma->payload;
+    p.status = a->status;
+    return p;
+}
+} // namespace
+
+int batch_refit_prepare(gwnb_geometry_f32 const *geoms, gwnb_bvh4_f32 *const *bvhs, gwnb_moment4_f32 *const *moms,
+                        std::uint32_t n, int order, batch_refit_state *st, cudaStream_t s) {
+    std::vector<batch_bounds_mesh> bd(n);
+    std::vector<moment_params> md(n);
+    std::vector<std::uint64_t> bb(n + 1, 0), mb(n + 1, 0);
+    for (std::uint32_t i = 0; i < n; ++i) {
+        gwnb_bvh4_f32 const *b = bvhs[i];
+        auto *a = reinterpret_cast<bvh_aux_impl *>(b->aux);
+        bd[i].p = make_refit_params(geoms[i], b);
+        bool const leaf_root = ref_leaf(b->root.reference);
+        bd[i].leaf_root_first = leaf_root ? ref_offset(b->root.reference) : 0;
+        bd[i].leaf_root_count = leaf_root ? ref_count(b->root.reference) : 0;
+        bb[i + 1] = bb[i] + (leaf_root ? 1 : a->leaf_node_count);
+        // a leaf root has no moment nodes (and no moment refit work)
+        md[i] = leaf_root ? moment_params{} : make_moment_params(b, moms[i]);
+        mb[i + 1] = mb[i] + (leaf_root ? 0 : a->leaf_node_count);
+    }
+    st->mesh_count = n;
+    st->order = order;
+    st->bounds_items = bb[n];
+    st->moment_items = mb[n];
+    batch_bounds_mesh *dbd = nullptr;
+    moment_params *dmd = nullptr;
+    GWNB_TRY(alloc(&dbd, n, s));
+    GWNB_TRY(alloc(&dmd, n, s));
+    GWNB_TRY(alloc(&st->bounds_begin, n + 1, s));
+    GWNB_TRY(alloc(&st->moment_begin, n + 1, s));
+    st->bounds_meshes = dbd;
+    st->moment_meshes = dmd;
+    GWNB_CUDA_TRY(cudaMemcpyAsync(dbd, bd.data(), n * sizeof(batch_bounds_mesh), cudaMemcpyHostToDevice, s));
+    GWNB_CUDA_TRY(cudaMemcpyAsync(dmd, md.data(), n * sizeof(moment_params), cudaMemcpyHostToDevice, s));
+    GWNB_CUDA_TRY(cudaMemcpyAsync(st->bounds_begin, bb.data(), (n + 1) * sizeof(std::uint64_t), cudaMemcpyHostToDevice, s));
+    GWNB_CUDA_TRY(cudaMemcpyAsync(st->moment_begin, mb.data(), (n + 1) * sizeof(std::uint64_t), cudaMemcpyHostToDevice, s));
+    // the host vectors are released on return: wait for the copies
+    GWNB_CUDA_TRY(cudaStreamSynchronize(s));
+    return GWNB_OK;
+}
+
+int batch_refit_launch(batch_refit_state const &st, int block, cudaStream_t s) {
+    if (block < 32 || block > k_batch_block_max || (block % 32) != 0)
+        return set_error(GWNB_INVALID_ARGUMENT, "Batch refit block size must be a multiple of 32 in [32, 256].");
+    int const sms = device_sm_count();
+    auto grid = [&](std::uint64_t items) {
+        std::uint64_t const need = (items + block - 1) / block;
+        std::uint64_t const cap = static_cast<std::uint64_t>(sms) * (2048 / block);
+        return static_cast<unsigned>(need < cap ? need : cap);
+    };
+    if (st.bounds_items > 0)
+        k_batch_refit_bounds<<<grid(st.bounds_items), block, 0, s>>>(
+            static_cast<batch_bounds_mesh const *>(st.bounds_meshes), st.bounds_begin, st.mesh_count);
+    if (st.moment_items > 0) {
+        auto const *md = static_cast<moment_params const *>(st.moment_meshes);
+        unsigned const g = grid(st.moment_items);
+        switch (st.order) {
+        case 0: k_batch_refit_moments<0><<<g, block, 0, s>>>(md, st.moment_begin, st.mesh_count); break;
+        case 1: k_batch_refit_moments<1><<<g, block, 0, s>>>(md, st.moment_begin, st.mesh_count); break;
+        default: k_batch_refit_moments<2><<<g, block, 0, s>>>(md, st.moment_begin, st.mesh_count); break;
+        }
+    }
+    GWNB_CUDA_TRY(cudaGetLastError());
+    return GWNB_OK;
+}
+
+void batch_refit_release(batch_refit_state &st, cudaStream_t s) {
+    auto *bd = static_cast<batch_bounds_mesh *>(st.bounds_meshes);
+    auto *md = static_cast<moment_params *>(st.moment_meshes);
+    release(bd, s);
+    release(md, s);
+    release(st.bounds_begin, s);
+    release(st.moment_begin, s);
+    st.bounds_meshes = nullptr;
+    st.moment_meshes = nullptr;
 }
 
 int refit_bounds_async(gwnb_geometry_f32 const &g, gwnb_bvh4_f32 *bvh, cudaStream_t s) {

@@ -150,6 +150,32 @@ def mixed_queries(mesh: dict, n: int, seed: int, offset_sigma: float = 1e-3,
     return tuple(np.ascontiguousarray(out[:, k]) for k in range(3))
 
 
+class SurfaceSampler:
+    """Queries at surface samples offset along the unit normal by a log-uniform magnitude in
+    [lo, hi] of random sign (the precision-stress query set); triangles are picked uniformly among
+    non-degenerate ones. `sample(n, seed)` returns (qx, qy, qz, signed offsets)."""
+
+    def __init__(self, mesh: dict, lo: float = 1e-6, hi: float = 1e-1) -> None:
+        a, b, c, nrm, area2 = triangle_normals(mesh)
+        good = np.flatnonzero(area2 > 0)
+        self.a, self.ab, self.ac = a[good], (b - a)[good], (c - a)[good]
+        self.unit = nrm[good] / area2[good, None]
+        self.lo, self.hi = lo, hi
+
+    def sample(self, n: int, seed: int):
+        rng = np.random.default_rng(seed)
+        tri = rng.integers(0, self.a.shape[0], size=n)
+        u = rng.uniform(0.0, 1.0, size=(n, 2))
+        flip = u.sum(axis=1) > 1.0
+        u[flip] = 1.0 - u[flip]
+        mag = np.exp(rng.uniform(np.log(self.lo), np.log(self.hi), size=n))
+        off = mag * np.where(rng.uniform(size=n) < 0.5, -1.0, 1.0)
+        out = self.a[tri] + u[:, :1] * self.ab[tri] + u[:, 1:] * self.ac[tri] + off[:, None] * self.unit[tri]
+        out = out.astype(np.float32)
+        return (np.ascontiguousarray(out[:, 0]), np.ascontiguousarray(out[:, 1]), np.ascontiguousarray(out[:, 2]),
+                off)
+
+
 def soup_mesh(n: int = 316, seed: int = 3, delete_frac: float = 0.2, flip_frac: float = 0.05) -> dict:
     V, F = uv_sphere(n, n, seed)
     rng = np.random.default_rng(seed)

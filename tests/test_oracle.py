@@ -231,6 +231,16 @@ def test_frozen_fp64_taylor_is_the_float_traversal_in_fp64(order):
     np.testing.assert_allclose(full, oracle.exact_winding(m, *q64, fp64=True), atol=1e-12)
 
 
+def test_mesh_distance_known_answers():
+    """Unit right triangle in z = 0: above the interior, beside the edge v0 v1, beside the
+    hypotenuse, beyond vertex v0, beyond vertex v1."""
+    m = single_triangle()
+    q = [np.array([0.25, 0.5, 2.0, -1.0, 2.0]), np.array([0.25, -1.0, 2.0, -1.0, -1.0]),
+         np.array([0.5, 0.0, 0.0, 0.0, 0.0])]
+    d = oracle.mesh_distance(m, *q)
+    np.testing.assert_allclose(d, [0.5, 1.0, np.sqrt(4.5), np.sqrt(2.0), np.sqrt(2.0)], atol=1e-15)
+
+
 def test_leaf_root_build_record():
     b = oracle.build_lbvh(single_triangle())
     assert b["root_reference"] == VALID | (1 << 48)
