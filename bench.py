@@ -47,7 +47,7 @@ def parse() -> argparse.Namespace:
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="taylor", choices=["taylor", "adjoint", "precision", "exact"],
+    ap.add_argument("--workload", default="taylor", choices=["taylor", "adjoint", "precision", "exact", "batched"],
                     help="taylor: the headline (1M-triangle sphere, 10M queries); adjoint: forward + backward "
                          "on the 159k-triangle soup; precision: 8.4M-triangle sphere, 100M near-surface queries "
                          "in 16M chunks; exact: brute-force exact batch on the small icosphere")
@@ -568,6 +568,158 @@ def run_precision_workload(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+def run_batched_workload(args) -> None:
+    """Batched dynamic refit: 256 displaced spheres with triangle counts log-uniform in [1k, 200k]
+    and query counts log-uniform in [10k, 1M] (seed 4), all vertices in one device buffer. A frame
+    deforms every mesh, v += 0.02 sin(2 pi f / 100 + w . v) n_v (w ~ N(0, I) per mesh, n_v the rest
+    vertex normal), then refits every BVH and its order-1 moments and evaluates every mesh's Taylor
+    queries (accuracy scale 2): the deformation and the library's three batched launches are one
+    CUDA graph, replayed 100 times with device-timed frames. Beside it, the per-mesh loop of plain
+    calls (gwn_refit_bvh, gwn_refit_bvh_moment, Taylor batch per mesh) on the same state."""
+    import torch
+
+    import smallgwn_b200 as g
+    from smallgwn_b200 import api, meshes
+
+    order, beta, n_mesh, frames = 1, 2.0, 256, 100
+    rng = np.random.default_rng(4)
+    tris = np.exp(rng.uniform(np.log(1e3), np.log(2e5), n_mesh))
+    nqs = np.exp(rng.uniform(np.log(1e4), np.log(1e6), n_mesh)).astype(np.int64)
+    W = rng.normal(size=(n_mesh, 3))
+    parts = []
+    for i in range(n_mesh):
+        k = max(int(round(np.sqrt(tris[i] / 4.0))), 4)
+        V, F = meshes.uv_sphere(2 * k, k + 1, seed=4000 + i)
+        mesh = meshes.to_soa(V, F)
+        a, b, c, nrm, _ = meshes.triangle_normals(mesh)
+        vn = np.zeros_like(V, dtype=np.float64)
+        for j in range(3):
+            np.add.at(vn, F[:, j], nrm)
+        vn /= np.maximum(np.linalg.norm(vn, axis=1, keepdims=True), 1e-30)
+        parts.append((V.astype(np.float32), F.astype(np.int32), vn.astype(np.float32), mesh))
+    nv = sum(p[0].shape[0] for p in parts)
+    X = torch.empty(3, nv, device="cuda")
+    Nv = torch.empty(3, nv, device="cuda")
+    Wv = torch.empty(3, nv, device="cuda")
+    stream = torch.cuda.current_stream()
+    objs, off = [], 0
+    for i, (V, F, vn, mesh) in enumerate(parts):
+        n = V.shape[0]
+        X[:, off:off + n] = torch.from_numpy(V.T.copy()).cuda()
+        Nv[:, off:off + n] = torch.from_numpy(vn.T.copy()).cuda()
+        Wv[:, off:off + n] = torch.from_numpy(W[i].astype(np.float32)).cuda()[:, None]
+        idx = [torch.from_numpy(np.ascontiguousarray(F[:, j])).cuda() for j in range(3)]
+        geo = api.gwn_geometry_view(X[0, off:off + n], X[1, off:off + n], X[2, off:off + n], *idx)
+        bvh = g.gwn_bvh4_object()
+        assert g.gwn_build_bvh(geo, bvh, g.gwn_bvh_build_options(method=0, hploc_search_radius=8)).is_ok()
+        mom = g.gwn_bvh4_moment_object(order)
+        assert g.gwn_refit_bvh_moment(order, bvh, mom).is_ok()
+        q = meshes.mixed_queries(mesh, int(nqs[i]), seed=40_000 + i)
+        dq = [torch.from_numpy(v).cuda() for v in q]
+        objs.append((geo, bvh, mom, *dq, torch.empty(int(nqs[i]), device="cuda")))
+        off += n
+    X0 = X.clone()
+    fidx = torch.zeros(1, device="cuda")
+
+    def deform():
+        phase = (2 * np.pi / 100.0) * fidx + (Wv * X).sum(0)
+        X.add_(0.02 * torch.sin(phase) * Nv)
+        fidx.add_(1.0)
+
+    batch = g.gwn_batch(objs, accuracy_scale=beta, stream=stream)
+    assert batch.ok(), batch.status.message
+    st, tuning = batch.tune(repetitions=3, stream=stream)
+    assert st.is_ok(), st.message
+    # graph: deformation + one batched frame
+    X.copy_(X0)
+    fidx.zero_()
+    side = torch.cuda.Stream()
+    side.wait_stream(torch.cuda.current_stream())
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.stream(side):
+        assert batch.frame(side.cuda_stream).is_ok()
+        side.synchronize()
+        with torch.cuda.graph(graph, stream=side):
+            deform()
+            assert batch.frame(side.cuda_stream).is_ok()
+    torch.cuda.synchronize()
+    X.copy_(X0)
+    fidx.zero_()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(frames)]
+    cur = torch.cuda.current_stream()
+    with ClockSampler(torch.cuda.current_device()) as clocks:
+        for e0, e1 in ev:
+            e0.record(cur)
+            graph.replay()
+            e1.record(cur)
+        torch.cuda.synchronize()
+    lat = np.array([a.elapsed_time(b) for a, b in ev])
+    assert batch.sync().is_ok()
+    got = [o[-1].cpu().numpy() for o in objs]
+
+    def stage_ms() -> dict:
+        out = {}
+        for name, st_ in (("refit", batch.REFIT), ("moments", batch.MOMENTS), ("query", batch.QUERY)):
+            t = timed_steps(lambda st_=st_: batch.run(st_, cur.cuda_stream), 3, 1, cur, flush)
+            out[name] = float(np.mean(t))
+        return out
+
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    # stage times at the last frame's state and half way through the deformation
+    stages_end = stage_ms()
+    X.copy_(X0)
+    fidx.zero_()
+    for _ in range(50):
+        graph.replay()
+    torch.cuda.synchronize()
+    stages_mid = stage_ms()
+    X.copy_(X0)
+    fidx.zero_()
+    for _ in range(frames):
+        graph.replay()
+    torch.cuda.synchronize()
+    assert batch.sync().is_ok()
+    # the per-mesh loop on the same final state: refit, moments, query per mesh
+    def per_mesh_frame():
+        for geo, bvh, mom, qx, qy, qz, out in objs:
+            assert g.gwn_refit_bvh(geo, bvh).is_ok()
+            assert g.gwn_refit_bvh_moment(order, bvh, mom).is_ok()
+            assert g.gwn_compute_winding_number_taylor_batch(order, bvh, mom, qx, qy, qz, out,
+                                                             accuracy_scale=beta).is_ok()
+    per_mesh_frame()
+    torch.cuda.synchronize()
+    ref = [o[-1].cpu().numpy() for o in objs]
+    max_diff = max(float(np.max(np.abs(a - b))) if a.size else 0.0 for a, b in zip(got, ref))
+    loop_frames = 5
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(loop_frames):
+        deform()
+        per_mesh_frame()
+    torch.cuda.synchronize()
+    loop_ms = (time.perf_counter() - t0) * 1e3 / loop_frames
+    del graph
+    batch.release()
+    total_ms = float(lat.sum())
+    line = {
+        "metric": "Batched dynamic refit + Taylor query frames/s (256 meshes, CUDA graph)",
+        "value": frames / (total_ms / 1e3), "unit": "frames/s", "n_gpus": 1, "steps": frames, "warmup": 1,
+        "ms_per_step": total_ms / frames, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "256 displaced spheres, tris log-U[1k,200k], queries log-U[10k,1M] (seed 4), "
+                               "100 deformed frames", "meshes": n_mesh,
+                   "triangles": int(sum(p[1].shape[0] for p in parts)), "vertices": int(nv),
+                   "queries_per_frame": int(nqs.sum()), "taylor_order": order, "accuracy_scale": beta,
+                   "frame_ms_p50": float(np.percentile(lat, 50)), "frame_ms_p99": float(np.percentile(lat, 99)),
+                   "per_mesh_loop_ms_per_frame": loop_ms, "speedup_vs_per_mesh_loop": loop_ms / (total_ms / frames),
+                   "max_abs_diff_vs_per_mesh_loop": max_diff, "tuning": tuning,
+                   "stage_ms_frame_100": stages_end, "stage_ms_frame_50": stages_mid},
+        "gpu_launches": None,
+        "clocks": clocks.summary(),
+    }
+    print(json.dumps(line), flush=True)
+
+
 def run_exact_workload(args) -> None:
     """Plain exact winding number, small: icosphere level 4 (5,120 triangles, radial noise seed 0),
     100k queries uniform in [-1.5, 1.5]^3 (seed 1), LBVH, exact batch; the oracle's FP32 brute force
@@ -624,8 +776,8 @@ def main() -> None:
         run_reference_arm(args)
         return
     if args.workload != "taylor":
-        {"adjoint": run_adjoint_workload, "precision": run_precision_workload,
-         "exact": run_exact_workload}[args.workload](args)
+        {"adjoint": run_adjoint_workload, "precision": run_precision_workload, "exact": run_exact_workload,
+         "batched": run_batched_workload}[args.workload](args)
         return
     import torch
 

@@ -387,6 +387,13 @@ GWNB_API int gwnb_batch_set_tuning_f32(gwnb_batch *batch, const gwnb_batch_tunin
 /* Enqueues one frame (refit, moment refit, queries) on `stream`; asynchronous and capturable once
  * a frame or a tuning has run outside capture. */
 GWNB_API int gwnb_batch_frame_f32(gwnb_batch *batch, gwnb_stream_t stream);
+
+/* Stages of a frame, for gwnb_batch_run_f32 (a frame is all three, in this order). */
+#define GWNB_BATCH_REFIT 1u   /* bounds and triangle records of every BVH                */
+#define GWNB_BATCH_MOMENTS 2u /* Taylor moments of every BVH (after the bounds)          */
+#define GWNB_BATCH_QUERY 4u   /* every mesh's Taylor queries                             */
+/* Enqueues the selected stages of a frame (e.g. refit once, then query several times). */
+GWNB_API int gwnb_batch_run_f32(gwnb_batch *batch, unsigned int stages, gwnb_stream_t stream);
 /* Synchronizes `stream` and reports device-side errors of any mesh (index or topology faults,
  * stack overflow) as GWNB_INTERNAL_ERROR. */
 GWNB_API int gwnb_batch_sync_f32(gwnb_batch *batch, gwnb_stream_t stream);

@@ -21,6 +21,10 @@ GWNB_METHOD_LBVH = 1
 GWNB_NEAR_PLAIN = 0
 GWNB_NEAR_COMPENSATED = 1
 
+GWNB_BATCH_REFIT = 1
+GWNB_BATCH_MOMENTS = 2
+GWNB_BATCH_QUERY = 4
+
 
 class aabb_f32(C.Structure):
     _fields_ = [(n, C.c_float) for n in ("min_x", "min_y", "min_z", "max_x", "max_y", "max_z")]
@@ -178,6 +182,7 @@ SIGNATURES: dict[str, tuple] = {
     "gwnb_batch_tune_f32": (I, [P, I, C.POINTER(batch_tuning), P]),
     "gwnb_batch_set_tuning_f32": (I, [P, C.POINTER(batch_tuning)]),
     "gwnb_batch_frame_f32": (I, [P, P]),
+    "gwnb_batch_run_f32": (I, [P, C.c_uint, P]),
     "gwnb_batch_sync_f32": (I, [P, P]),
     "gwnb_batch_release_f32": (I, [P, P]),
 }

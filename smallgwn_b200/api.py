@@ -524,6 +524,12 @@ class gwn_batch:
     def frame(self, stream=None) -> gwn_status:
         return _status(_lib.load().gwnb_batch_frame_f32(self._handle, _stream(stream)))
 
+    REFIT, MOMENTS, QUERY = _lib.GWNB_BATCH_REFIT, _lib.GWNB_BATCH_MOMENTS, _lib.GWNB_BATCH_QUERY
+
+    def run(self, stages: int, stream=None) -> gwn_status:
+        """Selected stages of a frame (REFIT | MOMENTS | QUERY)."""
+        return _status(_lib.load().gwnb_batch_run_f32(self._handle, int(stages), _stream(stream)))
+
     def sync(self, stream=None) -> gwn_status:
         return _status(_lib.load().gwnb_batch_sync_f32(self._handle, _stream(stream)))
 

@@ -60,19 +60,16 @@ struct adjoint_params {
     unsigned int *status;
 };
 
-template <int K> __device__ __forceinline__ void warp_sum(float (&v)[K]) {
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1)
-#pragma unroll
-        for (int k = 0; k < K; ++k)
-            v[k] += __shfl_xor_sync(0xffffffffu, v[k], off);
-}
-
-// Adds the shares of the lanes in `mask` (warp-uniform; other lanes hold zeros) to dst[0..K): a
-// lone lane adds its own share, otherwise the warp sums first and the lowest lane of `mask` adds.
-// Every lane of the warp must call it.
+// Adds the shares of the lanes in `mask` (warp-uniform; other lanes hold zeros) to dst[0..K),
+// K <= 16. A lone lane adds its own share. Otherwise a recursive-halving reduce-scatter: at stride
+// d = 1, 2, 4, 8 every lane keeps half of its remaining values (the lower half when its bit d is
+// clear) and adds its partner's copy of that half, so after four steps lane l holds the sum over its
+// 16-lane group of value bitrev4(l); one more exchange across the two groups completes the sums
+// (16 shuffles where a butterfly per value would take 5 K), and 16 lanes add the K totals with one
+// coalesced atomic instruction. Every lane of the warp must call it.
 template <int K>
-__device__ __forceinline__ void warp_scatter_add(float *dst, float (&v)[K], unsigned mask, unsigned lane) {
+__device__ __forceinline__ void warp_scatter_add(float *dst, float const (&v)[K], unsigned mask, unsigned lane) {
+    static_assert(K <= 16, "reduce-scatter holds at most 16 values");
     if (__popc(mask) == 1) {
         if (((mask >> lane) & 1u) != 0u) {
 #pragma unroll
@@ -81,12 +78,24 @@ __device__ __forceinline__ void warp_scatter_add(float *dst, float (&v)[K], unsi
         }
         return;
     }
-    warp_sum(v);
-    if (lane == static_cast<unsigned>(__ffs(static_cast<int>(mask)) - 1)) {
+    float r[16];
 #pragma unroll
-        for (int k = 0; k < K; ++k)
-            atomicAdd(dst + k, v[k]);
+    for (int k = 0; k < 16; ++k)
+        r[k] = k < K ? v[k] : 0.0f;
+#pragma unroll
+    for (int d = 1, m = 16; d <= 8; d <<= 1, m >>= 1) {
+        bool const upper = (lane & static_cast<unsigned>(d)) != 0u;
+#pragma unroll
+        for (int j = 0; j < m / 2; ++j) {
+            float const send = upper ? r[j] : r[j + m / 2];
+            float const keep = upper ? r[j + m / 2] : r[j];
+            r[j] = keep + __shfl_xor_sync(0xffffffffu, send, d);
+        }
     }
+    r[0] += __shfl_xor_sync(0xffffffffu, r[0], 16);
+    unsigned const idx = __brev(lane & 15u) >> 28;
+    if (lane < 16u && idx < static_cast<unsigned>(K))
+        atomicAdd(dst + idx, r[0]);
 }
 
 template <int Order, int Cap>

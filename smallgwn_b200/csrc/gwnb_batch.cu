@@ -47,10 +47,19 @@ void release_batch(gwnb_batch *b, cudaStream_t s) {
     release(b->d_flags, s);
 }
 
+int run_stages(gwnb_batch *b, gwnb_batch_tuning const &t, unsigned stages, cudaStream_t s) {
+    bool const bounds = (stages & GWNB_BATCH_REFIT) != 0u, moments = (stages & GWNB_BATCH_MOMENTS) != 0u;
+    if (bounds || moments)
+        GWNB_TRY(batch_refit_launch(b->refit, t.refit_block, bounds, moments, s));
+    if ((stages & GWNB_BATCH_QUERY) != 0u) {
+        batch_query_config const c{t.query_block, t.per_thread, t.sorted, t.grid_scale};
+        return batch_query_launch(b->query, c, s);
+    }
+    return GWNB_OK;
+}
+
 int frame(gwnb_batch *b, gwnb_batch_tuning const &t, cudaStream_t s) {
-    GWNB_TRY(batch_refit_launch(b->refit, t.refit_block, s));
-    batch_query_config const c{t.query_block, t.per_thread, t.sorted, t.grid_scale};
-    return batch_query_launch(b->query, c, s);
+    return run_stages(b, t, GWNB_BATCH_REFIT | GWNB_BATCH_MOMENTS | GWNB_BATCH_QUERY, s);
 }
 
 bool tuning_valid(gwnb_batch_tuning const &t) {
@@ -176,6 +185,14 @@ int gwnb_batch_frame_f32(gwnb_batch *b, gwnb_stream_t stream) {
     if (b == nullptr)
         return set_error(GWNB_INVALID_ARGUMENT, "batch: null handle.");
     return frame(b, b->tuning, as_cuda(stream));
+}
+
+int gwnb_batch_run_f32(gwnb_batch *b, unsigned int stages, gwnb_stream_t stream) {
+    if (b == nullptr)
+        return set_error(GWNB_INVALID_ARGUMENT, "batch: null handle.");
+    if ((stages & ~(GWNB_BATCH_REFIT | GWNB_BATCH_MOMENTS | GWNB_BATCH_QUERY)) != 0u)
+        return set_error(GWNB_INVALID_ARGUMENT, "batch: unknown stage bits.");
+    return run_stages(b, b->tuning, stages, as_cuda(stream));
 }
 
 int gwnb_batch_tune_f32(gwnb_batch *b, int reps, gwnb_batch_tuning *chosen, gwnb_stream_t stream) {

@@ -275,7 +275,7 @@ struct batch_refit_state {
 };
 int batch_refit_prepare(gwnb_geometry_f32 const *geoms, gwnb_bvh4_f32 *const *bvhs, gwnb_moment4_f32 *const *moms,
                         std::uint32_t n, int order, batch_refit_state *st, cudaStream_t s);
-int batch_refit_launch(batch_refit_state const &st, int block, cudaStream_t s);
+int batch_refit_launch(batch_refit_state const &st, int block, bool bounds, bool moments, cudaStream_t s);
 void batch_refit_release(batch_refit_state &st, cudaStream_t s);
 
 // Batched Taylor queries of many BVHs in one persistent launch: each mesh's queries occupy a

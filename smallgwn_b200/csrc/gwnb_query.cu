@@ -47,12 +47,20 @@ constexpr int k_exact_block = 256;
 constexpr int k_exact_tile = 256;
 constexpr int k_exact_q = 2; // queries per thread
 
-__global__ void __launch_bounds__(k_exact_block)
+// Block (x, y) takes queries [x * 512, x * 512 + 512) against the y-th of gridDim.y contiguous
+// ranges of tiles (every range a whole number of tiles). With one range the result is written to
+// `out`; with several, each range's FP64 partial sum goes to partial[y * nq + i] and k_exact_finish
+// adds the ranges in order (small query batches split the triangles to fill the GPU).
+__global__ void __launch_bounds__(k_exact_block, 3)
     k_exact(triangle const *__restrict__ tris, std::uint64_t nt, float const *__restrict__ qx,
             float const *__restrict__ qy, float const *__restrict__ qz, float *__restrict__ out,
-            std::uint64_t nq) {
+            std::uint64_t nq, double *__restrict__ partial) {
     __shared__ float4 s_tri[k_exact_tile][3];
     std::uint64_t const base = static_cast<std::uint64_t>(blockIdx.x) * (k_exact_block * k_exact_q);
+    std::uint64_t const tiles = (nt + k_exact_tile - 1) / k_exact_tile;
+    std::uint64_t const per = (tiles + gridDim.y - 1) / gridDim.y;
+    std::uint64_t const t_begin = static_cast<std::uint64_t>(blockIdx.y) * per * k_exact_tile;
+    std::uint64_t const t_end = std::min<std::uint64_t>(t_begin + per * k_exact_tile, nt);
     float px[k_exact_q], py[k_exact_q], pz[k_exact_q];
     accum<true> acc[k_exact_q];
 #pragma unroll
@@ -63,11 +71,11 @@ __global__ void __launch_bounds__(k_exact_block)
         py[k] = v ? qy[i] : 0.0f;
         pz[k] = v ? qz[i] : 0.0f;
     }
-    for (std::uint64_t t0 = 0; t0 < nt; t0 += k_exact_tile) {
+    for (std::uint64_t t0 = t_begin; t0 < t_end; t0 += k_exact_tile) {
         __syncthreads();
         std::uint64_t const t = t0 + threadIdx.x;
         if (threadIdx.x < k_exact_tile) {
-            if (t < nt) {
+            if (t < t_end) {
                 triangle const r = tris[t];
                 float const nx = r.e1_y * r.e2_z - r.e1_z * r.e2_y;
                 float const ny = r.e1_z * r.e2_x - r.e1_x * r.e2_z;
@@ -83,7 +91,7 @@ __global__ void __launch_bounds__(k_exact_block)
             }
         }
         __syncthreads();
-        std::uint64_t const rem = nt - t0;
+        std::uint64_t const rem = t_end - t0;
         int const cnt = rem < static_cast<std::uint64_t>(k_exact_tile) ? static_cast<int>(rem) : k_exact_tile;
 #pragma unroll 2
         for (int j = 0; j < cnt; ++j) {
@@ -99,9 +107,24 @@ __global__ void __launch_bounds__(k_exact_block)
 #pragma unroll
     for (int k = 0; k < k_exact_q; ++k) {
         std::uint64_t const i = base + threadIdx.x + static_cast<std::uint64_t>(k) * k_exact_block;
-        if (i < nq)
+        if (i >= nq)
+            continue;
+        if (partial == nullptr)
             out[i] = acc[k].value() / (4.0f * k_pi_f);
+        else
+            partial[static_cast<std::uint64_t>(blockIdx.y) * nq + i] = acc[k].s;
     }
+}
+
+__global__ void __launch_bounds__(256)
+    k_exact_finish(double const *__restrict__ partial, unsigned ranges, float *__restrict__ out, std::uint64_t nq) {
+    std::uint64_t const i = static_cast<std::uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= nq)
+        return;
+    double s = 0.0;
+    for (unsigned r = 0; r < ranges; ++r)
+        s += partial[static_cast<std::uint64_t>(r) * nq + i];
+    out[i] = static_cast<float>(s) / (4.0f * k_pi_f);
 }
 
 // ---- FP64 exact over the float geometry ---------------------------------------------------------
@@ -657,9 +680,26 @@ int exact_batch(triangle const *tris, std::uint64_t nt, float const *qx, float c
                 float const *qz, float *out, std::uint64_t nq, cudaStream_t s) {
     if (nq == 0)
         return GWNB_OK;
-    unsigned const grid = static_cast<unsigned>((nq + k_exact_block * k_exact_q - 1) / (k_exact_block * k_exact_q));
-    k_exact<<<grid, k_exact_block, 0, s>>>(tris, nt, qx, qy, qz, out, nq);
-    GWNB_CUDA_TRY(cudaGetLastError());
+    std::uint64_t const qblocks = (nq + k_exact_block * k_exact_q - 1) / (k_exact_block * k_exact_q);
+    // Split the triangles into ranges of at least 4 tiles until ~6 blocks per SM are in flight
+    // (3 are resident at 72 registers); one range writes the result directly.
+    std::uint64_t const tiles = (nt + k_exact_tile - 1) / k_exact_tile;
+    std::uint64_t const want = static_cast<std::uint64_t>(device_sm_count()) * 6;
+    std::uint64_t ranges = qblocks >= want ? 1 : (want + qblocks - 1) / qblocks;
+    ranges = std::min<std::uint64_t>(ranges, std::max<std::uint64_t>(tiles / 4, 1));
+    ranges = std::min<std::uint64_t>(ranges, 64);
+    double *partial = nullptr;
+    if (ranges > 1)
+        GWNB_TRY(alloc(&partial, ranges * nq, s));
+    dim3 const grid(static_cast<unsigned>(qblocks), static_cast<unsigned>(ranges));
+    k_exact<<<grid, k_exact_block, 0, s>>>(tris, nt, qx, qy, qz, out, nq, partial);
+    if (ranges > 1)
+        k_exact_finish<<<static_cast<unsigned>((nq + 255) / 256), 256, 0, s>>>(partial, static_cast<unsigned>(ranges),
+                                                                             out, nq);
+    cudaError_t const e = cudaGetLastError();
+    release(partial, s);
+    if (e != cudaSuccess)
+        return set_cuda_error(e, "exact batch launch");
     return GWNB_OK;
 }
 

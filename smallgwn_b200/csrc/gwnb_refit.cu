@@ -855,7 +855,7 @@ int batch_refit_prepare(gwnb_geometry_f32 const *geoms, gwnb_bvh4_f32 *const *bv
     return GWNB_OK;
 }
 
-int batch_refit_launch(batch_refit_state const &st, int block, cudaStream_t s) {
+int batch_refit_launch(batch_refit_state const &st, int block, bool bounds, bool moments, cudaStream_t s) {
     if (block < 32 || block > k_batch_block_max || (block % 32) != 0)
         return set_error(GWNB_INVALID_ARGUMENT, "Batch refit block size must be a multiple of 32 in [32, 256].");
     int const sms = device_sm_count();
@@ -864,10 +864,10 @@ int batch_refit_launch(batch_refit_state const &st, int block, cudaStream_t s) {
         std::uint64_t const cap = static_cast<std::uint64_t>(sms) * (2048 / block);
         return static_cast<unsigned>(need < cap ? need : cap);
     };
-    if (st.bounds_items > 0)
+    if (bounds && st.bounds_items > 0)
         k_batch_refit_bounds<<<grid(st.bounds_items), block, 0, s>>>(
             static_cast<batch_bounds_mesh const *>(st.bounds_meshes), st.bounds_begin, st.mesh_count);
-    if (st.moment_items > 0) {
+    if (moments && st.moment_items > 0) {
         auto const *md = static_cast<moment_params const *>(st.moment_meshes);
         unsigned const g = grid(st.moment_items);
         switch (st.order) {
