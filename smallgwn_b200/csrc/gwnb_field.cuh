@@ -231,9 +231,13 @@ __device__ __forceinline__ vertex_grad solid_angle_vertex_grad(float ax, float a
     return r;
 }
 
-// Far-field Taylor terms of one accepted child (smallgwn gwn_query_winding_impl.cuh:193-327).
-// r = q - P, q2 = |r|^2; b = (N, ref); cd.. = packed order-1/2 coefficients. With Grad, g is the
-// derivative with respect to the query.
+// Far-field Taylor terms of one accepted child: smallgwn's expansion
+// (gwn_query_winding_impl.cuh:193-327) on the folded sidecar coefficients the moment refit writes.
+// r = q - P, q2 = |r|^2, n = r / |r|; b = (N, ref); cd.. = order-1 quadratic form M' (xx yy zz xy yz
+// zx) then order-2 cubic form K (xxx yyy zzz xxy xxz yyx yyz zzx zzy xyz):
+//   w = -(n.N) / |r|^2 + n^T M' n / |r|^3 + K(n,n,n) / |r|^4.
+// With Grad, g is the derivative with respect to the query: the terms are P(r) / |r|^(2p+1) for
+// homogeneous P of degree p = 1, 2, 3, whose gradient is (grad P(n) - (2p+1) P(n) n) / |r|^(p+2).
 template <int Order, bool Grad>
 __device__ __forceinline__ float far_field(float rx, float ry, float rz, float q2, float4 const &b,
                                            float4 const *__restrict__ cd, float &g0, float &g1, float &g2) {
@@ -248,55 +252,54 @@ __device__ __forceinline__ float far_field(float rx, float ry, float rz, float q
         g1 = m3 * (3.0f * ny * rdn - b.y);
         g2 = m3 * (3.0f * nz * rdn - b.z);
     }
+    if constexpr (Order >= 1 && !Grad) {
+        // value only: the forms factored by components (Q1 in 7 and Q2 in 13 operations on the
+        // shared squares), grouped explicitly since the compiler keeps the written FP order
+        float4 const c = __ldg(cd);
+        float4 const d = __ldg(cd + 1);
+        float const xx = nx * nx, yy = ny * ny, zz = nz * nz, yz = ny * nz;
+        float const Q1 = c.x * xx + c.y * yy + c.z * zz + d.x * yz + nx * (c.w * ny + d.y * nz);
+        float t = Q1;
+        if constexpr (Order >= 2) {
+            float4 const e = __ldg(cd + 2);
+            float4 const f = __ldg(cd + 3);
+            float const Q2 = nx * (d.z * xx + e.w * yy + f.y * zz + f.w * yz) + ny * (d.w * yy + e.y * xx + f.z * zz) +
+                             nz * (e.x * zz + e.z * xx + f.x * yy);
+            t += m1 * Q2;
+        }
+        w += m3 * t;
+        return w;
+    }
     if constexpr (Order >= 1) {
         float4 const c = __ldg(cd);
         float4 const d = __ldg(cd + 1);
-        float const T = c.x + c.y + c.z;
-        float const S = nx * nx * c.x + ny * ny * c.y + nz * nz * c.z + nx * ny * c.w + nx * nz * d.y + ny * nz * d.x;
-        w += m3 * (T - 3.0f * S);
+        float const xx = nx * nx, yy = ny * ny, zz = nz * nz, xy = nx * ny, yz = ny * nz, zx = nz * nx;
+        float const Q1 = c.x * xx + c.y * yy + c.z * zz + c.w * xy + d.x * yz + d.y * zx;
+        w += m3 * Q1;
         if constexpr (Grad) {
             float const m4 = m2 * m2;
-            float const vx = 2.0f * c.x * nx + c.w * ny + d.y * nz;
-            float const vy = c.w * nx + 2.0f * c.y * ny + d.x * nz;
-            float const vz = d.y * nx + d.x * ny + 2.0f * c.z * nz;
-            float const co = 15.0f * S - 3.0f * T;
-            g0 += m4 * (co * nx - 3.0f * vx);
-            g1 += m4 * (co * ny - 3.0f * vy);
-            g2 += m4 * (co * nz - 3.0f * vz);
+            float const k = 5.0f * Q1;
+            g0 += m4 * (2.0f * c.x * nx + c.w * ny + d.y * nz - k * nx);
+            g1 += m4 * (c.w * nx + 2.0f * c.y * ny + d.x * nz - k * ny);
+            g2 += m4 * (d.y * nx + d.x * ny + 2.0f * c.z * nz - k * nz);
         }
         if constexpr (Order >= 2) {
             float4 const e = __ldg(cd + 2);
             float4 const f = __ldg(cd + 3);
-            float const xxx = d.z, yyy = d.w, zzz = e.x, spn = e.y;
-            float const Axy = e.z, Axz = e.w, Ayz = f.x, Ayx = f.y, Azx = f.z, Azy = f.w;
+            // K over xxx yyy zzz xxy | xxz yyx yyz zzx | zzy xyz
+            float const Q2 = d.z * xx * nx + d.w * yy * ny + e.x * zz * nz + e.y * xx * ny + e.z * xx * nz +
+                             e.w * yy * nx + f.x * yy * nz + f.y * zz * nx + f.z * zz * ny + f.w * xy * nz;
             float const m4 = m2 * m2;
-            float const nx2 = nx * nx, ny2 = ny * ny, nz2 = nz * nz;
-            float const nx3 = nx2 * nx, ny3 = ny2 * ny, nz3 = nz2 * nz;
-            float const t0x = Ayx + Azx, t0y = Azy + Axy, t0z = Axz + Ayz;
-            float const t1x = ny * Axy + nz * Axz;
-            float const t1y = nz * Ayz + nx * Ayx;
-            float const t1z = nx * Azx + ny * Azy;
-            w += m4 * (1.5f * (nx * (3.0f * xxx + t0x) + ny * (3.0f * yyy + t0y) + nz * (3.0f * zzz + t0z)) -
-                       7.5f * (nx3 * xxx + ny3 * yyy + nz3 * zzz + nx * ny * nz * spn + nx2 * t1x + ny2 * t1y +
-                               nz2 * t1z));
+            w += m4 * Q2;
             if constexpr (Grad) {
                 float const m5 = m4 * m1;
-                float const Px = 3.0f * xxx + Ayx + Azx;
-                float const Py = 3.0f * yyy + Azy + Axy;
-                float const Pz = 3.0f * zzz + Axz + Ayz;
-                float const L2 = nx * Px + ny * Py + nz * Pz;
-                float const C2 = nx3 * xxx + ny3 * yyy + nz3 * zzz + nx * ny * nz * spn + nx2 * (ny * Axy + nz * Axz) +
-                                 ny2 * (nz * Ayz + nx * Ayx) + nz2 * (nx * Azx + ny * Azy);
-                float const Rx = 3.0f * xxx * nx2 + 2.0f * Axy * nx * ny + 2.0f * Axz * nx * nz + Ayx * ny2 + Azx * nz2 +
-                                 spn * ny * nz;
-                float const Ry = 3.0f * yyy * ny2 + 2.0f * Ayx * nx * ny + 2.0f * Ayz * ny * nz + Axy * nx2 + Azy * nz2 +
-                                 spn * nx * nz;
-                float const Rz = 3.0f * zzz * nz2 + 2.0f * Azx * nx * nz + 2.0f * Azy * ny * nz + Axz * nx2 + Ayz * ny2 +
-                                 spn * nx * ny;
-                float const h = 52.5f * C2;
-                g0 += m5 * (1.5f * Px - 7.5f * (nx * L2 + Rx) + nx * h);
-                g1 += m5 * (1.5f * Py - 7.5f * (ny * L2 + Ry) + ny * h);
-                g2 += m5 * (1.5f * Pz - 7.5f * (nz * L2 + Rz) + nz * h);
+                float const k = 7.0f * Q2;
+                float const Gx = 3.0f * d.z * xx + 2.0f * e.y * xy + 2.0f * e.z * zx + e.w * yy + f.y * zz + f.w * yz;
+                float const Gy = 3.0f * d.w * yy + e.y * xx + 2.0f * e.w * xy + 2.0f * f.x * yz + f.z * zz + f.w * zx;
+                float const Gz = 3.0f * e.x * zz + e.z * xx + f.x * yy + 2.0f * f.y * zx + 2.0f * f.z * yz + f.w * xy;
+                g0 += m5 * (Gx - k * nx);
+                g1 += m5 * (Gy - k * ny);
+                g2 += m5 * (Gz - k * nz);
             }
         }
     }

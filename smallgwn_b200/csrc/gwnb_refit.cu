@@ -479,6 +479,40 @@ __device__ inline coeffs<Order> finalize_slot(aabb const &b, payload<Order> cons
     return c;
 }
 
+// Sidecar coefficients of the far-field terms, folded for the traversal (the reference layout keeps
+// smallgwn's fields). With n = r / |r| a unit vector, smallgwn's order-1 term (T - 3S) / |r|^3
+// (T = tr M, S = n^T M n) is the single quadratic form n^T M' n, M' = T I - 3 M; its order-2 term
+// (1.5 n.V - 7.5 C(n,n,n)) / |r|^4 (V_x = 3 N_xxx + A_yx + A_zx and cyclically) becomes, since
+// n.V = (n.V)(n.n), the single cubic form K(n,n,n). Written: order 1 the 6 coefficients of M' over
+// xx yy zz xy yz zx; order 2 the 10 of K over xxx yyy zzz xxy xxz yyx yyz zzx zzy xyz.
+template <int Order>
+__device__ inline void fold_far_field_coefficients(coeffs<Order> const &c, float *out) {
+    float const T = c.f[7] + c.f[8] + c.f[9];
+    out[0] = T - 3.0f * c.f[7];
+    out[1] = T - 3.0f * c.f[8];
+    out[2] = T - 3.0f * c.f[9];
+    out[3] = -3.0f * c.f[10];
+    out[4] = -3.0f * c.f[11];
+    out[5] = -3.0f * c.f[12];
+    if constexpr (Order >= 2) {
+        float const xxx = c.f[13], yyy = c.f[14], zzz = c.f[15], spn = c.f[16];
+        float const Axy = c.f[17], Axz = c.f[18], Ayz = c.f[19], Ayx = c.f[20], Azx = c.f[21], Azy = c.f[22];
+        float const vx = 1.5f * (3.0f * xxx + Ayx + Azx);
+        float const vy = 1.5f * (3.0f * yyy + Azy + Axy);
+        float const vz = 1.5f * (3.0f * zzz + Axz + Ayz);
+        out[6] = vx - 7.5f * xxx;
+        out[7] = vy - 7.5f * yyy;
+        out[8] = vz - 7.5f * zzz;
+        out[9] = vy - 7.5f * Axy;
+        out[10] = vz - 7.5f * Axz;
+        out[11] = vx - 7.5f * Ayx;
+        out[12] = vz - 7.5f * Ayz;
+        out[13] = vx - 7.5f * Azx;
+        out[14] = vy - 7.5f * Azy;
+        out[15] = -7.5f * spn;
+    }
+}
+
 struct moment_params {
     node4 const *nodes;
     std::uint64_t node_count;
@@ -581,9 +615,8 @@ __device__ inline void finish_node(moment_params const &p, std::uint32_t n) {
             q[5] = c.f[5];
             q[6] = c.f[6];
             q[7] = __uint_as_float(qref);
-#pragma unroll
-            for (int f = 7; f < F; ++f)
-                q[f + 1] = c.f[f];
+            if constexpr (Order >= 1)
+                fold_far_field_coefficients<Order>(c, q + 8);
             if (init)
                 accumulate(total, m);
             else
