@@ -117,9 +117,11 @@ __device__ __forceinline__ float solid_angle_guarded(float ax, float ay, float a
     return 2.0f * atan2f(num, den);
 }
 
-// Compensated near field (Taylor traversal): the triple product and the atan2 denominator from
-// compensated (Dot2) dot products; pairs whose numerator and denominator are both below
-// threshold * |a||b||c| take the FP64 evaluation.
+// Compensated near field (Taylor traversal): the two atan2 arguments -- the triple product
+// a.(e1 x e2) and the denominator's sum |a||b||c| + (a.b)|c| + (a.c)|b| + (b.c)|a| -- as compensated
+// (Dot2) sums; pairs whose numerator and denominator are both below threshold * |a||b||c| take the
+// FP64 evaluation. The rounding of b = a + e1 and c = a + e2 themselves bounds what compensation can
+// recover (the FP64 branch removes it), so the three inner dot products stay plain FP32.
 __device__ __forceinline__ float solid_angle_comp(float ax, float ay, float az, float e1x, float e1y,
                                                   float e1z, float e2x, float e2y, float e2z, float nx,
                                                   float ny, float nz, float threshold,
@@ -132,11 +134,10 @@ __device__ __forceinline__ float solid_angle_comp(float ax, float ay, float az, 
     float const lc = sqrtf(cx * cx + cy * cy + cz * cz);
     if (la == 0.0f || lb == 0.0f || lc == 0.0f)
         return 0.0f;
-    // the triple product and the denominator cancel near the triangle's plane and edges
     float const num = dot3_comp(ax, ay, az, nx, ny, nz);
-    float const ab = dot3_comp(ax, ay, az, bx, by, bz);
-    float const ac = dot3_comp(ax, ay, az, cx, cy, cz);
-    float const bc = dot3_comp(bx, by, bz, cx, cy, cz);
+    float const ab = ax * bx + ay * by + az * bz;
+    float const ac = ax * cx + ay * cy + az * cz;
+    float const bc = bx * cx + by * cy + bz * cz;
     float const labc = la * lb * lc;
     float const den = labc + dot3_comp(ab, ac, bc, lc, lb, la);
     float const scale = labc;
