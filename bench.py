@@ -4,7 +4,7 @@ Workload (per rank): displaced UV sphere 1024 x 512 (1,046,528 triangles, seed 2
 queries (half uniform in the 1.2x bounding box, half at surface samples offset along the normal by
 N(0, 1e-3), seed 2 + rank), H-PLOC (radius 8) BVH4, Taylor order 2 at accuracy scale 3.5,
 compensated near field. A step is one call of the Taylor batch on the 10M device-resident queries
-(Morton ordering of the queries included).
+(Hilbert ordering of the queries included).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -297,7 +297,7 @@ def config_dict(args, mesh) -> dict:
     return {"workload": "displaced UV sphere 1024x512 (1,046,528 tris), 10M mixed queries per GPU",
             "triangles": int(mesh["i0"].size), "queries_per_gpu": int(args.queries), "builder": "hploc r=8",
             "width": 4, "taylor_order": int(args.order), "accuracy_scale": float(args.beta),
-            "near_field": "compensated fp32 (fp64 on flagged triangles)", "query_order": "morton-sorted in batch",
+            "near_field": "compensated fp32 (fp64 on flagged triangles)", "query_order": "hilbert-sorted in batch",
             "l2": "flushed (256 MiB write) between timed steps", "parallelism": f"replicas x{args.gpus}"}
 
 

@@ -117,7 +117,7 @@ typedef struct gwnb_moment4_f32 {
 typedef struct gwnb_taylor_options {
     int block_size;     /* smallgwn gwn_query_batch_config::block_size (0 = default 256)        */
     int stack_capacity; /* smallgwn gwn_query_batch_config::stack_capacity (0 = default 64)     */
-    int sort_queries;   /* 1: Morton-order the batch internally for traversal coherence          */
+    int sort_queries;   /* 1: Hilbert-order the batch internally for traversal coherence         */
     int near_precision; /* GWNB_NEAR_PLAIN or GWNB_NEAR_COMPENSATED                               */
     float fp64_threshold; /* compensated mode: |den| < threshold * |a||b||c| takes the FP64 path */
     int per_thread;       /* 0: warp-cooperative traversal (default); 1: one traversal per thread  */
@@ -280,7 +280,7 @@ GWNB_API int gwnb_winding_exact_geometry_fp64(const gwnb_geometry_f32 *geometry,
                                               const float *query_y, const float *query_z, double *output,
                                               uint64_t count, gwnb_stream_t stream);
 
-/* Morton order of a query batch relative to the BVH root bounds: order[i] is the index of the
+/* Hilbert order of a query batch relative to the BVH root bounds: order[i] is the index of the
  * i-th query in traversal-coherent order (the permutation the Taylor batch applies internally when
  * sort_queries is set). No smallgwn counterpart. */
 GWNB_API int gwnb_query_order_f32(const gwnb_bvh4_f32 *bvh, const float *query_x, const float *query_y,
@@ -370,7 +370,7 @@ typedef struct gwnb_batch_tuning {
     int refit_block;  /* threads per block of the refit launches                                  */
     int query_block;  /* threads per block of the query launch (multiple of 32, at most 256)      */
     int per_thread;   /* 0: 32 queries per warp walk one traversal; 1: one traversal per thread   */
-    int sorted;       /* 1: traverse each mesh's queries in Morton order (computed at creation)   */
+    int sorted;       /* 1: traverse each mesh's queries in Hilbert order (computed at creation)  */
     int grid_scale;   /* persistent grids of SMs x grid_scale blocks                              */
     float frame_ms;   /* measured frame time of this shape (output of tuning)                     */
 } gwnb_batch_tuning;

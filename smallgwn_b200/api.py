@@ -403,7 +403,7 @@ def exact_winding_fp64(geometry: gwn_geometry_object, qx, qy, qz, out, stream=No
 
 
 def query_order(bvh: gwn_bvh4_object, qx, qy, qz, order, stream=None) -> gwn_status:
-    """Traversal-coherent (Morton) order of a query batch; `order` is an int32 CUDA tensor."""
+    """Traversal-coherent (Hilbert) order of a query batch; `order` is an int32 CUDA tensor."""
     rc = _lib.load().gwnb_query_order_f32(C.byref(bvh._view), _ptr(qx), _ptr(qy), _ptr(qz), _numel(qx), _ptr(order),
                                           _stream(stream))
     return _status(rc)

@@ -8,8 +8,8 @@
 // synchronizes, so applications capture frames (with their own vertex updates) in a CUDA graph.
 //
 // The autotuner times candidate launch shapes -- refit block size; query block size, traversal
-// form (a warp of 32 Morton-adjacent queries walking one traversal, or one traversal per thread),
-// Morton-ordered or input order, persistent grid size -- on the batch itself and keeps the fastest.
+// form (a warp of 32 Hilbert-adjacent queries walking one traversal, or one traversal per thread),
+// Hilbert-ordered or input order, persistent grid size -- on the batch itself and keeps the fastest.
 #include "gwnb_internal.cuh"
 
 #include <algorithm>

@@ -82,7 +82,8 @@ __host__ __device__ inline std::uint64_t make_ref(std::uint64_t offset, std::uin
 
 // Query sidecar (one record per wide node, written by the moment refit). Per child slot the
 // record holds float4 blocks: a = (P.xyz, r2) with r2 < 0 marking an invalid slot,
-// b = (N.xyz, ref bits), then the order-1/2 coefficients. ref bits: internal child -> node index;
+// b = (N.xyz, ref bits), then the folded far-field coefficients (order 1: the 6 entries of
+// M' = trace(M) I - 3M; order 2: those 6 and the 10 of the cubic form K). ref bits: internal child -> node index;
 // leaf -> 0x80000000 | first sorted triangle; bit 30 set when the leaf holds more than one
 // triangle (its count is then read from the per-node count table).
 constexpr std::uint32_t k_qref_leaf = 0x80000000u;
@@ -285,16 +286,16 @@ struct batch_query_state {
     int order = 0;
     int near_mode = GWNB_NEAR_PLAIN;
     std::uint64_t warps = 0;               // total warps of the slot space
-    void *meshes = nullptr;                // device per-mesh traversal descriptors (Morton order)
+    void *meshes = nullptr;                // device per-mesh traversal descriptors (Hilbert order)
     void *meshes_unsorted = nullptr;       // the same in input order
     std::uint64_t *warp_begin = nullptr;   // mesh_count + 1 warp offsets
-    std::uint32_t *orders = nullptr;       // per-mesh Morton orders, concatenated
+    std::uint32_t *orders = nullptr;       // per-mesh Hilbert orders, concatenated
     int max_stack_bound = 0;
 };
 struct batch_query_config {
     int block;      // threads per block (multiple of 32)
     int per_thread; // 0: warp-cooperative traversal, 1: one traversal per thread
-    int sorted;     // 1: traverse in each mesh's Morton order
+    int sorted;     // 1: traverse in each mesh's Hilbert order
     int grid_scale; // persistent grid = SMs x grid_scale blocks
 };
 int batch_query_prepare(taylor_request const *meshes, std::uint32_t n, batch_query_state *st, cudaStream_t s);

@@ -12,7 +12,7 @@
 // traversal order, acceptance test and far-field terms follow detail/gwn_query_winding_impl.cuh
 // :101-374 (accept a child iff |q-P|^2 > 0, |q-P|^2 > r^2 beta^2 and the expansion is finite;
 // otherwise enter internal children, the last directly and the others through the stack, and sum
-// leaf triangles exactly). Differences: the batch is Morton-ordered internally for coherence, node
+// leaf triangles exactly). Differences: the batch is Hilbert-ordered internally for coherence, node
 // data comes from a per-node query sidecar with 128-bit loads, the stack lives in shared memory,
 // and stack overflow writes NaN and raises a device error bit instead of trapping.
 #include "gwnb_field.cuh"
@@ -418,7 +418,7 @@ __global__ void __launch_bounds__(256) k_taylor(taylor_params p) {
         p, static_cast<std::uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x, s_stack + threadIdx.x);
 }
 
-// Warp-cooperative traversal: the 32 lanes of a warp (32 Morton-adjacent queries) walk one
+// Warp-cooperative traversal: the 32 lanes of a warp (32 Hilbert-adjacent queries) walk one
 // depth-first traversal together. Every stack entry carries the mask of lanes that still need the
 // subtree; a lane leaves a subtree as soon as it accepts the child's far field. Node records are
 // loaded with warp-uniform addresses and the stack lives in the lanes' registers (lane k holds
@@ -935,7 +935,7 @@ int radix_sort_pairs_u32_in_scratch(std::uint32_t const *keys_in, std::uint32_t 
                                     int key_bits, std::uint32_t *keys_tmp, std::uint32_t *vals_tmp,
                                     std::uint32_t *words, cudaStream_t s, unsigned int *status);
 
-// The Taylor batch of taylor_batch() with every temporary in caller-provided scratch (query Morton
+// The Taylor batch of taylor_batch() with every temporary in caller-provided scratch (query Hilbert
 // codes, sorted codes, the order, the sort's ping-pong buffers and its words); allocates nothing.
 int taylor_batch_in_scratch(taylor_request const &r, std::uint32_t *scratch, std::uint64_t capacity,
                             cudaStream_t s) {
