@@ -47,15 +47,18 @@ def parse() -> argparse.Namespace:
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="taylor", choices=["taylor", "adjoint", "precision", "exact", "batched"],
+    ap.add_argument("--workload", default="taylor",
+                    choices=["taylor", "adjoint", "precision", "exact", "batched", "distance", "ray"],
                     help="taylor: the headline (1M-triangle sphere, 10M queries); adjoint: forward + backward "
                          "on the 159k-triangle soup; precision: 8.4M-triangle sphere, 100M near-surface queries "
-                         "in 16M chunks; exact: brute-force exact batch on the small icosphere")
+                         "in 16M chunks; exact: brute-force exact batch on the small icosphere; distance / ray: "
+                         "unsigned distance / ray first hit on the 1M-triangle sphere, 10M queries / rays")
     ap.add_argument("--queries", type=int, default=N_QUERIES)
     ap.add_argument("--order", type=int, default=ORDER)
     ap.add_argument("--beta", type=float, default=BETA)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--profile", choices=["taylor", "taylor-plain", "taylor-thread", "build", "exact", "adjoint"],
+    ap.add_argument("--profile", choices=["taylor", "taylor-plain", "taylor-thread", "build", "exact", "adjoint",
+                                          "distance", "ray"],
                     default=None,
                     help="run one small workload for a profiler (no JSON): 2 launches of the kernel")
     return ap.parse_args()
@@ -72,6 +75,30 @@ def run_profile(args) -> None:
     from smallgwn_b200 import api, meshes
 
     stream = torch.cuda.current_stream()
+    if args.profile in ("distance", "ray"):
+        # the traversal kernel over inputs already in the batch's own order, twice
+        ray = args.profile == "ray"
+        mesh = meshes.sphere_mesh()
+        inp = spatial_inputs(args.profile, mesh, args.queries)
+        geo = g.gwn_geometry_object()
+        assert g.gwn_upload_geometry(geo, mesh["x"], mesh["y"], mesh["z"], mesh["i0"], mesh["i1"], mesh["i2"]).is_ok()
+        bvh = g.gwn_bvh4_object()
+        assert g.gwn_build_bvh(geo, bvh, g.gwn_bvh_build_options(method=0, hploc_search_radius=8)).is_ok()
+        din = [torch.from_numpy(v).to("cuda") for v in inp]
+        order = torch.empty(args.queries, dtype=torch.int32, device="cuda")
+        assert (api.ray_order(bvh, *din, order) if ray else api.query_order(bvh, *din, order)).is_ok()
+        sin = [d[order.long()].contiguous() for d in din]
+        if ray:
+            out = torch.empty((args.queries, api.RAY_HIT_WORDS), dtype=torch.int32, device="cuda")
+            for _ in range(2):
+                assert g.gwn_compute_ray_first_hit_batch(bvh, *sin, out, sort_queries=False).is_ok()
+        else:
+            out = torch.empty(args.queries, device="cuda")
+            for _ in range(2):
+                assert g.gwn_compute_unsigned_distance_batch(bvh, *sin, out, sort_queries=False).is_ok()
+        torch.cuda.synchronize()
+        print(f"profile {args.profile} ok")
+        return
     if args.profile == "adjoint":
         # forward + backward (order 1) on the 159k-triangle soup, twice
         mesh = meshes.soup_mesh(316, seed=3)
@@ -767,6 +794,209 @@ def run_exact_workload(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+def profiled_spatial_traffic(kind: str, n: int) -> float | None:
+    """DRAM bytes of one distance / ray traversal launch over this workload, from the committed ncu
+    summary (profiles/spatial_<kind>_sphere1m.md); None when not recorded."""
+    path = ROOT / "profiles" / f"spatial_{kind}_sphere1m.md"
+    if not path.exists():
+        return None
+    key = f"dram_bytes_per_launch[{kind},queries={n}]:"
+    for line in path.read_text().splitlines():
+        if line.startswith(key):
+            return float(line.split(":", 1)[1].split()[0])
+    return None
+
+
+def spatial_inputs(kind: str, mesh, n: int, seed: int = 2):
+    """Query points (distance) or ray origins and directions (ray): the mixed queries of the
+    headline workload, directions N(0, I) (seed 3)."""
+    from smallgwn_b200 import meshes
+
+    q = [np.ascontiguousarray(v) for v in meshes.mixed_queries(mesh, n, seed=seed)]
+    if kind == "ray":
+        d = np.random.default_rng(seed + 1).normal(size=(3, n)).astype(np.float32)
+        q += [np.ascontiguousarray(v) for v in d]
+    return q
+
+
+def run_spatial_workload(args) -> None:
+    """Unsigned distance (`--workload distance`) or ray first hit (`--workload ray`) on the headline
+    mesh: displaced UV sphere 1024 x 512 (1,046,528 triangles), H-PLOC r = 8 BVH4, 10M queries per
+    GPU -- the mixed query points (distance: unbounded culling band) or rays from those points in
+    N(0, I) directions (ray: t in [0, inf)). A step is one batch call on device-resident inputs
+    (Hilbert ordering included; rays by origin and direction). Every result of a 20k subset is
+    compared with the oracle's canonical traversal of the same tree (bit for bit). smallgwn's own
+    kernel (oracle/_ref, when built) is timed on the same inputs for context."""
+    import torch
+
+    import oracle
+    import smallgwn_b200 as g
+    from smallgwn_b200 import api, meshes
+
+    kind = args.workload
+    ray = kind == "ray"
+    rank, world, dist = dist_setup(args.gpus)
+    dev = torch.cuda.current_device()
+    stream = torch.cuda.current_stream()
+    mesh = meshes.sphere_mesh()
+    n = args.queries
+    inp = spatial_inputs(kind, mesh, n, seed=2 + rank)
+    geo = g.gwn_geometry_object()
+    assert g.gwn_upload_geometry(geo, mesh["x"], mesh["y"], mesh["z"], mesh["i0"], mesh["i1"], mesh["i2"], stream).is_ok()
+    bvh = g.gwn_bvh4_object()
+    assert g.gwn_build_bvh(geo, bvh, g.gwn_bvh_build_options(method=0, hploc_search_radius=8), stream).is_ok()
+    din = [torch.from_numpy(v).to("cuda") for v in inp]
+    out = (torch.empty((n, api.RAY_HIT_WORDS), dtype=torch.int32, device="cuda") if ray
+           else torch.empty(n, dtype=torch.float32, device="cuda"))
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+    def call(xs, o, sort=True):
+        if ray:
+            st = g.gwn_compute_ray_first_hit_batch(bvh, *xs, o, stream=stream, sort_queries=sort)
+        else:
+            st = g.gwn_compute_unsigned_distance_batch(bvh, *xs, o, stream=stream, sort_queries=sort)
+        assert st.is_ok(), st.message
+
+    for _ in range(args.warmup):
+        call(din, out)
+    torch.cuda.synchronize()
+    events = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(dev) as clocks:
+        for e0, e1 in events:
+            flush.fill_(1)
+            e0.record(stream)
+            call(din, out)
+            e1.record(stream)
+        torch.cuda.synchronize()
+    total_ms = sum(a.elapsed_time(b) for a, b in events)
+    t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    total_ms = float(t.item())
+    value = world * n * args.steps / (total_ms / 1e3)
+
+    # end to end: pinned host inputs in, results back to pinned host memory, every step
+    hin = [torch.from_numpy(v).pin_memory() for v in inp]
+    hout = torch.empty(out.shape, dtype=out.dtype).pin_memory()
+    dbuf = [torch.empty(n, dtype=torch.float32, device="cuda") for _ in inp]
+
+    def e2e_step():
+        for d, h in zip(dbuf, hin):
+            d.copy_(h, non_blocking=True)
+        call(dbuf, out)
+        hout.copy_(out, non_blocking=True)
+
+    e2e = timed_steps(e2e_step, max(3, min(args.steps, 10)), 1, stream, flush)
+    e2e_value = world * n / (float(np.mean(e2e)) / 1e3)
+
+    # the traversal kernel alone over pre-ordered inputs, and the bytes it touches
+    order = torch.empty(n, dtype=torch.int32, device="cuda")
+    if ray:
+        assert api.ray_order(bvh, *din, order, stream).is_ok()
+    else:
+        assert api.query_order(bvh, *din, order, stream).is_ok()
+    idx = order.long()
+    sin = [d[idx].contiguous() for d in din]
+    kt = timed_steps(lambda: call(sin, out, sort=False), 3, 1, stream, flush)
+    kernel_ms = float(np.mean(kt))
+    sn = torch.empty(n, dtype=torch.int32, device="cuda")
+    stri = torch.empty_like(sn)
+    if ray:
+        assert api.spatial_traversal_stats(bvh, *din[:3], sn, stri, *din[3:], stream=stream).is_ok()
+    else:
+        assert api.spatial_traversal_stats(bvh, *din, sn, stri, stream=stream).is_ok()
+    torch.cuda.synchronize()
+    nodes_entered = float(sn.double().sum().item())
+    tris_tested = float(stri.double().sum().item())
+    in_bytes, out_bytes = (24, 32) if ray else (12, 4)
+    alg_bytes = n * (in_bytes + out_bytes) + nodes_entered * 128 + tris_tested * 48
+    pk = peaks()
+    achieved = alg_bytes / (kernel_ms / 1e3) / 1e9
+
+    # parity on a subset against the oracle's traversal of the same tree
+    call(din, out)
+    torch.cuda.synchronize()
+    bh = api.bvh_host_arrays(bvh)
+    sub = slice(0, min(20_000, n))
+    if ray:
+        got = api.ray_hit_records(out[sub])
+        ref = oracle.ray_first_hit(bh["nodes"], bh["triangles"], bh["primitive_indices"], bh["root_reference"],
+                                   *[v[sub] for v in inp])
+        mismatches = int(np.count_nonzero(got.view(np.uint8).reshape(-1, 32) != ref.view(np.uint8).reshape(-1, 32)))
+        hit_frac = float((api.ray_hit_records(out)["status"] == 1).mean())
+    else:
+        got = out[sub].cpu().numpy()
+        ref = oracle.unsigned_distance(bh["nodes"], bh["triangles"], bh["root_reference"], *[v[sub] for v in inp])
+        mismatches = int(np.count_nonzero(got != ref))
+        hit_frac = None
+
+    ref_gpu = None
+    if oracle.ref_lib() is not None:
+        r = oracle.Reference(mesh)
+        r.build(method=0, radius=8)
+        m = min(n, 2_000_000)
+        ms = r.time_spatial(*[v[:m] for v in inp[:3]], dirs=[v[:m] for v in inp[3:]] if ray else None, iters=3)
+        ref_gpu = m / (ms / 1e3)
+        r.close()
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        threads = oracle.max_threads()
+        done, chunk, t0 = 0, (200_000 if ray else 20_000), time.perf_counter()
+        while time.perf_counter() - t0 < 10.0 and done < n:
+            s = slice(done, min(done + chunk, n))
+            if ray:
+                oracle.ray_first_hit(bh["nodes"], bh["triangles"], bh["primitive_indices"], bh["root_reference"],
+                                     *[v[s] for v in inp], threads=threads)
+            else:
+                oracle.unsigned_distance(bh["nodes"], bh["triangles"], bh["root_reference"], *[v[s] for v in inp],
+                                         threads=threads)
+            done = s.stop
+        dt = time.perf_counter() - t0
+        cpu = {"value": done / dt, "unit": "queries/s", "cores": threads, "kind": "port",
+               "sample": f"{done} of the {n} {'rays' if ray else 'queries'} in {dt:.1f} s (canonical traversal)"}
+
+    if rank == 0:
+        unit = "rays/s" if ray else "queries/s"
+        if cpu is not None:
+            cpu["unit"] = unit
+        line = {
+            "metric": ("Ray first-hit rays/s at 1M tris" if ray else "Unsigned-distance queries/s at 1M tris"),
+            "value": value, "unit": unit, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic",
+            "config": {"workload": ("displaced UV sphere 1024x512 (1,046,528 tris), 10M rays per GPU from the mixed "
+                                    "query points, N(0, I) directions, t in [0, inf)" if ray else
+                                    "displaced UV sphere 1024x512 (1,046,528 tris), 10M mixed queries per GPU, "
+                                    "unbounded culling band"),
+                       "builder": "hploc r=8", "width": 4,
+                       "order": "hilbert(origin) + octahedral direction cell" if ray else "hilbert-sorted in batch",
+                       "l2": "flushed (256 MiB write) between timed steps", "parallelism": f"replicas x{world}",
+                       "subset_mismatches_vs_oracle": mismatches, "parity_subset": int(sub.stop),
+                       "mean_nodes_entered": nodes_entered / n, "mean_triangles_tested": tris_tested / n,
+                       "hit_fraction": hit_frac, "smallgwn_gpu_kernel_per_s": ref_gpu},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
+                         "frac": achieved / pk["hbm_gbs"], "peak_source": pk["source"],
+                         "traffic": profiled_spatial_traffic(kind, n),
+                         "kernel": ("k_ray" if ray else "k_distance") + " (pre-ordered inputs)",
+                         "kernel_ms": kernel_ms, "algorithmic_bytes": alg_bytes,
+                         "bytes_model": f"{in_bytes} B in + {out_bytes} B out per query + 128 B per node entered + "
+                                        "48 B per triangle tested"},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": unit, "h2d_bytes_per_step": 4 * len(inp) * n,
+                    "d2h_bytes_per_step": out_bytes * n},
+            "gpu_launches": 7 * args.steps,  # codes, histogram, 4 digit passes, traversal
+            "clocks": clocks.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def main() -> None:
     args = parse()
     if args.profile is not None:
@@ -777,7 +1007,8 @@ def main() -> None:
         return
     if args.workload != "taylor":
         {"adjoint": run_adjoint_workload, "precision": run_precision_workload, "exact": run_exact_workload,
-         "batched": run_batched_workload}[args.workload](args)
+         "batched": run_batched_workload, "distance": run_spatial_workload,
+         "ray": run_spatial_workload}[args.workload](args)
         return
     import torch
 

@@ -280,6 +280,70 @@ GWNB_API int gwnb_winding_exact_geometry_fp64(const gwnb_geometry_f32 *geometry,
                                               const float *query_y, const float *query_z, double *output,
                                               uint64_t count, gwnb_stream_t stream);
 
+/* ---- spatial queries (include/gwn/gwn_query.cuh:63-282) ----------------------------------- */
+
+/* Launch options of the distance and ray batches (smallgwn gwn_query_batch_config plus ordering). */
+typedef struct gwnb_spatial_options {
+    int block_size;     /* gwn_query_batch_config::block_size, multiple of 32 (0 = default 256)  */
+    int stack_capacity; /* gwn_query_batch_config::stack_capacity (0 = default 64)               */
+    int sort_queries;   /* 1: traverse in Hilbert order of the query points / ray origins        */
+} gwnb_spatial_options;
+
+/* gwn::gwn_ray_first_hit_status (include/gwn/gwn_query.cuh:63-68). */
+enum { GWNB_RAY_MISS = 0, GWNB_RAY_HIT = 1, GWNB_RAY_OVERFLOW = 2 };
+
+/* Layout of gwn::gwn_ray_first_hit_result<float, uint32_t> (include/gwn/gwn_query.cuh:70-96),
+ * 32 bytes. A miss has t = -1, primitive_id = 0xffffffff and zero weights and normal. */
+typedef struct gwnb_ray_hit_f32 {
+    float t;                  /* ray parameter of the hit                                   */
+    float u, v;               /* barycentric weights of the second and third vertex          */
+    float geometric_normal_x; /* unnormalized oriented geometric normal                      */
+    float geometric_normal_y;
+    float geometric_normal_z;
+    uint32_t primitive_id; /* original mesh primitive id                                   */
+    uint8_t status;        /* GWNB_RAY_MISS, GWNB_RAY_HIT or GWNB_RAY_OVERFLOW             */
+    uint8_t padding[3];    /* zero                                                          */
+} gwnb_ray_hit_f32;
+
+/* Replaces gwn::gwn_compute_unsigned_distance_batch<Config> (include/gwn/gwn_query.cuh:135-183,
+ * detail/gwn_query_distance_impl.cuh:40-160): distance of each query point to the nearest
+ * triangle, at most `culling_band` (negative bands clamp to 0, infinity searches unbounded).
+ * `options` may be NULL (block 256, stack 64, input order). Asynchronous. A traversal that would
+ * overflow its stack writes NaN and sets the BVH's device error word instead of trapping. */
+GWNB_API int gwnb_unsigned_distance_batch_f32(const gwnb_bvh4_f32 *bvh, const float *query_x,
+                                              const float *query_y, const float *query_z, float *output,
+                                              uint64_t count, float culling_band,
+                                              const gwnb_spatial_options *options, gwnb_stream_t stream);
+
+/* Replaces gwn::gwn_compute_ray_first_hit_batch<Config> (include/gwn/gwn_query.cuh:214-282,
+ * detail/gwn_query_ray_impl.cuh:376-560): nearest hit of each ray on the closed interval
+ * [t_min, t_max] (t_max >= t_min required). Among hits at the same t the lower primitive id is
+ * reported. Asynchronous. */
+GWNB_API int gwnb_ray_first_hit_batch_f32(const gwnb_bvh4_f32 *bvh, const float *ray_origin_x,
+                                          const float *ray_origin_y, const float *ray_origin_z,
+                                          const float *ray_dir_x, const float *ray_dir_y, const float *ray_dir_z,
+                                          gwnb_ray_hit_f32 *output, uint64_t count, float t_min, float t_max,
+                                          const gwnb_spatial_options *options, gwnb_stream_t stream);
+
+enum { GWNB_SPATIAL_DISTANCE = 0, GWNB_SPATIAL_RAY = 1 };
+
+/* Per-query traversal statistics of a distance (kind GWNB_SPATIAL_DISTANCE; dir_* unused) or ray
+ * batch (GWNB_SPATIAL_RAY): internal nodes entered and triangles tested, two uint32 arrays of
+ * `count` (diagnostics behind the benchmark's bytes model). No smallgwn counterpart. */
+GWNB_API int gwnb_spatial_stats_f32(const gwnb_bvh4_f32 *bvh, int kind, const float *query_x, const float *query_y,
+                                    const float *query_z, const float *dir_x, const float *dir_y,
+                                    const float *dir_z, uint64_t count, float culling_band, float t_min,
+                                    float t_max, uint32_t *nodes_entered, uint32_t *triangles_tested,
+                                    gwnb_stream_t stream);
+
+/* Traversal order of a ray batch (the permutation the ray batch applies when sort_queries is
+ * set): rays sorted by the octahedral cell of their direction, then by the Hilbert index of their
+ * origin relative to the BVH root bounds. order[i] is the index of the i-th ray. No smallgwn
+ * counterpart. */
+GWNB_API int gwnb_ray_order_f32(const gwnb_bvh4_f32 *bvh, const float *ray_origin_x, const float *ray_origin_y,
+                                const float *ray_origin_z, const float *ray_dir_x, const float *ray_dir_y,
+                                const float *ray_dir_z, uint64_t count, uint32_t *order, gwnb_stream_t stream);
+
 /* Hilbert order of a query batch relative to the BVH root bounds: order[i] is the index of the
  * i-th query in traversal-coherent order (the permutation the Taylor batch applies internally when
  * sort_queries is set). No smallgwn counterpart. */

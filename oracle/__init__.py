@@ -241,6 +241,86 @@ def mesh_distance(mesh: dict, qx, qy, qz, threads: int = 0) -> np.ndarray:
     return out
 
 
+def unsigned_distance(nodes: np.ndarray, tris: np.ndarray, root_ref: int, qx, qy, qz,
+                      culling_band: float = float("inf"), stack_capacity: int = 256, threads: int = 0,
+                      stats: bool = False):
+    """gwn_unsigned_distance_impl restated (detail/gwn_query_distance_impl.cuh:40-160); with stats
+    also (internal nodes entered, triangles evaluated) per query."""
+    threads = threads or max_threads()
+    nd = np.ascontiguousarray(nodes.reshape(-1, 4), dtype=NODE_DTYPE)
+    t = np.ascontiguousarray(tris, np.float32)
+    q = [_f32(v) for v in (qx, qy, qz)]
+    n = q[0].size
+    out = np.empty(n, np.float32)
+    st = np.zeros((n, 2), np.uint32) if stats else None
+    lib().oracle_unsigned_distance(_p(nd), C.c_uint64(nd.shape[0]), _p(t), C.c_uint64(t.shape[0]),
+                                   C.c_uint64(root_ref), _p(q[0]), _p(q[1]), _p(q[2]), C.c_uint64(n),
+                                   C.c_float(culling_band), C.c_int(stack_capacity), _p(out), _p(st),
+                                   C.c_int(threads))
+    return (out, st) if stats else out
+
+
+def distance_brute(tris: np.ndarray, qx, qy, qz, culling_band: float = float("inf"), threads: int = 0) -> np.ndarray:
+    """Minimum over every record of the same float point-triangle distance (no traversal)."""
+    threads = threads or max_threads()
+    t = np.ascontiguousarray(tris, np.float32)
+    q = [_f32(v) for v in (qx, qy, qz)]
+    out = np.empty(q[0].size, np.float32)
+    lib().oracle_distance_brute(_p(t), C.c_uint64(t.shape[0]), _p(q[0]), _p(q[1]), _p(q[2]), C.c_uint64(out.size),
+                                C.c_float(culling_band), _p(out), C.c_int(threads))
+    return out
+
+
+# gwn::gwn_ray_first_hit_result<float, uint32_t> (include/gwn/gwn_query.cuh:63-96), 32 bytes.
+HIT_DTYPE = np.dtype([("t", np.float32), ("u", np.float32), ("v", np.float32), ("nx", np.float32),
+                      ("ny", np.float32), ("nz", np.float32), ("primitive_id", np.uint32), ("status", np.uint8),
+                      ("pad", np.uint8, (3,))])
+
+
+def ray_first_hit(nodes: np.ndarray, tris: np.ndarray, primitive_indices: np.ndarray, root_ref: int, ox, oy, oz,
+                  dx, dy, dz, t_min: float = 0.0, t_max: float = float("inf"), stack_capacity: int = 256,
+                  threads: int = 0, stats: bool = False):
+    """gwn_ray_first_hit_impl restated (detail/gwn_query_ray_impl.cuh:376-560, canonical traversal;
+    equal-t hits resolved to the lower original primitive id)."""
+    threads = threads or max_threads()
+    nd = np.ascontiguousarray(nodes.reshape(-1, 4), dtype=NODE_DTYPE)
+    t = np.ascontiguousarray(tris, np.float32)
+    prim = _u32(primitive_indices)
+    r = [_f32(v) for v in (ox, oy, oz, dx, dy, dz)]
+    n = r[0].size
+    out = np.zeros(n, HIT_DTYPE)
+    st = np.zeros((n, 2), np.uint32) if stats else None
+    lib().oracle_ray_first_hit(_p(nd), C.c_uint64(nd.shape[0]), _p(t), _p(prim), C.c_uint64(t.shape[0]),
+                               C.c_uint64(root_ref), *[_p(v) for v in r], C.c_uint64(n), C.c_float(t_min),
+                               C.c_float(t_max), C.c_int(stack_capacity), _p(out), _p(st), C.c_int(threads))
+    return (out, st) if stats else out
+
+
+def ray_brute(tris: np.ndarray, primitive_indices: np.ndarray, ox, oy, oz, dx, dy, dz, t_min: float = 0.0,
+              t_max: float = float("inf"), threads: int = 0) -> np.ndarray:
+    """Nearest hit over every record with the same per-triangle test and tie rule (no traversal)."""
+    threads = threads or max_threads()
+    t = np.ascontiguousarray(tris, np.float32)
+    prim = _u32(primitive_indices)
+    r = [_f32(v) for v in (ox, oy, oz, dx, dy, dz)]
+    out = np.zeros(r[0].size, HIT_DTYPE)
+    lib().oracle_ray_brute(_p(t), _p(prim), C.c_uint64(t.shape[0]), *[_p(v) for v in r], C.c_uint64(out.size),
+                           C.c_float(t_min), C.c_float(t_max), _p(out), C.c_int(threads))
+    return out
+
+
+def build_bvh(mesh: dict, method: str = "lbvh", bits: int = 64, radius: int = 8) -> dict:
+    """build_lbvh, or the same pipeline with H-PLOC (radius) in place of Karras' builder."""
+    if method == "lbvh":
+        return build_lbvh(mesh, bits)
+    out = build_lbvh(mesh, bits)
+    if out["sorted_ids"].size > 1:
+        bn, bb, root = hploc(out["sorted_codes"], bits, out["sorted_aabbs"], radius)
+        nodes, ib, pb = collapse(bn, bb, out["sorted_aabbs"], root)
+        out.update(binary_nodes=bn, binary_bounds=bb, nodes=nodes, internal_stack_bound=ib, packed_stack_bound=pb)
+    return out
+
+
 def build_lbvh(mesh: dict, bits: int = 64) -> dict:
     """Full CPU pipeline: Morton, stable sort, Karras, bounds, BVH4 collapse, triangle records."""
     aabbs, codes, scene = morton(mesh, bits)
@@ -359,6 +439,32 @@ class Reference:
         ms = C.c_float()
         self._check(self.lib.ref_time_exact(self.h, _p(q[0]), _p(q[1]), _p(q[2]), C.c_uint64(q[0].size),
                                             C.c_int(warmup), C.c_int(iters), C.byref(ms)))
+        return float(ms.value)
+
+    def distance(self, qx, qy, qz, culling_band: float = float("inf")) -> np.ndarray:
+        q = [_f32(v) for v in (qx, qy, qz)]
+        out = np.empty(q[0].size, np.float32)
+        self._check(self.lib.ref_distance(self.h, _p(q[0]), _p(q[1]), _p(q[2]), _p(out), C.c_uint64(out.size),
+                                          C.c_float(culling_band)))
+        return out
+
+    def ray(self, ox, oy, oz, dx, dy, dz, t_min: float = 0.0, t_max: float = float("inf")) -> np.ndarray:
+        r = [_f32(v) for v in (ox, oy, oz, dx, dy, dz)]
+        out = np.zeros(r[0].size, HIT_DTYPE)
+        self._check(self.lib.ref_ray(self.h, *[_p(v) for v in r], _p(out), C.c_uint64(out.size), C.c_float(t_min),
+                                     C.c_float(t_max)))
+        return out
+
+    def time_spatial(self, qx, qy, qz, dirs=None, culling_band: float = float("inf"), t_min: float = 0.0,
+                     t_max: float = float("inf"), warmup: int = 2, iters: int = 5) -> float:
+        """Average ms of smallgwn's distance batch (dirs None) or ray batch on device-resident inputs."""
+        q = [_f32(v) for v in (qx, qy, qz)]
+        d = [_f32(v) for v in dirs] if dirs is not None else q
+        ms = C.c_float()
+        self._check(self.lib.ref_time_spatial(self.h, C.c_int(1 if dirs is not None else 0), *[_p(v) for v in q],
+                                              *[_p(v) for v in d], C.c_uint64(q[0].size), C.c_float(culling_band),
+                                              C.c_float(t_min), C.c_float(t_max), C.c_int(warmup), C.c_int(iters),
+                                              C.byref(ms)))
         return float(ms.value)
 
     def time_build(self, method: int, radius: int, bits: int, iters: int) -> float:

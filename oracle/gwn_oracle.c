@@ -1265,3 +1265,519 @@ void oracle_taylor_frozen_f64(int order, const o_node4 *nodes, uint64_t nn, uint
     free(slots);
     free(pend);
 }
+
+/* ---------------------------------------------------------------------------------------------- */
+/* Spatial queries on the BVH4: unsigned point-to-mesh distance and ray first hit.                 */
+/* smallgwn's formulas and its canonical near-first traversal (detail/gwn_query_distance_impl.cuh, */
+/* detail/gwn_query_ray_impl.cuh), with every dot product, cross product, multiply-add and slab    */
+/* bound fused in one fixed pattern (fmaf) that the CUDA kernels use identically; smallgwn leaves   */
+/* that contraction to its compiler.                                                             */
+
+#include <float.h>
+
+typedef struct {
+    float x, y, z;
+} o_v3;
+
+static inline o_v3 v3(float x, float y, float z) {
+    o_v3 r = {x, y, z};
+    return r;
+}
+static inline o_v3 v3_add(o_v3 a, o_v3 b) { return v3(a.x + b.x, a.y + b.y, a.z + b.z); }
+static inline o_v3 v3_sub(o_v3 a, o_v3 b) { return v3(a.x - b.x, a.y - b.y, a.z - b.z); }
+/* a * s + c, fused per component */
+static inline o_v3 v3_fma(o_v3 a, float s, o_v3 c) { return v3(fmaf(a.x, s, c.x), fmaf(a.y, s, c.y), fmaf(a.z, s, c.z)); }
+/* detail/gwn_query_vec3_impl.cuh:109-121, fused: x*x' first, then y and z accumulated */
+static inline float v3_dot(o_v3 a, o_v3 b) { return fmaf(a.z, b.z, fmaf(a.y, b.y, a.x * b.x)); }
+static inline o_v3 v3_cross(o_v3 a, o_v3 b) {
+    return v3(fmaf(a.y, b.z, -(a.z * b.y)), fmaf(a.z, b.x, -(a.x * b.z)), fmaf(a.x, b.y, -(a.y * b.x)));
+}
+/* a * b - c * d with the second product rounded first */
+static inline float o_dop(float a, float b, float c, float d) { return fmaf(a, b, -(c * d)); }
+
+/* Vertices of a leaf-ordered record, reconstructed as v0 + e (detail/gwn_query_distance_impl.cuh:20-33). */
+static inline void record_vertices(const o_tri *t, o_v3 *a, o_v3 *b, o_v3 *c) {
+    *a = v3(t->v0_x, t->v0_y, t->v0_z);
+    *b = v3(t->v0_x + t->e1_x, t->v0_y + t->e1_y, t->v0_z + t->e1_z);
+    *c = v3(t->v0_x + t->e2_x, t->v0_y + t->e2_y, t->v0_z + t->e2_z);
+}
+
+/* Squared point-triangle distance, Voronoi-region tests (detail/gwn_query_geometry_impl.cuh:49-100). */
+static float o_point_tri_d2(o_v3 p, o_v3 a, o_v3 b, o_v3 c) {
+    o_v3 const ab = v3_sub(b, a), ac = v3_sub(c, a), ap = v3_sub(p, a);
+    float const d1 = v3_dot(ab, ap), d2 = v3_dot(ac, ap);
+    if (d1 <= 0.0f && d2 <= 0.0f)
+        return v3_dot(ap, ap);
+    o_v3 const bp = v3_sub(p, b);
+    float const d3 = v3_dot(ab, bp), d4 = v3_dot(ac, bp);
+    if (d3 >= 0.0f && d4 <= d3)
+        return v3_dot(bp, bp);
+    float const vc = o_dop(d1, d4, d3, d2);
+    if (vc <= 0.0f && d1 >= 0.0f && d3 <= 0.0f) {
+        float const v = d1 / (d1 - d3);
+        o_v3 const q = v3_sub(p, v3_fma(ab, v, a));
+        return v3_dot(q, q);
+    }
+    o_v3 const cp = v3_sub(p, c);
+    float const d5 = v3_dot(ab, cp), d6 = v3_dot(ac, cp);
+    if (d6 >= 0.0f && d5 <= d6)
+        return v3_dot(cp, cp);
+    float const vb = o_dop(d5, d2, d1, d6);
+    if (vb <= 0.0f && d2 >= 0.0f && d6 <= 0.0f) {
+        float const w = d2 / (d2 - d6);
+        o_v3 const q = v3_sub(p, v3_fma(ac, w, a));
+        return v3_dot(q, q);
+    }
+    float const va = o_dop(d3, d6, d5, d4);
+    if (va <= 0.0f && (d4 - d3) >= 0.0f && (d5 - d6) >= 0.0f) {
+        float const w = (d4 - d3) / ((d4 - d3) + (d5 - d6));
+        o_v3 const q = v3_sub(p, v3_fma(v3_sub(c, b), w, b));
+        return v3_dot(q, q);
+    }
+    float const denom = 1.0f / (va + vb + vc);
+    float const v = vb * denom, w = vc * denom;
+    o_v3 const q = v3_sub(p, v3_fma(ac, w, v3_fma(ab, v, a)));
+    return v3_dot(q, q);
+}
+
+/* std::max(v, 0) with its NaN behaviour (the first operand is returned when unordered). */
+static inline float o_pos(float v) { return (v < 0.0f) ? 0.0f : v; }
+
+/* detail/gwn_query_geometry_impl.cuh:104-114 */
+static inline float o_aabb_d2(float qx, float qy, float qz, const o_aabb *b) {
+    float const dx = o_pos(b->min_x - qx) + o_pos(qx - b->max_x);
+    float const dy = o_pos(b->min_y - qy) + o_pos(qy - b->max_y);
+    float const dz = o_pos(b->min_z - qz) + o_pos(qz - b->max_z);
+    return fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+}
+
+/* One query of detail/gwn_query_distance_impl.cuh:40-160: near-first descent with the culling band
+ * as initial bound, leaf children visited inside their node before internal children are queued,
+ * an early return of 0 once a triangle touches the query. Stack overflow returns NaN. */
+static float o_distance_one(const o_node4 *nodes, uint64_t nn, const o_tri *tris, uint64_t nt, uint64_t root_ref,
+                            float qx, float qy, float qz, float culling_band, int cap, uint32_t *st) {
+    o_v3 const p = v3(qx, qy, qz);
+    float const band = (culling_band < 0.0f) ? 0.0f : culling_band;
+    float best = band * band;
+    uint32_t n_nodes = 0, n_tris = 0;
+    uint64_t stack[256];
+    int sp = 0;
+    uint64_t ref = root_ref;
+    float result = NAN;
+    int done = 0;
+#define VISIT_LEAF(R, ALIVE)                                                                        \
+    do {                                                                                            \
+        for (uint32_t k_ = 0; k_ < ref_count(R); ++k_) {                                            \
+            uint64_t const si_ = ref_offset(R) + k_;                                                \
+            if (si_ >= nt)                                                                          \
+                continue;                                                                           \
+            o_v3 a_, b_, c_;                                                                        \
+            record_vertices(&tris[si_], &a_, &b_, &c_);                                             \
+            float const d2_ = o_point_tri_d2(p, a_, b_, c_);                                        \
+            ++n_tris;                                                                               \
+            if (d2_ < best)                                                                         \
+                best = d2_;                                                                         \
+        }                                                                                           \
+        ALIVE = best > 0.0f;                                                                        \
+    } while (0)
+    for (;;) {
+        uint64_t next = 0;
+        if (ref_leaf(ref)) {
+            int alive;
+            VISIT_LEAF(ref, alive);
+            if (!alive) {
+                result = 0.0f;
+                done = 1;
+                break;
+            }
+        } else if (ref_internal(ref) && ref_offset(ref) < nn) {
+            ++n_nodes;
+            const o_node4 *nd = &nodes[ref_offset(ref)];
+            float cd[4];
+            uint64_t cr[4];
+            int cnt = 0;
+            for (int s = 0; s < 4; ++s) {
+                if (!ref_valid(nd->c[s].reference))
+                    continue;
+                float const d2 = o_aabb_d2(qx, qy, qz, &nd->c[s].bounds);
+                if (d2 >= best)
+                    continue;
+                cd[cnt] = d2;
+                cr[cnt] = nd->c[s].reference;
+                ++cnt;
+            }
+            for (int s = cnt; s < 4; ++s) {
+                cd[s] = INFINITY;
+                cr[s] = 0;
+            }
+#define CSWAP(L, R)                                                                                 \
+    if (cd[L] > cd[R]) {                                                                            \
+        float tf_ = cd[L];                                                                          \
+        cd[L] = cd[R];                                                                              \
+        cd[R] = tf_;                                                                                \
+        uint64_t tr_ = cr[L];                                                                       \
+        cr[L] = cr[R];                                                                              \
+        cr[R] = tr_;                                                                                \
+    }
+            CSWAP(0, 1) CSWAP(2, 3) CSWAP(0, 2) CSWAP(1, 3) CSWAP(1, 2)
+            int stop = 0;
+            for (int s = 0; s < cnt && !stop; ++s) {
+                if (ref_leaf(cr[s]) && cd[s] < best) {
+                    int alive;
+                    VISIT_LEAF(cr[s], alive);
+                    if (!alive)
+                        stop = 1;
+                }
+            }
+            if (stop) {
+                result = 0.0f;
+                done = 1;
+                break;
+            }
+            for (int s = cnt - 1; s >= 0; --s) {
+                if (!ref_internal(cr[s]) || cd[s] >= best)
+                    continue;
+                if (next != 0) {
+                    if (sp >= cap) {
+                        done = 1;
+                        break;
+                    }
+                    stack[sp++] = next;
+                }
+                next = cr[s];
+            }
+            if (done)
+                break; /* overflow: result stays NaN */
+        }
+        if (next != 0) {
+            ref = next;
+            continue;
+        }
+        if (sp == 0)
+            break;
+        ref = stack[--sp];
+    }
+#undef VISIT_LEAF
+    if (!done)
+        result = sqrtf(best);
+    if (st) {
+        st[0] = n_nodes;
+        st[1] = n_tris;
+    }
+    return result;
+}
+
+void oracle_unsigned_distance(const o_node4 *nodes, uint64_t nn, const o_tri *tris, uint64_t nt, uint64_t root_ref,
+                              const float *qx, const float *qy, const float *qz, uint64_t n, float culling_band,
+                              int stack_capacity, float *out, uint32_t *stats, int threads) {
+    int const cap = stack_capacity > 256 ? 256 : stack_capacity;
+#pragma omp parallel for schedule(dynamic, 64) num_threads(threads)
+    for (int64_t i = 0; i < (int64_t)n; ++i)
+        out[i] = o_distance_one(nodes, nn, tris, nt, root_ref, qx[i], qy[i], qz[i], culling_band, cap,
+                                stats ? stats + 2 * i : NULL);
+}
+
+/* Brute force over every record (same per-triangle arithmetic, no pruning): the minimum squared
+ * distance under the band, then its square root. */
+void oracle_distance_brute(const o_tri *tris, uint64_t nt, const float *qx, const float *qy, const float *qz,
+                           uint64_t n, float culling_band, float *out, int threads) {
+    float const band = (culling_band < 0.0f) ? 0.0f : culling_band;
+#pragma omp parallel for schedule(dynamic, 64) num_threads(threads)
+    for (int64_t i = 0; i < (int64_t)n; ++i) {
+        o_v3 const p = v3(qx[i], qy[i], qz[i]);
+        float best = band * band;
+        for (uint64_t t = 0; t < nt; ++t) {
+            o_v3 a, b, c;
+            record_vertices(&tris[t], &a, &b, &c);
+            float const d2 = o_point_tri_d2(p, a, b, c);
+            if (d2 < best)
+                best = d2;
+        }
+        out[i] = sqrtf(best);
+    }
+}
+
+/* Ray first-hit record; same layout as gwn::gwn_ray_first_hit_result<float, uint32_t>
+ * (include/gwn/gwn_query.cuh:63-96): 32 bytes. status 0 miss, 1 hit, 2 overflow. */
+typedef struct {
+    float t, u, v, nx, ny, nz;
+    uint32_t primitive_id;
+    uint8_t status;
+    uint8_t pad[3];
+} o_hit;
+
+/* detail/gwn_query_ray_impl.cuh:63-81: reciprocal direction, parallel axes flagged; here also
+ * -o * inv per axis so that a slab bound is one fused lo * inv - o * inv. */
+typedef struct {
+    float inv[3], noi[3];
+    int zero[3];
+} o_raydir;
+
+static o_raydir o_make_raydir(const float o[3], float dx, float dy, float dz) {
+    o_raydir r;
+    float const d[3] = {dx, dy, dz};
+    for (int k = 0; k < 3; ++k) {
+        r.zero[k] = d[k] == 0.0f;
+        r.inv[k] = r.zero[k] ? 0.0f : 1.0f / d[k];
+        r.noi[k] = -(o[k] * r.inv[k]);
+    }
+    return r;
+}
+
+/* detail/gwn_query_ray_impl.cuh:84-139 and :259-271: closed slab test against [t_min, t_max]; a
+ * parallel axis is a containment test, the others bound the interval (std::min / std::max operand
+ * order, axes folded x, y, z). t_max >= t_min holds for every call (the running best never drops
+ * below t_min). */
+static int o_ray_box(const float o[3], const o_raydir *rd, const o_aabb *b, float t_min, float t_max, float *t_near_out) {
+    float t_near = t_min, t_far = t_max;
+    float const lo[3] = {b->min_x, b->min_y, b->min_z};
+    float const hi[3] = {b->max_x, b->max_y, b->max_z};
+    for (int k = 0; k < 3; ++k) {
+        if (rd->zero[k]) {
+            if (!(o[k] >= lo[k] && o[k] <= hi[k]))
+                return 0;
+            continue;
+        }
+        float const t0 = fmaf(lo[k], rd->inv[k], rd->noi[k]);
+        float const t1 = fmaf(hi[k], rd->inv[k], rd->noi[k]);
+        t_near = fmax_r(t_near, fmin_r(t0, t1));
+        t_far = fmin_r(t_far, fmax_r(t0, t1));
+    }
+    if (!(t_near <= t_far))
+        return 0;
+    *t_near_out = t_near;
+    return 1;
+}
+
+/* detail/gwn_query_ray_impl.cuh:142-171: component-wise stable cross products. */
+static o_v3 o_stable_normal(o_v3 a, o_v3 b, o_v3 c) {
+    float const abx = a.z * b.y, aby = a.x * b.z, abz = a.y * b.x;
+    float const bcx = b.z * c.y, bcy = b.x * c.z, bcz = b.y * c.x;
+    o_v3 const cab = v3(fmaf(a.y, b.z, -abx), fmaf(a.z, b.x, -aby), fmaf(a.x, b.y, -abz));
+    o_v3 n = v3(fmaf(b.y, c.z, -bcx), fmaf(b.z, c.x, -bcy), fmaf(b.x, c.y, -bcz));
+    if (fabsf(abx) < fabsf(bcx))
+        n.x = cab.x;
+    if (fabsf(aby) < fabsf(bcy))
+        n.y = cab.y;
+    if (fabsf(abz) < fabsf(bcz))
+        n.z = cab.z;
+    return n;
+}
+
+/* detail/gwn_query_ray_impl.cuh:174-238: oriented Pluecker edge functions. */
+static int o_ray_tri(o_v3 o, o_v3 d, o_v3 v0, o_v3 v1, o_v3 v2, float t_min, float t_max, float *t_out,
+                     float *u_out, float *v_out, o_v3 *n_out) {
+    o_v3 const p0 = v3_sub(v0, o), p1 = v3_sub(v1, o), p2 = v3_sub(v2, o);
+    o_v3 const e0 = v3_sub(p2, p0), e1 = v3_sub(p0, p1), e2 = v3_sub(p1, p2);
+    float const u = v3_dot(v3_cross(e0, v3_add(p2, p0)), d);
+    float const v = v3_dot(v3_cross(e1, v3_add(p0, p1)), d);
+    float const w = v3_dot(v3_cross(e2, v3_add(p1, p2)), d);
+    float const uvw = u + v + w;
+    float const eps = FLT_EPSILON * fabsf(uvw);
+    float const mn = fmin_r(u, fmin_r(v, w));
+    float const mx = fmax_r(u, fmax_r(v, w));
+    if (!(mn >= -eps || mx <= eps))
+        return 0;
+    o_v3 const ng = o_stable_normal(e0, e1, e2);
+    float const den = 2.0f * v3_dot(ng, d);
+    if (den == 0.0f)
+        return 0;
+    float const t = (2.0f * v3_dot(p0, ng)) / den;
+    if (!(t_min <= t && t <= t_max))
+        return 0;
+    if (fabsf(uvw) >= FLT_MIN) {
+        float const inv = 1.0f / uvw;
+        *u_out = u * inv;
+        *v_out = v * inv;
+    } else {
+        if (uvw == 0.0f)
+            return 0;
+        *u_out = u / uvw;
+        *v_out = v / uvw;
+    }
+    *t_out = t;
+    *n_out = ng;
+    return 1;
+}
+
+typedef struct {
+    float t, u, v;
+    o_v3 n;
+    uint32_t id;
+    int found;
+} o_best;
+
+/* A candidate replaces the best hit when it is nearer, or equally near with a lower original
+ * primitive id (smallgwn keeps the first one its traversal meets, detail/gwn_query_ray_impl.cuh:
+ * 436-437; the id rule makes the result independent of the traversal order). */
+static void o_ray_leaf(const o_tri *tris, const uint32_t *prim, uint64_t nt, uint64_t r, o_v3 o, o_v3 d, float t_min,
+                       o_best *best, uint32_t *n_tris) {
+    for (uint32_t k = 0; k < ref_count(r); ++k) {
+        uint64_t const si = ref_offset(r) + k;
+        if (si >= nt)
+            continue;
+        o_v3 a, b, c, n;
+        record_vertices(&tris[si], &a, &b, &c);
+        float t, u, v;
+        ++*n_tris;
+        if (!o_ray_tri(o, d, a, b, c, t_min, best->t, &t, &u, &v, &n))
+            continue;
+        uint32_t const id = prim[si];
+        if (best->found && !(t < best->t || (t == best->t && id < best->id)))
+            continue;
+        best->t = t;
+        best->u = u;
+        best->v = v;
+        best->n = n;
+        best->id = id;
+        best->found = 1;
+    }
+}
+
+/* One ray of detail/gwn_query_ray_impl.cuh:376-560 (canonical traversal). */
+static o_hit o_ray_one(const o_node4 *nodes, uint64_t nn, const o_tri *tris, const uint32_t *prim, uint64_t nt,
+                       uint64_t root_ref, const float org[3], const float dir[3], float t_min, float t_max, int cap,
+                       uint32_t *st) {
+    o_hit h;
+    memset(&h, 0, sizeof(h));
+    h.t = -1.0f;
+    h.primitive_id = 0xffffffffu;
+    uint32_t n_nodes = 0, n_tris = 0;
+    float const len2 = dir[0] * dir[0] + dir[1] * dir[1] + dir[2] * dir[2];
+    if (!(len2 > 0.0f)) {
+        if (st)
+            st[0] = st[1] = 0;
+        return h;
+    }
+    o_v3 const o = v3(org[0], org[1], org[2]), d = v3(dir[0], dir[1], dir[2]);
+    o_raydir const rd = o_make_raydir(org, dir[0], dir[1], dir[2]);
+    o_best best;
+    memset(&best, 0, sizeof(best));
+    best.t = t_max;
+    uint64_t stack[256];
+    int sp = 0, overflow = 0;
+    uint64_t ref = root_ref;
+    for (;;) {
+        uint64_t next = 0;
+        if (ref_leaf(ref)) {
+            o_ray_leaf(tris, prim, nt, ref, o, d, t_min, &best, &n_tris);
+        } else if (ref_internal(ref) && ref_offset(ref) < nn) {
+            ++n_nodes;
+            const o_node4 *nd = &nodes[ref_offset(ref)];
+            float et[4];
+            uint64_t cr[4];
+            int cnt = 0;
+            for (int s = 0; s < 4; ++s) {
+                if (!ref_valid(nd->c[s].reference))
+                    continue;
+                float tn;
+                if (!o_ray_box(org, &rd, &nd->c[s].bounds, t_min, best.t, &tn))
+                    continue;
+                et[cnt] = tn;
+                cr[cnt] = nd->c[s].reference;
+                ++cnt;
+            }
+            for (int s = cnt; s < 4; ++s) {
+                et[s] = INFINITY;
+                cr[s] = 0;
+            }
+#define ESWAP(L, R)                                                                                 \
+    if (et[L] > et[R]) {                                                                            \
+        float tf_ = et[L];                                                                          \
+        et[L] = et[R];                                                                              \
+        et[R] = tf_;                                                                                \
+        uint64_t tr_ = cr[L];                                                                       \
+        cr[L] = cr[R];                                                                              \
+        cr[R] = tr_;                                                                                \
+    }
+            ESWAP(0, 1) ESWAP(2, 3) ESWAP(0, 2) ESWAP(1, 3) ESWAP(1, 2)
+            for (int s = 0; s < cnt; ++s)
+                if (ref_leaf(cr[s]) && et[s] <= best.t)
+                    o_ray_leaf(tris, prim, nt, cr[s], o, d, t_min, &best, &n_tris);
+            for (int s = cnt - 1; s >= 0; --s) {
+                if (!ref_internal(cr[s]) || et[s] > best.t)
+                    continue;
+                if (next != 0) {
+                    if (sp >= cap) {
+                        overflow = 1;
+                        break;
+                    }
+                    stack[sp++] = next;
+                }
+                next = cr[s];
+            }
+            if (overflow)
+                break;
+        }
+        if (next != 0) {
+            ref = next;
+            continue;
+        }
+        if (sp == 0)
+            break;
+        ref = stack[--sp];
+    }
+    if (best.found) {
+        h.t = best.t;
+        h.u = best.u;
+        h.v = best.v;
+        h.nx = best.n.x;
+        h.ny = best.n.y;
+        h.nz = best.n.z;
+        h.primitive_id = best.id;
+        h.status = 1;
+    }
+    if (overflow)
+        h.status = 2;
+    if (st) {
+        st[0] = n_nodes;
+        st[1] = n_tris;
+    }
+    return h;
+}
+
+void oracle_ray_first_hit(const o_node4 *nodes, uint64_t nn, const o_tri *tris, const uint32_t *prim, uint64_t nt,
+                          uint64_t root_ref, const float *ox, const float *oy, const float *oz, const float *dx,
+                          const float *dy, const float *dz, uint64_t n, float t_min, float t_max, int stack_capacity,
+                          o_hit *out, uint32_t *stats, int threads) {
+    int const cap = stack_capacity > 256 ? 256 : stack_capacity;
+#pragma omp parallel for schedule(dynamic, 64) num_threads(threads)
+    for (int64_t i = 0; i < (int64_t)n; ++i) {
+        float const o[3] = {ox[i], oy[i], oz[i]}, d[3] = {dx[i], dy[i], dz[i]};
+        out[i] = o_ray_one(nodes, nn, tris, prim, nt, root_ref, o, d, t_min, t_max, cap, stats ? stats + 2 * i : NULL);
+    }
+}
+
+/* Brute force over every record with the same per-triangle test and tie rule. */
+void oracle_ray_brute(const o_tri *tris, const uint32_t *prim, uint64_t nt, const float *ox, const float *oy,
+                      const float *oz, const float *dx, const float *dy, const float *dz, uint64_t n, float t_min,
+                      float t_max, o_hit *out, int threads) {
+#pragma omp parallel for schedule(dynamic, 64) num_threads(threads)
+    for (int64_t i = 0; i < (int64_t)n; ++i) {
+        o_hit h;
+        memset(&h, 0, sizeof(h));
+        h.t = -1.0f;
+        h.primitive_id = 0xffffffffu;
+        float const len2 = dx[i] * dx[i] + dy[i] * dy[i] + dz[i] * dz[i];
+        if (len2 > 0.0f) {
+            o_v3 const o = v3(ox[i], oy[i], oz[i]), d = v3(dx[i], dy[i], dz[i]);
+            o_best best;
+            memset(&best, 0, sizeof(best));
+            best.t = t_max;
+            uint32_t dummy = 0;
+            for (uint64_t t = 0; t < nt; ++t)
+                o_ray_leaf(tris, prim, nt, make_ref(t, 1), o, d, t_min, &best, &dummy);
+            if (best.found) {
+                h.t = best.t;
+                h.u = best.u;
+                h.v = best.v;
+                h.nx = best.n.x;
+                h.ny = best.n.y;
+                h.nz = best.n.z;
+                h.primitive_id = best.id;
+                h.status = 1;
+            }
+        }
+        out[i] = h;
+    }
+}

@@ -102,6 +102,38 @@ gwn::gwn_status taylor_order(ctx &c, int order, dbuf<float> &x, dbuf<float> &y, 
     return taylor_any<2>(c, c.m2, x, y, z, o, beta);
 }
 
+using ray_result = gwn::gwn_ray_first_hit_result<Real, Index>;
+static_assert(sizeof(ray_result) == 32, "smallgwn's ray record is 32 bytes");
+
+template <gwn::gwn_query_batch_config Config>
+gwn::gwn_status distance_cfg(ctx &c, dbuf<float> &x, dbuf<float> &y, dbuf<float> &z, dbuf<float> &o, float band) {
+    return gwn::gwn_compute_unsigned_distance_batch<Config, 4, Real, Index, no_trap>(
+        c.bvh, gwn::gwn_device_span<float const>(x.p, x.n), gwn::gwn_device_span<float const>(y.p, y.n),
+        gwn::gwn_device_span<float const>(z.p, z.n), gwn::gwn_device_span<float>(o.p, o.n), band,
+        gwn::gwn_default_stream(), no_trap{});
+}
+
+gwn::gwn_status distance_any(ctx &c, dbuf<float> &x, dbuf<float> &y, dbuf<float> &z, dbuf<float> &o, float band) {
+    if (c.bvh.accessor().internal_stack_bound <= 64)
+        return distance_cfg<gwn::gwn_query_batch_config{256, 64}>(c, x, y, z, o, band);
+    return distance_cfg<gwn::gwn_query_batch_config{256, 256}>(c, x, y, z, o, band);
+}
+
+template <gwn::gwn_query_batch_config Config>
+gwn::gwn_status ray_cfg(ctx &c, dbuf<float> *r, dbuf<ray_result> &o, float t_min, float t_max) {
+    return gwn::gwn_compute_ray_first_hit_batch<Config, 4, Real, Index, no_trap>(
+        c.bvh, gwn::gwn_device_span<float const>(r[0].p, r[0].n), gwn::gwn_device_span<float const>(r[1].p, r[1].n),
+        gwn::gwn_device_span<float const>(r[2].p, r[2].n), gwn::gwn_device_span<float const>(r[3].p, r[3].n),
+        gwn::gwn_device_span<float const>(r[4].p, r[4].n), gwn::gwn_device_span<float const>(r[5].p, r[5].n),
+        gwn::gwn_device_span<ray_result>(o.p, o.n), t_min, t_max, gwn::gwn_default_stream(), no_trap{});
+}
+
+gwn::gwn_status ray_any(ctx &c, dbuf<float> *r, dbuf<ray_result> &o, float t_min, float t_max) {
+    if (c.bvh.accessor().internal_stack_bound <= 64)
+        return ray_cfg<gwn::gwn_query_batch_config{256, 64}>(c, r, o, t_min, t_max);
+    return ray_cfg<gwn::gwn_query_batch_config{256, 256}>(c, r, o, t_min, t_max);
+}
+
 } // namespace
 
 extern "C" {
@@ -424,6 +456,67 @@ int ref_exact_f64(const double *x, const double *y, const double *z, uint64_t nv
         return fail(s);
     cudaDeviceSynchronize();
     o.to_host(out);
+    return static_cast<int>(cudaGetLastError());
+}
+
+// smallgwn's unsigned-distance batch (gwn_compute_unsigned_distance_batch) of a host batch.
+int ref_distance(void *p, const float *qx, const float *qy, const float *qz, float *out, uint64_t n, float band) {
+    auto &c = *static_cast<ctx *>(p);
+    dbuf<float> x(qx, n), y(qy, n), z(qz, n), o(n);
+    auto s = distance_any(c, x, y, z, o, band);
+    if (!s.is_ok())
+        return fail(s);
+    cudaDeviceSynchronize();
+    o.to_host(out);
+    return static_cast<int>(cudaGetLastError());
+}
+
+// smallgwn's ray first-hit batch (gwn_compute_ray_first_hit_batch) of a host batch; `out` receives
+// n 32-byte gwn_ray_first_hit_result records.
+int ref_ray(void *p, const float *ox, const float *oy, const float *oz, const float *dx, const float *dy,
+            const float *dz, void *out, uint64_t n, float t_min, float t_max) {
+    auto &c = *static_cast<ctx *>(p);
+    dbuf<float> r[6] = {dbuf<float>(ox, n), dbuf<float>(oy, n), dbuf<float>(oz, n),
+                        dbuf<float>(dx, n), dbuf<float>(dy, n), dbuf<float>(dz, n)};
+    dbuf<ray_result> o(n);
+    auto s = ray_any(c, r, o, t_min, t_max);
+    if (!s.is_ok())
+        return fail(s);
+    cudaDeviceSynchronize();
+    o.to_host(static_cast<ray_result *>(out));
+    return static_cast<int>(cudaGetLastError());
+}
+
+// Times `iters` distance (kind 0) or ray (kind 1) batches on device-resident inputs after `warmup`
+// untimed ones; average ms per batch.
+int ref_time_spatial(void *p, int kind, const float *qx, const float *qy, const float *qz, const float *dx,
+                     const float *dy, const float *dz, uint64_t n, float band, float t_min, float t_max, int warmup,
+                     int iters, float *ms) {
+    auto &c = *static_cast<ctx *>(p);
+    dbuf<float> r[6] = {dbuf<float>(qx, n), dbuf<float>(qy, n), dbuf<float>(qz, n),
+                        dbuf<float>(kind ? dx : qx, n), dbuf<float>(kind ? dy : qy, n), dbuf<float>(kind ? dz : qz, n)};
+    dbuf<float> od(kind ? 0 : n);
+    dbuf<ray_result> orr(kind ? n : 0);
+    auto run = [&]() { return kind ? ray_any(c, r, orr, t_min, t_max) : distance_any(c, r[0], r[1], r[2], od, band); };
+    for (int i = 0; i < warmup; ++i) {
+        auto s = run();
+        if (!s.is_ok())
+            return fail(s);
+    }
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaDeviceSynchronize();
+    cudaEventRecord(e0, cudaStreamLegacy);
+    for (int i = 0; i < iters; ++i)
+        (void)run();
+    cudaEventRecord(e1, cudaStreamLegacy);
+    cudaEventSynchronize(e1);
+    float t = 0;
+    cudaEventElapsedTime(&t, e0, e1);
+    *ms = t / static_cast<float>(iters > 0 ? iters : 1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
     return static_cast<int>(cudaGetLastError());
 }
 

@@ -11,6 +11,8 @@ from .api import (  # noqa: F401
     gwn_bvh_build_method,
     gwn_bvh_build_options,
     gwn_build_bvh,
+    gwn_compute_ray_first_hit_batch,
+    gwn_compute_unsigned_distance_batch,
     gwn_compute_winding_gradient_taylor_batch,
     gwn_compute_winding_number_exact_batch,
     gwn_compute_winding_number_taylor_batch,
@@ -18,6 +20,7 @@ from .api import (  # noqa: F401
     gwn_geometry_object,
     gwn_geometry_view,
     gwn_query_batch_config,
+    gwn_ray_first_hit_status,
     gwn_refit_bvh,
     gwn_refit_bvh_moment,
     gwn_status,
@@ -27,4 +30,5 @@ from .api import (  # noqa: F401
     gwn_winding_taylor_backward,
     gwn_winding_taylor_forward,
     near_precision,
+    ray_hit_records,
 )

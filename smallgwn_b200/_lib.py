@@ -25,6 +25,13 @@ GWNB_BATCH_REFIT = 1
 GWNB_BATCH_MOMENTS = 2
 GWNB_BATCH_QUERY = 4
 
+GWNB_RAY_MISS = 0
+GWNB_RAY_HIT = 1
+GWNB_RAY_OVERFLOW = 2
+
+GWNB_SPATIAL_DISTANCE = 0
+GWNB_SPATIAL_RAY = 1
+
 
 class aabb_f32(C.Structure):
     _fields_ = [(n, C.c_float) for n in ("min_x", "min_y", "min_z", "max_x", "max_y", "max_z")]
@@ -125,11 +132,28 @@ class batch_tuning(C.Structure):
     ]
 
 
+class spatial_options(C.Structure):
+    _fields_ = [
+        ("block_size", C.c_int),
+        ("stack_capacity", C.c_int),
+        ("sort_queries", C.c_int),
+    ]
+
+
+class ray_hit_f32(C.Structure):
+    _fields_ = [
+        ("t", C.c_float), ("u", C.c_float), ("v", C.c_float),
+        ("geometric_normal_x", C.c_float), ("geometric_normal_y", C.c_float), ("geometric_normal_z", C.c_float),
+        ("primitive_id", C.c_uint32), ("status", C.c_uint8), ("padding", C.c_uint8 * 3),
+    ]
+
+
 class binary_node(C.Structure):
     _fields_ = [(n, C.c_uint32) for n in ("left_index", "left_kind", "right_index", "right_kind")]
 
 
 assert C.sizeof(child_f32) == 32 and C.sizeof(node4_f32) == 128 and C.sizeof(triangle_f32) == 36
+assert C.sizeof(ray_hit_f32) == 32
 
 P = C.c_void_p
 U64 = C.c_uint64
@@ -169,6 +193,13 @@ SIGNATURES: dict[str, tuple] = {
     "gwnb_bvh4_fp64_fallback_count": (I, [C.POINTER(bvh4_f32), C.POINTER(U64), P]),
     "gwnb_winding_exact_geometry_fp64": (I, [C.POINTER(geometry_f32), P, P, P, P, U64, P]),
     "gwnb_query_order_f32": (I, [C.POINTER(bvh4_f32), P, P, P, U64, P, P]),
+    "gwnb_unsigned_distance_batch_f32": (
+        I, [C.POINTER(bvh4_f32), P, P, P, P, U64, F, C.POINTER(spatial_options), P]),
+    "gwnb_ray_first_hit_batch_f32": (
+        I, [C.POINTER(bvh4_f32), P, P, P, P, P, P, P, U64, F, F, C.POINTER(spatial_options), P]),
+    "gwnb_ray_order_f32": (I, [C.POINTER(bvh4_f32), P, P, P, P, P, P, U64, P, P]),
+    "gwnb_spatial_stats_f32": (
+        I, [C.POINTER(bvh4_f32), I, P, P, P, P, P, P, U64, F, F, F, P, P, P]),
     "gwnb_winding_taylor_batch_noalloc_f32": (
         I, [C.POINTER(bvh4_f32), C.POINTER(moment4_f32), P, P, P, P, U64, F, C.POINTER(taylor_options), P]),
     "gwnb_winding_taylor_forward_f32": (

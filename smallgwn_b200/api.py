@@ -402,6 +402,94 @@ def exact_winding_fp64(geometry: gwn_geometry_object, qx, qy, qz, out, stream=No
     return _status(rc)
 
 
+# gwn::gwn_ray_first_hit_status / gwn_ray_first_hit_result<float, uint32_t>
+# (include/gwn/gwn_query.cuh:63-96): one 32-byte record per ray.
+class gwn_ray_first_hit_status(enum.IntEnum):
+    k_miss = _lib.GWNB_RAY_MISS
+    k_hit = _lib.GWNB_RAY_HIT
+    k_overflow = _lib.GWNB_RAY_OVERFLOW
+
+
+RAY_HIT_DTYPE = np.dtype([("t", np.float32), ("u", np.float32), ("v", np.float32),
+                          ("geometric_normal_x", np.float32), ("geometric_normal_y", np.float32),
+                          ("geometric_normal_z", np.float32), ("primitive_id", np.uint32), ("status", np.uint8),
+                          ("padding", np.uint8, (3,))])
+RAY_HIT_WORDS = 8  # four-byte words per record
+
+
+def ray_hit_records(out) -> np.ndarray:
+    """Host copy of a ray-hit output buffer (CUDA tensor of 8 four-byte words per ray) as a numpy
+    structured array with the fields of gwn_ray_first_hit_result."""
+    raw = out.detach().contiguous().view(-1).cpu().numpy().view(np.uint8)
+    return raw.view(RAY_HIT_DTYPE)
+
+
+def _ray_rows(out) -> int:
+    n = _numel(out)
+    if out is not None and out.element_size() != 4:
+        raise ValueError("ray-hit output must be a tensor of 4-byte words (8 per ray)")
+    return n // RAY_HIT_WORDS
+
+
+def _spatial_options(config: gwn_query_batch_config, sort_queries: bool):
+    return _lib.spatial_options(int(config.block_size), int(config.stack_capacity), 1 if sort_queries else 0)
+
+
+def gwn_compute_unsigned_distance_batch(bvh: gwn_bvh4_object, qx, qy, qz, out, culling_band: float = float("inf"),
+                                        stream=None, config: gwn_query_batch_config = gwn_query_batch_config(),
+                                        sort_queries: bool = False) -> gwn_status:
+    """Unsigned point-to-mesh distances of a device batch, at most ``culling_band`` (asynchronous).
+    ``sort_queries`` traverses in Hilbert order of the points (results stay at input positions)."""
+    if not bvh.has_data():
+        return gwn_status(gwn_error.invalid_argument, "BVH object contains no queryable data.")
+    bad = _check_spans(qx, qy, qz, out)
+    if bad is not None:
+        return bad
+    opt = _spatial_options(config, sort_queries)
+    rc = _lib.load().gwnb_unsigned_distance_batch_f32(C.byref(bvh._view), _ptr(qx), _ptr(qy), _ptr(qz), _ptr(out),
+                                                      _numel(out), float(culling_band), C.byref(opt), _stream(stream))
+    return _status(rc)
+
+
+def gwn_compute_ray_first_hit_batch(bvh: gwn_bvh4_object, ox, oy, oz, dx, dy, dz, out, t_min: float = 0.0,
+                                    t_max: float = float("inf"), stream=None,
+                                    config: gwn_query_batch_config = gwn_query_batch_config(),
+                                    sort_queries: bool = False) -> gwn_status:
+    """Nearest ray-triangle hits of a device batch on [t_min, t_max] (asynchronous). ``out`` holds
+    8 four-byte words per ray (a gwn_ray_first_hit_result record; see ray_hit_records)."""
+    if not bvh.has_data():
+        return gwn_status(gwn_error.invalid_argument, "BVH object contains no queryable data.")
+    n = _numel(ox)
+    if any(_numel(a) != n for a in (oy, oz, dx, dy, dz)) or _ray_rows(out) != n or \
+            (out is not None and _numel(out) % RAY_HIT_WORDS != 0):
+        return gwn_status(gwn_error.invalid_argument, "ray first-hit: mismatched span sizes")
+    opt = _spatial_options(config, sort_queries)
+    rc = _lib.load().gwnb_ray_first_hit_batch_f32(C.byref(bvh._view), _ptr(ox), _ptr(oy), _ptr(oz), _ptr(dx),
+                                                  _ptr(dy), _ptr(dz), _ptr(out), n, float(t_min), float(t_max),
+                                                  C.byref(opt), _stream(stream))
+    return _status(rc)
+
+
+def spatial_traversal_stats(bvh: gwn_bvh4_object, qx, qy, qz, nodes, tris, dx=None, dy=None, dz=None,
+                            culling_band: float = float("inf"), t_min: float = 0.0, t_max: float = float("inf"),
+                            stream=None) -> gwn_status:
+    """Per-query internal nodes entered and triangles tested by the distance batch (no directions)
+    or the ray batch (directions given); int32 CUDA tensors `nodes`, `tris`."""
+    kind = _lib.GWNB_SPATIAL_RAY if dx is not None else _lib.GWNB_SPATIAL_DISTANCE
+    rc = _lib.load().gwnb_spatial_stats_f32(C.byref(bvh._view), kind, _ptr(qx), _ptr(qy), _ptr(qz), _ptr(dx),
+                                            _ptr(dy), _ptr(dz), _numel(qx), float(culling_band), float(t_min),
+                                            float(t_max), _ptr(nodes), _ptr(tris), _stream(stream))
+    return _status(rc)
+
+
+def ray_order(bvh: gwn_bvh4_object, ox, oy, oz, dx, dy, dz, order, stream=None) -> gwn_status:
+    """Traversal order of a ray batch (direction cell, then origin Hilbert index); `order` is an
+    int32 CUDA tensor."""
+    rc = _lib.load().gwnb_ray_order_f32(C.byref(bvh._view), _ptr(ox), _ptr(oy), _ptr(oz), _ptr(dx), _ptr(dy), _ptr(dz),
+                                        _numel(ox), _ptr(order), _stream(stream))
+    return _status(rc)
+
+
 def query_order(bvh: gwn_bvh4_object, qx, qy, qz, order, stream=None) -> gwn_status:
     """Traversal-coherent (Hilbert) order of a query batch; `order` is an int32 CUDA tensor."""
     rc = _lib.load().gwnb_query_order_f32(C.byref(bvh._view), _ptr(qx), _ptr(qy), _ptr(qz), _numel(qx), _ptr(order),

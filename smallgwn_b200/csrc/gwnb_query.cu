@@ -192,15 +192,6 @@ __global__ void __launch_bounds__(k_exact_block)
 
 // ---- query ordering -----------------------------------------------------------------------------
 
-__device__ inline std::uint32_t expand10(std::uint32_t v) {
-    std::uint32_t x = v & 0x3ffu;
-    x = (x | (x << 16)) & 0x030000ffu;
-    x = (x | (x << 8)) & 0x0300f00fu;
-    x = (x | (x << 4)) & 0x030c30c3u;
-    x = (x | (x << 2)) & 0x09249249u;
-    return x;
-}
-
 __global__ void __launch_bounds__(256)
     k_query_codes(float const *__restrict__ qx, float const *__restrict__ qy,
                   float const *__restrict__ qz, std::uint64_t n, aabb const *__restrict__ root,
@@ -208,45 +199,7 @@ __global__ void __launch_bounds__(256)
     std::uint64_t const i = static_cast<std::uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= n)
         return;
-    aabb const b = *root;
-    float const ex = fmaxf(b.max_x - b.min_x, 1e-30f);
-    float const ey = fmaxf(b.max_y - b.min_y, 1e-30f);
-    float const ez = fmaxf(b.max_z - b.min_z, 1e-30f);
-    // the root box maps to [0.1, 0.9]: a margin keeps queries around the mesh spread as well
-    float const fx = (qx[i] - b.min_x) / ex * 0.8f + 0.1f;
-    float const fy = (qy[i] - b.min_y) / ey * 0.8f + 0.1f;
-    float const fz = (qz[i] - b.min_z) / ez * 0.8f + 0.1f;
-    auto q = [](float f) -> std::uint32_t {
-        f = fminf(fmaxf(f, 0.0f), 1.0f); // NaN -> 0
-        return static_cast<std::uint32_t>(f * 1023.0f);
-    };
-    // 3D Hilbert index of the 10-bit cell (Skilling, "Programming the Hilbert curve", 2004: undo the
-    // excess work of the Gray-code rotation, Gray-encode, then interleave the transposed axes). Its
-    // consecutive cells are face neighbours, so the 32 queries of a warp are more compact than in
-    // Morton order.
-    std::uint32_t X[3] = {q(fx), q(fy), q(fz)};
-#pragma unroll
-    for (std::uint32_t Q = 1u << 9; Q > 1u; Q >>= 1) {
-        std::uint32_t const P = Q - 1u;
-#pragma unroll
-        for (int k = 0; k < 3; ++k) {
-            if (X[k] & Q) {
-                X[0] ^= P;
-            } else {
-                std::uint32_t const t = (X[0] ^ X[k]) & P;
-                X[0] ^= t;
-                X[k] ^= t;
-            }
-        }
-    }
-    X[1] ^= X[0];
-    X[2] ^= X[1];
-    std::uint32_t t = 0;
-#pragma unroll
-    for (std::uint32_t Q = 1u << 9; Q > 1u; Q >>= 1)
-        if (X[2] & Q)
-            t ^= Q - 1u;
-    codes[i] = (expand10(X[0] ^ t) << 2) | (expand10(X[1] ^ t) << 1) | expand10(X[2] ^ t);
+    codes[i] = hilbert_code30(*root, qx[i], qy[i], qz[i]);
 }
 
 // ---- Taylor traversal ---------------------------------------------------------------------------

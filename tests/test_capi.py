@@ -162,6 +162,70 @@ def test_adjoint_pair_validation():
     assert "all null or all non-null" in _lib.last_error()
 
 
+def test_spatial_batches_reject_invalid_contracts_before_launch():
+    """Distance and ray batches: empty BVH, capacity below the bound, t_max < t_min and null
+    storage are refused on the host (tests/unit_gwn_query_distance_ray.cu:563-640)."""
+    lib = _lib.load()
+    empty = _lib.bvh4_f32()
+    assert lib.gwnb_unsigned_distance_batch_f32(C.byref(empty), None, None, None, None, 0, float("inf"), None,
+                                                None) == _lib.GWNB_INVALID_ARGUMENT
+    assert "no queryable data" in _lib.last_error()
+    assert lib.gwnb_ray_first_hit_batch_f32(C.byref(empty), None, None, None, None, None, None, None, 0, 0.0,
+                                            float("inf"), None, None) == _lib.GWNB_INVALID_ARGUMENT
+    fake = _lib.bvh4_f32()
+    fake.nodes = 8
+    fake.node_count = 3
+    fake.primitive_count = 9
+    fake.primitive_indices = 8
+    fake.triangles = 8
+    fake.revision = 5
+    fake.internal_stack_bound = 2
+    fake.root.reference = 1 << 47
+    one = _lib.spatial_options(256, 1, 0)
+    assert lib.gwnb_unsigned_distance_batch_f32(C.byref(fake), None, None, None, None, 0, 1.0, C.byref(one),
+                                                None) == _lib.GWNB_INVALID_ARGUMENT
+    assert "Traversal stack capacity" in _lib.last_error()
+    assert lib.gwnb_ray_first_hit_batch_f32(C.byref(fake), None, None, None, None, None, None, None, 0, 0.0, 1.0,
+                                            C.byref(one), None) == _lib.GWNB_INVALID_ARGUMENT
+    assert "Traversal stack capacity" in _lib.last_error()
+    # empty batches with a valid capacity are accepted; t_max < t_min (or NaN) is not
+    assert lib.gwnb_unsigned_distance_batch_f32(C.byref(fake), None, None, None, None, 0, 1.0, None, None) == 0
+    assert lib.gwnb_ray_first_hit_batch_f32(C.byref(fake), None, None, None, None, None, None, None, 0, 0.0, 1.0,
+                                            None, None) == 0
+    for t_min, t_max in ((2.0, 1.0), (0.0, float("nan"))):
+        assert lib.gwnb_ray_first_hit_batch_f32(C.byref(fake), None, None, None, None, None, None, None, 0, t_min,
+                                                t_max, None, None) == _lib.GWNB_INVALID_ARGUMENT
+        assert "t_max >= t_min" in _lib.last_error()
+    # non-empty batches with null storage
+    assert lib.gwnb_unsigned_distance_batch_f32(C.byref(fake), None, None, None, None, 1, 1.0, None,
+                                                None) == _lib.GWNB_INVALID_ARGUMENT
+    assert lib.gwnb_ray_first_hit_batch_f32(C.byref(fake), 8, None, None, None, None, None, None, 1, 0.0, 1.0,
+                                            None, None) == _lib.GWNB_INVALID_ARGUMENT
+    assert "non-null storage" in _lib.last_error()
+    # a leaf root needs no stack: capacity 1 is accepted
+    leaf = _lib.bvh4_f32()
+    leaf.primitive_count = 1
+    leaf.primitive_indices = 8
+    leaf.triangles = 8
+    leaf.revision = 5
+    leaf.root.reference = (1 << 47) | (1 << 48)
+    assert lib.gwnb_unsigned_distance_batch_f32(C.byref(leaf), None, None, None, None, 0, 1.0, C.byref(one),
+                                                None) == 0
+    assert C.sizeof(_lib.ray_hit_f32) == 32 and api.RAY_HIT_DTYPE.itemsize == 32
+
+
+def test_spatial_python_mirror_rejects_span_mismatch():
+    import torch
+    bvh = api.gwn_bvh4_object()
+    st = api.gwn_compute_unsigned_distance_batch(bvh, None, None, None, None)
+    assert st.error == api.gwn_error.invalid_argument and "no queryable data" in st.message
+    st = api.gwn_compute_ray_first_hit_batch(bvh, None, None, None, None, None, None, None)
+    assert st.error == api.gwn_error.invalid_argument
+    hits = torch.zeros((2, 8), dtype=torch.int32)
+    recs = api.ray_hit_records(hits)
+    assert recs.shape == (2,) and recs.dtype == api.RAY_HIT_DTYPE
+
+
 def test_status_mirror():
     assert api.gwn_status().is_ok()
     assert not api.gwn_status(api.gwn_error.internal_error, "x").is_ok()
