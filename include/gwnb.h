@@ -336,6 +336,51 @@ GWNB_API int gwnb_spatial_stats_f32(const gwnb_bvh4_f32 *bvh, int kind, const fl
                                     float t_max, uint32_t *nodes_entered, uint32_t *triangles_tested,
                                     gwnb_stream_t stream);
 
+/* ---- boundary chain and antipodal winding numbers (include/gwn/gwn_boundary.cuh,
+ *      include/gwn/gwn_query.cuh:446-656) ------------------------------------------------------ */
+
+/* Device boundary chain; mirrors gwn::gwn_boundary_chain_accessor<uint32_t>
+ * (include/gwn/gwn_boundary.cuh:22-59): directed boundary edges (start, end vertex) with their
+ * positive net multiplicity, rows in ascending (low vertex, high vertex) order. */
+typedef struct gwnb_boundary_chain_u32 {
+    uint32_t *start_vertex;
+    uint32_t *end_vertex;
+    uint64_t *multiplicity;
+    uint64_t edge_count;
+    uint64_t mesh_vertex_count;   /* vertex count of the mesh the chain was built from   */
+    uint64_t mesh_triangle_count; /* triangle count of the mesh the chain was built from */
+    int is_built;                 /* 1 after a successful build, closed meshes included   */
+} gwnb_boundary_chain_u32;
+
+/* Replaces gwn::gwn_build_boundary_chain (include/gwn/gwn_boundary.cuh:116-125,
+ * detail/gwn_boundary_impl.cuh:182-415): the algebraic boundary of the oriented triangle chain.
+ * Writes a new chain into *out (the caller releases any previous one). Synchronizes `stream` once
+ * to size the output, as smallgwn does. */
+GWNB_API int gwnb_boundary_chain_build_u32(const gwnb_geometry_f32 *geometry, gwnb_boundary_chain_u32 *out,
+                                           gwnb_stream_t stream);
+
+/* Replaces gwn::detail::gwn_release_boundary_chain_accessor (detail/gwn_boundary_impl.cuh:98-110). */
+GWNB_API void gwnb_boundary_chain_release_u32(gwnb_boundary_chain_u32 *chain, gwnb_stream_t stream);
+
+/* Replaces gwn::gwn_compute_winding_number_antipodal_batch<Config> (include/gwn/gwn_query.cuh:
+ * 497-556): signed crossings of the +z (then +x, +y) coordinate ray through the BVH plus the
+ * boundary spherical-area term; NaN where all three axes are singular. `options` may be NULL
+ * (block 256, stack 64, input order; sort_queries = 1 traverses in Hilbert order). Asynchronous. */
+GWNB_API int gwnb_winding_antipodal_batch_f32(const gwnb_geometry_f32 *geometry, const gwnb_bvh4_f32 *bvh,
+                                              const gwnb_boundary_chain_u32 *chain, const float *query_x,
+                                              const float *query_y, const float *query_z, float *output,
+                                              uint64_t count, const gwnb_spatial_options *options,
+                                              gwnb_stream_t stream);
+
+/* Replaces gwn::gwn_compute_winding_gradient_antipodal_batch<Config> (include/gwn/gwn_query.cuh:
+ * 596-654): gradient of the boundary term; (NaN, NaN, NaN) where all three axes are singular.
+ * block_size 0 selects 256. Asynchronous. */
+GWNB_API int gwnb_winding_gradient_antipodal_batch_f32(const gwnb_geometry_f32 *geometry,
+                                                       const gwnb_boundary_chain_u32 *chain, const float *query_x,
+                                                       const float *query_y, const float *query_z, float *grad_x,
+                                                       float *grad_y, float *grad_z, uint64_t count, int block_size,
+                                                       gwnb_stream_t stream);
+
 /* Traversal order of a ray batch (the permutation the ray batch applies when sort_queries is
  * set): rays sorted by the octahedral cell of their direction, then by the Hilbert index of their
  * origin relative to the BVH root bounds. order[i] is the index of the i-th ray. No smallgwn

@@ -4,7 +4,8 @@ TEST INFRASTRUCTURE ONLY -- imported by tests/, __graft_entry__.smoke() and benc
 baseline, never by the product (smallgwn_b200/). Two libraries back it:
   * _build/liboracle.so   gwn_oracle.c (C, OpenMP): exact winding FP32/FP64, Morton codes, stable
                           sort, Karras LBVH, H-PLOC, BVH4 collapse, triangle records, Taylor
-                          moments and Taylor traversal with per-query counts;
+                          moments and Taylor traversal with per-query counts, unsigned distance,
+                          ray first hit, boundary chains and antipodal winding numbers;
   * _ref/libgwnref.so     smallgwn's CUDA implementation compiled from its headers (ref_shim.cu),
                           present when the reference project was available at build time.
 Parity pins: tests/test_oracle.py checks the C restatement against analytic known answers and
@@ -271,6 +272,51 @@ def distance_brute(tris: np.ndarray, qx, qy, qz, culling_band: float = float("in
     return out
 
 
+def boundary_chain(mesh: dict) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
+    """detail/gwn_boundary_impl.cuh restated: (start, end, multiplicity) rows of the algebraic
+    boundary of the oriented triangle chain, in ascending (low, high) vertex order."""
+    i0, i1, i2 = _u32(mesh["i0"]), _u32(mesh["i1"]), _u32(mesh["i2"])
+    nt = C.c_uint64(i0.size)
+    lib().oracle_boundary_chain.restype = C.c_uint64
+    rows = int(lib().oracle_boundary_chain(_p(i0), _p(i1), _p(i2), nt, None, None, None))
+    start = np.empty(rows, np.uint32)
+    end = np.empty(rows, np.uint32)
+    mult = np.empty(rows, np.uint64)
+    lib().oracle_boundary_chain(_p(i0), _p(i1), _p(i2), nt, _p(start), _p(end), _p(mult))
+    return start, end, mult
+
+
+def antipodal(mesh: dict, nodes: np.ndarray, tris: np.ndarray, root_ref: int, chain, qx, qy, qz,
+              stack_capacity: int = 256, threads: int = 0) -> np.ndarray:
+    """gwn_winding_number_antipodal_impl restated (detail/gwn_query_winding_antipodal_impl.cuh:
+    380-568): signed +axis ray crossings through the BVH plus the boundary spherical-area term,
+    axes z, x, y until one is not singular; NaN when none is."""
+    threads = threads or max_threads()
+    x, y, z = (_f32(mesh[k]) for k in "xyz")
+    nd = np.ascontiguousarray(nodes.reshape(-1, 4), dtype=NODE_DTYPE)
+    t = np.ascontiguousarray(tris, np.float32)
+    s, e, m = (np.ascontiguousarray(a) for a in chain)
+    q = [_f32(v) for v in (qx, qy, qz)]
+    out = np.empty(q[0].size, np.float32)
+    lib().oracle_antipodal(_p(x), _p(y), _p(z), _p(nd), C.c_uint64(nd.shape[0]), _p(t), C.c_uint64(t.shape[0]),
+                           C.c_uint64(root_ref), _p(s), _p(e), _p(m), C.c_uint64(s.size), _p(q[0]), _p(q[1]),
+                           _p(q[2]), C.c_uint64(out.size), C.c_int(stack_capacity), _p(out), C.c_int(threads))
+    return out
+
+
+def antipodal_gradient(mesh: dict, chain, qx, qy, qz, threads: int = 0) -> np.ndarray:
+    """gwn_winding_gradient_point_antipodal_impl restated (:261-372): (n, 3) gradients of the
+    boundary term, NaN rows where every axis is singular."""
+    threads = threads or max_threads()
+    x, y, z = (_f32(mesh[k]) for k in "xyz")
+    s, e, m = (np.ascontiguousarray(a) for a in chain)
+    q = [_f32(v) for v in (qx, qy, qz)]
+    g = [np.empty(q[0].size, np.float32) for _ in range(3)]
+    lib().oracle_antipodal_gradient(_p(x), _p(y), _p(z), _p(s), _p(e), _p(m), C.c_uint64(s.size), _p(q[0]), _p(q[1]),
+                                    _p(q[2]), C.c_uint64(q[0].size), _p(g[0]), _p(g[1]), _p(g[2]), C.c_int(threads))
+    return np.stack(g, axis=1)
+
+
 # gwn::gwn_ray_first_hit_result<float, uint32_t> (include/gwn/gwn_query.cuh:63-96), 32 bytes.
 HIT_DTYPE = np.dtype([("t", np.float32), ("u", np.float32), ("v", np.float32), ("nx", np.float32),
                       ("ny", np.float32), ("nz", np.float32), ("primitive_id", np.uint32), ("status", np.uint8),
@@ -465,6 +511,35 @@ class Reference:
                                               *[_p(v) for v in d], C.c_uint64(q[0].size), C.c_float(culling_band),
                                               C.c_float(t_min), C.c_float(t_max), C.c_int(warmup), C.c_int(iters),
                                               C.byref(ms)))
+        return float(ms.value)
+
+    def boundary(self) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
+        """smallgwn's boundary chain of this mesh (rows as its kernels emit them)."""
+        cnt = C.c_uint64()
+        self._check(self.lib.ref_boundary(self.h, None, None, None, C.byref(cnt)))
+        n = cnt.value
+        s, e, m = np.empty(n, np.uint32), np.empty(n, np.uint32), np.empty(n, np.uint64)
+        self._check(self.lib.ref_boundary(self.h, _p(s), _p(e), _p(m), C.byref(cnt)))
+        return s, e, m
+
+    def antipodal(self, qx, qy, qz) -> np.ndarray:
+        q = [_f32(v) for v in (qx, qy, qz)]
+        out = np.empty(q[0].size, np.float32)
+        self._check(self.lib.ref_antipodal(self.h, _p(q[0]), _p(q[1]), _p(q[2]), _p(out), C.c_uint64(out.size)))
+        return out
+
+    def antipodal_gradient(self, qx, qy, qz) -> np.ndarray:
+        q = [_f32(v) for v in (qx, qy, qz)]
+        g = [np.empty(q[0].size, np.float32) for _ in range(3)]
+        self._check(self.lib.ref_antipodal_gradient(self.h, _p(q[0]), _p(q[1]), _p(q[2]), _p(g[0]), _p(g[1]),
+                                                    _p(g[2]), C.c_uint64(q[0].size)))
+        return np.stack(g, axis=1)
+
+    def time_antipodal(self, qx, qy, qz, warmup: int = 2, iters: int = 5) -> float:
+        q = [_f32(v) for v in (qx, qy, qz)]
+        ms = C.c_float()
+        self._check(self.lib.ref_time_antipodal(self.h, _p(q[0]), _p(q[1]), _p(q[2]), C.c_uint64(q[0].size),
+                                                C.c_int(warmup), C.c_int(iters), C.byref(ms)))
         return float(ms.value)
 
     def time_build(self, method: int, radius: int, bits: int, iters: int) -> float:

@@ -1781,3 +1781,431 @@ void oracle_ray_brute(const o_tri *tris, const uint32_t *prim, uint64_t nt, cons
         out[i] = h;
     }
 }
+
+/* ---------------------------------------------------------------------------------------------- */
+/* Boundary chain and antipodal winding numbers (smallgwn detail/gwn_boundary_impl.cuh and         */
+/* detail/gwn_query_winding_antipodal_impl.cuh; Martens, Trettner and Bessmeltsev, "The Antipodal */
+/* Method", ACM TOG 45(4), 2026). Products and sums fused in the pattern of the spatial queries.   */
+
+typedef struct {
+    uint64_t key; /* (lo << 32) | hi */
+    int orientation;
+} o_edge;
+
+static int edge_cmp(const void *a, const void *b) {
+    uint64_t const x = ((const o_edge *)a)->key, y = ((const o_edge *)b)->key;
+    return x < y ? -1 : (x > y ? 1 : 0);
+}
+
+/* detail/gwn_boundary_impl.cuh:34-60 and :127-171: every triangle edge keyed by its (low, high)
+ * vertex pair with orientation +1 when it runs low to high, -1 when high to low, 0 when both ends
+ * coincide; a key whose orientations sum to s != 0 emits one directed edge (low -> high for s > 0,
+ * high -> low otherwise) of multiplicity |s|, rows in ascending (low, high) order. Returns the
+ * number of rows; with start == NULL only counts. */
+uint64_t oracle_boundary_chain(const uint32_t *i0, const uint32_t *i1, const uint32_t *i2, uint64_t nt, uint32_t *start,
+                               uint32_t *end, uint64_t *mult) {
+    uint64_t const ne = nt * 3;
+    o_edge *e = (o_edge *)malloc((ne ? ne : 1) * sizeof(o_edge));
+    for (uint64_t t = 0; t < nt; ++t) {
+        uint32_t const v[3] = {i0[t], i1[t], i2[t]};
+        for (int k = 0; k < 3; ++k) {
+            uint32_t const s = v[k], d = v[(k + 1) % 3];
+            uint32_t const lo = s < d ? s : d, hi = s < d ? d : s;
+            e[t * 3 + k].key = ((uint64_t)lo << 32) | hi;
+            e[t * 3 + k].orientation = s < d ? 1 : (d < s ? -1 : 0);
+        }
+    }
+    /* the order within a key group does not matter for the sum */
+    qsort(e, ne, sizeof(o_edge), edge_cmp);
+    uint64_t rows = 0;
+    for (uint64_t i = 0; i < ne;) {
+        uint64_t j = i;
+        int64_t sum = 0;
+        while (j < ne && e[j].key == e[i].key)
+            sum += e[j++].orientation;
+        if (sum != 0) {
+            if (start) {
+                uint32_t const lo = (uint32_t)(e[i].key >> 32), hi = (uint32_t)e[i].key;
+                start[rows] = sum > 0 ? lo : hi;
+                end[rows] = sum > 0 ? hi : lo;
+                mult[rows] = (uint64_t)(sum > 0 ? sum : -sum);
+            }
+            ++rows;
+        }
+        i = j;
+    }
+    free(e);
+    return rows;
+}
+
+/* Projection onto the plane orthogonal to the ray axis (detail/gwn_query_winding_antipodal_impl.cuh:
+ * 54-63): x -> (y, z), y -> (z, x), z -> (x, y). */
+static inline void ap_project(o_v3 v, int axis, float *px, float *py) {
+    if (axis == 0) {
+        *px = v.y;
+        *py = v.z;
+    } else if (axis == 1) {
+        *px = v.z;
+        *py = v.x;
+    } else {
+        *px = v.x;
+        *py = v.y;
+    }
+}
+
+static inline int ap_sign(float v) { return v > 0.0f ? 1 : (v < 0.0f ? -1 : 0); }
+
+/* :76-111: projected determinant, its sign with the lexicographic symbolic perturbation, and the
+ * singular flag of a collinear edge whose endpoints lie on opposite sides of the query. */
+static inline void ap_classify(o_v3 s, o_v3 e, int axis, int *sign, int *singular, float *det) {
+    float ax, ay, bx, by;
+    ap_project(s, axis, &ax, &ay);
+    ap_project(e, axis, &bx, &by);
+    float const d = o_dop(ax, by, ay, bx);
+    int sg = ap_sign(d);
+    if (sg == 0) {
+        sg = ap_sign(ay - by);
+        if (sg == 0)
+            sg = ap_sign(bx - ax);
+    }
+    *sign = sg;
+    *det = d;
+    *singular = d == 0.0f && fmaf(ay, by, ax * bx) <= 0.0f;
+}
+
+static inline float ap_axis_component(o_v3 v, int axis) { return axis == 0 ? v.x : (axis == 1 ? v.y : v.z); }
+
+/* :123-177: crossing sign of one oriented triangle with the positive axis ray; 1 when singular. */
+static int ap_triangle_crossing(o_v3 q, int axis, o_v3 a, o_v3 b, o_v3 c, float *crossing) {
+    o_v3 const pa = v3_sub(a, q), pb = v3_sub(b, q), pc = v3_sub(c, q);
+    o_v3 const n = v3_cross(v3_sub(pb, pa), v3_sub(pc, pa));
+    float const na = ap_axis_component(n, axis);
+    if (na == 0.0f)
+        return 0;
+    int s0, s1, s2, g0, g1, g2;
+    float d;
+    ap_classify(pa, pb, axis, &s0, &g0, &d);
+    ap_classify(pb, pc, axis, &s1, &g1, &d);
+    ap_classify(pc, pa, axis, &s2, &g2, &d);
+    if (g0 || g1 || g2)
+        return 1;
+    if (s0 == 0 || s1 == 0 || s2 == 0)
+        return 1;
+    if (!((s0 >= 0 && s1 >= 0 && s2 >= 0) || (s0 <= 0 && s1 <= 0 && s2 <= 0)))
+        return 0;
+    float const t = v3_dot(n, pa) / na;
+    if (t == 0.0f)
+        return 1;
+    if (!(t > 0.0f))
+        return 0;
+    *crossing += na > 0.0f ? 1.0f : -1.0f;
+    return 0;
+}
+
+/* :380-489: signed crossings of the positive axis ray through the canonical BVH (children in slot
+ * order, leaves evaluated in place, the last internal child entered directly). Returns 1 when
+ * singular, 2 on stack overflow. */
+static int ap_crossings(const o_node4 *nodes, uint64_t nn, const o_tri *tris, uint64_t nt, uint64_t root_ref, o_v3 q,
+                        int axis, int cap, float *sum) {
+    float const qc[3] = {q.x, q.y, q.z};
+    int const u = axis == 0 ? 1 : (axis == 1 ? 2 : 0), w = axis == 0 ? 2 : (axis == 1 ? 0 : 1);
+    *sum = 0.0f;
+#define AP_LEAF(R)                                                                                  \
+    for (uint32_t k_ = 0; k_ < ref_count(R); ++k_) {                                                \
+        uint64_t const si_ = ref_offset(R) + k_;                                                    \
+        if (si_ >= nt)                                                                              \
+            continue;                                                                               \
+        o_v3 a_, b_, c_;                                                                            \
+        record_vertices(&tris[si_], &a_, &b_, &c_);                                                 \
+        if (ap_triangle_crossing(q, axis, a_, b_, c_, sum))                                          \
+            return 1;                                                                               \
+    }
+    if (ref_leaf(root_ref)) {
+        AP_LEAF(root_ref)
+        return 0;
+    }
+    uint32_t stack[256];
+    int sp = 0;
+    uint64_t node = ref_offset(root_ref);
+    for (;;) {
+        uint64_t next = (uint64_t)-1;
+        if (node < nn) {
+            const o_node4 *nd = &nodes[node];
+            for (int s = 0; s < 4; ++s) {
+                uint64_t const r = nd->c[s].reference;
+                if (!ref_valid(r))
+                    continue;
+                const o_aabb *b = &nd->c[s].bounds;
+                float const lo[3] = {b->min_x, b->min_y, b->min_z}, hi[3] = {b->max_x, b->max_y, b->max_z};
+                if (!(qc[u] >= lo[u] && qc[u] <= hi[u] && qc[w] >= lo[w] && qc[w] <= hi[w] && hi[axis] >= qc[axis]))
+                    continue;
+                if (ref_leaf(r)) {
+                    AP_LEAF(r)
+                    continue;
+                }
+                if (!ref_internal(r))
+                    continue;
+                if (next != (uint64_t)-1) {
+                    if (sp >= cap)
+                        return 2;
+                    stack[sp++] = (uint32_t)next;
+                }
+                next = ref_offset(r);
+            }
+        }
+        if (next != (uint64_t)-1) {
+            node = next;
+            continue;
+        }
+        if (sp == 0)
+            break;
+        node = stack[--sp];
+    }
+#undef AP_LEAF
+    return 0;
+}
+
+static const double ap_pi = 3.141592653589793238462643383279502884;
+
+/* Terms whose atan2 arguments are both below this fraction of |s||e| are evaluated in FP64: the
+ * edge passes close to the ray line seen from the query, the term (and its gradient, which grows
+ * like the inverse of that distance) is dominated by float rounding there, and neighbouring terms
+ * of that size cancel. The decision is made on the float values, identically on the GPU. */
+static const float ap_guard = 1.0f / 16.0f;
+
+static inline int ap_guarded(float num, float den, float ls, float le) {
+    float const sl = ls * le;
+    return fmaf(den, den, num * num) < (ap_guard * ap_guard) * (sl * sl);
+}
+
+/* The term's vectors in FP64 from the float end points and query. */
+static inline void ap_vectors_d(o_v3 S, o_v3 E, o_v3 q, double s[3], double e[3]) {
+    s[0] = (double)S.x - (double)q.x;
+    s[1] = (double)S.y - (double)q.y;
+    s[2] = (double)S.z - (double)q.z;
+    e[0] = (double)E.x - (double)q.x;
+    e[1] = (double)E.y - (double)q.y;
+    e[2] = (double)E.z - (double)q.z;
+}
+
+/* -ray . (s x e), |s|, |e| and the atan2 denominator in FP64. */
+static inline void ap_terms_d(int axis, const double s[3], const double e[3], double *num, double *den, double *ls,
+                              double *le) {
+    double const c[3] = {s[1] * e[2] - s[2] * e[1], s[2] * e[0] - s[0] * e[2], s[0] * e[1] - s[1] * e[0]};
+    *ls = sqrt(s[0] * s[0] + s[1] * s[1] + s[2] * s[2]);
+    *le = sqrt(e[0] * e[0] + e[1] * e[1] + e[2] * e[2]);
+    *num = -c[axis];
+    *den = *ls * *le - s[axis] * *le - e[axis] * *ls + (s[0] * e[0] + s[1] * e[1] + s[2] * e[2]);
+}
+
+/* :188-205: signed spherical area of (-ray, edge start, edge end), 2 atan2(numerator, denominator);
+ * for guarded terms the atan2 arguments come from FP64 vectors (S, E and q). */
+static double ap_area(int axis, o_v3 mr, o_v3 s, o_v3 e, float det, o_v3 S, o_v3 E, o_v3 q, int *guarded) {
+    float const ls = sqrtf(v3_dot(s, s)), le = sqrtf(v3_dot(e, e));
+    *guarded = 0;
+    if (!(ls > 0.0f) || !(le > 0.0f))
+        return NAN;
+    float num = -det;
+    if (det == 0.0f)
+        num = v3_dot(mr, v3_cross(s, e));
+    float const den = fmaf(v3_dot(e, mr), ls, fmaf(v3_dot(mr, s), le, ls * le) + v3_dot(s, e));
+    if (ap_guarded(num, den, ls, le)) {
+        /* the angle of accurately known arguments is well conditioned: atan2 in float suffices */
+        double sd[3], ed[3], nd, dd, lsd, led;
+        ap_vectors_d(S, E, q, sd, ed);
+        ap_terms_d(axis, sd, ed, &nd, &dd, &lsd, &led);
+        *guarded = 1;
+        return (double)(2.0f * atan2f((float)nd, (float)dd));
+    }
+    return (double)(2.0f * atan2f(num, den));
+}
+
+/* Edge records (start, end, multiplicity) gathered from the geometry. */
+static inline void ap_edge(const float *vx, const float *vy, const float *vz, uint32_t a, uint32_t b, o_v3 q, o_v3 *s,
+                           o_v3 *e) {
+    *s = v3(vx[a] - q.x, vy[a] - q.y, vz[a] - q.z);
+    *e = v3(vx[b] - q.x, vy[b] - q.y, vz[b] - q.z);
+}
+
+/* :209-256: boundary term of one axis, summed in FP64 in row order. Returns 1 when singular. */
+static int ap_boundary(const float *vx, const float *vy, const float *vz, const uint32_t *start, const uint32_t *end,
+                       const uint64_t *mult, uint64_t ne, o_v3 q, int axis, double *out) {
+    o_v3 mr = v3(0.0f, 0.0f, 0.0f);
+    if (axis == 0)
+        mr.x = -1.0f;
+    else if (axis == 1)
+        mr.y = -1.0f;
+    else
+        mr.z = -1.0f;
+    double sum = 0.0;
+    for (uint64_t i = 0; i < ne; ++i) {
+        o_v3 s, e;
+        ap_edge(vx, vy, vz, start[i], end[i], q, &s, &e);
+        int sign, singular;
+        float det;
+        ap_classify(s, e, axis, &sign, &singular, &det);
+        if (singular)
+            return 1;
+        o_v3 const S = v3(vx[start[i]], vy[start[i]], vz[start[i]]), E = v3(vx[end[i]], vy[end[i]], vz[end[i]]);
+        int guarded;
+        float area = (float)ap_area(axis, mr, s, e, det, S, E, q, &guarded);
+        if (axis != 2 && sign > 0 && area < 0.0f)
+            area += (float)(2.0 * ap_pi);
+        sum += (double)((float)mult[i] * area);
+    }
+    *out = sum / (4.0 * ap_pi);
+    return 0;
+}
+
+/* :533-568 (z, then x, then y): crossings plus boundary term of the first axis on which neither is
+ * singular; NaN when all three are (or on stack overflow). */
+void oracle_antipodal(const float *vx, const float *vy, const float *vz, const o_node4 *nodes, uint64_t nn,
+                      const o_tri *tris, uint64_t nt, uint64_t root_ref, const uint32_t *start, const uint32_t *end,
+                      const uint64_t *mult, uint64_t ne, const float *qx, const float *qy, const float *qz, uint64_t n,
+                      int stack_capacity, float *out, int threads) {
+    int const cap = stack_capacity > 256 ? 256 : stack_capacity;
+    static const int order[3] = {2, 0, 1};
+#pragma omp parallel for schedule(dynamic, 64) num_threads(threads)
+    for (int64_t i = 0; i < (int64_t)n; ++i) {
+        o_v3 const q = v3(qx[i], qy[i], qz[i]);
+        float result = NAN;
+        for (int k = 0; k < 3; ++k) {
+            float cross;
+            int const c = ap_crossings(nodes, nn, tris, nt, root_ref, q, order[k], cap, &cross);
+            if (c == 2)
+                break;
+            if (c == 1)
+                continue;
+            double b;
+            if (ap_boundary(vx, vy, vz, start, end, mult, ne, q, order[k], &b))
+                continue;
+            result = (float)((double)cross + b);
+            break;
+        }
+        out[i] = result;
+    }
+}
+
+static inline o_v3 v3_scale(o_v3 a, float s) { return v3(a.x * s, a.y * s, a.z * s); }
+
+/* The same gradient in FP64 (guarded terms). */
+static void ap_area_gradient_d(int axis, o_v3 S, o_v3 E, o_v3 q, double g[3]) {
+    double s[3], e[3], num, den, ls, le;
+    ap_vectors_d(S, E, q, s, e);
+    ap_terms_d(axis, s, e, &num, &den, &ls, &le);
+    double mr[3] = {0.0, 0.0, 0.0};
+    mr[axis] = -1.0;
+    double const d2 = num * num + den * den;
+    if (ls == 0.0 || le == 0.0 || d2 == 0.0) {
+        g[0] = g[1] = g[2] = NAN;
+        return;
+    }
+    double su[3], eu[3];
+    for (int k = 0; k < 3; ++k) {
+        su[k] = s[k] / ls;
+        eu[k] = e[k] / le;
+    }
+    double const cn = 2.0 * den / d2, cd = -2.0 * num / d2;
+    double const me = mr[0] * eu[0] + mr[1] * eu[1] + mr[2] * eu[2];
+    double const ms = mr[0] * su[0] + mr[1] * su[1] + mr[2] * su[2];
+    /* e x mr + mr x s */
+    double const gn[3] = {-((e[1] * mr[2] - e[2] * mr[1]) + (mr[1] * s[2] - mr[2] * s[1])),
+                          -((e[2] * mr[0] - e[0] * mr[2]) + (mr[2] * s[0] - mr[0] * s[2])),
+                          -((e[0] * mr[1] - e[1] * mr[0]) + (mr[0] * s[1] - mr[1] * s[0]))};
+    for (int k = 0; k < 3; ++k) {
+        double const t1 = le * (mr[k] + eu[k] + (1.0 + me) * su[k]);
+        double const t2 = ls * (mr[k] + su[k] + (1.0 + ms) * eu[k]);
+        g[k] = cn * gn[k] - cd * (t1 + t2);
+    }
+}
+
+/* :261-304: gradient of one signed spherical-area term with respect to the query; FP64 for guarded
+ * terms (returned in gd with *guarded set). */
+static o_v3 ap_area_gradient(int axis, o_v3 mr, o_v3 s, o_v3 e, float det, o_v3 S, o_v3 E, o_v3 q, int *guarded,
+                             double gd_out[3]) {
+    o_v3 const nan3 = v3(NAN, NAN, NAN);
+    *guarded = 0;
+    float const ls = sqrtf(v3_dot(s, s)), le = sqrtf(v3_dot(e, e));
+    if (ls == 0.0f || le == 0.0f)
+        return nan3;
+    o_v3 const su = v3_scale(s, 1.0f / ls), eu = v3_scale(e, 1.0f / le);
+    float num = -det;
+    if (det == 0.0f)
+        num = v3_dot(mr, v3_cross(s, e));
+    float const den = fmaf(v3_dot(mr, e), ls, fmaf(v3_dot(mr, s), le, ls * le) + v3_dot(s, e));
+    if (ap_guarded(num, den, ls, le)) {
+        *guarded = 1;
+        ap_area_gradient_d(axis, S, E, q, gd_out);
+        return nan3;
+    }
+    float const d2 = fmaf(den, den, num * num);
+    if (d2 == 0.0f)
+        return nan3;
+    float const cn = 2.0f * den / d2, cd = -2.0f * num / d2;
+    o_v3 const gn = v3_scale(v3_add(v3_cross(e, mr), v3_cross(mr, s)), -1.0f);
+    o_v3 const t1 = v3_scale(v3_fma(su, 1.0f + v3_dot(mr, eu), v3_add(mr, eu)), le);
+    o_v3 const t2 = v3_scale(v3_fma(eu, 1.0f + v3_dot(mr, su), v3_add(mr, su)), ls);
+    o_v3 const gd = v3_scale(v3_add(t1, t2), -1.0f);
+    return v3_fma(gd, cd, v3_scale(gn, cn));
+}
+
+/* :307-372: gradient of the boundary term (FP64 sums), axis retries z, x, y; NaN when all three
+ * are singular. */
+void oracle_antipodal_gradient(const float *vx, const float *vy, const float *vz, const uint32_t *start,
+                               const uint32_t *end, const uint64_t *mult, uint64_t ne, const float *qx,
+                               const float *qy, const float *qz, uint64_t n, float *gx, float *gy, float *gz,
+                               int threads) {
+    static const int order[3] = {2, 0, 1};
+#pragma omp parallel for schedule(dynamic, 64) num_threads(threads)
+    for (int64_t i = 0; i < (int64_t)n; ++i) {
+        o_v3 const q = v3(qx[i], qy[i], qz[i]);
+        float r[3] = {NAN, NAN, NAN};
+        for (int k = 0; k < 3; ++k) {
+            int const axis = order[k];
+            o_v3 mr = v3(0.0f, 0.0f, 0.0f);
+            if (axis == 0)
+                mr.x = -1.0f;
+            else if (axis == 1)
+                mr.y = -1.0f;
+            else
+                mr.z = -1.0f;
+            double sx = 0.0, sy = 0.0, sz = 0.0;
+            int singular = 0;
+            for (uint64_t j = 0; j < ne && !singular; ++j) {
+                o_v3 s, e;
+                ap_edge(vx, vy, vz, start[j], end[j], q, &s, &e);
+                int sign;
+                float det;
+                ap_classify(s, e, axis, &sign, &singular, &det);
+                if (singular)
+                    break;
+                o_v3 const S = v3(vx[start[j]], vy[start[j]], vz[start[j]]);
+                o_v3 const E = v3(vx[end[j]], vy[end[j]], vz[end[j]]);
+                int guarded;
+                double gd[3];
+                o_v3 const g = ap_area_gradient(axis, mr, s, e, det, S, E, q, &guarded, gd);
+                if (guarded) {
+                    double const md = (double)mult[j];
+                    sx += md * gd[0];
+                    sy += md * gd[1];
+                    sz += md * gd[2];
+                } else {
+                    float const m = (float)mult[j];
+                    sx += (double)(m * g.x);
+                    sy += (double)(m * g.y);
+                    sz += (double)(m * g.z);
+                }
+            }
+            if (singular)
+                continue;
+            double const k4 = 4.0 * ap_pi;
+            r[0] = (float)(sx / k4);
+            r[1] = (float)(sy / k4);
+            r[2] = (float)(sz / k4);
+            break;
+        }
+        gx[i] = r[0];
+        gy[i] = r[1];
+        gz[i] = r[2];
+    }
+}

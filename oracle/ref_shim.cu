@@ -41,6 +41,7 @@ struct ctx {
     gwn::gwn_bvh4_moment_object<0, Real, Index> m0;
     gwn::gwn_bvh4_moment_object<1, Real, Index> m1;
     gwn::gwn_bvh4_moment_object<2, Real, Index> m2;
+    gwn::gwn_boundary_chain_object<Index> chain;
 };
 
 template <class T> struct dbuf {
@@ -498,6 +499,98 @@ int ref_time_spatial(void *p, int kind, const float *qx, const float *qy, const 
     dbuf<float> od(kind ? 0 : n);
     dbuf<ray_result> orr(kind ? n : 0);
     auto run = [&]() { return kind ? ray_any(c, r, orr, t_min, t_max) : distance_any(c, r[0], r[1], r[2], od, band); };
+    for (int i = 0; i < warmup; ++i) {
+        auto s = run();
+        if (!s.is_ok())
+            return fail(s);
+    }
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaDeviceSynchronize();
+    cudaEventRecord(e0, cudaStreamLegacy);
+    for (int i = 0; i < iters; ++i)
+        (void)run();
+    cudaEventRecord(e1, cudaStreamLegacy);
+    cudaEventSynchronize(e1);
+    float t = 0;
+    cudaEventElapsedTime(&t, e0, e1);
+    *ms = t / static_cast<float>(iters > 0 ? iters : 1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return static_cast<int>(cudaGetLastError());
+}
+
+// smallgwn's boundary chain of the context's geometry (gwn_build_boundary_chain). With start ==
+// nullptr only builds and reports the row count.
+int ref_boundary(void *p, uint32_t *start, uint32_t *end, uint64_t *mult, uint64_t *count) {
+    auto &c = *static_cast<ctx *>(p);
+    auto s = gwn::gwn_build_boundary_chain(c.geometry, c.chain);
+    if (!s.is_ok())
+        return fail(s);
+    cudaDeviceSynchronize();
+    auto const &a = c.chain.accessor();
+    *count = a.edge_count();
+    if (start != nullptr && a.edge_count() > 0) {
+        cudaMemcpy(start, a.start_vertex.data(), a.edge_count() * sizeof(uint32_t), cudaMemcpyDeviceToHost);
+        cudaMemcpy(end, a.end_vertex.data(), a.edge_count() * sizeof(uint32_t), cudaMemcpyDeviceToHost);
+        cudaMemcpy(mult, a.multiplicity.data(), a.edge_count() * sizeof(uint64_t), cudaMemcpyDeviceToHost);
+    }
+    return static_cast<int>(cudaGetLastError());
+}
+
+// smallgwn's antipodal winding batch (needs ref_build and ref_boundary first).
+int ref_antipodal(void *p, const float *qx, const float *qy, const float *qz, float *out, uint64_t n) {
+    auto &c = *static_cast<ctx *>(p);
+    dbuf<float> x(qx, n), y(qy, n), z(qz, n), o(n);
+    gwn::gwn_status s;
+    if (c.bvh.accessor().internal_stack_bound <= 64)
+        s = gwn::gwn_compute_winding_number_antipodal_batch<gwn::gwn_query_batch_config{256, 64}, 4, Real, Index, no_trap>(
+            c.geometry, c.bvh, c.chain, gwn::gwn_device_span<float const>(x.p, n), gwn::gwn_device_span<float const>(y.p, n),
+            gwn::gwn_device_span<float const>(z.p, n), gwn::gwn_device_span<float>(o.p, n), gwn::gwn_default_stream(),
+            no_trap{});
+    else
+        s = gwn::gwn_compute_winding_number_antipodal_batch<gwn::gwn_query_batch_config{256, 256}, 4, Real, Index, no_trap>(
+            c.geometry, c.bvh, c.chain, gwn::gwn_device_span<float const>(x.p, n), gwn::gwn_device_span<float const>(y.p, n),
+            gwn::gwn_device_span<float const>(z.p, n), gwn::gwn_device_span<float>(o.p, n), gwn::gwn_default_stream(),
+            no_trap{});
+    if (!s.is_ok())
+        return fail(s);
+    cudaDeviceSynchronize();
+    o.to_host(out);
+    return static_cast<int>(cudaGetLastError());
+}
+
+// smallgwn's antipodal gradient batch (needs ref_boundary first).
+int ref_antipodal_gradient(void *p, const float *qx, const float *qy, const float *qz, float *gx, float *gy, float *gz,
+                           uint64_t n) {
+    auto &c = *static_cast<ctx *>(p);
+    dbuf<float> x(qx, n), y(qy, n), z(qz, n), ox(n), oy(n), oz(n);
+    auto s = gwn::gwn_compute_winding_gradient_antipodal_batch(
+        c.geometry, c.chain, gwn::gwn_device_span<float const>(x.p, n), gwn::gwn_device_span<float const>(y.p, n),
+        gwn::gwn_device_span<float const>(z.p, n), gwn::gwn_device_span<float>(ox.p, n),
+        gwn::gwn_device_span<float>(oy.p, n), gwn::gwn_device_span<float>(oz.p, n));
+    if (!s.is_ok())
+        return fail(s);
+    cudaDeviceSynchronize();
+    ox.to_host(gx);
+    oy.to_host(gy);
+    oz.to_host(gz);
+    return static_cast<int>(cudaGetLastError());
+}
+
+// Average ms of `iters` antipodal batches on device-resident queries after `warmup` untimed ones.
+int ref_time_antipodal(void *p, const float *qx, const float *qy, const float *qz, uint64_t n, int warmup, int iters,
+                       float *ms) {
+    auto &c = *static_cast<ctx *>(p);
+    dbuf<float> x(qx, n), y(qy, n), z(qz, n), o(n);
+    auto run = [&]() {
+        return gwn::gwn_compute_winding_number_antipodal_batch<gwn::gwn_query_batch_config{256, 64}, 4, Real, Index,
+                                                               no_trap>(
+            c.geometry, c.bvh, c.chain, gwn::gwn_device_span<float const>(x.p, n), gwn::gwn_device_span<float const>(y.p, n),
+            gwn::gwn_device_span<float const>(z.p, n), gwn::gwn_device_span<float>(o.p, n), gwn::gwn_default_stream(),
+            no_trap{});
+    };
     for (int i = 0; i < warmup; ++i) {
         auto s = run();
         if (!s.is_ok())

@@ -6,12 +6,16 @@ The product is libgwnb.so (CUDA kernels + the C ABI of include/gwnb.h). This pac
 """
 from .api import (  # noqa: F401
     gwn_batch,
+    gwn_boundary_chain_object,
+    gwn_build_boundary_chain,
     gwn_bvh4_moment_object,
     gwn_bvh4_object,
     gwn_bvh_build_method,
     gwn_bvh_build_options,
     gwn_build_bvh,
     gwn_compute_ray_first_hit_batch,
+    gwn_compute_winding_gradient_antipodal_batch,
+    gwn_compute_winding_number_antipodal_batch,
     gwn_compute_unsigned_distance_batch,
     gwn_compute_winding_gradient_taylor_batch,
     gwn_compute_winding_number_exact_batch,

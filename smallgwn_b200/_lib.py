@@ -148,6 +148,18 @@ class ray_hit_f32(C.Structure):
     ]
 
 
+class boundary_chain_u32(C.Structure):
+    _fields_ = [
+        ("start_vertex", C.c_void_p),
+        ("end_vertex", C.c_void_p),
+        ("multiplicity", C.c_void_p),
+        ("edge_count", C.c_uint64),
+        ("mesh_vertex_count", C.c_uint64),
+        ("mesh_triangle_count", C.c_uint64),
+        ("is_built", C.c_int),
+    ]
+
+
 class binary_node(C.Structure):
     _fields_ = [(n, C.c_uint32) for n in ("left_index", "left_kind", "right_index", "right_kind")]
 
@@ -197,6 +209,13 @@ SIGNATURES: dict[str, tuple] = {
         I, [C.POINTER(bvh4_f32), P, P, P, P, U64, F, C.POINTER(spatial_options), P]),
     "gwnb_ray_first_hit_batch_f32": (
         I, [C.POINTER(bvh4_f32), P, P, P, P, P, P, P, U64, F, F, C.POINTER(spatial_options), P]),
+    "gwnb_boundary_chain_build_u32": (I, [C.POINTER(geometry_f32), C.POINTER(boundary_chain_u32), P]),
+    "gwnb_boundary_chain_release_u32": (None, [C.POINTER(boundary_chain_u32), P]),
+    "gwnb_winding_antipodal_batch_f32": (
+        I, [C.POINTER(geometry_f32), C.POINTER(bvh4_f32), C.POINTER(boundary_chain_u32), P, P, P, P, U64,
+            C.POINTER(spatial_options), P]),
+    "gwnb_winding_gradient_antipodal_batch_f32": (
+        I, [C.POINTER(geometry_f32), C.POINTER(boundary_chain_u32), P, P, P, P, P, P, U64, I, P]),
     "gwnb_ray_order_f32": (I, [C.POINTER(bvh4_f32), P, P, P, P, P, P, U64, P, P]),
     "gwnb_spatial_stats_f32": (
         I, [C.POINTER(bvh4_f32), I, P, P, P, P, P, P, U64, F, F, F, P, P, P]),

@@ -435,6 +435,97 @@ def _spatial_options(config: gwn_query_batch_config, sort_queries: bool):
     return _lib.spatial_options(int(config.block_size), int(config.stack_capacity), 1 if sort_queries else 0)
 
 
+class gwn_boundary_chain_object(_stream_mixin):
+    """Mirror of gwn::gwn_boundary_chain_object<uint32_t> (include/gwn/gwn_boundary.cuh:61-110): the
+    algebraic boundary of an oriented triangle chain (directed edges with positive multiplicity).
+    ``has_data()`` means built; a closed mesh has ``has_data()`` and ``edge_count() == 0``."""
+
+    def __init__(self) -> None:
+        super().__init__()
+        self._view = _lib.boundary_chain_u32()
+
+    def accessor(self) -> _lib.boundary_chain_u32:
+        return self._view
+
+    def has_data(self) -> bool:
+        return bool(self._view.is_built)
+
+    def edge_count(self) -> int:
+        return int(self._view.edge_count)
+
+    def empty(self) -> bool:
+        return self.edge_count() == 0
+
+    def rows(self) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
+        """Host copy of the (start, end, multiplicity) rows."""
+        n = self.edge_count()
+        if n == 0:
+            return np.zeros(0, np.uint32), np.zeros(0, np.uint32), np.zeros(0, np.uint64)
+        v = self._view
+        return (np.frombuffer(_copy_to_host(v.start_vertex, 4 * n), np.uint32),
+                np.frombuffer(_copy_to_host(v.end_vertex, 4 * n), np.uint32),
+                np.frombuffer(_copy_to_host(v.multiplicity, 8 * n), np.uint64))
+
+    def clear(self) -> None:
+        if self.has_data():
+            _lib.load().gwnb_boundary_chain_release_u32(C.byref(self._view), _stream(self._stream))
+        self._view = _lib.boundary_chain_u32()
+
+    def __del__(self) -> None:
+        try:
+            self.clear()
+        except Exception:
+            pass
+
+
+def gwn_build_boundary_chain(geometry, out: gwn_boundary_chain_object, stream=None) -> gwn_status:
+    """Build the algebraic boundary chain of an uploaded geometry; replaces ``out`` only on success
+    (include/gwn/gwn_boundary.cuh:116-125)."""
+    staging = _lib.boundary_chain_u32()
+    rc = _lib.load().gwnb_boundary_chain_build_u32(C.byref(geometry.accessor()), C.byref(staging), _stream(stream))
+    if rc != _lib.GWNB_OK:
+        return _status(rc)
+    out.clear()
+    out._view = staging
+    out.set_stream(stream)
+    return gwn_status()
+
+
+def gwn_compute_winding_number_antipodal_batch(geometry, bvh: gwn_bvh4_object, boundary: gwn_boundary_chain_object,
+                                               qx, qy, qz, out, stream=None,
+                                               config: gwn_query_batch_config = gwn_query_batch_config(),
+                                               sort_queries: bool = False) -> gwn_status:
+    """Antipodal winding numbers of a device batch (asynchronous): signed +z (+x, +y on retry) ray
+    crossings through the BVH plus the boundary spherical-area term; NaN where every axis is
+    singular (include/gwn/gwn_query.cuh:497-556)."""
+    n = _numel(qx)
+    if not (_numel(qy) == n == _numel(qz)):
+        return gwn_status(gwn_error.invalid_argument, "Query SoA spans require identical lengths.")
+    if _numel(out) != n:
+        return gwn_status(gwn_error.invalid_argument, "Output span size differs from query count.")
+    opt = _spatial_options(config, sort_queries)
+    rc = _lib.load().gwnb_winding_antipodal_batch_f32(C.byref(geometry.accessor()), C.byref(bvh._view),
+                                                      C.byref(boundary._view), _ptr(qx), _ptr(qy), _ptr(qz),
+                                                      _ptr(out), n, C.byref(opt), _stream(stream))
+    return _status(rc)
+
+
+def gwn_compute_winding_gradient_antipodal_batch(geometry, boundary: gwn_boundary_chain_object, qx, qy, qz, gx, gy,
+                                                 gz, stream=None,
+                                                 config: gwn_query_batch_config = gwn_query_batch_config()
+                                                 ) -> gwn_status:
+    """Gradient of the antipodal boundary term (include/gwn/gwn_query.cuh:596-654)."""
+    n = _numel(qx)
+    if not (_numel(qy) == n == _numel(qz)):
+        return gwn_status(gwn_error.invalid_argument, "Query SoA spans require identical lengths.")
+    if not (_numel(gx) == n == _numel(gy) == _numel(gz)):
+        return gwn_status(gwn_error.invalid_argument, "Output span sizes differ from query count.")
+    rc = _lib.load().gwnb_winding_gradient_antipodal_batch_f32(
+        C.byref(geometry.accessor()), C.byref(boundary._view), _ptr(qx), _ptr(qy), _ptr(qz), _ptr(gx), _ptr(gy),
+        _ptr(gz), n, int(config.block_size), _stream(stream))
+    return _status(rc)
+
+
 def gwn_compute_unsigned_distance_batch(bvh: gwn_bvh4_object, qx, qy, qz, out, culling_band: float = float("inf"),
                                         stream=None, config: gwn_query_batch_config = gwn_query_batch_config(),
                                         sort_queries: bool = False) -> gwn_status:
