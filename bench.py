@@ -48,11 +48,12 @@ def parse() -> argparse.Namespace:
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="taylor",
-                    choices=["taylor", "adjoint", "precision", "exact", "batched", "distance", "ray"],
+                    choices=["taylor", "adjoint", "precision", "exact", "batched", "distance", "ray", "antipodal"],
                     help="taylor: the headline (1M-triangle sphere, 10M queries); adjoint: forward + backward "
                          "on the 159k-triangle soup; precision: 8.4M-triangle sphere, 100M near-surface queries "
                          "in 16M chunks; exact: brute-force exact batch on the small icosphere; distance / ray: "
-                         "unsigned distance / ray first hit on the 1M-triangle sphere, 10M queries / rays")
+                         "unsigned distance / ray first hit on the 1M-triangle sphere, 10M queries / rays; "
+                         "antipodal: antipodal winding numbers on the 159k-triangle open soup, 200k queries")
     ap.add_argument("--queries", type=int, default=N_QUERIES)
     ap.add_argument("--order", type=int, default=ORDER)
     ap.add_argument("--beta", type=float, default=BETA)
@@ -997,6 +998,108 @@ def run_spatial_workload(args) -> None:
         dist.destroy_process_group()
 
 
+def run_antipodal_workload(args) -> None:
+    """Antipodal winding numbers on an open mesh: the 316 x 316 displaced sphere with 20 % of the
+    triangles deleted and 5 % flipped (seed 3; 159k triangles, 113,712 boundary rows), 200k mixed
+    queries (seed 3), H-PLOC r = 8 BVH4. A step is one antipodal batch on device-resident queries
+    (Hilbert order, +z crossings through the BVH, the boundary term over every boundary row).
+    Accuracy against the FP64 exact winding number on a 2,000-query subset; smallgwn's own kernel
+    (oracle/_ref, when built) timed on the same queries for context."""
+    import torch
+
+    import oracle
+    import smallgwn_b200 as g
+    from smallgwn_b200 import meshes
+
+    mesh = meshes.soup_mesh(316, seed=3)
+    n = min(args.queries, 200_000)
+    q = [np.ascontiguousarray(v) for v in meshes.mixed_queries(mesh, n, seed=3)]
+    stream = torch.cuda.current_stream()
+    geo = g.gwn_geometry_object()
+    assert g.gwn_upload_geometry(geo, mesh["x"], mesh["y"], mesh["z"], mesh["i0"], mesh["i1"], mesh["i2"], stream).is_ok()
+    bvh = g.gwn_bvh4_object()
+    assert g.gwn_build_bvh(geo, bvh, g.gwn_bvh_build_options(method=0, hploc_search_radius=8), stream).is_ok()
+    ch = g.gwn_boundary_chain_object()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    assert g.gwn_build_boundary_chain(geo, ch, stream).is_ok()
+    chain_ms = (time.perf_counter() - t0) * 1e3
+    dq = [torch.from_numpy(v).cuda() for v in q]
+    out = torch.empty(n, device="cuda")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+    def call(xs, o):
+        assert g.gwn_compute_winding_number_antipodal_batch(geo, bvh, ch, *xs, o, stream=stream,
+                                                            sort_queries=True).is_ok()
+
+    with ClockSampler(torch.cuda.current_device()) as clocks:
+        t = timed_steps(lambda: call(dq, out), args.steps, args.warmup, stream, flush)
+    ms = float(np.mean(t))
+    hq = [torch.from_numpy(v).pin_memory() for v in q]
+    hout = torch.empty(n).pin_memory()
+    dbuf = [torch.empty(n, device="cuda") for _ in range(3)]
+
+    def e2e_step():
+        for d, h in zip(dbuf, hq):
+            d.copy_(h, non_blocking=True)
+        call(dbuf, out)
+        hout.copy_(out, non_blocking=True)
+
+    e2e = timed_steps(e2e_step, max(3, min(args.steps, 10)), 1, stream, flush)
+    call(dq, out)
+    torch.cuda.synchronize()
+    sub = slice(0, 2000)
+    got = out[sub].cpu().numpy()
+    exact = oracle.exact_winding(mesh, *[v[sub].astype(np.float64) for v in q], fp64=True)
+    err = np.abs(got - exact)
+    ref_ms = None
+    ref_err = None
+    if oracle.ref_lib() is not None:
+        r = oracle.Reference(mesh)
+        r.build(method=0, radius=8)
+        r.boundary()
+        ref_ms = r.time_antipodal(*q, iters=3)
+        ref_err = float(np.nanmax(np.abs(r.antipodal(*[v[sub] for v in q]) - exact)))
+        r.close()
+    edges = ch.edge_count()
+    cpu = None
+    if not args.no_cpu_baseline:
+        from smallgwn_b200 import api
+
+        bh = api.bvh_host_arrays(bvh)
+        rows = ch.rows()
+        threads = oracle.max_threads()
+        done, t0 = 0, time.perf_counter()
+        while time.perf_counter() - t0 < 10.0 and done < n:
+            s = slice(done, min(done + 1000, n))
+            oracle.antipodal(mesh, bh["nodes"], bh["triangles"], bh["root_reference"], rows, *[v[s] for v in q],
+                             threads=threads)
+            done = s.stop
+        dt = time.perf_counter() - t0
+        cpu = {"value": done / dt, "unit": "queries/s", "cores": threads, "kind": "port",
+               "sample": f"{done} of the {n} queries in {dt:.1f} s"}
+    line = {
+        "metric": "Antipodal winding queries/s on the 159k-triangle open soup",
+        "value": n / (ms / 1e3), "unit": "queries/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": "UV 316x316 displaced sphere, 20% of triangles deleted, 5% flipped (seed 3), "
+                               f"{n} mixed queries", "triangles": int(mesh["i0"].size), "boundary_rows": edges,
+                   "builder": "hploc r=8", "query_order": "hilbert-sorted in batch",
+                   "l2": "flushed (256 MiB write) between timed steps",
+                   "row_evaluations_per_s": n * edges / (ms / 1e3), "boundary_chain_build_ms": chain_ms,
+                   "max_err_vs_fp64_exact": float(err.max()), "p99_err_vs_fp64_exact": float(np.quantile(err, 0.99)),
+                   "error_subset": 2000, "smallgwn_gpu_queries_per_s": (n / (ref_ms / 1e3)) if ref_ms else None,
+                   "smallgwn_max_err_vs_fp64_exact": ref_err},
+        "cpu_baseline": cpu,
+        "e2e": {"value": n / (float(np.mean(e2e)) / 1e3), "unit": "queries/s", "h2d_bytes_per_step": 12 * n,
+                "d2h_bytes_per_step": 4 * n},
+        "gpu_launches": 8 * args.steps,  # edge records, codes, histogram, 4 digit passes, antipodal
+        "clocks": clocks.summary(),
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main() -> None:
     args = parse()
     if args.profile is not None:
@@ -1008,7 +1111,7 @@ def main() -> None:
     if args.workload != "taylor":
         {"adjoint": run_adjoint_workload, "precision": run_precision_workload, "exact": run_exact_workload,
          "batched": run_batched_workload, "distance": run_spatial_workload,
-         "ray": run_spatial_workload}[args.workload](args)
+         "ray": run_spatial_workload, "antipodal": run_antipodal_workload}[args.workload](args)
         return
     import torch
 

@@ -7,6 +7,8 @@
 //   exact vs CPU, asymmetric octahedron  tests/unit_gwn_query_winding.cu:193-215
 //   full-descent Taylor == exact    tests/unit_gwn_bvh_moment.cu:42-114
 //   stale moments are rejected      tests/unit_gwn_bvh_moment.cu:116-156
+//   distance and ray on 12 layers   tests/unit_gwn_query_distance_ray.cu:361-396
+//   open-cube boundary, antipodal   tests/unit_gwn_boundary.cu:125-150, tests/unit_gwn_query_antipodal.cu:368-381
 // Exit code 0 when every check passes; `--compile-only` exits before touching the GPU.
 #include <gwn/gwn.cuh>
 
@@ -188,6 +190,79 @@ void queries_match_cpu() {
     }
 }
 
+void distance_and_ray_on_layers() {
+    std::vector<float> x, y, z;
+    std::vector<Index> i0, i1, i2;
+    for (Index t = 0; t < 12; ++t) {
+        Index const v = static_cast<Index>(x.size());
+        x.insert(x.end(), {0, 1, 0});
+        y.insert(y.end(), {0, 0, 1});
+        z.insert(z.end(), {float(t), float(t), float(t)});
+        i0.push_back(v);
+        i1.push_back(v + 1);
+        i2.push_back(v + 2);
+    }
+    gwn::gwn_geometry_object<Real, Index> geometry;
+    CHECK(gwn::gwn_upload_geometry(geometry, hs(x), hs(y), hs(z), hs(i0), hs(i1), hs(i2)).is_ok());
+    gwn::gwn_bvh4_object<Real, Index> bvh;
+    CHECK(gwn::gwn_build_bvh(geometry, bvh).is_ok());
+    dbuf ox(std::vector<float>{0.25f, 2, 0}), oy(std::vector<float>{0.25f, 2, 0.25f}), oz(std::vector<float>{20, 20, 20});
+    dbuf dx(std::vector<float>{0, 0, 0}), dy(std::vector<float>{0, 0, 0}), dz(std::vector<float>{-1, -1, -1});
+    gwn::gwn_ray_first_hit_result<Real, Index> *hits = nullptr;
+    cudaMalloc(&hits, 3 * sizeof(*hits));
+    CHECK(gwn::gwn_compute_ray_first_hit_batch(bvh, ox.in(), oy.in(), oz.in(), dx.in(), dy.in(), dz.in(),
+                                               gwn::gwn_device_span<gwn::gwn_ray_first_hit_result<Real, Index>>(hits, 3))
+              .is_ok());
+    std::vector<gwn::gwn_ray_first_hit_result<Real, Index>> h(3);
+    cudaDeviceSynchronize();
+    cudaMemcpy(h.data(), hits, 3 * sizeof(*hits), cudaMemcpyDeviceToHost);
+    cudaFree(hits);
+    CHECK(h[0].hit() && h[0].t == 9 && h[0].primitive_id == 11);
+    CHECK(!h[1].hit() && h[1].t == -1 && h[1].primitive_id == gwn::gwn_invalid_index<Index>());
+    CHECK(h[2].hit() && h[2].t == 9 && h[2].primitive_id == 11);
+    dbuf qx(std::vector<float>{0.25f, 0.25f, 0}), qy(std::vector<float>{0.25f, 0.25f, 0.25f}),
+        qz(std::vector<float>{10.25f, 30, 10.25f}), d(3);
+    CHECK(gwn::gwn_compute_unsigned_distance_batch(bvh, qx.in(), qy.in(), qz.in(), d.out(), Real(2)).is_ok());
+    auto hd = d.host();
+    CHECK(hd[0] == 0.25f && hd[1] == 2 && hd[2] == 0.25f);
+}
+
+void open_cube_boundary_and_antipodal() {
+    std::vector<float> x{-1, 1, 1, -1, -1, 1, 1, -1}, y{-1, -1, 1, 1, -1, -1, 1, 1}, z{-1, -1, -1, -1, 1, 1, 1, 1};
+    std::vector<Index> i0{0, 0, 0, 0, 1, 1, 0, 0, 3, 3}, i1{2, 3, 4, 7, 2, 6, 1, 5, 7, 6}, i2{1, 2, 7, 3, 6, 5, 5, 4, 6, 2};
+    gwn::gwn_geometry_object<Real, Index> geometry;
+    CHECK(gwn::gwn_upload_geometry(geometry, hs(x), hs(y), hs(z), hs(i0), hs(i1), hs(i2)).is_ok());
+    gwn::gwn_boundary_chain_object<Index> chain;
+    CHECK(gwn::gwn_build_boundary_chain(geometry, chain).is_ok());
+    CHECK(chain.has_data() && chain.accessor().edge_count() == 4);
+    auto st = to_host(chain.accessor().start_vertex);
+    auto en = to_host(chain.accessor().end_vertex);
+    auto mu = to_host(chain.accessor().multiplicity);
+    int found = 0;
+    for (std::size_t i = 0; i < st.size(); ++i)
+        for (auto [a, b] : {std::pair<Index, Index>{4, 7}, {5, 4}, {6, 5}, {7, 6}})
+            found += (st[i] == a && en[i] == b && mu[i] == 1) ? 1 : 0;
+    CHECK(found == 4);
+    gwn::gwn_bvh4_object<Real, Index> bvh;
+    CHECK(gwn::gwn_build_bvh(geometry, bvh).is_ok());
+    std::vector<float> qx{0.23f, 2.2f, -0.41f, -2.3f}, qy{0.17f, 0.3f, 0.26f, -0.4f}, qz{0.11f, 0.2f, 1.7f, 0.5f};
+    dbuf dx(qx), dy(qy), dz(qz), w(qx.size()), gx(qx.size()), gy(qx.size()), gz(qx.size());
+    CHECK(gwn::gwn_compute_winding_number_antipodal_batch(geometry, bvh, chain, dx.in(), dy.in(), dz.in(), w.out())
+              .is_ok());
+    CHECK(gwn::gwn_compute_winding_gradient_antipodal_batch(geometry, chain, dx.in(), dy.in(), dz.in(), gx.out(),
+                                                            gy.out(), gz.out())
+              .is_ok());
+    auto hw = w.host();
+    auto hg = gx.host();
+    for (std::size_t i = 0; i < qx.size(); ++i) {
+        CHECK(std::abs(hw[i] - cpu_winding(x, y, z, i0, i1, i2, qx[i], qy[i], qz[i])) <= 3e-4);
+        CHECK(std::isfinite(hg[i]));
+    }
+    gwn::gwn_boundary_chain_object<Index> missing;
+    CHECK(gwn::gwn_compute_winding_number_antipodal_batch(geometry, bvh, missing, dx.in(), dy.in(), dz.in(), w.out())
+              .error() == gwn::gwn_error::invalid_argument);
+}
+
 } // namespace
 
 int main(int argc, char **argv) {
@@ -197,6 +272,8 @@ int main(int argc, char **argv) {
     two_triangle_records_and_refit();
     rejected_options_keep_bvh();
     queries_match_cpu();
+    distance_and_ray_on_layers();
+    open_cube_boundary_and_antipodal();
     if (g_failures == 0)
         std::printf("dropin_test: all checks passed\n");
     return g_failures == 0 ? 0 : 1;
