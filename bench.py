@@ -59,7 +59,7 @@ def parse() -> argparse.Namespace:
     ap.add_argument("--beta", type=float, default=BETA)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile", choices=["taylor", "taylor-plain", "taylor-thread", "build", "exact", "adjoint",
-                                          "distance", "ray"],
+                                          "distance", "ray", "antipodal"],
                     default=None,
                     help="run one small workload for a profiler (no JSON): 2 launches of the kernel")
     return ap.parse_args()
@@ -76,6 +76,23 @@ def run_profile(args) -> None:
     from smallgwn_b200 import api, meshes
 
     stream = torch.cuda.current_stream()
+    if args.profile == "antipodal":
+        # two antipodal batches on the open soup (316 x 316, seed 3), queries in Hilbert order
+        mesh = meshes.soup_mesh(316, seed=3)
+        q = meshes.mixed_queries(mesh, args.queries, seed=3)
+        geo = g.gwn_geometry_object()
+        assert g.gwn_upload_geometry(geo, mesh["x"], mesh["y"], mesh["z"], mesh["i0"], mesh["i1"], mesh["i2"]).is_ok()
+        bvh = g.gwn_bvh4_object()
+        assert g.gwn_build_bvh(geo, bvh, g.gwn_bvh_build_options(method=0, hploc_search_radius=8)).is_ok()
+        ch = g.gwn_boundary_chain_object()
+        assert g.gwn_build_boundary_chain(geo, ch).is_ok()
+        dq = [torch.from_numpy(np.ascontiguousarray(v)).cuda() for v in q]
+        out = torch.empty_like(dq[0])
+        for _ in range(2):
+            assert g.gwn_compute_winding_number_antipodal_batch(geo, bvh, ch, *dq, out, sort_queries=True).is_ok()
+        torch.cuda.synchronize()
+        print("profile antipodal ok")
+        return
     if args.profile in ("distance", "ray"):
         # the traversal kernel over inputs already in the batch's own order, twice
         ray = args.profile == "ray"
