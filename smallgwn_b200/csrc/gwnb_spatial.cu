@@ -6,9 +6,10 @@
 // 63-238. Same traversal order as smallgwn's canonical traversal -- a node's valid children are
 // compacted in slot order, sorted near-first by the five-comparator network, leaf children are
 // evaluated inside their node, internal children queued far to near with the nearest entered
-// directly -- and the same float arithmetic in the same operation order with every product, sum,
-// quotient and square root rounded on its own (explicit _rn intrinsics, no FMA contraction), so
-// the results equal a plain IEEE single-precision evaluation of smallgwn's source bit for bit.
+// directly -- and smallgwn's formulas in its operation order, every sum, quotient and square root
+// rounded on its own and dot products, cross products, 2 x 2 determinants and slab bounds fused in
+// one fixed pattern of multiply-adds (explicit _rn intrinsics); the oracle restates the same pattern
+// with C's fmaf, so results equal it bit for bit (smallgwn leaves contraction to its compiler).
 //
 // Differences: queries may be taken in Hilbert order of the query points / ray origins (the batch
 // writes results at their input positions); node children are read as 128-bit loads and triangles
