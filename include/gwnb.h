@@ -395,6 +395,45 @@ GWNB_API int gwnb_ray_order_f32(const gwnb_bvh4_f32 *bvh, const float *ray_origi
 GWNB_API int gwnb_query_order_f32(const gwnb_bvh4_f32 *bvh, const float *query_x, const float *query_y,
                                   const float *query_z, uint64_t count, uint32_t *order, gwnb_stream_t stream);
 
+/* ---- mesh and scene files ------------------------------------------------------------------ */
+
+/* Host triangle mesh (SoA): what smallgwn's tests load into their HostMesh
+ * (tests/test_mesh_io.hpp). Arrays from gwnb_mesh_read_ply are malloc'd; free them with
+ * gwnb_host_mesh_free. */
+typedef struct gwnb_host_mesh_f32 {
+    float *x, *y, *z;
+    uint64_t vertex_count;
+    uint32_t *i0, *i1, *i2;
+    uint64_t triangle_count;
+} gwnb_host_mesh_f32;
+
+/* Replaces smallgwn's test helper gwn::tests::load_ply_mesh (tests/test_mesh_io.cpp:43-92, libigl's
+ * reader): ASCII or binary (either byte order) PLY with any numeric property types; vertex x, y, z
+ * narrowed to float; the face index list ("vertex_indices", else the face element's first list)
+ * with polygons split into triangle fans. Refuses non-finite positions, out-of-range indices,
+ * faces with fewer than three vertices and meshes without vertices or triangles. */
+GWNB_API int gwnb_mesh_read_ply(const char *path, gwnb_host_mesh_f32 *out);
+
+/* Frees the arrays of a mesh read by gwnb_mesh_read_ply and zeroes it. */
+GWNB_API void gwnb_host_mesh_free(gwnb_host_mesh_f32 *mesh);
+
+/* Writes a host mesh as PLY (float positions, uint32 index lists); binary = 1 for
+ * binary_little_endian, 0 for ASCII. No smallgwn counterpart. */
+GWNB_API int gwnb_mesh_write_ply(const char *path, const gwnb_host_mesh_f32 *mesh, int binary);
+
+/* Saves geometry, BVH and up to three moment objects (one per order) in one file, so that a later
+ * process skips the build (no smallgwn counterpart: smallgwn rebuilds every run). Synchronizes
+ * `stream`. */
+GWNB_API int gwnb_scene_save_f32(const char *path, const gwnb_geometry_f32 *geometry, const gwnb_bvh4_f32 *bvh,
+                                 const gwnb_moment4_f32 *const *moments, int moment_count, gwnb_stream_t stream);
+
+/* Loads a scene file: new geometry and BVH views (a fresh revision) and, for every moment order
+ * saved in the file, a moment view in moments[order] refit from the loaded BVH and checked equal to
+ * the saved nodes. *moment_mask (may be NULL) receives the saved orders as bits 0-2. Refuses
+ * files with a bad magic, version or checksum. Synchronizes `stream`. */
+GWNB_API int gwnb_scene_load_f32(const char *path, gwnb_geometry_f32 *geometry, gwnb_bvh4_f32 *bvh,
+                                 gwnb_moment4_f32 moments[3], int *moment_mask, gwnb_stream_t stream);
+
 /* Largest batch gwnb_winding_taylor_batch_noalloc_f32 accepts. */
 #define GWNB_NOALLOC_MAX_QUERIES 262144u
 

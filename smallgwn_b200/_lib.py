@@ -160,6 +160,13 @@ class boundary_chain_u32(C.Structure):
     ]
 
 
+class host_mesh_f32(C.Structure):
+    _fields_ = [
+        ("x", C.c_void_p), ("y", C.c_void_p), ("z", C.c_void_p), ("vertex_count", C.c_uint64),
+        ("i0", C.c_void_p), ("i1", C.c_void_p), ("i2", C.c_void_p), ("triangle_count", C.c_uint64),
+    ]
+
+
 class binary_node(C.Structure):
     _fields_ = [(n, C.c_uint32) for n in ("left_index", "left_kind", "right_index", "right_kind")]
 
@@ -216,6 +223,13 @@ SIGNATURES: dict[str, tuple] = {
             C.POINTER(spatial_options), P]),
     "gwnb_winding_gradient_antipodal_batch_f32": (
         I, [C.POINTER(geometry_f32), C.POINTER(boundary_chain_u32), P, P, P, P, P, P, U64, I, P]),
+    "gwnb_mesh_read_ply": (I, [C.c_char_p, C.POINTER(host_mesh_f32)]),
+    "gwnb_host_mesh_free": (None, [C.POINTER(host_mesh_f32)]),
+    "gwnb_mesh_write_ply": (I, [C.c_char_p, C.POINTER(host_mesh_f32), I]),
+    "gwnb_scene_save_f32": (
+        I, [C.c_char_p, C.POINTER(geometry_f32), C.POINTER(bvh4_f32), C.POINTER(C.POINTER(moment4_f32)), I, P]),
+    "gwnb_scene_load_f32": (
+        I, [C.c_char_p, C.POINTER(geometry_f32), C.POINTER(bvh4_f32), C.POINTER(moment4_f32), C.POINTER(I), P]),
     "gwnb_ray_order_f32": (I, [C.POINTER(bvh4_f32), P, P, P, P, P, P, U64, P, P]),
     "gwnb_spatial_stats_f32": (
         I, [C.POINTER(bvh4_f32), I, P, P, P, P, P, P, U64, F, F, F, P, P, P]),

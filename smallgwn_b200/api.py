@@ -581,6 +581,75 @@ def ray_order(bvh: gwn_bvh4_object, ox, oy, oz, dx, dy, dz, order, stream=None) 
     return _status(rc)
 
 
+# ---- mesh and scene files ---------------------------------------------------------------------------
+
+def read_ply(path) -> dict:
+    """Triangle mesh of a PLY file (ASCII or binary; polygons split into fans) as the SoA dict the
+    upload takes (x, y, z float32; i0, i1, i2 uint32). Raises ValueError on a refused file, as
+    smallgwn's test loader returns no mesh (tests/test_mesh_io.cpp:43-92)."""
+    lib = _lib.load()
+    m = _lib.host_mesh_f32()
+    rc = lib.gwnb_mesh_read_ply(str(path).encode(), C.byref(m))
+    if rc != _lib.GWNB_OK:
+        raise ValueError(_lib.last_error())
+    try:
+        nv, nt = int(m.vertex_count), int(m.triangle_count)
+        fa = C.POINTER(C.c_float)
+        ua = C.POINTER(C.c_uint32)
+        out = {k: np.ctypeslib.as_array(C.cast(getattr(m, k), fa), (nv,)).copy() for k in "xyz"}
+        out.update({k: np.ctypeslib.as_array(C.cast(getattr(m, k), ua), (nt,)).copy() for k in ("i0", "i1", "i2")})
+    finally:
+        lib.gwnb_host_mesh_free(C.byref(m))
+    return out
+
+
+def write_ply(path, mesh: dict, binary: bool = True) -> None:
+    """Write a SoA mesh dict as PLY (float positions, uint32 index lists)."""
+    arrs = {k: np.ascontiguousarray(mesh[k], np.float32) for k in "xyz"}
+    arrs.update({k: np.ascontiguousarray(mesh[k], np.uint32) for k in ("i0", "i1", "i2")})
+    m = _lib.host_mesh_f32(arrs["x"].ctypes.data, arrs["y"].ctypes.data, arrs["z"].ctypes.data, arrs["x"].size,
+                           arrs["i0"].ctypes.data, arrs["i1"].ctypes.data, arrs["i2"].ctypes.data, arrs["i0"].size)
+    rc = _lib.load().gwnb_mesh_write_ply(str(path).encode(), C.byref(m), 1 if binary else 0)
+    if rc != _lib.GWNB_OK:
+        raise ValueError(_lib.last_error())
+
+
+def save_scene(path, geometry, bvh: gwn_bvh4_object, moments=(), stream=None) -> gwn_status:
+    """Save geometry, BVH and moment objects (at most one per order) to one file."""
+    ms = list(moments)
+    arr = (C.POINTER(_lib.moment4_f32) * max(len(ms), 1))(*[C.pointer(m._view) for m in ms])
+    rc = _lib.load().gwnb_scene_save_f32(str(path).encode(), C.byref(geometry.accessor()), C.byref(bvh._view), arr,
+                                         len(ms), _stream(stream))
+    return _status(rc)
+
+
+def load_scene(path, stream=None):
+    """Load a scene file: (status, geometry object, BVH object, {order: moment object}) with the
+    moments refit from the loaded BVH and checked equal to the saved ones."""
+    g = _lib.geometry_f32()
+    b = _lib.bvh4_f32()
+    ms = (_lib.moment4_f32 * 3)()
+    mask = C.c_int(0)
+    rc = _lib.load().gwnb_scene_load_f32(str(path).encode(), C.byref(g), C.byref(b), ms, C.byref(mask),
+                                         _stream(stream))
+    if rc != _lib.GWNB_OK:
+        return _status(rc), None, None, {}
+    geo = gwn_geometry_object()
+    geo._view = g
+    geo.set_stream(stream)
+    bvh = gwn_bvh4_object()
+    bvh._view = b
+    bvh.set_stream(stream)
+    moments = {}
+    for order in range(3):
+        if mask.value & (1 << order):
+            mo = gwn_bvh4_moment_object(order)
+            mo._view = ms[order]
+            mo.set_stream(stream)
+            moments[order] = mo
+    return gwn_status(), geo, bvh, moments
+
+
 def query_order(bvh: gwn_bvh4_object, qx, qy, qz, order, stream=None) -> gwn_status:
     """Traversal-coherent (Hilbert) order of a query batch; `order` is an int32 CUDA tensor."""
     rc = _lib.load().gwnb_query_order_f32(C.byref(bvh._view), _ptr(qx), _ptr(qy), _ptr(qz), _numel(qx), _ptr(order),
