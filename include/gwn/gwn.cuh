@@ -9,5 +9,6 @@
 #include "gwn_bvh_build.cuh"
 #include "gwn_bvh_refit.cuh"
 #include "gwn_geometry.cuh"
+#include "gwn_mesh_io.cuh"
 #include "gwn_query.cuh"
 #include "gwn_utils.cuh"

@@ -140,7 +140,7 @@ template <int Order, gwn_query_batch_config Config = gwn_query_batch_config{}, i
         gwnb_bvh4_f32 v = detail::query_view(bvh);
         gwnb_moment4_f32 m = moment.view();
         gwnb_taylor_options o{Config.block_size, Config.stack_capacity, options.sort_queries ? 1 : 0,
-                              options.near_precision, options.fp64_threshold};
+                              options.near_precision, options.fp64_threshold, 0};
         int const rc = gwnb_winding_taylor_batch_f32(&v, &m, qx.data(), qy.data(), qz.data(), output.data(),
                                                      output.size(), accuracy_scale, &o, detail::gwnb_stream(stream));
         detail::store_aux(bvh, v);

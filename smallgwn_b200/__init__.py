@@ -31,8 +31,13 @@ from .api import (  # noqa: F401
     gwn_taylor_saved,
     gwn_update_geometry,
     gwn_upload_geometry,
+    gwn_upload_geometry_from_eigen,
     gwn_winding_taylor_backward,
     gwn_winding_taylor_forward,
+    load_scene,
     near_precision,
     ray_hit_records,
+    read_ply,
+    save_scene,
+    write_ply,
 )

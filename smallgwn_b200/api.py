@@ -200,6 +200,33 @@ def gwn_upload_geometry(obj: gwn_geometry_object, x, y, z, i0, i1, i2, stream=No
     return gwn_status()
 
 
+def gwn_upload_geometry_from_eigen(obj: gwn_geometry_object, vertices, triangles, stream=None) -> gwn_status:
+    """Upload an N x 3 vertex matrix and an M x 3 triangle matrix (any array-like: numpy arrays as
+    libigl's bindings return them, row- or column-major). Checks and messages follow smallgwn's
+    include/gwn/gwn_eigen_bridge.cuh:26-132: floating-point indices must be finite and
+    integer-valued, every index in [0, vertex_count); replaces ``obj`` only on success."""
+    V = np.asarray(vertices)
+    F = np.asarray(triangles)
+    if V.ndim != 2 or F.ndim != 2 or V.shape[1] != 3 or F.shape[1] != 3:
+        return gwn_status(gwn_error.invalid_argument, "Eigen inputs must be Nx3 vertices and Mx3 triangles.")
+    nv = V.shape[0]
+    if nv > 0 and nv - 1 > 0xFFFFFFFF:
+        return gwn_status(gwn_error.invalid_argument, "Vertex count exceeds index range.")
+    bad = gwn_status(gwn_error.invalid_argument, "Eigen triangle indices must be integer-valued in [0, vertex_count).")
+    if F.size:
+        if F.dtype.kind == "f":
+            with np.errstate(invalid="ignore"):
+                if not (np.isfinite(F).all() and (np.floor(F) == F).all()):
+                    return bad
+        elif F.dtype.kind not in "iu":
+            return bad
+        if F.min() < 0 or F.max() >= nv:
+            return bad
+    Fi = F.astype(np.uint32)
+    Vf = V.astype(np.float32)
+    return gwn_upload_geometry(obj, Vf[:, 0], Vf[:, 1], Vf[:, 2], Fi[:, 0], Fi[:, 1], Fi[:, 2], stream)
+
+
 def gwn_update_geometry(obj: gwn_geometry_object, x, y, z, stream=None) -> gwn_status:
     """Copy new host (numpy) or device (torch CUDA) positions into an uploaded geometry."""
     lib = _lib.load()

@@ -358,6 +358,41 @@ std::uint64_t checksum(unsigned char const *p, std::size_t n, std::uint64_t h = 
     return h;
 }
 
+// The saved hierarchy is a tree the kernels can walk: a leaf root comes with no nodes; an internal
+// root is node 0; every other node is the internal child of exactly one node with a smaller index
+// (so no cycles); leaf ranges lie inside the primitive order; primitive ids name triangles.
+bool scene_topology_ok(unsigned char const *node_bytes, std::size_t N, std::size_t P, std::size_t T,
+                       std::uint32_t const *prims, std::uint64_t root) {
+    for (std::size_t i = 0; i < P; ++i)
+        if (prims[i] >= T)
+            return false;
+    if (ref_leaf(root))
+        return N == 0 && ref_offset(root) <= P && ref_count(root) <= P - ref_offset(root);
+    if (!ref_internal(root) || ref_offset(root) != 0 || N == 0)
+        return false;
+    std::vector<unsigned char> parents(N, 0);
+    for (std::size_t n = 0; n < N; ++n) {
+        node4 node;
+        std::memcpy(&node, node_bytes + n * sizeof(node4), sizeof(node4));
+        for (child const &c : node.c) {
+            std::uint64_t const r = c.reference;
+            if (!ref_valid(r))
+                continue;
+            std::uint64_t const off = ref_offset(r);
+            if (ref_internal(r)) {
+                if (off <= n || off >= N || parents[off]++ != 0)
+                    return false;
+            } else if (off > P || ref_count(r) > P - off) {
+                return false;
+            }
+        }
+    }
+    for (std::size_t n = 1; n < N; ++n)
+        if (parents[n] != 1)
+            return false;
+    return true;
+}
+
 int copy_to_host(void *dst, void const *src, std::size_t bytes, cudaStream_t s) {
     if (bytes == 0)
         return GWNB_OK;
@@ -536,6 +571,8 @@ int gwnb_scene_load_f32(const char *path, gwnb_geometry_f32 *g_out, gwnb_bvh4_f3
     if (checksum(blob.data(), blob.size() - 8) != stored)
         return set_error(GWNB_INVALID_ARGUMENT, "scene: checksum mismatch (corrupt or truncated file).");
     std::size_t const V = h.vertex_count, T = h.triangle_count, N = h.node_count, P = h.primitive_count;
+    if (V > blob.size() || T > blob.size() || N > blob.size() || P > blob.size()) // keeps the sum below exact
+        return set_error(GWNB_INVALID_ARGUMENT, "scene: inconsistent counts in the header.");
     std::size_t total = sizeof(h) + 3 * V * 4 + 3 * T * 4 + N * 128 + P * 4 + P * 36 + 8;
     for (int o = 0; o < 3; ++o)
         if (h.moment_mask & (1u << o))
@@ -557,6 +594,10 @@ int gwnb_scene_load_f32(const char *path, gwnb_geometry_f32 *g_out, gwnb_bvh4_f3
     unsigned char const *nodes = take(N * 128);
     unsigned char const *prims = take(P * 4);
     unsigned char const *tris = take(P * 36);
+    std::vector<std::uint32_t> prim_ids(P);
+    std::memcpy(prim_ids.data(), prims, P * 4);
+    if (!scene_topology_ok(nodes, N, P, T, prim_ids.data(), h.root.reference))
+        return set_error(GWNB_INVALID_ARGUMENT, "scene: the saved hierarchy is not a valid BVH4 tree.");
     cudaStream_t const s = as_cuda(stream);
     gwnb_geometry_f32 g{};
     GWNB_TRY(gwnb_geometry_upload_f32(&g, x, y, z, V, i0, i1, i2, T, stream));

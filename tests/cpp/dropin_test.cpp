@@ -9,13 +9,21 @@
 //   stale moments are rejected      tests/unit_gwn_bvh_moment.cu:116-156
 //   distance and ray on 12 layers   tests/unit_gwn_query_distance_ray.cu:361-396
 //   open-cube boundary, antipodal   tests/unit_gwn_boundary.cu:125-150, tests/unit_gwn_query_antipodal.cu:368-381
-// Exit code 0 when every check passes; `--compile-only` exits before touching the GPU.
+//   matrix upload (Eigen bridge)    include/gwn/gwn_eigen_bridge.cuh:26-132
+//   PLY meshes, scene files         tests/test_mesh_io.cpp:43-92 (scene files have no counterpart)
+// Exit code 0 when every check passes; `--compile-only` exits before touching the GPU and
+// `--host-checks` runs only the cases that need no GPU.
 #include <gwn/gwn.cuh>
+#include <gwn/gwn_eigen_bridge.cuh>
 
 #include <array>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <filesystem>
+#include <limits>
+#include <string>
+#include <unistd.h>
 #include <vector>
 
 namespace {
@@ -263,17 +271,185 @@ void open_cube_boundary_and_antipodal() {
               .error() == gwn::gwn_error::invalid_argument);
 }
 
+
+/// Row- or column-major dense matrix with Eigen's element interface (rows(), cols(), (r, c)).
+template <class T, bool RowMajor> struct fake_matrix {
+    long r = 0, c = 0;
+    std::vector<T> data;
+    fake_matrix(long rows, long cols, std::vector<T> row_major) : r(rows), c(cols), data(rows * cols) {
+        for (long i = 0; i < rows; ++i)
+            for (long j = 0; j < cols; ++j)
+                (*this)(i, j) = row_major[i * cols + j];
+    }
+    long rows() const { return r; }
+    long cols() const { return c; }
+    T &operator()(long i, long j) { return RowMajor ? data[i * c + j] : data[j * r + i]; }
+    T const &operator()(long i, long j) const { return RowMajor ? data[i * c + j] : data[j * r + i]; }
+};
+
+std::vector<double> const k_cube_v{-1, -1, -1, 1, -1, -1, 1, 1, -1, -1, 1, -1, -1, -1, 1, 1, -1, 1, 1, 1, 1, -1, 1, 1};
+std::vector<int> const k_cube_f{0, 2, 1, 0, 3, 2, 4, 5, 6, 4, 6, 7, 0, 1, 5, 0, 5, 4,
+                                3, 7, 6, 3, 6, 2, 0, 4, 7, 0, 7, 3, 1, 2, 6, 1, 6, 5};
+
+std::filesystem::path scratch(char const *name) {
+    return std::filesystem::temp_directory_path() / (std::string("gwnb_dropin_") + std::to_string(getpid()) + "_" + name);
+}
+
+void eigen_bridge_refusals() {
+    gwn::gwn_geometry_object<Real, Index> geometry;
+    fake_matrix<double, true> v(8, 3, k_cube_v);
+    fake_matrix<double, true> v2(4, 2, std::vector<double>(8, 0.0));
+    fake_matrix<int, false> f(12, 3, k_cube_f);
+    auto st = gwn::gwn_upload_geometry_from_eigen(geometry, v2, f);
+    CHECK(st.error() == gwn::gwn_error::invalid_argument && st.message().find("Nx3") != std::string::npos);
+    for (double bad : {-1.0, 8.0, 1.5, std::numeric_limits<double>::quiet_NaN(), 1e30}) {
+        std::vector<double> fv(k_cube_f.begin(), k_cube_f.end());
+        fv[7] = bad;
+        fake_matrix<double, true> fd(12, 3, fv);
+        st = gwn::gwn_upload_geometry_from_eigen(geometry, v, fd);
+        CHECK(st.error() == gwn::gwn_error::invalid_argument &&
+              st.message().find("integer-valued") != std::string::npos);
+    }
+    std::vector<int> fi = k_cube_f;
+    fi[35] = -3;
+    st = gwn::gwn_upload_geometry_from_eigen(geometry, v, fake_matrix<int, false>(12, 3, fi));
+    CHECK(st.error() == gwn::gwn_error::invalid_argument);
+    CHECK(!geometry.has_data());
+}
+
+void ply_round_trip_on_host() {
+    gwn::gwn_host_mesh mesh;
+    for (std::size_t i = 0; i < 8; ++i) {
+        mesh.vertex_x.push_back(float(k_cube_v[3 * i]) * 0.5f + 0.125f);
+        mesh.vertex_y.push_back(float(k_cube_v[3 * i + 1]));
+        mesh.vertex_z.push_back(float(k_cube_v[3 * i + 2]) * 3.0f);
+    }
+    for (std::size_t t = 0; t < 12; ++t) {
+        mesh.tri_i0.push_back(Index(k_cube_f[3 * t]));
+        mesh.tri_i1.push_back(Index(k_cube_f[3 * t + 1]));
+        mesh.tri_i2.push_back(Index(k_cube_f[3 * t + 2]));
+    }
+    for (bool binary : {true, false}) {
+        auto const path = scratch(binary ? "bin.ply" : "ascii.ply");
+        CHECK(gwn::gwn_write_ply_mesh(path, mesh, binary).is_ok());
+        auto back = gwn::gwn_load_ply_mesh(path);
+        CHECK(back.has_value());
+        if (back) {
+            CHECK(back->vertex_x == mesh.vertex_x && back->vertex_y == mesh.vertex_y && back->vertex_z == mesh.vertex_z);
+            CHECK(back->tri_i0 == mesh.tri_i0 && back->tri_i1 == mesh.tri_i1 && back->tri_i2 == mesh.tri_i2);
+        }
+        std::filesystem::remove(path);
+    }
+    CHECK(!gwn::gwn_load_ply_mesh(scratch("missing.ply")).has_value());
+    gwn::gwn_host_mesh ragged = mesh;
+    ragged.tri_i2.pop_back();
+    CHECK(gwn::gwn_write_ply_mesh(scratch("ragged.ply"), ragged).error() == gwn::gwn_error::invalid_argument);
+}
+
+void eigen_upload_and_scene_files() {
+    // a column-major int index matrix and a row-major double vertex matrix give the same geometry
+    // as the SoA upload
+    gwn::gwn_geometry_object<Real, Index> from_matrix;
+    CHECK(gwn::gwn_upload_geometry_from_eigen(from_matrix, fake_matrix<double, true>(8, 3, k_cube_v),
+                                              fake_matrix<int, false>(12, 3, k_cube_f))
+              .is_ok());
+    CHECK(from_matrix.vertex_count() == 8 && from_matrix.triangle_count() == 12);
+    auto hx = to_host(from_matrix.accessor().vertex_y);
+    auto h2 = to_host(from_matrix.accessor().tri_i2);
+    for (std::size_t i = 0; i < 8; ++i)
+        CHECK(hx[i] == float(k_cube_v[3 * i + 1]));
+    for (std::size_t t = 0; t < 12; ++t)
+        CHECK(h2[t] == Index(k_cube_f[3 * t + 2]));
+
+    // PLY -> upload -> build -> moments -> scene file -> load: equal Taylor results
+    gwn::gwn_host_mesh mesh;
+    auto const ply = scratch("scene_mesh.ply");
+    {
+        gwn::gwn_host_mesh m;
+        for (int k = 0; k < 3; ++k) // three nested cubes
+            for (std::size_t i = 0; i < 8; ++i) {
+                m.vertex_x.push_back(float(k_cube_v[3 * i]) * (1 + k) + 0.1f * k);
+                m.vertex_y.push_back(float(k_cube_v[3 * i + 1]) * (1 + k));
+                m.vertex_z.push_back(float(k_cube_v[3 * i + 2]) * (1 + k) - 0.2f * k);
+            }
+        for (int k = 0; k < 3; ++k)
+            for (std::size_t t = 0; t < 12; ++t) {
+                m.tri_i0.push_back(Index(k_cube_f[3 * t] + 8 * k));
+                m.tri_i1.push_back(Index(k_cube_f[3 * t + 1] + 8 * k));
+                m.tri_i2.push_back(Index(k_cube_f[3 * t + 2] + 8 * k));
+            }
+        CHECK(gwn::gwn_write_ply_mesh(ply, m).is_ok());
+    }
+    CHECK(gwn::gwn_read_ply_mesh(ply, mesh).is_ok());
+    std::filesystem::remove(ply);
+    gwn::gwn_geometry_object<Real, Index> geometry;
+    CHECK(gwn::gwn_upload_geometry(geometry, mesh).is_ok());
+    gwn::gwn_bvh4_object<Real, Index> bvh;
+    CHECK(gwn::gwn_build_bvh(geometry, bvh).is_ok());
+    gwn::gwn_bvh4_moment_object<1, Real, Index> m1;
+    gwn::gwn_bvh4_moment_object<2, Real, Index> m2;
+    CHECK(gwn::gwn_refit_bvh_moment<1>(bvh, m1).is_ok());
+    CHECK(gwn::gwn_refit_bvh_moment<2>(bvh, m2).is_ok());
+    auto const scene = scratch("scene.gwnb");
+    CHECK(gwn::gwn_save_scene(scene, geometry, bvh, m1, m2).is_ok());
+
+    gwn::gwn_geometry_object<Real, Index> g2;
+    gwn::gwn_bvh4_object<Real, Index> b2;
+    gwn::gwn_bvh4_moment_object<0, Real, Index> l0;
+    gwn::gwn_bvh4_moment_object<1, Real, Index> l1;
+    gwn::gwn_bvh4_moment_object<2, Real, Index> l2;
+    CHECK(gwn::gwn_refit_bvh_moment<0>(bvh, l0).is_ok()); // replaced by "not saved" on load
+    int orders = 0;
+    CHECK(gwn::gwn_load_scene(scene, g2, b2, &l0, &l1, &l2, &orders).is_ok());
+    CHECK(orders == 6 && !l0.has_data() && l1.accessor().is_valid_for(b2.accessor()) &&
+          l2.accessor().is_valid_for(b2.accessor()));
+    CHECK(g2.vertex_count() == 24 && g2.triangle_count() == 36 && b2.accessor().revision != bvh.accessor().revision);
+    std::vector<float> qx{0.05f, 1.5f, 2.5f, -3.9f, 7}, qy{0.1f, -0.3f, 2.2f, 0.4f, 1}, qz{-0.2f, 0.7f, -2.1f, 3.3f, 0};
+    dbuf dx(qx), dy(qy), dz(qz), a(qx.size()), b(qx.size());
+    CHECK(gwn::gwn_compute_winding_number_taylor_batch<2>(bvh, m2, dx.in(), dy.in(), dz.in(), a.out()).is_ok());
+    CHECK(gwn::gwn_compute_winding_number_taylor_batch<2>(b2, l2, dx.in(), dy.in(), dz.in(), b.out()).is_ok());
+    auto ha = a.host();
+    auto hb = b.host();
+    CHECK(ha == hb);
+    CHECK(std::abs(ha[0] - 3) < 2e-2 && std::abs(ha[1] - 2) < 2e-2 && std::abs(ha[4]) < 2e-2);
+
+    // a damaged file is refused and leaves the targets as they were
+    {
+        std::FILE *f = std::fopen(scene.string().c_str(), "r+b");
+        CHECK(f != nullptr);
+        if (f) {
+            std::fseek(f, 120, SEEK_SET);
+            int const c = std::fgetc(f);
+            std::fseek(f, 120, SEEK_SET);
+            std::fputc(c ^ 0x10, f);
+            std::fclose(f);
+        }
+    }
+    auto const *before = b2.accessor().nodes.data();
+    auto st = gwn::gwn_load_scene(scene, g2, b2, nullptr, &l1);
+    CHECK(st.error() == gwn::gwn_error::invalid_argument && b2.accessor().nodes.data() == before && l1.has_data());
+    std::filesystem::remove(scene);
+}
+
 } // namespace
 
 int main(int argc, char **argv) {
     if (argc > 1 && std::strcmp(argv[1], "--compile-only") == 0)
         return 0;
+    eigen_bridge_refusals();
+    ply_round_trip_on_host();
+    if (argc > 1 && std::strcmp(argv[1], "--host-checks") == 0) {
+        if (g_failures == 0)
+            std::printf("dropin_test: host checks passed\n");
+        return g_failures == 0 ? 0 : 1;
+    }
     leaf_root_build();
     two_triangle_records_and_refit();
     rejected_options_keep_bvh();
     queries_match_cpu();
     distance_and_ray_on_layers();
     open_cube_boundary_and_antipodal();
+    eigen_upload_and_scene_files();
     if (g_failures == 0)
         std::printf("dropin_test: all checks passed\n");
     return g_failures == 0 ? 0 : 1;

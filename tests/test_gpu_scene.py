@@ -92,3 +92,19 @@ def test_damaged_and_partial_files(cuda, tmp_path):
     m1b = g.gwn_bvh4_moment_object(1)
     assert g.gwn_refit_bvh_moment(1, bvh, m1b).is_ok()
     assert "same order" in api.save_scene(path, geo, bvh, [m1, m1b]).message
+
+
+@pytest.mark.parametrize("order", ["C", "F"])
+def test_matrix_upload_equals_soa_upload(cuda, order):
+    """N x 3 / M x 3 matrices (double positions, int32 or integer-valued float indices, either
+    memory order) upload to the same device arrays as the SoA upload."""
+    mesh = meshes.soup_mesh(40, seed=8)
+    V = np.asarray(np.stack([mesh["x"], mesh["y"], mesh["z"]], axis=1).astype(np.float64), order=order)
+    F = np.stack([mesh["i0"], mesh["i1"], mesh["i2"]], axis=1)
+    ref = host_geometry(upload(mesh))
+    for Fm in (np.asarray(F.astype(np.int32), order=order), F.astype(np.float64)):
+        geo = g.gwn_geometry_object()
+        assert g.gwn_upload_geometry_from_eigen(geo, V, Fm).is_ok()
+        got = host_geometry(geo)
+        for k in ref:
+            np.testing.assert_array_equal(got[k], ref[k])

@@ -138,3 +138,75 @@ def test_scene_files_are_checked_on_the_host(tmp_path):
                                    None) == _lib.GWNB_INVALID_ARGUMENT
     status, *_ = api.load_scene(tmp_path / "missing")
     assert status.error == api.gwn_error.invalid_argument
+
+
+def test_matrix_upload_refusals():
+    """gwn_upload_geometry_from_eigen refuses what smallgwn's Eigen bridge refuses, before any
+    device work (include/gwn/gwn_eigen_bridge.cuh:32-113)."""
+    geo = api.gwn_geometry_object()
+    m = cube()
+    V = np.stack([m["x"], m["y"], m["z"]], axis=1).astype(np.float64)
+    F = np.stack([m["i0"], m["i1"], m["i2"]], axis=1).astype(np.int64)
+    st = api.gwn_upload_geometry_from_eigen(geo, V[:, :2], F)
+    assert st.error == api.gwn_error.invalid_argument and "Nx3" in st.message
+    for bad in (-1, 8, 1.5, np.nan, np.inf):
+        Fb = F.astype(np.float64)
+        Fb[3, 1] = bad
+        st = api.gwn_upload_geometry_from_eigen(geo, V, Fb)
+        assert st.error == api.gwn_error.invalid_argument and "integer-valued" in st.message, bad
+    Fi = F.copy()
+    Fi[0, 0] = -2
+    assert api.gwn_upload_geometry_from_eigen(geo, V, Fi).error == api.gwn_error.invalid_argument
+    assert api.gwn_upload_geometry_from_eigen(geo, V, F.astype(bool)).error == api.gwn_error.invalid_argument
+    assert not geo.has_data()
+
+
+def _scene_checksum(body: bytes) -> int:
+    """FNV-1a over little-endian 8-byte words, then the tail bytes (the scene file's checksum)."""
+    h, prime, mask = 0xCBF29CE484222325, 0x100000001B3, (1 << 64) - 1
+    n8 = len(body) // 8 * 8
+    for (w,) in np.frombuffer(body[:n8], "<u8").reshape(-1, 1):
+        h = ((h ^ int(w)) * prime) & mask
+    for b in body[n8:]:
+        h = ((h ^ b) * prime) & mask
+    return h
+
+
+def _crafted_scene(nodes_refs, prims, root_ref) -> bytes:
+    """A scene of 4 vertices / 2 triangles with the given node references (one list of 4 per node),
+    primitive order and root reference, and a correct checksum."""
+    V, T, N, P = 4, 2, len(nodes_refs), len(prims)
+    root = np.zeros(1, [("b", "<f4", 6), ("r", "<u8")])
+    root["r"] = root_ref
+    head = b"GWNBSCN1" + np.array([1, 0], "<u4").tobytes() + np.array([V, T, N, P], "<u8").tobytes()
+    head += root.tobytes() + np.array([4, 8], "<u4").tobytes()
+    assert len(head) == 88
+    body = np.zeros(3 * V, "<f4").tobytes() + np.array([0, 1, 2, 3, 2, 1], "<u4").tobytes()
+    node = np.zeros((N, 4), [("b", "<f4", 6), ("r", "<u8")])
+    for n, refs in enumerate(nodes_refs):
+        node["r"][n] = refs
+    body += node.tobytes() + np.asarray(prims, "<u4").tobytes() + np.zeros(P * 9, "<f4").tobytes()
+    blob = head + body
+    return blob + _scene_checksum(blob).to_bytes(8, "little")
+
+
+@pytest.mark.parametrize("nodes_refs, prims, root, why", [
+    ([[(1 << 47) | 0, 0, 0, 0]], [0, 1], 1 << 47, "self loop"),                  # node 0 names itself
+    ([[(1 << 47) | (1 << 48) | 1, (1 << 47) | (2 << 48) | 1, 0, 0]], [0, 1], 1 << 47, "leaf past the end"),
+    ([[(1 << 47) | (1 << 48) | 0, (1 << 47) | (1 << 48) | 1, 0, 0]], [0, 5], 1 << 47, "bad primitive id"),
+    ([[(1 << 47) | 1, (1 << 47) | (2 << 48) | 0, 0, 0], [0, 0, 0, 0]], [0, 1], (1 << 47) | 1, "root not node 0"),
+    ([[(1 << 47) | 1, (1 << 47) | 1, 0, 0], [(1 << 47) | (2 << 48), 0, 0, 0]], [0, 1], 1 << 47, "two parents"),
+    ([[], ], [0, 1], (1 << 47) | (2 << 48), "leaf root with nodes"),
+])
+def test_scene_load_refuses_malformed_trees_on_host(tmp_path, nodes_refs, prims, root, why):
+    """Files with a correct checksum whose hierarchy is not a tree the kernels can walk are refused
+    before any upload."""
+    refs = [r + [0] * (4 - len(r)) for r in nodes_refs]
+    p = tmp_path / "crafted.gwnb"
+    p.write_bytes(_crafted_scene(refs, prims, root))
+    lib = _lib.load()
+    g, b = _lib.geometry_f32(), _lib.bvh4_f32()
+    ms, mask = (_lib.moment4_f32 * 3)(), C.c_int()
+    rc = lib.gwnb_scene_load_f32(str(p).encode(), C.byref(g), C.byref(b), ms, C.byref(mask), None)
+    assert rc == _lib.GWNB_INVALID_ARGUMENT, why
+    assert "not a valid BVH4 tree" in _lib.last_error(), (why, _lib.last_error())
