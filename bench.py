@@ -378,11 +378,19 @@ def run_adjoint_workload(args) -> None:
     import smallgwn_b200 as g
     from smallgwn_b200 import api, meshes
 
+    from smallgwn_b200 import sharding
+
+    rank, world, dist_ = dist_setup(args.gpus)
     n = args.queries if args.queries != N_QUERIES else 1_000_000
     order, beta, h = 1, 2.0, 1e-4
     mesh = meshes.soup_mesh(316, seed=3)
-    q = meshes.mixed_queries(mesh, n, seed=3)
-    w = np.random.default_rng(3).normal(size=n).astype(np.float32)
+    q_all = meshes.mixed_queries(mesh, n, seed=3)
+    w_all = np.random.default_rng(3).normal(size=n).astype(np.float32)
+    # several GPUs: the query batch is split into contiguous ranges, dL/dV summed by one all-reduce
+    lo, hi = sharding.shard_range(n, rank, world)
+    q = [x[lo:hi] for x in q_all]
+    w = w_all[lo:hi]
+    n_total, n = n, hi - lo
     stream = torch.cuda.current_stream()
     geo = g.gwn_geometry_object()
     assert g.gwn_upload_geometry(geo, mesh["x"], mesh["y"], mesh["z"], mesh["i0"], mesh["i1"], mesh["i2"]).is_ok()
@@ -410,11 +418,55 @@ def run_adjoint_workload(args) -> None:
     def step():
         fwd()
         bwd()
+        if world > 1:
+            sharding.allreduce_sum_(dV)
 
-    t_step = timed_steps(step, args.steps, args.warmup, stream, flush)
+    if dist_ is not None:
+        dist_.barrier()
+    with ClockSampler(torch.cuda.current_device()) as clocks:
+        t_step = timed_steps(step, args.steps, args.warmup, stream, flush)
     t_fwd = timed_steps(fwd, 3, 1, stream, flush)
     t_bwd = timed_steps(bwd, 3, 1, stream, flush)
     assert api.sync_bvh_status(bvh).is_ok()
+    total_ms, fwd_ms, bwd_ms = sharding.max_over_ranks([sum(t_step), float(np.mean(t_fwd)), float(np.mean(t_bwd))])
+    if world > 1:
+        # the all-reduced dL/dV against one GPU's backward over the whole batch (untimed, rank 0)
+        step()
+        torch.cuda.synchronize()
+        reduced = torch.stack(dV, -1).cpu().numpy()
+        dist_.barrier()
+        if rank == 0:
+            full_q = [torch.from_numpy(v).cuda() for v in q_all]
+            full_out = torch.empty(n_total, device="cuda")
+            st, saved = g.gwn_winding_taylor_forward(order, bvh, mom, *full_q, full_out, accuracy_scale=beta,
+                                                     stream=stream)
+            assert st.is_ok(), st.message
+            fdV = [torch.empty(nv, device="cuda") for _ in range(3)]
+            fdQ = [torch.empty(n_total, device="cuda") for _ in range(3)]
+            st = g.gwn_winding_taylor_backward(saved, geo, bvh, mom, torch.from_numpy(w_all).cuda(), *fdV, *fdQ,
+                                               stream=stream)
+            assert st.is_ok(), st.message
+            one = torch.stack(fdV, -1).cpu().numpy()
+            shard_check = {"dV_max_abs_diff_vs_one_gpu": float(np.max(np.abs(reduced - one))),
+                           "dV_max_abs": float(np.max(np.abs(one)))}
+        dist_.barrier()
+        if rank == 0:
+            line = {
+                "metric": "Adjoint (forward + backward) queries/s, order 1, 159k-triangle open soup",
+                "value": n_total * args.steps / (total_ms / 1e3), "unit": "queries/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
+                "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic",
+                "config": {"workload": "UV 316x316 displaced sphere, 20% of triangles deleted, 5% flipped (seed 3), "
+                                       f"{n_total} mixed queries, g ~ N(0,1)", "triangles": int(mesh["i0"].size),
+                           "vertices": int(nv), "taylor_order": order, "accuracy_scale": beta,
+                           "parallelism": f"queries split over {world} ranks, dL/dV all-reduced",
+                           "forward_ms": fwd_ms, "backward_ms": bwd_ms,
+                           "l2": "flushed (256 MiB write) between timed steps", **shard_check},
+                "gpu_launches": None, "clocks": clocks.summary(),
+            }
+            print(json.dumps(line), flush=True)
+        return
 
     # ---- FD checks on losses restricted to 4096 queries away from the surface (untimed) ----
     dist = oracle.mesh_distance(mesh, *[x[:8000] for x in q])
@@ -475,19 +527,20 @@ def run_adjoint_workload(args) -> None:
                 "dV": errs(adj_v[verts], fd_v), "dq": errs(adj_q[far][sel], fd_q)}
 
     checks = [fd_check(h, 30.0), fd_check(1e-6, 100.0)]
-    ms = float(np.mean(t_step))
+    ms = total_ms / args.steps
     line = {
         "metric": "Adjoint (forward + backward) queries/s, order 1, 159k-triangle open soup",
         "value": n / (ms / 1e3), "unit": "queries/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "ms_per_step": ms, "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic",
         "config": {"workload": "UV 316x316 displaced sphere, 20% of triangles deleted, 5% flipped (seed 3), "
                                f"{n} mixed queries, g ~ N(0,1)", "triangles": int(mesh["i0"].size),
                    "vertices": int(nv), "taylor_order": order, "accuracy_scale": beta,
-                   "forward_ms": float(np.mean(t_fwd)), "backward_ms": float(np.mean(t_bwd)),
+                   "forward_ms": fwd_ms, "backward_ms": bwd_ms,
                    "l2": "flushed (256 MiB write) between timed steps"},
         "fd_checks": checks,
         "gpu_launches": None,
+        "clocks": clocks.summary(),
     }
     print(json.dumps(line), flush=True)
 
@@ -624,15 +677,19 @@ def run_batched_workload(args) -> None:
     import torch
 
     import smallgwn_b200 as g
-    from smallgwn_b200 import api, meshes
+    from smallgwn_b200 import api, meshes, sharding
 
+    rank, world, dist_ = dist_setup(args.gpus)
     order, beta, n_mesh, frames = 1, 2.0, 256, 100
     rng = np.random.default_rng(4)
     tris = np.exp(rng.uniform(np.log(1e3), np.log(2e5), n_mesh))
-    nqs = np.exp(rng.uniform(np.log(1e4), np.log(1e6), n_mesh)).astype(np.int64)
+    nqs_all = np.exp(rng.uniform(np.log(1e4), np.log(1e6), n_mesh)).astype(np.int64)
     W = rng.normal(size=(n_mesh, 3))
+    # several GPUs: whole meshes per rank, longest-processing-time-first on the per-frame cost model
+    mine = sharding.lpt_partition([sharding.mesh_cost(int(t), int(q)) for t, q in zip(tris, nqs_all)], world)[rank]
+    nqs = nqs_all[mine]
     parts = []
-    for i in range(n_mesh):
+    for i in mine:
         k = max(int(round(np.sqrt(tris[i] / 4.0))), 4)
         V, F = meshes.uv_sphere(2 * k, k + 1, seed=4000 + i)
         mesh = meshes.to_soa(V, F)
@@ -652,16 +709,16 @@ def run_batched_workload(args) -> None:
         n = V.shape[0]
         X[:, off:off + n] = torch.from_numpy(V.T.copy()).cuda()
         Nv[:, off:off + n] = torch.from_numpy(vn.T.copy()).cuda()
-        Wv[:, off:off + n] = torch.from_numpy(W[i].astype(np.float32)).cuda()[:, None]
+        Wv[:, off:off + n] = torch.from_numpy(W[mine[i]].astype(np.float32)).cuda()[:, None]
         idx = [torch.from_numpy(np.ascontiguousarray(F[:, j])).cuda() for j in range(3)]
         geo = api.gwn_geometry_view(X[0, off:off + n], X[1, off:off + n], X[2, off:off + n], *idx)
         bvh = g.gwn_bvh4_object()
         assert g.gwn_build_bvh(geo, bvh, g.gwn_bvh_build_options(method=0, hploc_search_radius=8)).is_ok()
         mom = g.gwn_bvh4_moment_object(order)
         assert g.gwn_refit_bvh_moment(order, bvh, mom).is_ok()
-        q = meshes.mixed_queries(mesh, int(nqs[i]), seed=40_000 + i)
+        q = meshes.mixed_queries(mesh, int(nqs_all[mine[i]]), seed=40_000 + mine[i])
         dq = [torch.from_numpy(v).cuda() for v in q]
-        objs.append((geo, bvh, mom, *dq, torch.empty(int(nqs[i]), device="cuda")))
+        objs.append((geo, bvh, mom, *dq, torch.empty(int(nqs_all[mine[i]]), device="cuda")))
         off += n
     X0 = X.clone()
     fidx = torch.zeros(1, device="cuda")
@@ -698,7 +755,7 @@ def run_batched_workload(args) -> None:
             graph.replay()
             e1.record(cur)
         torch.cuda.synchronize()
-    lat = np.array([a.elapsed_time(b) for a, b in ev])
+    lat = np.array(sharding.max_over_ranks([a.elapsed_time(b) for a, b in ev]))
     assert batch.sync().is_ok()
     got = [o[-1].cpu().numpy() for o in objs]
 
@@ -743,18 +800,24 @@ def run_batched_workload(args) -> None:
         per_mesh_frame()
     torch.cuda.synchronize()
     loop_ms = (time.perf_counter() - t0) * 1e3 / loop_frames
+    loop_ms, max_diff = sharding.max_over_ranks([loop_ms, max_diff])
     del graph
     batch.release()
     total_ms = float(lat.sum())
+    if rank != 0:
+        return
     line = {
         "metric": "Batched dynamic refit + Taylor query frames/s (256 meshes, CUDA graph)",
-        "value": frames / (total_ms / 1e3), "unit": "frames/s", "n_gpus": 1, "steps": frames, "warmup": 1,
-        "ms_per_step": total_ms / frames, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "value": frames / (total_ms / 1e3), "unit": "frames/s", "n_gpus": world, "steps": frames, "warmup": 1,
+        "ms_per_step": total_ms / frames, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic",
         "config": {"workload": "256 displaced spheres, tris log-U[1k,200k], queries log-U[10k,1M] (seed 4), "
                                "100 deformed frames", "meshes": n_mesh,
-                   "triangles": int(sum(p[1].shape[0] for p in parts)), "vertices": int(nv),
-                   "queries_per_frame": int(nqs.sum()), "taylor_order": order, "accuracy_scale": beta,
+                   ("triangles" if world == 1 else "triangles_rank0"): int(sum(p[1].shape[0] for p in parts)),
+                   ("vertices" if world == 1 else "vertices_rank0"): int(nv), "meshes_rank0": len(mine),
+                   "queries_per_frame": int(nqs_all.sum()), "taylor_order": order, "accuracy_scale": beta,
+                   "parallelism": (f"whole meshes over {world} ranks (LPT on T log T + Q depth), frame time = max "
+                                   "over ranks" if world > 1 else "one GPU"),
                    "frame_ms_p50": float(np.percentile(lat, 50)), "frame_ms_p99": float(np.percentile(lat, 99)),
                    "per_mesh_loop_ms_per_frame": loop_ms, "speedup_vs_per_mesh_loop": loop_ms / (total_ms / frames),
                    "max_abs_diff_vs_per_mesh_loop": max_diff, "tuning": tuning,
