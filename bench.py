@@ -48,12 +48,14 @@ def parse() -> argparse.Namespace:
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="taylor",
-                    choices=["taylor", "adjoint", "precision", "exact", "batched", "distance", "ray", "antipodal"],
+                    choices=["taylor", "adjoint", "precision", "exact", "batched", "distance", "ray", "antipodal",
+                             "build"],
                     help="taylor: the headline (1M-triangle sphere, 10M queries); adjoint: forward + backward "
                          "on the 159k-triangle soup; precision: 8.4M-triangle sphere, 100M near-surface queries "
                          "in 16M chunks; exact: brute-force exact batch on the small icosphere; distance / ray: "
                          "unsigned distance / ray first hit on the 1M-triangle sphere, 10M queries / rays; "
-                         "antipodal: antipodal winding numbers on the 159k-triangle open soup, 200k queries")
+                         "antipodal: antipodal winding numbers on the 159k-triangle open soup, 200k queries; "
+                         "build: H-PLOC / LBVH builds, refit and moment refits of the 1M-triangle sphere")
     ap.add_argument("--queries", type=int, default=N_QUERIES)
     ap.add_argument("--order", type=int, default=ORDER)
     ap.add_argument("--beta", type=float, default=BETA)
@@ -151,8 +153,12 @@ def run_profile(args) -> None:
     method = 1 if args.profile == "exact" else 0
     assert g.gwn_build_bvh(geo, bvh, g.gwn_bvh_build_options(method=method, hploc_search_radius=8)).is_ok()
     if args.profile == "build":
+        # two H-PLOC builds, one refit, one moment refit of each order
         for _ in range(2):
             assert g.gwn_build_bvh(geo, bvh, g.gwn_bvh_build_options(method=0, hploc_search_radius=8)).is_ok()
+        assert g.gwn_refit_bvh(geo, bvh).is_ok()
+        for o in range(3):
+            assert g.gwn_refit_bvh_moment(o, bvh, g.gwn_bvh4_moment_object(o)).is_ok()
         torch.cuda.synchronize()
         print("profile build ok")
         return
@@ -828,6 +834,118 @@ def run_batched_workload(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+def run_build_workload(args) -> None:
+    """Builds/s, refits/s and moment refits/s on the 1M-triangle sphere (1024 x 512, seed 2).
+
+    A step is one gwn_build_bvh (H-PLOC radius 8, 64-bit Morton codes; the LBVH builder is timed
+    beside it), host-synchronous like smallgwn's, timed with CUDA events around the call; refit
+    and moment refits (orders 0-2) likewise. Each stage's roofline uses its compulsory HBM bytes:
+    build and refit 12 V + 12 T + 4 T + 36 T + 128 N, moment refit 36 T + 128 N + M_o N
+    (M_o = 112 / 208 / 368 B per node). smallgwn's own implementation runs on the same mesh beside
+    it; the CPU baseline is the oracle's restatement of the H-PLOC pipeline on one host thread."""
+    import torch
+
+    import oracle
+    import smallgwn_b200 as g
+    from smallgwn_b200 import api, meshes
+
+    stream = torch.cuda.current_stream()
+    mesh = meshes.sphere_mesh()
+    V, T = int(mesh["x"].size), int(mesh["i0"].size)
+    geo = g.gwn_geometry_object()
+    assert g.gwn_upload_geometry(geo, mesh["x"], mesh["y"], mesh["z"], mesh["i0"], mesh["i1"], mesh["i2"]).is_ok()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    bvh = g.gwn_bvh4_object()
+
+    def build(method):
+        st = g.gwn_build_bvh(geo, bvh, g.gwn_bvh_build_options(method=method, hploc_search_radius=8), stream)
+        assert st.is_ok(), st.message
+
+    with ClockSampler(torch.cuda.current_device()) as clocks:
+        t_lbvh = timed_steps(lambda: build(g.gwn_bvh_build_method.k_lbvh), args.steps, args.warmup, stream, flush)
+        t_hploc = timed_steps(lambda: build(g.gwn_bvh_build_method.k_hploc), args.steps, args.warmup, stream, flush)
+        N = int(bvh.accessor().node_count)
+        t_refit = timed_steps(lambda: g.gwn_refit_bvh(geo, bvh, stream), args.steps, args.warmup, stream, flush)
+        moms = {o: g.gwn_bvh4_moment_object(o) for o in range(3)}
+        t_mom = {o: timed_steps(lambda o=o: g.gwn_refit_bvh_moment(o, bvh, moms[o], stream), args.steps, args.warmup,
+                                stream, flush) for o in range(3)}
+        t_refit_async = timed_steps(lambda: api.refit_bvh_async(geo, bvh, stream), args.steps, args.warmup, stream,
+                                    flush)
+    assert api.sync_bvh_status(bvh).is_ok()
+    # e2e: pinned host arrays -> upload -> build, through the public API
+    geo2 = g.gwn_geometry_object()
+    bvh2 = g.gwn_bvh4_object()
+    pinned = {k: torch.from_numpy(np.ascontiguousarray(mesh[k]).view(np.int32)).pin_memory().numpy().view(mesh[k].dtype)
+              for k in ("x", "y", "z", "i0", "i1", "i2")}
+
+    def e2e():
+        assert g.gwn_upload_geometry(geo2, pinned["x"], pinned["y"], pinned["z"], pinned["i0"], pinned["i1"],
+                                     pinned["i2"], stream).is_ok()
+        assert g.gwn_build_bvh(geo2, bvh2, g.gwn_bvh_build_options(method=0, hploc_search_radius=8), stream).is_ok()
+
+    t_e2e = timed_steps(e2e, max(3, min(args.steps, 10)), 1, stream, flush)
+
+    pk = peaks()
+    b_build = 12 * V + 12 * T + 4 * T + 36 * T + 128 * N
+    b_mom = {o: 36 * T + 128 * N + MOMENT_BYTES[o] * N for o in range(3)}
+
+    def stage(ms_list, nbytes):
+        ms = float(np.mean(ms_list))
+        gbs = nbytes / (ms / 1e3) / 1e9
+        return {"ms": ms, "per_s": 1e3 / ms, "bytes": int(nbytes), "achieved_gbs": gbs, "frac": gbs / pk["hbm_gbs"]}
+
+    stages = {"build_hploc": stage(t_hploc, b_build), "build_lbvh": stage(t_lbvh, b_build),
+              "refit": stage(t_refit, b_build), "refit_async": stage(t_refit_async, b_build)}
+    stages.update({f"moment_refit_o{o}": stage(t_mom[o], b_mom[o]) for o in range(3)})
+
+    ref = None
+    if oracle.ref_lib() is not None:
+        r = oracle.Reference(mesh)
+        try:
+            r.build(method=0, radius=8, bits=64)
+            ref = {"build_hploc_ms": r.time_build(0, 8, 64, 5), "build_lbvh_ms": r.time_build(1, 8, 64, 5)}
+            r.build(method=0, radius=8, bits=64)
+            ref["refit_ms"] = r.time_refit(-1, 5)
+            ref.update({f"moment_refit_o{o}_ms": r.time_refit(o, 5) for o in range(3)})
+        finally:
+            r.close()
+        ref["impl"] = "smallgwn's own kernels (oracle/_ref), same mesh, CUDA events"
+
+    cpu = None
+    if not args.no_cpu_baseline:
+        t0 = time.perf_counter()
+        oracle.build_bvh(mesh, "hploc", radius=8)
+        cpu_s = time.perf_counter() - t0
+        cpu = {"value": 1.0 / cpu_s, "unit": "builds/s", "cores": 1, "kind": "port",
+               "sample": f"one H-PLOC build of the {T}-triangle mesh by the oracle's C restatement in {cpu_s:.2f} s"}
+
+    ms = float(np.mean(t_hploc))
+    line = {
+        "metric": "BVH4 builds/s (H-PLOC r=8, 64-bit Morton, 1M-triangle sphere)",
+        "value": 1e3 / ms, "unit": "builds/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": "displaced UV sphere 1024x512 (1,046,528 tris, seed 2)", "vertices": V, "triangles": T,
+                   "bvh_nodes": N, "l2": "flushed (256 MiB write) between timed steps", "stages": stages,
+                   "reference": ref,
+                   "speedup_vs_reference": ({k: ref[f"{k}_ms"] / stages[k]["ms"] for k in
+                                             ("build_hploc", "build_lbvh", "refit")} | {
+                                                f"moment_refit_o{o}": ref[f"moment_refit_o{o}_ms"] /
+                                                stages[f"moment_refit_o{o}"]["ms"] for o in range(3)})
+                   if ref else None},
+        "roofline": {"bound": "hbm", "achieved": stages["build_hploc"]["achieved_gbs"], "peak": pk["hbm_gbs"],
+                     "unit": "GB/s", "frac": stages["build_hploc"]["frac"], "peak_source": pk["source"],
+                     "traffic": None, "kernel": "whole H-PLOC build (all launches of one gwn_build_bvh)",
+                     "bytes_model": "12 V + 12 T + 4 T + 36 T + 128 N compulsory bytes"},
+        "cpu_baseline": cpu,
+        "e2e": {"value": 1e3 / float(np.mean(t_e2e)), "unit": "builds/s", "h2d_bytes_per_step": 12 * V + 12 * T,
+                "d2h_bytes_per_step": 0},
+        "gpu_launches": None,
+        "clocks": clocks.summary(),
+    }
+    print(json.dumps(line), flush=True)
+
+
 def run_exact_workload(args) -> None:
     """Plain exact winding number, small: icosphere level 4 (5,120 triangles, radial noise seed 0),
     100k queries uniform in [-1.5, 1.5]^3 (seed 1), LBVH, exact batch; the oracle's FP32 brute force
@@ -1191,7 +1309,8 @@ def main() -> None:
     if args.workload != "taylor":
         {"adjoint": run_adjoint_workload, "precision": run_precision_workload, "exact": run_exact_workload,
          "batched": run_batched_workload, "distance": run_spatial_workload,
-         "ray": run_spatial_workload, "antipodal": run_antipodal_workload}[args.workload](args)
+         "ray": run_spatial_workload, "antipodal": run_antipodal_workload,
+         "build": run_build_workload}[args.workload](args)
         return
     import torch
 

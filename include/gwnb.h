@@ -133,6 +133,20 @@ GWNB_API int gwnb_last_cuda_error(void);
 /* Library version string. */
 GWNB_API const char *gwnb_version(void);
 
+/* ---- device memory ------------------------------------------------------------------------- */
+/* Every device allocation of the library comes from one memory pool per device that keeps freed
+ * memory mapped between host synchronizations (no smallgwn counterpart: smallgwn allocates with
+ * the CUDA defaults, which return freed memory to the driver at each synchronization). These two
+ * calls act on the current device's pool. */
+
+/* Bytes the pool holds from the driver (*reserved) and bytes in live allocations (*used); either
+ * pointer may be NULL. */
+GWNB_API int gwnb_memory_stats(uint64_t *reserved, uint64_t *used);
+
+/* Returns cached memory to the driver until the pool holds at most max(keep_bytes, bytes in use).
+ * Call it after the stream work that freed the memory has completed. */
+GWNB_API int gwnb_memory_trim(uint64_t keep_bytes);
+
 /* ---- geometry (include/gwn/gwn_geometry.cuh:66-90) ---------------------------------------- */
 
 /* Replaces gwn::gwn_upload_geometry (include/gwn/gwn_geometry.cuh:66-72,

@@ -548,6 +548,12 @@ class Reference:
                                             C.c_int(iters), C.byref(ms)))
         return float(ms.value)
 
+    def time_refit(self, order: int = -1, iters: int = 5) -> float:
+        """Device ms of gwn_refit_bvh (order -1) or gwn_refit_bvh_moment<order> on the built BVH."""
+        ms = C.c_float()
+        self._check(self.lib.ref_time_refit(self.h, C.c_int(order), C.c_int(iters), C.byref(ms)))
+        return float(ms.value)
+
     def update_refit(self, x, y, z) -> None:
         xs, ys, zs = (_f32(v) for v in (x, y, z))
         self._check(self.lib.ref_update_refit(self.h, _p(xs), _p(ys), _p(zs), C.c_uint64(xs.size)))

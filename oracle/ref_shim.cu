@@ -340,6 +340,37 @@ int ref_time_build(void *p, int method, uint32_t radius, int morton_bits, int it
     return 0;
 }
 
+// Device time of one gwn_refit_bvh (order < 0) or gwn_refit_bvh_moment<order> on the built BVH,
+// average over iters after one untimed call.
+int ref_time_refit(void *p, int order, int iters, float *ms) {
+    auto &c = *static_cast<ctx *>(p);
+    auto run = [&]() -> int {
+        if (order < 0) {
+            auto s = gwn::gwn_refit_bvh(c.geometry, c.bvh);
+            return s.is_ok() ? 0 : fail(s);
+        }
+        return ref_moment(p, order);
+    };
+    int rc = run();
+    if (rc != 0)
+        return rc;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaDeviceSynchronize();
+    cudaEventRecord(e0, cudaStreamLegacy);
+    for (int i = 0; i < iters && rc == 0; ++i)
+        rc = run();
+    cudaEventRecord(e1, cudaStreamLegacy);
+    cudaEventSynchronize(e1);
+    float t = 0;
+    cudaEventElapsedTime(&t, e0, e1);
+    *ms = t / static_cast<float>(iters > 0 ? iters : 1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return rc;
+}
+
 int ref_update_refit(void *p, const float *x, const float *y, const float *z, uint64_t nv) {
     auto &c = *static_cast<ctx *>(p);
     auto s = gwn::gwn_update_geometry(c.geometry, gwn::gwn_host_span<float const>(x, nv),

@@ -704,6 +704,20 @@ def refit_bvh_moment_async(bvh: gwn_bvh4_object, moment: gwn_bvh4_moment_object,
                                                            _stream(stream)))
 
 
+def memory_stats() -> tuple[int, int]:
+    """(bytes the library's device memory pool holds, bytes in live allocations), current device."""
+    r, u = C.c_uint64(), C.c_uint64()
+    rc = _lib.load().gwnb_memory_stats(C.byref(r), C.byref(u))
+    if rc != _lib.GWNB_OK:
+        raise RuntimeError(_lib.last_error())
+    return int(r.value), int(u.value)
+
+
+def memory_trim(keep_bytes: int = 0) -> gwn_status:
+    """Return the pool's cached device memory to the driver down to keep_bytes (or what is in use)."""
+    return _status(_lib.load().gwnb_memory_trim(int(keep_bytes)))
+
+
 def sync_bvh_status(bvh: gwn_bvh4_object, stream=None) -> gwn_status:
     """Synchronize, publish device-side root bounds and turn device error bits into a status."""
     return _status(_lib.load().gwnb_bvh4_sync_status_f32(C.byref(bvh._view), _stream(stream)))

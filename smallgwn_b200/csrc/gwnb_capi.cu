@@ -10,6 +10,7 @@
 #include <cmath>
 #include <cstring>
 #include <limits>
+#include <mutex>
 #include <new>
 #include <string>
 
@@ -43,6 +44,35 @@ std::uint64_t reserve_revision() {
         if (next.compare_exchange_weak(r, r + 1, std::memory_order_relaxed))
             return r;
     }
+}
+
+int library_pool(cudaMemPool_t *pool) {
+    constexpr int k_max_devices = 64;
+    static std::mutex mutex;
+    static cudaMemPool_t pools[k_max_devices] = {};
+    int dev = 0;
+    GWNB_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= k_max_devices)
+        return set_error(GWNB_INTERNAL_ERROR, "library memory pool: device ordinal out of range.");
+    std::lock_guard<std::mutex> lock(mutex);
+    if (pools[dev] == nullptr) {
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.handleTypes = cudaMemHandleTypeNone;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        cudaMemPool_t created = nullptr;
+        GWNB_CUDA_TRY(cudaMemPoolCreate(&created, &props));
+        std::uint64_t keep = std::numeric_limits<std::uint64_t>::max();
+        cudaError_t const e = cudaMemPoolSetAttribute(created, cudaMemPoolAttrReleaseThreshold, &keep);
+        if (e != cudaSuccess) {
+            (void)cudaMemPoolDestroy(created);
+            return set_cuda_error(e, "cudaMemPoolSetAttribute(release threshold)");
+        }
+        pools[dev] = created;
+    }
+    *pool = pools[dev];
+    return GWNB_OK;
 }
 
 int device_sm_count() {
@@ -255,6 +285,26 @@ using namespace gwnb;
 extern "C" {
 
 const char *gwnb_last_error_message(void) { return g_message.c_str(); }
+
+int gwnb_memory_stats(uint64_t *reserved, uint64_t *used) {
+    cudaMemPool_t pool = nullptr;
+    GWNB_TRY(library_pool(&pool));
+    std::uint64_t r = 0, u = 0;
+    GWNB_CUDA_TRY(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &r));
+    GWNB_CUDA_TRY(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &u));
+    if (reserved != nullptr)
+        *reserved = r;
+    if (used != nullptr)
+        *used = u;
+    return GWNB_OK;
+}
+
+int gwnb_memory_trim(uint64_t keep_bytes) {
+    cudaMemPool_t pool = nullptr;
+    GWNB_TRY(library_pool(&pool));
+    GWNB_CUDA_TRY(cudaMemPoolTrimTo(pool, static_cast<std::size_t>(keep_bytes)));
+    return GWNB_OK;
+}
 int gwnb_last_cuda_error(void) { return g_cuda_error; }
 const char *gwnb_version(void) { return "gwnb 0.1 (sm_100a)"; }
 

@@ -1,0 +1,44 @@
+"""The library's device memory pool: freed scratch stays mapped across host synchronizations (so
+repeated builds do not map memory again), gwnb_memory_trim hands it back, and work after a trim is
+unaffected."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import smallgwn_b200 as g
+from smallgwn_b200 import api, meshes
+from test_gpu_build import upload
+
+pytestmark = pytest.mark.gpu
+
+
+def test_pool_retains_and_trims(cuda):
+    mesh = meshes.sphere_mesh()  # 1M triangles: the build's scratch spans several pool chunks
+    geo = upload(mesh)
+    bvh = g.gwn_bvh4_object()
+    assert g.gwn_build_bvh(geo, bvh, g.gwn_bvh_build_options(method=0, hploc_search_radius=8)).is_ok()
+    cuda.cuda.synchronize()
+    reserved, used = api.memory_stats()
+    # the build's scratch (codes, sorted boxes, binary nodes, collapse lists) was freed but is kept
+    assert reserved - used > (64 << 20) and used > 0
+    first = api.bvh_host_arrays(bvh)
+    # building again reuses the retained memory and gives the same tree
+    bvh2 = g.gwn_bvh4_object()
+    assert g.gwn_build_bvh(geo, bvh2, g.gwn_bvh_build_options(method=0, hploc_search_radius=8)).is_ok()
+    again = api.bvh_host_arrays(bvh2)
+    np.testing.assert_array_equal(first["nodes"], again["nodes"])
+    np.testing.assert_array_equal(first["primitive_indices"], again["primitive_indices"])
+    # freed objects leave whole pool chunks unused; a trim hands them back to the driver
+    bvh2.clear()
+    bvh.clear()
+    geo.clear()
+    cuda.cuda.synchronize()
+    reserved3, used3 = api.memory_stats()
+    assert used3 < used and reserved3 >= reserved
+    assert api.memory_trim(0).is_ok()
+    reserved4, used4 = api.memory_stats()
+    assert used4 == used3 and reserved4 < reserved3
+    # and work after a trim is unaffected
+    geo = upload(meshes.soup_mesh(30, seed=2))
+    assert g.gwn_build_bvh(geo, bvh).is_ok()
