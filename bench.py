@@ -352,21 +352,27 @@ def config_dict(args, mesh) -> dict:
             "l2": "flushed (256 MiB write) between timed steps", "parallelism": f"replicas x{args.gpus}"}
 
 
-def timed_steps(fn, steps: int, warmup: int, stream, flush) -> list[float]:
+def timed_steps(fn, steps: int, warmup: int, stream, flush, launches: list | None = None) -> list[float]:
     """Per-step device times (ms) of fn() on `stream` after `warmup` untimed calls; L2 flushed
-    before every timed step."""
+    before every timed step. `launches`, if given, receives the number of the library's kernel
+    launches inside the timed steps."""
     import torch
+
+    from smallgwn_b200 import api
 
     for _ in range(warmup):
         fn()
     torch.cuda.synchronize()
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    before = api.launch_count()
     for e0, e1 in ev:
         flush.fill_(1)
         e0.record(stream)
         fn()
         e1.record(stream)
     torch.cuda.synchronize()
+    if launches is not None:
+        launches.append(api.launch_count() - before)
     return [a.elapsed_time(b) for a, b in ev]
 
 
@@ -430,7 +436,8 @@ def run_adjoint_workload(args) -> None:
     if dist_ is not None:
         dist_.barrier()
     with ClockSampler(torch.cuda.current_device()) as clocks:
-        t_step = timed_steps(step, args.steps, args.warmup, stream, flush)
+        adj_launches = []
+        t_step = timed_steps(step, args.steps, args.warmup, stream, flush, adj_launches)
     t_fwd = timed_steps(fwd, 3, 1, stream, flush)
     t_bwd = timed_steps(bwd, 3, 1, stream, flush)
     assert api.sync_bvh_status(bvh).is_ok()
@@ -469,7 +476,7 @@ def run_adjoint_workload(args) -> None:
                            "parallelism": f"queries split over {world} ranks, dL/dV all-reduced",
                            "forward_ms": fwd_ms, "backward_ms": bwd_ms,
                            "l2": "flushed (256 MiB write) between timed steps", **shard_check},
-                "gpu_launches": None, "clocks": clocks.summary(),
+                "gpu_launches": adj_launches[0], "clocks": clocks.summary(),
             }
             print(json.dumps(line), flush=True)
         return
@@ -545,7 +552,7 @@ def run_adjoint_workload(args) -> None:
                    "forward_ms": fwd_ms, "backward_ms": bwd_ms,
                    "l2": "flushed (256 MiB write) between timed steps"},
         "fd_checks": checks,
-        "gpu_launches": None,
+        "gpu_launches": adj_launches[0],
         "clocks": clocks.summary(),
     }
     print(json.dumps(line), flush=True)
@@ -605,6 +612,7 @@ def run_precision_workload(args) -> None:
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     comp = g.near_precision.compensated
     times, fp64_pairs, done = [], 0, 0
+    chunk_launches: list[int] = []
     first = None
     k = 0
     while done < total:
@@ -619,7 +627,7 @@ def run_precision_workload(args) -> None:
                                                            stream=stream, precision=comp)
             assert st.is_ok(), st.message
 
-        times += timed_steps(run, 1, 1 if k == 0 else 0, stream, flush)
+        times += timed_steps(run, 1, 1 if k == 0 else 0, stream, flush, chunk_launches)
         fp64_pairs += api.fp64_fallback_count(bvh, stream)
         done += m
         k += 1
@@ -668,6 +676,7 @@ def run_precision_workload(args) -> None:
         "fp64_pairs": {"all_chunks": int(fp64_pairs), "subset": int(sub_fp64),
                        "subset_near_field_pairs": near_pairs,
                        "subset_fraction": sub_fp64 / max(near_pairs, 1.0)},
+        "gpu_launches": int(sum(chunk_launches)),
     }
     print(json.dumps(line), flush=True)
 
@@ -747,9 +756,11 @@ def run_batched_workload(args) -> None:
     with torch.cuda.stream(side):
         assert batch.frame(side.cuda_stream).is_ok()
         side.synchronize()
+        before = api.launch_count()
         with torch.cuda.graph(graph, stream=side):
             deform()
             assert batch.frame(side.cuda_stream).is_ok()
+        frame_launches = api.launch_count() - before
     torch.cuda.synchronize()
     X.copy_(X0)
     fidx.zero_()
@@ -828,7 +839,7 @@ def run_batched_workload(args) -> None:
                    "per_mesh_loop_ms_per_frame": loop_ms, "speedup_vs_per_mesh_loop": loop_ms / (total_ms / frames),
                    "max_abs_diff_vs_per_mesh_loop": max_diff, "tuning": tuning,
                    "stage_ms_frame_100": stages_end, "stage_ms_frame_50": stages_mid},
-        "gpu_launches": None,
+        "gpu_launches": frame_launches * frames,  # the library kernels recorded in one frame's graph
         "clocks": clocks.summary(),
     }
     print(json.dumps(line), flush=True)
@@ -863,7 +874,9 @@ def run_build_workload(args) -> None:
 
     with ClockSampler(torch.cuda.current_device()) as clocks:
         t_lbvh = timed_steps(lambda: build(g.gwn_bvh_build_method.k_lbvh), args.steps, args.warmup, stream, flush)
-        t_hploc = timed_steps(lambda: build(g.gwn_bvh_build_method.k_hploc), args.steps, args.warmup, stream, flush)
+        build_launches = []
+        t_hploc = timed_steps(lambda: build(g.gwn_bvh_build_method.k_hploc), args.steps, args.warmup, stream, flush,
+                              build_launches)
         N = int(bvh.accessor().node_count)
         t_refit = timed_steps(lambda: g.gwn_refit_bvh(geo, bvh, stream), args.steps, args.warmup, stream, flush)
         moms = {o: g.gwn_bvh4_moment_object(o) for o in range(3)}
@@ -940,7 +953,7 @@ def run_build_workload(args) -> None:
         "cpu_baseline": cpu,
         "e2e": {"value": 1e3 / float(np.mean(t_e2e)), "unit": "builds/s", "h2d_bytes_per_step": 12 * V + 12 * T,
                 "d2h_bytes_per_step": 0},
-        "gpu_launches": None,
+        "gpu_launches": build_launches[0],
         "clocks": clocks.summary(),
     }
     print(json.dumps(line), flush=True)
@@ -970,7 +983,8 @@ def run_exact_workload(args) -> None:
     def run():
         assert g.gwn_compute_winding_number_exact_batch(bvh, *dq, out, stream).is_ok()
 
-    t = timed_steps(run, args.steps, args.warmup, stream, flush)
+    exact_launches: list[int] = []
+    t = timed_steps(run, args.steps, args.warmup, stream, flush, exact_launches)
     ms = float(np.mean(t))
     nq, nt = dq[0].numel(), int(mesh["i0"].size)
     ref = oracle.exact_winding(mesh, *q)
@@ -989,6 +1003,7 @@ def run_exact_workload(args) -> None:
                    "max_abs_diff_vs_oracle_fp32": err},
         "cpu_baseline": {"value": m * nt / cpu_s, "unit": "evaluations/s", "cores": threads, "kind": "port",
                          "sample": f"{m} of the queries against all triangles"},
+        "gpu_launches": exact_launches[0],
     }
     print(json.dumps(line), flush=True)
 
@@ -1063,6 +1078,7 @@ def run_spatial_workload(args) -> None:
     if dist is not None:
         dist.barrier()
     torch.cuda.synchronize()
+    launches0 = api.launch_count()
     with ClockSampler(dev) as clocks:
         for e0, e1 in events:
             flush.fill_(1)
@@ -1070,6 +1086,7 @@ def run_spatial_workload(args) -> None:
             call(din, out)
             e1.record(stream)
         torch.cuda.synchronize()
+    timed_launches = api.launch_count() - launches0
     total_ms = sum(a.elapsed_time(b) for a, b in events)
     t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
     if dist is not None:
@@ -1187,7 +1204,7 @@ def run_spatial_workload(args) -> None:
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": unit, "h2d_bytes_per_step": 4 * len(inp) * n,
                     "d2h_bytes_per_step": out_bytes * n},
-            "gpu_launches": 7 * args.steps,  # codes, histogram, 4 digit passes, traversal
+            "gpu_launches": timed_launches,  # per step: codes, histogram, 4 digit passes, traversal
             "clocks": clocks.summary(),
         }
         print(json.dumps(line), flush=True)
@@ -1230,8 +1247,9 @@ def run_antipodal_workload(args) -> None:
         assert g.gwn_compute_winding_number_antipodal_batch(geo, bvh, ch, *xs, o, stream=stream,
                                                             sort_queries=True).is_ok()
 
+    ap_launches = []
     with ClockSampler(torch.cuda.current_device()) as clocks:
-        t = timed_steps(lambda: call(dq, out), args.steps, args.warmup, stream, flush)
+        t = timed_steps(lambda: call(dq, out), args.steps, args.warmup, stream, flush, ap_launches)
     ms = float(np.mean(t))
     hq = [torch.from_numpy(v).pin_memory() for v in q]
     hout = torch.empty(n).pin_memory()
@@ -1292,7 +1310,7 @@ def run_antipodal_workload(args) -> None:
         "cpu_baseline": cpu,
         "e2e": {"value": n / (float(np.mean(e2e)) / 1e3), "unit": "queries/s", "h2d_bytes_per_step": 12 * n,
                 "d2h_bytes_per_step": 4 * n},
-        "gpu_launches": 8 * args.steps,  # edge records, codes, histogram, 4 digit passes, antipodal
+        "gpu_launches": ap_launches[0],  # per step: edge records, codes, histogram, 4 digit passes, antipodal
         "clocks": clocks.summary(),
     }
     print(json.dumps(line), flush=True)
@@ -1359,6 +1377,7 @@ def main() -> None:
     if dist is not None:
         dist.barrier()
     torch.cuda.synchronize()
+    launches0 = api.launch_count()
     with ClockSampler(dev) as clocks:
         for e0, e1 in events:
             flush.fill_(1)
@@ -1366,6 +1385,7 @@ def main() -> None:
             batch(dq, out)
             e1.record(stream)
         torch.cuda.synchronize()
+    timed_launches = api.launch_count() - launches0
     if dist is not None:
         dist.barrier()
     torch.cuda.synchronize()
@@ -1465,7 +1485,6 @@ def main() -> None:
                     "chosen_over_plain": (value / world) / (n / (plain_ms / 1e3)),
                     "build_ms_hploc": build_ms, "bvh_nodes": int(bvh.accessor().node_count),
                     "fp64_fallbacks_per_batch": api.fp64_fallback_count(bvh, stream)})
-        launches_per_step = 7  # query codes, sort histogram, 4 digit passes, traversal
         line = {
             "metric": METRIC, "value": value, "unit": "queries/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
@@ -1479,7 +1498,7 @@ def main() -> None:
                          "bytes_model": "16 B/query + (128 B node + moment node) per node entered + 36 B per exact triangle"},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": "queries/s", "h2d_bytes_per_step": 12 * n, "d2h_bytes_per_step": 4 * n},
-            "gpu_launches": launches_per_step * args.steps,
+            "gpu_launches": timed_launches,
             "clocks": clocks.summary(),
         }
         print(json.dumps(line), flush=True)

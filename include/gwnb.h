@@ -133,6 +133,11 @@ GWNB_API int gwnb_last_cuda_error(void);
 /* Library version string. */
 GWNB_API const char *gwnb_version(void);
 
+/* Number of kernel launches this library has issued in the process (all threads and devices); a
+ * launch recorded into a CUDA graph counts once, when it is captured. For benchmarks and tests that
+ * check which work ran on the GPU. */
+GWNB_API uint64_t gwnb_launch_count(void);
+
 /* ---- device memory ------------------------------------------------------------------------- */
 /* Every device allocation of the library comes from one memory pool per device that keeps freed
  * memory mapped between host synchronizations (no smallgwn counterpart: smallgwn allocates with

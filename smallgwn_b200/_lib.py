@@ -187,6 +187,7 @@ SIGNATURES: dict[str, tuple] = {
     "gwnb_version": (C.c_char_p, []),
     "gwnb_memory_stats": (C.c_int, [C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     "gwnb_memory_trim": (C.c_int, [C.c_uint64]),
+    "gwnb_launch_count": (C.c_uint64, []),
     "gwnb_geometry_upload_f32": (I, [C.POINTER(geometry_f32), P, P, P, U64, P, P, P, U64, P]),
     "gwnb_geometry_update_f32": (I, [C.POINTER(geometry_f32), P, P, P, U64, P]),
     "gwnb_geometry_update_device_f32": (I, [C.POINTER(geometry_f32), P, P, P, U64, P]),

@@ -713,6 +713,11 @@ def memory_stats() -> tuple[int, int]:
     return int(r.value), int(u.value)
 
 
+def launch_count() -> int:
+    """Kernel launches the library has issued in this process (graph-captured launches count once)."""
+    return int(_lib.load().gwnb_launch_count())
+
+
 def memory_trim(keep_bytes: int = 0) -> gwn_status:
     """Return the pool's cached device memory to the driver down to keep_bytes (or what is in use)."""
     return _status(_lib.load().gwnb_memory_trim(int(keep_bytes)))

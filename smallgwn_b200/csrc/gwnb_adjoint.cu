@@ -463,9 +463,9 @@ template <int Order>
 int launch_traverse(adjoint_params const &p, int cap, int block, cudaStream_t s) {
     unsigned const grid = grid_for(p.n, block);
     if (cap <= 32)
-        k_adjoint_traverse<Order, 32><<<grid, block, 0, s>>>(p);
+        note_launch(), k_adjoint_traverse<Order, 32><<<grid, block, 0, s>>>(p);
     else
-        k_adjoint_traverse<Order, 64><<<grid, block, 0, s>>>(p);
+        note_launch(), k_adjoint_traverse<Order, 64><<<grid, block, 0, s>>>(p);
     GWNB_CUDA_TRY(cudaGetLastError());
     return GWNB_OK;
 }
@@ -539,7 +539,7 @@ int taylor_adjoint(adjoint_request const &r, cudaStream_t s) {
                 return fail(rc);
             if (cudaMemsetAsync(tri_slot, 0xff, nt * sizeof(std::uint32_t), s) != cudaSuccess)
                 return fail(set_cuda_error(cudaGetLastError(), "adjoint leaf slots"));
-            k_leaf_slots<<<grid_for(nn), 256, 0, s>>>(r.nodes, nn, nt, tri_slot);
+            note_launch(), k_leaf_slots<<<grid_for(nn), 256, 0, s>>>(r.nodes, nn, nt, tri_slot);
         }
         adjoint_tri_params tp{};
         tp.qnodes = r.qnodes;
@@ -560,9 +560,9 @@ int taylor_adjoint(adjoint_request const &r, cudaStream_t s) {
         tp.dvz = r.dvz;
         tp.status = r.status;
         if (r.order == 0)
-            k_adjoint_triangles<0><<<grid_for(nt), 256, 0, s>>>(tp);
+            note_launch(), k_adjoint_triangles<0><<<grid_for(nt), 256, 0, s>>>(tp);
         else
-            k_adjoint_triangles<1><<<grid_for(nt), 256, 0, s>>>(tp);
+            note_launch(), k_adjoint_triangles<1><<<grid_for(nt), 256, 0, s>>>(tp);
         cudaError_t const e = cudaGetLastError();
         if (e != cudaSuccess)
             return fail(set_cuda_error(e, "adjoint triangle pass"));

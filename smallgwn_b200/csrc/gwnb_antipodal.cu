@@ -709,7 +709,7 @@ int gwnb_boundary_chain_build_u32(const gwnb_geometry_f32 *g, gwnb_boundary_chai
     }
     cudaError_t e = cudaMemsetAsync(flags, 0, 2 * sizeof(unsigned int), s);
     if (e == cudaSuccess) {
-        k_edge_keys<<<static_cast<unsigned>((nt + 255) / 256), 256, 0, s>>>(g->tri_i0, g->tri_i1, g->tri_i2, nt, nv, bits,
+        note_launch(), k_edge_keys<<<static_cast<unsigned>((nt + 255) / 256), 256, 0, s>>>(g->tri_i0, g->tri_i1, g->tri_i2, nt, nv, bits,
                                                                            keys, orient, flags);
         e = cudaGetLastError();
     }
@@ -721,8 +721,8 @@ int gwnb_boundary_chain_build_u32(const gwnb_geometry_f32 *g, gwnb_boundary_chai
         cleanup();
         return rc;
     }
-    k_chain_count<<<static_cast<unsigned>(nblocks), k_chain_block, 0, s>>>(keys_sorted, orient_sorted, ne, blocks);
-    k_chain_scan<<<1, 1024, 0, s>>>(blocks, nblocks);
+    note_launch(), k_chain_count<<<static_cast<unsigned>(nblocks), k_chain_block, 0, s>>>(keys_sorted, orient_sorted, ne, blocks);
+    note_launch(), k_chain_scan<<<1, 1024, 0, s>>>(blocks, nblocks);
     unsigned int host_flags[2] = {0, 0};
     std::uint32_t rows = 0;
     e = cudaMemcpyAsync(&rows, blocks + nblocks, sizeof(rows), cudaMemcpyDeviceToHost, s);
@@ -750,7 +750,7 @@ int gwnb_boundary_chain_build_u32(const gwnb_geometry_f32 *g, gwnb_boundary_chai
             cleanup();
             return rc;
         }
-        k_chain_emit<<<static_cast<unsigned>(nblocks), k_chain_block, 0, s>>>(
+        note_launch(), k_chain_emit<<<static_cast<unsigned>(nblocks), k_chain_block, 0, s>>>(
             keys_sorted, orient_sorted, ne, bits, blocks, staging.start_vertex, staging.end_vertex, staging.multiplicity);
         e = cudaGetLastError();
         if (e != cudaSuccess) {
@@ -836,7 +836,7 @@ static int antipodal_common(const gwnb_geometry_f32 *g, const gwnb_bvh4_f32 *b_i
     int rc = GWNB_OK;
     if (c->edge_count > 0) {
         GWNB_TRY(alloc(&edges, 2 * c->edge_count, s));
-        k_edge_records<<<static_cast<unsigned>((c->edge_count + 255) / 256), 256, 0, s>>>(
+        note_launch(), k_edge_records<<<static_cast<unsigned>((c->edge_count + 255) / 256), 256, 0, s>>>(
             *g, c->start_vertex, c->end_vertex, c->multiplicity, c->edge_count, edges);
     }
     if (o.sort_queries != 0 && n > 1 && a != nullptr) {
@@ -858,7 +858,7 @@ static int antipodal_common(const gwnb_geometry_f32 *g, const gwnb_bvh4_f32 *b_i
         p.n = n;
         if (gradient) {
             unsigned const grid = static_cast<unsigned>((n + o.block_size - 1) / o.block_size);
-            k_antipodal_gradient<<<grid, o.block_size, 0, s>>>(p);
+            note_launch(), k_antipodal_gradient<<<grid, o.block_size, 0, s>>>(p);
         } else {
             std::uint64_t const per_block = static_cast<std::uint64_t>(o.block_size) * k_ap_q;
             unsigned const grid = static_cast<unsigned>((n + per_block - 1) / per_block);
@@ -868,7 +868,7 @@ static int antipodal_common(const gwnb_geometry_f32 *g, const gwnb_bvh4_f32 *b_i
             if (smem > 48 * 1024)
                 e = cudaFuncSetAttribute(k_antipodal, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
             if (e == cudaSuccess)
-                k_antipodal<<<grid, o.block_size, smem, s>>>(p);
+                note_launch(), k_antipodal<<<grid, o.block_size, smem, s>>>(p);
         }
         cudaError_t const e = cudaGetLastError();
         if (e != cudaSuccess)

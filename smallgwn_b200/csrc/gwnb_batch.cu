@@ -253,7 +253,7 @@ int gwnb_batch_sync_f32(gwnb_batch *b, gwnb_stream_t stream) {
         return set_error(GWNB_INVALID_ARGUMENT, "batch: null handle.");
     cudaStream_t const s = as_cuda(stream);
     GWNB_CUDA_TRY(cudaMemsetAsync(b->d_flags, 0, sizeof(unsigned int), s));
-    k_gather_status<<<1, 256, 0, s>>>(b->d_status, static_cast<std::uint32_t>(b->status_words.size()), b->d_flags);
+    note_launch(), k_gather_status<<<1, 256, 0, s>>>(b->d_status, static_cast<std::uint32_t>(b->status_words.size()), b->d_flags);
     GWNB_CUDA_TRY(cudaGetLastError());
     unsigned int flags = 0;
     GWNB_CUDA_TRY(cudaMemcpyAsync(&flags, b->d_flags, sizeof(flags), cudaMemcpyDeviceToHost, s));

@@ -511,13 +511,13 @@ int build_scene_and_morton(gwnb_geometry_f32 const &g, int morton_bits, aabb *aa
     GWNB_CUDA_TRY(cudaMemcpyAsync(scene, init, sizeof(init), cudaMemcpyHostToDevice, s));
     unsigned const grid = static_cast<unsigned>(
         std::min<std::uint64_t>(grid_for(g.vertex_count), static_cast<std::uint64_t>(device_sm_count()) * 4));
-    k_scene_bounds<<<std::max(1u, grid), k_block, 0, s>>>(g.vertex_x, g.vertex_y, g.vertex_z,
+    note_launch(), k_scene_bounds<<<std::max(1u, grid), k_block, 0, s>>>(g.vertex_x, g.vertex_y, g.vertex_z,
                                                           g.vertex_count, scene);
     if (morton_bits == 32)
-        k_morton<std::uint32_t><<<grid_for(nt), k_block, 0, s>>>(
+        note_launch(), k_morton<std::uint32_t><<<grid_for(nt), k_block, 0, s>>>(
             g, scene, aabbs, static_cast<std::uint32_t *>(codes));
     else
-        k_morton<std::uint64_t><<<grid_for(nt), k_block, 0, s>>>(
+        note_launch(), k_morton<std::uint64_t><<<grid_for(nt), k_block, 0, s>>>(
             g, scene, aabbs, static_cast<std::uint64_t *>(codes));
     GWNB_CUDA_TRY(cudaGetLastError());
     release(scene, s);
@@ -538,7 +538,7 @@ int build_preprocess(gwnb_geometry_f32 const &g, int morton_bits, void *sorted_c
     GWNB_TRY(alloc(reinterpret_cast<unsigned char **>(&codes), nt * kb, s));
     GWNB_TRY(build_scene_and_morton(g, morton_bits, aabbs, codes, s));
     GWNB_TRY(radix_sort_pairs(codes, sorted_codes, nullptr, sorted_ids, nt, kb, morton_bits, s, status));
-    k_gather_aabbs<<<grid_for(nt), k_block, 0, s>>>(aabbs, sorted_ids, sorted_aabbs, nt);
+    note_launch(), k_gather_aabbs<<<grid_for(nt), k_block, 0, s>>>(aabbs, sorted_ids, sorted_aabbs, nt);
     GWNB_CUDA_TRY(cudaGetLastError());
     release(aabbs, s);
     release(codes, s);
@@ -561,14 +561,14 @@ int build_binary_lbvh(void const *sorted_codes, int morton_bits, std::uint64_t n
     GWNB_CUDA_TRY(cudaMemsetAsync(leaf_parent, 0xff, n * sizeof(std::uint32_t), s));
     GWNB_CUDA_TRY(cudaMemsetAsync(arrivals, 0, ni * sizeof(unsigned int), s));
     if (morton_bits == 32)
-        k_karras<std::uint32_t><<<grid_for(ni), k_block, 0, s>>>(
+        note_launch(), k_karras<std::uint32_t><<<grid_for(ni), k_block, 0, s>>>(
             static_cast<std::uint32_t const *>(sorted_codes), static_cast<std::int64_t>(n), nodes,
             internal_parent, leaf_parent);
     else
-        k_karras<std::uint64_t><<<grid_for(ni), k_block, 0, s>>>(
+        note_launch(), k_karras<std::uint64_t><<<grid_for(ni), k_block, 0, s>>>(
             static_cast<std::uint64_t const *>(sorted_codes), static_cast<std::int64_t>(n), nodes,
             internal_parent, leaf_parent);
-    k_binary_bounds<<<grid_for(n), k_block, 0, s>>>(sorted_aabbs, n, leaf_parent, internal_parent,
+    note_launch(), k_binary_bounds<<<grid_for(n), k_block, 0, s>>>(sorted_aabbs, n, leaf_parent, internal_parent,
                                                     pending, internal_bounds, arrivals, status);
     GWNB_CUDA_TRY(cudaGetLastError());
     release(leaf_parent, s);
@@ -612,7 +612,7 @@ int collapse_to_bvh4(binary_node const *binary, aabb const *binary_bounds, aabb 
     p.tile_counter = words + 2 * (k_max_levels + 1);
     p.stack_bounds = words + 3 * (k_max_levels + 1);
     p.status = status;
-    k_collapse_init<<<1, 1, 0, s>>>(p, root_binary);
+    note_launch(), k_collapse_init<<<1, 1, 0, s>>>(p, root_binary);
     int const sms = device_sm_count();
     unsigned const grid = static_cast<unsigned>(std::min<std::uint64_t>(max_tiles, static_cast<std::uint64_t>(sms) * 4));
     std::vector<std::uint32_t> host_counts(k_max_levels + 1);
@@ -620,7 +620,7 @@ int collapse_to_bvh4(binary_node const *binary, aabb const *binary_bounds, aabb 
     bool done = false;
     while (!done) {
         for (int b = 0; b < 8 && level < k_max_levels; ++b, ++level)
-            k_collapse_level<<<grid, k_block, 0, s>>>(p, level);
+            note_launch(), k_collapse_level<<<grid, k_block, 0, s>>>(p, level);
         GWNB_CUDA_TRY(cudaGetLastError());
         std::uint32_t c = 0;
         GWNB_CUDA_TRY(cudaMemcpyAsync(&c, p.level_count + level, sizeof(c), cudaMemcpyDeviceToHost, s));
@@ -659,7 +659,7 @@ int build_triangles(gwnb_geometry_f32 const &g, std::uint32_t const *ids, std::u
                     triangle *tris, triangle48 *tri48, cudaStream_t s, unsigned int *status) {
     if (n == 0)
         return GWNB_OK;
-    k_triangles<<<grid_for(n), k_block, 0, s>>>(g, ids, n, tris, tri48, status);
+    note_launch(), k_triangles<<<grid_for(n), k_block, 0, s>>>(g, ids, n, tris, tri48, status);
     GWNB_CUDA_TRY(cudaGetLastError());
     return GWNB_OK;
 }

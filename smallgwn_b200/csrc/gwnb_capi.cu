@@ -35,6 +35,8 @@ int set_cuda_error(cudaError_t err, char const *what) {
     return GWNB_CUDA_RUNTIME_ERROR;
 }
 
+std::atomic<std::uint64_t> g_launch_count{0};
+
 std::uint64_t reserve_revision() {
     static std::atomic<std::uint64_t> next{1};
     std::uint64_t r = next.load(std::memory_order_relaxed);
@@ -286,6 +288,8 @@ extern "C" {
 
 const char *gwnb_last_error_message(void) { return g_message.c_str(); }
 
+uint64_t gwnb_launch_count(void) { return g_launch_count.load(std::memory_order_relaxed); }
+
 int gwnb_memory_stats(uint64_t *reserved, uint64_t *used) {
     cudaMemPool_t pool = nullptr;
     GWNB_TRY(library_pool(&pool));
@@ -352,7 +356,7 @@ int gwnb_geometry_upload_f32(gwnb_geometry_f32 *out, const float *x, const float
         unsigned int host_flag = 0;
         if ((e = cudaMemsetAsync(flag, 0, sizeof(unsigned int), s)) != cudaSuccess)
             return fail(set_cuda_error(e, "cudaMemsetAsync"));
-        k_validate_indices<<<static_cast<unsigned>((nt + 255) / 256), 256, 0, s>>>(g.tri_i0, g.tri_i1, g.tri_i2, nt,
+        note_launch(), k_validate_indices<<<static_cast<unsigned>((nt + 255) / 256), 256, 0, s>>>(g.tri_i0, g.tri_i1, g.tri_i2, nt,
                                                                                  nv, flag);
         if ((e = cudaGetLastError()) != cudaSuccess ||
             (e = cudaMemcpyAsync(&host_flag, flag, sizeof(host_flag), cudaMemcpyDeviceToHost, s)) != cudaSuccess ||

@@ -271,14 +271,14 @@ int build_binary_hploc(void const *sorted_codes, int morton_bits, std::uint64_t 
     GWNB_CUDA_TRY(cudaMemsetAsync(internal_parent, 0xff, (n - 1) * sizeof(std::uint32_t), s));
     std::uint32_t const n32 = static_cast<std::uint32_t>(n);
     GWNB_CUDA_TRY(cudaMemcpyAsync(counter, &n32, sizeof(n32), cudaMemcpyHostToDevice, s));
-    k_iota<<<(n32 + 255) / 256, 256, 0, s>>>(cluster, n32);
+    note_launch(), k_iota<<<(n32 + 255) / 256, 256, 0, s>>>(cluster, n32);
     hploc_params p{n32, radius, sorted_aabbs, nodes, internal_bounds, internal_parent, cluster,
                    boundary, counter, status};
     unsigned const grid = static_cast<unsigned>((n + k_hploc_block - 1) / k_hploc_block);
     if (morton_bits == 32)
-        k_hploc<std::uint32_t><<<grid, k_hploc_block, 0, s>>>(p, static_cast<std::uint32_t const *>(sorted_codes));
+        note_launch(), k_hploc<std::uint32_t><<<grid, k_hploc_block, 0, s>>>(p, static_cast<std::uint32_t const *>(sorted_codes));
     else
-        k_hploc<std::uint64_t><<<grid, k_hploc_block, 0, s>>>(p, static_cast<std::uint64_t const *>(sorted_codes));
+        note_launch(), k_hploc<std::uint64_t><<<grid, k_hploc_block, 0, s>>>(p, static_cast<std::uint64_t const *>(sorted_codes));
     GWNB_CUDA_TRY(cudaGetLastError());
     std::uint32_t host_count = 0;
     unsigned int host_status = 0;

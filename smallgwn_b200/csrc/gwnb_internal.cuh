@@ -9,6 +9,7 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstddef>
 #include <cstdint>
 #include <string>
@@ -182,6 +183,11 @@ int set_cuda_error(cudaError_t err, char const *what);
 
 std::uint64_t reserve_revision();
 int device_sm_count();
+
+// Counts the kernel launches the library issues (every launch site is `note_launch(), k<<<...>>>`);
+// gwnb_launch_count reports the total. A launch recorded into a CUDA graph counts once, at capture.
+extern std::atomic<std::uint64_t> g_launch_count;
+inline void note_launch() { g_launch_count.fetch_add(1, std::memory_order_relaxed); }
 
 // ---- allocation (stream ordered) ---------------------------------------------------------------
 // Every device allocation of the library comes from one memory pool per device that keeps freed

@@ -613,7 +613,7 @@ __global__ void __launch_bounds__(256)
 template <int Order, int Cap, int Mode, bool Grad, bool Stats>
 int launch_taylor_warp(taylor_params const &p, int block, cudaStream_t s) {
     unsigned const grid = static_cast<unsigned>((p.n + block - 1) / block);
-    k_taylor_warp<Order, Cap, Mode, Grad, Stats><<<grid, block, 0, s>>>(p);
+    note_launch(), k_taylor_warp<Order, Cap, Mode, Grad, Stats><<<grid, block, 0, s>>>(p);
     GWNB_CUDA_TRY(cudaGetLastError());
     return GWNB_OK;
 }
@@ -626,7 +626,7 @@ int launch_taylor_cap(taylor_params const &p, int block, cudaStream_t s) {
         GWNB_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            static_cast<int>(smem)));
     unsigned const grid = static_cast<unsigned>((p.n + block - 1) / block);
-    kern<<<grid, block, smem, s>>>(p);
+    note_launch(), kern<<<grid, block, smem, s>>>(p);
     GWNB_CUDA_TRY(cudaGetLastError());
     return GWNB_OK;
 }
@@ -671,9 +671,9 @@ int exact_batch(triangle const *tris, std::uint64_t nt, float const *qx, float c
     if (ranges > 1)
         GWNB_TRY(alloc(&partial, ranges * nq, s));
     dim3 const grid(static_cast<unsigned>(qblocks), static_cast<unsigned>(ranges));
-    k_exact<<<grid, k_exact_block, 0, s>>>(tris, nt, qx, qy, qz, out, nq, partial);
+    note_launch(), k_exact<<<grid, k_exact_block, 0, s>>>(tris, nt, qx, qy, qz, out, nq, partial);
     if (ranges > 1)
-        k_exact_finish<<<static_cast<unsigned>((nq + 255) / 256), 256, 0, s>>>(partial, static_cast<unsigned>(ranges),
+        note_launch(), k_exact_finish<<<static_cast<unsigned>((nq + 255) / 256), 256, 0, s>>>(partial, static_cast<unsigned>(ranges),
                                                                              out, nq);
     cudaError_t const e = cudaGetLastError();
     release(partial, s);
@@ -686,7 +686,7 @@ int exact_batch_f64(gwnb_geometry_f32 const &g, float const *qx, float const *qy
                     std::uint64_t nq, cudaStream_t s) {
     if (nq == 0)
         return GWNB_OK;
-    k_exact_f64<<<static_cast<unsigned>((nq + k_exact_block - 1) / k_exact_block), k_exact_block, 0, s>>>(
+    note_launch(), k_exact_f64<<<static_cast<unsigned>((nq + k_exact_block - 1) / k_exact_block), k_exact_block, 0, s>>>(
         g, qx, qy, qz, out, nq);
     GWNB_CUDA_TRY(cudaGetLastError());
     return GWNB_OK;
@@ -699,7 +699,7 @@ int query_order(aabb const *root_bounds, float const *qx, float const *qy, float
     std::uint32_t *codes = nullptr, *sorted = nullptr;
     GWNB_TRY(alloc(&codes, n, s));
     GWNB_TRY(alloc(&sorted, n, s));
-    k_query_codes<<<static_cast<unsigned>((n + 255) / 256), 256, 0, s>>>(qx, qy, qz, n, root_bounds, codes);
+    note_launch(), k_query_codes<<<static_cast<unsigned>((n + 255) / 256), 256, 0, s>>>(qx, qy, qz, n, root_bounds, codes);
     int const rc = radix_sort_pairs(codes, sorted, nullptr, order, n, 4, 30, s, status);
     release(codes, s);
     release(sorted, s);
@@ -746,7 +746,7 @@ int taylor_batch(taylor_request const &r, cudaStream_t s) {
         GWNB_TRY(alloc(&codes, r.n, s));
         GWNB_TRY(alloc(&sorted_codes, r.n, s));
         GWNB_TRY(alloc(&order, r.n, s));
-        k_query_codes<<<static_cast<unsigned>((r.n + 255) / 256), 256, 0, s>>>(r.qx, r.qy, r.qz, r.n,
+        note_launch(), k_query_codes<<<static_cast<unsigned>((r.n + 255) / 256), 256, 0, s>>>(r.qx, r.qy, r.qz, r.n,
                                                                             r.root_bounds, codes);
         GWNB_TRY(radix_sort_pairs(codes, sorted_codes, nullptr, order, r.n, 4, 30, s, r.status));
         p.order = order;
@@ -830,13 +830,13 @@ int launch_batch_cap(batch_query_state const &st, batch_query_config const &c, c
     std::uint64_t const cap = static_cast<std::uint64_t>(device_sm_count()) * std::max(c.grid_scale, 1);
     unsigned const grid = static_cast<unsigned>(std::max<std::uint64_t>(std::min(need, cap), 1));
     if (c.per_thread == 0) {
-        k_batch_taylor_warp<Order, Cap, Mode><<<grid, block, 0, s>>>(meshes, st.warp_begin, st.mesh_count, st.warps);
+        note_launch(), k_batch_taylor_warp<Order, Cap, Mode><<<grid, block, 0, s>>>(meshes, st.warp_begin, st.mesh_count, st.warps);
     } else {
         std::size_t const smem = static_cast<std::size_t>(Cap) * block * sizeof(std::uint32_t);
         auto kern = k_batch_taylor_thread<Order, Cap, Mode>;
         if (smem > 48 * 1024)
             GWNB_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
-        kern<<<grid, block, smem, s>>>(meshes, st.warp_begin, st.mesh_count, st.warps);
+        note_launch(), kern<<<grid, block, smem, s>>>(meshes, st.warp_begin, st.mesh_count, st.warps);
     }
     GWNB_CUDA_TRY(cudaGetLastError());
     return GWNB_OK;
@@ -920,7 +920,7 @@ int taylor_batch_in_scratch(taylor_request const &r, std::uint32_t *scratch, std
         std::uint32_t *keys_tmp = scratch + 3 * capacity;
         std::uint32_t *vals_tmp = scratch + 4 * capacity;
         std::uint32_t *words = scratch + 5 * capacity;
-        k_query_codes<<<static_cast<unsigned>((r.n + 255) / 256), 256, 0, s>>>(r.qx, r.qy, r.qz, r.n,
+        note_launch(), k_query_codes<<<static_cast<unsigned>((r.n + 255) / 256), 256, 0, s>>>(r.qx, r.qy, r.qz, r.n,
                                                                             r.root_bounds, codes);
         GWNB_TRY(radix_sort_pairs_u32_in_scratch(codes, sorted_codes, nullptr, order, r.n, 30, keys_tmp, vals_tmp,
                                                  words, s, r.status));

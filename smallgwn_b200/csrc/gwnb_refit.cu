@@ -770,7 +770,7 @@ int ensure_bvh_aux(gwnb_bvh4_f32 *bvh, cudaStream_t s) {
         GWNB_CUDA_TRY(cudaMemsetAsync(a->parent_slot, 0xff, nn * sizeof(std::uint32_t), s));
         GWNB_CUDA_TRY(cudaMemsetAsync(a->arrivals, 0, 2 * nn * sizeof(std::uint32_t), s));
         GWNB_CUDA_TRY(cudaMemsetAsync(a->leaf_nodes + nn, 0, sizeof(std::uint32_t), s));
-        k_prepare_aux<<<grid_for(nn, 256), 256, 0, s>>>(
+        note_launch(), k_prepare_aux<<<grid_for(nn, 256), 256, 0, s>>>(
             reinterpret_cast<node4 const *>(bvh->nodes), nn, bvh->primitive_count, a->parent_slot,
             a->expected, a->leaf_nodes, a->leaf_nodes + nn, a->status);
         GWNB_CUDA_TRY(cudaGetLastError());
@@ -801,7 +801,7 @@ int write_tri48(gwnb_bvh4_f32 const *bvh, cudaStream_t s) {
     auto *a = reinterpret_cast<bvh_aux_impl *>(bvh->aux);
     if (bvh->primitive_count == 0)
         return GWNB_OK;
-    k_tri48<<<grid_for(bvh->primitive_count, 256), 256, 0, s>>>(
+    note_launch(), k_tri48<<<grid_for(bvh->primitive_count, 256), 256, 0, s>>>(
         reinterpret_cast<triangle const *>(bvh->triangles), a->tri48, bvh->primitive_count);
     GWNB_CUDA_TRY(cudaGetLastError());
     return GWNB_OK;
@@ -898,15 +898,15 @@ int batch_refit_launch(batch_refit_state const &st, int block, bool bounds, bool
         return static_cast<unsigned>(need < cap ? need : cap);
     };
     if (bounds && st.bounds_items > 0)
-        k_batch_refit_bounds<<<grid(st.bounds_items), block, 0, s>>>(
+        note_launch(), k_batch_refit_bounds<<<grid(st.bounds_items), block, 0, s>>>(
             static_cast<batch_bounds_mesh const *>(st.bounds_meshes), st.bounds_begin, st.mesh_count);
     if (moments && st.moment_items > 0) {
         auto const *md = static_cast<moment_params const *>(st.moment_meshes);
         unsigned const g = grid(st.moment_items);
         switch (st.order) {
-        case 0: k_batch_refit_moments<0><<<g, block, 0, s>>>(md, st.moment_begin, st.mesh_count); break;
-        case 1: k_batch_refit_moments<1><<<g, block, 0, s>>>(md, st.moment_begin, st.mesh_count); break;
-        default: k_batch_refit_moments<2><<<g, block, 0, s>>>(md, st.moment_begin, st.mesh_count); break;
+        case 0: note_launch(), k_batch_refit_moments<0><<<g, block, 0, s>>>(md, st.moment_begin, st.mesh_count); break;
+        case 1: note_launch(), k_batch_refit_moments<1><<<g, block, 0, s>>>(md, st.moment_begin, st.mesh_count); break;
+        default: note_launch(), k_batch_refit_moments<2><<<g, block, 0, s>>>(md, st.moment_begin, st.mesh_count); break;
         }
     }
     GWNB_CUDA_TRY(cudaGetLastError());
@@ -942,9 +942,9 @@ int refit_bounds_async(gwnb_geometry_f32 const &g, gwnb_bvh4_f32 *bvh, cudaStrea
     p.root_bounds = a->root_bounds;
     p.status = a->status;
     if (bvh->root.reference != 0 && ref_leaf(bvh->root.reference)) {
-        k_refit_leaf_root<<<1, 1, 0, s>>>(p, ref_offset(bvh->root.reference), ref_count(bvh->root.reference));
+        note_launch(), k_refit_leaf_root<<<1, 1, 0, s>>>(p, ref_offset(bvh->root.reference), ref_count(bvh->root.reference));
     } else if (a->leaf_node_count > 0) {
-        k_refit_bounds<<<grid_for(a->leaf_node_count), k_block, 0, s>>>(p);
+        note_launch(), k_refit_bounds<<<grid_for(a->leaf_node_count), k_block, 0, s>>>(p);
     }
     GWNB_CUDA_TRY(cudaGetLastError());
     return GWNB_OK;
@@ -974,9 +974,9 @@ int refit_moments_async(gwnb_bvh4_f32 const *bvh, gwnb_moment4_f32 *m, cudaStrea
     if (grid == 0)
         return set_error(GWNB_INTERNAL_ERROR, "bvh.refit.moment: BVH has no leaf-bearing node.");
     switch (m->order) {
-    case 0: k_refit_moments<0><<<grid, k_block, 0, s>>>(p); break;
-    case 1: k_refit_moments<1><<<grid, k_block, 0, s>>>(p); break;
-    default: k_refit_moments<2><<<grid, k_block, 0, s>>>(p); break;
+    case 0: note_launch(), k_refit_moments<0><<<grid, k_block, 0, s>>>(p); break;
+    case 1: note_launch(), k_refit_moments<1><<<grid, k_block, 0, s>>>(p); break;
+    default: note_launch(), k_refit_moments<2><<<grid, k_block, 0, s>>>(p); break;
     }
     GWNB_CUDA_TRY(cudaGetLastError());
     return GWNB_OK;

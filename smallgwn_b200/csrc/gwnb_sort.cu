@@ -255,7 +255,7 @@ int sort_impl(K const *keys_in, K *keys_out, std::uint32_t const *vals_in,
     int const sms = device_sm_count();
     unsigned const hist_grid = static_cast<unsigned>(
         std::min<std::uint64_t>((n + k_threads - 1) / k_threads, static_cast<std::uint64_t>(sms) * 8));
-    k_sort_histogram<K><<<hist_grid, k_threads, 0, s>>>(keys_in, n, passes, key_bits, hist);
+    note_launch(), k_sort_histogram<K><<<hist_grid, k_threads, 0, s>>>(keys_in, n, passes, key_bits, hist);
 
     // Ping-pong so that the last pass lands in the output buffers.
     bool to_out = (passes % 2) == 1;
@@ -266,7 +266,7 @@ int sort_impl(K const *keys_in, K *keys_out, std::uint32_t const *vals_in,
         std::uint32_t *dst_v = to_out ? vals_out : vals_tmp;
         int const bits = std::min(8, key_bits - 8 * p);
         std::uint32_t const mask = (1u << bits) - 1u;
-        k_onesweep<K, k_items><<<static_cast<unsigned>(tiles), k_threads, 0, s>>>(
+        note_launch(), k_onesweep<K, k_items><<<static_cast<unsigned>(tiles), k_threads, 0, s>>>(
             src_k, src_v, dst_k, dst_v, n, 8 * p, mask, hist + p * 256,
             tile_status + static_cast<std::size_t>(p) * tiles * 256, counters + p, status);
         src_k = dst_k;
@@ -300,7 +300,7 @@ int sort_in_scratch(K const *keys_in, K *keys_out, std::uint32_t const *vals_in,
     int const sms = device_sm_count();
     unsigned const hist_grid = static_cast<unsigned>(
         std::min<std::uint64_t>((n + k_threads - 1) / k_threads, static_cast<std::uint64_t>(sms) * 8));
-    k_sort_histogram<K><<<hist_grid, k_threads, 0, s>>>(keys_in, n, passes, key_bits, hist);
+    note_launch(), k_sort_histogram<K><<<hist_grid, k_threads, 0, s>>>(keys_in, n, passes, key_bits, hist);
     bool to_out = (passes % 2) == 1;
     K const *src_k = keys_in;
     std::uint32_t const *src_v = vals_in;
@@ -309,7 +309,7 @@ int sort_in_scratch(K const *keys_in, K *keys_out, std::uint32_t const *vals_in,
         std::uint32_t *dst_v = to_out ? vals_out : vals_tmp;
         int const bits = std::min(8, key_bits - 8 * p);
         std::uint32_t const mask = (1u << bits) - 1u;
-        k_onesweep<K, k_items><<<static_cast<unsigned>(tiles), k_threads, 0, s>>>(
+        note_launch(), k_onesweep<K, k_items><<<static_cast<unsigned>(tiles), k_threads, 0, s>>>(
             src_k, src_v, dst_k, dst_v, n, 8 * p, mask, hist + p * 256,
             tile_status + static_cast<std::size_t>(p) * tiles * 256, counters + p, status);
         src_k = dst_k;

@@ -617,7 +617,7 @@ template <class Kern> int launch_with_stack(Kern kern, spatial_params const &p, 
     if (smem > 48 * 1024)
         GWNB_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
     unsigned const grid = static_cast<unsigned>((p.n + block - 1) / block);
-    kern<<<grid, block, smem, s>>>(p);
+    note_launch(), kern<<<grid, block, smem, s>>>(p);
     GWNB_CUDA_TRY(cudaGetLastError());
     return GWNB_OK;
 }
@@ -636,7 +636,7 @@ int ray_order(bvh_aux_impl const *a, float const *ox, float const *oy, float con
     if (rc == GWNB_OK)
         rc = alloc(&sorted, n, s);
     if (rc == GWNB_OK) {
-        k_ray_codes<<<static_cast<unsigned>((n + 255) / 256), 256, 0, s>>>(ox, oy, oz, dx, dy, dz, n, a->root_bounds,
+        note_launch(), k_ray_codes<<<static_cast<unsigned>((n + 255) / 256), 256, 0, s>>>(ox, oy, oz, dx, dy, dz, n, a->root_bounds,
                                                                           codes);
         rc = radix_sort_pairs(codes, sorted, nullptr, order, n, 4, 30, s, a->status);
     }

@@ -42,3 +42,26 @@ def test_pool_retains_and_trims(cuda):
     # and work after a trim is unaffected
     geo = upload(meshes.soup_mesh(30, seed=2))
     assert g.gwn_build_bvh(geo, bvh).is_ok()
+
+
+def test_launch_counter_counts_library_kernels(cuda):
+    """gwnb_launch_count moves by exactly the kernels a call issues: one traversal for a Taylor
+    batch in input order; query codes, the radix sort (histogram and four 8-bit passes over the
+    30-bit codes) and the traversal for an ordered batch; nothing for a rejected call."""
+    mesh = meshes.soup_mesh(40, seed=6)
+    geo = upload(mesh)
+    bvh = g.gwn_bvh4_object()
+    assert g.gwn_build_bvh(geo, bvh).is_ok()
+    mom = g.gwn_bvh4_moment_object(1)
+    assert g.gwn_refit_bvh_moment(1, bvh, mom).is_ok()
+    q = [cuda.from_numpy(v).cuda() for v in meshes.mixed_queries(mesh, 5000, seed=1)]
+    out = cuda.empty_like(q[0])
+    c0 = api.launch_count()
+    assert g.gwn_compute_winding_number_taylor_batch(1, bvh, mom, *q, out, sort_queries=False).is_ok()
+    c1 = api.launch_count()
+    assert g.gwn_compute_winding_number_taylor_batch(1, bvh, mom, *q, out, sort_queries=True).is_ok()
+    c2 = api.launch_count()
+    stale = g.gwn_bvh4_moment_object(1)
+    assert not g.gwn_compute_winding_number_taylor_batch(1, bvh, stale, *q, out).is_ok()
+    c3 = api.launch_count()
+    assert (c1 - c0, c2 - c1, c3 - c2) == (1, 7, 0)
