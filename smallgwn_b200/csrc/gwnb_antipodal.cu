@@ -669,7 +669,7 @@ using namespace gwnb;
 
 extern "C" {
 
-int gwnb_boundary_chain_build_u32(const gwnb_geometry_f32 *g, gwnb_boundary_chain_u32 *out, gwnb_stream_t stream) {
+int gwnb_boundary_chain_build_u32(const gwnb_geometry_f32 *g, gwnb_boundary_chain_u32 *out, gwnb_stream_t stream) try {
     if (out == nullptr)
         return set_error(GWNB_INVALID_ARGUMENT, "Boundary chain output is null.");
     if (!geometry_valid(g))
@@ -762,6 +762,8 @@ int gwnb_boundary_chain_build_u32(const gwnb_geometry_f32 *g, gwnb_boundary_chai
     cleanup();
     *out = staging;
     return GWNB_OK;
+} catch (...) {
+    return host_exception();
 }
 
 void gwnb_boundary_chain_release_u32(gwnb_boundary_chain_u32 *chain, gwnb_stream_t stream) {
@@ -882,13 +884,15 @@ static int antipodal_common(const gwnb_geometry_f32 *g, const gwnb_bvh4_f32 *b_i
 int gwnb_winding_antipodal_batch_f32(const gwnb_geometry_f32 *g, const gwnb_bvh4_f32 *b,
                                      const gwnb_boundary_chain_u32 *chain, const float *qx, const float *qy,
                                      const float *qz, float *out, uint64_t n, const gwnb_spatial_options *options,
-                                     gwnb_stream_t stream) {
+                                     gwnb_stream_t stream) try {
     return antipodal_common(g, b, chain, qx, qy, qz, out, nullptr, nullptr, nullptr, n, options, stream);
+} catch (...) {
+    return host_exception();
 }
 
 int gwnb_winding_gradient_antipodal_batch_f32(const gwnb_geometry_f32 *g, const gwnb_boundary_chain_u32 *chain,
                                               const float *qx, const float *qy, const float *qz, float *gx, float *gy,
-                                              float *gz, uint64_t n, int block_size, gwnb_stream_t stream) {
+                                              float *gz, uint64_t n, int block_size, gwnb_stream_t stream) try {
     if (n > 0 && (gx == nullptr || gy == nullptr || gz == nullptr))
         return set_error(GWNB_INVALID_ARGUMENT, "Query/output spans require non-null storage when non-empty.");
     gwnb_spatial_options const o{block_size, 64, 0};
@@ -896,6 +900,8 @@ int gwnb_winding_gradient_antipodal_batch_f32(const gwnb_geometry_f32 *g, const 
     float marker = 0.0f;
     return antipodal_common(g, nullptr, chain, qx, qy, qz, nullptr, gx ? gx : &marker, gy ? gy : &marker,
                             gz ? gz : &marker, n, &o, stream);
+} catch (...) {
+    return host_exception();
 }
 
 } // extern "C"

@@ -76,7 +76,7 @@ using namespace gwnb;
 extern "C" {
 
 int gwnb_batch_create_f32(const gwnb_batch_mesh_f32 *meshes, uint32_t mesh_count, float beta,
-                          const gwnb_taylor_options *opt, gwnb_batch **out, gwnb_stream_t stream) {
+                          const gwnb_taylor_options *opt, gwnb_batch **out, gwnb_stream_t stream) try {
     if (out == nullptr)
         return set_error(GWNB_INVALID_ARGUMENT, "batch: output handle must be non-null.");
     *out = nullptr;
@@ -172,30 +172,38 @@ int gwnb_batch_create_f32(const gwnb_batch_mesh_f32 *meshes, uint32_t mesh_count
         return fail(set_cuda_error(cudaGetLastError(), "batch descriptors"));
     *out = b;
     return GWNB_OK;
+} catch (...) {
+    return host_exception();
 }
 
-int gwnb_batch_set_tuning_f32(gwnb_batch *b, const gwnb_batch_tuning *t) {
+int gwnb_batch_set_tuning_f32(gwnb_batch *b, const gwnb_batch_tuning *t) try {
     if (b == nullptr || t == nullptr || !tuning_valid(*t))
         return set_error(GWNB_INVALID_ARGUMENT, "batch: invalid tuning.");
     b->tuning = *t;
     return GWNB_OK;
+} catch (...) {
+    return host_exception();
 }
 
-int gwnb_batch_frame_f32(gwnb_batch *b, gwnb_stream_t stream) {
+int gwnb_batch_frame_f32(gwnb_batch *b, gwnb_stream_t stream) try {
     if (b == nullptr)
         return set_error(GWNB_INVALID_ARGUMENT, "batch: null handle.");
     return frame(b, b->tuning, as_cuda(stream));
+} catch (...) {
+    return host_exception();
 }
 
-int gwnb_batch_run_f32(gwnb_batch *b, unsigned int stages, gwnb_stream_t stream) {
+int gwnb_batch_run_f32(gwnb_batch *b, unsigned int stages, gwnb_stream_t stream) try {
     if (b == nullptr)
         return set_error(GWNB_INVALID_ARGUMENT, "batch: null handle.");
     if ((stages & ~(GWNB_BATCH_REFIT | GWNB_BATCH_MOMENTS | GWNB_BATCH_QUERY)) != 0u)
         return set_error(GWNB_INVALID_ARGUMENT, "batch: unknown stage bits.");
     return run_stages(b, b->tuning, stages, as_cuda(stream));
+} catch (...) {
+    return host_exception();
 }
 
-int gwnb_batch_tune_f32(gwnb_batch *b, int reps, gwnb_batch_tuning *chosen, gwnb_stream_t stream) {
+int gwnb_batch_tune_f32(gwnb_batch *b, int reps, gwnb_batch_tuning *chosen, gwnb_stream_t stream) try {
     if (b == nullptr || reps <= 0)
         return set_error(GWNB_INVALID_ARGUMENT, "batch: tuning needs a handle and a positive repetition count.");
     cudaStream_t const s = as_cuda(stream);
@@ -246,9 +254,11 @@ int gwnb_batch_tune_f32(gwnb_batch *b, int reps, gwnb_batch_tuning *chosen, gwnb
     if (chosen != nullptr)
         *chosen = best;
     return GWNB_OK;
+} catch (...) {
+    return host_exception();
 }
 
-int gwnb_batch_sync_f32(gwnb_batch *b, gwnb_stream_t stream) {
+int gwnb_batch_sync_f32(gwnb_batch *b, gwnb_stream_t stream) try {
     if (b == nullptr)
         return set_error(GWNB_INVALID_ARGUMENT, "batch: null handle.");
     cudaStream_t const s = as_cuda(stream);
@@ -265,15 +275,19 @@ int gwnb_batch_sync_f32(gwnb_batch *b, gwnb_stream_t stream) {
             return std::string(buf);
         }() + " (index, topology, wait timeout, stack overflow) on at least one mesh.");
     return GWNB_OK;
+} catch (...) {
+    return host_exception();
 }
 
-int gwnb_batch_release_f32(gwnb_batch *b, gwnb_stream_t stream) {
+int gwnb_batch_release_f32(gwnb_batch *b, gwnb_stream_t stream) try {
     if (b == nullptr)
         return GWNB_OK;
     cudaStream_t const s = stream != nullptr ? as_cuda(stream) : b->stream;
     release_batch(b, s);
     delete b;
     return GWNB_OK;
+} catch (...) {
+    return host_exception();
 }
 
 } // extern "C"

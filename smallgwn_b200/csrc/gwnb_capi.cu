@@ -9,6 +9,7 @@
 #include <atomic>
 #include <cmath>
 #include <cstring>
+#include <exception>
 #include <limits>
 #include <mutex>
 #include <new>
@@ -36,6 +37,27 @@ int set_cuda_error(cudaError_t err, char const *what) {
 }
 
 std::atomic<std::uint64_t> g_launch_count{0};
+
+int host_exception() noexcept {
+    char const *what = "Unhandled unknown exception.";
+    std::string detail;
+    try {
+        throw;
+    } catch (std::bad_alloc const &) {
+        what = "Host memory allocation failed.";
+    } catch (std::exception const &e) {
+        try {
+            detail = std::string("Unhandled std::exception: ") + e.what();
+        } catch (...) {
+        }
+    } catch (...) {
+    }
+    try {
+        return set_error(GWNB_INTERNAL_ERROR, detail.empty() ? std::string(what) : detail);
+    } catch (...) {
+        return GWNB_INTERNAL_ERROR;
+    }
+}
 
 std::uint64_t reserve_revision() {
     static std::atomic<std::uint64_t> next{1};
@@ -290,7 +312,7 @@ const char *gwnb_last_error_message(void) { return g_message.c_str(); }
 
 uint64_t gwnb_launch_count(void) { return g_launch_count.load(std::memory_order_relaxed); }
 
-int gwnb_memory_stats(uint64_t *reserved, uint64_t *used) {
+int gwnb_memory_stats(uint64_t *reserved, uint64_t *used) try {
     cudaMemPool_t pool = nullptr;
     GWNB_TRY(library_pool(&pool));
     std::uint64_t r = 0, u = 0;
@@ -301,20 +323,24 @@ int gwnb_memory_stats(uint64_t *reserved, uint64_t *used) {
     if (used != nullptr)
         *used = u;
     return GWNB_OK;
+} catch (...) {
+    return host_exception();
 }
 
-int gwnb_memory_trim(uint64_t keep_bytes) {
+int gwnb_memory_trim(uint64_t keep_bytes) try {
     cudaMemPool_t pool = nullptr;
     GWNB_TRY(library_pool(&pool));
     GWNB_CUDA_TRY(cudaMemPoolTrimTo(pool, static_cast<std::size_t>(keep_bytes)));
     return GWNB_OK;
+} catch (...) {
+    return host_exception();
 }
 int gwnb_last_cuda_error(void) { return g_cuda_error; }
 const char *gwnb_version(void) { return "gwnb 0.1 (sm_100a)"; }
 
 int gwnb_geometry_upload_f32(gwnb_geometry_f32 *out, const float *x, const float *y, const float *z,
                              uint64_t nv, const uint32_t *i0, const uint32_t *i1, const uint32_t *i2,
-                             uint64_t nt, gwnb_stream_t stream) {
+                             uint64_t nt, gwnb_stream_t stream) try {
     if (out == nullptr)
         return set_error(GWNB_INVALID_ARGUMENT, "gwnb_geometry_upload_f32 requires an output view.");
     if (nv > std::numeric_limits<std::uint32_t>::max())
@@ -370,6 +396,8 @@ int gwnb_geometry_upload_f32(gwnb_geometry_f32 *out, const float *x, const float
     }
     *out = g;
     return GWNB_OK;
+} catch (...) {
+    return host_exception();
 }
 
 static int update_common(gwnb_geometry_f32 *g, const float *x, const float *y, const float *z, uint64_t nv,
@@ -390,13 +418,17 @@ static int update_common(gwnb_geometry_f32 *g, const float *x, const float *y, c
 }
 
 int gwnb_geometry_update_f32(gwnb_geometry_f32 *g, const float *x, const float *y, const float *z, uint64_t nv,
-                             gwnb_stream_t stream) {
+                             gwnb_stream_t stream) try {
     return update_common(g, x, y, z, nv, stream, cudaMemcpyDefault);
+} catch (...) {
+    return host_exception();
 }
 
 int gwnb_geometry_update_device_f32(gwnb_geometry_f32 *g, const float *x, const float *y, const float *z,
-                                    uint64_t nv, gwnb_stream_t stream) {
+                                    uint64_t nv, gwnb_stream_t stream) try {
     return update_common(g, x, y, z, nv, stream, cudaMemcpyDeviceToDevice);
+} catch (...) {
+    return host_exception();
 }
 
 void gwnb_geometry_release_f32(gwnb_geometry_f32 *g, gwnb_stream_t stream) {
@@ -405,7 +437,7 @@ void gwnb_geometry_release_f32(gwnb_geometry_f32 *g, gwnb_stream_t stream) {
 }
 
 int gwnb_bvh4_build_f32(const gwnb_geometry_f32 *g, int method, uint32_t radius, int morton_bits,
-                        gwnb_bvh4_f32 *out, gwnb_stream_t stream) {
+                        gwnb_bvh4_f32 *out, gwnb_stream_t stream) try {
     if (out == nullptr)
         return set_error(GWNB_INVALID_ARGUMENT, "bvh.build: output view is null.");
     if (!geometry_valid(g))
@@ -428,6 +460,8 @@ int gwnb_bvh4_build_f32(const gwnb_geometry_f32 *g, int method, uint32_t radius,
         return GWNB_OK;
     }
     return build_impl(g, method, radius, morton_bits, out, as_cuda(stream));
+} catch (...) {
+    return host_exception();
 }
 
 void gwnb_bvh4_release_f32(gwnb_bvh4_f32 *b, gwnb_stream_t stream) {
@@ -436,7 +470,7 @@ void gwnb_bvh4_release_f32(gwnb_bvh4_f32 *b, gwnb_stream_t stream) {
 }
 
 int gwnb_build_preprocess_f32(const gwnb_geometry_f32 *g, int morton_bits, void *sorted_codes, uint32_t *sorted_ids,
-                              gwnb_aabb_f32 *sorted_aabbs, gwnb_stream_t stream) {
+                              gwnb_aabb_f32 *sorted_aabbs, gwnb_stream_t stream) try {
     if (!geometry_valid(g))
         return set_error(GWNB_INVALID_ARGUMENT, "bvh.build.preprocess: geometry is invalid.");
     if (morton_bits != 32 && morton_bits != 64)
@@ -456,11 +490,13 @@ int gwnb_build_preprocess_f32(const gwnb_geometry_f32 *g, int morton_bits, void 
     if (rc == GWNB_OK && host != 0)
         return set_error(GWNB_INTERNAL_ERROR, "bvh.build.preprocess: device sort reported an error.");
     return rc;
+} catch (...) {
+    return host_exception();
 }
 
 int gwnb_build_binary_lbvh(const void *sorted_codes, int morton_bits, uint64_t n, const gwnb_aabb_f32 *sorted_aabbs,
                            gwnb_binary_node *nodes, uint32_t *internal_parent, gwnb_aabb_f32 *internal_bounds,
-                           gwnb_stream_t stream) {
+                           gwnb_stream_t stream) try {
     if (morton_bits != 32 && morton_bits != 64)
         return set_error(GWNB_INVALID_ARGUMENT, "bvh.build.binary.lbvh: morton_bits must be 32 or 64.");
     cudaStream_t const s = as_cuda(stream);
@@ -479,11 +515,13 @@ int gwnb_build_binary_lbvh(const void *sorted_codes, int morton_bits, uint64_t n
     if (rc == GWNB_OK && host != 0)
         return set_error(GWNB_INTERNAL_ERROR, "bvh.build.binary.lbvh: device builder reported an error.");
     return rc;
+} catch (...) {
+    return host_exception();
 }
 
 int gwnb_build_binary_hploc(const void *sorted_codes, int morton_bits, uint64_t n, const gwnb_aabb_f32 *sorted_aabbs,
                             uint32_t radius, gwnb_binary_node *nodes, uint32_t *internal_parent,
-                            gwnb_aabb_f32 *internal_bounds, uint32_t *root, gwnb_stream_t stream) {
+                            gwnb_aabb_f32 *internal_bounds, uint32_t *root, gwnb_stream_t stream) try {
     if (morton_bits != 32 && morton_bits != 64)
         return set_error(GWNB_INVALID_ARGUMENT, "bvh.build.binary.hploc: morton_bits must be 32 or 64.");
     if (radius == 0 || radius > 8)
@@ -499,10 +537,12 @@ int gwnb_build_binary_hploc(const void *sorted_codes, int morton_bits, uint64_t 
                                       reinterpret_cast<aabb *>(internal_bounds), root, s, status);
     release(status, s);
     return rc;
+} catch (...) {
+    return host_exception();
 }
 
 int gwnb_radix_sort_pairs(const void *keys_in, void *keys_out, const uint32_t *values_in, uint32_t *values_out,
-                          uint64_t count, int key_bytes, int key_bits, gwnb_stream_t stream) {
+                          uint64_t count, int key_bytes, int key_bits, gwnb_stream_t stream) try {
     if (count > 0 && (keys_in == nullptr || keys_out == nullptr || values_out == nullptr))
         return set_error(GWNB_INVALID_ARGUMENT, "radix sort: null buffer.");
     cudaStream_t const s = as_cuda(stream);
@@ -519,11 +559,13 @@ int gwnb_radix_sort_pairs(const void *keys_in, void *keys_out, const uint32_t *v
     if (rc == GWNB_OK && host != 0)
         return set_error(GWNB_INTERNAL_ERROR, "radix sort: device look-back timed out.");
     return rc;
+} catch (...) {
+    return host_exception();
 }
 
 // ---- refit --------------------------------------------------------------------------------------
 
-int gwnb_bvh4_refit_async_f32(const gwnb_geometry_f32 *g, gwnb_bvh4_f32 *b, gwnb_stream_t stream) {
+int gwnb_bvh4_refit_async_f32(const gwnb_geometry_f32 *g, gwnb_bvh4_f32 *b, gwnb_stream_t stream) try {
     if (!geometry_valid(g))
         return set_error(GWNB_INVALID_ARGUMENT, "bvh.refit: Geometry accessor is invalid.");
     if (!bvh_valid(b))
@@ -540,9 +582,11 @@ int gwnb_bvh4_refit_async_f32(const gwnb_geometry_f32 *g, gwnb_bvh4_f32 *b, gwnb
     b->revision = next;
     reinterpret_cast<bvh_aux_impl *>(b->aux)->revision = next;
     return GWNB_OK;
+} catch (...) {
+    return host_exception();
 }
 
-int gwnb_bvh4_sync_status_f32(gwnb_bvh4_f32 *b, gwnb_stream_t stream) {
+int gwnb_bvh4_sync_status_f32(gwnb_bvh4_f32 *b, gwnb_stream_t stream) try {
     if (b == nullptr || b->aux == nullptr)
         return set_error(GWNB_INVALID_ARGUMENT, "bvh.status: BVH has no device state.");
     cudaStream_t const s = as_cuda(stream);
@@ -566,11 +610,15 @@ int gwnb_bvh4_sync_status_f32(gwnb_bvh4_f32 *b, gwnb_stream_t stream) {
     }
     std::memcpy(&b->root.bounds, &rb, sizeof(rb));
     return GWNB_OK;
+} catch (...) {
+    return host_exception();
 }
 
-int gwnb_bvh4_refit_f32(const gwnb_geometry_f32 *g, gwnb_bvh4_f32 *b, gwnb_stream_t stream) {
+int gwnb_bvh4_refit_f32(const gwnb_geometry_f32 *g, gwnb_bvh4_f32 *b, gwnb_stream_t stream) try {
     GWNB_TRY(gwnb_bvh4_refit_async_f32(g, b, stream));
     return gwnb_bvh4_sync_status_f32(b, stream);
+} catch (...) {
+    return host_exception();
 }
 
 uint64_t gwnb_moment_node_bytes(int order) {
@@ -597,7 +645,7 @@ static int moment_alloc(gwnb_bvh4_f32 const *b, int order, gwnb_moment4_f32 &m, 
     return GWNB_OK;
 }
 
-int gwnb_moment4_refit_f32(const gwnb_bvh4_f32 *b_in, int order, gwnb_moment4_f32 *out, gwnb_stream_t stream) {
+int gwnb_moment4_refit_f32(const gwnb_bvh4_f32 *b_in, int order, gwnb_moment4_f32 *out, gwnb_stream_t stream) try {
     if (out == nullptr)
         return set_error(GWNB_INVALID_ARGUMENT, "bvh.refit.moment: output view is null.");
     if (order < 0 || order > 2)
@@ -627,9 +675,11 @@ int gwnb_moment4_refit_f32(const gwnb_bvh4_f32 *b_in, int order, gwnb_moment4_f3
     m.bvh_revision = b->revision;
     *out = m;
     return GWNB_OK;
+} catch (...) {
+    return host_exception();
 }
 
-int gwnb_moment4_refit_async_f32(const gwnb_bvh4_f32 *b_in, gwnb_moment4_f32 *m, gwnb_stream_t stream) {
+int gwnb_moment4_refit_async_f32(const gwnb_bvh4_f32 *b_in, gwnb_moment4_f32 *m, gwnb_stream_t stream) try {
     if (m == nullptr || !bvh_valid(b_in))
         return set_error(GWNB_INVALID_ARGUMENT, "bvh.refit.moment: BVH accessor is invalid for moment refit.");
     if (m->node_count != b_in->node_count || (b_in->node_count > 0 && m->aux == nullptr))
@@ -641,6 +691,8 @@ int gwnb_moment4_refit_async_f32(const gwnb_bvh4_f32 *b_in, gwnb_moment4_f32 *m,
         GWNB_TRY(refit_moments_async(b, m, s));
     m->bvh_revision = b->revision;
     return GWNB_OK;
+} catch (...) {
+    return host_exception();
 }
 
 void gwnb_moment4_release_f32(gwnb_moment4_f32 *m, gwnb_stream_t stream) {
@@ -657,7 +709,7 @@ static int check_query_spans(const float *qx, const float *qy, const float *qz, 
 }
 
 int gwnb_winding_exact_batch_f32(const gwnb_bvh4_f32 *b, const float *qx, const float *qy, const float *qz,
-                                 float *out, uint64_t n, int block_size, gwnb_stream_t stream) {
+                                 float *out, uint64_t n, int block_size, gwnb_stream_t stream) try {
     if (!bvh_valid(b))
         return set_error(GWNB_INVALID_ARGUMENT, "BVH object contains no queryable data.");
     if (block_size < 0 || block_size > 1024)
@@ -667,6 +719,8 @@ int gwnb_winding_exact_batch_f32(const gwnb_bvh4_f32 *b, const float *qx, const 
         return GWNB_OK;
     return exact_batch(reinterpret_cast<triangle const *>(b->triangles), b->primitive_count, qx, qy, qz, out, n,
                        as_cuda(stream));
+} catch (...) {
+    return host_exception();
 }
 
 static int taylor_common(const gwnb_bvh4_f32 *b_in, const gwnb_moment4_f32 *m, const float *qx, const float *qy,
@@ -746,41 +800,49 @@ static int taylor_common(const gwnb_bvh4_f32 *b_in, const gwnb_moment4_f32 *m, c
 
 int gwnb_winding_taylor_batch_f32(const gwnb_bvh4_f32 *b, const gwnb_moment4_f32 *m, const float *qx,
                                   const float *qy, const float *qz, float *out, uint64_t n, float beta,
-                                  const gwnb_taylor_options *opt, gwnb_stream_t stream) {
+                                  const gwnb_taylor_options *opt, gwnb_stream_t stream) try {
     return taylor_common(b, m, qx, qy, qz, out, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, n, beta, opt,
                          stream);
+} catch (...) {
+    return host_exception();
 }
 
 int gwnb_winding_gradient_taylor_batch_f32(const gwnb_bvh4_f32 *b, const gwnb_moment4_f32 *m, const float *qx,
                                            const float *qy, const float *qz, float *gx, float *gy, float *gz,
                                            uint64_t n, float beta, const gwnb_taylor_options *opt,
-                                           gwnb_stream_t stream) {
+                                           gwnb_stream_t stream) try {
     if (n > 0 && (gx == nullptr || gy == nullptr || gz == nullptr))
         return set_error(GWNB_INVALID_ARGUMENT, "Query/output spans must use non-null storage when non-empty.");
     return taylor_common(b, m, qx, qy, qz, nullptr, gx, gy, gz, nullptr, nullptr, nullptr, n, beta, opt, stream);
+} catch (...) {
+    return host_exception();
 }
 
 int gwnb_winding_taylor_stats_f32(const gwnb_bvh4_f32 *b, const gwnb_moment4_f32 *m, const float *qx,
                                   const float *qy, const float *qz, uint64_t n, float beta, uint32_t *nodes,
-                                  uint32_t *far_evals, uint32_t *near_tris, gwnb_stream_t stream) {
+                                  uint32_t *far_evals, uint32_t *near_tris, gwnb_stream_t stream) try {
     if (n > 0 && (nodes == nullptr || far_evals == nullptr || near_tris == nullptr))
         return set_error(GWNB_INVALID_ARGUMENT, "Statistics outputs must be non-null.");
     gwnb_taylor_options o{256, 0, 1, GWNB_NEAR_PLAIN, 1.0f / 16.0f};
     return taylor_common(b, m, qx, qy, qz, nullptr, nullptr, nullptr, nullptr, nodes, far_evals, near_tris, n, beta,
                          &o, stream);
+} catch (...) {
+    return host_exception();
 }
 
 int gwnb_winding_exact_geometry_fp64(const gwnb_geometry_f32 *g, const float *qx, const float *qy, const float *qz,
-                                     double *out, uint64_t n, gwnb_stream_t stream) {
+                                     double *out, uint64_t n, gwnb_stream_t stream) try {
     if (!geometry_valid(g))
         return set_error(GWNB_INVALID_ARGUMENT, "Geometry accessor is invalid.");
     if (!has_storage(qx, n) || !has_storage(qy, n) || !has_storage(qz, n) || !has_storage(out, n))
         return set_error(GWNB_INVALID_ARGUMENT, "Query/output spans must use non-null storage when non-empty.");
     return exact_batch_f64(*g, qx, qy, qz, out, n, as_cuda(stream));
+} catch (...) {
+    return host_exception();
 }
 
 int gwnb_query_order_f32(const gwnb_bvh4_f32 *b_in, const float *qx, const float *qy, const float *qz, uint64_t n,
-                         uint32_t *order, gwnb_stream_t stream) {
+                         uint32_t *order, gwnb_stream_t stream) try {
     if (!bvh_valid(b_in))
         return set_error(GWNB_INVALID_ARGUMENT, "BVH object contains no queryable data.");
     if (!has_storage(qx, n) || !has_storage(qy, n) || !has_storage(qz, n) || !has_storage(order, n))
@@ -790,9 +852,11 @@ int gwnb_query_order_f32(const gwnb_bvh4_f32 *b_in, const float *qx, const float
     GWNB_TRY(ensure_bvh_aux(b, s));
     auto *a = reinterpret_cast<bvh_aux_impl *>(b->aux);
     return query_order(a->root_bounds, qx, qy, qz, n, order, s, a->status);
+} catch (...) {
+    return host_exception();
 }
 
-int gwnb_bvh4_fp64_fallback_count(const gwnb_bvh4_f32 *b, uint64_t *count, gwnb_stream_t stream) {
+int gwnb_bvh4_fp64_fallback_count(const gwnb_bvh4_f32 *b, uint64_t *count, gwnb_stream_t stream) try {
     if (b == nullptr || b->aux == nullptr || count == nullptr)
         return set_error(GWNB_INVALID_ARGUMENT, "fp64 counter: BVH has no device state.");
     auto *a = reinterpret_cast<bvh_aux_impl *>(b->aux);
@@ -802,12 +866,14 @@ int gwnb_bvh4_fp64_fallback_count(const gwnb_bvh4_f32 *b, uint64_t *count, gwnb_
     GWNB_CUDA_TRY(cudaStreamSynchronize(s));
     *count = host;
     return GWNB_OK;
+} catch (...) {
+    return host_exception();
 }
 
 int gwnb_winding_taylor_forward_f32(const gwnb_bvh4_f32 *b, const gwnb_moment4_f32 *m, const float *qx,
                                     const float *qy, const float *qz, float *out, uint64_t n, float beta,
                                     const gwnb_taylor_options *opt, gwnb_taylor_saved_f32 *saved,
-                                    gwnb_stream_t stream) {
+                                    gwnb_stream_t stream) try {
     if (saved == nullptr)
         return set_error(GWNB_INVALID_ARGUMENT, "Taylor forward: saved state must be non-null.");
     if (m == nullptr || (m->order != 0 && m->order != 1))
@@ -830,12 +896,14 @@ int gwnb_winding_taylor_forward_f32(const gwnb_bvh4_f32 *b, const gwnb_moment4_f
     saved->bvh_revision = b->revision;
     saved->options = o;
     return GWNB_OK;
+} catch (...) {
+    return host_exception();
 }
 
 int gwnb_winding_taylor_backward_f32(const gwnb_taylor_saved_f32 *saved, const gwnb_geometry_f32 *g,
                                      const gwnb_bvh4_f32 *b_in, const gwnb_moment4_f32 *m, const float *gout,
                                      float *dvx, float *dvy, float *dvz, float *dqx, float *dqy, float *dqz,
-                                     gwnb_stream_t stream) {
+                                     gwnb_stream_t stream) try {
     if (saved == nullptr)
         return set_error(GWNB_INVALID_ARGUMENT, "Taylor backward: saved state must be non-null.");
     if (saved->order != 0 && saved->order != 1)
@@ -905,6 +973,8 @@ int gwnb_winding_taylor_backward_f32(const gwnb_taylor_saved_f32 *saved, const g
     r.sort_queries = saved->options.sort_queries;
     r.status = a->status;
     return taylor_adjoint(r, s);
+} catch (...) {
+    return host_exception();
 }
 
 } // extern "C"

@@ -181,6 +181,10 @@ int set_cuda_error(cudaError_t err, char const *what);
             return gwnb_rc_;                                                                       \
     } while (0)
 
+// The status of a C entry point whose host code threw (std::bad_alloc and the like): no C++
+// exception crosses the C ABI; every `int gwnb_*` entry point is a function-try-block ending in it.
+int host_exception() noexcept;
+
 std::uint64_t reserve_revision();
 int device_sm_count();
 

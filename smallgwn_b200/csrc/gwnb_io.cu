@@ -121,6 +121,11 @@ public:
         return true;
     }
 
+    // Bytes left in the body, and the fewest bytes one value of type t can take (a digit and a
+    // separator in ASCII): counts in the header are checked against them before any allocation.
+    std::size_t remaining() const { return pos_ < d_.size() ? d_.size() - pos_ : 0; }
+    std::size_t min_bytes(ply_type t) const { return fmt_ == ply_format::ascii ? 2 : type_size(t); }
+
 private:
     bool read_ascii(double &out) {
         while (pos_ < d_.size() && std::isspace(static_cast<unsigned char>(d_[pos_])))
@@ -257,10 +262,16 @@ int read_ply(std::string const &path, std::vector<float> &x, std::vector<float> 
                 return ply_fail(path, "vertex element without x, y and z");
             if (e.count > 0xffffffffull)
                 return ply_fail(path, "more vertices than 32-bit indices address");
-            x.reserve(e.count), y.reserve(e.count), z.reserve(e.count);
         }
         if (is_face && !have_vertices)
             return ply_fail(path, "face element before the vertex element");
+        std::size_t record_bytes = 0;
+        for (ply_property const &p : e.props)
+            record_bytes += body.min_bytes(p.list ? p.count_type : p.type);
+        if (record_bytes > 0 && e.count > body.remaining() / record_bytes)
+            return ply_fail(path, "truncated element '" + e.name + "'");
+        if (is_vertex)
+            x.reserve(e.count), y.reserve(e.count), z.reserve(e.count);
         std::vector<double> poly;
         for (std::uint64_t r = 0; r < e.count; ++r) {
             double xyz[3] = {0.0, 0.0, 0.0};
@@ -271,6 +282,8 @@ int read_ply(std::string const &path, std::vector<float> &x, std::vector<float> 
                     if (!body.read(p.count_type, cnt) || cnt < 0.0)
                         return ply_fail(path, "truncated list in element '" + e.name + "'");
                     auto const n = static_cast<std::uint64_t>(cnt);
+                    if (n > body.remaining() / std::max<std::size_t>(1, body.min_bytes(p.type)))
+                        return ply_fail(path, "truncated list in element '" + e.name + "'");
                     bool const keep = is_face && static_cast<int>(k) == iface;
                     if (keep)
                         poly.assign(n, 0.0);
@@ -407,7 +420,7 @@ using namespace gwnb;
 
 extern "C" {
 
-int gwnb_mesh_read_ply(const char *path, gwnb_host_mesh_f32 *out) {
+int gwnb_mesh_read_ply(const char *path, gwnb_host_mesh_f32 *out) try {
     if (path == nullptr || out == nullptr)
         return set_error(GWNB_INVALID_ARGUMENT, "ply: null path or output.");
     std::vector<float> x, y, z;
@@ -428,6 +441,8 @@ int gwnb_mesh_read_ply(const char *path, gwnb_host_mesh_f32 *out) {
     }
     *out = m;
     return GWNB_OK;
+} catch (...) {
+    return host_exception();
 }
 
 void gwnb_host_mesh_free(gwnb_host_mesh_f32 *m) {
@@ -442,7 +457,7 @@ void gwnb_host_mesh_free(gwnb_host_mesh_f32 *m) {
     *m = gwnb_host_mesh_f32{};
 }
 
-int gwnb_mesh_write_ply(const char *path, const gwnb_host_mesh_f32 *m, int binary) {
+int gwnb_mesh_write_ply(const char *path, const gwnb_host_mesh_f32 *m, int binary) try {
     if (path == nullptr || m == nullptr)
         return set_error(GWNB_INVALID_ARGUMENT, "ply: null path or mesh.");
     if (!has_storage(m->x, m->vertex_count) || !has_storage(m->y, m->vertex_count) ||
@@ -478,10 +493,12 @@ int gwnb_mesh_write_ply(const char *path, const gwnb_host_mesh_f32 *m, int binar
     if (!o)
         return set_error(GWNB_INTERNAL_ERROR, std::string("ply: write failed for ") + path);
     return GWNB_OK;
+} catch (...) {
+    return host_exception();
 }
 
 int gwnb_scene_save_f32(const char *path, const gwnb_geometry_f32 *g, const gwnb_bvh4_f32 *b,
-                        const gwnb_moment4_f32 *const *moments, int moment_count, gwnb_stream_t stream) {
+                        const gwnb_moment4_f32 *const *moments, int moment_count, gwnb_stream_t stream) try {
     if (path == nullptr)
         return set_error(GWNB_INVALID_ARGUMENT, "scene: null path.");
     if (!geometry_valid(g) || g->triangle_count == 0)
@@ -548,10 +565,12 @@ int gwnb_scene_save_f32(const char *path, const gwnb_geometry_f32 *g, const gwnb
     if (!out)
         return set_error(GWNB_INTERNAL_ERROR, std::string("scene: write failed for ") + path);
     return GWNB_OK;
+} catch (...) {
+    return host_exception();
 }
 
 int gwnb_scene_load_f32(const char *path, gwnb_geometry_f32 *g_out, gwnb_bvh4_f32 *b_out, gwnb_moment4_f32 *m_out,
-                        int *moment_mask, gwnb_stream_t stream) {
+                        int *moment_mask, gwnb_stream_t stream) try {
     if (path == nullptr || g_out == nullptr || b_out == nullptr || m_out == nullptr)
         return set_error(GWNB_INVALID_ARGUMENT, "scene: null path or output.");
     std::ifstream in(path, std::ios::binary);
@@ -664,6 +683,8 @@ int gwnb_scene_load_f32(const char *path, gwnb_geometry_f32 *g_out, gwnb_bvh4_f3
     if (moment_mask != nullptr)
         *moment_mask = static_cast<int>(h.moment_mask);
     return GWNB_OK;
+} catch (...) {
+    return host_exception();
 }
 
 } // extern "C"

@@ -68,7 +68,7 @@ using namespace gwnb;
 extern "C" int gwnb_winding_taylor_batch_noalloc_f32(const gwnb_bvh4_f32 *b, const gwnb_moment4_f32 *m,
                                                      const float *qx, const float *qy, const float *qz,
                                                      float *out, uint64_t n, float beta,
-                                                     const gwnb_taylor_options *opt, gwnb_stream_t stream) {
+                                                     const gwnb_taylor_options *opt, gwnb_stream_t stream) try {
     if (radix_sort_u32_scratch_words(k_capacity, 30) > k_sort_words)
         return set_error(GWNB_INTERNAL_ERROR, "no-allocation Taylor batch: scratch layout mismatch.");
     if (n > k_capacity)
@@ -146,4 +146,6 @@ extern "C" int gwnb_winding_taylor_batch_noalloc_f32(const gwnb_bvh4_f32 *b, con
     if (o.near_precision == GWNB_NEAR_COMPENSATED)
         GWNB_CUDA_TRY(cudaMemsetAsync(a->fp64_count, 0, sizeof(unsigned long long), s));
     return taylor_batch_in_scratch(r, scratch, k_capacity, s);
+} catch (...) {
+    return host_exception();
 }

@@ -745,7 +745,7 @@ extern "C" {
 
 int gwnb_unsigned_distance_batch_f32(const gwnb_bvh4_f32 *b, const float *qx, const float *qy, const float *qz,
                                      float *out, uint64_t n, float culling_band, const gwnb_spatial_options *opt,
-                                     gwnb_stream_t stream) {
+                                     gwnb_stream_t stream) try {
     if (!bvh_valid(b))
         return set_error(GWNB_INVALID_ARGUMENT, "BVH object contains no queryable data.");
     gwnb_spatial_options o;
@@ -766,11 +766,13 @@ int gwnb_unsigned_distance_batch_f32(const gwnb_bvh4_f32 *b, const float *qx, co
     r.culling_band = culling_band;
     r.opt = o;
     return spatial_batch(const_cast<gwnb_bvh4_f32 *>(b), r, as_cuda(stream));
+} catch (...) {
+    return host_exception();
 }
 
 int gwnb_ray_first_hit_batch_f32(const gwnb_bvh4_f32 *b, const float *ox, const float *oy, const float *oz,
                                  const float *dx, const float *dy, const float *dz, gwnb_ray_hit_f32 *out, uint64_t n,
-                                 float t_min, float t_max, const gwnb_spatial_options *opt, gwnb_stream_t stream) {
+                                 float t_min, float t_max, const gwnb_spatial_options *opt, gwnb_stream_t stream) try {
     if (!bvh_valid(b))
         return set_error(GWNB_INVALID_ARGUMENT, "BVH object contains no queryable data.");
     gwnb_spatial_options o;
@@ -799,12 +801,14 @@ int gwnb_ray_first_hit_batch_f32(const gwnb_bvh4_f32 *b, const float *ox, const 
     r.t_max = t_max;
     r.opt = o;
     return spatial_batch(const_cast<gwnb_bvh4_f32 *>(b), r, as_cuda(stream));
+} catch (...) {
+    return host_exception();
 }
 
 int gwnb_spatial_stats_f32(const gwnb_bvh4_f32 *b, int kind, const float *qx, const float *qy, const float *qz,
                            const float *dx, const float *dy, const float *dz, uint64_t n, float culling_band,
                            float t_min, float t_max, uint32_t *nodes_entered, uint32_t *triangles_tested,
-                           gwnb_stream_t stream) {
+                           gwnb_stream_t stream) try {
     if (!bvh_valid(b))
         return set_error(GWNB_INVALID_ARGUMENT, "BVH object contains no queryable data.");
     if (kind != GWNB_SPATIAL_DISTANCE && kind != GWNB_SPATIAL_RAY)
@@ -853,11 +857,13 @@ int gwnb_spatial_stats_f32(const gwnb_bvh4_f32 *b, int kind, const float *qx, co
     release(hits, s);
     release(dist, s);
     return rc;
+} catch (...) {
+    return host_exception();
 }
 
 int gwnb_ray_order_f32(const gwnb_bvh4_f32 *b_in, const float *ox, const float *oy, const float *oz,
                        const float *dx, const float *dy, const float *dz, uint64_t n, uint32_t *order,
-                       gwnb_stream_t stream) {
+                       gwnb_stream_t stream) try {
     if (!bvh_valid(b_in))
         return set_error(GWNB_INVALID_ARGUMENT, "BVH object contains no queryable data.");
     if (!has_storage(ox, n) || !has_storage(oy, n) || !has_storage(oz, n) || !has_storage(dx, n) ||
@@ -869,6 +875,8 @@ int gwnb_ray_order_f32(const gwnb_bvh4_f32 *b_in, const float *ox, const float *
     auto *b = const_cast<gwnb_bvh4_f32 *>(b_in);
     GWNB_TRY(ensure_bvh_aux(b, s));
     return ray_order(reinterpret_cast<bvh_aux_impl const *>(b->aux), ox, oy, oz, dx, dy, dz, n, order, s);
+} catch (...) {
+    return host_exception();
 }
 
 } // extern "C"

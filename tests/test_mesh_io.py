@@ -210,3 +210,22 @@ def test_scene_load_refuses_malformed_trees_on_host(tmp_path, nodes_refs, prims,
     rc = lib.gwnb_scene_load_f32(str(p).encode(), C.byref(g), C.byref(b), ms, C.byref(mask), None)
     assert rc == _lib.GWNB_INVALID_ARGUMENT, why
     assert "not a valid BVH4 tree" in _lib.last_error(), (why, _lib.last_error())
+
+
+@pytest.mark.parametrize("header_count, body", [
+    ("element vertex 4000000000", "0 0 0\n"),                       # vertex count far beyond the body
+    ("element vertex 3", "0 0 0\n1 0 0\n0 1 0\n4000000000 0 1 2\n"),  # list length far beyond the body
+])
+def test_refuses_counts_the_body_cannot_hold(tmp_path, header_count, body):
+    """Counts in the header are checked against the bytes left before anything is allocated."""
+    head = ("ply\nformat ascii 1.0\n" + header_count + "\nproperty float x\nproperty float y\nproperty float z\n"
+            "element face 1\nproperty list uint int vertex_indices\nend_header\n")
+    p = tmp_path / "huge.ply"
+    p.write_text(head + body)
+    with pytest.raises(ValueError, match="truncated"):
+        api.read_ply(p)
+    binary = tmp_path / "huge_bin.ply"
+    binary.write_bytes(("ply\nformat binary_little_endian 1.0\nelement vertex 4000000000\nproperty float x\n"
+                        "property float y\nproperty float z\nend_header\n").encode() + bytes(24))
+    with pytest.raises(ValueError, match="truncated"):
+        api.read_ply(binary)
