@@ -235,10 +235,10 @@ __global__ void __launch_bounds__(k_block)
             return;
         }
         pending[2 * static_cast<std::uint64_t>(p) + slot] = cur;
-        __threadfence();
+        fence_acq_rel_gpu();
         if (atomicAdd(&arrivals[p], 1u) == 0u)
             return;
-        __threadfence();
+        fence_acq_rel_gpu();
         aabb l, r;
         {
             float const *pl = reinterpret_cast<float const *>(&pending[2 * static_cast<std::uint64_t>(p)]);

@@ -202,7 +202,6 @@ template <class K> __global__ void __launch_bounds__(k_hploc_block) k_hploc(hplo
         }
         if (lane < nl + nr)
             p.cluster_indices[l + lane] = cid;
-        __threadfence();
     };
 
     std::uint32_t left = static_cast<std::uint32_t>(gidx < n ? gidx : 0);
@@ -216,14 +215,14 @@ template <class K> __global__ void __launch_bounds__(k_hploc_block) k_hploc(hplo
             if (parent_is_right(left, right)) {
                 prev = atomicExch(&p.boundary_parent[right], left);
                 if (prev != k_inv) {
-                    __threadfence();
+                    fence_acq_rel_gpu();
                     split = right + 1;
                     right = prev;
                 }
             } else {
                 prev = atomicExch(&p.boundary_parent[left - 1], right);
                 if (prev != k_inv) {
-                    __threadfence();
+                    fence_acq_rel_gpu();
                     split = left;
                     left = prev;
                 }
@@ -231,14 +230,22 @@ template <class K> __global__ void __launch_bounds__(k_hploc_block) k_hploc(hplo
             if (prev == k_inv)
                 active = false;
         }
+        // a lane that acquired its sibling's range above orders the whole warp's reads of it
+        __syncwarp();
         std::uint32_t const size = right - left + 1u;
         bool const fin = active && size == n;
         unsigned mask = __ballot_sync(0xffffffffu, (active && size > k_threshold) || fin);
+        bool const merged_any = mask != 0u;
         while (mask != 0u) {
             int const sel = __ffs(static_cast<int>(mask)) - 1;
             ploc(sel, left, right, split, fin);
             mask &= mask - 1u;
         }
+        // one release for every range this warp rewrote, before its next boundary exchange: the
+        // lanes that wrote a range's list are ordered before its owner lane by the warp barrier
+        __syncwarp();
+        if (merged_any)
+            fence_acq_rel_gpu();
         if (++outer_guard > 4096) {
             atomicOr(p.status, k_err_hploc);
             break;

@@ -193,6 +193,13 @@ int device_sm_count();
 extern std::atomic<std::uint64_t> g_launch_count;
 inline void note_launch() { g_launch_count.fetch_add(1, std::memory_order_relaxed); }
 
+// Release / acquire fence at GPU scope (PTX fence.acq_rel.gpu). The bottom-up kernels publish a
+// node's data with plain stores, this fence, then a relaxed atomic on the node's counter; the
+// thread that reads the counter's final value runs this fence before reading the data -- the
+// fence-based release/acquire pattern of the PTX memory model. It is cheaper than the sequentially
+// consistent __threadfence (fence.sc.gpu), which these patterns do not need.
+__device__ __forceinline__ void fence_acq_rel_gpu() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
+
 // ---- allocation (stream ordered) ---------------------------------------------------------------
 // Every device allocation of the library comes from one memory pool per device that keeps freed
 // memory mapped (release threshold at its maximum). With the default pool's threshold of zero,

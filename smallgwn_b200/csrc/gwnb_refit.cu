@@ -161,7 +161,7 @@ __device__ __forceinline__ void refit_bounds_item(refit_params const &p, std::ui
     // Climb: the last arrival at a node unions its children and continues to the parent.
     std::uint64_t guard = 0;
     for (;;) {
-        __threadfence();
+        fence_acq_rel_gpu();
         std::uint32_t const arrived = atomicAdd(&p.arrivals[cur], 1u) + 1u;
         std::uint32_t const expect = p.expected[cur];
         if (arrived < expect)
@@ -171,7 +171,7 @@ __device__ __forceinline__ void refit_bounds_item(refit_params const &p, std::ui
             return;
         }
         p.arrivals[cur] = 0u;
-        __threadfence();
+        fence_acq_rel_gpu();
         aabb u{0, 0, 0, 0, 0, 0};
         bool init = false;
 #pragma unroll
@@ -636,7 +636,7 @@ template <int Order> __device__ __forceinline__ void refit_moments_item(moment_p
     std::uint32_t cur = p.leaf_nodes[t];
     std::uint64_t guard = 0;
     for (;;) {
-        __threadfence();
+        fence_acq_rel_gpu();
         std::uint32_t const arrived = atomicAdd(&p.arrivals[cur], 1u) + 1u;
         std::uint32_t const expect = p.expected[cur];
         if (arrived < expect)
@@ -646,7 +646,7 @@ template <int Order> __device__ __forceinline__ void refit_moments_item(moment_p
             return;
         }
         p.arrivals[cur] = 0u;
-        __threadfence();
+        fence_acq_rel_gpu();
         finish_node<Order>(p, cur);
         std::uint32_t const ps = p.parent_slot[cur];
         if (ps == k_invalid_u32)
