@@ -48,25 +48,31 @@ def icosphere(level: int) -> tuple[np.ndarray, np.ndarray]:
     return np.array(verts), np.array(faces, dtype=np.int64)
 
 
+def displaced_radius(theta, phi, seed: int) -> np.ndarray:
+    """r(theta, phi) = 1 + 0.1 sum_k a_k sin(m_k theta + p_k) cos(n_k phi + q_k), k = 1..8, with
+    a_k ~ U(0, 1) / k, integer m_k, n_k in [1, 12] and phases ~ U[0, 2 pi), all drawn from seed."""
+    rng = np.random.default_rng(seed)
+    k = np.arange(1, 9)
+    a = rng.uniform(0.0, 1.0, 8) / k
+    m = rng.integers(1, 13, 8)
+    n = rng.integers(1, 13, 8)
+    p = rng.uniform(0.0, 2.0 * np.pi, 8)
+    q = rng.uniform(0.0, 2.0 * np.pi, 8)
+    theta = np.asarray(theta, dtype=np.float64)
+    phi = np.asarray(phi, dtype=np.float64)
+    s = np.zeros(np.broadcast(theta, phi).shape)
+    for i in range(8):
+        s += a[i] * np.sin(m[i] * theta + p[i]) * np.cos(n[i] * phi + q[i])
+    return 1.0 + 0.1 * s
+
+
 def uv_sphere(n_phi: int, n_theta: int, seed: int, displaced: bool = True) -> tuple[np.ndarray, np.ndarray]:
     """Displaced UV sphere: n_theta rings from pole to pole (poles included), n_phi vertices per
     ring, wrapped in phi; 2 * n_phi * (n_theta - 1) outward-oriented triangles."""
-    rng = np.random.default_rng(seed)
     theta = np.linspace(0.0, np.pi, n_theta)
     phi = np.arange(n_phi) * (2.0 * np.pi / n_phi)
     th, ph = np.meshgrid(theta, phi, indexing="ij")  # [n_theta, n_phi]
-    r = np.ones_like(th)
-    if displaced:
-        k = np.arange(1, 9)
-        a = rng.uniform(0.0, 1.0, 8) / k
-        m = rng.integers(1, 13, 8)
-        n = rng.integers(1, 13, 8)
-        p = rng.uniform(0.0, 2.0 * np.pi, 8)
-        q = rng.uniform(0.0, 2.0 * np.pi, 8)
-        s = np.zeros_like(th)
-        for i in range(8):
-            s += a[i] * np.sin(m[i] * th + p[i]) * np.cos(n[i] * ph + q[i])
-        r = 1.0 + 0.1 * s
+    r = displaced_radius(th, ph, seed) if displaced else np.ones_like(th)
     V = np.stack([r * np.sin(th) * np.cos(ph), r * np.sin(th) * np.sin(ph), r * np.cos(th)], axis=-1).reshape(-1, 3)
     j = np.arange(n_theta - 1)[:, None]
     i = np.arange(n_phi)[None, :]
