@@ -1395,6 +1395,9 @@ def main() -> None:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     total_ms = float(t.item())
     value = world * n * args.steps / (total_ms / 1e3)
+    from smallgwn_b200 import sharding
+
+    timed_launches = int(sharding.sum_over_ranks([timed_launches])[0])  # the whole job's launches
 
     # ---- end to end through the public API with host buffers (pinned), same step definition ----
     hq = [torch.from_numpy(v).pin_memory() for v in q]

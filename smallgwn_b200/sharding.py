@@ -98,3 +98,17 @@ def max_over_ranks(values, group=None) -> list[float]:
     t = torch.tensor(vals, dtype=torch.float64, device=_device_for(group))
     dist.all_reduce(t, op=dist.ReduceOp.MAX, group=group)
     return [float(x) for x in t.cpu().tolist()]
+
+
+def sum_over_ranks(values, group=None) -> list[float]:
+    """Element-wise sum of a list of floats over the ranks of `group` (whole-job counts).
+    Identity without an initialised process group."""
+    import torch
+    import torch.distributed as dist
+
+    vals = [float(v) for v in values]
+    if not dist.is_initialized() or dist.get_world_size(group) == 1:
+        return vals
+    t = torch.tensor(vals, dtype=torch.float64, device=_device_for(group))
+    dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
+    return [float(x) for x in t.cpu().tolist()]

@@ -69,6 +69,7 @@ def test_single_process_helpers_are_identities():
     sharding.allreduce_sum_([t])
     assert t.tolist() == list(range(6))
     assert sharding.max_over_ranks([1.5, 2.0]) == [1.5, 2.0]
+    assert sharding.sum_over_ranks([3.0]) == [3.0]
 
 
 # ---- world size 2 over gloo -------------------------------------------------------------------------
@@ -124,6 +125,8 @@ def _worker(rank: int, world: int, port: int, out_dir: str) -> None:
         # the job's time is its slowest rank's
         mx = sharding.max_over_ranks([10.0 + rank, 5.0 - rank])
         assert mx == [10.0 + world - 1, 5.0]
+        # and its launch count is every rank's
+        assert sharding.sum_over_ranks([7.0, float(rank)]) == [7.0 * world, float(sum(range(world)))]
         with open(os.path.join(out_dir, f"ok{rank}"), "w") as f:
             f.write("ok")
     finally:
