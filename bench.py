@@ -302,23 +302,14 @@ def run_reference_arm(args) -> None:
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    import torch
-
     import oracle
-    import smallgwn_b200 as g
-    from smallgwn_b200 import api
 
     mesh, q = make_workload(0, args.queries)
-    # The BVH and moments the CPU traverses are the same ones the GPU path uses.
-    geo = g.gwn_geometry_object()
-    assert g.gwn_upload_geometry(geo, mesh["x"], mesh["y"], mesh["z"], mesh["i0"], mesh["i1"], mesh["i2"]).is_ok()
-    bvh = g.gwn_bvh4_object()
-    assert g.gwn_build_bvh(geo, bvh, g.gwn_bvh_build_options(method=0, hploc_search_radius=8)).is_ok()
-    mom = g.gwn_bvh4_moment_object(args.order)
-    assert g.gwn_refit_bvh_moment(args.order, bvh, mom).is_ok()
-    bh = api.bvh_host_arrays(bvh)
-    mh = api.moment_host_array(mom)
-    torch.cuda.synchronize()
+    # Everything on the host: the oracle's H-PLOC build (radius 8) and moments of the same mesh,
+    # then its Taylor traversal; no kernel of this library runs in this arm.
+    bh = oracle.build_bvh(mesh, "hploc", radius=8)
+    bh["root_reference"] = int(bh["root_reference"])
+    mh = oracle.moments(args.order, bh["nodes"], bh["triangles"])
     threads = oracle.max_threads()
     sample = 40_000
     rng = np.random.default_rng(0)
@@ -986,6 +977,11 @@ def run_exact_workload(args) -> None:
     def run():
         assert g.gwn_compute_winding_number_exact_batch(bvh, *dq, out, stream).is_ok()
 
+    props = torch.cuda.get_device_properties(torch.cuda.current_device())
+    max_mhz = 1965.0
+    if (ROOT / "MEASURED_PEAKS.json").exists():
+        max_mhz = float(json.loads((ROOT / "MEASURED_PEAKS.json").read_text()).get("sm_max_mhz", max_mhz))
+    fp32_peak = props.multi_processor_count * 128 * 2 * max_mhz * 1e6 / 1e12
     exact_launches: list[int] = []
     t = timed_steps(run, args.steps, args.warmup, stream, flush, exact_launches)
     ms = float(np.mean(t))
@@ -1006,6 +1002,12 @@ def run_exact_workload(args) -> None:
                    "max_abs_diff_vs_oracle_fp32": err},
         "cpu_baseline": {"value": m * nt / cpu_s, "unit": "evaluations/s", "cores": threads, "kind": "port",
                          "sample": f"{m} of the queries against all triangles"},
+        # FP32 CUDA-core roofline: 70 FP32 add/mul per evaluation (plus 3 sqrt, 1 atan2 on the
+        # SFU, not counted); no FP32 peak is measured, so the nominal one of the device is used
+        "roofline": {"bound": "fp32", "achieved": nq * nt * 70 / (ms / 1e3) / 1e12, "peak": fp32_peak,
+                     "unit": "TFLOP/s", "frac": nq * nt * 70 / (ms / 1e3) / 1e12 / fp32_peak,
+                     "peak_source": "nominal: SMs x 128 FP32 lanes x 2 FLOP x max SM clock",
+                     "traffic": None, "kernel": "k_exact", "bytes_model": "70 FLOP per (query, triangle)"},
         "gpu_launches": exact_launches[0],
     }
     print(json.dumps(line), flush=True)
