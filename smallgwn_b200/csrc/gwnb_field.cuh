@@ -100,11 +100,14 @@ __device__ __forceinline__ float solid_angle_guarded(float ax, float ay, float a
                                                      float nx, float ny, float nz) {
     float const bx = ax + e1x, by = ay + e1y, bz = az + e1z;
     float const cx = ax + e2x, cy = ay + e2y, cz = az + e2z;
-    float const la = sqrtf(ax * ax + ay * ay + az * az);
-    float const lb = sqrtf(bx * bx + by * by + bz * bz);
-    float const lc = sqrtf(cx * cx + cy * cy + cz * cz);
-    if (la == 0.0f || lb == 0.0f || lc == 0.0f)
+    float const a2 = ax * ax + ay * ay + az * az;
+    float const b2 = bx * bx + by * by + bz * bz;
+    float const c2 = cx * cx + cy * cy + cz * cz;
+    if (a2 == 0.0f || b2 == 0.0f || c2 == 0.0f)
         return 0.0f;
+    // lengths as x * rsqrt(x) (within 2 ulp of the rounded square root): the brute-force batch
+    // evaluates every pair, and the pairs it cannot take in float go to the FP64 branch below
+    float const la = a2 * rsqrtf(a2), lb = b2 * rsqrtf(b2), lc = c2 * rsqrtf(c2);
     float const num = ax * nx + ay * ny + az * nz;
     float const labc = la * lb * lc;
     float const den = labc + (ax * bx + ay * by + az * bz) * lc + (ax * cx + ay * cy + az * cz) * lb +
