@@ -208,4 +208,20 @@ template <class Real, class Index> inline constexpr bool k_supported = std::is_s
 }
 
 } // namespace detail
+
+/// Device memory the library's pool holds from the driver and the part of it in live allocations
+/// (current device). No smallgwn counterpart: its allocations use the CUDA defaults.
+[[nodiscard]] inline gwn_status gwn_memory_stats(std::uint64_t &reserved_bytes, std::uint64_t &used_bytes) noexcept {
+    return detail::gwnb_to_status(gwnb_memory_stats(&reserved_bytes, &used_bytes));
+}
+
+/// Returns the pool's cached device memory to the driver down to keep_bytes (or what is in use).
+[[nodiscard]] inline gwn_status gwn_memory_trim(std::uint64_t const keep_bytes = 0) noexcept {
+    return detail::gwnb_to_status(gwnb_memory_trim(keep_bytes));
+}
+
+/// Kernel launches the library has issued in this process (a launch recorded into a CUDA graph
+/// counts once, when captured).
+[[nodiscard]] inline std::uint64_t gwn_launch_count() noexcept { return gwnb_launch_count(); }
+
 } // namespace gwn

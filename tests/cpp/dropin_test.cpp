@@ -450,6 +450,14 @@ int main(int argc, char **argv) {
     distance_and_ray_on_layers();
     open_cube_boundary_and_antipodal();
     eigen_upload_and_scene_files();
+    {
+        std::uint64_t const before = gwn::gwn_launch_count();
+        leaf_root_build();
+        CHECK(gwn::gwn_launch_count() > before);
+        std::uint64_t reserved = 0, used = 0;
+        CHECK(gwn::gwn_memory_stats(reserved, used).is_ok() && reserved >= used);
+        CHECK(gwn::gwn_memory_trim().is_ok());
+    }
     if (g_failures == 0)
         std::printf("dropin_test: all checks passed\n");
     return g_failures == 0 ? 0 : 1;
