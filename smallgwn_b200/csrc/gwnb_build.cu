@@ -583,7 +583,7 @@ int build_binary_hploc(void const *sorted_codes, int morton_bits, std::uint64_t 
                        cudaStream_t s, unsigned int *status);
 
 // Collapse a binary hierarchy into canonical breadth-first BVH4 nodes. Synchronizes after the
-// first 24 levels and then every 8 to learn when the tree is exhausted (one synchronization for
+// first 24 levels and then every 8 to learn when the tree is exhausted (one synchronization for the
 // tree of the 1M-triangle sphere instead of three: 1.46 -> 1.43 ms per build).
 int collapse_to_bvh4(binary_node const *binary, aabb const *binary_bounds, aabb const *leaf_aabbs,
                      std::uint64_t leaf_count, std::uint32_t root_binary, node4 *nodes,
