@@ -257,18 +257,65 @@ def peaks() -> dict:
     return {"hbm_gbs": 6650.0, "source": "fallback"}
 
 
-def profiled_traffic(order: int, beta: float, n: int) -> float | None:
-    """DRAM bytes (read + write) of one traversal launch over this workload, from the committed
-    ncu summary of the same launch (profiles/taylor_warp_o{order}_sphere1m.md); None when no
-    capture of this exact configuration is recorded."""
+def profiled_metric(name: str, order: int, beta: float, n: int) -> float | None:
+    """A per-launch ncu figure of the traversal over this exact workload (`dram_bytes_per_launch`:
+    DRAM read + write bytes; `l2_hit_rate_pct`: lts__t_sector_hit_rate), from the committed ncu
+    summary of the same launch (profiles/taylor_warp_o{order}_sphere1m.md); None when no capture of
+    this configuration is recorded there."""
     path = ROOT / "profiles" / f"taylor_warp_o{order}_sphere1m.md"
     if not path.exists():
         return None
-    key = f"dram_bytes_per_launch[order={order},beta={beta:g},queries={n}]:"
+    key = f"{name}[order={order},beta={beta:g},queries={n}]:"
     for line in path.read_text().splitlines():
         if line.startswith(key):
             return float(line.split(":", 1)[1].split()[0])
     return None
+
+
+# FP32 operations (add, multiply; a fused multiply-add counts 2) per unit of traversal work, counted
+# from the source of csrc/gwnb_field.cuh and csrc/gwnb_query.cu; square roots, reciprocal square
+# roots, atan2 and FP64 work are not counted.
+#   child test: r = q - P (3), |r|^2 (1 mul + 2 fma = 5), r^2 beta^2 (1)
+#   far field, value only: 1/|r| powers and r^ (5), r^.N (5), -(r^.N)/|r|^2 (1); order 1 adds the
+#     quadratic form (4 squares + 12) and its scaling (2); order 2 the cubic form (22) and its
+#     scaling (2)
+#   near-field triangle: b, c (6), three squared lengths (15), the numerator (plain 5; compensated
+#     Dot2 26), a.b, a.c, b.c (15), the denominator (plain 8; compensated |a||b||c| 2 + Dot2 26 + 1
+#     and the two FP64-flag thresholds 2), 2 atan2 (1)
+FLOP_CHILD_TEST = 9
+FLOP_FAR = {0: 11, 1: 11 + 18, 2: 11 + 18 + 24}
+FLOP_NEAR = {"plain": 50, "compensated": 94}
+
+
+def traversal_flops(order: int, compensated: bool, tests: float, far: float, near: float) -> float:
+    return (tests * FLOP_CHILD_TEST + far * FLOP_FAR[order] +
+            near * FLOP_NEAR["compensated" if compensated else "plain"])
+
+
+def smallgwn_taylor_points(mesh, q, sub, ref64, points, iters: int = 3):
+    """smallgwn's own Taylor batch (gwn_compute_winding_number_taylor_batch<Order>, compiled for
+    sm_100a into oracle/_ref) on the same mesh and queries, over its own H-PLOC (radius 8) BVH4 and
+    moments: mean device ms per 10M-query batch with the L2 flushed before each, queries/s, and max /
+    p99 error against FP64 on the error subset. A baseline beside the headline, not part of `value`;
+    None when oracle/_ref was not built."""
+    import oracle
+
+    if oracle.ref_lib() is None:
+        return None
+    R = oracle.Reference(mesh)
+    out = {}
+    try:
+        R.build(0, 8, 64)
+        for order, beta in points:
+            R.refit_moments(order)
+            ms = R.time_taylor(order, *q, beta=beta, warmup=1, iters=iters)
+            w = R.taylor(order, *[v[sub] for v in q], beta=beta).astype(np.float64)
+            e = np.abs(w - ref64)
+            out[(order, beta)] = {"ms_per_batch": ms, "queries_per_s": q[0].size / (ms / 1e3),
+                                  "max_err_vs_fp64": float(e.max()), "p99_err_vs_fp64": float(np.quantile(e, 0.99))}
+    finally:
+        R.close()
+    return out
 
 
 def make_workload(rank: int, n_queries: int):
@@ -1469,11 +1516,17 @@ def main() -> None:
     assert api.taylor_traversal_stats(bvh, mom, *dq, *stats, accuracy_scale=args.beta, stream=stream).is_ok()
     torch.cuda.synchronize()
     nodes_entered = float(stats[0].double().sum().item())
+    far_accepted = float(stats[1].double().sum().item())
     near_tris = float(stats[2].double().sum().item())
-    alg_bytes = n * 16 + nodes_entered * (128 + MOMENT_BYTES[args.order]) + near_tris * 36
+    host_nodes = api.bvh_host_arrays(bvh)["nodes"]
+    slots_per_node = float((((host_nodes["reference"] >> 47) & 1) != 0).sum(axis=1).mean())
+    flops = traversal_flops(args.order, True, nodes_entered * slots_per_node, far_accepted, near_tris)
+    fp32_peak, _ = api.fp32_fma_peak(stream=stream)
+    achieved = flops / (kernel_ms / 1e3) / 1e12
+    touched_bytes = n * 16 + nodes_entered * (128 + MOMENT_BYTES[args.order]) + near_tris * 36
     pk = peaks()
-    achieved = alg_bytes / (kernel_ms / 1e3) / 1e9
-    traffic = profiled_traffic(args.order, args.beta, n)
+    traffic = profiled_metric("dram_bytes_per_launch", args.order, args.beta, n)
+    l2_hit = profiled_metric("l2_hit_rate_pct", args.order, args.beta, n)
 
     # ---- accuracy against FP64 on a 100k subset (untimed) ----
     sub = slice(0, min(ERROR_SUBSET, n))
@@ -1481,11 +1534,37 @@ def main() -> None:
     assert api.exact_winding_fp64(geo, *[d[sub] for d in dq], ref64, stream).is_ok()
     batch(dq, out)
     torch.cuda.synchronize()
-    err = (out[sub].double() - ref64).abs().cpu().numpy()
+    ref64_h = ref64.cpu().numpy()
+    err = np.abs(out[sub].double().cpu().numpy() - ref64_h)
     plain_out = torch.empty_like(out)
     plain_batch(dq, plain_out)
     torch.cuda.synchronize()
-    perr = (plain_out[sub].double() - ref64).abs().cpu().numpy()
+    perr = np.abs(plain_out[sub].double().cpu().numpy() - ref64_h)
+
+    # ---- the Taylor-at-scale points as configured (orders 1 and 2 at accuracy scale 2) beside the
+    # chosen scale, ours (chosen form) and smallgwn's own kernels on the same B200 (untimed for value)
+    points = [(1, 2.0), (2, 2.0), (args.order, args.beta)]
+    ours_points = {}
+    moms = {args.order: mom}
+    for o, b in points:
+        if o not in moms:
+            moms[o] = g.gwn_bvh4_moment_object(o)
+            assert g.gwn_refit_bvh_moment(o, bvh, moms[o], stream).is_ok()
+
+        def point_batch(o=o, b=b):
+            st = g.gwn_compute_winding_number_taylor_batch(o, bvh, moms[o], *dq, out, accuracy_scale=b, stream=stream,
+                                                           precision=g.near_precision.compensated)
+            assert st.is_ok(), st.message
+
+        ms = statistics.mean(timed_steps(point_batch, 3, 1, stream, flush))
+        point_batch()
+        torch.cuda.synchronize()
+        e = np.abs(out[sub].double().cpu().numpy() - ref64_h)
+        ours_points[(o, b)] = {"ms_per_batch": ms, "queries_per_s": n / (ms / 1e3), "max_err_vs_fp64": float(e.max()),
+                               "p99_err_vs_fp64": float(np.quantile(e, 0.99))}
+    sg = None
+    if rank == 0:
+        sg = smallgwn_taylor_points(mesh, q, sub, ref64_h, points)
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
@@ -1500,17 +1579,41 @@ def main() -> None:
                     "chosen_over_plain": (value / world) / (n / (plain_ms / 1e3)),
                     "build_ms_hploc": build_ms, "bvh_nodes": int(bvh.accessor().node_count),
                     "fp64_fallbacks_per_batch": api.fp64_fallback_count(bvh, stream)})
+        head = sg.get((args.order, args.beta)) if sg else None
+        cfg["smallgwn_gpu"] = None if head is None else {
+            "kernel": f"gwn_compute_winding_number_taylor_batch<{args.order}> of smallgwn, compiled for sm_100a, on "
+                      f"its own H-PLOC (radius 8) BVH4 and moments; same mesh, queries and accuracy scale; L2 "
+                      f"flushed before each batch",
+            **head}
+        cfg["over_smallgwn"] = None if head is None else (value / world) / head["queries_per_s"]
+        cfg["taylor_at_scale_points"] = [
+            {"order": o, "accuracy_scale": b, "ours": ours_points[(o, b)],
+             "smallgwn": None if sg is None else sg.get((o, b)),
+             "ours_meets_1e-3": ours_points[(o, b)]["max_err_vs_fp64"] <= 1e-3}
+            for o, b in points]
         line = {
             "metric": METRIC, "value": value, "unit": "queries/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": cfg,
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
-                         "frac": achieved / pk["hbm_gbs"], "peak_source": pk["source"],
+            "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
+                         "frac": achieved / fp32_peak,
+                         "peak_source": "measured in this run: FP32 FMA chains on every SM, CUDA events "
+                                        "(gwnb_fp32_fma_peak)",
                          "traffic": traffic,
-                         "kernel": "k_taylor_warp (traversal, compensated, pre-ordered queries)",
+                         "kernel": "k_taylor_warp (traversal, compensated near field, pre-ordered queries)",
                          "kernel_ms": kernel_ms,
-                         "algorithmic_bytes": alg_bytes,
-                         "bytes_model": "16 B/query + (128 B node + moment node) per node entered + 36 B per exact triangle"},
+                         "flop_per_launch": flops,
+                         "flop_model": f"{FLOP_CHILD_TEST} per child test ({slots_per_node:.2f} valid slots per "
+                                       f"node entered) + {FLOP_FAR[args.order]} per far field + "
+                                       f"{FLOP_NEAR['compensated']} per compensated near-field triangle",
+                         "dram_gbs": None if traffic is None else traffic / (kernel_ms / 1e3) / 1e9,
+                         "hbm_peak_gbs": pk["hbm_gbs"], "hbm_peak_source": pk["source"],
+                         "dram_frac_of_hbm": None if traffic is None else
+                         traffic / (kernel_ms / 1e3) / 1e9 / pk["hbm_gbs"],
+                         "l2_hit_rate_pct": l2_hit,
+                         "touched_bytes_per_launch": touched_bytes,
+                         "touched_bytes_model": "16 B/query + (128 B node + moment node) per node entered + 36 B "
+                                                "per exact triangle, served mostly from L1/L2"},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": "queries/s", "h2d_bytes_per_step": 12 * n, "d2h_bytes_per_step": 4 * n},
             "gpu_launches": timed_launches,

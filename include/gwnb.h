@@ -138,6 +138,13 @@ GWNB_API const char *gwnb_version(void);
  * check which work ran on the GPU. */
 GWNB_API uint64_t gwnb_launch_count(void);
 
+/* Measured FP32 fused-multiply-add throughput of the current device (no smallgwn counterpart): one
+ * launch of independent FMA chains on every SM, timed with CUDA events on `stream` after one
+ * untimed launch; *tflops = 2 x FMAs / device time, *ms (may be NULL) = that time. The compute
+ * roofline of the Taylor traversal, which is bound by instruction issue on the CUDA cores, is
+ * reported against it. */
+GWNB_API int gwnb_fp32_fma_peak(int iters, double *tflops, double *ms, gwnb_stream_t stream);
+
 /* ---- device memory ------------------------------------------------------------------------- */
 /* Every device allocation of the library comes from one memory pool per device that keeps freed
  * memory mapped between host synchronizations (no smallgwn counterpart: smallgwn allocates with

@@ -439,6 +439,10 @@ class Reference:
         return {"nodes": nodes, "primitive_indices": prims, "triangles": tris, "root_reference": rr.value,
                 "root_bounds": rb, "internal_stack_bound": ib.value, "packed_stack_bound": pb.value}
 
+    def refit_moments(self, order: int) -> None:
+        """smallgwn's moment refit of `order` on its current BVH (kept on the device)."""
+        self._check(self.lib.ref_moment(self.h, C.c_int(order)))
+
     def moments(self, order: int) -> np.ndarray:
         self._check(self.lib.ref_moment(self.h, C.c_int(order)))
         F = {0: 7, 1: 13, 2: 23}[order]
@@ -647,6 +651,39 @@ def binary_leaf_sets(nodes: np.ndarray, root: int) -> set:
         leaves[v] = s
     assert len(order) == n, "binary tree does not reach every internal node"
     return {frozenset(v) for v in leaves.values()}
+
+
+def binary_leaf_set_hashes(nodes: np.ndarray, root: int, seed: int = 0x5EED) -> np.ndarray:
+    """Numbering-independent fingerprint of a binary tree for million-leaf trees: per internal node
+    the sum (mod 2^64) of one random 64-bit word per leaf under it, mixed with the leaf count,
+    sorted. Two trees with the same family of leaf sets give equal arrays; two that differ in any
+    node's leaf set collide with probability about 2^-64 per pair. Vectorised bottom-up over the
+    breadth-first levels; raises if the tree does not reach every internal node."""
+    nd = np.asarray(nodes, np.uint32).reshape(-1, 4)
+    n_int = nd.shape[0]
+    words = np.random.default_rng(seed).integers(0, np.iinfo(np.uint64).max, n_int + 1, dtype=np.uint64,
+                                                 endpoint=True)
+    levels = []
+    frontier = np.array([root], np.int64)
+    seen = 0
+    while frontier.size:
+        levels.append(frontier)
+        seen += frontier.size
+        if seen > n_int:
+            raise AssertionError("binary tree revisits internal nodes")
+        kids = [nd[frontier, 0][nd[frontier, 1] == 1], nd[frontier, 2][nd[frontier, 3] == 1]]
+        frontier = np.concatenate(kids).astype(np.int64)
+    if seen != n_int:
+        raise AssertionError("binary tree does not reach every internal node")
+    h = np.zeros(n_int, np.uint64)
+    cnt = np.zeros(n_int, np.uint64)
+    for lev in reversed(levels):
+        for side in (0, 2):
+            idx = nd[lev, side].astype(np.int64)
+            leaf = nd[lev, side + 1] == 2
+            h[lev] += np.where(leaf, words[np.minimum(idx, n_int)], h[np.minimum(idx, n_int - 1)])
+            cnt[lev] += np.where(leaf, np.uint64(1), cnt[np.minimum(idx, n_int - 1)])
+    return np.sort(h ^ (cnt * np.uint64(0x9E3779B97F4A7C15)))
 
 
 def match_wide_nodes(nodes_a: np.ndarray, root_a: int, nodes_b: np.ndarray, root_b: int) -> np.ndarray:

@@ -5,9 +5,11 @@
 1. oracle/_build/liboracle.so -- gcc build of gwn_oracle.c, the CPU restatement of smallgwn's
    algorithms (OpenMP, -ffp-contract=off).
 2. oracle/_ref/libgwnref.so -- smallgwn's own CUDA kernels, compiled for sm_100a from the
-   project's headers where they lie (GWN_REFERENCE_ROOT, default /root/reference/include) through
-   the thin extern "C" shim oracle/ref_shim.cu. Built only when those headers exist; the built
-   library travels with the repository to GPU machines, the headers do not.
+   project's headers where they lie through the thin extern "C" shim oracle/ref_shim.cu. Built
+   only when those headers exist; the built library travels with the repository to GPU machines,
+   the headers do not.
+The reference project's location is this recipe's one input: GWN_REFERENCE_ROOT when set, else the
+read-only mount the reference is provided at in the build container.
 Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg load these libraries.
 """
 from __future__ import annotations
@@ -23,7 +25,8 @@ BUILD = HERE / "_build"
 REF = HERE / "_ref"
 ORACLE_SO = BUILD / "liboracle.so"
 REF_SO = REF / "libgwnref.so"
-REFERENCE_INCLUDE = Path(os.environ.get("GWN_REFERENCE_ROOT", "/root/reference")) / "include"
+REFERENCE_ROOT = Path(os.environ.get("GWN_REFERENCE_ROOT", "/root/reference"))
+REFERENCE_INCLUDE = REFERENCE_ROOT / "include"
 
 
 def _newer(target: Path, *deps: Path) -> bool:

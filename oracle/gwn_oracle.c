@@ -857,6 +857,12 @@ void oracle_moments(int order, const o_node4 *nodes, uint64_t nn, const o_tri *t
 }
 
 /* ---------------------------------------------------------------------------------------------- */
+/* |q - P|^2 of the acceptance test in one fixed rounding pattern: rx * rx rounded, then two fused  */
+/* multiply-adds. The CUDA traversals write the same pattern with __fmul_rn / __fmaf_rn, so the     */
+/* oracle's accept / descend decisions equal theirs for the same tree, moments and query.          */
+static float accept_dist2(float rx, float ry, float rz) { return fmaf(rz, rz, fmaf(ry, ry, rx * rx)); }
+
+/* ---------------------------------------------------------------------------------------------- */
 /* Taylor traversal: gwn_winding_taylor_impl (detail/gwn_query_winding_impl.cuh:101-374), with    */
 /* per-query counts of nodes entered, accepted far-field children and exact triangles.             */
 
@@ -889,7 +895,7 @@ static float taylor_one(int order, const o_node4 *nodes, uint64_t nn, const floa
                 if (!ref_valid(r))
                     continue;
                 float rx = qx - T[1 * 4 + s], ry = qy - T[2 * 4 + s], rz = qz - T[3 * 4 + s];
-                float q2 = rx * rx + ry * ry + rz * rz;
+                float q2 = accept_dist2(rx, ry, rz);
                 int descend = !(q2 > 0.0f);
                 if (!descend)
                     descend = q2 <= T[0 * 4 + s] * beta2;
@@ -1210,7 +1216,7 @@ void oracle_taylor_frozen_f64(int order, const o_node4 *nodes, uint64_t nn, uint
                     if (!ref_valid(r))
                         continue;
                     float rx = dx[q] - T[1 * 4 + s], ry = dy[q] - T[2 * 4 + s], rz = dz[q] - T[3 * 4 + s];
-                    float q2 = rx * rx + ry * ry + rz * rz;
+                    float q2 = accept_dist2(rx, ry, rz);
                     int descend = !(q2 > 0.0f);
                     if (!descend)
                         descend = q2 <= T[0 * 4 + s] * beta2;

@@ -135,6 +135,39 @@ gwn::gwn_status ray_any(ctx &c, dbuf<float> *r, dbuf<ray_result> &o, float t_min
     return ray_cfg<gwn::gwn_query_batch_config{256, 256}>(c, r, o, t_min, t_max);
 }
 
+// Mean device time (ms) of `iters` calls of run() after `warmup` untimed ones, each timed call
+// bracketed by its own events on the legacy stream and preceded by a 256 MiB memset that flushes
+// the L2 (126 MB on B200), as the library's own benchmark times its steps.
+template <class F> int time_flushed(F &&run, int warmup, int iters, float *ms) {
+    for (int i = 0; i < warmup; ++i) {
+        auto s = run();
+        if (!s.is_ok())
+            return fail(s);
+    }
+    dbuf<unsigned char> flush(std::size_t(256) << 20);
+    std::vector<cudaEvent_t> ev(2 * static_cast<std::size_t>(iters > 0 ? iters : 1));
+    for (auto &e : ev)
+        cudaEventCreate(&e);
+    cudaDeviceSynchronize();
+    for (int i = 0; i < iters; ++i) {
+        cudaMemsetAsync(flush.p, i & 0xff, flush.n, cudaStreamLegacy);
+        cudaEventRecord(ev[2 * i], cudaStreamLegacy);
+        (void)run();
+        cudaEventRecord(ev[2 * i + 1], cudaStreamLegacy);
+    }
+    cudaDeviceSynchronize();
+    float total = 0;
+    for (int i = 0; i < iters; ++i) {
+        float t = 0;
+        cudaEventElapsedTime(&t, ev[2 * i], ev[2 * i + 1]);
+        total += t;
+    }
+    *ms = total / static_cast<float>(iters > 0 ? iters : 1);
+    for (auto &e : ev)
+        cudaEventDestroy(e);
+    return static_cast<int>(cudaGetLastError());
+}
+
 } // namespace
 
 extern "C" {
@@ -258,31 +291,13 @@ int ref_taylor_gradient(void *p, int order, const float *qx, const float *qy, co
     return static_cast<int>(cudaGetLastError());
 }
 
-// Times `iters` Taylor batches (device-resident queries) after `warmup` untimed ones; average ms.
+// Times `iters` Taylor batches (device-resident queries, L2 flushed before each) after `warmup`
+// untimed ones; mean ms per batch. The moments of `order` must have been refit (ref_moment).
 int ref_time_taylor(void *p, int order, const float *qx, const float *qy, const float *qz, uint64_t n, float beta,
                     int warmup, int iters, float *ms) {
     auto &c = *static_cast<ctx *>(p);
     dbuf<float> x(qx, n), y(qy, n), z(qz, n), o(n);
-    for (int i = 0; i < warmup; ++i) {
-        auto s = taylor_order(c, order, x, y, z, o, beta);
-        if (!s.is_ok())
-            return fail(s);
-    }
-    cudaEvent_t e0, e1;
-    cudaEventCreate(&e0);
-    cudaEventCreate(&e1);
-    cudaDeviceSynchronize();
-    cudaEventRecord(e0, cudaStreamLegacy);
-    for (int i = 0; i < iters; ++i)
-        (void)taylor_order(c, order, x, y, z, o, beta);
-    cudaEventRecord(e1, cudaStreamLegacy);
-    cudaEventSynchronize(e1);
-    float t = 0;
-    cudaEventElapsedTime(&t, e0, e1);
-    *ms = t / static_cast<float>(iters > 0 ? iters : 1);
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    return static_cast<int>(cudaGetLastError());
+    return time_flushed([&]() { return taylor_order(c, order, x, y, z, o, beta); }, warmup, iters, ms);
 }
 
 int ref_time_exact(void *p, const float *qx, const float *qy, const float *qz, uint64_t n, int warmup, int iters,
@@ -294,26 +309,7 @@ int ref_time_exact(void *p, const float *qx, const float *qy, const float *qz, u
             c.bvh, gwn::gwn_device_span<float const>(x.p, n), gwn::gwn_device_span<float const>(y.p, n),
             gwn::gwn_device_span<float const>(z.p, n), gwn::gwn_device_span<float>(o.p, n));
     };
-    for (int i = 0; i < warmup; ++i) {
-        auto s = run();
-        if (!s.is_ok())
-            return fail(s);
-    }
-    cudaEvent_t e0, e1;
-    cudaEventCreate(&e0);
-    cudaEventCreate(&e1);
-    cudaDeviceSynchronize();
-    cudaEventRecord(e0, cudaStreamLegacy);
-    for (int i = 0; i < iters; ++i)
-        (void)run();
-    cudaEventRecord(e1, cudaStreamLegacy);
-    cudaEventSynchronize(e1);
-    float t = 0;
-    cudaEventElapsedTime(&t, e0, e1);
-    *ms = t / static_cast<float>(iters > 0 ? iters : 1);
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    return static_cast<int>(cudaGetLastError());
+    return time_flushed(run, warmup, iters, ms);
 }
 
 // Wall time of one gwn_build_bvh (host-synchronous by design in smallgwn), average over iters.

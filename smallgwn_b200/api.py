@@ -718,6 +718,15 @@ def launch_count() -> int:
     return int(_lib.load().gwnb_launch_count())
 
 
+def fp32_fma_peak(iters: int = 16384, stream=None) -> tuple[float, float]:
+    """Measured FP32 FMA throughput of the current GPU: (TFLOP/s, ms of the timed launch)."""
+    tf, ms = C.c_double(), C.c_double()
+    rc = _lib.load().gwnb_fp32_fma_peak(int(iters), C.byref(tf), C.byref(ms), _stream(stream))
+    if rc != _lib.GWNB_OK:
+        raise RuntimeError(_lib.last_error())
+    return float(tf.value), float(ms.value)
+
+
 def memory_trim(keep_bytes: int = 0) -> gwn_status:
     """Return the pool's cached device memory to the driver down to keep_bytes (or what is in use)."""
     return _status(_lib.load().gwnb_memory_trim(int(keep_bytes)))

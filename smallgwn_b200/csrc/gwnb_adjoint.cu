@@ -180,10 +180,8 @@ __global__ void __launch_bounds__(256, 4) k_adjoint_traverse(adjoint_params p) {
                     sv[j] = 0.0f;
                 if (active) {
                     float const rx = qx - a.x, ry = qy - a.y, rz = qz - a.z;
-                    float const q2 = rx * rx + ry * ry + rz * rz;
-                    desc = !(q2 > 0.0f);
-                    if (!desc)
-                        desc = q2 <= a.w * p.beta2;
+                    float const q2 = accept_dist2(rx, ry, rz);
+                    desc = !far_accepted(q2, a.w, p.beta2);
                     if (!desc) {
                         float g0 = 0.0f, g1 = 0.0f, g2 = 0.0f;
                         float const w = far_field<Order, true>(rx, ry, rz, q2, b, nd + s * Q + 2, g0, g1, g2);
@@ -528,7 +526,7 @@ int taylor_adjoint(adjoint_request const &r, cudaStream_t s) {
     p.n = r.n;
     p.beta2 = r.accuracy_scale * r.accuracy_scale;
     p.status = r.status;
-    int const block = r.block > 0 ? r.block : 256;
+    int const block = query_launch_block(r.block);
     rc = r.order == 0 ? launch_traverse<0>(p, r.stack_capacity, block, s)
                       : launch_traverse<1>(p, r.stack_capacity, block, s);
     if (rc != GWNB_OK)

@@ -797,7 +797,8 @@ static int antipodal_common(const gwnb_geometry_f32 *g, const gwnb_bvh4_f32 *b_i
         if (ref_internal(b_in->root.reference) && b_in->internal_stack_bound > static_cast<std::uint32_t>(o.stack_capacity))
             return set_error(GWNB_INVALID_ARGUMENT, "Traversal stack capacity is below the BVH internal stack bound.");
         if (ref_internal(b_in->root.reference) &&
-            static_cast<std::uint64_t>(b_in->internal_stack_bound) * o.block_size * 4u + 2u * k_ap_tile * 16u >
+            static_cast<std::uint64_t>(b_in->internal_stack_bound) * query_launch_block(o.block_size) * 4u +
+                    2u * k_ap_tile * 16u >
                 227u * 1024u)
             return set_error(GWNB_INVALID_ARGUMENT,
                              "Traversal stack bound times block size exceeds the 227 KB of shared memory per block.");
@@ -858,19 +859,20 @@ static int antipodal_common(const gwnb_geometry_f32 *g, const gwnb_bvh4_f32 *b_i
         p.gy = gy;
         p.gz = gz;
         p.n = n;
+        int const block = query_launch_block(o.block_size);
         if (gradient) {
-            unsigned const grid = static_cast<unsigned>((n + o.block_size - 1) / o.block_size);
-            note_launch(), k_antipodal_gradient<<<grid, o.block_size, 0, s>>>(p);
+            unsigned const grid = static_cast<unsigned>((n + block - 1) / block);
+            note_launch(), k_antipodal_gradient<<<grid, block, 0, s>>>(p);
         } else {
-            std::uint64_t const per_block = static_cast<std::uint64_t>(o.block_size) * k_ap_q;
+            std::uint64_t const per_block = static_cast<std::uint64_t>(block) * k_ap_q;
             unsigned const grid = static_cast<unsigned>((n + per_block - 1) / per_block);
             std::size_t const smem = 2 * k_ap_tile * sizeof(float4) +
-                                     static_cast<std::size_t>(p.stack_cap) * o.block_size * sizeof(std::uint32_t);
+                                     static_cast<std::size_t>(p.stack_cap) * block * sizeof(std::uint32_t);
             cudaError_t e = cudaSuccess;
             if (smem > 48 * 1024)
                 e = cudaFuncSetAttribute(k_antipodal, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
             if (e == cudaSuccess)
-                note_launch(), k_antipodal<<<grid, o.block_size, smem, s>>>(p);
+                note_launch(), k_antipodal<<<grid, block, smem, s>>>(p);
         }
         cudaError_t const e = cudaGetLastError();
         if (e != cudaSuccess)

@@ -19,6 +19,21 @@ namespace field {
 
 constexpr float k_pi_f = 3.14159265358979323846f;
 
+// |q - P|^2 for the acceptance test, with one fixed rounding pattern (rx * rx rounded, then two
+// fused multiply-adds) written out so that no compiler contraction choice can change it. Every
+// traversal (value, gradient, statistics, adjoint, batched) and the oracle's C restatement use
+// this pattern, so their accept / descend decisions are identical for identical inputs.
+__device__ __forceinline__ float accept_dist2(float rx, float ry, float rz) {
+    return __fmaf_rn(rz, rz, __fmaf_rn(ry, ry, __fmul_rn(rx, rx)));
+}
+
+// smallgwn's acceptance rule (detail/gwn_query_winding_impl.cuh:186-189): descend iff
+// !(|q - P|^2 > 0) or |q - P|^2 <= r^2 beta^2 (the product rounded on its own); a NaN bound
+// therefore accepts, as there.
+__device__ __forceinline__ bool far_accepted(float q2, float r2, float beta2) {
+    return q2 > 0.0f && !(q2 <= __fmul_rn(r2, beta2));
+}
+
 // a = v0 - q, e1, e2 edges, n = e1 x e2.
 __device__ __forceinline__ float solid_angle_plain(float ax, float ay, float az, float e1x, float e1y,
                                                    float e1z, float e2x, float e2y, float e2z,

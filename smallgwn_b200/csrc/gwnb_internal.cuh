@@ -193,6 +193,15 @@ int device_sm_count();
 extern std::atomic<std::uint64_t> g_launch_count;
 inline void note_launch() { g_launch_count.fetch_add(1, std::memory_order_relaxed); }
 
+// Threads per block of a query launch. smallgwn's batch configurations accept block sizes up to 1024
+// (include/gwn/gwn_query.cuh:37); the query kernels here are compiled for blocks of at most 256
+// threads (__launch_bounds__(256): 64 registers per thread at 4 blocks per SM), so a larger request
+// launches 256-thread blocks. Every query's result is independent of the block it runs in.
+constexpr int k_query_block_max = 256;
+inline int query_launch_block(int requested) {
+    return requested <= 0 ? k_query_block_max : (requested < k_query_block_max ? requested : k_query_block_max);
+}
+
 // Release / acquire fence at GPU scope (PTX fence.acq_rel.gpu). The bottom-up kernels publish a
 // node's data with plain stores, this fence, then a relaxed atomic on the node's counter; the
 // thread that reads the counter's final value runs this fence before reading the data -- the

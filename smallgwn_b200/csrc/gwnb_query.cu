@@ -290,10 +290,8 @@ __device__ __forceinline__ void taylor_thread_item(taylor_params const &p, std::
                     continue;
                 float4 const b = __ldg(nd + s * Q + 1);
                 float const rx = qx - a.x, ry = qy - a.y, rz = qz - a.z;
-                float const q2 = rx * rx + ry * ry + rz * rz;
-                bool descend = !(q2 > 0.0f);
-                if (!descend)
-                    descend = q2 <= a.w * p.beta2;
+                float const q2 = accept_dist2(rx, ry, rz);
+                bool descend = !far_accepted(q2, a.w, p.beta2);
                 if (!descend) {
                     float g0 = 0.0f, g1 = 0.0f, g2 = 0.0f;
                     float const w = far_field<Order, Grad>(rx, ry, rz, q2, b, nd + s * Q + 2, g0, g1, g2);
@@ -460,10 +458,8 @@ __device__ __forceinline__ void taylor_warp_item(taylor_params const &p, std::ui
                 bool desc = false;
                 if (active) {
                     float const rx = qx - a.x, ry = qy - a.y, rz = qz - a.z;
-                    float const q2 = rx * rx + ry * ry + rz * rz;
-                    desc = !(q2 > 0.0f);
-                    if (!desc)
-                        desc = q2 <= a.w * p.beta2;
+                    float const q2 = accept_dist2(rx, ry, rz);
+                    desc = !far_accepted(q2, a.w, p.beta2);
                     if (!desc) {
                         float g0 = 0.0f, g1 = 0.0f, g2 = 0.0f;
                         float const w = far_field<Order, Grad>(rx, ry, rz, q2, b, nd + s * Q + 2, g0, g1, g2);
@@ -754,7 +750,7 @@ int taylor_batch(taylor_request const &r, cudaStream_t s) {
     bool const grad = r.gx != nullptr;
     bool const stats = r.stat_nodes != nullptr;
     int rc = GWNB_OK;
-    int const block = r.block > 0 ? r.block : 256;
+    int const block = query_launch_block(r.block);
     int const cap = r.stack_capacity;
     bool const per_thread = r.per_thread != 0;
 #define GWNB_DISPATCH(O)                                                                           \
@@ -926,7 +922,7 @@ int taylor_batch_in_scratch(taylor_request const &r, std::uint32_t *scratch, std
                                                  words, s, r.status));
         p.order = order;
     }
-    int const block = r.block > 0 ? r.block : 256;
+    int const block = query_launch_block(r.block);
     bool const per_thread = r.per_thread != 0;
     if (r.order == 0)
         return launch_taylor_order<0, false, false>(p, block, r.stack_capacity, r.near_mode, per_thread, s);

@@ -875,10 +875,11 @@ int spatial_batch(gwnb_bvh4_f32 *b, spatial_request const &r, cudaStream_t s) {
     bool const stats = r.stat_nodes != nullptr;
     int rc;
     if (r.ray)
-        rc = stats ? launch_spatial<true, true>(p, r.opt.block_size, s) : launch_spatial<true, false>(p, r.opt.block_size, s);
+        rc = stats ? launch_spatial<true, true>(p, query_launch_block(r.opt.block_size), s)
+                   : launch_spatial<true, false>(p, query_launch_block(r.opt.block_size), s);
     else
-        rc = stats ? launch_spatial<false, true>(p, r.opt.block_size, s)
-                   : launch_spatial<false, false>(p, r.opt.block_size, s);
+        rc = stats ? launch_spatial<false, true>(p, query_launch_block(r.opt.block_size), s)
+                   : launch_spatial<false, false>(p, query_launch_block(r.opt.block_size), s);
     release(order, s);
     return rc;
 }
@@ -901,7 +902,9 @@ int spatial_options(gwnb_bvh4_f32 const *b, gwnb_spatial_options const *in, gwnb
         return set_error(GWNB_INVALID_ARGUMENT, "Traversal stack capacity is below the BVH internal stack bound.");
     // the shared-memory stack holds the internal stack bound for every thread of a block
     if (ref_internal(b->root.reference) &&
-        static_cast<std::uint64_t>(b->internal_stack_bound) * o.block_size * sizeof(std::uint32_t) > 227u * 1024u)
+        static_cast<std::uint64_t>(b->internal_stack_bound) * query_launch_block(o.block_size) *
+                sizeof(std::uint32_t) >
+            227u * 1024u)
         return set_error(GWNB_INVALID_ARGUMENT,
                          "Traversal stack bound times block size exceeds the 227 KB of shared memory per block.");
     // candidate payloads hold internal node indices below 2^31 (the top bit marks leaves)

@@ -182,6 +182,20 @@ void queries_match_cpu() {
         CHECK(std::abs(he[i] - ref) <= 1e-5);
         CHECK(std::abs(ht[i] - he[i]) <= 1e-6);
     }
+    // smallgwn accepts batch block sizes up to 1024: the same results with 512- and 1024-thread configs
+    constexpr gwn::gwn_query_batch_config k_wide{512, 64};
+    constexpr gwn::gwn_query_batch_config k_widest{1024, 64};
+    dbuf wide(qx.size()), widest(qx.size());
+    CHECK((gwn::gwn_compute_winding_number_taylor_batch<1, k_wide>(bvh, moment, dx.in(), dy.in(), dz.in(),
+                                                                   wide.out(), Real(1e6))
+               .is_ok()));
+    CHECK((gwn::gwn_compute_winding_number_taylor_batch<1, k_widest>(bvh, moment, dx.in(), dy.in(), dz.in(),
+                                                                     widest.out(), Real(1e6))
+               .is_ok()));
+    auto hw = wide.host();
+    auto hww = widest.host();
+    for (std::size_t i = 0; i < qx.size(); ++i)
+        CHECK(hw[i] == ht[i] && hww[i] == ht[i]);
     // a refit publishes a new revision: the old moments are stale
     CHECK(gwn::gwn_refit_bvh(geometry, bvh).is_ok());
     CHECK(!moment.accessor().is_valid_for(bvh.accessor()));

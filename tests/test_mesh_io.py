@@ -16,9 +16,11 @@ import numpy as np
 import pytest
 
 from conftest import cube, open_cube
+from oracle.build import REFERENCE_ROOT
 from smallgwn_b200 import _lib, api, meshes
 
-REFERENCE_DATA = Path("/root/reference/tests/data")
+# smallgwn's own PLY fixtures, where the oracle's build recipe finds the reference project
+REFERENCE_DATA = REFERENCE_ROOT / "tests" / "data"
 
 
 def ply_text(mesh: dict, comment: str = "fixture") -> str:

@@ -7,8 +7,12 @@ forbids new allocations. It keeps its query-ordering scratch in one file-scope d
 GWNB_NOALLOC_MAX_QUERIES queries instead of allocating per call.
 
 The test calls it through the C ABI twice in a row (the second call runs on scratch left over from
-the first) and compares both results with gwnb_winding_taylor_batch_f32 on the same inputs. It
-builds everything it needs, so it passes in a fresh process as well as after the other tests.
+the first) on a batch of exactly GWNB_NOALLOC_MAX_QUERIES queries, so every scratch region and the
+sort's last tile are full, and compares both results with gwnb_winding_taylor_batch_f32 on the same
+inputs. It checks the property the entry point exists for: across both calls the library's device
+memory pool neither grows nor hands out memory (gwnb_memory_stats, after the allocating batch's
+scratch is trimmed back). It builds everything it needs, so it passes in a fresh process as well as
+after the other tests.
 """
 from __future__ import annotations
 
@@ -18,7 +22,7 @@ import numpy as np
 import pytest
 
 import smallgwn_b200 as g
-from smallgwn_b200 import _lib, meshes
+from smallgwn_b200 import _lib, api, meshes
 
 pytestmark = pytest.mark.gpu
 
@@ -37,7 +41,7 @@ def test_no_alloc_taylor_batch_matches_allocating_batch():
     mom = g.gwn_bvh4_moment_object(2)
     assert g.gwn_refit_bvh_moment(2, bvh, mom).is_ok()
 
-    n = 100_000
+    n = MAX_QUERIES
     q = [torch.from_numpy(v).cuda() for v in meshes.mixed_queries(mesh, n, seed=23)]
     expected = torch.empty(n, device="cuda")
     assert g.gwn_compute_winding_number_taylor_batch(2, bvh, mom, *q, expected, accuracy_scale=3.0).is_ok()
@@ -46,13 +50,18 @@ def test_no_alloc_taylor_batch_matches_allocating_batch():
 
     lib = _lib.load()
     opt = _lib.taylor_options(256, 64, 1, _lib.GWNB_NEAR_PLAIN, 1e-3, 0)
-    for _ in range(2):
-        out = torch.full((n,), float("nan"), device="cuda")
+    outs = [torch.full((n,), float("nan"), device="cuda") for _ in range(2)]
+    torch.cuda.synchronize()
+    assert api.memory_trim(0).is_ok()
+    pool_before = api.memory_stats()
+    for out in outs:
         rc = lib.gwnb_winding_taylor_batch_noalloc_f32(
             C.byref(bvh.accessor()), C.byref(mom.accessor()), q[0].data_ptr(), q[1].data_ptr(), q[2].data_ptr(),
             out.data_ptr(), n, 3.0, C.byref(opt), None)
         assert rc == _lib.GWNB_OK, _lib.last_error()
         torch.cuda.synchronize()
+        assert api.memory_stats() == pool_before
+    for out in outs:
         got = out.cpu().numpy()
         assert np.all(np.isfinite(got))
         np.testing.assert_allclose(got, want, atol=1e-6, rtol=1e-6)
