@@ -96,6 +96,7 @@ def test_taylor_matches_reference_kernel_at_size(cuda, order):
         rb = R.bvh()
         pairing = oracle.match_wide_nodes(h["nodes"], h["root_reference"], rb["nodes"], rb["root_reference"])
         q = meshes.mixed_queries(mesh, 20_000, seed=2)
+        R.refit_moments(order)
         theirs = R.taylor(order, *q, beta=2.0)
         d = [cuda.from_numpy(v).cuda() for v in q]
         out = cuda.empty_like(d[0])
@@ -103,7 +104,7 @@ def test_taylor_matches_reference_kernel_at_size(cuda, order):
         cuda.cuda.synchronize()
         ours = out.cpu().numpy()
         rep = assert_agree_or_explained(ours, theirs, q, h, api.moment_host_array(mom), R.moments(order), pairing,
-                                        2.0, allow=("decision", "conditioning"))
+                                        2.0, allow=("decision", "conditioning", "moments"))
         # flips move a query by the local truncation error; they stay rare
         assert rep["outside"].size <= 0.02 * ours.size
         sub = slice(0, 2000)
