@@ -156,9 +156,10 @@ def run_profile(args) -> None:
     method = 1 if args.profile == "exact" else 0
     assert g.gwn_build_bvh(geo, bvh, g.gwn_bvh_build_options(method=method, hploc_search_radius=8)).is_ok()
     if args.profile == "build":
-        # two H-PLOC builds, one refit, one moment refit of each order
+        # two H-PLOC builds, one LBVH build, one refit, one moment refit of each order
         for _ in range(2):
             assert g.gwn_build_bvh(geo, bvh, g.gwn_bvh_build_options(method=0, hploc_search_radius=8)).is_ok()
+        assert g.gwn_build_bvh(geo, g.gwn_bvh4_object(), g.gwn_bvh_build_options(method=1)).is_ok()
         assert g.gwn_refit_bvh(geo, bvh).is_ok()
         for o in range(3):
             assert g.gwn_refit_bvh_moment(o, bvh, g.gwn_bvh4_moment_object(o)).is_ok()
@@ -858,7 +859,12 @@ def run_batched_workload(args) -> None:
         per_mesh_frame()
     torch.cuda.synchronize()
     loop_ms = (time.perf_counter() - t0) * 1e3 / loop_frames
+    # smallgwn's own per-mesh dynamic stage (tests/benchmark_main.cu:847-866: host positions up,
+    # gwn_refit_bvh, gwn_refit_bvh_moment, Taylor batch on device-resident queries) over the same
+    # meshes (its own H-PLOC trees of the rest shape), queries and final-frame positions
+    sg_ms = smallgwn_dynamic_frames(parts, objs, X, order, beta)
     loop_ms, max_diff = sharding.max_over_ranks([loop_ms, max_diff])
+    sg_ms = sharding.max_over_ranks([sg_ms if sg_ms is not None else -1.0])[0]
     del graph
     batch.release()
     total_ms = float(lat.sum())
@@ -878,12 +884,53 @@ def run_batched_workload(args) -> None:
                                    "over ranks" if world > 1 else "one GPU"),
                    "frame_ms_p50": float(np.percentile(lat, 50)), "frame_ms_p99": float(np.percentile(lat, 99)),
                    "per_mesh_loop_ms_per_frame": loop_ms, "speedup_vs_per_mesh_loop": loop_ms / (total_ms / frames),
+                   "smallgwn_per_mesh_ms_per_frame": sg_ms if sg_ms > 0 else None,
+                   "over_smallgwn": (sg_ms / (total_ms / frames)) if sg_ms > 0 else None,
+                   "smallgwn_kernels": "smallgwn's own dynamic stage per mesh (gwn_update_geometry from the host, "
+                                       "gwn_refit_bvh, gwn_refit_bvh_moment<1>, Taylor batch), oracle/_ref, sm_100a; "
+                                       "wall clock per frame over all meshes",
                    "max_abs_diff_vs_per_mesh_loop": max_diff, "tuning": tuning,
                    "stage_ms_frame_100": stages_end, "stage_ms_frame_50": stages_mid},
         "gpu_launches": frame_launches * frames,  # the library kernels recorded in one frame's graph
         "clocks": clocks.summary(),
     }
     print(json.dumps(line), flush=True)
+
+
+def smallgwn_dynamic_frames(parts, objs, X, order, beta, frames: int = 3):
+    """Wall-clock ms per frame of smallgwn's dynamic stage run mesh by mesh (a baseline beside the
+    batched frame, not part of its value); None when oracle/_ref was not built."""
+    import torch
+
+    import oracle
+
+    if oracle.ref_lib() is None:
+        return None
+    refs = []
+    try:
+        Xh = X.cpu().numpy()
+        off = 0
+        pos = []
+        for (V, F, vn, mesh), o in zip(parts, objs):
+            R = oracle.Reference(mesh)
+            refs.append(R)
+            R.build(0, 8, 64)
+            R.set_queries(*[t.cpu().numpy() for t in o[3:6]])
+            n = V.shape[0]
+            pos.append([np.ascontiguousarray(Xh[k, off:off + n]) for k in range(3)])
+            off += n
+        for R, p in zip(refs, pos):  # untimed warm frame
+            R.dynamic_frame(*p, order, beta)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(frames):
+            for R, p in zip(refs, pos):
+                R.dynamic_frame(*p, order, beta)
+        torch.cuda.synchronize()
+        return (time.perf_counter() - t0) * 1e3 / frames
+    finally:
+        for R in refs:
+            R.close()
 
 
 def run_build_workload(args) -> None:
@@ -1024,17 +1071,33 @@ def run_exact_workload(args) -> None:
     def run():
         assert g.gwn_compute_winding_number_exact_batch(bvh, *dq, out, stream).is_ok()
 
-    props = torch.cuda.get_device_properties(torch.cuda.current_device())
-    max_mhz = 1965.0
-    if (ROOT / "MEASURED_PEAKS.json").exists():
-        max_mhz = float(json.loads((ROOT / "MEASURED_PEAKS.json").read_text()).get("sm_max_mhz", max_mhz))
-    fp32_peak = props.multi_processor_count * 128 * 2 * max_mhz * 1e6 / 1e12
+    from smallgwn_b200 import api
+
+    fp32_peak, _ = api.fp32_fma_peak(stream=stream)
     exact_launches: list[int] = []
     t = timed_steps(run, args.steps, args.warmup, stream, flush, exact_launches)
     ms = float(np.mean(t))
     nq, nt = dq[0].numel(), int(mesh["i0"].size)
     ref = oracle.exact_winding(mesh, *q)
-    err = float(np.abs(out.cpu().numpy() - ref).max())
+    ref64 = oracle.exact_winding(mesh, *q, fp64=True)
+    ours = out.cpu().numpy()
+    err = float(np.abs(ours - ref).max())
+    e64 = np.abs(ours - ref64)
+    # smallgwn's own exact batch (gwn_compute_winding_number_exact_batch, oracle/_ref, sm_100a) on the
+    # same mesh, queries and LBVH, L2 flushed before each batch
+    sg = None
+    if oracle.ref_lib() is not None:
+        R = oracle.Reference(mesh)
+        try:
+            R.build(1, 8, 64)
+            sg_ms = R.time_exact(*q, warmup=args.warmup, iters=args.steps)
+            e_sg = np.abs(R.exact(*q).astype(np.float64) - ref64)
+            sg = {"kernel": "gwn_compute_winding_number_exact_batch of smallgwn, compiled for sm_100a, same mesh, "
+                            "queries and LBVH; L2 flushed before each batch",
+                  "ms_per_batch": sg_ms, "evaluations_per_s": nq * nt / (sg_ms / 1e3),
+                  "max_err_vs_fp64": float(e_sg.max()), "p99_err_vs_fp64": float(np.quantile(e_sg, 0.99))}
+        finally:
+            R.close()
     threads = oracle.max_threads()
     t0 = time.perf_counter()
     m = 10_000
@@ -1046,14 +1109,17 @@ def run_exact_workload(args) -> None:
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic",
         "config": {"workload": "icosphere L4 (5,120 tris), 100k queries in [-1.5,1.5]^3", "builder": "lbvh",
-                   "max_abs_diff_vs_oracle_fp32": err},
+                   "max_abs_diff_vs_oracle_fp32": err, "max_err_vs_fp64": float(e64.max()),
+                   "p99_err_vs_fp64": float(np.quantile(e64, 0.99)), "smallgwn_gpu": sg,
+                   "over_smallgwn": None if sg is None else sg["ms_per_batch"] / ms},
         "cpu_baseline": {"value": m * nt / cpu_s, "unit": "evaluations/s", "cores": threads, "kind": "port",
                          "sample": f"{m} of the queries against all triangles"},
         # FP32 CUDA-core roofline: 70 FP32 add/mul per evaluation (plus 3 sqrt, 1 atan2 on the
-        # SFU, not counted); no FP32 peak is measured, so the nominal one of the device is used
+        # SFU, not counted) against the FP32 FMA throughput measured in this run
         "roofline": {"bound": "fp32", "achieved": nq * nt * 70 / (ms / 1e3) / 1e12, "peak": fp32_peak,
                      "unit": "TFLOP/s", "frac": nq * nt * 70 / (ms / 1e3) / 1e12 / fp32_peak,
-                     "peak_source": "nominal: SMs x 128 FP32 lanes x 2 FLOP x max SM clock",
+                     "peak_source": "measured in this run: FP32 FMA chains on every SM, CUDA events "
+                                    "(gwnb_fp32_fma_peak)",
                      "traffic": None, "kernel": "k_exact", "bytes_model": "70 FLOP per (query, triangle)"},
         "gpu_launches": exact_launches[0],
     }

@@ -145,6 +145,25 @@ GWNB_API uint64_t gwnb_launch_count(void);
  * reported against it. */
 GWNB_API int gwnb_fp32_fma_peak(int iters, double *tflops, double *ms, gwnb_stream_t stream);
 
+/* ---- bounded device waits (no smallgwn counterpart) ----------------------------------------------
+ * smallgwn's BVH4 collapse spins without a limit on its work queue (detail/gwn_bvh_build_collapse.cuh
+ * :142-144). Every device-side wait of this library -- the decoupled look-back of the radix sort and
+ * of the level-synchronous collapse -- gives up after a number of polls, sets a timeout bit in the
+ * call's device status word and lets the launch complete; the synchronizing call that reads the
+ * status then returns GWNB_INTERNAL_ERROR. */
+
+/* Polls after which a device wait gives up, for launches issued after the call by any thread of
+ * the process; polls <= 0 restores the default (2^22, about 10 ms of polling). A small limit lets a
+ * test make a wait run out quickly. */
+GWNB_API int gwnb_set_wait_limit(int64_t polls);
+
+/* Runs one look-back whose predecessor tile is never published and reports how the wait ended:
+ * stage 0 is a real radix-sort pass over two tiles whose first tile is never processed, stage 1
+ * the BVH4 collapse's tile-prefix wait on an unpublished tile. Returns GWNB_INTERNAL_ERROR with a
+ * "timed out" message once the wait gives up (the expected outcome), after at most the wait limit
+ * in polls; synchronizes `stream`. */
+GWNB_API int gwnb_wait_timeout_probe(int stage, gwnb_stream_t stream);
+
 /* ---- device memory ------------------------------------------------------------------------- */
 /* Every device allocation of the library comes from one memory pool per device that keeps freed
  * memory mapped between host synchronizations (no smallgwn counterpart: smallgwn allocates with

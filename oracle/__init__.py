@@ -439,6 +439,17 @@ class Reference:
         return {"nodes": nodes, "primitive_indices": prims, "triangles": tris, "root_reference": rr.value,
                 "root_bounds": rb, "internal_stack_bound": ib.value, "packed_stack_bound": pb.value}
 
+    def set_queries(self, qx, qy, qz) -> None:
+        """Device-resident query batch for dynamic_frame."""
+        q = [_f32(v) for v in (qx, qy, qz)]
+        self._check(self.lib.ref_set_queries(self.h, _p(q[0]), _p(q[1]), _p(q[2]), C.c_uint64(q[0].size)))
+
+    def dynamic_frame(self, x, y, z, order: int, beta: float) -> None:
+        """smallgwn's dynamic stage for one frame: host positions up, refit, moment refit, Taylor batch."""
+        v = [_f32(a) for a in (x, y, z)]
+        self._check(self.lib.ref_dynamic_frame(self.h, _p(v[0]), _p(v[1]), _p(v[2]), C.c_uint64(v[0].size),
+                                               C.c_int(order), C.c_float(beta)))
+
     def refit_moments(self, order: int) -> None:
         """smallgwn's moment refit of `order` on its current BVH (kept on the device)."""
         self._check(self.lib.ref_moment(self.h, C.c_int(order)))

@@ -16,6 +16,7 @@
 
 #include <cstdint>
 #include <cstring>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -35,6 +36,8 @@ struct no_trap {
     __device__ void operator()() const noexcept {}
 };
 
+template <class T> struct dbuf;
+
 struct ctx {
     gwn::gwn_geometry_object<Real, Index> geometry;
     gwn::gwn_bvh4_object<Real, Index> bvh;
@@ -42,6 +45,8 @@ struct ctx {
     gwn::gwn_bvh4_moment_object<1, Real, Index> m1;
     gwn::gwn_bvh4_moment_object<2, Real, Index> m2;
     gwn::gwn_boundary_chain_object<Index> chain;
+    // device-resident query batch of the dynamic frame (ref_set_queries / ref_dynamic_frame)
+    std::unique_ptr<dbuf<float>> qx, qy, qz, out;
 };
 
 template <class T> struct dbuf {
@@ -374,6 +379,39 @@ int ref_update_refit(void *p, const float *x, const float *y, const float *z, ui
     if (!s.is_ok())
         return fail(s);
     s = gwn::gwn_refit_bvh(c.geometry, c.bvh);
+    return s.is_ok() ? 0 : fail(s);
+}
+
+// Uploads a query batch that ref_dynamic_frame evaluates on the device.
+int ref_set_queries(void *p, const float *qx, const float *qy, const float *qz, uint64_t n) {
+    auto &c = *static_cast<ctx *>(p);
+    c.qx = std::make_unique<dbuf<float>>(qx, n);
+    c.qy = std::make_unique<dbuf<float>>(qy, n);
+    c.qz = std::make_unique<dbuf<float>>(qz, n);
+    c.out = std::make_unique<dbuf<float>>(n);
+    return static_cast<int>(cudaGetLastError());
+}
+
+// One frame of smallgwn's dynamic benchmark stage (tests/benchmark_main.cu:847-866): upload the
+// frame's vertex positions from the host, refit the BVH, refit the moments of `order`, Taylor batch
+// over the device-resident queries of ref_set_queries.
+int ref_dynamic_frame(void *p, const float *x, const float *y, const float *z, uint64_t nv, int order, float beta) {
+    auto &c = *static_cast<ctx *>(p);
+    if (!c.qx)
+        return 1;
+    auto s = gwn::gwn_update_geometry(c.geometry, gwn::gwn_host_span<float const>(x, nv),
+                                      gwn::gwn_host_span<float const>(y, nv), gwn::gwn_host_span<float const>(z, nv));
+    if (!s.is_ok())
+        return fail(s);
+    s = gwn::gwn_refit_bvh(c.geometry, c.bvh);
+    if (!s.is_ok())
+        return fail(s);
+    s = order == 0 ? gwn::gwn_refit_bvh_moment<0>(c.bvh, c.m0)
+        : order == 1 ? gwn::gwn_refit_bvh_moment<1>(c.bvh, c.m1)
+                     : gwn::gwn_refit_bvh_moment<2>(c.bvh, c.m2);
+    if (!s.is_ok())
+        return fail(s);
+    s = taylor_order(c, order, *c.qx, *c.qy, *c.qz, *c.out, beta);
     return s.is_ok() ? 0 : fail(s);
 }
 

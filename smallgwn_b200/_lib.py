@@ -189,6 +189,8 @@ SIGNATURES: dict[str, tuple] = {
     "gwnb_memory_trim": (C.c_int, [C.c_uint64]),
     "gwnb_launch_count": (C.c_uint64, []),
     "gwnb_fp32_fma_peak": (C.c_int, [C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_void_p]),
+    "gwnb_set_wait_limit": (C.c_int, [C.c_int64]),
+    "gwnb_wait_timeout_probe": (C.c_int, [C.c_int, C.c_void_p]),
     "gwnb_geometry_upload_f32": (I, [C.POINTER(geometry_f32), P, P, P, U64, P, P, P, U64, P]),
     "gwnb_geometry_update_f32": (I, [C.POINTER(geometry_f32), P, P, P, U64, P]),
     "gwnb_geometry_update_device_f32": (I, [C.POINTER(geometry_f32), P, P, P, U64, P]),

@@ -10,9 +10,11 @@
 //   Karras: detail/gwn_bvh_build_binary.cuh:29-129 (delta with the index tie-break);
 //   collapse rule: detail/gwn_bvh_build_collapse.cuh:163-199 (expand the internal candidate with
 //           the largest half-area, ties to the lower binary index, right child appended).
-// The collapse itself is restructured: one kernel per tree level allocates child node ids with a
+// The collapse itself is restructured: every tree level allocates its child node ids with a
 // decoupled look-back scan, which yields a canonical breadth-first node order directly (no
-// persistent work queue, no reorder sort).
+// persistent work queue, no reorder sort). A build enqueues the first 32 levels without a host
+// round trip (a level past the bottom exits at once) and learns from its single read-back whether
+// the tree was deeper.
 #include "gwnb_internal.cuh"
 
 #include <algorithm>
@@ -277,23 +279,60 @@ struct collapse_params {
     unsigned long long *tile_status; // tagged (level+1) << 34 | flag << 32 | value
     std::uint32_t *stack_bounds;     // [2]: internal, packed
     unsigned int *status;
+    std::uint64_t list_capacity;     // items per level list (binary internal node count)
+    long long wait_limit;            // polls before a look-back wait gives up (wait_limit())
 };
 
 constexpr unsigned long long k_ts_agg = 1ull << 32;
 constexpr unsigned long long k_ts_incl = 2ull << 32;
-constexpr long long k_collapse_spin_limit = 1ll << 22;
 
-__global__ void k_collapse_init(collapse_params p, std::uint32_t root_binary) {
-    p.lists[0][0] = collapse_item{root_binary, 0u, 0u};
-    p.level_count[0] = 1u;
-    p.level_base[0] = 0u;
+// Decoupled look-back of one collapse tile: publishes the tile's aggregate, adds the published
+// values of the tiles before it (tagged with this level, so a previous level's words never count)
+// until an inclusive prefix is found, publishes the inclusive prefix and returns the exclusive
+// one. A predecessor that stays unpublished for `limit` polls sets k_err_wait_timeout and ends the
+// wait with the prefix gathered so far, so the launch always completes.
+__device__ std::uint32_t collapse_tile_prefix(unsigned long long *st, std::uint32_t tile, unsigned long long tag,
+                                              std::uint32_t block_total, unsigned int *status, long long limit) {
+    std::uint32_t excl = 0;
+    if (tile == 0) {
+        atomicExch(&st[0], tag | k_ts_incl | block_total);
+        return 0;
+    }
+    atomicExch(&st[tile], tag | k_ts_agg | block_total);
+    long long spins = 0;
+    std::int64_t j = static_cast<std::int64_t>(tile) - 1;
+    while (j >= 0) {
+        unsigned long long const s = *reinterpret_cast<volatile unsigned long long *>(&st[j]);
+        if ((s & ~((1ull << 34) - 1)) != tag || (s & (3ull << 32)) == 0) {
+            if (++spins > limit) {
+                atomicOr(status, k_err_wait_timeout);
+                break;
+            }
+            continue;
+        }
+        excl += static_cast<std::uint32_t>(s & 0xffffffffull);
+        if ((s & (3ull << 32)) == k_ts_incl)
+            break;
+        --j;
+    }
+    atomicExch(&st[tile], tag | k_ts_incl | (excl + block_total));
+    return excl;
 }
 
+// One level of the collapse: blocks claim tiles of k_block items from the level's counter in launch
+// order (so a tile's look-back only ever waits on tiles claimed before it) until the level is
+// exhausted.
 __global__ void __launch_bounds__(k_block) k_collapse_level(collapse_params p, int level) {
     __shared__ std::uint32_t s_tile;
     __shared__ std::uint32_t s_prefix;
     __shared__ std::uint32_t s_scan[k_block / 32];
-    std::uint32_t const n_in = *reinterpret_cast<volatile std::uint32_t *>(&p.level_count[level]);
+    std::uint32_t n_in = *reinterpret_cast<volatile std::uint32_t *>(&p.level_count[level]);
+    if (n_in > p.list_capacity) {
+        // only a broken binary hierarchy can hold more items on one level than internal nodes
+        if (threadIdx.x == 0)
+            atomicOr(p.status, k_err_collapse);
+        n_in = 0;
+    }
     std::uint32_t const base = *reinterpret_cast<volatile std::uint32_t *>(&p.level_base[level]);
     collapse_item const *items_in = p.lists[level & 1];
     collapse_item *items_out = p.lists[(level + 1) & 1];
@@ -379,34 +418,8 @@ __global__ void __launch_bounds__(k_block) k_collapse_level(collapse_params p, i
         std::uint32_t const local_excl = warp_prefix + incl - k_int;
 
         // Decoupled look-back over tiles of this level.
-        if (tid == 0) {
-            unsigned long long *const st = p.tile_status;
-            std::uint32_t excl = 0;
-            if (tile == 0) {
-                atomicExch(&st[0], tag | k_ts_incl | block_total);
-            } else {
-                atomicExch(&st[tile], tag | k_ts_agg | block_total);
-                long long spins = 0;
-                std::int64_t j = static_cast<std::int64_t>(tile) - 1;
-                while (j >= 0) {
-                    unsigned long long const s =
-                        *reinterpret_cast<volatile unsigned long long *>(&st[j]);
-                    if ((s & ~((1ull << 34) - 1)) != tag || (s & (3ull << 32)) == 0) {
-                        if (++spins > k_collapse_spin_limit) {
-                            atomicOr(p.status, k_err_wait_timeout);
-                            break;
-                        }
-                        continue;
-                    }
-                    excl += static_cast<std::uint32_t>(s & 0xffffffffull);
-                    if ((s & (3ull << 32)) == k_ts_incl)
-                        break;
-                    --j;
-                }
-                atomicExch(&st[tile], tag | k_ts_incl | (excl + block_total));
-            }
-            s_prefix = excl;
-        }
+        if (tid == 0)
+            s_prefix = collapse_tile_prefix(p.tile_status, tile, tag, block_total, p.status, p.wait_limit);
         __syncthreads();
         std::uint32_t const tile_prefix = s_prefix;
         __syncthreads();
@@ -439,7 +452,10 @@ __global__ void __launch_bounds__(k_block) k_collapse_level(collapse_params p, i
                     std::uint32_t const id = id_first + m;
                     nd.c[c].bounds = p.binary_bounds[cidx[c]];
                     nd.c[c].reference = make_ref(id, 0u);
-                    items_out[out_first + m] = collapse_item{cidx[c], node_int, node_pk};
+                    if (static_cast<std::uint64_t>(out_first) + m < p.list_capacity)
+                        items_out[out_first + m] = collapse_item{cidx[c], node_int, node_pk};
+                    else
+                        atomicOr(p.status, k_err_collapse);
                     ++m;
                 }
             }
@@ -460,6 +476,32 @@ __global__ void __launch_bounds__(k_block) k_collapse_level(collapse_params p, i
             p.level_base[level + 1] = base + n_in;
         }
     }
+}
+
+// Starts the collapse at the binary root. The H-PLOC builder's cluster counter, when given, must
+// read 2n - 1 (a complete hierarchy), else the collapse reports an error and produces no nodes.
+__global__ void k_collapse_init(collapse_params p, std::uint32_t root_binary, std::uint32_t const *hploc_count,
+                                std::uint32_t hploc_expected) {
+    bool ok = true;
+    if (hploc_count != nullptr && *hploc_count != hploc_expected) {
+        atomicOr(p.status, k_err_hploc);
+        ok = false;
+    }
+    p.lists[0][0] = collapse_item{root_binary, 0u, 0u};
+    p.level_count[0] = ok ? 1u : 0u;
+    p.level_base[0] = 0u;
+}
+
+// Sizes after `levels` levels: the node count is the base of the first empty level and the stack
+// bounds the maxima the levels recorded; `pending` is set when level `levels` still holds items.
+__global__ void k_collapse_summary(collapse_params p, int levels, collapse_summary *summary) {
+    int l = 0;
+    while (l < levels && p.level_count[l] != 0u)
+        ++l;
+    summary->node_count = p.level_base[l];
+    summary->internal_bound = p.stack_bounds[0];
+    summary->packed_bound = p.stack_bounds[1];
+    summary->pending = p.level_count[l] != 0u ? 1u : 0u;
 }
 
 __global__ void __launch_bounds__(k_block)
@@ -485,13 +527,8 @@ __global__ void __launch_bounds__(k_block)
     float const e2x = __fsub_rn(g.vertex_x[c], ax), e2y = __fsub_rn(g.vertex_y[c], ay),
                 e2z = __fsub_rn(g.vertex_z[c], az);
     tris[i] = triangle{ax, ay, az, e1x, e1y, e1z, e2x, e2y, e2z};
-    if (tri48 != nullptr) {
-        float const nx = e1y * e2z - e1z * e2y;
-        float const ny = e1z * e2x - e1x * e2z;
-        float const nz = e1x * e2y - e1y * e2x;
-        tri48[i] = triangle48{make_float4(ax, ay, az, e1x), make_float4(e1y, e1z, e2x, e2y),
-                              make_float4(e2z, nx, ny, nz)};
-    }
+    if (tri48 != nullptr)
+        tri48[i] = make_triangle48(ax, ay, az, e1x, e1y, e1z, e2x, e2y, e2z);
 }
 
 inline unsigned grid_for(std::uint64_t n, int block = k_block) {
@@ -580,17 +617,20 @@ int build_binary_lbvh(void const *sorted_codes, int morton_bits, std::uint64_t n
 int build_binary_hploc(void const *sorted_codes, int morton_bits, std::uint64_t n,
                        aabb const *sorted_aabbs, std::uint32_t radius, binary_node *nodes,
                        std::uint32_t *internal_parent, aabb *internal_bounds, std::uint32_t *root,
-                       cudaStream_t s, unsigned int *status);
+                       cudaStream_t s, unsigned int *status, std::uint32_t *counter);
 
-// Collapse a binary hierarchy into canonical breadth-first BVH4 nodes. Synchronizes after the
-// first 24 levels and then every 8 to learn when the tree is exhausted (one synchronization for the
-// tree of the 1M-triangle sphere instead of three: 1.46 -> 1.43 ms per build).
+// Collapse a binary hierarchy into canonical breadth-first BVH4 nodes. With sync == false the first
+// k_async_levels levels are enqueued without a host round trip and *summary (device memory) says
+// whether the tree was deeper (summary->pending): the caller then repeats the collapse with sync ==
+// true, which continues level batches until one comes back empty. The node count and both stack
+// bounds land in *summary. hploc_count, when non-null, is the H-PLOC builder's cluster counter,
+// checked on the device against 2n - 1.
 int collapse_to_bvh4(binary_node const *binary, aabb const *binary_bounds, aabb const *leaf_aabbs,
-                     std::uint64_t leaf_count, std::uint32_t root_binary, node4 *nodes,
-                     std::uint64_t node_capacity, std::uint64_t *node_count,
-                     std::uint32_t *internal_bound, std::uint32_t *packed_bound, cudaStream_t s,
-                     unsigned int *status) {
+                     std::uint64_t leaf_count, std::uint32_t root_binary, std::uint32_t const *hploc_count,
+                     node4 *nodes, std::uint64_t node_capacity, collapse_summary *summary, bool sync,
+                     cudaStream_t s, unsigned int *status) {
     constexpr int k_max_levels = 4096;
+    constexpr int k_async_levels = 32;
     std::uint64_t const ni = leaf_count - 1;
     std::uint64_t const max_tiles = (ni + k_block - 1) / k_block;
     collapse_params p{};
@@ -600,6 +640,8 @@ int collapse_to_bvh4(binary_node const *binary, aabb const *binary_bounds, aabb 
     p.leaf_count = leaf_count;
     p.nodes = nodes;
     p.node_capacity = node_capacity;
+    p.list_capacity = ni;
+    p.wait_limit = wait_limit();
     std::uint32_t *words = nullptr;
     std::size_t const nwords = 3 * (k_max_levels + 1) + 2;
     GWNB_TRY(alloc(&p.lists[0], ni, s));
@@ -613,49 +655,55 @@ int collapse_to_bvh4(binary_node const *binary, aabb const *binary_bounds, aabb 
     p.tile_counter = words + 2 * (k_max_levels + 1);
     p.stack_bounds = words + 3 * (k_max_levels + 1);
     p.status = status;
-    note_launch(), k_collapse_init<<<1, 1, 0, s>>>(p, root_binary);
-    int const sms = device_sm_count();
-    unsigned const grid = static_cast<unsigned>(std::min<std::uint64_t>(max_tiles, static_cast<std::uint64_t>(sms) * 4));
-    std::vector<std::uint32_t> host_counts(k_max_levels + 1);
+    note_launch(), k_collapse_init<<<1, 1, 0, s>>>(p, root_binary, hploc_count,
+                                                   static_cast<std::uint32_t>(2 * leaf_count - 1));
+    unsigned const grid = static_cast<unsigned>(
+        std::min<std::uint64_t>(max_tiles, static_cast<std::uint64_t>(device_sm_count()) * 4));
     int level = 0;
-    bool done = false;
-    while (!done) {
-        // the first batch covers the depth of trees up to ~10M triangles without a host round
-        // trip (a level past the bottom returns at once); deeper trees continue 8 levels at a time
-        int const batch = level == 0 ? 24 : 8;
+    for (;;) {
+        int const batch = sync && level > 0 ? 8 : k_async_levels;
         for (int b = 0; b < batch && level < k_max_levels; ++b, ++level)
             note_launch(), k_collapse_level<<<grid, k_block, 0, s>>>(p, level);
         GWNB_CUDA_TRY(cudaGetLastError());
+        if (!sync)
+            break;
         std::uint32_t c = 0;
         GWNB_CUDA_TRY(cudaMemcpyAsync(&c, p.level_count + level, sizeof(c), cudaMemcpyDeviceToHost, s));
         GWNB_CUDA_TRY(cudaStreamSynchronize(s));
         if (c == 0)
-            done = true;
-        else if (level >= k_max_levels)
+            break;
+        if (level >= k_max_levels)
             return set_error(GWNB_INTERNAL_ERROR, "bvh.build.collapse: tree deeper than 4096 levels.");
     }
-    std::vector<std::uint32_t> counts(level + 1), bases(level + 1);
-    std::uint32_t sb[2] = {0, 0};
-    GWNB_CUDA_TRY(cudaMemcpyAsync(counts.data(), p.level_count, (level + 1) * sizeof(std::uint32_t),
-                                  cudaMemcpyDeviceToHost, s));
-    GWNB_CUDA_TRY(cudaMemcpyAsync(bases.data(), p.level_base, (level + 1) * sizeof(std::uint32_t),
-                                  cudaMemcpyDeviceToHost, s));
-    GWNB_CUDA_TRY(cudaMemcpyAsync(sb, p.stack_bounds, sizeof(sb), cudaMemcpyDeviceToHost, s));
-    GWNB_CUDA_TRY(cudaStreamSynchronize(s));
-    std::uint64_t total = 0;
-    for (int l = 0; l <= level; ++l) {
-        if (counts[l] == 0) {
-            total = bases[l];
-            break;
-        }
-    }
-    *node_count = total;
-    *internal_bound = sb[0];
-    *packed_bound = sb[1];
+    note_launch(), k_collapse_summary<<<1, 1, 0, s>>>(p, level, summary);
+    GWNB_CUDA_TRY(cudaGetLastError());
     release(p.lists[0], s);
     release(p.lists[1], s);
     release(words, s);
     release(p.tile_status, s);
+    return GWNB_OK;
+}
+
+namespace {
+// Tile 1 of a level waits on tile 0, which nothing publishes.
+__global__ void k_collapse_wait_probe(unsigned long long *st, unsigned int *status, long long limit) {
+    if (blockIdx.x == 0 && threadIdx.x == 0)
+        (void)collapse_tile_prefix(st, 1u, 1ull << 34, 1u, status, limit);
+}
+} // namespace
+
+// The collapse's look-back wait on a predecessor tile that is never published: one thread runs the
+// wait of tile 1 against a zeroed tile-status array; it gives up after wait_limit() polls and sets
+// k_err_wait_timeout in *status.
+int collapse_wait_probe(unsigned int *status, cudaStream_t s) {
+    unsigned long long *st = nullptr;
+    GWNB_TRY(alloc(&st, 2, s));
+    GWNB_CUDA_TRY(cudaMemsetAsync(st, 0, 2 * sizeof(unsigned long long), s));
+    note_launch(), k_collapse_wait_probe<<<1, 32, 0, s>>>(st, status, wait_limit());
+    cudaError_t const e = cudaGetLastError();
+    release(st, s);
+    if (e != cudaSuccess)
+        return set_cuda_error(e, "collapse wait probe");
     return GWNB_OK;
 }
 

@@ -38,6 +38,12 @@ int set_cuda_error(cudaError_t err, char const *what) {
 
 std::atomic<std::uint64_t> g_launch_count{0};
 
+namespace {
+std::atomic<long long> g_wait_limit{k_default_wait_limit};
+} // namespace
+
+long long wait_limit() { return g_wait_limit.load(std::memory_order_relaxed); }
+
 int host_exception() noexcept {
     char const *what = "Unhandled unknown exception.";
     std::string detail;
@@ -117,11 +123,16 @@ int build_binary_lbvh(void const *sorted_codes, int morton_bits, std::uint64_t n
                       cudaStream_t s, unsigned int *status);
 int build_binary_hploc(void const *sorted_codes, int morton_bits, std::uint64_t n, aabb const *sorted_aabbs,
                        std::uint32_t radius, binary_node *nodes, std::uint32_t *internal_parent,
-                       aabb *internal_bounds, std::uint32_t *root, cudaStream_t s, unsigned int *status);
+                       aabb *internal_bounds, std::uint32_t *root, cudaStream_t s, unsigned int *status,
+                       std::uint32_t *counter);
 int collapse_to_bvh4(binary_node const *binary, aabb const *binary_bounds, aabb const *leaf_aabbs,
-                     std::uint64_t leaf_count, std::uint32_t root_binary, node4 *nodes,
-                     std::uint64_t node_capacity, std::uint64_t *node_count, std::uint32_t *internal_bound,
-                     std::uint32_t *packed_bound, cudaStream_t s, unsigned int *status);
+                     std::uint64_t leaf_count, std::uint32_t root_binary, std::uint32_t const *hploc_count,
+                     node4 *nodes, std::uint64_t node_capacity, collapse_summary *summary, bool sync,
+                     cudaStream_t s, unsigned int *status);
+int prepare_bvh_aux_async(gwnb_bvh4_f32 *bvh, std::uint64_t node_capacity, collapse_summary const *summary,
+                          std::uint32_t *leaf_node_count, cudaStream_t s);
+int onesweep_wait_probe(unsigned int *status, cudaStream_t s);
+int collapse_wait_probe(unsigned int *status, cudaStream_t s);
 int build_triangles(gwnb_geometry_f32 const &g, std::uint32_t const *ids, std::uint64_t n, triangle *tris,
                     triangle48 *tri48, cudaStream_t s, unsigned int *status);
 int refit_bounds_async(gwnb_geometry_f32 const &g, gwnb_bvh4_f32 *bvh, cudaStream_t s);
@@ -203,6 +214,19 @@ int read_status(gwnb_bvh4_f32 const *b, unsigned int *out, cudaStream_t s) {
     return GWNB_OK;
 }
 
+// Device-side results of a build, read back in one copy at its end.
+struct build_readback {
+    collapse_summary collapse;
+    aabb root_bounds;
+    unsigned int status;
+    std::uint32_t leaf_node_count;
+    std::uint32_t hploc_count;
+    std::uint32_t pad;
+};
+
+// The build enqueues every stage on the stream without a host round trip (the H-PLOC convergence
+// check, the collapse's depth and node count, the leaf-node list of the refit state all stay on
+// the device) and synchronizes once, to read the tree's sizes, bounds and error word.
 int build_impl(gwnb_geometry_f32 const *g, int method, std::uint32_t radius, int morton_bits,
                gwnb_bvh4_f32 *out, cudaStream_t s) {
     std::uint64_t const nt = g->triangle_count;
@@ -219,12 +243,14 @@ int build_impl(gwnb_geometry_f32 const *g, int method, std::uint32_t radius, int
     binary_node *bin = nullptr;
     std::uint32_t *bin_parent = nullptr;
     aabb *bin_bounds = nullptr;
+    build_readback *rb = nullptr;
     auto cleanup = [&]() {
         release(codes, s);
         release(sorted_aabbs, s);
         release(bin, s);
         release(bin_parent, s);
         release(bin_bounds, s);
+        release(rb, s);
     };
     auto fail = [&](int code) {
         cleanup();
@@ -240,63 +266,101 @@ int build_impl(gwnb_geometry_f32 const *g, int method, std::uint32_t radius, int
         return fail(rc);
     if ((rc = alloc(&sorted_aabbs, nt, s)) != GWNB_OK)
         return fail(rc);
+    if ((rc = alloc(&rb, 1, s)) != GWNB_OK)
+        return fail(rc);
+    GWNB_CUDA_TRY(cudaMemsetAsync(rb, 0, sizeof(build_readback), s));
     if ((rc = build_preprocess(*g, morton_bits, codes, b.primitive_indices, sorted_aabbs, s, status)) != GWNB_OK)
         return fail(rc);
-    aabb root_bounds{};
+    std::uint64_t capacity = 0;
+    std::uint32_t root_binary = 0;
     if (nt == 1) {
-        GWNB_CUDA_TRY(cudaMemcpyAsync(&root_bounds, sorted_aabbs, sizeof(aabb), cudaMemcpyDeviceToHost, s));
+        GWNB_CUDA_TRY(cudaMemcpyAsync(&rb->root_bounds, sorted_aabbs, sizeof(aabb), cudaMemcpyDeviceToDevice, s));
         b.root.reference = make_ref(0, 1);
     } else {
         std::uint64_t const ni = nt - 1;
         if ((rc = alloc(&bin, ni, s)) != GWNB_OK || (rc = alloc(&bin_parent, ni, s)) != GWNB_OK ||
             (rc = alloc(&bin_bounds, ni, s)) != GWNB_OK)
             return fail(rc);
-        std::uint32_t root_binary = 0;
+        root_binary = 0;
+        std::uint32_t *hploc_count = nullptr;
         if (method == GWNB_METHOD_LBVH) {
             rc = build_binary_lbvh(codes, morton_bits, nt, sorted_aabbs, bin, bin_parent, bin_bounds, s, status);
         } else {
+            hploc_count = &rb->hploc_count;
             rc = build_binary_hploc(codes, morton_bits, nt, sorted_aabbs, radius, bin, bin_parent, bin_bounds,
-                                    &root_binary, s, status);
+                                    &root_binary, s, status, hploc_count);
         }
         if (rc != GWNB_OK)
             return fail(rc);
-        GWNB_CUDA_TRY(cudaMemcpyAsync(&root_bounds, bin_bounds + root_binary, sizeof(aabb), cudaMemcpyDeviceToHost, s));
+        GWNB_CUDA_TRY(cudaMemcpyAsync(&rb->root_bounds, bin_bounds + root_binary, sizeof(aabb),
+                                      cudaMemcpyDeviceToDevice, s));
         if ((rc = alloc(reinterpret_cast<node4 **>(&b.nodes), ni, s)) != GWNB_OK)
             return fail(rc);
         b.node_capacity = ni;
-        std::uint64_t node_count = 0;
-        if ((rc = collapse_to_bvh4(bin, bin_bounds, sorted_aabbs, nt, root_binary,
-                                   reinterpret_cast<node4 *>(b.nodes), ni, &node_count, &b.internal_stack_bound,
-                                   &b.packed_stack_bound, s, status)) != GWNB_OK)
+        capacity = ni;
+        if ((rc = collapse_to_bvh4(bin, bin_bounds, sorted_aabbs, nt, root_binary, hploc_count,
+                                   reinterpret_cast<node4 *>(b.nodes), ni, &rb->collapse, false, s, status)) != GWNB_OK)
             return fail(rc);
-        b.node_count = node_count;
         b.root.reference = make_ref(0, 0);
     }
-    if ((rc = build_triangles(*g, b.primitive_indices, nt, reinterpret_cast<triangle *>(b.triangles), nullptr,
+    // refit / query state: parent links and leaf-node list over the collapsed nodes (sized by the
+    // node capacity; the kernels read the node count from the device), padded triangle records
+    // written with the leaf-ordered ones
+    if ((rc = prepare_bvh_aux_async(&b, capacity, &rb->collapse, &rb->leaf_node_count, s)) != GWNB_OK)
+        return fail(rc);
+    if ((rc = build_triangles(*g, b.primitive_indices, nt, reinterpret_cast<triangle *>(b.triangles), aux->tri48,
                               s, status)) != GWNB_OK)
         return fail(rc);
-    unsigned int host_status = 0;
-    if ((rc = read_status(&b, &host_status, s)) != GWNB_OK)
-        return fail(rc);
-    if (host_status != 0u) {
-        if (host_status & k_err_index)
+    GWNB_CUDA_TRY(cudaMemcpyAsync(aux->root_bounds, &rb->root_bounds, sizeof(aabb), cudaMemcpyDeviceToDevice, s));
+    GWNB_CUDA_TRY(cudaMemcpyAsync(&rb->status, status, sizeof(unsigned int), cudaMemcpyDeviceToDevice, s));
+    build_readback host{};
+    GWNB_CUDA_TRY(cudaMemcpyAsync(&host, rb, sizeof(host), cudaMemcpyDeviceToHost, s));
+    GWNB_CUDA_TRY(cudaStreamSynchronize(s));
+    if (host.status == 0u && nt > 1 && host.collapse.pending != 0u) {
+        // a tree deeper than the levels enqueued up front: collapse again level batch by level batch,
+        // then derive the refit state again from the complete nodes
+        if ((rc = collapse_to_bvh4(bin, bin_bounds, sorted_aabbs, nt, root_binary, nullptr,
+                                   reinterpret_cast<node4 *>(b.nodes), capacity, &rb->collapse, true, s, status)) !=
+            GWNB_OK)
+            return fail(rc);
+        if ((rc = prepare_bvh_aux_async(&b, capacity, &rb->collapse, &rb->leaf_node_count, s)) != GWNB_OK)
+            return fail(rc);
+        if ((rc = build_triangles(*g, b.primitive_indices, nt, reinterpret_cast<triangle *>(b.triangles), aux->tri48,
+                                  s, status)) != GWNB_OK)
+            return fail(rc);
+        GWNB_CUDA_TRY(cudaMemcpyAsync(&rb->status, status, sizeof(unsigned int), cudaMemcpyDeviceToDevice, s));
+        GWNB_CUDA_TRY(cudaMemcpyAsync(&host, rb, sizeof(host), cudaMemcpyDeviceToHost, s));
+        GWNB_CUDA_TRY(cudaStreamSynchronize(s));
+    }
+    if (host.status != 0u) {
+        if (host.status & k_err_index)
             return fail(set_error(GWNB_INTERNAL_ERROR,
                                   "bvh.build: Leaf-ordered triangle construction encountered invalid geometry."));
+        if (host.status & k_err_hploc)
+            return fail(set_error(GWNB_INTERNAL_ERROR,
+                                  "bvh.build.binary.hploc: H-PLOC builder did not converge to a complete binary hierarchy."));
         return fail(set_error(GWNB_INTERNAL_ERROR, "bvh.build: device builder reported an inconsistent hierarchy (status " +
-                                                       std::to_string(host_status) + ")."));
+                                                       std::to_string(host.status) + ")."));
     }
-    if (nt > 1 && b.node_count == 0)
-        return fail(set_error(GWNB_INTERNAL_ERROR, "bvh.build.collapse: collapse produced no nodes."));
-    std::memcpy(&b.root.bounds, &root_bounds, sizeof(aabb));
+    if (nt > 1) {
+        b.node_count = host.collapse.node_count;
+        b.internal_stack_bound = host.collapse.internal_bound;
+        b.packed_stack_bound = host.collapse.packed_bound;
+        if (b.node_count == 0)
+            return fail(set_error(GWNB_INTERNAL_ERROR, "bvh.build.collapse: collapse produced no nodes."));
+    }
+    aux->leaf_node_count = host.leaf_node_count;
+    std::memcpy(&b.root.bounds, &host.root_bounds, sizeof(aabb));
     cleanup();
     b.revision = reserve_revision();
     if (b.revision == 0)
         return fail(set_error(GWNB_INTERNAL_ERROR, "bvh.build: BVH geometry-derived state revision is exhausted."));
-    // Derived state for refit/query (parent links, padded triangle records).
-    if ((rc = ensure_bvh_aux(&b, s)) != GWNB_OK)
-        return fail(rc);
-    GWNB_CUDA_TRY(cudaMemcpyAsync(aux->root_bounds, &b.root.bounds, sizeof(aabb), cudaMemcpyHostToDevice, s));
-    GWNB_CUDA_TRY(cudaStreamSynchronize(s));
+    aux->nodes_ptr = b.nodes;
+    aux->triangles_ptr = b.triangles;
+    aux->node_count = b.node_count;
+    aux->primitive_count = b.primitive_count;
+    aux->revision = b.revision;
+    aux->derived = true;
     *out = b;
     return GWNB_OK;
 }
@@ -322,6 +386,43 @@ int gwnb_memory_stats(uint64_t *reserved, uint64_t *used) try {
         *reserved = r;
     if (used != nullptr)
         *used = u;
+    return GWNB_OK;
+} catch (...) {
+    return host_exception();
+}
+
+int gwnb_set_wait_limit(int64_t polls) try {
+    g_wait_limit.store(polls > 0 ? static_cast<long long>(polls) : k_default_wait_limit, std::memory_order_relaxed);
+    return GWNB_OK;
+} catch (...) {
+    return host_exception();
+}
+
+int gwnb_wait_timeout_probe(int stage, gwnb_stream_t stream) try {
+    if (stage != 0 && stage != 1)
+        return set_error(GWNB_INVALID_ARGUMENT, "wait probe: stage must be 0 (radix sort) or 1 (BVH4 collapse).");
+    cudaStream_t const s = as_cuda(stream);
+    unsigned int *status = nullptr;
+    GWNB_TRY(alloc(&status, 1, s));
+    int rc = GWNB_OK;
+    if (cudaMemsetAsync(status, 0, sizeof(unsigned int), s) != cudaSuccess)
+        rc = set_cuda_error(cudaGetLastError(), "wait probe status");
+    if (rc == GWNB_OK)
+        rc = stage == 0 ? onesweep_wait_probe(status, s) : collapse_wait_probe(status, s);
+    unsigned int host = 0;
+    if (rc == GWNB_OK) {
+        cudaError_t e = cudaMemcpyAsync(&host, status, sizeof(host), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess)
+            e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess)
+            rc = set_cuda_error(e, "wait probe status read-back");
+    }
+    release(status, s);
+    if (rc != GWNB_OK)
+        return rc;
+    if (host & k_err_wait_timeout)
+        return set_error(GWNB_INTERNAL_ERROR, std::string(stage == 0 ? "radix sort" : "BVH4 collapse") +
+                                                  ": device wait timed out (predecessor tile never published).");
     return GWNB_OK;
 } catch (...) {
     return host_exception();
@@ -534,7 +635,7 @@ int gwnb_build_binary_hploc(const void *sorted_codes, int morton_bits, uint64_t 
     GWNB_CUDA_TRY(cudaMemsetAsync(status, 0, sizeof(unsigned int), s));
     int const rc = build_binary_hploc(sorted_codes, morton_bits, n, reinterpret_cast<aabb const *>(sorted_aabbs), radius,
                                       reinterpret_cast<binary_node *>(nodes), internal_parent,
-                                      reinterpret_cast<aabb *>(internal_bounds), root, s, status);
+                                      reinterpret_cast<aabb *>(internal_bounds), root, s, status, nullptr);
     release(status, s);
     return rc;
 } catch (...) {

@@ -261,19 +261,25 @@ __global__ void k_iota(std::uint32_t *v, std::uint32_t n) {
 
 } // namespace
 
+// H-PLOC over n sorted leaves. The cluster counter ends at 2n - 1 when the hierarchy is complete,
+// and the root is then internal node n - 2. With a caller-owned `counter` (one device word that
+// must outlive the check) the call only enqueues work and the caller checks the counter on the
+// device; with counter == nullptr it synchronizes the stream and checks it on the host.
 int build_binary_hploc(void const *sorted_codes, int morton_bits, std::uint64_t n,
                        aabb const *sorted_aabbs, std::uint32_t radius, binary_node *nodes,
                        std::uint32_t *internal_parent, aabb *internal_bounds, std::uint32_t *root,
-                       cudaStream_t s, unsigned int *status) {
+                       cudaStream_t s, unsigned int *status, std::uint32_t *counter) {
     *root = k_invalid_u32;
     if (n < 2)
         return GWNB_OK;
     if (n > 0x7fffffffull)
         return set_error(GWNB_INVALID_ARGUMENT, "bvh.build.binary.hploc: too many primitives.");
-    std::uint32_t *cluster = nullptr, *boundary = nullptr, *counter = nullptr;
+    bool const deferred_check = counter != nullptr;
+    std::uint32_t *cluster = nullptr, *boundary = nullptr;
     GWNB_TRY(alloc(&cluster, n, s));
     GWNB_TRY(alloc(&boundary, n, s));
-    GWNB_TRY(alloc(&counter, 1, s));
+    if (!deferred_check)
+        GWNB_TRY(alloc(&counter, 1, s));
     GWNB_CUDA_TRY(cudaMemsetAsync(boundary, 0xff, n * sizeof(std::uint32_t), s));
     GWNB_CUDA_TRY(cudaMemsetAsync(internal_parent, 0xff, (n - 1) * sizeof(std::uint32_t), s));
     std::uint32_t const n32 = static_cast<std::uint32_t>(n);
@@ -287,6 +293,12 @@ int build_binary_hploc(void const *sorted_codes, int morton_bits, std::uint64_t 
     else
         note_launch(), k_hploc<std::uint64_t><<<grid, k_hploc_block, 0, s>>>(p, static_cast<std::uint64_t const *>(sorted_codes));
     GWNB_CUDA_TRY(cudaGetLastError());
+    if (deferred_check) {
+        release(cluster, s);
+        release(boundary, s);
+        *root = n32 - 2;
+        return GWNB_OK;
+    }
     std::uint32_t host_count = 0;
     unsigned int host_status = 0;
     GWNB_CUDA_TRY(cudaMemcpyAsync(&host_count, counter, sizeof(host_count), cudaMemcpyDeviceToHost, s));

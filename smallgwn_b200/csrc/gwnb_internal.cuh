@@ -60,6 +60,27 @@ struct alignas(16) triangle48 {
     float4 a, b, c;
 };
 
+// The padded record of one triangle: {v0, e1.x | e1.yz, e2.xy | e2.z, n} with n = e1 x e2 in one
+// fixed rounding pattern (each component: one product rounded, then one fused multiply-add), so
+// every kernel that writes padded records (build, refit, derivation from plain records) stores the
+// same bits for the same triangle.
+__device__ __forceinline__ triangle48 make_triangle48(float ax, float ay, float az, float e1x, float e1y, float e1z,
+                                                      float e2x, float e2y, float e2z) {
+    float const nx = __fmaf_rn(e1y, e2z, -__fmul_rn(e1z, e2y));
+    float const ny = __fmaf_rn(e1z, e2x, -__fmul_rn(e1x, e2z));
+    float const nz = __fmaf_rn(e1x, e2y, -__fmul_rn(e1y, e2x));
+    return triangle48{make_float4(ax, ay, az, e1x), make_float4(e1y, e1z, e2x, e2y), make_float4(e2z, nx, ny, nz)};
+}
+
+// Sizes of a collapsed BVH4, written by the device for the single read-back that ends a build.
+struct collapse_summary {
+    unsigned long long node_count;
+    std::uint32_t internal_bound;
+    std::uint32_t packed_bound;
+    std::uint32_t pending; // the levels enqueued did not reach the bottom of the tree
+    std::uint32_t pad;
+};
+
 struct binary_node {
     std::uint32_t left_index, left_kind, right_index, right_kind;
 };
@@ -187,6 +208,12 @@ int host_exception() noexcept;
 
 std::uint64_t reserve_revision();
 int device_sm_count();
+
+// Polls after which a device-side wait (the look-back of the radix sort and of the BVH4 collapse)
+// gives up, sets k_err_wait_timeout and lets its launch complete. Read by the host when a kernel is
+// launched; 2^22 by default, settable with gwnb_set_wait_limit.
+constexpr long long k_default_wait_limit = 1ll << 22;
+long long wait_limit();
 
 // Counts the kernel launches the library issues (every launch site is `note_launch(), k<<<...>>>`);
 // gwnb_launch_count reports the total. A launch recorded into a CUDA graph counts once, at capture.

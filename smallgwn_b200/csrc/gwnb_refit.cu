@@ -25,11 +25,20 @@ constexpr int k_block = 128;
 
 // ---- aux preparation ---------------------------------------------------------------------------
 
+// summary, when non-null, is a build's device-side collapse summary (the build has not read it back
+// yet and launches over its node capacity): its node count bounds the nodes, and a collapse that
+// has not reached the bottom of the tree yet (pending) leaves nothing to derive.
 __global__ void __launch_bounds__(256)
     k_prepare_aux(node4 const *__restrict__ nodes, std::uint64_t node_count,
                   std::uint64_t primitive_count, std::uint32_t *__restrict__ parent_slot,
                   std::uint32_t *__restrict__ expected, std::uint32_t *__restrict__ leaf_nodes,
-                  std::uint32_t *leaf_node_counter, unsigned int *status) {
+                  std::uint32_t *leaf_node_counter, unsigned int *status, collapse_summary const *summary) {
+    if (summary != nullptr) {
+        if (summary->pending != 0u)
+            return;
+        if (summary->node_count < node_count)
+            node_count = summary->node_count;
+    }
     std::uint64_t const n = static_cast<std::uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (n >= node_count)
         return;
@@ -95,14 +104,8 @@ __device__ inline tri_payload make_triangle(gwnb_geometry_f32 const &g, std::uin
 
 __device__ inline void store_tri(triangle *tris, triangle48 *tri48, std::uint64_t i, triangle const &t) {
     tris[i] = t;
-    if (tri48 != nullptr) {
-        float const nx = t.e1_y * t.e2_z - t.e1_z * t.e2_y;
-        float const ny = t.e1_z * t.e2_x - t.e1_x * t.e2_z;
-        float const nz = t.e1_x * t.e2_y - t.e1_y * t.e2_x;
-        tri48[i] = triangle48{make_float4(t.v0_x, t.v0_y, t.v0_z, t.e1_x),
-                              make_float4(t.e1_y, t.e1_z, t.e2_x, t.e2_y),
-                              make_float4(t.e2_z, nx, ny, nz)};
-    }
+    if (tri48 != nullptr)
+        tri48[i] = make_triangle48(t.v0_x, t.v0_y, t.v0_z, t.e1_x, t.e1_y, t.e1_z, t.e2_x, t.e2_y, t.e2_z);
 }
 
 __device__ inline aabb load_bounds_cg(node4 const *nodes, std::uint64_t n, int s) {
@@ -772,7 +775,7 @@ int ensure_bvh_aux(gwnb_bvh4_f32 *bvh, cudaStream_t s) {
         GWNB_CUDA_TRY(cudaMemsetAsync(a->leaf_nodes + nn, 0, sizeof(std::uint32_t), s));
         note_launch(), k_prepare_aux<<<grid_for(nn, 256), 256, 0, s>>>(
             reinterpret_cast<node4 const *>(bvh->nodes), nn, bvh->primitive_count, a->parent_slot,
-            a->expected, a->leaf_nodes, a->leaf_nodes + nn, a->status);
+            a->expected, a->leaf_nodes, a->leaf_nodes + nn, a->status, nullptr);
         GWNB_CUDA_TRY(cudaGetLastError());
         std::uint32_t count = 0;
         GWNB_CUDA_TRY(cudaMemcpyAsync(&count, a->leaf_nodes + nn, sizeof(count), cudaMemcpyDeviceToHost, s));
@@ -786,6 +789,36 @@ int ensure_bvh_aux(gwnb_bvh4_f32 *bvh, cudaStream_t s) {
     a->node_count = nn;
     a->primitive_count = bvh->primitive_count;
     a->revision = bvh->revision;
+    return GWNB_OK;
+}
+
+int prepare_bvh_aux_async(gwnb_bvh4_f32 *bvh, std::uint64_t cap, collapse_summary const *summary,
+                          std::uint32_t *leaf_node_count, cudaStream_t s) {
+    GWNB_TRY(create_bvh_aux(bvh, s));
+    auto *a = reinterpret_cast<bvh_aux_impl *>(bvh->aux);
+    release(a->parent_slot, s);
+    release(a->expected, s);
+    release(a->arrivals, s);
+    release(a->leaf_nodes, s);
+    release(a->tri48, s);
+    a->leaf_node_count = 0;
+    a->derived = false;
+    GWNB_TRY(alloc(&a->tri48, std::max<std::uint64_t>(bvh->primitive_count, 1), s));
+    if (cap == 0)
+        return GWNB_OK;
+    GWNB_TRY(alloc(&a->parent_slot, cap, s));
+    GWNB_TRY(alloc(&a->expected, cap, s));
+    GWNB_TRY(alloc(&a->arrivals, 2 * cap, s));
+    GWNB_TRY(alloc(&a->leaf_nodes, cap + 1, s));
+    GWNB_CUDA_TRY(cudaMemsetAsync(a->parent_slot, 0xff, cap * sizeof(std::uint32_t), s));
+    GWNB_CUDA_TRY(cudaMemsetAsync(a->arrivals, 0, 2 * cap * sizeof(std::uint32_t), s));
+    GWNB_CUDA_TRY(cudaMemsetAsync(a->leaf_nodes + cap, 0, sizeof(std::uint32_t), s));
+    note_launch(), k_prepare_aux<<<grid_for(cap, 256), 256, 0, s>>>(
+        reinterpret_cast<node4 const *>(bvh->nodes), cap, bvh->primitive_count, a->parent_slot, a->expected,
+        a->leaf_nodes, a->leaf_nodes + cap, a->status, summary);
+    GWNB_CUDA_TRY(cudaGetLastError());
+    GWNB_CUDA_TRY(cudaMemcpyAsync(leaf_node_count, a->leaf_nodes + cap, sizeof(std::uint32_t), cudaMemcpyDeviceToDevice,
+                                  s));
     return GWNB_OK;
 }
 

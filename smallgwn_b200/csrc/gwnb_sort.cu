@@ -21,7 +21,6 @@ constexpr int k_warps = k_threads / 32;
 constexpr std::uint32_t k_flag_agg = 1u << 30;
 constexpr std::uint32_t k_flag_incl = 2u << 30;
 constexpr std::uint32_t k_value_mask = (1u << 30) - 1u;
-constexpr long long k_spin_limit = 1ll << 22;
 
 template <class K> struct sort_items;
 template <> struct sort_items<std::uint32_t> { static constexpr int value = 16; };
@@ -91,7 +90,7 @@ __global__ void __launch_bounds__(k_threads)
     k_onesweep(K const *__restrict__ keys_in, std::uint32_t const *__restrict__ vals_in,
                K *__restrict__ keys_out, std::uint32_t *__restrict__ vals_out, std::uint64_t n,
                int shift, std::uint32_t mask, std::uint32_t const *__restrict__ hist,
-               std::uint32_t *tile_status, std::uint32_t *tile_counter, unsigned int *status) {
+               std::uint32_t *tile_status, std::uint32_t *tile_counter, unsigned int *status, long long wait_limit) {
     constexpr int k_tile = k_threads * Items;
     __shared__ std::uint32_t s_warp_hist[k_warps][256];
     __shared__ std::uint32_t s_block_excl[256];
@@ -182,7 +181,7 @@ __global__ void __launch_bounds__(k_threads)
                     *reinterpret_cast<volatile std::uint32_t *>(&tile_status[j * 256 + d]);
                 std::uint32_t const f = s & ~k_value_mask;
                 if (f == 0u) {
-                    if (++spins > k_spin_limit) {
+                    if (++spins > wait_limit) {
                         atomicOr(status, k_err_wait_timeout);
                         break;
                     }
@@ -258,6 +257,7 @@ int sort_impl(K const *keys_in, K *keys_out, std::uint32_t const *vals_in,
     note_launch(), k_sort_histogram<K><<<hist_grid, k_threads, 0, s>>>(keys_in, n, passes, key_bits, hist);
 
     // Ping-pong so that the last pass lands in the output buffers.
+    long long const limit = wait_limit();
     bool to_out = (passes % 2) == 1;
     K const *src_k = keys_in;
     std::uint32_t const *src_v = vals_in;
@@ -268,7 +268,7 @@ int sort_impl(K const *keys_in, K *keys_out, std::uint32_t const *vals_in,
         std::uint32_t const mask = (1u << bits) - 1u;
         note_launch(), k_onesweep<K, k_items><<<static_cast<unsigned>(tiles), k_threads, 0, s>>>(
             src_k, src_v, dst_k, dst_v, n, 8 * p, mask, hist + p * 256,
-            tile_status + static_cast<std::size_t>(p) * tiles * 256, counters + p, status);
+            tile_status + static_cast<std::size_t>(p) * tiles * 256, counters + p, status, limit);
         src_k = dst_k;
         src_v = dst_v;
         to_out = !to_out;
@@ -301,6 +301,7 @@ int sort_in_scratch(K const *keys_in, K *keys_out, std::uint32_t const *vals_in,
     unsigned const hist_grid = static_cast<unsigned>(
         std::min<std::uint64_t>((n + k_threads - 1) / k_threads, static_cast<std::uint64_t>(sms) * 8));
     note_launch(), k_sort_histogram<K><<<hist_grid, k_threads, 0, s>>>(keys_in, n, passes, key_bits, hist);
+    long long const limit = wait_limit();
     bool to_out = (passes % 2) == 1;
     K const *src_k = keys_in;
     std::uint32_t const *src_v = vals_in;
@@ -311,7 +312,7 @@ int sort_in_scratch(K const *keys_in, K *keys_out, std::uint32_t const *vals_in,
         std::uint32_t const mask = (1u << bits) - 1u;
         note_launch(), k_onesweep<K, k_items><<<static_cast<unsigned>(tiles), k_threads, 0, s>>>(
             src_k, src_v, dst_k, dst_v, n, 8 * p, mask, hist + p * 256,
-            tile_status + static_cast<std::size_t>(p) * tiles * 256, counters + p, status);
+            tile_status + static_cast<std::size_t>(p) * tiles * 256, counters + p, status, limit);
         src_k = dst_k;
         src_v = dst_v;
         to_out = !to_out;
@@ -321,6 +322,40 @@ int sort_in_scratch(K const *keys_in, K *keys_out, std::uint32_t const *vals_in,
 }
 
 } // namespace
+
+// One real onesweep pass whose first tile is never processed: two tiles of keys, the tile counter
+// starting at 1 and one block, so the block takes tile 1 and its look-back waits on tile 0, which
+// nothing publishes. The wait gives up after wait_limit() polls and sets k_err_wait_timeout in
+// *status; every access stays inside the two-tile buffers (tile 1's prefix is then what it gathered
+// before giving up, zero, and its keys land in the first tile's positions).
+int onesweep_wait_probe(unsigned int *status, cudaStream_t s) {
+    constexpr int k_items = sort_items<std::uint32_t>::value;
+    constexpr std::uint64_t k_tile = static_cast<std::uint64_t>(k_threads) * k_items;
+    constexpr std::uint64_t n = 2 * k_tile;
+    std::uint32_t *keys = nullptr, *out_keys = nullptr, *out_vals = nullptr, *words = nullptr;
+    // words: histogram (256) | tile counter (1) | tile status (2 tiles x 256)
+    std::size_t const word_count = 256 + 1 + 2 * 256;
+    GWNB_TRY(alloc(&keys, n, s));
+    GWNB_TRY(alloc(&out_keys, n, s));
+    GWNB_TRY(alloc(&out_vals, n, s));
+    GWNB_TRY(alloc(&words, word_count, s));
+    GWNB_CUDA_TRY(cudaMemsetAsync(keys, 0, n * sizeof(std::uint32_t), s));
+    GWNB_CUDA_TRY(cudaMemsetAsync(words, 0, word_count * sizeof(std::uint32_t), s));
+    std::uint32_t const first_tile = 1;
+    GWNB_CUDA_TRY(cudaMemcpyAsync(words + 256, &first_tile, sizeof(first_tile), cudaMemcpyHostToDevice, s));
+    note_launch(), k_sort_histogram<std::uint32_t><<<2, k_threads, 0, s>>>(keys, n, 1, 8, words);
+    note_launch(), k_onesweep<std::uint32_t, k_items><<<1, k_threads, 0, s>>>(
+        keys, nullptr, out_keys, out_vals, n, 0, 0xffu, words, words + 257, words + 256, status, wait_limit());
+    cudaError_t const e = cudaGetLastError();
+    GWNB_CUDA_TRY(cudaStreamSynchronize(s));
+    release(keys, s);
+    release(out_keys, s);
+    release(out_vals, s);
+    release(words, s);
+    if (e != cudaSuccess)
+        return set_cuda_error(e, "onesweep wait probe");
+    return GWNB_OK;
+}
 
 std::size_t radix_sort_u32_scratch_words(std::uint64_t n, int key_bits) {
     constexpr std::uint64_t k_tile = static_cast<std::uint64_t>(k_threads) * sort_items<std::uint32_t>::value;

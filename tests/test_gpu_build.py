@@ -314,3 +314,30 @@ def test_build_matches_reference_kernels(cuda, name):
     np.testing.assert_array_equal(h["primitive_indices"], rb["primitive_indices"])
     np.testing.assert_array_equal(h["triangles"], rb["triangles"])
     R.close()
+
+
+def deep_mesh(n: int = 420) -> dict:
+    """Small triangles at x = 1.1^k: H-PLOC merges them into a caterpillar whose BVH4 has 40 levels,
+    deeper than the levels a build enqueues before its single read-back."""
+    xs = (1.1 ** np.arange(n)).astype(np.float32)
+    return {"x": np.concatenate([xs, xs + xs * np.float32(1e-3), xs]).astype(np.float32),
+            "y": np.concatenate([np.zeros(n), np.zeros(n), xs * np.float32(1e-3)]).astype(np.float32),
+            "z": np.zeros(3 * n, np.float32), "i0": np.arange(n, dtype=np.uint32),
+            "i1": np.arange(n, 2 * n, dtype=np.uint32), "i2": np.arange(2 * n, 3 * n, dtype=np.uint32)}
+
+
+def test_build_deeper_than_first_collapse_batch(cuda):
+    mesh = deep_mesh()
+    h = api.bvh_host_arrays(build(upload(mesh), g.gwn_bvh_build_method.k_hploc))
+    ob = oracle.build_bvh(mesh, "hploc", radius=8)
+    assert oracle.canonical_wide(h["nodes"], h["root_reference"]) == oracle.canonical_wide(ob["nodes"], (1 << 47))
+    assert (h["internal_stack_bound"], h["packed_stack_bound"]) == (ob["internal_stack_bound"],
+                                                                   ob["packed_stack_bound"])
+    ib, pb, reach = host_stack_bounds(h["nodes"], h["root_reference"], mesh["i0"].size)
+    assert (ib, pb, reach) == (h["internal_stack_bound"], h["packed_stack_bound"], len(h["nodes"]))
+    # the refit state derived on that path is complete: a refit reproduces the bounds
+    before = api.bvh_host_arrays(build(upload(mesh), g.gwn_bvh_build_method.k_hploc))
+    geo = upload(mesh)
+    bvh = build(geo, g.gwn_bvh_build_method.k_hploc)
+    assert g.gwn_refit_bvh(geo, bvh).is_ok()
+    np.testing.assert_array_equal(api.bvh_host_arrays(bvh)["nodes"]["bounds"], before["nodes"]["bounds"])
