@@ -11,8 +11,9 @@ compensated near field. A step is one call of the Taylor batch on the 10M device
 For N > 1 run one process per GPU with torch.distributed.run; every rank processes its own 10M
 queries against its own copy of the BVH (queries are independent: weak scaling, no data-path
 collective; the only collective is the max over ranks of the measured time).
-``--impl reference`` times the CPU implementation of the same path (the oracle's port of the
-reference traversal, all host threads) on bounded samples of the same workload.
+``--impl reference`` times the reference's own CPU implementation of the same path (smallgwn's
+CPU Taylor path, the SideFX HDK tree of its tests/reference_hdk.cuh, compiled into oracle/_ref;
+all host threads) on bounded samples of the same workload.
 """
 from __future__ import annotations
 
@@ -328,9 +329,26 @@ def make_workload(rank: int, n_queries: int):
 
 
 def cpu_baseline(mesh, bvh_host, mom_host, q, order, beta, budget_s=12.0) -> dict:
-    """The oracle's port of the reference Taylor traversal on all host threads, bounded sample."""
+    """smallgwn's own CPU Taylor path (the SideFX HDK tree of tests/reference_hdk.cuh, compiled into
+    oracle/_ref) on all host threads over a bounded sample of the workload's queries; the oracle's
+    port of the reference traversal when that library was not built."""
     import oracle
 
+    if oracle.ref_cpu_lib() is not None:
+        hdk = oracle.ReferenceHDK(mesh, order)
+        try:
+            chunk, done = 50_000, 0
+            t0 = time.perf_counter()
+            while time.perf_counter() - t0 < budget_s and done < q[0].size:
+                sl = slice(done, min(done + chunk, q[0].size))
+                hdk.query(q[0][sl], q[1][sl], q[2][sl], beta)
+                done = sl.stop
+            dt = time.perf_counter() - t0
+            return {"value": done / dt, "unit": "queries/s", "cores": hdk.threads, "kind": "reference",
+                    "sample": f"{done} of the {q[0].size} queries through smallgwn's CPU Taylor path (SideFX HDK "
+                              f"tree, order {order}, accuracy scale {beta}; tree built untimed) in {dt:.1f} s"}
+        finally:
+            hdk.close()
     threads = oracle.max_threads()
     chunk = 20_000
     done = 0
@@ -353,20 +371,34 @@ def run_reference_arm(args) -> None:
     import oracle
 
     mesh, q = make_workload(0, args.queries)
-    # Everything on the host: the oracle's H-PLOC build (radius 8) and moments of the same mesh,
-    # then its Taylor traversal; no kernel of this library runs in this arm.
-    bh = oracle.build_bvh(mesh, "hploc", radius=8)
-    bh["root_reference"] = int(bh["root_reference"])
-    mh = oracle.moments(args.order, bh["nodes"], bh["triangles"])
-    threads = oracle.max_threads()
-    sample = 40_000
     rng = np.random.default_rng(0)
+    if oracle.ref_cpu_lib() is not None:
+        # smallgwn's own CPU Taylor path: the SideFX HDK tree of tests/reference_hdk.cuh, compiled
+        # from the reference's sources into oracle/_ref, built once (untimed), queried on all host
+        # threads; no kernel of this library runs in this arm
+        hdk = oracle.ReferenceHDK(mesh, args.order)
+        threads, kind, sample = hdk.threads, "reference", 200_000
+        what = "smallgwn's CPU Taylor path (SideFX HDK tree)"
+
+        def query(ix):
+            hdk.query(q[0][ix], q[1][ix], q[2][ix], args.beta)
+    else:
+        # the oracle's H-PLOC build (radius 8) and moments of the same mesh, then its restatement of
+        # smallgwn's Taylor traversal
+        bh = oracle.build_bvh(mesh, "hploc", radius=8)
+        bh["root_reference"] = int(bh["root_reference"])
+        mh = oracle.moments(args.order, bh["nodes"], bh["triangles"])
+        threads, kind, sample = oracle.max_threads(), "port", 40_000
+        what = "the oracle's port of smallgwn's Taylor traversal"
+
+        def query(ix):
+            oracle.taylor(args.order, bh["nodes"], mh, bh["triangles"], bh["root_reference"], q[0][ix], q[1][ix],
+                          q[2][ix], beta=args.beta, threads=threads)
 
     def step():
         idx = rng.integers(0, q[0].size, sample)
         t0 = time.perf_counter()
-        oracle.taylor(args.order, bh["nodes"], mh, bh["triangles"], bh["root_reference"], q[0][idx], q[1][idx],
-                      q[2][idx], beta=args.beta, threads=threads)
+        query(idx)
         return time.perf_counter() - t0
 
     for _ in range(args.warmup):
@@ -378,9 +410,9 @@ def run_reference_arm(args) -> None:
         "warmup": args.warmup, "ms_per_step": total / args.steps * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
         "config": config_dict(args, mesh),
-        "cpu_baseline": {"value": value, "unit": "queries/s", "cores": threads, "kind": "port",
-                         "sample": f"{sample} random queries of the workload per step, Taylor order {args.order}, "
-                                   f"beta {args.beta}, {threads} host threads"},
+        "cpu_baseline": {"value": value, "unit": "queries/s", "cores": threads, "kind": kind,
+                         "sample": f"{sample} random queries of the workload per step through {what}, Taylor "
+                                   f"order {args.order}, accuracy scale {args.beta}, {threads} host threads"},
         "e2e": {"value": value, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -529,10 +561,11 @@ def run_adjoint_workload(args) -> None:
     V = np.stack([mesh["x"], mesh["y"], mesh["z"]], -1).astype(np.float64)
     used = np.unique(np.concatenate([mesh["i0"], mesh["i1"], mesh["i2"]]))
 
-    def fd_check(step: float, clearance: float) -> dict:
+    def fd_check(step: float, clearance: float, converged: float | None = None) -> dict:
         """Central differences (Richardson with step and step / 2) of the oracle's frozen-decision
-        FP64 sum for the loss over queries farther than clearance * step from the surface (the
-        extrapolation error grows like 120 (step / distance)^4), against the adjoint of that loss."""
+        FP64 sum for the loss over queries farther than clearance * step from the surface, against the
+        adjoint of that loss. With `converged`, the same differences at that smaller step too: the
+        gap between the two is the truncation of the differences at `step` itself."""
         far = np.flatnonzero(dist > clearance * step)[:4096]
         ws = np.zeros(n, np.float32)
         ws[far] = w[far]
@@ -550,19 +583,24 @@ def run_adjoint_workload(args) -> None:
             return oracle.taylor_frozen_f64(order, hb["nodes"], mh, hb["root_reference"], Vp, mesh,
                                             hb["primitive_indices"], d, ev, beta=beta)
 
-        def richardson(f):
-            return (4 * (f(step / 2) - f(-step / 2)) / step - (f(step) - f(-step)) / (2 * step)) / 3
+        def richardson(f, h=step):
+            return (4 * (f(h / 2) - f(-h / 2)) / h - (f(h) - f(-h)) / (2 * h)) / 3
 
         rng = np.random.default_rng(5)
         verts = rng.choice(used, 64, replace=False)
-        fd_v = np.zeros((64, 3))
-        for i, v in enumerate(verts):
-            for k in range(3):
-                def fv(s, v=v, k=k):
-                    Vp = V.copy()
-                    Vp[v, k] += s
-                    return float(wf @ frozen(Vp, ev0))
-                fd_v[i, k] = richardson(fv)
+
+        def vertex_fd(h):
+            out = np.zeros((64, 3))
+            for i, v in enumerate(verts):
+                for k in range(3):
+                    def fv(s, v=v, k=k):
+                        Vp = V.copy()
+                        Vp[v, k] += s
+                        return float(wf @ frozen(Vp, ev0))
+                    out[i, k] = richardson(fv, h)
+            return out
+
+        fd_v = vertex_fd(step)
         sel = rng.choice(far.size, 64, replace=False)
         fd_q = np.zeros((64, 3))
         for k in range(3):
@@ -577,11 +615,20 @@ def run_adjoint_workload(args) -> None:
                     "max_rel_floor_1pct": float(np.max(np.abs(a - f) / np.maximum(np.abs(f), 1e-2 * np.abs(f).max())))}
 
         near = int(np.count_nonzero(dist[far] < 1e-2))
-        return {"h": step, "clearance": clearance * step, "richardson": True, "vertices": 64, "queries": 64,
-                "loss_queries": int(far.size), "loss_queries_within_1e-2": near,
-                "dV": errs(adj_v[verts], fd_v), "dq": errs(adj_q[far][sel], fd_q)}
+        res = {"h": step, "clearance": clearance * step, "richardson": True, "vertices": 64, "queries": 64,
+               "loss_queries": int(far.size), "loss_queries_within_1e-2": near,
+               "dV": errs(adj_v[verts], fd_v), "dq": errs(adj_q[far][sel], fd_q)}
+        if converged is not None:
+            fd_c = vertex_fd(converged)
+            res["dV_vs_converged_fd"] = {"h": converged, **errs(adj_v[verts], fd_c)}
+            res["fd_truncation_at_h"] = errs(fd_v, fd_c)
+            # the north-star criterion: 1e-3 relative per element (1 % floor) against differences
+            # that have converged
+            res["pass_1e-3"] = bool(res["dV_vs_converged_fd"]["max_rel_floor_1pct"] <= 1e-3 and
+                                    res["dq"]["max_rel_floor_1pct"] <= 1e-3)
+        return res
 
-    checks = [fd_check(h, 30.0), fd_check(1e-6, 100.0)]
+    checks = [fd_check(h, 30.0, converged=1e-5), fd_check(1e-6, 100.0)]
     ms = total_ms / args.steps
     line = {
         "metric": "Adjoint (forward + backward) queries/s, order 1, 159k-triangle open soup",

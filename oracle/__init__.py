@@ -56,6 +56,79 @@ def ref_lib() -> C.CDLL | None:
     return _REF
 
 
+_REF_CPU = None
+
+
+def ref_cpu_lib() -> C.CDLL | None:
+    """smallgwn's own CPU reference code (oracle/_ref/libgwnrefcpu.so) or None when not built."""
+    global _REF_CPU
+    if _REF_CPU is None:
+        path = HERE / "_ref" / "libgwnrefcpu.so"
+        if not path.exists():
+            return None
+        lib = C.CDLL(str(path))
+        lib.refcpu_set_threads.restype = C.c_int
+        lib.refcpu_set_threads.argtypes = [C.c_int]
+        lib.refcpu_exact.restype = C.c_int
+        lib.refcpu_exact.argtypes = [C.c_void_p] * 3 + [C.c_uint64] + [C.c_void_p] * 3 + [C.c_uint64] + \
+            [C.c_void_p] * 3 + [C.c_uint64, C.c_void_p]
+        lib.refcpu_hdk_create.restype = C.c_void_p
+        lib.refcpu_hdk_create.argtypes = [C.c_void_p] * 3 + [C.c_uint64] + [C.c_void_p] * 3 + [C.c_uint64, C.c_int]
+        lib.refcpu_hdk_query.restype = C.c_int
+        lib.refcpu_hdk_query.argtypes = [C.c_void_p] * 4 + [C.c_uint64, C.c_float, C.c_void_p]
+        lib.refcpu_hdk_destroy.argtypes = [C.c_void_p]
+        _REF_CPU = lib
+    return _REF_CPU
+
+
+def reference_cpu_exact(mesh: dict, qx, qy, qz, threads: int = 0) -> np.ndarray:
+    """smallgwn's own CPU exact brute force (tests/reference_cpu.cuh:84-114), FP32."""
+    lib = ref_cpu_lib()
+    lib.refcpu_set_threads(int(threads))
+    x, y, z = (_f32(mesh[k]) for k in "xyz")
+    i0, i1, i2 = _u32(mesh["i0"]), _u32(mesh["i1"]), _u32(mesh["i2"])
+    q = [_f32(v) for v in (qx, qy, qz)]
+    out = np.empty(q[0].size, np.float32)
+    if lib.refcpu_exact(_p(x), _p(y), _p(z), x.size, _p(i0), _p(i1), _p(i2), i0.size, _p(q[0]), _p(q[1]), _p(q[2]),
+                        out.size, _p(out)) != 0:
+        raise RuntimeError("reference CPU exact batch failed")
+    return out
+
+
+class ReferenceHDK:
+    """smallgwn's CPU Taylor path: the vendored SideFX HDK solid-angle tree of a mesh
+    (tests/reference_hdk.cuh:18-89), built once, queried at an accuracy scale."""
+
+    def __init__(self, mesh: dict, order: int, threads: int = 0):
+        self.lib = ref_cpu_lib()
+        if self.lib is None:
+            raise RuntimeError("oracle/_ref/libgwnrefcpu.so is not built")
+        self.threads = self.lib.refcpu_set_threads(int(threads))
+        x, y, z = (_f32(mesh[k]) for k in "xyz")
+        i0, i1, i2 = _u32(mesh["i0"]), _u32(mesh["i1"]), _u32(mesh["i2"])
+        self.h = self.lib.refcpu_hdk_create(_p(x), _p(y), _p(z), x.size, _p(i0), _p(i1), _p(i2), i0.size, int(order))
+        if not self.h:
+            raise RuntimeError("reference HDK tree construction failed")
+
+    def query(self, qx, qy, qz, beta: float) -> np.ndarray:
+        q = [_f32(v) for v in (qx, qy, qz)]
+        out = np.empty(q[0].size, np.float32)
+        if self.lib.refcpu_hdk_query(self.h, _p(q[0]), _p(q[1]), _p(q[2]), out.size, C.c_float(beta), _p(out)) != 0:
+            raise RuntimeError("reference HDK query failed")
+        return out
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.refcpu_hdk_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def max_threads() -> int:
     return int(lib().oracle_max_threads())
 

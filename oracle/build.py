@@ -10,6 +10,12 @@
    the headers do not.
 The reference project's location is this recipe's one input: GWN_REFERENCE_ROOT when set, else the
 read-only mount the reference is provided at in the build container.
+3. oracle/_ref/libgwnrefcpu.so -- smallgwn's own CPU reference code compiled with g++ from where it
+   lies: the exact brute force of tests/reference_cpu.cuh and the vendored SideFX HDK Taylor tree
+   (tests/reference_hdk/UT_SolidAngle.cpp, UT_Array.cpp) behind oracle/ref_cpu.cpp, with the small
+   Eigen / oneTBB stand-ins of oracle/shims/ in place of those libraries (not installed here).
+   Built only when the reference sources exist; portable x86-64 flags (SSE4.2, which the HDK's
+   SIMD code needs), so the library also runs on the GPU machines.
 Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg load these libraries.
 """
 from __future__ import annotations
@@ -25,6 +31,7 @@ BUILD = HERE / "_build"
 REF = HERE / "_ref"
 ORACLE_SO = BUILD / "liboracle.so"
 REF_SO = REF / "libgwnref.so"
+REF_CPU_SO = REF / "libgwnrefcpu.so"
 REFERENCE_ROOT = Path(os.environ.get("GWN_REFERENCE_ROOT", "/root/reference"))
 REFERENCE_INCLUDE = REFERENCE_ROOT / "include"
 
@@ -58,7 +65,28 @@ def build_reference(force: bool = False) -> Path | None:
     return REF_SO
 
 
+def build_reference_cpu(force: bool = False) -> Path | None:
+    """Compile smallgwn's CPU reference code into oracle/_ref when its sources are present; else skip."""
+    shim = HERE / "ref_cpu.cpp"
+    tests = REFERENCE_ROOT / "tests"
+    hdk = tests / "reference_hdk"
+    sources = [shim, hdk / "UT_SolidAngle.cpp", hdk / "UT_Array.cpp"]
+    if not (tests / "reference_cpu.cuh").exists() or not all(p.exists() for p in sources[1:]):
+        return REF_CPU_SO if REF_CPU_SO.exists() else None
+    shims = HERE / "shims"
+    deps = [*sources, Path(__file__), *shims.rglob("*")]
+    if force or _newer(REF_CPU_SO, *deps):
+        REF.mkdir(exist_ok=True)
+        cuda_include = Path(shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc").resolve().parents[1] / "include"
+        cmd = ["g++", "-std=c++20", "-O3", "-msse4.2", "-fPIC", "-shared", "-pthread", "-I", str(shims),
+               "-I", str(REFERENCE_INCLUDE), "-I", str(tests), "-I", str(hdk), "-I", str(cuda_include),
+               *map(str, sources), "-o", str(REF_CPU_SO)]
+        subprocess.run(cmd, check=True)
+    return REF_CPU_SO
+
+
 if __name__ == "__main__":
     force = "--force" in sys.argv
     print(build_oracle(force))
     print(build_reference(force))
+    print(build_reference_cpu(force))

@@ -290,3 +290,43 @@ def test_oracle_matches_reference_golden(path):
         np.testing.assert_allclose(w2, g[f"taylor{order}_b2"], atol=1e-5, rtol=2e-5)
         w6 = oracle.taylor(order, g["lbvh_nodes"], ref_mom, g["lbvh_tris"], int(meta[0]), *q, beta=1e6)
         np.testing.assert_allclose(w6, g[f"taylor{order}_b1e6"], atol=1e-5, rtol=2e-5)
+
+
+# ---- the oracle against smallgwn's own CPU reference code (oracle/_ref/libgwnrefcpu.so) -------------
+
+REF_CPU = oracle.ref_cpu_lib() is not None
+
+
+@pytest.mark.skipif(not REF_CPU, reason="smallgwn's CPU reference code (oracle/_ref/libgwnrefcpu.so) not built")
+@pytest.mark.parametrize("name", ["small", "soup", "octahedron"])
+def test_oracle_exact_is_the_reference_cpu_exact_bit_for_bit(name):
+    """The oracle's FP32 exact brute force restates tests/reference_cpu.cuh:22-114; compiled from
+    the reference's own source (Eigen / oneTBB stand-ins), that code gives the same bits."""
+    from conftest import octahedron
+    from smallgwn_b200 import meshes
+
+    mesh = {"small": meshes.small_mesh, "soup": lambda: meshes.soup_mesh(24, seed=11), "octahedron": octahedron}[name]()
+    q = meshes.small_queries(3000) if name != "soup" else meshes.mixed_queries(mesh, 3000, seed=7)
+    np.testing.assert_array_equal(oracle.reference_cpu_exact(mesh, *q), oracle.exact_winding(mesh, *q))
+
+
+@pytest.mark.skipif(not REF_CPU, reason="smallgwn's CPU reference code (oracle/_ref/libgwnrefcpu.so) not built")
+def test_reference_hdk_taylor_within_the_reference_tolerances_of_the_oracle_traversal():
+    """smallgwn's CPU Taylor path (the vendored SideFX HDK tree, tests/reference_hdk.cuh) against the
+    oracle's restatement of smallgwn's GPU traversal on the same mesh at accuracy scale 2, within the
+    tolerances smallgwn holds its GPU Taylor batch to against HDK (tests/e2e_gwn.cu:103-106):
+    5e-2, 3e-2, 2e-2 for orders 0, 1, 2."""
+    from smallgwn_b200 import meshes
+
+    mesh = meshes.to_soa(*meshes.uv_sphere(64, 32, seed=9))
+    q = meshes.mixed_queries(mesh, 4000, seed=3)
+    b = oracle.build_bvh(mesh, "hploc", radius=8)
+    for order, eps in ((0, 5e-2), (1, 3e-2), (2, 2e-2)):
+        hdk = oracle.ReferenceHDK(mesh, order)
+        try:
+            got = hdk.query(*q, beta=2.0)
+        finally:
+            hdk.close()
+        mom = oracle.moments(order, b["nodes"], b["triangles"])
+        ref = oracle.taylor(order, b["nodes"], mom, b["triangles"], b["root_reference"], *q, beta=2.0)
+        assert np.max(np.abs(got - ref)) <= eps, (order, np.max(np.abs(got - ref)))
