@@ -317,6 +317,30 @@ GWNB_API int gwnb_winding_taylor_stats_f32(const gwnb_bvh4_f32 *bvh, const gwnb_
                                   uint32_t *far_evaluations, uint32_t *near_triangles,
                                   gwnb_stream_t stream);
 
+/* ---- Taylor order and accuracy scale from an error target (no smallgwn counterpart) ------------
+ * smallgwn leaves the Taylor order (a template parameter) and the accuracy scale to the caller. */
+
+typedef struct gwnb_taylor_choice {
+    int order;              /* chosen Taylor order                                               */
+    float accuracy_scale;   /* chosen beta                                                       */
+    float max_error;        /* max |w - w_fp64| over the sample with that choice                 */
+    float sample_ms;        /* device time of one Taylor batch over the sample with that choice  */
+    int stack_capacity;     /* traversal stack the tree needs: its exact internal stack bound    */
+    int candidates_passing; /* orders with some candidate beta within the bound                  */
+} gwnb_taylor_choice;
+
+/* Picks the Taylor order and accuracy scale for a caller's error bound on a sample of the caller's
+ * queries (device arrays qx/qy/qz of n): the sample's FP64 exact winding numbers are the reference;
+ * for every order o whose moments[o] is non-NULL (valid for `bvh`), the smallest of the candidate
+ * `betas` whose maximum error on the sample is at most max_error is that order's candidate; the
+ * candidates are timed on the sample (CUDA events, same stream) and the fastest is returned in *out.
+ * GWNB_INVALID_ARGUMENT when no candidate meets the bound. Synchronizes `stream`. */
+GWNB_API int gwnb_taylor_select_f32(const gwnb_geometry_f32 *geometry, const gwnb_bvh4_f32 *bvh,
+                                    const gwnb_moment4_f32 *const *moments, const float *qx, const float *qy,
+                                    const float *qz, uint64_t n, float max_error, const float *betas,
+                                    int beta_count, int near_precision, gwnb_taylor_choice *out,
+                                    gwnb_stream_t stream);
+
 /* Exact winding numbers of the float mesh evaluated in FP64 (brute force over the geometry's
  * triangles, double-precision Van Oosterom-Strackee). Counterpart of smallgwn's Real = double
  * instantiation of gwn_compute_winding_number_exact_batch (tests/reference_cpu.cuh:84-114 is its
@@ -594,6 +618,20 @@ GWNB_API int gwnb_batch_run_f32(gwnb_batch *batch, unsigned int stages, gwnb_str
  * stack overflow) as GWNB_INTERNAL_ERROR. */
 GWNB_API int gwnb_batch_sync_f32(gwnb_batch *batch, gwnb_stream_t stream);
 GWNB_API int gwnb_batch_release_f32(gwnb_batch *batch, gwnb_stream_t stream);
+
+/* Tree quality (no smallgwn counterpart): per mesh, the surface-area cost of its BVH now -- the sum
+ * over nodes of the children's box half-areas over the root box's half-area -- divided by that cost
+ * when the tree was built (cost_ratio: mesh_count floats, host). Refitting keeps the rest shape's
+ * topology, so the ratio grows as the meshes deform and queries visit more nodes. Synchronizes. */
+GWNB_API int gwnb_batch_quality_f32(gwnb_batch *batch, float *cost_ratio, gwnb_stream_t stream);
+
+/* Rebuilds (method, radius as gwnb_bvh4_build_f32, 64-bit Morton codes) every BVH whose cost ratio
+ * exceeds `threshold`, from its geometry's current positions, refits its moments, replaces the
+ * caller's BVH and moment objects in place and re-derives the batch's descriptors (*rebuilt: how
+ * many). Between frames: a CUDA graph captured before a rebuild that rebuilt anything refers to the
+ * released arrays and must be captured again. Synchronizes. */
+GWNB_API int gwnb_batch_rebuild_f32(gwnb_batch *batch, float threshold, int method, uint32_t radius,
+                                    uint32_t *rebuilt, gwnb_stream_t stream);
 
 #ifdef __cplusplus
 }

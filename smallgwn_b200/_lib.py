@@ -121,6 +121,17 @@ class batch_mesh_f32(C.Structure):
     ]
 
 
+class taylor_choice(C.Structure):
+    _fields_ = [
+        ("order", C.c_int),
+        ("accuracy_scale", C.c_float),
+        ("max_error", C.c_float),
+        ("sample_ms", C.c_float),
+        ("stack_capacity", C.c_int),
+        ("candidates_passing", C.c_int),
+    ]
+
+
 class batch_tuning(C.Structure):
     _fields_ = [
         ("refit_block", C.c_int),
@@ -190,6 +201,13 @@ SIGNATURES: dict[str, tuple] = {
     "gwnb_launch_count": (C.c_uint64, []),
     "gwnb_fp32_fma_peak": (C.c_int, [C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_void_p]),
     "gwnb_set_wait_limit": (C.c_int, [C.c_int64]),
+    "gwnb_batch_quality_f32": (C.c_int, [C.c_void_p, C.POINTER(C.c_float), C.c_void_p]),
+    "gwnb_batch_rebuild_f32": (C.c_int, [C.c_void_p, C.c_float, C.c_int, C.c_uint32, C.POINTER(C.c_uint32),
+                                         C.c_void_p]),
+    "gwnb_taylor_select_f32": (C.c_int, [C.POINTER(geometry_f32), C.POINTER(bvh4_f32), C.POINTER(C.POINTER(moment4_f32)),
+                                         C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_float,
+                                         C.POINTER(C.c_float), C.c_int, C.c_int, C.POINTER(taylor_choice),
+                                         C.c_void_p]),
     "gwnb_wait_timeout_probe": (C.c_int, [C.c_int, C.c_void_p]),
     "gwnb_geometry_upload_f32": (I, [C.POINTER(geometry_f32), P, P, P, U64, P, P, P, U64, P]),
     "gwnb_geometry_update_f32": (I, [C.POINTER(geometry_f32), P, P, P, U64, P]),

@@ -419,6 +419,23 @@ def taylor_traversal_stats(bvh: gwn_bvh4_object, moment: gwn_bvh4_moment_object,
     return _status(rc)
 
 
+def select_taylor_form(geometry: gwn_geometry_object, bvh: gwn_bvh4_object, moments: dict, qx, qy, qz,
+                       max_error: float, accuracy_scales=(1.0, 1.5, 2.0, 2.5, 3.0, 3.25, 3.5, 4.0, 5.0, 6.0, 8.0),
+                       precision: int = near_precision.compensated, stream=None) -> tuple[gwn_status, dict]:
+    """Taylor order and accuracy scale for an error bound, chosen on a device sample of queries
+    (gwnb_taylor_select_f32): ``moments`` maps the orders to consider to their moment objects. Returns
+    (status, {order, accuracy_scale, max_error, sample_ms, stack_capacity, candidates_passing})."""
+    arr = (C.POINTER(_lib.moment4_f32) * 3)()
+    for o, m in moments.items():
+        arr[int(o)] = C.pointer(m._view)
+    betas = (C.c_float * len(accuracy_scales))(*accuracy_scales)
+    out = _lib.taylor_choice()
+    rc = _lib.load().gwnb_taylor_select_f32(C.byref(geometry._view), C.byref(bvh._view), arr, _ptr(qx), _ptr(qy),
+                                            _ptr(qz), _numel(qx), float(max_error), betas, len(accuracy_scales),
+                                            int(precision), C.byref(out), _stream(stream))
+    return _status(rc), {f: getattr(out, f) for f, _ in _lib.taylor_choice._fields_}
+
+
 def exact_winding_fp64(geometry: gwn_geometry_object, qx, qy, qz, out, stream=None) -> gwn_status:
     """FP64 exact winding numbers of the float mesh (float32 queries, float64 output tensor)."""
     bad = _check_spans(qx, qy, qz, out)
@@ -835,6 +852,22 @@ class gwn_batch:
 
     def sync(self, stream=None) -> gwn_status:
         return _status(_lib.load().gwnb_batch_sync_f32(self._handle, _stream(stream)))
+
+    def quality(self, stream=None) -> tuple[gwn_status, list]:
+        """Per mesh, the BVH's surface-area cost now over its cost when built (gwnb_batch_quality_f32)."""
+        out = (C.c_float * len(self._keep))()
+        rc = _lib.load().gwnb_batch_quality_f32(self._handle, out, _stream(stream))
+        return _status(rc), list(out)
+
+    def rebuild(self, threshold: float, method: int = gwn_bvh_build_method.k_hploc, radius: int = 8,
+                stream=None) -> tuple[gwn_status, int]:
+        """Rebuild the BVHs (and moments) whose cost ratio exceeds ``threshold``; the mesh objects are
+        updated in place. A frame graph captured before a rebuild that rebuilt anything must be
+        captured again."""
+        n = C.c_uint32()
+        rc = _lib.load().gwnb_batch_rebuild_f32(self._handle, float(threshold), int(method), int(radius), C.byref(n),
+                                                _stream(stream))
+        return _status(rc), int(n.value)
 
     def release(self, stream=None) -> None:
         if self._handle:

@@ -10,6 +10,13 @@
 // The autotuner times candidate launch shapes -- refit block size; query block size, traversal
 // form (a warp of 32 Hilbert-adjacent queries walking one traversal, or one traversal per thread),
 // Hilbert-ordered or input order, persistent grid size -- on the batch itself and keeps the fastest.
+//
+// Refitting keeps the topology built for the rest shape; as the meshes deform, the boxes of a
+// refit tree grow and overlap and every query visits more nodes. The batch measures each tree's
+// quality as its surface-area cost (the sum over nodes of the children's box half-areas, over the
+// root's half-area: the expected number of child boxes a uniformly placed probe enters) relative to
+// the cost when the tree was built, and rebuilds the trees whose cost grew past a caller's
+// threshold (gwnb_batch_rebuild_f32), between frames.
 #include "gwnb_internal.cuh"
 
 #include <algorithm>
@@ -19,6 +26,11 @@
 #include <vector>
 
 struct gwnb_batch {
+    std::vector<gwnb_batch_mesh_f32> meshes; // the caller's mesh descriptors (objects updated in place)
+    std::vector<double> base_cost;           // surface-area cost of each tree when built
+    float beta = 2.0f;
+    gwnb_taylor_options options{};
+    int order = 0;
     std::vector<gwnb_bvh4_f32 *> bvhs;
     std::vector<unsigned int *> status_words;
     gwnb::batch_refit_state refit{};
@@ -45,6 +57,121 @@ void release_batch(gwnb_batch *b, cudaStream_t s) {
     batch_query_release(b->query, s);
     release(b->d_status, s);
     release(b->d_flags, s);
+}
+
+// Surface-area cost terms of one tree: out[0] += sum over nodes of the children's box half-areas,
+// out[1] = the half-area of the union of the root node's children (the root box).
+__global__ void __launch_bounds__(256)
+    k_tree_cost(node4 const *__restrict__ nodes, std::uint64_t node_count, double *out) {
+    std::uint64_t const n = static_cast<std::uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    double sum = 0.0;
+    if (n < node_count) {
+        aabb u{__int_as_float(0x7f800000), __int_as_float(0x7f800000), __int_as_float(0x7f800000),
+               -__int_as_float(0x7f800000), -__int_as_float(0x7f800000), -__int_as_float(0x7f800000)};
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            if (!ref_valid(nodes[n].c[c].reference))
+                continue;
+            aabb const &b = nodes[n].c[c].bounds;
+            sum += static_cast<double>(aabb_half_area(b));
+            u = aabb_union(u, b);
+        }
+        if (n == 0)
+            out[1] = static_cast<double>(aabb_half_area(u));
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+        sum += __shfl_xor_sync(0xffffffffu, sum, o);
+    if ((threadIdx.x & 31u) == 0u && sum != 0.0)
+        atomicAdd(out, sum);
+}
+
+// Each mesh's surface-area cost (1 for a tree whose root is a leaf). Synchronizes the stream.
+int tree_costs(gwnb_batch *b, std::vector<double> &cost, cudaStream_t s) {
+    std::size_t const m = b->meshes.size();
+    double *d = nullptr;
+    GWNB_TRY(alloc(&d, 2 * m, s));
+    int rc = GWNB_OK;
+    if (cudaMemsetAsync(d, 0, 2 * m * sizeof(double), s) != cudaSuccess)
+        rc = set_cuda_error(cudaGetLastError(), "batch tree cost");
+    for (std::size_t i = 0; i < m && rc == GWNB_OK; ++i) {
+        gwnb_bvh4_f32 const *bv = b->meshes[i].bvh;
+        if (bv->node_count == 0)
+            continue;
+        note_launch(), k_tree_cost<<<static_cast<unsigned>((bv->node_count + 255) / 256), 256, 0, s>>>(
+            reinterpret_cast<node4 const *>(bv->nodes), bv->node_count, d + 2 * i);
+        if (cudaGetLastError() != cudaSuccess)
+            rc = set_cuda_error(cudaGetLastError(), "batch tree cost");
+    }
+    std::vector<double> h(2 * m, 0.0);
+    if (rc == GWNB_OK && (cudaMemcpyAsync(h.data(), d, 2 * m * sizeof(double), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+                          cudaStreamSynchronize(s) != cudaSuccess))
+        rc = set_cuda_error(cudaGetLastError(), "batch tree cost read-back");
+    release(d, s);
+    if (rc != GWNB_OK)
+        return rc;
+    cost.assign(m, 1.0);
+    for (std::size_t i = 0; i < m; ++i)
+        if (b->meshes[i].bvh->node_count > 0 && h[2 * i + 1] > 0.0)
+            cost[i] = h[2 * i] / h[2 * i + 1];
+    return GWNB_OK;
+}
+
+// The batch's device descriptors (refit items, traversal descriptors and Hilbert orders, status
+// words) from its meshes' current objects; replaces any previous ones.
+int prepare_states(gwnb_batch *b, cudaStream_t s) {
+    batch_refit_release(b->refit, s);
+    batch_query_release(b->query, s);
+    b->refit = batch_refit_state{};
+    b->query = batch_query_state{};
+    std::uint32_t const mesh_count = static_cast<std::uint32_t>(b->meshes.size());
+    std::vector<gwnb_geometry_f32> geoms(mesh_count);
+    std::vector<gwnb_moment4_f32 *> moms(mesh_count);
+    std::vector<taylor_request> reqs(mesh_count);
+    b->bvhs.resize(mesh_count);
+    b->status_words.resize(mesh_count);
+    for (uint32_t i = 0; i < mesh_count; ++i) {
+        gwnb_batch_mesh_f32 const &m = b->meshes[i];
+        GWNB_TRY(ensure_bvh_aux(m.bvh, s));
+        auto *a = reinterpret_cast<bvh_aux_impl *>(m.bvh->aux);
+        auto *ma = reinterpret_cast<moment_aux_impl *>(m.moment->aux);
+        geoms[i] = m.geometry;
+        moms[i] = m.moment;
+        b->bvhs[i] = m.bvh;
+        b->status_words[i] = a->status;
+        taylor_request &r = reqs[i];
+        r.order = b->order;
+        r.qnodes = ma != nullptr ? ma->qnodes : nullptr;
+        r.qcounts = ma != nullptr ? ma->qcounts : nullptr;
+        r.tri48 = a->tri48;
+        r.primitive_count = m.bvh->primitive_count;
+        r.node_count = m.bvh->node_count;
+        r.root_ref = m.bvh->root.reference;
+        r.root_bounds = a->root_bounds;
+        r.qx = m.query_x;
+        r.qy = m.query_y;
+        r.qz = m.query_z;
+        r.out = m.output;
+        r.n = m.query_count;
+        r.accuracy_scale = b->beta;
+        r.stack_capacity = std::max<int>(static_cast<int>(m.bvh->internal_stack_bound), 1);
+        r.sort_queries = 1;
+        r.near_mode = b->options.near_precision;
+        r.fp64_threshold = b->options.fp64_threshold;
+        r.fp64_count = a->fp64_count;
+        r.status = a->status;
+    }
+    GWNB_TRY(batch_refit_prepare(geoms.data(), b->bvhs.data(), moms.data(), mesh_count, b->order, &b->refit, s));
+    GWNB_TRY(batch_query_prepare(reqs.data(), mesh_count, &b->query, s));
+    if (b->d_status == nullptr)
+        GWNB_TRY(alloc(&b->d_status, mesh_count, s));
+    if (b->d_flags == nullptr)
+        GWNB_TRY(alloc(&b->d_flags, 1, s));
+    if (cudaMemcpyAsync(b->d_status, b->status_words.data(), mesh_count * sizeof(unsigned int *),
+                        cudaMemcpyHostToDevice, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess)
+        return set_cuda_error(cudaGetLastError(), "batch descriptors");
+    return GWNB_OK;
 }
 
 int run_stages(gwnb_batch *b, gwnb_batch_tuning const &t, unsigned stages, cudaStream_t s) {
@@ -116,61 +243,71 @@ int gwnb_batch_create_f32(const gwnb_batch_mesh_f32 *meshes, uint32_t mesh_count
     if (b == nullptr)
         return set_error(GWNB_INTERNAL_ERROR, "out of host memory");
     b->stream = s;
-    std::vector<gwnb_geometry_f32> geoms(mesh_count);
-    std::vector<gwnb_moment4_f32 *> moms(mesh_count);
-    std::vector<taylor_request> reqs(mesh_count);
-    b->bvhs.resize(mesh_count);
-    b->status_words.resize(mesh_count);
-    auto fail = [&](int rc) {
+    b->meshes.assign(meshes, meshes + mesh_count);
+    b->beta = beta;
+    b->options = o;
+    b->order = order;
+    int rc = prepare_states(b, s);
+    if (rc == GWNB_OK)
+        rc = tree_costs(b, b->base_cost, s);
+    if (rc != GWNB_OK) {
         release_batch(b, s);
         delete b;
         return rc;
-    };
-    int rc = GWNB_OK;
-    for (uint32_t i = 0; i < mesh_count; ++i) {
-        gwnb_batch_mesh_f32 const &m = meshes[i];
-        if ((rc = ensure_bvh_aux(m.bvh, s)) != GWNB_OK)
-            return fail(rc);
-        auto *a = reinterpret_cast<bvh_aux_impl *>(m.bvh->aux);
-        auto *ma = reinterpret_cast<moment_aux_impl *>(m.moment->aux);
-        geoms[i] = m.geometry;
-        moms[i] = m.moment;
-        b->bvhs[i] = m.bvh;
-        b->status_words[i] = a->status;
-        taylor_request &r = reqs[i];
-        r.order = order;
-        r.qnodes = ma != nullptr ? ma->qnodes : nullptr;
-        r.qcounts = ma != nullptr ? ma->qcounts : nullptr;
-        r.tri48 = a->tri48;
-        r.primitive_count = m.bvh->primitive_count;
-        r.node_count = m.bvh->node_count;
-        r.root_ref = m.bvh->root.reference;
-        r.root_bounds = a->root_bounds;
-        r.qx = m.query_x;
-        r.qy = m.query_y;
-        r.qz = m.query_z;
-        r.out = m.output;
-        r.n = m.query_count;
-        r.accuracy_scale = beta;
-        r.stack_capacity = std::max<int>(static_cast<int>(m.bvh->internal_stack_bound), 1);
-        r.sort_queries = 1;
-        r.near_mode = o.near_precision;
-        r.fp64_threshold = o.fp64_threshold;
-        r.fp64_count = a->fp64_count;
-        r.status = a->status;
     }
-    if ((rc = batch_refit_prepare(geoms.data(), b->bvhs.data(), moms.data(), mesh_count, order, &b->refit, s)) !=
-        GWNB_OK)
-        return fail(rc);
-    if ((rc = batch_query_prepare(reqs.data(), mesh_count, &b->query, s)) != GWNB_OK)
-        return fail(rc);
-    if ((rc = alloc(&b->d_status, mesh_count, s)) != GWNB_OK || (rc = alloc(&b->d_flags, 1, s)) != GWNB_OK)
-        return fail(rc);
-    if (cudaMemcpyAsync(b->d_status, b->status_words.data(), mesh_count * sizeof(unsigned int *),
-                        cudaMemcpyHostToDevice, s) != cudaSuccess ||
-        cudaStreamSynchronize(s) != cudaSuccess)
-        return fail(set_cuda_error(cudaGetLastError(), "batch descriptors"));
     *out = b;
+    return GWNB_OK;
+} catch (...) {
+    return host_exception();
+}
+
+int gwnb_batch_quality_f32(gwnb_batch *b, float *cost_ratio, gwnb_stream_t stream) try {
+    if (b == nullptr || cost_ratio == nullptr)
+        return set_error(GWNB_INVALID_ARGUMENT, "batch: null handle or output.");
+    std::vector<double> cost;
+    GWNB_TRY(tree_costs(b, cost, as_cuda(stream)));
+    for (std::size_t i = 0; i < cost.size(); ++i)
+        cost_ratio[i] = static_cast<float>(b->base_cost[i] > 0.0 ? cost[i] / b->base_cost[i] : 1.0);
+    return GWNB_OK;
+} catch (...) {
+    return host_exception();
+}
+
+int gwnb_batch_rebuild_f32(gwnb_batch *b, float threshold, int method, uint32_t radius, uint32_t *rebuilt,
+                           gwnb_stream_t stream) try {
+    if (b == nullptr)
+        return set_error(GWNB_INVALID_ARGUMENT, "batch: null handle.");
+    if (!(threshold >= 1.0f))
+        return set_error(GWNB_INVALID_ARGUMENT, "batch: the rebuild threshold is a cost ratio of at least 1.");
+    cudaStream_t const s = as_cuda(stream);
+    std::vector<double> cost;
+    GWNB_TRY(tree_costs(b, cost, s));
+    std::uint32_t count = 0;
+    std::vector<char> redo(b->meshes.size(), 0);
+    for (std::size_t i = 0; i < b->meshes.size(); ++i) {
+        if (!(cost[i] > threshold * b->base_cost[i]))
+            continue;
+        redo[i] = 1;
+        gwnb_batch_mesh_f32 &m = b->meshes[i];
+        gwnb_bvh4_f32 fresh{};
+        GWNB_TRY(gwnb_bvh4_build_f32(&m.geometry, method, radius, 64, &fresh, stream));
+        gwnb_bvh4_release_f32(m.bvh, stream);
+        *m.bvh = fresh;
+        gwnb_moment4_f32 mom{};
+        GWNB_TRY(gwnb_moment4_refit_f32(m.bvh, b->order, &mom, stream));
+        gwnb_moment4_release_f32(m.moment, stream);
+        *m.moment = mom;
+        ++count;
+    }
+    if (count > 0) {
+        GWNB_TRY(prepare_states(b, s));
+        GWNB_TRY(tree_costs(b, cost, s));
+        for (std::size_t i = 0; i < cost.size(); ++i)
+            if (redo[i])
+                b->base_cost[i] = cost[i]; // the other trees keep the cost they were built with
+    }
+    if (rebuilt != nullptr)
+        *rebuilt = count;
     return GWNB_OK;
 } catch (...) {
     return host_exception();

@@ -150,3 +150,36 @@ def test_batch_rejects_bad_meshes(cuda):
     bad = g.gwn_batch([objs[0], (geo, bvh, m0, qx, qy, qz, out)])
     assert bad.status.error == g.gwn_error.invalid_argument and "order" in bad.status.message
     assert g.gwn_batch([], accuracy_scale=BETA).status.error == g.gwn_error.invalid_argument
+
+
+def test_quality_driven_rebuild(cuda):
+    """Refit trees keep the rest shape's topology; a deformation that scrambles a mesh raises its
+    surface-area cost ratio. rebuild() rebuilds exactly the meshes past the threshold (the caller's
+    objects in place), after which the frame again equals the per-mesh path on the same objects and
+    the rebuilt trees' ratios are back at 1."""
+    X, objs = make_batch(cuda, [24, 40, 31], seed=11)
+    batch = g.gwn_batch(objs, accuracy_scale=BETA)
+    assert batch.ok(), batch.status.message
+    st, ratios = batch.quality()
+    assert st.is_ok() and np.allclose(ratios, 1.0, atol=1e-5)
+    # scramble the second mesh: every vertex moves to another vertex's position (mirrored in x)
+    n0 = objs[0][0].vertex_count()
+    n1 = objs[1][0].vertex_count()
+    perm = cuda.from_numpy(np.random.default_rng(3).permutation(n1)).cuda()
+    sub = X[:, n0:n0 + n1]
+    X[:, n0:n0 + n1] = sub[:, perm] * cuda.tensor([[-1.0], [1.0], [1.0]], device="cuda")
+    assert batch.frame().is_ok()
+    st, ratios = batch.quality()
+    assert st.is_ok()
+    assert ratios[1] > 2.0 and abs(ratios[0] - 1.0) < 1e-5 and abs(ratios[2] - 1.0) < 1e-5
+    old_revision = objs[1][1].accessor().revision
+    st, n = batch.rebuild(1.5)
+    assert st.is_ok(), st.message
+    assert n == 1 and objs[1][1].accessor().revision != old_revision
+    st, ratios = batch.quality()
+    assert st.is_ok() and np.allclose(ratios, 1.0, atol=1e-5)
+    assert batch.frame().is_ok()
+    assert batch.sync().is_ok()
+    for a, b in zip(outputs(cuda, objs), per_mesh(cuda, objs, refit=True)):
+        np.testing.assert_array_equal(a, b)
+    batch.release()
