@@ -334,8 +334,10 @@ __global__ void __launch_bounds__(k_block) k_collapse_level(collapse_params p, i
         n_in = 0;
     }
     std::uint32_t const base = *reinterpret_cast<volatile std::uint32_t *>(&p.level_base[level]);
-    collapse_item const *items_in = p.lists[level & 1];
-    collapse_item *items_out = p.lists[(level + 1) & 1];
+    // selected, not indexed: a run-time index into the parameter array would copy it to local memory
+    bool const odd = (level & 1) != 0;
+    collapse_item const *items_in = odd ? p.lists[1] : p.lists[0];
+    collapse_item *items_out = odd ? p.lists[0] : p.lists[1];
     unsigned const tid = threadIdx.x;
     unsigned const lane = tid & 31u;
     unsigned const warp = tid >> 5;
@@ -368,12 +370,17 @@ __global__ void __launch_bounds__(k_block) k_collapse_level(collapse_params p, i
                 cidx[1] = root.right_index;
                 ckind[1] = root.right_kind;
                 k = 2;
-                while (k < 4) {
+                // Expand the largest-area internal child (ties: smallest binary index) until four
+                // children or only leaves remain; every index into cidx/ckind is a compile-time
+                // constant, so both stay in registers.
+#pragma unroll
+                for (int step = 0; step < 2; ++step) {
                     int best = -1;
                     float best_area = -__int_as_float(0x7f800000);
                     std::uint32_t best_index = k_invalid_u32;
-                    for (int c = 0; c < k; ++c) {
-                        if (ckind[c] != k_kind_internal || cidx[c] >= p.leaf_count - 1)
+#pragma unroll
+                    for (int c = 0; c < 4; ++c) {
+                        if (c >= k || ckind[c] != k_kind_internal || cidx[c] >= p.leaf_count - 1)
                             continue;
                         float const area = aabb_half_area(p.binary_bounds[cidx[c]]);
                         if (best >= 0 && area < best_area)
@@ -386,15 +393,22 @@ __global__ void __launch_bounds__(k_block) k_collapse_level(collapse_params p, i
                     }
                     if (best < 0)
                         break;
-                    binary_node const e = p.binary[cidx[best]];
-                    cidx[best] = e.left_index;
-                    ckind[best] = e.left_kind;
-                    cidx[k] = e.right_index;
-                    ckind[k] = e.right_kind;
+                    binary_node const e = p.binary[best_index];
+#pragma unroll
+                    for (int c = 0; c < 4; ++c) {
+                        if (c == best) {
+                            cidx[c] = e.left_index;
+                            ckind[c] = e.left_kind;
+                        } else if (c == k) {
+                            cidx[c] = e.right_index;
+                            ckind[c] = e.right_kind;
+                        }
+                    }
                     ++k;
                 }
-                for (int c = 0; c < k; ++c)
-                    k_int += (ckind[c] == k_kind_internal) ? 1u : 0u;
+#pragma unroll
+                for (int c = 0; c < 4; ++c)
+                    k_int += (c < k && ckind[c] == k_kind_internal) ? 1u : 0u;
             }
         }
 
@@ -430,43 +444,44 @@ __global__ void __launch_bounds__(k_block) k_collapse_level(collapse_params p, i
             std::uint32_t const id_first = base + n_in + out_first;
             std::uint32_t const node_int = item.prefix_internal + (k_int > 0 ? k_int - 1u : 0u);
             std::uint32_t const node_pk = item.prefix_packed + static_cast<std::uint32_t>(k - 1);
-            node4 nd;
+            // only a broken binary hierarchy can produce more items than the list holds
+            bool const room = static_cast<std::uint64_t>(out_first) + k_int <= p.list_capacity;
+            if (!room)
+                atomicOr(p.status, k_err_collapse);
+            bool const node_ok = w < p.node_capacity;
+            if (!node_ok)
+                atomicOr(p.status, k_err_collapse);
+            float4 *const dst = reinterpret_cast<float4 *>(p.nodes + (node_ok ? w : 0u));
             std::uint32_t m = 0;
+            // Each child is written as two 16-byte stores straight from registers.
 #pragma unroll
             for (int c = 0; c < 4; ++c) {
-                if (c >= k) {
-                    nd.c[c].bounds = aabb{0, 0, 0, 0, 0, 0};
-                    nd.c[c].reference = 0;
-                    continue;
-                }
-                if (ckind[c] == k_kind_leaf) {
-                    if (cidx[c] >= p.leaf_count) {
-                        atomicOr(p.status, k_err_collapse);
-                        nd.c[c].bounds = aabb{0, 0, 0, 0, 0, 0};
-                        nd.c[c].reference = 0;
-                        continue;
+                aabb bb{0, 0, 0, 0, 0, 0};
+                std::uint64_t ref = 0;
+                if (c < k) {
+                    if (ckind[c] == k_kind_leaf) {
+                        if (cidx[c] < p.leaf_count) {
+                            bb = p.leaf_aabbs[cidx[c]];
+                            ref = make_ref(cidx[c], 1u);
+                        } else {
+                            atomicOr(p.status, k_err_collapse);
+                        }
+                    } else {
+                        if (cidx[c] < p.leaf_count - 1)
+                            bb = p.binary_bounds[cidx[c]];
+                        else
+                            atomicOr(p.status, k_err_collapse);
+                        ref = make_ref(id_first + m, 0u);
+                        if (room)
+                            items_out[out_first + m] = collapse_item{cidx[c], node_int, node_pk};
+                        ++m;
                     }
-                    nd.c[c].bounds = p.leaf_aabbs[cidx[c]];
-                    nd.c[c].reference = make_ref(cidx[c], 1u);
-                } else {
-                    std::uint32_t const id = id_first + m;
-                    nd.c[c].bounds = p.binary_bounds[cidx[c]];
-                    nd.c[c].reference = make_ref(id, 0u);
-                    if (static_cast<std::uint64_t>(out_first) + m < p.list_capacity)
-                        items_out[out_first + m] = collapse_item{cidx[c], node_int, node_pk};
-                    else
-                        atomicOr(p.status, k_err_collapse);
-                    ++m;
                 }
-            }
-            if (w < p.node_capacity) {
-                float4 const *src = reinterpret_cast<float4 const *>(&nd);
-                float4 *dst = reinterpret_cast<float4 *>(&p.nodes[w]);
-#pragma unroll
-                for (int q = 0; q < 8; ++q)
-                    dst[q] = src[q];
-            } else {
-                atomicOr(p.status, k_err_collapse);
+                if (node_ok) {
+                    dst[2 * c] = make_float4(bb.min_x, bb.min_y, bb.min_z, bb.max_x);
+                    dst[2 * c + 1] = make_float4(bb.max_y, bb.max_z, __uint_as_float(static_cast<std::uint32_t>(ref)),
+                                                 __uint_as_float(static_cast<std::uint32_t>(ref >> 32)));
+                }
             }
             atomicMax(&p.stack_bounds[0], node_int);
             atomicMax(&p.stack_bounds[1], node_pk);
