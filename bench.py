@@ -18,6 +18,7 @@ all host threads) on bounded samples of the same workload.
 from __future__ import annotations
 
 import argparse
+import faulthandler
 import json
 import os
 import statistics
@@ -39,6 +40,12 @@ ORDER = 2
 BETA = 3.5
 N_QUERIES = 10_000_000
 ERROR_SUBSET = 100_000
+# the autotuner's candidate accuracy scales and the fraction of the 1e-3 bound it must meet on its sample
+SELECT_SCALES = (2.0, 2.5, 3.0, 3.25, 3.5, 4.0, 5.0)
+SELECT_MARGIN = 0.8
+# batched workload: quality check interval (frames) and surface-area cost ratio that triggers a rebuild
+REBUILD_EVERY = 10
+REBUILD_THRESHOLD = 1.25
 MOMENT_BYTES = {0: 112, 1: 208, 2: 368}
 
 
@@ -913,7 +920,71 @@ def run_batched_workload(args) -> None:
     loop_ms, max_diff = sharding.max_over_ranks([loop_ms, max_diff])
     sg_ms = sharding.max_over_ranks([sg_ms if sg_ms is not None else -1.0])[0]
     del graph
+
+    # ---- the same 100 frames from the rest shape with a quality-driven rebuild: every
+    # REBUILD_EVERY frames the trees' surface-area cost ratios are read and the meshes past
+    # REBUILD_THRESHOLD are rebuilt (H-PLOC) in place; the graph is captured again after a rebuild.
+    # A frame's time includes the check, the rebuild and the re-capture that precede it.
+    def capture():
+        gr = torch.cuda.CUDAGraph()
+        with torch.cuda.stream(side):
+            with torch.cuda.graph(gr, stream=side):
+                deform()
+                assert batch.frame(side.cuda_stream).is_ok()
+        torch.cuda.synchronize()
+        return gr
+
+    # the per-mesh loop above refit moments into new objects: a new batch over trees and moments
+    # built again from the rest shape, with the launch shape the autotuner chose for the first
     batch.release()
+    X.copy_(X0)
+    fidx.zero_()
+    for geo, bvh, mom, *_ in objs:
+        assert g.gwn_build_bvh(geo, bvh, g.gwn_bvh_build_options(method=0, hploc_search_radius=8)).is_ok()
+        assert g.gwn_refit_bvh_moment(order, bvh, mom).is_ok()
+    batch = g.gwn_batch(objs, accuracy_scale=beta, stream=stream)
+    assert batch.ok(), batch.status.message
+    assert batch.set_tuning(tuning["refit_block"], tuning["query_block"], tuning["per_thread"], tuning["sorted"],
+                            tuning["grid_scale"]).is_ok()
+    assert batch.frame(cur.cuda_stream).is_ok()  # one frame outside capture (no deformation)
+    torch.cuda.synchronize()
+    rgraph = capture()
+    X.copy_(X0)
+    fidx.zero_()
+    rb_lat, rb_events, rebuilds, checks = [], [], 0, 0
+    for f in range(frames):
+        extra_ms = 0.0
+        if f > 0 and f % REBUILD_EVERY == 0:
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            st, nreb = batch.rebuild(REBUILD_THRESHOLD)
+            assert st.is_ok(), st.message
+            checks += 1
+            if nreb:
+                rebuilds += nreb
+                del rgraph
+                rgraph = capture()
+            torch.cuda.synchronize()
+            extra_ms = (time.perf_counter() - t0) * 1e3
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(cur)
+        rgraph.replay()
+        e1.record(cur)
+        rb_events.append((e0, e1, extra_ms))
+    torch.cuda.synchronize()
+    assert batch.sync().is_ok()
+    rb_lat = np.array(sharding.max_over_ranks([a.elapsed_time(b) + x for a, b, x in rb_events]))
+    rb_stages_end = stage_ms()
+    _, ratios_end = batch.quality()
+    del rgraph
+    batch.release()
+    rebuild_policy = {
+        "policy": f"every {REBUILD_EVERY} frames: surface-area cost ratio of each refit tree against its build; "
+                  f"meshes above {REBUILD_THRESHOLD} rebuilt (H-PLOC r=8) in place, graph captured again",
+        "frames_per_s": frames / (float(rb_lat.sum()) / 1e3), "frame_ms_p50": float(np.percentile(rb_lat, 50)),
+        "frame_ms_p99": float(np.percentile(rb_lat, 99)), "checks": checks, "meshes_rebuilt": int(rebuilds),
+        "stage_ms_frame_100": rb_stages_end, "max_cost_ratio_frame_100": float(max(ratios_end) if ratios_end else 1.0),
+        "timing": "device time of each replay plus the host-synchronous check, rebuild and re-capture before it"}
     total_ms = float(lat.sum())
     if rank != 0:
         return
@@ -937,7 +1008,8 @@ def run_batched_workload(args) -> None:
                                        "gwn_refit_bvh, gwn_refit_bvh_moment<1>, Taylor batch), oracle/_ref, sm_100a; "
                                        "wall clock per frame over all meshes",
                    "max_abs_diff_vs_per_mesh_loop": max_diff, "tuning": tuning,
-                   "stage_ms_frame_100": stages_end, "stage_ms_frame_50": stages_mid},
+                   "stage_ms_frame_100": stages_end, "stage_ms_frame_50": stages_mid,
+                   "with_rebuild": rebuild_policy},
         "gpu_launches": frame_launches * frames,  # the library kernels recorded in one frame's graph
         "clocks": clocks.summary(),
     }
@@ -1486,6 +1558,7 @@ def run_antipodal_workload(args) -> None:
 
 
 def main() -> None:
+    faulthandler.enable()  # a crash in native code prints the Python stack that led to it
     args = parse()
     if args.profile is not None:
         run_profile(args)
@@ -1675,6 +1748,21 @@ def main() -> None:
         e = np.abs(out[sub].double().cpu().numpy() - ref64_h)
         ours_points[(o, b)] = {"ms_per_batch": ms, "queries_per_s": n / (ms / 1e3), "max_err_vs_fp64": float(e.max()),
                                "p99_err_vs_fp64": float(np.quantile(e, 0.99))}
+    # ---- the autotuner's pick for the same bound (untimed): order and accuracy scale chosen on a
+    # sample disjoint from the error subset, with the bound tightened by SELECT_MARGIN for the gap
+    # between a sample's maximum and the whole batch's ----
+    sel_sample = slice(sub.stop, min(sub.stop + ERROR_SUBSET, n))
+    tuned = None
+    if sel_sample.stop > sel_sample.start:
+        st, tuned = api.select_taylor_form(geo, bvh, dict(sorted(moms.items())),
+                                           *[d[sel_sample] for d in dq], max_error=1e-3 * SELECT_MARGIN,
+                                           accuracy_scales=SELECT_SCALES, stream=stream)
+        tuned = {"ok": st.is_ok(), **(tuned if st.is_ok() else {"message": st.message})}
+        if st.is_ok():
+            tuned["agrees_with_headline"] = (tuned["order"], tuned["accuracy_scale"]) == (args.order, args.beta)
+        tuned.update({"sample": f"queries [{sel_sample.start}, {sel_sample.stop}) of the batch",
+                      "bound_on_sample": 1e-3 * SELECT_MARGIN, "accuracy_scales": list(SELECT_SCALES),
+                      "near_field": "compensated"})
     sg = None
     if rank == 0:
         sg = smallgwn_taylor_points(mesh, q, sub, ref64_h, points)
@@ -1699,6 +1787,7 @@ def main() -> None:
                       f"flushed before each batch",
             **head}
         cfg["over_smallgwn"] = None if head is None else (value / world) / head["queries_per_s"]
+        cfg["autotuned_form"] = tuned
         cfg["taylor_at_scale_points"] = [
             {"order": o, "accuracy_scale": b, "ours": ours_points[(o, b)],
              "smallgwn": None if sg is None else sg.get((o, b)),

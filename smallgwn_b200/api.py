@@ -247,6 +247,12 @@ def gwn_update_geometry(obj: gwn_geometry_object, x, y, z, stream=None) -> gwn_s
     return _status(rc)
 
 
+def _assign(view, value) -> None:
+    """Overwrites a view structure in place, so that C code holding its address (a batch lends the
+    BVH and moment objects of its meshes) keeps seeing the object rather than a dropped copy."""
+    C.memmove(C.addressof(view), C.addressof(value), C.sizeof(view))
+
+
 class gwn_bvh4_object(_stream_mixin):
     """Mirror of gwn::gwn_bvh4_object<float, uint32_t> (include/gwn/gwn_bvh.cuh:329-381)."""
 
@@ -266,7 +272,7 @@ class gwn_bvh4_object(_stream_mixin):
     def clear(self) -> None:
         if self._view.primitive_count or self._view.aux:
             _lib.load().gwnb_bvh4_release_f32(C.byref(self._view), _stream(self._stream))
-        self._view = _lib.bvh4_f32()
+        _assign(self._view, _lib.bvh4_f32())
 
     def __del__(self) -> None:
         try:
@@ -285,7 +291,7 @@ def gwn_build_bvh(geometry: gwn_geometry_object, bvh: gwn_bvh4_object,
     if rc != _lib.GWNB_OK:
         return _status(rc)
     bvh.clear()
-    bvh._view = staging
+    _assign(bvh._view, staging)
     bvh.set_stream(stream)
     return gwn_status()
 
@@ -321,7 +327,7 @@ class gwn_bvh4_moment_object(_stream_mixin):
     def clear(self) -> None:
         if self._view.nodes or self._view.aux:
             _lib.load().gwnb_moment4_release_f32(C.byref(self._view), _stream(self._stream))
-        self._view = _lib.moment4_f32(order=self.order)
+        _assign(self._view, _lib.moment4_f32(order=self.order))
 
     def __del__(self) -> None:
         try:
@@ -339,7 +345,7 @@ def gwn_refit_bvh_moment(order: int, bvh: gwn_bvh4_object, moment: gwn_bvh4_mome
     if rc != _lib.GWNB_OK:
         return _status(rc)
     moment.clear()
-    moment._view = staging
+    _assign(moment._view, staging)
     moment.set_stream(stream)
     return gwn_status()
 
@@ -682,13 +688,13 @@ def load_scene(path, stream=None):
     geo._view = g
     geo.set_stream(stream)
     bvh = gwn_bvh4_object()
-    bvh._view = b
+    _assign(bvh._view, b)
     bvh.set_stream(stream)
     moments = {}
     for order in range(3):
         if mask.value & (1 << order):
             mo = gwn_bvh4_moment_object(order)
-            mo._view = ms[order]
+            _assign(mo._view, ms[order])
             mo.set_stream(stream)
             moments[order] = mo
     return gwn_status(), geo, bvh, moments

@@ -25,8 +25,17 @@
 #include <string>
 #include <vector>
 
+// The arrays a mesh's BVH and moment objects held when the batch derived its descriptors from them.
+struct gwnb_batch_ident {
+    void const *bvh_nodes;
+    void const *bvh_aux;
+    void const *moment_nodes;
+    void const *moment_aux;
+};
+
 struct gwnb_batch {
     std::vector<gwnb_batch_mesh_f32> meshes; // the caller's mesh descriptors (objects updated in place)
+    std::vector<gwnb_batch_ident> idents;    // per mesh, the arrays the device descriptors point into
     std::vector<double> base_cost;           // surface-area cost of each tree when built
     float beta = 2.0f;
     gwnb_taylor_options options{};
@@ -161,6 +170,10 @@ int prepare_states(gwnb_batch *b, cudaStream_t s) {
         r.fp64_count = a->fp64_count;
         r.status = a->status;
     }
+    b->idents.resize(mesh_count);
+    for (uint32_t i = 0; i < mesh_count; ++i)
+        b->idents[i] = gwnb_batch_ident{b->meshes[i].bvh->nodes, b->meshes[i].bvh->aux, b->meshes[i].moment->nodes,
+                                        b->meshes[i].moment->aux};
     GWNB_TRY(batch_refit_prepare(geoms.data(), b->bvhs.data(), moms.data(), mesh_count, b->order, &b->refit, s));
     GWNB_TRY(batch_query_prepare(reqs.data(), mesh_count, &b->query, s));
     if (b->d_status == nullptr)
@@ -174,7 +187,25 @@ int prepare_states(gwnb_batch *b, cudaStream_t s) {
     return GWNB_OK;
 }
 
+// The batch's device descriptors point into its meshes' BVH and moment arrays as they were when
+// it derived them. A BVH built again or moments refit into new arrays outside the batch (the caller
+// replacing an object it lent) leave those pointers dangling: every entry point that launches over
+// or reads the meshes refuses the batch from then on.
+int check_current(gwnb_batch const *b) {
+    for (std::size_t i = 0; i < b->meshes.size(); ++i) {
+        gwnb_batch_mesh_f32 const &m = b->meshes[i];
+        gwnb_batch_ident const &id = b->idents[i];
+        if (m.bvh->nodes != id.bvh_nodes || m.bvh->aux != id.bvh_aux || m.moment->nodes != id.moment_nodes ||
+            m.moment->aux != id.moment_aux)
+            return set_error(GWNB_INVALID_ARGUMENT,
+                             "batch: mesh " + std::to_string(i) + "'s BVH or moments were replaced after the batch "
+                             "was made (a build or moment refit outside the batch); make a new batch.");
+    }
+    return GWNB_OK;
+}
+
 int run_stages(gwnb_batch *b, gwnb_batch_tuning const &t, unsigned stages, cudaStream_t s) {
+    GWNB_TRY(check_current(b));
     bool const bounds = (stages & GWNB_BATCH_REFIT) != 0u, moments = (stages & GWNB_BATCH_MOMENTS) != 0u;
     if (bounds || moments)
         GWNB_TRY(batch_refit_launch(b->refit, t.refit_block, bounds, moments, s));
@@ -264,6 +295,7 @@ int gwnb_batch_create_f32(const gwnb_batch_mesh_f32 *meshes, uint32_t mesh_count
 int gwnb_batch_quality_f32(gwnb_batch *b, float *cost_ratio, gwnb_stream_t stream) try {
     if (b == nullptr || cost_ratio == nullptr)
         return set_error(GWNB_INVALID_ARGUMENT, "batch: null handle or output.");
+    GWNB_TRY(check_current(b));
     std::vector<double> cost;
     GWNB_TRY(tree_costs(b, cost, as_cuda(stream)));
     for (std::size_t i = 0; i < cost.size(); ++i)
@@ -279,28 +311,42 @@ int gwnb_batch_rebuild_f32(gwnb_batch *b, float threshold, int method, uint32_t 
         return set_error(GWNB_INVALID_ARGUMENT, "batch: null handle.");
     if (!(threshold >= 1.0f))
         return set_error(GWNB_INVALID_ARGUMENT, "batch: the rebuild threshold is a cost ratio of at least 1.");
+    GWNB_TRY(check_current(b));
     cudaStream_t const s = as_cuda(stream);
     std::vector<double> cost;
     GWNB_TRY(tree_costs(b, cost, s));
     std::uint32_t count = 0;
     std::vector<char> redo(b->meshes.size(), 0);
-    for (std::size_t i = 0; i < b->meshes.size(); ++i) {
+    int rc = GWNB_OK;
+    for (std::size_t i = 0; i < b->meshes.size() && rc == GWNB_OK; ++i) {
         if (!(cost[i] > threshold * b->base_cost[i]))
             continue;
-        redo[i] = 1;
         gwnb_batch_mesh_f32 &m = b->meshes[i];
+        // both new objects first: on failure the mesh keeps its current BVH and moments
         gwnb_bvh4_f32 fresh{};
-        GWNB_TRY(gwnb_bvh4_build_f32(&m.geometry, method, radius, 64, &fresh, stream));
+        if ((rc = gwnb_bvh4_build_f32(&m.geometry, method, radius, 64, &fresh, stream)) != GWNB_OK)
+            break;
+        gwnb_moment4_f32 mom{};
+        if ((rc = gwnb_moment4_refit_f32(&fresh, b->order, &mom, stream)) != GWNB_OK) {
+            gwnb_bvh4_release_f32(&fresh, stream);
+            break;
+        }
         gwnb_bvh4_release_f32(m.bvh, stream);
         *m.bvh = fresh;
-        gwnb_moment4_f32 mom{};
-        GWNB_TRY(gwnb_moment4_refit_f32(m.bvh, b->order, &mom, stream));
         gwnb_moment4_release_f32(m.moment, stream);
         *m.moment = mom;
+        redo[i] = 1;
         ++count;
     }
     if (count > 0) {
-        GWNB_TRY(prepare_states(b, s));
+        // the descriptors follow the replaced objects even when a later mesh failed
+        int const prc = prepare_states(b, s);
+        if (rc == GWNB_OK)
+            rc = prc;
+    }
+    if (rc != GWNB_OK)
+        return rc;
+    if (count > 0) {
         GWNB_TRY(tree_costs(b, cost, s));
         for (std::size_t i = 0; i < cost.size(); ++i)
             if (redo[i])
@@ -398,6 +444,7 @@ int gwnb_batch_tune_f32(gwnb_batch *b, int reps, gwnb_batch_tuning *chosen, gwnb
 int gwnb_batch_sync_f32(gwnb_batch *b, gwnb_stream_t stream) try {
     if (b == nullptr)
         return set_error(GWNB_INVALID_ARGUMENT, "batch: null handle.");
+    GWNB_TRY(check_current(b));
     cudaStream_t const s = as_cuda(stream);
     GWNB_CUDA_TRY(cudaMemsetAsync(b->d_flags, 0, sizeof(unsigned int), s));
     note_launch(), k_gather_status<<<1, 256, 0, s>>>(b->d_status, static_cast<std::uint32_t>(b->status_words.size()), b->d_flags);

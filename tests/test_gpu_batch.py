@@ -59,10 +59,13 @@ def make_batch(cuda, sizes, seed=4):
 
 
 def per_mesh(cuda, objs, refit: bool):
+    """The per-mesh path of plain calls. With refit, the BVH is refit in place and the moments go to a
+    moment object of its own: the batch's moment objects stay the ones it was made over."""
     res = []
     for geo, bvh, mom, qx, qy, qz, _ in objs:
         if refit:
             assert g.gwn_refit_bvh(geo, bvh).is_ok()
+            mom = g.gwn_bvh4_moment_object(ORDER)
             assert g.gwn_refit_bvh_moment(ORDER, bvh, mom).is_ok()
         o = cuda.empty_like(qx)
         assert g.gwn_compute_winding_number_taylor_batch(ORDER, bvh, mom, qx, qy, qz, o, accuracy_scale=BETA).is_ok()
@@ -183,3 +186,38 @@ def test_quality_driven_rebuild(cuda):
     for a, b in zip(outputs(cuda, objs), per_mesh(cuda, objs, refit=True)):
         np.testing.assert_array_equal(a, b)
     batch.release()
+
+
+def test_replaced_objects_are_refused(cuda):
+    """A batch's device descriptors point into the arrays of the BVH and moment objects it was made
+    over. Moments refit into a new object in place of one of them (or a BVH built again) leave those
+    pointers dangling: every entry point then refuses the batch with invalid_argument instead of
+    launching over released arrays, and a new batch over the same objects works."""
+    X, objs = make_batch(cuda, [20, 28, 16], seed=5)
+    batch = g.gwn_batch(objs, accuracy_scale=BETA)
+    assert batch.ok(), batch.status.message
+    assert batch.frame().is_ok() and batch.sync().is_ok()
+    geo, bvh, mom = objs[1][:3]
+    assert g.gwn_refit_bvh_moment(ORDER, bvh, mom).is_ok()  # new moment arrays for mesh 1
+    st = batch.frame()
+    assert st.error == g.gwn_error.invalid_argument and "mesh 1" in st.message and "replaced" in st.message
+    assert batch.run(batch.QUERY).error == g.gwn_error.invalid_argument
+    assert batch.sync().error == g.gwn_error.invalid_argument
+    assert batch.quality()[0].error == g.gwn_error.invalid_argument
+    assert batch.rebuild(1.5)[0].error == g.gwn_error.invalid_argument
+    assert batch.tune(repetitions=1)[0].error == g.gwn_error.invalid_argument
+    batch.release()
+    # a BVH built again is refused the same way
+    fresh = g.gwn_batch(objs, accuracy_scale=BETA)
+    assert fresh.ok(), fresh.status.message
+    assert g.gwn_build_bvh(objs[2][0], objs[2][1], g.gwn_bvh_build_options(method=0)).is_ok()
+    assert fresh.frame().error == g.gwn_error.invalid_argument
+    fresh.release()
+    # objects rebuilt and refit, then a new batch: frames equal the per-mesh path again
+    assert g.gwn_refit_bvh_moment(ORDER, objs[2][1], objs[2][2]).is_ok()
+    again = g.gwn_batch(objs, accuracy_scale=BETA)
+    assert again.ok(), again.status.message
+    assert again.frame().is_ok() and again.sync().is_ok()
+    for a, b in zip(outputs(cuda, objs), per_mesh(cuda, objs, refit=False)):
+        np.testing.assert_array_equal(a, b)
+    again.release()
