@@ -597,7 +597,9 @@ typedef struct gwnb_batch_tuning {
 
 /* Creates a batch over `mesh_count` meshes (copies the descriptors; the pointed-to objects must
  * outlive the batch). Computes each mesh's query order. While the batch exists its frames refit the
- * BVHs and moments in place and leave their revisions unchanged. */
+ * BVHs and moments in place and leave their revisions unchanged. A BVH or moment object given new
+ * arrays outside the batch (built again, moments refit into it) makes every later call on the
+ * batch except release return GWNB_INVALID_ARGUMENT. */
 GWNB_API int gwnb_batch_create_f32(const gwnb_batch_mesh_f32 *meshes, uint32_t mesh_count, float accuracy_scale,
                                    const gwnb_taylor_options *options, gwnb_batch **batch, gwnb_stream_t stream);
 /* Times `repetitions` frames of every candidate launch shape on `stream` and keeps the fastest
