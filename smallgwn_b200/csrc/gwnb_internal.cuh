@@ -209,6 +209,10 @@ int host_exception() noexcept;
 std::uint64_t reserve_revision();
 int device_sm_count();
 
+// Keys per tile of the 32-bit radix sort (256 threads x 12 keys): callers that size the sort's
+// scratch themselves (the allocation-free Taylor batch) use it.
+constexpr std::uint64_t k_sort_tile_u32 = 3072;
+
 // Polls after which a device-side wait (the look-back of the radix sort and of the BVH4 collapse)
 // gives up, sets k_err_wait_timeout and lets its launch complete. Read by the host when a kernel is
 // launched; 2^22 by default, settable with gwnb_set_wait_limit.

@@ -29,8 +29,8 @@ namespace {
 
 constexpr std::uint64_t k_capacity = GWNB_NOALLOC_MAX_QUERIES;
 // five regions of k_capacity words (codes, sorted codes, order, two sort buffers) plus the sort's
-// histograms, tile counters and tile status: 4 passes x (256 + 1 + 256 per 4096-key tile)
-constexpr std::uint64_t k_sort_words = 4 * 256 + 4 + 4 * ((k_capacity + 4095) / 4096) * 256;
+// histograms, tile counters and tile status: 4 passes x (256 + 1 + 256 per sort tile)
+constexpr std::uint64_t k_sort_words = 4 * 256 + 4 + 4 * ((k_capacity + k_sort_tile_u32 - 1) / k_sort_tile_u32) * 256;
 constexpr std::uint64_t k_scratch_words = 5 * k_capacity + k_sort_words;
 
 static __device__ __align__(256) std::uint32_t g_noalloc_scratch[k_scratch_words];
