@@ -215,6 +215,7 @@ struct taylor_params {
     float const *qy;
     float const *qz;
     std::uint32_t const *order; // sorted position -> query index (nullptr: identity)
+    int gathered;               // 1: qx/qy/qz are already in sorted order (read at the sorted position)
     float *out;
     float *grad_x;
     float *grad_y;
@@ -238,7 +239,8 @@ __device__ __forceinline__ void taylor_thread_item(taylor_params const &p, std::
     if (idx >= p.n)
         return;
     std::uint32_t const qi = p.order != nullptr ? p.order[idx] : static_cast<std::uint32_t>(idx);
-    float const qx = p.qx[qi], qy = p.qy[qi], qz = p.qz[qi];
+    std::uint64_t const li = p.gathered ? idx : qi;
+    float const qx = p.qx[li], qy = p.qy[li], qz = p.qz[li];
     accum<Mode == GWNB_NEAR_COMPENSATED> omega;
     float gx = 0.0f, gy = 0.0f, gz = 0.0f;
     std::uint32_t st_nodes = 0, st_far = 0, st_near = 0;
@@ -408,9 +410,10 @@ __device__ __forceinline__ void taylor_warp_item(taylor_params const &p, std::ui
     if (full == 0u)
         return;
     std::uint32_t const qi = valid ? (p.order != nullptr ? p.order[idx] : static_cast<std::uint32_t>(idx)) : 0u;
-    float const qx = valid ? p.qx[qi] : 0.0f;
-    float const qy = valid ? p.qy[qi] : 0.0f;
-    float const qz = valid ? p.qz[qi] : 0.0f;
+    std::uint64_t const li = p.gathered ? idx : qi;
+    float const qx = valid ? p.qx[li] : 0.0f;
+    float const qy = valid ? p.qy[li] : 0.0f;
+    float const qz = valid ? p.qz[li] : 0.0f;
     accum<Mode == GWNB_NEAR_COMPENSATED> omega;
     float gx = 0.0f, gy = 0.0f, gz = 0.0f;
     std::uint32_t st_nodes = 0, st_far = 0, st_near = 0;
@@ -718,6 +721,19 @@ int query_order(aabb const *root_bounds, float const *qx, float const *qy, float
 
 
 namespace {
+__global__ void __launch_bounds__(256)
+    k_gather_queries(std::uint32_t const *__restrict__ order, float const *__restrict__ qx,
+                     float const *__restrict__ qy, float const *__restrict__ qz, std::uint64_t n,
+                     float *__restrict__ sx, float *__restrict__ sy, float *__restrict__ sz) {
+    std::uint64_t const i = static_cast<std::uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    std::uint32_t const j = order[i];
+    sx[i] = __ldg(qx + j);
+    sy[i] = __ldg(qy + j);
+    sz[i] = __ldg(qz + j);
+}
+
 taylor_params make_taylor_params(taylor_request const &r) {
     taylor_params p{};
     p.qnodes = r.qnodes;
@@ -750,6 +766,7 @@ int taylor_batch(taylor_request const &r, cudaStream_t s) {
         return GWNB_OK;
     taylor_params p = make_taylor_params(r);
     std::uint32_t *codes = nullptr, *sorted_codes = nullptr, *order = nullptr;
+    float *gathered = nullptr;
     bool const sorted = r.sort_queries != 0 && r.n > 1 && r.root_bounds != nullptr;
     if (sorted) {
         GWNB_TRY(alloc(&codes, r.n, s));
@@ -759,6 +776,16 @@ int taylor_batch(taylor_request const &r, cudaStream_t s) {
                                                                             r.root_bounds, codes);
         GWNB_TRY(radix_sort_pairs(codes, sorted_codes, nullptr, order, r.n, 4, 30, s, r.status));
         p.order = order;
+        // the queries themselves in traversal order: the traversal then reads them contiguously
+        release(sorted_codes, s);
+        sorted_codes = nullptr;
+        GWNB_TRY(alloc(&gathered, 3 * r.n, s));
+        note_launch(), k_gather_queries<<<static_cast<unsigned>((r.n + 255) / 256), 256, 0, s>>>(
+            order, r.qx, r.qy, r.qz, r.n, gathered, gathered + r.n, gathered + 2 * r.n);
+        p.qx = gathered;
+        p.qy = gathered + r.n;
+        p.qz = gathered + 2 * r.n;
+        p.gathered = 1;
     }
     bool const grad = r.gx != nullptr;
     bool const stats = r.stat_nodes != nullptr;
@@ -784,6 +811,7 @@ int taylor_batch(taylor_request const &r, cudaStream_t s) {
     release(codes, s);
     release(sorted_codes, s);
     release(order, s);
+    release(gathered, s);
     return rc;
 }
 
