@@ -57,13 +57,15 @@ def parse() -> argparse.Namespace:
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="taylor",
                     choices=["taylor", "adjoint", "precision", "exact", "batched", "distance", "ray", "antipodal",
-                             "build"],
+                             "build", "stages"],
                     help="taylor: the headline (1M-triangle sphere, 10M queries); adjoint: forward + backward "
                          "on the 159k-triangle soup; precision: 8.4M-triangle sphere, 100M near-surface queries "
                          "in 16M chunks; exact: brute-force exact batch on the small icosphere; distance / ray: "
                          "unsigned distance / ray first hit on the 1M-triangle sphere, 10M queries / rays; "
                          "antipodal: antipodal winding numbers on the 159k-triangle open soup, 200k queries; "
-                         "build: H-PLOC / LBVH builds, refit and moment refits of the 1M-triangle sphere")
+                         "build: H-PLOC / LBVH builds, refit and moment refits of the 1M-triangle sphere; "
+                         "stages: every stage of smallgwn's benchmark harness on the 1M-triangle sphere")
+    ap.add_argument("--csv", default=None, help="stages: also write smallgwn's CSV schema to this path")
     ap.add_argument("--queries", type=int, default=N_QUERIES)
     ap.add_argument("--order", type=int, default=ORDER)
     ap.add_argument("--beta", type=float, default=BETA)
@@ -1166,6 +1168,80 @@ def run_build_workload(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+def run_stages_workload(args) -> None:
+    """Every stage of smallgwn's benchmark harness (smallgwn_b200/stages.py: its stage names, units,
+    timing rule and CSV schema) on the 1M-triangle sphere with the harness defaults: 1M queries of its
+    seeded mix, 5 warm-up and 20 measured calls each synchronized, accuracy scale 2, stack capacity
+    96, H-PLOC; query_exact is skipped as with the harness's --skip-exact (10^12 pairs per call on this
+    mesh). `value` is the query_taylor_o2 stage's queries/s. Beside it, smallgwn's own kernels
+    (oracle/_ref) on the same mesh and queries for the stages they time (averages of CUDA-event-timed
+    calls with the L2 flushed before each, where the harness does not flush: a baseline, not part of
+    the value)."""
+    import torch
+
+    from smallgwn_b200 import meshes, stages
+
+    dev = torch.cuda.current_device()
+    mesh = meshes.sphere_mesh()
+    opts = stages.options(skip_exact=True)
+    with ClockSampler(dev) as clocks:
+        results, context = stages.run_model(mesh, opts)
+    rows = {r.stage: ({"mean_ms": r.latency_mean_ms, "p50_ms": r.latency_p50_ms, "p95_ms": r.latency_p95_ms,
+                       "throughput_per_s": r.throughput_per_s, "unit": r.unit} if r.success else
+                      {"success": False, "error_message": r.error_message}) for r in results}
+    if args.csv:
+        Path(args.csv).write_text(stages.csv_rows(
+            results, context, "synthetic:displaced_uv_sphere_1024x512_seed2", opts, torch.cuda.get_device_name(),
+            0, time.strftime("%Y-%m-%dT%H:%M:%SZ", time.gmtime())))
+    sg = smallgwn_stage_times(mesh, opts)
+    head = rows["query_taylor_o2"]
+    line = {
+        "metric": "smallgwn harness stage query_taylor_o2 queries/s (1M-triangle sphere, 1M harness queries)",
+        "value": head.get("throughput_per_s"), "unit": "queries/s", "n_gpus": 1, "steps": opts.measure_iters,
+        "warmup": opts.warmup_iters, "ms_per_step": head.get("mean_ms"), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "displaced UV sphere 1024x512 (1,046,528 tris, seed 2), smallgwn's benchmark "
+                               "harness stages and defaults", "query_count": opts.query_count,
+                   "accuracy_scale": opts.accuracy_scale, "stack_capacity": opts.stack_capacity,
+                   "builder": opts.builder, "stream_sync_per_iter": opts.stream_sync_per_iter,
+                   "skip_exact": opts.skip_exact,
+                   "boundary_edge_count": context.get("boundary_edge_count"),
+                   "ray_mix_hit_ratio": context.get("ray_mix_hit_ratio"), "stages": rows,
+                   "smallgwn_kernels_mean_ms": sg,
+                   "over_smallgwn": {k: sg[k] / rows[k]["mean_ms"] for k in (sg or {})
+                                     if rows.get(k, {}).get("mean_ms")}},
+        "clocks": clocks.summary(),
+    }
+    print(json.dumps(line), flush=True)
+
+
+def smallgwn_stage_times(mesh, opts) -> dict | None:
+    """Mean ms of smallgwn's own kernels (oracle/_ref) for the harness stages they cover, on the same
+    mesh, its H-PLOC tree and the harness's queries and rays; None when oracle/_ref was not built."""
+    import oracle
+    from smallgwn_b200 import meshes
+
+    if oracle.ref_lib() is None:
+        return None
+    R = oracle.Reference(mesh)
+    try:
+        it = opts.measure_iters
+        out = {f"bvh_build_{opts.builder}": R.time_build(0 if opts.builder == "hploc" else 1, 8, 64, it)}
+        R.build(0 if opts.builder == "hploc" else 1, 8, 64)
+        out["refit_bvh"] = R.time_refit(-1, it)
+        q = meshes.reference_mixed_queries(mesh, opts.query_count, opts.seed)
+        for o in (0, 1, 2):
+            out[f"refit_moment_o{o}"] = R.time_refit(o, it)
+            R.refit_moments(o)
+            out[f"query_taylor_o{o}"] = R.time_taylor(o, *q, opts.accuracy_scale, opts.warmup_iters, it)
+        out["query_antipodal"] = R.time_antipodal(*q, 2, 5)
+        rays = meshes.reference_mixed_rays(mesh, opts.query_count, opts.seed)
+        out["query_ray_first_hit"] = R.time_spatial(*rays[:3], dirs=rays[3:], warmup=2, iters=5)
+        return out
+    finally:
+        R.close()
+
+
 def run_exact_workload(args) -> None:
     """Plain exact winding number, small: icosphere level 4 (5,120 triangles, radial noise seed 0),
     100k queries uniform in [-1.5, 1.5]^3 (seed 1), LBVH, exact batch; the oracle's FP32 brute force
@@ -1570,7 +1646,7 @@ def main() -> None:
         {"adjoint": run_adjoint_workload, "precision": run_precision_workload, "exact": run_exact_workload,
          "batched": run_batched_workload, "distance": run_spatial_workload,
          "ray": run_spatial_workload, "antipodal": run_antipodal_workload,
-         "build": run_build_workload}[args.workload](args)
+         "build": run_build_workload, "stages": run_stages_workload}[args.workload](args)
         return
     import torch
 

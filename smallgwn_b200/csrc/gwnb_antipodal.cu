@@ -670,6 +670,7 @@ using namespace gwnb;
 extern "C" {
 
 int gwnb_boundary_chain_build_u32(const gwnb_geometry_f32 *g, gwnb_boundary_chain_u32 *out, gwnb_stream_t stream) try {
+    GWNB_NVTX("gwnb::build_boundary_chain");
     if (out == nullptr)
         return set_error(GWNB_INVALID_ARGUMENT, "Boundary chain output is null.");
     if (!geometry_valid(g))
@@ -887,6 +888,7 @@ int gwnb_winding_antipodal_batch_f32(const gwnb_geometry_f32 *g, const gwnb_bvh4
                                      const gwnb_boundary_chain_u32 *chain, const float *qx, const float *qy,
                                      const float *qz, float *out, uint64_t n, const gwnb_spatial_options *options,
                                      gwnb_stream_t stream) try {
+    GWNB_NVTX("gwnb::query_antipodal");
     return antipodal_common(g, b, chain, qx, qy, qz, out, nullptr, nullptr, nullptr, n, options, stream);
 } catch (...) {
     return host_exception();
@@ -895,6 +897,7 @@ int gwnb_winding_antipodal_batch_f32(const gwnb_geometry_f32 *g, const gwnb_bvh4
 int gwnb_winding_gradient_antipodal_batch_f32(const gwnb_geometry_f32 *g, const gwnb_boundary_chain_u32 *chain,
                                               const float *qx, const float *qy, const float *qz, float *gx, float *gy,
                                               float *gz, uint64_t n, int block_size, gwnb_stream_t stream) try {
+    GWNB_NVTX("gwnb::query_antipodal_gradient");
     if (n > 0 && (gx == nullptr || gy == nullptr || gz == nullptr))
         return set_error(GWNB_INVALID_ARGUMENT, "Query/output spans require non-null storage when non-empty.");
     gwnb_spatial_options const o{block_size, 64, 0};

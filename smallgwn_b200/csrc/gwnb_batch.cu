@@ -235,6 +235,7 @@ extern "C" {
 
 int gwnb_batch_create_f32(const gwnb_batch_mesh_f32 *meshes, uint32_t mesh_count, float beta,
                           const gwnb_taylor_options *opt, gwnb_batch **out, gwnb_stream_t stream) try {
+    GWNB_NVTX("gwnb::batch.create");
     if (out == nullptr)
         return set_error(GWNB_INVALID_ARGUMENT, "batch: output handle must be non-null.");
     *out = nullptr;
@@ -293,6 +294,7 @@ int gwnb_batch_create_f32(const gwnb_batch_mesh_f32 *meshes, uint32_t mesh_count
 }
 
 int gwnb_batch_quality_f32(gwnb_batch *b, float *cost_ratio, gwnb_stream_t stream) try {
+    GWNB_NVTX("gwnb::batch.quality");
     if (b == nullptr || cost_ratio == nullptr)
         return set_error(GWNB_INVALID_ARGUMENT, "batch: null handle or output.");
     GWNB_TRY(check_current(b));
@@ -307,6 +309,7 @@ int gwnb_batch_quality_f32(gwnb_batch *b, float *cost_ratio, gwnb_stream_t strea
 
 int gwnb_batch_rebuild_f32(gwnb_batch *b, float threshold, int method, uint32_t radius, uint32_t *rebuilt,
                            gwnb_stream_t stream) try {
+    GWNB_NVTX("gwnb::batch.rebuild");
     if (b == nullptr)
         return set_error(GWNB_INVALID_ARGUMENT, "batch: null handle.");
     if (!(threshold >= 1.0f))
@@ -369,6 +372,7 @@ int gwnb_batch_set_tuning_f32(gwnb_batch *b, const gwnb_batch_tuning *t) try {
 }
 
 int gwnb_batch_frame_f32(gwnb_batch *b, gwnb_stream_t stream) try {
+    GWNB_NVTX("gwnb::batch.frame");
     if (b == nullptr)
         return set_error(GWNB_INVALID_ARGUMENT, "batch: null handle.");
     return frame(b, b->tuning, as_cuda(stream));
@@ -377,6 +381,7 @@ int gwnb_batch_frame_f32(gwnb_batch *b, gwnb_stream_t stream) try {
 }
 
 int gwnb_batch_run_f32(gwnb_batch *b, unsigned int stages, gwnb_stream_t stream) try {
+    GWNB_NVTX("gwnb::batch.run");
     if (b == nullptr)
         return set_error(GWNB_INVALID_ARGUMENT, "batch: null handle.");
     if ((stages & ~(GWNB_BATCH_REFIT | GWNB_BATCH_MOMENTS | GWNB_BATCH_QUERY)) != 0u)
@@ -387,6 +392,7 @@ int gwnb_batch_run_f32(gwnb_batch *b, unsigned int stages, gwnb_stream_t stream)
 }
 
 int gwnb_batch_tune_f32(gwnb_batch *b, int reps, gwnb_batch_tuning *chosen, gwnb_stream_t stream) try {
+    GWNB_NVTX("gwnb::batch.tune");
     if (b == nullptr || reps <= 0)
         return set_error(GWNB_INVALID_ARGUMENT, "batch: tuning needs a handle and a positive repetition count.");
     cudaStream_t const s = as_cuda(stream);

@@ -269,7 +269,9 @@ int build_impl(gwnb_geometry_f32 const *g, int method, std::uint32_t radius, int
     if ((rc = alloc(&rb, 1, s)) != GWNB_OK)
         return fail(rc);
     GWNB_CUDA_TRY(cudaMemsetAsync(rb, 0, sizeof(build_readback), s));
-    if ((rc = build_preprocess(*g, morton_bits, codes, b.primitive_indices, sorted_aabbs, s, status)) != GWNB_OK)
+    if ((rc = nvtx_call("gwnb::build.morton_sort", [&] {
+             return build_preprocess(*g, morton_bits, codes, b.primitive_indices, sorted_aabbs, s, status);
+         })) != GWNB_OK)
         return fail(rc);
     std::uint64_t capacity = 0;
     std::uint32_t root_binary = 0;
@@ -284,11 +286,15 @@ int build_impl(gwnb_geometry_f32 const *g, int method, std::uint32_t radius, int
         root_binary = 0;
         std::uint32_t *hploc_count = nullptr;
         if (method == GWNB_METHOD_LBVH) {
-            rc = build_binary_lbvh(codes, morton_bits, nt, sorted_aabbs, bin, bin_parent, bin_bounds, s, status);
+            rc = nvtx_call("gwnb::build.binary_lbvh", [&] {
+                return build_binary_lbvh(codes, morton_bits, nt, sorted_aabbs, bin, bin_parent, bin_bounds, s, status);
+            });
         } else {
             hploc_count = &rb->hploc_count;
-            rc = build_binary_hploc(codes, morton_bits, nt, sorted_aabbs, radius, bin, bin_parent, bin_bounds,
-                                    &root_binary, s, status, hploc_count);
+            rc = nvtx_call("gwnb::build.binary_hploc", [&] {
+                return build_binary_hploc(codes, morton_bits, nt, sorted_aabbs, radius, bin, bin_parent, bin_bounds,
+                                          &root_binary, s, status, hploc_count);
+            });
         }
         if (rc != GWNB_OK)
             return fail(rc);
@@ -298,18 +304,22 @@ int build_impl(gwnb_geometry_f32 const *g, int method, std::uint32_t radius, int
             return fail(rc);
         b.node_capacity = ni;
         capacity = ni;
-        if ((rc = collapse_to_bvh4(bin, bin_bounds, sorted_aabbs, nt, root_binary, hploc_count,
-                                   reinterpret_cast<node4 *>(b.nodes), ni, &rb->collapse, false, s, status)) != GWNB_OK)
+        if ((rc = nvtx_call("gwnb::build.collapse", [&] {
+                 return collapse_to_bvh4(bin, bin_bounds, sorted_aabbs, nt, root_binary, hploc_count,
+                                         reinterpret_cast<node4 *>(b.nodes), ni, &rb->collapse, false, s, status);
+             })) != GWNB_OK)
             return fail(rc);
         b.root.reference = make_ref(0, 0);
     }
     // refit / query state: parent links and leaf-node list over the collapsed nodes (sized by the
     // node capacity; the kernels read the node count from the device), padded triangle records
     // written with the leaf-ordered ones
-    if ((rc = prepare_bvh_aux_async(&b, capacity, &rb->collapse, &rb->leaf_node_count, s)) != GWNB_OK)
-        return fail(rc);
-    if ((rc = build_triangles(*g, b.primitive_indices, nt, reinterpret_cast<triangle *>(b.triangles), aux->tri48,
-                              s, status)) != GWNB_OK)
+    if ((rc = nvtx_call("gwnb::build.records", [&] {
+             int const prc = prepare_bvh_aux_async(&b, capacity, &rb->collapse, &rb->leaf_node_count, s);
+             return prc != GWNB_OK ? prc
+                                   : build_triangles(*g, b.primitive_indices, nt,
+                                                     reinterpret_cast<triangle *>(b.triangles), aux->tri48, s, status);
+         })) != GWNB_OK)
         return fail(rc);
     GWNB_CUDA_TRY(cudaMemcpyAsync(aux->root_bounds, &rb->root_bounds, sizeof(aabb), cudaMemcpyDeviceToDevice, s));
     GWNB_CUDA_TRY(cudaMemcpyAsync(&rb->status, status, sizeof(unsigned int), cudaMemcpyDeviceToDevice, s));
@@ -442,6 +452,7 @@ const char *gwnb_version(void) { return "gwnb 0.1 (sm_100a)"; }
 int gwnb_geometry_upload_f32(gwnb_geometry_f32 *out, const float *x, const float *y, const float *z,
                              uint64_t nv, const uint32_t *i0, const uint32_t *i1, const uint32_t *i2,
                              uint64_t nt, gwnb_stream_t stream) try {
+    GWNB_NVTX("gwnb::upload_geometry");
     if (out == nullptr)
         return set_error(GWNB_INVALID_ARGUMENT, "gwnb_geometry_upload_f32 requires an output view.");
     if (nv > std::numeric_limits<std::uint32_t>::max())
@@ -520,6 +531,7 @@ static int update_common(gwnb_geometry_f32 *g, const float *x, const float *y, c
 
 int gwnb_geometry_update_f32(gwnb_geometry_f32 *g, const float *x, const float *y, const float *z, uint64_t nv,
                              gwnb_stream_t stream) try {
+    GWNB_NVTX("gwnb::update_geometry");
     return update_common(g, x, y, z, nv, stream, cudaMemcpyDefault);
 } catch (...) {
     return host_exception();
@@ -527,6 +539,7 @@ int gwnb_geometry_update_f32(gwnb_geometry_f32 *g, const float *x, const float *
 
 int gwnb_geometry_update_device_f32(gwnb_geometry_f32 *g, const float *x, const float *y, const float *z,
                                     uint64_t nv, gwnb_stream_t stream) try {
+    GWNB_NVTX("gwnb::update_geometry");
     return update_common(g, x, y, z, nv, stream, cudaMemcpyDeviceToDevice);
 } catch (...) {
     return host_exception();
@@ -539,6 +552,7 @@ void gwnb_geometry_release_f32(gwnb_geometry_f32 *g, gwnb_stream_t stream) {
 
 int gwnb_bvh4_build_f32(const gwnb_geometry_f32 *g, int method, uint32_t radius, int morton_bits,
                         gwnb_bvh4_f32 *out, gwnb_stream_t stream) try {
+    GWNB_NVTX("gwnb::bvh_build");
     if (out == nullptr)
         return set_error(GWNB_INVALID_ARGUMENT, "bvh.build: output view is null.");
     if (!geometry_valid(g))
@@ -667,6 +681,7 @@ int gwnb_radix_sort_pairs(const void *keys_in, void *keys_out, const uint32_t *v
 // ---- refit --------------------------------------------------------------------------------------
 
 int gwnb_bvh4_refit_async_f32(const gwnb_geometry_f32 *g, gwnb_bvh4_f32 *b, gwnb_stream_t stream) try {
+    GWNB_NVTX("gwnb::refit_bvh_async");
     if (!geometry_valid(g))
         return set_error(GWNB_INVALID_ARGUMENT, "bvh.refit: Geometry accessor is invalid.");
     if (!bvh_valid(b))
@@ -716,6 +731,7 @@ int gwnb_bvh4_sync_status_f32(gwnb_bvh4_f32 *b, gwnb_stream_t stream) try {
 }
 
 int gwnb_bvh4_refit_f32(const gwnb_geometry_f32 *g, gwnb_bvh4_f32 *b, gwnb_stream_t stream) try {
+    GWNB_NVTX("gwnb::refit_bvh");
     GWNB_TRY(gwnb_bvh4_refit_async_f32(g, b, stream));
     return gwnb_bvh4_sync_status_f32(b, stream);
 } catch (...) {
@@ -747,6 +763,7 @@ static int moment_alloc(gwnb_bvh4_f32 const *b, int order, gwnb_moment4_f32 &m, 
 }
 
 int gwnb_moment4_refit_f32(const gwnb_bvh4_f32 *b_in, int order, gwnb_moment4_f32 *out, gwnb_stream_t stream) try {
+    GWNB_NVTX("gwnb::refit_moment");
     if (out == nullptr)
         return set_error(GWNB_INVALID_ARGUMENT, "bvh.refit.moment: output view is null.");
     if (order < 0 || order > 2)
@@ -781,6 +798,7 @@ int gwnb_moment4_refit_f32(const gwnb_bvh4_f32 *b_in, int order, gwnb_moment4_f3
 }
 
 int gwnb_moment4_refit_async_f32(const gwnb_bvh4_f32 *b_in, gwnb_moment4_f32 *m, gwnb_stream_t stream) try {
+    GWNB_NVTX("gwnb::refit_moment_async");
     if (m == nullptr || !bvh_valid(b_in))
         return set_error(GWNB_INVALID_ARGUMENT, "bvh.refit.moment: BVH accessor is invalid for moment refit.");
     if (m->node_count != b_in->node_count || (b_in->node_count > 0 && m->aux == nullptr))
@@ -811,6 +829,7 @@ static int check_query_spans(const float *qx, const float *qy, const float *qz, 
 
 int gwnb_winding_exact_batch_f32(const gwnb_bvh4_f32 *b, const float *qx, const float *qy, const float *qz,
                                  float *out, uint64_t n, int block_size, gwnb_stream_t stream) try {
+    GWNB_NVTX("gwnb::query_exact");
     if (!bvh_valid(b))
         return set_error(GWNB_INVALID_ARGUMENT, "BVH object contains no queryable data.");
     if (block_size < 0 || block_size > 1024)
@@ -902,6 +921,7 @@ static int taylor_common(const gwnb_bvh4_f32 *b_in, const gwnb_moment4_f32 *m, c
 int gwnb_winding_taylor_batch_f32(const gwnb_bvh4_f32 *b, const gwnb_moment4_f32 *m, const float *qx,
                                   const float *qy, const float *qz, float *out, uint64_t n, float beta,
                                   const gwnb_taylor_options *opt, gwnb_stream_t stream) try {
+    GWNB_NVTX("gwnb::query_taylor");
     return taylor_common(b, m, qx, qy, qz, out, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, n, beta, opt,
                          stream);
 } catch (...) {
@@ -912,6 +932,7 @@ int gwnb_winding_gradient_taylor_batch_f32(const gwnb_bvh4_f32 *b, const gwnb_mo
                                            const float *qy, const float *qz, float *gx, float *gy, float *gz,
                                            uint64_t n, float beta, const gwnb_taylor_options *opt,
                                            gwnb_stream_t stream) try {
+    GWNB_NVTX("gwnb::query_taylor_gradient");
     if (n > 0 && (gx == nullptr || gy == nullptr || gz == nullptr))
         return set_error(GWNB_INVALID_ARGUMENT, "Query/output spans must use non-null storage when non-empty.");
     return taylor_common(b, m, qx, qy, qz, nullptr, gx, gy, gz, nullptr, nullptr, nullptr, n, beta, opt, stream);
@@ -922,6 +943,7 @@ int gwnb_winding_gradient_taylor_batch_f32(const gwnb_bvh4_f32 *b, const gwnb_mo
 int gwnb_winding_taylor_stats_f32(const gwnb_bvh4_f32 *b, const gwnb_moment4_f32 *m, const float *qx,
                                   const float *qy, const float *qz, uint64_t n, float beta, uint32_t *nodes,
                                   uint32_t *far_evals, uint32_t *near_tris, gwnb_stream_t stream) try {
+    GWNB_NVTX("gwnb::query_taylor_stats");
     if (n > 0 && (nodes == nullptr || far_evals == nullptr || near_tris == nullptr))
         return set_error(GWNB_INVALID_ARGUMENT, "Statistics outputs must be non-null.");
     gwnb_taylor_options o{256, 0, 1, GWNB_NEAR_PLAIN, 1.0f / 16.0f};
@@ -933,6 +955,7 @@ int gwnb_winding_taylor_stats_f32(const gwnb_bvh4_f32 *b, const gwnb_moment4_f32
 
 int gwnb_winding_exact_geometry_fp64(const gwnb_geometry_f32 *g, const float *qx, const float *qy, const float *qz,
                                      double *out, uint64_t n, gwnb_stream_t stream) try {
+    GWNB_NVTX("gwnb::query_exact_fp64");
     if (!geometry_valid(g))
         return set_error(GWNB_INVALID_ARGUMENT, "Geometry accessor is invalid.");
     if (!has_storage(qx, n) || !has_storage(qy, n) || !has_storage(qz, n) || !has_storage(out, n))
@@ -944,6 +967,7 @@ int gwnb_winding_exact_geometry_fp64(const gwnb_geometry_f32 *g, const float *qx
 
 int gwnb_query_order_f32(const gwnb_bvh4_f32 *b_in, const float *qx, const float *qy, const float *qz, uint64_t n,
                          uint32_t *order, gwnb_stream_t stream) try {
+    GWNB_NVTX("gwnb::query_order");
     if (!bvh_valid(b_in))
         return set_error(GWNB_INVALID_ARGUMENT, "BVH object contains no queryable data.");
     if (!has_storage(qx, n) || !has_storage(qy, n) || !has_storage(qz, n) || !has_storage(order, n))
@@ -975,6 +999,7 @@ int gwnb_winding_taylor_forward_f32(const gwnb_bvh4_f32 *b, const gwnb_moment4_f
                                     const float *qy, const float *qz, float *out, uint64_t n, float beta,
                                     const gwnb_taylor_options *opt, gwnb_taylor_saved_f32 *saved,
                                     gwnb_stream_t stream) try {
+    GWNB_NVTX("gwnb::taylor_forward");
     if (saved == nullptr)
         return set_error(GWNB_INVALID_ARGUMENT, "Taylor forward: saved state must be non-null.");
     if (m == nullptr || (m->order != 0 && m->order != 1))
@@ -1005,6 +1030,7 @@ int gwnb_winding_taylor_backward_f32(const gwnb_taylor_saved_f32 *saved, const g
                                      const gwnb_bvh4_f32 *b_in, const gwnb_moment4_f32 *m, const float *gout,
                                      float *dvx, float *dvy, float *dvz, float *dqx, float *dqy, float *dqz,
                                      gwnb_stream_t stream) try {
+    GWNB_NVTX("gwnb::taylor_backward");
     if (saved == nullptr)
         return set_error(GWNB_INVALID_ARGUMENT, "Taylor backward: saved state must be non-null.");
     if (saved->order != 0 && saved->order != 1)

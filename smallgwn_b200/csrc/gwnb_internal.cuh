@@ -7,7 +7,12 @@
 // Library-private layouts (query sidecar, padded triangles) are defined here too.
 #pragma once
 
+#define GWNB_NVTX_CAT2(a, b) a##b
+#define GWNB_NVTX_CAT(a, b) GWNB_NVTX_CAT2(a, b)
+#define GWNB_NVTX(name) ::gwnb::nvtx_scope const GWNB_NVTX_CAT(gwnb_nvtx_, __LINE__)(name)
+
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <atomic>
 #include <cstddef>
@@ -212,6 +217,21 @@ int device_sm_count();
 // Keys per tile of the 32-bit radix sort (256 threads x 12 keys): callers that size the sort's
 // scratch themselves (the allocation-free Taylor batch) use it.
 constexpr std::uint64_t k_sort_tile_u32 = 3072;
+
+// A named range on the host timeline (NVTX, header-only): with a profiler attached every library
+// call and build or query stage shows as a range around the work it enqueues; without one a
+// push / pop is a call through an empty hook.
+struct nvtx_scope {
+    explicit nvtx_scope(char const *name) { nvtxRangePushA(name); }
+    ~nvtx_scope() { nvtxRangePop(); }
+    nvtx_scope(nvtx_scope const &) = delete;
+    nvtx_scope &operator=(nvtx_scope const &) = delete;
+};
+
+template <class F> int nvtx_call(char const *name, F &&f) {
+    nvtx_scope const scope(name);
+    return f();
+}
 
 // Polls after which a device-side wait (the look-back of the radix sort and of the BVH4 collapse)
 // gives up, sets k_err_wait_timeout and lets its launch complete. Read by the host when a kernel is

@@ -499,6 +499,7 @@ int gwnb_mesh_write_ply(const char *path, const gwnb_host_mesh_f32 *m, int binar
 
 int gwnb_scene_save_f32(const char *path, const gwnb_geometry_f32 *g, const gwnb_bvh4_f32 *b,
                         const gwnb_moment4_f32 *const *moments, int moment_count, gwnb_stream_t stream) try {
+    GWNB_NVTX("gwnb::scene_save");
     if (path == nullptr)
         return set_error(GWNB_INVALID_ARGUMENT, "scene: null path.");
     if (!geometry_valid(g) || g->triangle_count == 0)
@@ -571,6 +572,7 @@ int gwnb_scene_save_f32(const char *path, const gwnb_geometry_f32 *g, const gwnb
 
 int gwnb_scene_load_f32(const char *path, gwnb_geometry_f32 *g_out, gwnb_bvh4_f32 *b_out, gwnb_moment4_f32 *m_out,
                         int *moment_mask, gwnb_stream_t stream) try {
+    GWNB_NVTX("gwnb::scene_load");
     if (path == nullptr || g_out == nullptr || b_out == nullptr || m_out == nullptr)
         return set_error(GWNB_INVALID_ARGUMENT, "scene: null path or output.");
     std::ifstream in(path, std::ios::binary);

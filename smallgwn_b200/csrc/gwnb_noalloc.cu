@@ -69,6 +69,7 @@ extern "C" int gwnb_winding_taylor_batch_noalloc_f32(const gwnb_bvh4_f32 *b, con
                                                      const float *qx, const float *qy, const float *qz,
                                                      float *out, uint64_t n, float beta,
                                                      const gwnb_taylor_options *opt, gwnb_stream_t stream) try {
+    GWNB_NVTX("gwnb::query_taylor_noalloc");
     if (radix_sort_u32_scratch_words(k_capacity, 30) > k_sort_words)
         return set_error(GWNB_INTERNAL_ERROR, "no-allocation Taylor batch: scratch layout mismatch.");
     if (n > k_capacity)

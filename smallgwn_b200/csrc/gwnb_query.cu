@@ -769,6 +769,7 @@ int taylor_batch(taylor_request const &r, cudaStream_t s) {
     float *gathered = nullptr;
     bool const sorted = r.sort_queries != 0 && r.n > 1 && r.root_bounds != nullptr;
     if (sorted) {
+        GWNB_NVTX("gwnb::taylor.order");
         GWNB_TRY(alloc(&codes, r.n, s));
         GWNB_TRY(alloc(&sorted_codes, r.n, s));
         GWNB_TRY(alloc(&order, r.n, s));
@@ -790,6 +791,7 @@ int taylor_batch(taylor_request const &r, cudaStream_t s) {
     bool const grad = r.gx != nullptr;
     bool const stats = r.stat_nodes != nullptr;
     int rc = GWNB_OK;
+    GWNB_NVTX("gwnb::taylor.traverse");
     int const block = query_launch_block(r.block);
     int const cap = r.stack_capacity;
     bool const per_thread = r.per_thread != 0;

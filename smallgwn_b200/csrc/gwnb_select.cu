@@ -50,6 +50,7 @@ int gwnb_taylor_select_f32(const gwnb_geometry_f32 *geometry, const gwnb_bvh4_f3
                            const gwnb_moment4_f32 *const *moments, const float *qx, const float *qy, const float *qz,
                            uint64_t n, float max_error, const float *betas, int beta_count, int near_precision,
                            gwnb_taylor_choice *out, gwnb_stream_t stream) try {
+    GWNB_NVTX("gwnb::taylor_select");
     if (out == nullptr || moments == nullptr || betas == nullptr || beta_count <= 0)
         return set_error(GWNB_INVALID_ARGUMENT, "taylor select: null argument or no candidate accuracy scale.");
     if (!geometry_valid(geometry) || !bvh_valid(bvh_in) || geometry->triangle_count != bvh_in->primitive_count)

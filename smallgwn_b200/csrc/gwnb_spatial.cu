@@ -923,6 +923,7 @@ extern "C" {
 int gwnb_unsigned_distance_batch_f32(const gwnb_bvh4_f32 *b, const float *qx, const float *qy, const float *qz,
                                      float *out, uint64_t n, float culling_band, const gwnb_spatial_options *opt,
                                      gwnb_stream_t stream) try {
+    GWNB_NVTX("gwnb::query_unsigned_distance");
     if (!bvh_valid(b))
         return set_error(GWNB_INVALID_ARGUMENT, "BVH object contains no queryable data.");
     gwnb_spatial_options o;
@@ -950,6 +951,7 @@ int gwnb_unsigned_distance_batch_f32(const gwnb_bvh4_f32 *b, const float *qx, co
 int gwnb_ray_first_hit_batch_f32(const gwnb_bvh4_f32 *b, const float *ox, const float *oy, const float *oz,
                                  const float *dx, const float *dy, const float *dz, gwnb_ray_hit_f32 *out, uint64_t n,
                                  float t_min, float t_max, const gwnb_spatial_options *opt, gwnb_stream_t stream) try {
+    GWNB_NVTX("gwnb::query_ray_first_hit");
     if (!bvh_valid(b))
         return set_error(GWNB_INVALID_ARGUMENT, "BVH object contains no queryable data.");
     gwnb_spatial_options o;

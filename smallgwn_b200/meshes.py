@@ -211,3 +211,67 @@ def reference_mixed_queries(mesh: dict, n: int, seed: int = 0xB3A9E5D4) -> tuple
     sign = np.where(rng.integers(0, 2, size=(nf, 3)) == 0, -1.0, 1.0)
     out[1:][~near] = ctr + (sign * rng.uniform(1.5, 3.0, size=(nf, 3)) + rng.uniform(-0.25, 0.25, size=(nf, 3))) * ext
     return tuple(np.ascontiguousarray(out[:, k]) for k in range(3))
+
+
+def _normalize_or(v: np.ndarray, fallback: np.ndarray) -> np.ndarray:
+    """Rows of v scaled to unit length; rows of zero (or non-finite) length take `fallback`'s row."""
+    n2 = np.einsum("ij,ij->i", v, v)
+    good = n2 > 0
+    out = np.array(fallback, dtype=v.dtype, copy=True)
+    out[good] = v[good] / np.sqrt(n2[good])[:, None]
+    return out
+
+
+def reference_mixed_rays(mesh: dict, n: int, seed: int = 0xB3A9E5D4) -> tuple[np.ndarray, ...]:
+    """The ray mix of smallgwn's benchmark harness (tests/benchmark_utils.cuh:210-370) as
+    (ox, oy, oz, dx, dy, dz), drawn here from numpy's PCG64: rays 4k and 4k + 1 start at the centroid
+    of triangle (ray id mod T) offset by U(0.2, 0.45) x the largest extent along its unit normal (to
+    the front for even ids, the back for odd ones) and point at the centroid (4k) or away from it
+    (4k + 1), jittered by U(-0.08, 0.08) times a random unit vector; rays 4k + 2 and 4k + 3 start on a
+    shell at U(1.6, 3.2) extents from the box centre, 4k + 2 aimed inward with jitter (hit-biased),
+    4k + 3 grazing: 0.2 inward + 0.8 of a unit tangent."""
+    P = np.stack([mesh["x"], mesh["y"], mesh["z"]], axis=-1).astype(np.float32)
+    lo, hi = P.min(axis=0), P.max(axis=0)
+    ctr = (lo + hi) * np.float32(0.5)
+    ext = np.maximum(hi - lo, np.float32(1e-3))
+    ext_max = np.float32(ext.max())
+    rng = np.random.default_rng((seed ^ 0x9E3779B97F4A7C15) & 0xFFFFFFFFFFFFFFFF)
+    ids = np.arange(n, dtype=np.int64)
+    o = np.empty((n, 3), np.float32)
+    d = np.empty((n, 3), np.float32)
+
+    def unit(k):
+        return _normalize_or(rng.uniform(-1, 1, size=(k, 3)).astype(np.float32),
+                             np.tile(np.float32([1, 0, 0]), (k, 1)))
+
+    T = int(mesh["i0"].size)
+    tri_rays = ((ids % 4) < 2) & (T > 0)
+    k = int(tri_rays.sum())
+    if k:
+        sel = ids[tri_rays]
+        t = sel % T
+        a, b, c = (P[np.asarray(mesh[f"i{j}"])[t].astype(np.int64)] for j in range(3))
+        cen = (a + b + c) / np.float32(3)
+        nrm = np.cross(b - a, c - a).astype(np.float32)
+        ru = unit(k)
+        nrm = _normalize_or(nrm, ru)
+        side = np.where((sel & 1) == 0, np.float32(1), np.float32(-1))[:, None]
+        off = rng.uniform(0.2, 0.45, size=(k, 1)).astype(np.float32) * ext_max
+        org = cen + side * off * nrm
+        dr = cen - org
+        dr[(sel % 4) == 1] *= -1
+        dr = dr + rng.uniform(-0.08, 0.08, size=(k, 3)).astype(np.float32) * ru
+        o[tri_rays], d[tri_rays] = org, _normalize_or(dr, -side * nrm)
+    m = n - k
+    if m:
+        sel = ids[~tri_rays]
+        outward = unit(m)
+        shell = rng.uniform(1.6, 3.2, size=(m, 1)).astype(np.float32)
+        org = ctr + outward * shell * ext
+        inward = _normalize_or(ctr - org, np.tile(np.float32([0, 0, 1]), (m, 1)))
+        j = unit(m)
+        jit = rng.uniform(-0.08, 0.08, size=(m, 3)).astype(np.float32)
+        tang = _normalize_or(np.cross(inward, j).astype(np.float32), np.tile(np.float32([1, 0, 0]), (m, 1)))
+        dr = np.where(((sel % 4) == 2)[:, None], inward + jit * j, np.float32(0.2) * inward + np.float32(0.8) * tang)
+        o[~tri_rays], d[~tri_rays] = org, _normalize_or(dr.astype(np.float32), inward)
+    return tuple(np.ascontiguousarray(a[:, i]) for a in (o, d) for i in range(3))

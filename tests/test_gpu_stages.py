@@ -1,0 +1,63 @@
+"""The benchmark-stage harness on the GPU: every stage of smallgwn's harness runs through this
+library's public API on a small mesh and writes its row (the two antipodal halves that this library
+evaluates in one kernel are written as unavailable with the reason), and the stage outputs are the
+library's own results (the Taylor stage's output equals a direct call)."""
+from __future__ import annotations
+
+import csv
+import io
+
+import numpy as np
+import pytest
+
+import smallgwn_b200 as g
+from smallgwn_b200 import api, meshes, stages
+
+pytestmark = pytest.mark.gpu
+
+
+def test_all_stages_run_and_write_rows(cuda, tmp_path):
+    mesh = meshes.to_soa(*meshes.uv_sphere(48, 25, seed=4))
+    opts = stages.options(query_count=3000, warmup_iters=1, measure_iters=3)
+    results, context = stages.run_model(mesh, opts)
+    names = [r.stage for r in results]
+    assert names == [s.format(builder="hploc") for s in stages.STAGES]
+    for r in results:
+        if r.stage in ("query_antipodal_crossings", "query_antipodal_boundary"):
+            assert not r.success and r.error_message == stages.FUSED_ANTIPODAL
+        else:
+            assert r.success, (r.stage, r.error_message)
+            assert len(r.samples_ms) == 3 and r.latency_p50_ms <= r.latency_p95_ms and r.throughput_per_s > 0
+    assert 0.05 < context["ray_mix_hit_ratio"] < 0.95
+    assert context["boundary_edge_count"] == 0  # a closed sphere
+    text = stages.csv_rows(results, context, "uv_sphere_48x25", opts, cuda.cuda.get_device_name(), 0, "t")
+    rows = list(csv.DictReader(io.StringIO(text)))
+    assert len(rows) == len(stages.STAGES) and rows[0]["stage"] == "bvh_build_hploc"
+
+
+def test_winding_query_only_and_lbvh(cuda):
+    mesh = meshes.to_soa(*meshes.uv_sphere(32, 17, seed=2))
+    opts = stages.options(query_count=2000, warmup_iters=0, measure_iters=2, builder="lbvh", winding_query_only=True)
+    results, _ = stages.run_model(mesh, opts)
+    assert [r.stage for r in results] == ["query_taylor_o1", "query_antipodal"] and all(r.success for r in results)
+
+
+def test_reference_query_mix_on_a_closed_sphere(cuda):
+    mesh = meshes.to_soa(*meshes.uv_sphere(40, 21, seed=3))
+    n = 2500
+    q = [cuda.from_numpy(v).cuda() for v in meshes.reference_mixed_queries(mesh, n, seed=9)]
+    geo = g.gwn_geometry_object()
+    assert g.gwn_upload_geometry(geo, mesh["x"], mesh["y"], mesh["z"], mesh["i0"], mesh["i1"], mesh["i2"]).is_ok()
+    bvh = g.gwn_bvh4_object()
+    assert g.gwn_build_bvh(geo, bvh).is_ok()
+    mom = g.gwn_bvh4_moment_object(2)
+    assert g.gwn_refit_bvh_moment(2, bvh, mom).is_ok()
+    out = cuda.empty(n, device="cuda")
+    cfg = api.gwn_query_batch_config(stack_capacity=96)
+    assert g.gwn_compute_winding_number_taylor_batch(2, bvh, mom, *q, out, 2.0, config=cfg).is_ok()
+    cuda.cuda.synchronize()
+    w = out.cpu().numpy()
+    # the box centre of a closed sphere is inside, far-field points outside
+    assert abs(w[0] - 1.0) < 1e-3
+    far = (np.arange(1, n) % 10) >= 7
+    assert np.all(np.abs(w[1:][far]) < 1e-2)
