@@ -1193,6 +1193,12 @@ def run_stages_workload(args) -> None:
         Path(args.csv).write_text(stages.csv_rows(
             results, context, "synthetic:displaced_uv_sphere_1024x512_seed2", opts, torch.cuda.get_device_name(),
             0, time.strftime("%Y-%m-%dT%H:%M:%SZ", time.gmtime())))
+    # the same Taylor stages with the library's per-thread traversal (identical results): the form
+    # that wins on this far-field-heavy mix at 1M queries
+    thr, _ = stages.run_model(mesh, stages.options(skip_exact=True, traversal="thread", only=(
+        "query_taylor_o0", "query_taylor_o1", "query_taylor_o2", "dynamic_refit_query_o2")))
+    per_thread = {r.stage: {"mean_ms": r.latency_mean_ms, "p50_ms": r.latency_p50_ms, "p95_ms": r.latency_p95_ms,
+                            "throughput_per_s": r.throughput_per_s} for r in thr if r.success}
     sg = smallgwn_stage_times(mesh, opts)
     head = rows["query_taylor_o2"]
     line = {
@@ -1207,9 +1213,12 @@ def run_stages_workload(args) -> None:
                    "skip_exact": opts.skip_exact,
                    "boundary_edge_count": context.get("boundary_edge_count"),
                    "ray_mix_hit_ratio": context.get("ray_mix_hit_ratio"), "stages": rows,
+                   "per_thread_traversal_stages": per_thread,
                    "smallgwn_kernels_mean_ms": sg,
                    "over_smallgwn": {k: sg[k] / rows[k]["mean_ms"] for k in (sg or {})
-                                     if rows.get(k, {}).get("mean_ms")}},
+                                     if rows.get(k, {}).get("mean_ms")},
+                   "per_thread_over_smallgwn": {k: sg[k] / per_thread[k]["mean_ms"] for k in (sg or {})
+                                                if per_thread.get(k, {}).get("mean_ms")}},
         "clocks": clocks.summary(),
     }
     print(json.dumps(line), flush=True)
@@ -1234,6 +1243,7 @@ def smallgwn_stage_times(mesh, opts) -> dict | None:
             out[f"refit_moment_o{o}"] = R.time_refit(o, it)
             R.refit_moments(o)
             out[f"query_taylor_o{o}"] = R.time_taylor(o, *q, opts.accuracy_scale, opts.warmup_iters, it)
+        R.boundary()  # the antipodal query reads the boundary chain
         out["query_antipodal"] = R.time_antipodal(*q, 2, 5)
         rays = meshes.reference_mixed_rays(mesh, opts.query_count, opts.seed)
         out["query_ray_first_hit"] = R.time_spatial(*rays[:3], dirs=rays[3:], warmup=2, iters=5)

@@ -233,6 +233,9 @@ SIGNATURES: dict[str, tuple] = {
         I, [C.POINTER(bvh4_f32), C.POINTER(moment4_f32), P, P, P, P, P, P, U64, F, C.POINTER(taylor_options), P]),
     "gwnb_winding_taylor_stats_f32": (
         I, [C.POINTER(bvh4_f32), C.POINTER(moment4_f32), P, P, P, U64, F, P, P, P, P]),
+    "gwnb_taylor_form_probe_f32": (
+        I, [C.POINTER(bvh4_f32), C.POINTER(moment4_f32), P, P, P, U64, F, C.POINTER(taylor_options),
+            C.POINTER(C.c_double), P]),
     "gwnb_bvh4_fp64_fallback_count": (I, [C.POINTER(bvh4_f32), C.POINTER(U64), P]),
     "gwnb_winding_exact_geometry_fp64": (I, [C.POINTER(geometry_f32), P, P, P, P, U64, P]),
     "gwnb_query_order_f32": (I, [C.POINTER(bvh4_f32), P, P, P, U64, P, P]),

@@ -425,6 +425,22 @@ def taylor_traversal_stats(bvh: gwn_bvh4_object, moment: gwn_bvh4_moment_object,
     return _status(rc)
 
 
+def taylor_form_probe(bvh: gwn_bvh4_object, moment: gwn_bvh4_moment_object, qx, qy, qz, accuracy_scale: float = 2.0,
+                      precision: int = near_precision.plain, sort_queries: bool = True,
+                      stream=None) -> tuple[gwn_status, dict]:
+    """Sampled-warp probe of a Taylor batch (gwnb_taylor_form_probe_f32): per sampled warp, the nodes
+    and leaf triangles the warp-cooperative form walks and the largest per-query node and triangle
+    counts (the per-thread form's lockstep work), and the number of sampled warps."""
+    out = (C.c_double * 5)()
+    opt = _options(gwn_query_batch_config(stack_capacity=max(64, bvh.accessor().internal_stack_bound)), sort_queries,
+                   precision, FP64_THRESHOLD)
+    rc = _lib.load().gwnb_taylor_form_probe_f32(C.byref(bvh._view), C.byref(moment._view), _ptr(qx), _ptr(qy),
+                                                _ptr(qz), _numel(qx), float(accuracy_scale), C.byref(opt), out,
+                                                _stream(stream))
+    keys = ("warp_nodes", "warp_tris", "lane_max_nodes", "lane_max_tris", "sampled_warps")
+    return _status(rc), dict(zip(keys, list(out)))
+
+
 def select_taylor_form(geometry: gwn_geometry_object, bvh: gwn_bvh4_object, moments: dict, qx, qy, qz,
                        max_error: float, accuracy_scales=(1.0, 1.5, 2.0, 2.5, 3.0, 3.25, 3.5, 4.0, 5.0, 6.0, 8.0),
                        precision: int = near_precision.compensated, stream=None) -> tuple[gwn_status, dict]:

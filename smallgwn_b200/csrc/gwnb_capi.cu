@@ -846,7 +846,7 @@ int gwnb_winding_exact_batch_f32(const gwnb_bvh4_f32 *b, const float *qx, const 
 static int taylor_common(const gwnb_bvh4_f32 *b_in, const gwnb_moment4_f32 *m, const float *qx, const float *qy,
                          const float *qz, float *out, float *gx, float *gy, float *gz, uint32_t *sn, uint32_t *sf,
                          uint32_t *snear, uint64_t n, float beta, const gwnb_taylor_options *opt,
-                         gwnb_stream_t stream) {
+                         gwnb_stream_t stream, double *probe = nullptr) {
     if (!bvh_valid(b_in))
         return set_error(GWNB_INVALID_ARGUMENT, "BVH object contains no queryable data.");
     gwnb_taylor_options o{256, 64, 1, GWNB_NEAR_PLAIN, 1.0f / 16.0f};
@@ -873,7 +873,7 @@ static int taylor_common(const gwnb_bvh4_f32 *b_in, const gwnb_moment4_f32 *m, c
         return set_error(GWNB_INVALID_ARGUMENT, "Unknown near-field precision mode.");
     if (!has_storage(qx, n) || !has_storage(qy, n) || !has_storage(qz, n))
         return set_error(GWNB_INVALID_ARGUMENT, "Query/output spans must use non-null storage when non-empty.");
-    if (out != nullptr || (gx == nullptr && sn == nullptr))
+    if (probe == nullptr && (out != nullptr || (gx == nullptr && sn == nullptr)))
         GWNB_TRY(check_query_spans(qx, qy, qz, out, n));
     if (n == 0)
         return GWNB_OK;
@@ -913,7 +913,8 @@ static int taylor_common(const gwnb_bvh4_f32 *b_in, const gwnb_moment4_f32 *m, c
     r.fp64_threshold = o.fp64_threshold;
     r.fp64_count = a->fp64_count;
     r.status = a->status;
-    if (o.near_precision == GWNB_NEAR_COMPENSATED)
+    r.probe = probe;
+    if (o.near_precision == GWNB_NEAR_COMPENSATED && probe == nullptr)
         GWNB_CUDA_TRY(cudaMemsetAsync(a->fp64_count, 0, sizeof(unsigned long long), s));
     return taylor_batch(r, s);
 }
@@ -949,6 +950,20 @@ int gwnb_winding_taylor_stats_f32(const gwnb_bvh4_f32 *b, const gwnb_moment4_f32
     gwnb_taylor_options o{256, 0, 1, GWNB_NEAR_PLAIN, 1.0f / 16.0f};
     return taylor_common(b, m, qx, qy, qz, nullptr, nullptr, nullptr, nullptr, nodes, far_evals, near_tris, n, beta,
                          &o, stream);
+} catch (...) {
+    return host_exception();
+}
+
+int gwnb_taylor_form_probe_f32(const gwnb_bvh4_f32 *b, const gwnb_moment4_f32 *m, const float *qx, const float *qy,
+                               const float *qz, uint64_t n, float beta, const gwnb_taylor_options *opt, double *out,
+                               gwnb_stream_t stream) try {
+    GWNB_NVTX("gwnb::taylor_form_probe");
+    if (out == nullptr)
+        return set_error(GWNB_INVALID_ARGUMENT, "taylor probe: output must be non-null.");
+    for (int k = 0; k < 5; ++k)
+        out[k] = 0.0;
+    return taylor_common(b, m, qx, qy, qz, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, n, beta, opt,
+                         stream, out);
 } catch (...) {
     return host_exception();
 }

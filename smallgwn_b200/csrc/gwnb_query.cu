@@ -223,6 +223,8 @@ struct taylor_params {
     std::uint32_t *stat_nodes;
     std::uint32_t *stat_far;
     std::uint32_t *stat_near;
+    std::uint32_t *stat_union;      // warp form: nodes the query's warp walked (nullptr: not recorded)
+    std::uint32_t *stat_union_near; // warp form: leaf triangles the query's warp evaluated
     std::uint64_t n;
     float beta2;
     float fp64_threshold;
@@ -417,6 +419,7 @@ __device__ __forceinline__ void taylor_warp_item(taylor_params const &p, std::ui
     accum<Mode == GWNB_NEAR_COMPENSATED> omega;
     float gx = 0.0f, gy = 0.0f, gz = 0.0f;
     std::uint32_t st_nodes = 0, st_far = 0, st_near = 0;
+    std::uint32_t st_union = 0, st_union_near = 0; // the warp's own work (the same in every lane)
 
     auto leaf = [&](std::uint32_t first, std::uint32_t cnt) {
         for (std::uint32_t k = 0; k < cnt; ++k) {
@@ -458,8 +461,10 @@ __device__ __forceinline__ void taylor_warp_item(taylor_params const &p, std::ui
             if (node >= p.node_count)
                 break;
             bool const active = ((mask >> lane) & 1u) != 0u;
-            if constexpr (Stats)
+            if constexpr (Stats) {
                 st_nodes += active ? 1u : 0u;
+                ++st_union;
+            }
             float4 const *nd = p.qnodes + static_cast<std::uint64_t>(node) * (4 * Q);
             std::uint32_t next = k_invalid_u32;
             unsigned next_mask = 0u;
@@ -514,10 +519,15 @@ __device__ __forceinline__ void taylor_warp_item(taylor_params const &p, std::ui
                     }
                     next = ref;
                     next_mask = dmask;
-                } else if (desc) {
-                    std::uint32_t const cnt =
-                        (ref & k_qref_multi) ? p.qcounts[static_cast<std::uint64_t>(node) * 4 + s] : 1u;
-                    leaf(ref & k_qref_index_mask, cnt);
+                } else {
+                    if constexpr (Stats) // the warp runs the leaf loop for its descending lanes
+                        st_union_near +=
+                            (ref & k_qref_multi) ? p.qcounts[static_cast<std::uint64_t>(node) * 4 + s] : 1u;
+                    if (desc) {
+                        std::uint32_t const cnt =
+                            (ref & k_qref_multi) ? p.qcounts[static_cast<std::uint64_t>(node) * 4 + s] : 1u;
+                        leaf(ref & k_qref_index_mask, cnt);
+                    }
                 }
             }
             if (overflow)
@@ -566,6 +576,10 @@ __device__ __forceinline__ void taylor_warp_item(taylor_params const &p, std::ui
         p.stat_nodes[qi] = st_nodes;
         p.stat_far[qi] = st_far;
         p.stat_near[qi] = st_near;
+        if (p.stat_union != nullptr) {
+            p.stat_union[qi] = st_union;
+            p.stat_union_near[qi] = st_union_near;
+        }
     }
 }
 
@@ -761,6 +775,122 @@ taylor_params make_taylor_params(taylor_request const &r) {
 }
 } // namespace
 
+namespace {
+
+// Whole warps of the traversal order, every `stride`-th one: sampled warp w takes ordered
+// positions [w * stride * 32, w * stride * 32 + 32), so its 32 queries are as close together as the
+// batch's own warps are.
+__global__ void __launch_bounds__(256)
+    k_probe_gather(std::uint32_t const *__restrict__ order, float const *__restrict__ qx,
+                   float const *__restrict__ qy, float const *__restrict__ qz, std::uint64_t stride,
+                   std::uint64_t sample_warps, float *__restrict__ sx, float *__restrict__ sy,
+                   float *__restrict__ sz) {
+    std::uint64_t const i = static_cast<std::uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= sample_warps * 32)
+        return;
+    std::uint64_t const src = (i >> 5) * stride * 32 + (i & 31u);
+    std::uint32_t const j = order != nullptr ? order[src] : static_cast<std::uint32_t>(src);
+    sx[i] = __ldg(qx + j);
+    sy[i] = __ldg(qy + j);
+    sz[i] = __ldg(qz + j);
+}
+
+// Per sampled warp: the nodes and leaf triangles the warp form walked (the same in every lane) and
+// the largest per-lane node and triangle counts; sums over the sample in sums[0..3].
+__global__ void __launch_bounds__(256)
+    k_probe_reduce(std::uint32_t const *__restrict__ nodes, std::uint32_t const *__restrict__ near,
+                   std::uint32_t const *__restrict__ union_nodes, std::uint32_t const *__restrict__ union_near,
+                   std::uint64_t sample_warps, unsigned long long *sums) {
+    std::uint64_t const i = static_cast<std::uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    bool const in = (i >> 5) < sample_warps;
+    std::uint32_t mn = in ? nodes[i] : 0u, mt = in ? near[i] : 0u;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        mn = max(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+        mt = max(mt, __shfl_xor_sync(0xffffffffu, mt, o));
+    }
+    if (in && (threadIdx.x & 31u) == 0u) {
+        atomicAdd(&sums[0], static_cast<unsigned long long>(union_nodes[i]));
+        atomicAdd(&sums[1], static_cast<unsigned long long>(union_near[i]));
+        atomicAdd(&sums[2], static_cast<unsigned long long>(mn));
+        atomicAdd(&sums[3], static_cast<unsigned long long>(mt));
+    }
+}
+
+} // namespace
+
+// Sampled-warp probe of a Taylor batch in traversal order `order` (nullptr: the queries are already
+// in that order): runs the warp form with statistics on about 1/128 of the warps (64 to 4,096) and
+// returns, per sampled warp, out[0] nodes walked by the warp, out[1] leaf triangles it evaluated,
+// out[2] the largest per-lane node count and out[3] the largest per-lane triangle count -- the
+// lockstep work of the per-thread form -- and out[4] the number of sampled warps (0: too few
+// queries to sample). Synchronizes the stream.
+int taylor_probe(taylor_request const &r, std::uint32_t const *order, cudaStream_t s, double out[5]) {
+    for (int k = 0; k < 5; ++k)
+        out[k] = 0.0;
+    std::uint64_t const warps = r.n / 32;
+    if (warps == 0)
+        return GWNB_OK;
+    std::uint64_t const target = std::min<std::uint64_t>(std::max<std::uint64_t>(warps / 128, 64), 4096);
+    std::uint64_t const stride = std::max<std::uint64_t>(warps / target, 1);
+    std::uint64_t const sample = std::min(warps / stride, target);
+    std::uint64_t const m = sample * 32;
+    float *sq = nullptr;
+    std::uint32_t *st = nullptr;
+    unsigned long long *sums = nullptr;
+    int rc = GWNB_OK;
+    auto cleanup = [&]() {
+        release(sq, s);
+        release(st, s);
+        release(sums, s);
+    };
+    if ((rc = alloc(&sq, 3 * m, s)) != GWNB_OK || (rc = alloc(&st, 5 * m, s)) != GWNB_OK ||
+        (rc = alloc(&sums, 4, s)) != GWNB_OK) {
+        cleanup();
+        return rc;
+    }
+    unsigned const grid = static_cast<unsigned>((m + 255) / 256);
+    note_launch(), k_probe_gather<<<grid, 256, 0, s>>>(order, r.qx, r.qy, r.qz, stride, sample, sq, sq + m, sq + 2 * m);
+    taylor_params p = make_taylor_params(r);
+    p.qx = sq;
+    p.qy = sq + m;
+    p.qz = sq + 2 * m;
+    p.order = nullptr;
+    p.gathered = 0;
+    p.out = nullptr;
+    p.n = m;
+    p.stat_nodes = st;
+    p.stat_far = st + m;
+    p.stat_near = st + 2 * m;
+    p.stat_union = st + 3 * m;
+    p.stat_union_near = st + 4 * m;
+    int const cap = r.stack_capacity;
+    if (r.order == 0)
+        rc = launch_taylor_order<0, false, true>(p, 256, cap, r.near_mode, false, s);
+    else if (r.order == 1)
+        rc = launch_taylor_order<1, false, true>(p, 256, cap, r.near_mode, false, s);
+    else
+        rc = launch_taylor_order<2, false, true>(p, 256, cap, r.near_mode, false, s);
+    unsigned long long h[4] = {0, 0, 0, 0};
+    if (rc == GWNB_OK) {
+        if (cudaMemsetAsync(sums, 0, 4 * sizeof(unsigned long long), s) != cudaSuccess) {
+            rc = set_cuda_error(cudaGetLastError(), "taylor probe");
+        } else {
+            note_launch(), k_probe_reduce<<<grid, 256, 0, s>>>(st, st + 2 * m, st + 3 * m, st + 4 * m, sample, sums);
+            if (cudaMemcpyAsync(h, sums, sizeof(h), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+                cudaStreamSynchronize(s) != cudaSuccess)
+                rc = set_cuda_error(cudaGetLastError(), "taylor probe read-back");
+        }
+    }
+    cleanup();
+    if (rc != GWNB_OK)
+        return rc;
+    for (int k = 0; k < 4; ++k)
+        out[k] = static_cast<double>(h[k]) / static_cast<double>(sample);
+    out[4] = static_cast<double>(sample);
+    return GWNB_OK;
+}
+
 int taylor_batch(taylor_request const &r, cudaStream_t s) {
     if (r.n == 0)
         return GWNB_OK;
@@ -787,6 +917,17 @@ int taylor_batch(taylor_request const &r, cudaStream_t s) {
         p.qy = gathered + r.n;
         p.qz = gathered + 2 * r.n;
         p.gathered = 1;
+    }
+    if (r.probe != nullptr) {
+        taylor_request rq = r;
+        rq.qx = p.qx;
+        rq.qy = p.qy;
+        rq.qz = p.qz;
+        int const prc = taylor_probe(rq, sorted ? nullptr : p.order, s, r.probe);
+        release(codes, s);
+        release(order, s);
+        release(gathered, s);
+        return prc;
     }
     bool const grad = r.gx != nullptr;
     bool const stats = r.stat_nodes != nullptr;

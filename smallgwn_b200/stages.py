@@ -21,8 +21,10 @@ Restated from smallgwn's tests (none of that code is used):
 `query_antipodal_crossings` and `query_antipodal_boundary` time the two halves of smallgwn's
 antipodal query, which smallgwn's harness launches through its own detail functors; this library
 evaluates both halves in one kernel, so those rows are written with success = 0 and the reason,
-and `query_antipodal` times the whole query. Every stage runs inside an NVTX range of its name
-(the library's own calls add ranges of theirs inside it).
+and `query_antipodal` times the whole query. The Taylor stages use the library's default
+warp-cooperative traversal; `--traversal thread` times its per-thread traversal instead (the same
+results). Every stage runs inside an NVTX range of its name (the library's own calls add ranges of
+theirs inside it).
 
 Usage: python -m smallgwn_b200.stages [--model mesh.ply | --sphere] [--queries N] [--csv PATH] ...
 """
@@ -65,6 +67,8 @@ class options:
     builder: str = "hploc"
     skip_exact: bool = False
     winding_query_only: bool = False
+    traversal: str = "warp"  # Taylor stages: the library's default warp-cooperative walk, or "thread"
+    only: tuple = ()         # run just these stages (empty: all)
 
 
 @dataclass
@@ -210,7 +214,7 @@ def run_model(mesh: dict, opts: options, stream=None) -> tuple[list, dict]:
 
     def taylor(o):
         return lambda: api.gwn_compute_winding_number_taylor_batch(o, bvh, mom[o], *q, out, opts.accuracy_scale, s,
-                                                                   config=cfg)
+                                                                   config=cfg, per_thread=opts.traversal == "thread")
 
     def setup_boundary():
         return api.gwn_build_boundary_chain(geo, chain, s)
@@ -241,13 +245,17 @@ def run_model(mesh: dict, opts: options, stream=None) -> tuple[list, dict]:
             r = api.gwn_refit_bvh_moment(2, bvh, mom[2], s)
         return r if not r.is_ok() else taylor(2)()
 
-    stage = lambda name, unit, denom, setup, fn: run_stage(name, unit, denom, opts, nv, nt, stream, setup, fn)  # noqa
+    def stage(name, unit, denom, setup, fn):
+        if opts.only and name not in opts.only:
+            return None
+        return run_stage(name, unit, denom, opts, nv, nt, stream, setup, fn)
+
     query_o1 = lambda: stage("query_taylor_o1", "queries/s", nq, build_moment(1), taylor(1))  # noqa: E731
     query_antipodal = lambda: stage(  # noqa: E731
         "query_antipodal", "queries/s", nq, setup_bvh_and_boundary,
         lambda: api.gwn_compute_winding_number_antipodal_batch(geo, bvh, chain, *q, out, stream=s, config=cfg))
     if opts.winding_query_only:
-        return [query_o1(), query_antipodal()], context
+        return [r for r in (query_o1(), query_antipodal()) if r is not None], context
 
     res = [stage(f"bvh_build_{opts.builder}", "triangles/s", nt, lambda: ok, build),
            stage("refit_bvh", "triangles/s", nt, build, lambda: api.gwn_refit_bvh(geo, bvh, s))]
@@ -264,7 +272,8 @@ def run_model(mesh: dict, opts: options, stream=None) -> tuple[list, dict]:
         res.append(stage("query_exact", "queries/s", nq, build,
                          lambda: api.gwn_compute_winding_number_exact_batch(bvh, *q, out, s, config=cfg)))
     for name in ("query_antipodal_crossings", "query_antipodal_boundary"):
-        res.append(_unavailable(name, "queries/s", opts, nv, nt, FUSED_ANTIPODAL))
+        if not opts.only or name in opts.only:
+            res.append(_unavailable(name, "queries/s", opts, nv, nt, FUSED_ANTIPODAL))
     res.append(stage("query_antipodal_gradient", "queries/s", nq, setup_boundary,
                      lambda: api.gwn_compute_winding_gradient_antipodal_batch(geo, chain, *q, *grad, stream=s,
                                                                               config=cfg)))
@@ -272,7 +281,7 @@ def run_model(mesh: dict, opts: options, stream=None) -> tuple[list, dict]:
     res.append(stage("query_ray_first_hit", "rays/s", nq, setup_rays,
                      lambda: api.gwn_compute_ray_first_hit_batch(bvh, *rays, hits, stream=s, config=cfg)))
     res.append(stage("dynamic_refit_query_o2", "queries/s", nq, build, dynamic_frame))
-    return res, context
+    return [r for r in res if r is not None], context
 
 
 def csv_rows(results, context: dict, model_path: str, opts: options, gpu_name: str, cuda_runtime: int,
@@ -310,10 +319,12 @@ def main(argv=None) -> int:
     ap.add_argument("--builder", choices=["hploc", "lbvh"], default=d.builder)
     ap.add_argument("--skip-exact", action="store_true")
     ap.add_argument("--winding-query-only", action="store_true")
+    ap.add_argument("--traversal", choices=["warp", "thread"], default=d.traversal,
+                    help="Taylor stages: warp-cooperative walk (the library's default) or one walk per thread")
     ap.add_argument("--csv", type=Path, default=Path("smallgwn_bench.csv"))
     a = ap.parse_args(argv)
     opts = options(a.queries, a.warmup, a.iters, a.accuracy_scale, a.stack_capacity, not a.no_stream_sync, a.seed,
-                   a.builder, a.skip_exact, a.winding_query_only)
+                   a.builder, a.skip_exact, a.winding_query_only, a.traversal)
     if a.model is not None:
         mesh, model = api.read_ply(a.model), str(a.model)
     else:

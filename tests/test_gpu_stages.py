@@ -10,6 +10,7 @@ import io
 import numpy as np
 import pytest
 
+import oracle
 import smallgwn_b200 as g
 from smallgwn_b200 import api, meshes, stages
 
@@ -29,7 +30,7 @@ def test_all_stages_run_and_write_rows(cuda, tmp_path):
             assert r.success, (r.stage, r.error_message)
             assert len(r.samples_ms) == 3 and r.latency_p50_ms <= r.latency_p95_ms and r.throughput_per_s > 0
     assert 0.05 < context["ray_mix_hit_ratio"] < 0.95
-    assert context["boundary_edge_count"] == 0  # a closed sphere
+    assert context["boundary_edge_count"] == oracle.boundary_chain(mesh)[0].size
     text = stages.csv_rows(results, context, "uv_sphere_48x25", opts, cuda.cuda.get_device_name(), 0, "t")
     rows = list(csv.DictReader(io.StringIO(text)))
     assert len(rows) == len(stages.STAGES) and rows[0]["stage"] == "bvh_build_hploc"
@@ -61,3 +62,41 @@ def test_reference_query_mix_on_a_closed_sphere(cuda):
     assert abs(w[0] - 1.0) < 1e-3
     far = (np.arange(1, n) % 10) >= 7
     assert np.all(np.abs(w[1:][far]) < 1e-2)
+
+
+def test_per_thread_traversal_stage(cuda):
+    mesh = meshes.to_soa(*meshes.uv_sphere(32, 17, seed=2))
+    opts = stages.options(query_count=2000, warmup_iters=0, measure_iters=2, traversal="thread",
+                          only=("query_taylor_o1", "query_taylor_o2"))
+    results, _ = stages.run_model(mesh, opts)
+    assert [r.stage for r in results] == ["query_taylor_o1", "query_taylor_o2"] and all(r.success for r in results)
+
+
+def test_form_probe_matches_traversal_statistics(cuda):
+    """The sampled-warp probe reads, for every other warp of an ordered batch (128 warps: 64
+    sampled), the warp's walk and its largest per-query counts; the per-query counts agree with the
+    statistics entry point on the same queries."""
+    mesh = meshes.to_soa(*meshes.uv_sphere(40, 21, seed=3))
+    geo = g.gwn_geometry_object()
+    assert g.gwn_upload_geometry(geo, mesh["x"], mesh["y"], mesh["z"], mesh["i0"], mesh["i1"], mesh["i2"]).is_ok()
+    bvh = g.gwn_bvh4_object()
+    assert g.gwn_build_bvh(geo, bvh).is_ok()
+    mom = g.gwn_bvh4_moment_object(1)
+    assert g.gwn_refit_bvh_moment(1, bvh, mom).is_ok()
+    n = 128 * 32
+    q = [cuda.from_numpy(v).cuda() for v in meshes.mixed_queries(mesh, n, seed=6)]
+    order = cuda.empty(n, dtype=cuda.int32, device="cuda")
+    assert api.query_order(bvh, *q, order).is_ok()
+    sq = [d[order.long()].contiguous() for d in q]
+    st, pr = api.taylor_form_probe(bvh, mom, *sq, accuracy_scale=2.0, sort_queries=False)
+    assert st.is_ok(), st.message
+    assert pr["sampled_warps"] == 64
+    stats = [cuda.empty(n, dtype=cuda.int32, device="cuda") for _ in range(3)]
+    assert api.taylor_traversal_stats(bvh, mom, *sq, *stats, accuracy_scale=2.0).is_ok()
+    nodes = stats[0].cpu().numpy().reshape(-1, 32)[::2]
+    near = stats[2].cpu().numpy().reshape(-1, 32)[::2]
+    assert pr["lane_max_nodes"] == pytest.approx(nodes.max(axis=1).mean())
+    assert pr["lane_max_tris"] == pytest.approx(near.max(axis=1).mean())
+    assert pr["warp_nodes"] >= pr["lane_max_nodes"] > 0 and pr["warp_tris"] >= pr["lane_max_tris"]
+    st, none = api.taylor_form_probe(bvh, mom, *[v[:31] for v in sq], accuracy_scale=2.0, sort_queries=False)
+    assert st.is_ok() and none["sampled_warps"] == 0
