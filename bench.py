@@ -1247,6 +1247,21 @@ def smallgwn_stage_times(mesh, opts) -> dict | None:
         out["query_antipodal"] = R.time_antipodal(*q, 2, 5)
         rays = meshes.reference_mixed_rays(mesh, opts.query_count, opts.seed)
         out["query_ray_first_hit"] = R.time_spatial(*rays[:3], dirs=rays[3:], warmup=2, iters=5)
+        # the dynamic stage (host positions up, refit, moment refit, order-2 Taylor batch), wall clock
+        # per synchronized call as the harness times it
+        import torch
+
+        dyn = [mesh["x"].astype(np.float32), mesh["y"].astype(np.float32), mesh["z"].astype(np.float32).copy()]
+        dyn[2] += np.float32(0.001) * ((np.arange(dyn[2].size) % 17) - 8).astype(np.float32)
+        R.set_queries(*q)
+        for _ in range(opts.warmup_iters):
+            R.dynamic_frame(*dyn, 2, opts.accuracy_scale)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(it):
+            R.dynamic_frame(*dyn, 2, opts.accuracy_scale)
+            torch.cuda.synchronize()
+        out["dynamic_refit_query_o2"] = (time.perf_counter() - t0) * 1e3 / it
         return out
     finally:
         R.close()
