@@ -1193,8 +1193,8 @@ def run_stages_workload(args) -> None:
         Path(args.csv).write_text(stages.csv_rows(
             results, context, "synthetic:displaced_uv_sphere_1024x512_seed2", opts, torch.cuda.get_device_name(),
             0, time.strftime("%Y-%m-%dT%H:%M:%SZ", time.gmtime())))
-    # the same Taylor stages with the library's per-thread traversal (identical results): the form
-    # that wins on this far-field-heavy mix at 1M queries
+    # the same Taylor stages with the per-thread walk (identical results), the walk that suits this
+    # far-field-heavy mix at 1M queries
     thr, _ = stages.run_model(mesh, stages.options(skip_exact=True, traversal="thread", only=(
         "query_taylor_o0", "query_taylor_o1", "query_taylor_o2", "dynamic_refit_query_o2")))
     per_thread = {r.stage: {"mean_ms": r.latency_mean_ms, "p50_ms": r.latency_p50_ms, "p95_ms": r.latency_p95_ms,

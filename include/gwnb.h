@@ -317,13 +317,15 @@ GWNB_API int gwnb_winding_taylor_stats_f32(const gwnb_bvh4_f32 *bvh, const gwnb_
                                   uint32_t *far_evaluations, uint32_t *near_triangles,
                                   gwnb_stream_t stream);
 
-/* Sampled-warp probe of a Taylor batch (diagnostics; what the choice between the warp-cooperative
- * and the per-thread traversal reads): orders the batch as the Taylor batch would (options'
- * sort_queries), runs the warp-cooperative traversal with statistics on about 1/128 of its warps
- * (64 to 4,096 whole warps of consecutive queries) and writes, per sampled warp, out[0] nodes the
- * warp walked, out[1] leaf triangles it evaluated, out[2] the largest per-query node count and out[3]
- * the largest per-query triangle count in the warp, and out[4] the sampled warps (0 below 32
- * queries). Synchronizes `stream`. */
+/* Sampled walk statistics of a Taylor batch (diagnostics; which of the two traversals suits it):
+ * orders the batch as the Taylor batch would (options' sort_queries), walks a sample of it
+ * warp-cooperatively with statistics and no outputs (every k-th unit of 32 consecutive ordered
+ * warps: one resident wave or 1/64 of the batch, up to 64 units for small batches) and writes, per
+ * sampled warp, out[0] nodes the warp walked, out[1]
+ * leaf triangles it evaluated, out[2] the largest per-query node count and out[3] the largest
+ * per-query triangle count in the warp; out[4] the sampled warps (0 below 1,024 queries); out[5] 1
+ * when the per-thread traversal suits the batch (sampled warps walked at least 1.3 times their
+ * longest path's nodes, that path met at most 8 leaf triangles). Synchronizes `stream`. */
 GWNB_API int gwnb_taylor_form_probe_f32(const gwnb_bvh4_f32 *bvh, const gwnb_moment4_f32 *moment,
                                         const float *query_x, const float *query_y, const float *query_z,
                                         uint64_t count, float accuracy_scale, const gwnb_taylor_options *options,

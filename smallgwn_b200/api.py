@@ -373,25 +373,33 @@ def gwn_compute_winding_number_exact_batch(bvh: gwn_bvh4_object, qx, qy, qz, out
     return _status(rc)
 
 
+TRAVERSALS = {"warp": 0, "thread": 1}  # gwnb_taylor_options::per_thread
+
+
 def _options(config: gwn_query_batch_config, sort_queries: bool, precision: int, fp64_threshold: float,
-             per_thread: bool = False):
+             per_thread: bool = False, traversal: str = "warp"):
+    walk = 1 if per_thread else TRAVERSALS[traversal]
     return _lib.taylor_options(int(config.block_size), int(config.stack_capacity), 1 if sort_queries else 0,
-                               int(precision), float(fp64_threshold), 1 if per_thread else 0)
+                               int(precision), float(fp64_threshold), walk)
 
 
 def gwn_compute_winding_number_taylor_batch(order: int, bvh: gwn_bvh4_object, moment: gwn_bvh4_moment_object,
                                             qx, qy, qz, out, accuracy_scale: float = 2.0, stream=None,
                                             config: gwn_query_batch_config = gwn_query_batch_config(),
                                             sort_queries: bool = True, precision: int = near_precision.plain,
-                                            fp64_threshold: float = FP64_THRESHOLD, per_thread: bool = False) -> gwn_status:
-    """Taylor-approximated winding numbers of a device batch (asynchronous). ``per_thread``
-    selects one independent traversal per thread instead of the warp-cooperative traversal."""
+                                            fp64_threshold: float = FP64_THRESHOLD, per_thread: bool = False,
+                                            traversal: str = "warp") -> gwn_status:
+    """Taylor-approximated winding numbers of a device batch (asynchronous). ``traversal``: "warp"
+    (the default: 32 ordered queries per warp walk one traversal together) or "thread" (one
+    independent walk per query; also ``per_thread=True``); both give identical results."""
     if moment.order != order:
         return gwn_status(gwn_error.invalid_argument, "Moment object order does not match the requested order.")
+    if traversal not in TRAVERSALS:
+        return gwn_status(gwn_error.invalid_argument, f"Unknown traversal {traversal!r}.")
     bad = _check_spans(qx, qy, qz, out)
     if bad is not None:
         return bad
-    opt = _options(config, sort_queries, precision, fp64_threshold, per_thread)
+    opt = _options(config, sort_queries, precision, fp64_threshold, per_thread, traversal)
     rc = _lib.load().gwnb_winding_taylor_batch_f32(
         C.byref(bvh._view), C.byref(moment._view), _ptr(qx), _ptr(qy), _ptr(qz), _ptr(out), _numel(out),
         float(accuracy_scale), C.byref(opt), _stream(stream))
@@ -428,16 +436,17 @@ def taylor_traversal_stats(bvh: gwn_bvh4_object, moment: gwn_bvh4_moment_object,
 def taylor_form_probe(bvh: gwn_bvh4_object, moment: gwn_bvh4_moment_object, qx, qy, qz, accuracy_scale: float = 2.0,
                       precision: int = near_precision.plain, sort_queries: bool = True,
                       stream=None) -> tuple[gwn_status, dict]:
-    """Sampled-warp probe of a Taylor batch (gwnb_taylor_form_probe_f32): per sampled warp, the nodes
-    and leaf triangles the warp-cooperative form walks and the largest per-query node and triangle
-    counts (the per-thread form's lockstep work), and the number of sampled warps."""
-    out = (C.c_double * 5)()
+    """Sampled walk statistics (gwnb_taylor_form_probe_f32): per sampled warp, the nodes and leaf
+    triangles the warp-cooperative walk takes and the largest per-query node and triangle counts (the
+    per-thread walk's lockstep work), the number of sampled warps, and per_thread = 1 when the
+    per-thread traversal suits the batch."""
+    out = (C.c_double * 6)()
     opt = _options(gwn_query_batch_config(stack_capacity=max(64, bvh.accessor().internal_stack_bound)), sort_queries,
                    precision, FP64_THRESHOLD)
     rc = _lib.load().gwnb_taylor_form_probe_f32(C.byref(bvh._view), C.byref(moment._view), _ptr(qx), _ptr(qy),
                                                 _ptr(qz), _numel(qx), float(accuracy_scale), C.byref(opt), out,
                                                 _stream(stream))
-    keys = ("warp_nodes", "warp_tris", "lane_max_nodes", "lane_max_tris", "sampled_warps")
+    keys = ("warp_nodes", "warp_tris", "lane_max_nodes", "lane_max_tris", "sampled_warps", "per_thread")
     return _status(rc), dict(zip(keys, list(out)))
 
 

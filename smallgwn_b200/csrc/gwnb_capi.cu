@@ -871,6 +871,8 @@ static int taylor_common(const gwnb_bvh4_f32 *b_in, const gwnb_moment4_f32 *m, c
         return set_error(GWNB_INVALID_ARGUMENT, "Taylor accuracy scale must be nonnegative.");
     if (o.near_precision != GWNB_NEAR_PLAIN && o.near_precision != GWNB_NEAR_COMPENSATED)
         return set_error(GWNB_INVALID_ARGUMENT, "Unknown near-field precision mode.");
+    if (o.per_thread != 0 && o.per_thread != 1)
+        return set_error(GWNB_INVALID_ARGUMENT, "Unknown traversal (per_thread must be 0 or 1).");
     if (!has_storage(qx, n) || !has_storage(qy, n) || !has_storage(qz, n))
         return set_error(GWNB_INVALID_ARGUMENT, "Query/output spans must use non-null storage when non-empty.");
     if (probe == nullptr && (out != nullptr || (gx == nullptr && sn == nullptr)))
@@ -960,7 +962,7 @@ int gwnb_taylor_form_probe_f32(const gwnb_bvh4_f32 *b, const gwnb_moment4_f32 *m
     GWNB_NVTX("gwnb::taylor_form_probe");
     if (out == nullptr)
         return set_error(GWNB_INVALID_ARGUMENT, "taylor probe: output must be non-null.");
-    for (int k = 0; k < 5; ++k)
+    for (int k = 0; k < 6; ++k)
         out[k] = 0.0;
     return taylor_common(b, m, qx, qy, qz, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, n, beta, opt,
                          stream, out);

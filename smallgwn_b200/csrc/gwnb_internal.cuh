@@ -315,7 +315,7 @@ struct taylor_request {
     float fp64_threshold;
     unsigned long long *fp64_count;
     unsigned int *status;
-    double *probe; // non-null: order the batch and write the sampled-warp probe (5 doubles) instead
+    double *probe; // non-null: order the batch and write the sampled-warp probe (6 doubles) instead
 };
 int taylor_batch(taylor_request const &r, cudaStream_t s);
 

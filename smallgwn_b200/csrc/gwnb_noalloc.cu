@@ -106,6 +106,8 @@ extern "C" int gwnb_winding_taylor_batch_noalloc_f32(const gwnb_bvh4_f32 *b, con
         return set_error(GWNB_INVALID_ARGUMENT, "Taylor accuracy scale must be nonnegative.");
     if (o.near_precision != GWNB_NEAR_PLAIN && o.near_precision != GWNB_NEAR_COMPENSATED)
         return set_error(GWNB_INVALID_ARGUMENT, "Unknown near-field precision mode.");
+    if (o.per_thread != 0 && o.per_thread != 1)
+        return set_error(GWNB_INVALID_ARGUMENT, "Unknown traversal (per_thread must be 0 or 1).");
     if (!has(qx, n) || !has(qy, n) || !has(qz, n) || !has(out, n))
         return set_error(GWNB_INVALID_ARGUMENT, "Query/output spans must use non-null storage when non-empty.");
     // The BVH's derived state must already exist: creating it would allocate.

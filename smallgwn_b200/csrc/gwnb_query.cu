@@ -225,6 +225,12 @@ struct taylor_params {
     std::uint32_t *stat_near;
     std::uint32_t *stat_union;      // warp form: nodes the query's warp walked (nullptr: not recorded)
     std::uint32_t *stat_union_near; // warp form: leaf triangles the query's warp evaluated
+    // Sampled walk (0: every ordered position is walked by this launch), on units of 32 consecutive
+    // warps (1,024 ordered positions): local unit u walks the ordered positions of unit
+    // u * sample_stride, and local warp w writes {nodes walked, triangles walked, largest per-query
+    // nodes, largest per-query triangles} to warp_stats[4 w ...].
+    std::uint64_t sample_stride;
+    std::uint32_t *warp_stats;
     std::uint64_t n;
     float beta2;
     float fp64_threshold;
@@ -411,8 +417,11 @@ __device__ __forceinline__ void taylor_warp_item(taylor_params const &p, std::ui
     unsigned const full = __ballot_sync(0xffffffffu, valid);
     if (full == 0u)
         return;
-    std::uint32_t const qi = valid ? (p.order != nullptr ? p.order[idx] : static_cast<std::uint32_t>(idx)) : 0u;
-    std::uint64_t const li = p.gathered ? idx : qi;
+    // ordered position: idx itself, or the sampled unit's positions in a sampled launch (units of 32
+    // consecutive warps, so that a sampled unit's warps share node records in L1 as the batch's do)
+    std::uint64_t const pos = p.sample_stride != 0 ? (idx >> 10) * p.sample_stride * 1024 + (idx & 1023u) : idx;
+    std::uint32_t const qi = valid ? (p.order != nullptr ? p.order[pos] : static_cast<std::uint32_t>(pos)) : 0u;
+    std::uint64_t const li = p.gathered ? pos : qi;
     float const qx = valid ? p.qx[li] : 0.0f;
     float const qy = valid ? p.qy[li] : 0.0f;
     float const qz = valid ? p.qz[li] : 0.0f;
@@ -550,6 +559,19 @@ __device__ __forceinline__ void taylor_warp_item(taylor_params const &p, std::ui
             }
         }
     }
+    if constexpr (Stats) {
+        if (p.warp_stats != nullptr) {
+            std::uint32_t const mn = __reduce_max_sync(0xffffffffu, valid ? st_nodes : 0u);
+            std::uint32_t const mt = __reduce_max_sync(0xffffffffu, valid ? st_near : 0u);
+            if (lane == 0) {
+                std::uint32_t *const w = p.warp_stats + 4 * (idx >> 5);
+                w[0] = st_union;
+                w[1] = st_union_near;
+                w[2] = mn;
+                w[3] = mt;
+            }
+        }
+    }
     if (!valid)
         return;
     float const inv4pi = 1.0f / (4.0f * k_pi_f);
@@ -573,9 +595,11 @@ __device__ __forceinline__ void taylor_warp_item(taylor_params const &p, std::ui
         p.grad_z[qi] = gz * inv4pi;
     }
     if constexpr (Stats) {
-        p.stat_nodes[qi] = st_nodes;
-        p.stat_far[qi] = st_far;
-        p.stat_near[qi] = st_near;
+        if (p.stat_nodes != nullptr) {
+            p.stat_nodes[qi] = st_nodes;
+            p.stat_far[qi] = st_far;
+            p.stat_near[qi] = st_near;
+        }
         if (p.stat_union != nullptr) {
             p.stat_union[qi] = st_union;
             p.stat_union_near[qi] = st_union_near;
@@ -777,117 +801,85 @@ taylor_params make_taylor_params(taylor_request const &r) {
 
 namespace {
 
-// Whole warps of the traversal order, every `stride`-th one: sampled warp w takes ordered
-// positions [w * stride * 32, w * stride * 32 + 32), so its 32 queries are as close together as the
-// batch's own warps are.
-__global__ void __launch_bounds__(256)
-    k_probe_gather(std::uint32_t const *__restrict__ order, float const *__restrict__ qx,
-                   float const *__restrict__ qy, float const *__restrict__ qz, std::uint64_t stride,
-                   std::uint64_t sample_warps, float *__restrict__ sx, float *__restrict__ sy,
-                   float *__restrict__ sz) {
-    std::uint64_t const i = static_cast<std::uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (i >= sample_warps * 32)
-        return;
-    std::uint64_t const src = (i >> 5) * stride * 32 + (i & 31u);
-    std::uint32_t const j = order != nullptr ? order[src] : static_cast<std::uint32_t>(src);
-    sx[i] = __ldg(qx + j);
-    sy[i] = __ldg(qy + j);
-    sz[i] = __ldg(qz + j);
+// Which walk suits a batch, from a sample of its own warps walked warp-cooperatively with statistics:
+// the per-thread walk pays off where the sampled warps walked at least 1.3 times the nodes of their
+// longest single path and that path met at most 8 leaf triangles on average. Every point of the
+// measured crossover (per-thread / warp-cooperative kernel time 0.54-0.78 on 1M far-field-heavy
+// queries, 1.1-3.0 on surface-heavy or dense batches) outside [0.9, 1.1] falls on the right side of
+// the rule; the sample itself is too slow to take before every batch (its few warps run at the
+// latency of whole walks), so it stays a diagnostic.
+constexpr double k_form_union_ratio = 1.3;
+constexpr double k_form_lane_tris = 8.0;
+
+struct form_sample {
+    std::uint64_t stride, count; // every stride-th full unit of 32 warps, count of them (0: none)
+};
+
+// Every stride-th unit of 32 consecutive ordered warps: one resident wave of units or 1/64 of the
+// batch, whichever is more, for batches of at least four waves; up to 64 units below that.
+form_sample choose_sample(std::uint64_t n) {
+    std::uint64_t const units = n / 1024; // full units
+    std::uint64_t const wave = static_cast<std::uint64_t>(device_sm_count()); // units in one resident wave
+    if (units == 0)
+        return {0, 0};
+    std::uint64_t const stride = units < 4 * wave ? std::max<std::uint64_t>(units / 64, 1)
+                                                  : std::max<std::uint64_t>(units / std::max(wave, units / 64), 2);
+    return {stride, (units + stride - 1) / stride};
 }
 
-// Per sampled warp: the nodes and leaf triangles the warp form walked (the same in every lane) and
-// the largest per-lane node and triangle counts; sums over the sample in sums[0..3].
-__global__ void __launch_bounds__(256)
-    k_probe_reduce(std::uint32_t const *__restrict__ nodes, std::uint32_t const *__restrict__ near,
-                   std::uint32_t const *__restrict__ union_nodes, std::uint32_t const *__restrict__ union_near,
-                   std::uint64_t sample_warps, unsigned long long *sums) {
-    std::uint64_t const i = static_cast<std::uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-    bool const in = (i >> 5) < sample_warps;
-    std::uint32_t mn = in ? nodes[i] : 0u, mt = in ? near[i] : 0u;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        mn = max(mn, __shfl_xor_sync(0xffffffffu, mn, o));
-        mt = max(mt, __shfl_xor_sync(0xffffffffu, mt, o));
-    }
-    if (in && (threadIdx.x & 31u) == 0u) {
-        atomicAdd(&sums[0], static_cast<unsigned long long>(union_nodes[i]));
-        atomicAdd(&sums[1], static_cast<unsigned long long>(union_near[i]));
-        atomicAdd(&sums[2], static_cast<unsigned long long>(mn));
-        atomicAdd(&sums[3], static_cast<unsigned long long>(mt));
-    }
+bool per_thread_wins(double walked, double lane_max, double lane_tris, double count) {
+    return walked >= k_form_union_ratio * lane_max && lane_tris <= k_form_lane_tris * count;
+}
+
+template <int O> int launch_probe(taylor_params const &p, int cap, int mode, cudaStream_t s) {
+    return launch_taylor_order<O, false, true>(p, 256, cap, mode, false, s);
+}
+int dispatch_probe(int order, taylor_params const &p, int cap, int mode, cudaStream_t s) {
+    return order == 0 ? launch_probe<0>(p, cap, mode, s)
+                      : (order == 1 ? launch_probe<1>(p, cap, mode, s) : launch_probe<2>(p, cap, mode, s));
 }
 
 } // namespace
 
-// Sampled-warp probe of a Taylor batch in traversal order `order` (nullptr: the queries are already
-// in that order): runs the warp form with statistics on about 1/128 of the warps (64 to 4,096) and
-// returns, per sampled warp, out[0] nodes walked by the warp, out[1] leaf triangles it evaluated,
-// out[2] the largest per-lane node count and out[3] the largest per-lane triangle count -- the
-// lockstep work of the per-thread form -- and out[4] the number of sampled warps (0: too few
-// queries to sample). Synchronizes the stream.
-int taylor_probe(taylor_request const &r, std::uint32_t const *order, cudaStream_t s, double out[5]) {
-    for (int k = 0; k < 5; ++k)
+// Sampled walk statistics of a batch in traversal order `order` (nullptr: the queries are already
+// in that order): the sample of choose_sample, walked warp-cooperatively with statistics and no
+// outputs; out[0..3] = per sampled warp, nodes walked, triangles walked, longest path nodes, longest
+// path triangles; out[4] sampled warps (0 below 1,024 queries); out[5] 1 when the rule above takes
+// the per-thread walk. Synchronizes the stream.
+int taylor_probe(taylor_request const &r, std::uint32_t const *order, cudaStream_t s, double out[6]) {
+    for (int k = 0; k < 6; ++k)
         out[k] = 0.0;
-    std::uint64_t const warps = r.n / 32;
-    if (warps == 0)
+    form_sample const fs = choose_sample(r.n);
+    if (fs.count == 0)
         return GWNB_OK;
-    std::uint64_t const target = std::min<std::uint64_t>(std::max<std::uint64_t>(warps / 128, 64), 4096);
-    std::uint64_t const stride = std::max<std::uint64_t>(warps / target, 1);
-    std::uint64_t const sample = std::min(warps / stride, target);
-    std::uint64_t const m = sample * 32;
-    float *sq = nullptr;
-    std::uint32_t *st = nullptr;
-    unsigned long long *sums = nullptr;
-    int rc = GWNB_OK;
-    auto cleanup = [&]() {
-        release(sq, s);
-        release(st, s);
-        release(sums, s);
-    };
-    if ((rc = alloc(&sq, 3 * m, s)) != GWNB_OK || (rc = alloc(&st, 5 * m, s)) != GWNB_OK ||
-        (rc = alloc(&sums, 4, s)) != GWNB_OK) {
-        cleanup();
-        return rc;
-    }
-    unsigned const grid = static_cast<unsigned>((m + 255) / 256);
-    note_launch(), k_probe_gather<<<grid, 256, 0, s>>>(order, r.qx, r.qy, r.qz, stride, sample, sq, sq + m, sq + 2 * m);
+    std::uint64_t const warps = fs.count * 32;
+    std::uint32_t *ws = nullptr;
+    GWNB_TRY(alloc(&ws, 4 * warps, s));
     taylor_params p = make_taylor_params(r);
-    p.qx = sq;
-    p.qy = sq + m;
-    p.qz = sq + 2 * m;
-    p.order = nullptr;
+    p.order = order;
     p.gathered = 0;
     p.out = nullptr;
-    p.n = m;
-    p.stat_nodes = st;
-    p.stat_far = st + m;
-    p.stat_near = st + 2 * m;
-    p.stat_union = st + 3 * m;
-    p.stat_union_near = st + 4 * m;
-    int const cap = r.stack_capacity;
-    if (r.order == 0)
-        rc = launch_taylor_order<0, false, true>(p, 256, cap, r.near_mode, false, s);
-    else if (r.order == 1)
-        rc = launch_taylor_order<1, false, true>(p, 256, cap, r.near_mode, false, s);
-    else
-        rc = launch_taylor_order<2, false, true>(p, 256, cap, r.near_mode, false, s);
-    unsigned long long h[4] = {0, 0, 0, 0};
-    if (rc == GWNB_OK) {
-        if (cudaMemsetAsync(sums, 0, 4 * sizeof(unsigned long long), s) != cudaSuccess) {
-            rc = set_cuda_error(cudaGetLastError(), "taylor probe");
-        } else {
-            note_launch(), k_probe_reduce<<<grid, 256, 0, s>>>(st, st + 2 * m, st + 3 * m, st + 4 * m, sample, sums);
-            if (cudaMemcpyAsync(h, sums, sizeof(h), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
-                cudaStreamSynchronize(s) != cudaSuccess)
-                rc = set_cuda_error(cudaGetLastError(), "taylor probe read-back");
-        }
-    }
-    cleanup();
+    p.sample_stride = fs.stride;
+    p.n = warps * 32;
+    p.warp_stats = ws;
+    int rc = dispatch_probe(r.order, p, r.stack_capacity, r.near_mode, s);
+    std::vector<std::uint32_t> h(4 * warps);
+    if (rc == GWNB_OK && (cudaMemcpyAsync(h.data(), ws, h.size() * sizeof(std::uint32_t), cudaMemcpyDeviceToHost, s) !=
+                              cudaSuccess ||
+                          cudaStreamSynchronize(s) != cudaSuccess))
+        rc = set_cuda_error(cudaGetLastError(), "taylor probe read-back");
+    release(ws, s);
     if (rc != GWNB_OK)
         return rc;
+    double t[4] = {0.0, 0.0, 0.0, 0.0};
+    for (std::uint64_t w = 0; w < warps; ++w)
+        for (int k = 0; k < 4; ++k)
+            t[k] += h[4 * w + k];
+    double const c = static_cast<double>(warps);
     for (int k = 0; k < 4; ++k)
-        out[k] = static_cast<double>(h[k]) / static_cast<double>(sample);
-    out[4] = static_cast<double>(sample);
+        out[k] = t[k] / c;
+    out[4] = c;
+    out[5] = per_thread_wins(t[0], t[2], t[3], c) ? 1.0 : 0.0;
     return GWNB_OK;
 }
 

@@ -22,8 +22,7 @@ Restated from smallgwn's tests (none of that code is used):
 antipodal query, which smallgwn's harness launches through its own detail functors; this library
 evaluates both halves in one kernel, so those rows are written with success = 0 and the reason,
 and `query_antipodal` times the whole query. The Taylor stages use the library's default
-warp-cooperative traversal; `--traversal thread` times its per-thread traversal instead (the same
-results). Every stage runs inside an NVTX range of its name (the library's own calls add ranges of
+warp-cooperative walk; `--traversal thread` times its per-thread walk instead (the same results). Every stage runs inside an NVTX range of its name (the library's own calls add ranges of
 theirs inside it).
 
 Usage: python -m smallgwn_b200.stages [--model mesh.ply | --sphere] [--queries N] [--csv PATH] ...
@@ -214,7 +213,7 @@ def run_model(mesh: dict, opts: options, stream=None) -> tuple[list, dict]:
 
     def taylor(o):
         return lambda: api.gwn_compute_winding_number_taylor_batch(o, bvh, mom[o], *q, out, opts.accuracy_scale, s,
-                                                                   config=cfg, per_thread=opts.traversal == "thread")
+                                                                   config=cfg, traversal=opts.traversal)
 
     def setup_boundary():
         return api.gwn_build_boundary_chain(geo, chain, s)

@@ -73,9 +73,9 @@ def test_per_thread_traversal_stage(cuda):
 
 
 def test_form_probe_matches_traversal_statistics(cuda):
-    """The sampled-warp probe reads, for every other warp of an ordered batch (128 warps: 64
-    sampled), the warp's walk and its largest per-query counts; the per-query counts agree with the
-    statistics entry point on the same queries."""
+    """The sample of the automatic walk choice, as a diagnostic: on a small ordered batch (128 warps,
+    4 units of 32 warps, all sampled) it reads every warp's walk and its largest per-query counts;
+    the per-query counts agree with the statistics entry point on the same queries."""
     mesh = meshes.to_soa(*meshes.uv_sphere(40, 21, seed=3))
     geo = g.gwn_geometry_object()
     assert g.gwn_upload_geometry(geo, mesh["x"], mesh["y"], mesh["z"], mesh["i0"], mesh["i1"], mesh["i2"]).is_ok()
@@ -90,13 +90,46 @@ def test_form_probe_matches_traversal_statistics(cuda):
     sq = [d[order.long()].contiguous() for d in q]
     st, pr = api.taylor_form_probe(bvh, mom, *sq, accuracy_scale=2.0, sort_queries=False)
     assert st.is_ok(), st.message
-    assert pr["sampled_warps"] == 64
+    assert pr["sampled_warps"] == 128
     stats = [cuda.empty(n, dtype=cuda.int32, device="cuda") for _ in range(3)]
     assert api.taylor_traversal_stats(bvh, mom, *sq, *stats, accuracy_scale=2.0).is_ok()
-    nodes = stats[0].cpu().numpy().reshape(-1, 32)[::2]
-    near = stats[2].cpu().numpy().reshape(-1, 32)[::2]
+    nodes = stats[0].cpu().numpy().reshape(-1, 32)
+    near = stats[2].cpu().numpy().reshape(-1, 32)
     assert pr["lane_max_nodes"] == pytest.approx(nodes.max(axis=1).mean())
     assert pr["lane_max_tris"] == pytest.approx(near.max(axis=1).mean())
     assert pr["warp_nodes"] >= pr["lane_max_nodes"] > 0 and pr["warp_tris"] >= pr["lane_max_tris"]
     st, none = api.taylor_form_probe(bvh, mom, *[v[:31] for v in sq], accuracy_scale=2.0, sort_queries=False)
     assert st.is_ok() and none["sampled_warps"] == 0
+
+
+@pytest.mark.parametrize("mix", ["harness", "surface"])
+def test_walks_agree_and_sample_rule(cuda, mix):
+    """Both walks give identical results on a batch of a few resident waves; the sampled statistics
+    (units of 32 consecutive ordered warps, every k-th) carry the rule's verdict, 1 exactly when the
+    sampled warps walked at least 1.3 times their longest path's nodes and that path met at most 8
+    leaf triangles on average."""
+    mesh = meshes.to_soa(*meshes.uv_sphere(96, 49, seed=7))
+    n = 700_000
+    src = (meshes.reference_mixed_queries(mesh, n, seed=11) if mix == "harness"
+           else meshes.mixed_queries(mesh, n, seed=12))
+    q = [cuda.from_numpy(v).cuda() for v in src]
+    geo = g.gwn_geometry_object()
+    assert g.gwn_upload_geometry(geo, mesh["x"], mesh["y"], mesh["z"], mesh["i0"], mesh["i1"], mesh["i2"]).is_ok()
+    bvh = g.gwn_bvh4_object()
+    assert g.gwn_build_bvh(geo, bvh).is_ok()
+    mom = g.gwn_bvh4_moment_object(2)
+    assert g.gwn_refit_bvh_moment(2, bvh, mom).is_ok()
+    outs = {}
+    for walk in ("warp", "thread"):
+        o = cuda.full((n,), float("nan"), device="cuda")
+        assert g.gwn_compute_winding_number_taylor_batch(2, bvh, mom, *q, o, 2.0, traversal=walk).is_ok()
+        cuda.cuda.synchronize()
+        outs[walk] = o.cpu().numpy()
+    assert not np.isnan(outs["warp"]).any()
+    np.testing.assert_array_equal(outs["warp"], outs["thread"])
+    st, pr = api.taylor_form_probe(bvh, mom, *q, accuracy_scale=2.0)
+    assert st.is_ok() and pr["sampled_warps"] > 0 and pr["sampled_warps"] % 32 == 0
+    rule = pr["warp_nodes"] >= 1.3 * pr["lane_max_nodes"] and pr["lane_max_tris"] <= 8.0
+    assert pr["per_thread"] == (1.0 if rule else 0.0)
+    assert g.gwn_compute_winding_number_taylor_batch(2, bvh, mom, *q, o, 2.0, traversal="sideways").error == \
+        g.gwn_error.invalid_argument
