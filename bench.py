@@ -1179,7 +1179,7 @@ def run_stages_workload(args) -> None:
     the value)."""
     import torch
 
-    from smallgwn_b200 import meshes, stages
+    from smallgwn_b200 import _lib, meshes, stages
 
     dev = torch.cuda.current_device()
     mesh = meshes.sphere_mesh()
@@ -1192,7 +1192,7 @@ def run_stages_workload(args) -> None:
     if args.csv:
         Path(args.csv).write_text(stages.csv_rows(
             results, context, "synthetic:displaced_uv_sphere_1024x512_seed2", opts, torch.cuda.get_device_name(),
-            0, time.strftime("%Y-%m-%dT%H:%M:%SZ", time.gmtime())))
+            _lib.load().gwnb_cuda_runtime_version(), time.strftime("%Y-%m-%dT%H:%M:%SZ", time.gmtime())))
     # the same Taylor stages with the per-thread walk (identical results), the walk that suits this
     # far-field-heavy mix at 1M queries
     thr, _ = stages.run_model(mesh, stages.options(skip_exact=True, traversal="thread", only=(

@@ -132,6 +132,8 @@ GWNB_API const char *gwnb_last_error_message(void);
 GWNB_API int gwnb_last_cuda_error(void);
 /* Library version string. */
 GWNB_API const char *gwnb_version(void);
+/* Version of the CUDA runtime the library runs on (1000 * major + 10 * minor; 0 if unknown). */
+GWNB_API int gwnb_cuda_runtime_version(void);
 
 /* Number of kernel launches this library has issued in the process (all threads and devices); a
  * launch recorded into a CUDA graph counts once, when it is captured. For benchmarks and tests that

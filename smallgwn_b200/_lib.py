@@ -196,6 +196,7 @@ SIGNATURES: dict[str, tuple] = {
     "gwnb_last_error_message": (C.c_char_p, []),
     "gwnb_last_cuda_error": (I, []),
     "gwnb_version": (C.c_char_p, []),
+    "gwnb_cuda_runtime_version": (C.c_int, []),
     "gwnb_memory_stats": (C.c_int, [C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     "gwnb_memory_trim": (C.c_int, [C.c_uint64]),
     "gwnb_launch_count": (C.c_uint64, []),

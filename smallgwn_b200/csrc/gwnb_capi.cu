@@ -449,6 +449,11 @@ int gwnb_memory_trim(uint64_t keep_bytes) try {
 int gwnb_last_cuda_error(void) { return g_cuda_error; }
 const char *gwnb_version(void) { return "gwnb 0.1 (sm_100a)"; }
 
+int gwnb_cuda_runtime_version(void) {
+    int v = 0;
+    return cudaRuntimeGetVersion(&v) == cudaSuccess ? v : 0;
+}
+
 int gwnb_geometry_upload_f32(gwnb_geometry_f32 *out, const float *x, const float *y, const float *z,
                              uint64_t nv, const uint32_t *i0, const uint32_t *i1, const uint32_t *i2,
                              uint64_t nt, gwnb_stream_t stream) try {

@@ -301,7 +301,7 @@ def csv_rows(results, context: dict, model_path: str, opts: options, gpu_name: s
 def main(argv=None) -> int:
     import torch
 
-    from . import api, meshes
+    from . import _lib, api, meshes
 
     ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
     src = ap.add_mutually_exclusive_group()
@@ -336,7 +336,7 @@ def main(argv=None) -> int:
         print(line, flush=True)
     stamp = datetime.datetime.now(datetime.timezone.utc).strftime("%Y-%m-%dT%H:%M:%SZ")
     a.csv.write_text(csv_rows(results, context, model, opts, torch.cuda.get_device_name(),
-                              torch.cuda.runtime_version() if hasattr(torch.cuda, "runtime_version") else 0, stamp))
+                              _lib.load().gwnb_cuda_runtime_version(), stamp))
     return 0 if all(r.success or r.error_message == FUSED_ANTIPODAL for r in results) else 1
 
 
