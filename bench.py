@@ -1286,12 +1286,25 @@ def run_stages_workload(args) -> None:
         Path(args.csv).write_text(stages.csv_rows(
             results, context, "synthetic:displaced_uv_sphere_1024x512_seed2", opts, torch.cuda.get_device_name(),
             _lib.load().gwnb_cuda_runtime_version(), time.strftime("%Y-%m-%dT%H:%M:%SZ", time.gmtime())))
-    # the same Taylor stages with the per-thread walk (identical results), the walk that suits this
-    # far-field-heavy mix at 1M queries
-    thr, _ = stages.run_model(mesh, stages.options(skip_exact=True, traversal="thread", only=(
-        "query_taylor_o0", "query_taylor_o1", "query_taylor_o2", "dynamic_refit_query_o2")))
-    per_thread = {r.stage: {"mean_ms": r.latency_mean_ms, "p50_ms": r.latency_p50_ms, "p95_ms": r.latency_p95_ms,
-                            "throughput_per_s": r.throughput_per_s} for r in thr if r.success}
+    # the same Taylor stages with each walk forced (identical results): the warp-cooperative walk
+    # (the library's default) and the per-thread walk, which suits this far-field-heavy mix at 1M
+    taylor_stages = ("query_taylor_o0", "query_taylor_o1", "query_taylor_o2", "dynamic_refit_query_o2")
+    forced = {}
+    for walk in ("warp", "thread"):
+        fr, _ = stages.run_model(mesh, stages.options(skip_exact=True, traversal=walk, only=taylor_stages))
+        forced[walk] = {r.stage: {"mean_ms": r.latency_mean_ms, "p50_ms": r.latency_p50_ms,
+                                  "p95_ms": r.latency_p95_ms, "throughput_per_s": r.throughput_per_s}
+                        for r in fr if r.success}
+    per_thread = forced["thread"]
+    # the query stages timed as smallgwn's kernels are timed beside them (L2 flushed before each call,
+    # no synchronization between calls), both walks
+    kernels = ("query_taylor_o0", "query_taylor_o1", "query_taylor_o2", "query_antipodal", "query_ray_first_hit")
+    like = {}
+    for walk in ("timed", "warp", "thread"):
+        rs, _ = stages.run_model(mesh, stages.options(skip_exact=True, traversal=walk, flush_l2=True,
+                                                      stream_sync_per_iter=False,
+                                                      only=kernels if walk == "timed" else kernels[:3]))
+        like[walk] = {r.stage: r.latency_mean_ms for r in rs if r.success}
     sg = smallgwn_stage_times(mesh, opts)
     head = rows["query_taylor_o2"]
     line = {
@@ -1306,12 +1319,19 @@ def run_stages_workload(args) -> None:
                    "skip_exact": opts.skip_exact,
                    "boundary_edge_count": context.get("boundary_edge_count"),
                    "ray_mix_hit_ratio": context.get("ray_mix_hit_ratio"), "stages": rows,
+                   "traversal": opts.traversal,
                    "per_thread_traversal_stages": per_thread,
+                   "warp_traversal_stages": forced["warp"],
                    "smallgwn_kernels_mean_ms": sg,
                    "over_smallgwn": {k: sg[k] / rows[k]["mean_ms"] for k in (sg or {})
                                      if rows.get(k, {}).get("mean_ms")},
                    "per_thread_over_smallgwn": {k: sg[k] / per_thread[k]["mean_ms"] for k in (sg or {})
-                                                if per_thread.get(k, {}).get("mean_ms")}},
+                                                if per_thread.get(k, {}).get("mean_ms")},
+                   "warp_over_smallgwn": {k: sg[k] / forced["warp"][k]["mean_ms"] for k in (sg or {})
+                                          if forced["warp"].get(k, {}).get("mean_ms")},
+                   "flushed_mean_ms": like,
+                   "flushed_over_smallgwn": {w: {k: sg[k] / v for k, v in like[w].items() if k in (sg or {})}
+                                             for w in like}},
         "clocks": clocks.summary(),
     }
     print(json.dumps(line), flush=True)

@@ -71,6 +71,9 @@ struct gwn_taylor_batch_options {
     // pairs whose numerator and denominator are both below threshold * |a||b||c| go to FP64; at
     // 1/16 that is ~0.03 pairs per query on near-surface sets, at no measurable cost
     float fp64_threshold = 1.0f / 16.0f;
+    // GWNB_WALK_WARP, GWNB_WALK_THREAD or GWNB_WALK_TIMED (the faster walk for calls of this kind,
+    // chosen from the timed first two); identical results
+    int walk = GWNB_WALK_WARP;
 };
 
 namespace detail {
@@ -140,7 +143,7 @@ template <int Order, gwn_query_batch_config Config = gwn_query_batch_config{}, i
         gwnb_bvh4_f32 v = detail::query_view(bvh);
         gwnb_moment4_f32 m = moment.view();
         gwnb_taylor_options o{Config.block_size, Config.stack_capacity, options.sort_queries ? 1 : 0,
-                              options.near_precision, options.fp64_threshold, 0};
+                              options.near_precision, options.fp64_threshold, options.walk};
         int const rc = gwnb_winding_taylor_batch_f32(&v, &m, qx.data(), qy.data(), qz.data(), output.data(),
                                                      output.size(), accuracy_scale, &o, detail::gwnb_stream(stream));
         detail::store_aux(bvh, v);

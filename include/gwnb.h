@@ -55,6 +55,18 @@ enum {
     GWNB_NEAR_COMPENSATED = 1, /* two-product compensated FP32, FP64 on flagged triangles    */
 };
 
+/* Walk of the Taylor traversal (gwnb_taylor_options::per_thread). Both walks give identical results.
+ * GWNB_WALK_TIMED: the first call of a kind (moment object, order, precision, gradient or value,
+ * accuracy scale, ordered or not, device, floor(log2 n)) walks warp-cooperatively and the second per
+ * thread, each timed with CUDA events; once both timings have completed, calls of that kind take the
+ * faster walk (until then the warp walk). Nothing blocks on the timings; calls under stream capture
+ * record nothing and take the decided walk, else the warp walk. */
+enum {
+    GWNB_WALK_WARP = 0,   /* 32 ordered queries per warp walk one traversal together (default) */
+    GWNB_WALK_THREAD = 1, /* one independent traversal per query                               */
+    GWNB_WALK_TIMED = 2,  /* the faster of the two, chosen from timed calls of the same kind    */
+};
+
 typedef struct gwnb_aabb_f32 {
     float min_x, min_y, min_z, max_x, max_y, max_z;
 } gwnb_aabb_f32;
@@ -120,7 +132,7 @@ typedef struct gwnb_taylor_options {
     int sort_queries;   /* 1: Hilbert-order the batch internally for traversal coherence         */
     int near_precision; /* GWNB_NEAR_PLAIN or GWNB_NEAR_COMPENSATED                               */
     float fp64_threshold; /* compensated mode: |den| < threshold * |a||b||c| takes the FP64 path */
-    int per_thread;       /* 0: warp-cooperative traversal (default); 1: one traversal per thread  */
+    int per_thread;       /* GWNB_WALK_WARP (0, default), GWNB_WALK_THREAD (1) or GWNB_WALK_TIMED (2) */
 } gwnb_taylor_options;
 
 /* ---- status ------------------------------------------------------------------------------ */
@@ -534,7 +546,8 @@ GWNB_API int gwnb_scene_load_f32(const char *path, gwnb_geometry_f32 *geometry, 
  * device array (about 5.5 MB) that every GPU loading the library holds until exit; calls whose
  * work overlaps on the GPU race on it. The BVH must already carry derived state (built or refit
  * by this library). The first call on a device looks up the array's address; make it before any
- * stream capture. */
+ * stream capture. options->per_thread takes GWNB_WALK_WARP or GWNB_WALK_THREAD only (the timed
+ * choice keeps events, which a call that allocates nothing does not create). */
 GWNB_API int gwnb_winding_taylor_batch_noalloc_f32(const gwnb_bvh4_f32 *bvh, const gwnb_moment4_f32 *moment,
                                                    const float *query_x, const float *query_y,
                                                    const float *query_z, float *output, uint64_t count,

@@ -21,6 +21,10 @@ GWNB_METHOD_LBVH = 1
 GWNB_NEAR_PLAIN = 0
 GWNB_NEAR_COMPENSATED = 1
 
+GWNB_WALK_WARP = 0
+GWNB_WALK_THREAD = 1
+GWNB_WALK_TIMED = 2
+
 GWNB_BATCH_REFIT = 1
 GWNB_BATCH_MOMENTS = 2
 GWNB_BATCH_QUERY = 4

@@ -373,7 +373,9 @@ def gwn_compute_winding_number_exact_batch(bvh: gwn_bvh4_object, qx, qy, qz, out
     return _status(rc)
 
 
-TRAVERSALS = {"warp": 0, "thread": 1}  # gwnb_taylor_options::per_thread
+# gwnb_taylor_options::per_thread: "timed" takes the faster of the two walks, chosen from the timed
+# first two calls of the same kind (identical results either way)
+TRAVERSALS = {"warp": _lib.GWNB_WALK_WARP, "thread": _lib.GWNB_WALK_THREAD, "timed": _lib.GWNB_WALK_TIMED}
 
 
 def _options(config: gwn_query_batch_config, sort_queries: bool, precision: int, fp64_threshold: float,
@@ -390,8 +392,9 @@ def gwn_compute_winding_number_taylor_batch(order: int, bvh: gwn_bvh4_object, mo
                                             fp64_threshold: float = FP64_THRESHOLD, per_thread: bool = False,
                                             traversal: str = "warp") -> gwn_status:
     """Taylor-approximated winding numbers of a device batch (asynchronous). ``traversal``: "warp"
-    (the default: 32 ordered queries per warp walk one traversal together) or "thread" (one
-    independent walk per query; also ``per_thread=True``); both give identical results."""
+    (the default: 32 ordered queries per warp walk one traversal together), "thread" (one
+    independent walk per query; also ``per_thread=True``) or "timed" (the faster of the two for
+    calls of this kind, from the timed first two); all give identical results."""
     if moment.order != order:
         return gwn_status(gwn_error.invalid_argument, "Moment object order does not match the requested order.")
     if traversal not in TRAVERSALS:
@@ -409,15 +412,18 @@ def gwn_compute_winding_number_taylor_batch(order: int, bvh: gwn_bvh4_object, mo
 def gwn_compute_winding_gradient_taylor_batch(order: int, bvh: gwn_bvh4_object, moment: gwn_bvh4_moment_object,
                                               qx, qy, qz, gx, gy, gz, accuracy_scale: float = 2.0, stream=None,
                                               config: gwn_query_batch_config = gwn_query_batch_config(),
-                                              sort_queries: bool = True) -> gwn_status:
-    """Gradient of the Taylor winding number with respect to the query point."""
+                                              sort_queries: bool = True, traversal: str = "warp") -> gwn_status:
+    """Gradient of the Taylor winding number with respect to the query point (``traversal`` as for
+    the value batch)."""
     if moment.order != order:
         return gwn_status(gwn_error.invalid_argument, "Moment object order does not match the requested order.")
+    if traversal not in TRAVERSALS:
+        return gwn_status(gwn_error.invalid_argument, f"Unknown traversal {traversal!r}.")
     for g in (gx, gy, gz):
         bad = _check_spans(qx, qy, qz, g)
         if bad is not None:
             return bad
-    opt = _options(config, sort_queries, near_precision.plain, FP64_THRESHOLD)
+    opt = _options(config, sort_queries, near_precision.plain, FP64_THRESHOLD, traversal=traversal)
     rc = _lib.load().gwnb_winding_gradient_taylor_batch_f32(
         C.byref(bvh._view), C.byref(moment._view), _ptr(qx), _ptr(qy), _ptr(qz), _ptr(gx), _ptr(gy), _ptr(gz),
         _numel(qx), float(accuracy_scale), C.byref(opt), _stream(stream))

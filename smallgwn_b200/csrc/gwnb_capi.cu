@@ -876,8 +876,8 @@ static int taylor_common(const gwnb_bvh4_f32 *b_in, const gwnb_moment4_f32 *m, c
         return set_error(GWNB_INVALID_ARGUMENT, "Taylor accuracy scale must be nonnegative.");
     if (o.near_precision != GWNB_NEAR_PLAIN && o.near_precision != GWNB_NEAR_COMPENSATED)
         return set_error(GWNB_INVALID_ARGUMENT, "Unknown near-field precision mode.");
-    if (o.per_thread != 0 && o.per_thread != 1)
-        return set_error(GWNB_INVALID_ARGUMENT, "Unknown traversal (per_thread must be 0 or 1).");
+    if (o.per_thread < GWNB_WALK_WARP || o.per_thread > GWNB_WALK_TIMED)
+        return set_error(GWNB_INVALID_ARGUMENT, "Unknown traversal (per_thread must be 0, 1 or 2).");
     if (!has_storage(qx, n) || !has_storage(qy, n) || !has_storage(qz, n))
         return set_error(GWNB_INVALID_ARGUMENT, "Query/output spans must use non-null storage when non-empty.");
     if (probe == nullptr && (out != nullptr || (gx == nullptr && sn == nullptr)))

@@ -18,6 +18,10 @@
 #include "gwnb_field.cuh"
 
 #include <algorithm>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <tuple>
 #include <vector>
 
 namespace gwnb {
@@ -883,6 +887,129 @@ int taylor_probe(taylor_request const &r, std::uint32_t const *order, cudaStream
     return GWNB_OK;
 }
 
+// ---- timed choice of the walk (per_thread = 2) -------------------------------------------------------
+//
+// Both walks give identical results; which one is faster depends on the batch (dense or
+// surface-heavy batches favour the warp walk, sparse far-field-heavy ones the per-thread walk). The
+// first call of a kind walks warp-cooperatively and the second per thread, each traversal launch
+// bracketed by CUDA events; a later call whose two measurements have completed takes the faster
+// walk from then on (until then: the warp walk, untimed). A kind is the moment sidecar's address,
+// order, precision mode, gradient form, accuracy scale, whether the batch is ordered, the device
+// and floor(log2 n). Nothing blocks: the events are polled. Calls under stream capture take the
+// decided walk, or the warp walk, and record nothing.
+namespace {
+
+struct walk_kind {
+    void const *qnodes;
+    int device, order, mode, grad, sorted, size_class;
+    std::uint32_t beta_bits;
+    bool operator<(walk_kind const &o) const {
+        return std::tie(qnodes, device, order, mode, grad, sorted, size_class, beta_bits) <
+               std::tie(o.qnodes, o.device, o.order, o.mode, o.grad, o.sorted, o.size_class, o.beta_bits);
+    }
+};
+struct walk_timing {
+    int phase = 0; // 0: nothing timed; 1: warp walk timed; 2: both timed; 3: decided
+    bool per_thread = false;
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr}; // warp start / end, per-thread start / end
+};
+struct walk_plan {
+    bool per_thread = false;
+    cudaEvent_t start = nullptr, stop = nullptr; // recorded around the traversal (null: untimed)
+};
+
+constexpr std::size_t k_walk_kinds = 256; // the table is emptied when it holds this many kinds
+
+std::mutex &walk_mutex() {
+    static std::mutex m;
+    return m;
+}
+std::map<walk_kind, walk_timing> &walk_table() {
+    static auto *t = new std::map<walk_kind, walk_timing>(); // never destroyed: outlives the runtime at exit
+    return *t;
+}
+
+void destroy_events(walk_timing &t) {
+    for (auto &e : t.ev)
+        if (e != nullptr) {
+            cudaEventDestroy(e);
+            e = nullptr;
+        }
+}
+
+// cudaSuccess when the event has completed, cudaErrorNotReady while it is pending (not left as the
+// thread's last error), another code on failure.
+cudaError_t poll(cudaEvent_t e) {
+    cudaError_t const q = cudaEventQuery(e);
+    if (q == cudaErrorNotReady && cudaPeekAtLastError() == cudaErrorNotReady)
+        (void)cudaGetLastError();
+    return q;
+}
+
+walk_plan plan_walk(walk_kind const &k, cudaStream_t s) {
+    walk_plan plan;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    bool const capturing = cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone;
+    std::lock_guard<std::mutex> lock(walk_mutex());
+    auto &table = walk_table();
+    auto it = table.find(k);
+    if (capturing) {
+        plan.per_thread = it != table.end() && it->second.phase == 3 && it->second.per_thread;
+        return plan;
+    }
+    if (it == table.end()) {
+        if (table.size() >= k_walk_kinds) {
+            for (auto &kv : table)
+                destroy_events(kv.second);
+            table.clear();
+        }
+        walk_timing t;
+        for (auto &e : t.ev)
+            if (cudaEventCreate(&e) != cudaSuccess) {
+                (void)cudaGetLastError();
+                destroy_events(t);
+                return plan; // untimed warp walk
+            }
+        it = table.emplace(k, t).first;
+    }
+    walk_timing &t = it->second;
+    switch (t.phase) {
+    case 0:
+        plan.start = t.ev[0];
+        plan.stop = t.ev[1];
+        t.phase = 1;
+        break;
+    case 1:
+        plan.per_thread = true;
+        plan.start = t.ev[2];
+        plan.stop = t.ev[3];
+        t.phase = 2;
+        break;
+    case 2: {
+        cudaError_t const a = poll(t.ev[1]);
+        cudaError_t const b = a == cudaSuccess ? poll(t.ev[3]) : a;
+        if (a == cudaErrorNotReady || b == cudaErrorNotReady)
+            break; // still pending: warp walk, untimed
+        float warp_ms = 0.0f, thread_ms = 0.0f;
+        bool const ok = a == cudaSuccess && b == cudaSuccess &&
+                        cudaEventElapsedTime(&warp_ms, t.ev[0], t.ev[1]) == cudaSuccess &&
+                        cudaEventElapsedTime(&thread_ms, t.ev[2], t.ev[3]) == cudaSuccess;
+        if (!ok)
+            (void)cudaGetLastError();
+        t.per_thread = ok && thread_ms < warp_ms;
+        t.phase = 3;
+        destroy_events(t);
+        plan.per_thread = t.per_thread;
+        break;
+    }
+    default:
+        plan.per_thread = t.per_thread;
+    }
+    return plan;
+}
+
+} // namespace
+
 int taylor_batch(taylor_request const &r, cudaStream_t s) {
     if (r.n == 0)
         return GWNB_OK;
@@ -927,7 +1054,24 @@ int taylor_batch(taylor_request const &r, cudaStream_t s) {
     GWNB_NVTX("gwnb::taylor.traverse");
     int const block = query_launch_block(r.block);
     int const cap = r.stack_capacity;
-    bool const per_thread = r.per_thread != 0;
+    walk_plan plan;
+    plan.per_thread = r.per_thread == 1;
+    if (r.per_thread == 2 && !stats) {
+        int device = 0;
+        (void)cudaGetDevice(&device);
+        float const beta = r.accuracy_scale;
+        std::uint32_t beta_bits = 0;
+        std::memcpy(&beta_bits, &beta, sizeof(beta_bits));
+        int size_class = 0;
+        for (std::uint64_t v = r.n; v > 1; v >>= 1)
+            ++size_class;
+        plan = plan_walk(walk_kind{r.qnodes, device, r.order, r.near_mode, grad ? 1 : 0, sorted ? 1 : 0, size_class,
+                                   beta_bits},
+                         s);
+    }
+    bool const per_thread = plan.per_thread;
+    if (plan.start != nullptr)
+        (void)cudaEventRecord(plan.start, s);
 #define GWNB_DISPATCH(O)                                                                           \
     if (grad)                                                                                      \
         rc = launch_taylor_order<O, true, false>(p, block, cap, r.near_mode, per_thread, s);       \
@@ -943,6 +1087,8 @@ int taylor_batch(taylor_request const &r, cudaStream_t s) {
         GWNB_DISPATCH(2)
     }
 #undef GWNB_DISPATCH
+    if (plan.stop != nullptr)
+        (void)cudaEventRecord(plan.stop, s);
     release(codes, s);
     release(sorted_codes, s);
     release(order, s);

@@ -21,9 +21,10 @@ Restated from smallgwn's tests (none of that code is used):
 `query_antipodal_crossings` and `query_antipodal_boundary` time the two halves of smallgwn's
 antipodal query, which smallgwn's harness launches through its own detail functors; this library
 evaluates both halves in one kernel, so those rows are written with success = 0 and the reason,
-and `query_antipodal` times the whole query. The Taylor stages use the library's default
-warp-cooperative walk; `--traversal thread` times its per-thread walk instead (the same results). Every stage runs inside an NVTX range of its name (the library's own calls add ranges of
-theirs inside it).
+and `query_antipodal` times the whole query. The Taylor stages take the library's timed walk choice
+(the warm-up's first two calls time the warp-cooperative and the per-thread walk, the measured calls
+take the faster); `--traversal warp|thread` forces one walk (the same results). Every stage runs
+inside an NVTX range of its name (the library's own calls add ranges of theirs inside it).
 
 Usage: python -m smallgwn_b200.stages [--model mesh.ply | --sphere] [--queries N] [--csv PATH] ...
 """
@@ -66,8 +67,14 @@ class options:
     builder: str = "hploc"
     skip_exact: bool = False
     winding_query_only: bool = False
-    traversal: str = "warp"  # Taylor stages: the library's default warp-cooperative walk, or "thread"
+    # Taylor stages: the walk that the timed calls of the warm-up pick ("timed"), or a forced
+    # "warp" / "thread" walk (identical results)
+    traversal: str = "timed"
     only: tuple = ()         # run just these stages (empty: all)
+    # Not smallgwn's: time the calls as its kernels are timed beside them -- a 256 MiB write that
+    # flushes the L2 before each measured call, the events read after the last call (no
+    # synchronization between calls), so the host's enqueueing overlaps the flush.
+    flush_l2: bool = False
 
 
 @dataclass
@@ -108,10 +115,13 @@ def summarize(samples) -> tuple[float, float, float]:
     return float(np.mean(np.asarray(samples, dtype=np.float64))), percentile_ms(samples, 0.5), percentile_ms(samples, 0.95)
 
 
-def measure_stage_latency_ms(warmup_iters: int, measure_iters: int, stream, sync_per_iter: bool, fn) -> list:
+def measure_stage_latency_ms(warmup_iters: int, measure_iters: int, stream, sync_per_iter: bool, fn,
+                             flush=None) -> list:
     """Per-call milliseconds of `fn` (a callable returning a gwn_status) after `warmup_iters` untimed
     calls, CUDA events around each call on `stream` (smallgwn's gwn_measure_stage_latency_ms).
-    Raises RuntimeError with the status message when a call fails."""
+    With `flush` (a device buffer larger than the L2), the buffer is written before each measured
+    call, outside its events, and the events are read after the last call. Raises RuntimeError with
+    the status message when a call fails."""
     import torch
 
     if warmup_iters < 0 or measure_iters <= 0:
@@ -126,6 +136,19 @@ def measure_stage_latency_ms(warmup_iters: int, measure_iters: int, stream, sync
         call()
         if sync_per_iter:
             stream.synchronize()
+    if flush is not None:
+        stream.synchronize()
+        ev = []
+        for i in range(measure_iters):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            with torch.cuda.stream(stream):
+                flush.fill_(i & 0xFF)
+            e0.record(stream)
+            call()
+            e1.record(stream)
+            ev.append((e0, e1))
+        stream.synchronize()
+        return [a.elapsed_time(b) for a, b in ev]
     out = []
     for _ in range(measure_iters):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -140,7 +163,7 @@ def measure_stage_latency_ms(warmup_iters: int, measure_iters: int, stream, sync
 
 
 def run_stage(name: str, unit: str, denominator: int, opts: options, vertex_count: int, triangle_count: int,
-              stream, setup, fn) -> stage_result:
+              stream, setup, fn, flush=None) -> stage_result:
     """One stage: `setup` once (untimed), then the timed calls of `fn`; failures become the row's
     error message, as in smallgwn's run_stage (tests/benchmark_main.cu:286-330)."""
     import torch
@@ -154,7 +177,7 @@ def run_stage(name: str, unit: str, denominator: int, opts: options, vertex_coun
                 r.error_message = st.message
                 return r
             r.samples_ms = measure_stage_latency_ms(opts.warmup_iters, opts.measure_iters, stream,
-                                                    opts.stream_sync_per_iter, fn)
+                                                    opts.stream_sync_per_iter, fn, flush)
         except RuntimeError as e:
             r.error_message = str(e)
             return r
@@ -201,6 +224,7 @@ def run_model(mesh: dict, opts: options, stream=None) -> tuple[list, dict]:
     hits = torch.empty((nq, 8), dtype=torch.int32, device="cuda")
     cfg = api.gwn_query_batch_config(stack_capacity=opts.stack_capacity)
     ok = api.gwn_status()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda") if opts.flush_l2 else None
 
     def build():
         return api.gwn_build_bvh(geo, bvh, api.gwn_bvh_build_options(method=method), s)
@@ -247,7 +271,7 @@ def run_model(mesh: dict, opts: options, stream=None) -> tuple[list, dict]:
     def stage(name, unit, denom, setup, fn):
         if opts.only and name not in opts.only:
             return None
-        return run_stage(name, unit, denom, opts, nv, nt, stream, setup, fn)
+        return run_stage(name, unit, denom, opts, nv, nt, stream, setup, fn, flush)
 
     query_o1 = lambda: stage("query_taylor_o1", "queries/s", nq, build_moment(1), taylor(1))  # noqa: E731
     query_antipodal = lambda: stage(  # noqa: E731
@@ -318,8 +342,9 @@ def main(argv=None) -> int:
     ap.add_argument("--builder", choices=["hploc", "lbvh"], default=d.builder)
     ap.add_argument("--skip-exact", action="store_true")
     ap.add_argument("--winding-query-only", action="store_true")
-    ap.add_argument("--traversal", choices=["warp", "thread"], default=d.traversal,
-                    help="Taylor stages: warp-cooperative walk (the library's default) or one walk per thread")
+    ap.add_argument("--traversal", choices=["timed", "warp", "thread"], default=d.traversal,
+                    help="Taylor stages: the faster walk from timed warm-up calls, the warp-cooperative walk "
+                         "or one walk per thread")
     ap.add_argument("--csv", type=Path, default=Path("smallgwn_bench.csv"))
     a = ap.parse_args(argv)
     opts = options(a.queries, a.warmup, a.iters, a.accuracy_scale, a.stack_capacity, not a.no_stream_sync, a.seed,

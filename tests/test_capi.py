@@ -104,6 +104,10 @@ def test_queries_reject_invalid_state_without_gpu():
     assert lib.gwnb_winding_taylor_batch_f32(C.byref(fake), C.byref(fresh), None, None, None, None, 0, 2.0,
                                              C.byref(bad_walk), None) == _lib.GWNB_INVALID_ARGUMENT
     assert "Unknown traversal" in _lib.last_error()
+    beyond = _lib.taylor_options(256, 64, 1, 0, 1.0 / 16.0, _lib.GWNB_WALK_TIMED + 1)
+    assert lib.gwnb_winding_taylor_batch_f32(C.byref(fake), C.byref(fresh), None, None, None, None, 0, 2.0,
+                                             C.byref(beyond), None) == _lib.GWNB_INVALID_ARGUMENT
+    assert "Unknown traversal" in _lib.last_error()
 
 
 def test_stack_capacity_below_bound_is_rejected():

@@ -443,6 +443,31 @@ def test_warp_cooperative_equals_per_thread_traversal(cuda, order):
             assert np.mean(a == b) > 0.999 and within(a, b, atol=1e-6, rtol=1e-6)
 
 
+def test_timed_walk_choice(cuda):
+    """GWNB_WALK_TIMED: the first call of a kind walks warp-cooperatively, the second per thread,
+    both timed, and later calls take the faster walk. Every call returns what one of the two forced
+    walks returns; another accuracy scale is another kind; the gradient batch takes the option too."""
+    mesh = WORKLOADS["uv64x32"]()
+    bvh = build(upload(mesh), g.gwn_bvh_build_method.k_hploc)
+    mom = moments_of(bvh, 2)
+    q = meshes.mixed_queries(mesh, 20000, seed=29)
+    for beta in (2.0, 3.0):
+        forced = [run_taylor(cuda, 2, bvh, mom, q, beta, traversal=w) for w in ("warp", "thread")]
+        for _ in range(6):
+            got = run_taylor(cuda, 2, bvh, mom, q, beta, traversal="timed")
+            assert any(np.array_equal(got, f) for f in forced)
+    d = dev(cuda, *q)
+    grads = []
+    for walk in ("warp", "timed", "timed", "timed"):
+        gr = [cuda.empty_like(d[0]) for _ in range(3)]
+        st = g.gwn_compute_winding_gradient_taylor_batch(2, bvh, mom, *d, *gr, accuracy_scale=2.0, traversal=walk)
+        assert st.is_ok(), st.message
+        cuda.cuda.synchronize()
+        grads.append(np.stack([v.cpu().numpy() for v in gr]))
+    for other in grads[1:]:
+        assert np.all(np.isfinite(other)) and within(other, grads[0], atol=1e-6, rtol=1e-6)
+
+
 @pytest.mark.parametrize("block", [32, 128, 512, 1024])
 def test_block_sizes_up_to_1024_give_the_same_results(cuda, block):
     """smallgwn accepts batch block sizes up to 1024 (include/gwn/gwn_query.cuh:37); the kernels here

@@ -72,6 +72,18 @@ def test_per_thread_traversal_stage(cuda):
     assert [r.stage for r in results] == ["query_taylor_o1", "query_taylor_o2"] and all(r.success for r in results)
 
 
+def test_flushed_timing_without_per_call_synchronization(cuda):
+    """The comparison timing (L2 flushed before each call, events read after the last call) runs
+    the same stages as the harness timing and times every call."""
+    mesh = meshes.to_soa(*meshes.uv_sphere(32, 17, seed=2))
+    only = ("query_taylor_o2", "query_ray_first_hit")
+    base, _ = stages.run_model(mesh, stages.options(query_count=2000, warmup_iters=1, measure_iters=3, only=only))
+    res, _ = stages.run_model(mesh, stages.options(query_count=2000, warmup_iters=1, measure_iters=3, only=only,
+                                                   flush_l2=True, stream_sync_per_iter=False))
+    assert [r.stage for r in res] == list(only) and all(r.success for r in res + base)
+    assert all(len(r.samples_ms) == 3 and min(r.samples_ms) > 0 for r in res)
+
+
 def test_form_probe_matches_traversal_statistics(cuda):
     """The sample of the automatic walk choice, as a diagnostic: on a small ordered batch (128 warps,
     4 units of 32 warps, all sampled) it reads every warp's walk and its largest per-query counts;

@@ -72,3 +72,9 @@ def test_no_alloc_taylor_batch_matches_allocating_batch():
         expected.data_ptr(), MAX_QUERIES + 1, 3.0, C.byref(opt), None)
     assert rc == _lib.GWNB_INVALID_ARGUMENT
     assert "maximum" in _lib.last_error()
+    # the timed walk choice keeps CUDA events, which this entry point does not create
+    timed = _lib.taylor_options(256, 64, 1, _lib.GWNB_NEAR_PLAIN, 1e-3, _lib.GWNB_WALK_TIMED)
+    rc = lib.gwnb_winding_taylor_batch_noalloc_f32(
+        C.byref(bvh.accessor()), C.byref(mom.accessor()), q[0].data_ptr(), q[1].data_ptr(), q[2].data_ptr(),
+        expected.data_ptr(), n, 3.0, C.byref(timed), None)
+    assert rc == _lib.GWNB_INVALID_ARGUMENT and "Unknown traversal" in _lib.last_error()
