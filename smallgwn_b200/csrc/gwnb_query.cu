@@ -235,6 +235,9 @@ struct taylor_params {
     // nodes, largest per-query triangles} to warp_stats[4 w ...].
     std::uint64_t sample_stride;
     std::uint32_t *warp_stats;
+    // per-thread walk: entries of this thread's shared-memory stack column when below the kernel's
+    // Cap (the BVH's internal stack bound, so that more blocks fit an SM); 0: Cap
+    int thread_stack_cap;
     std::uint64_t n;
     float beta2;
     float fp64_threshold;
@@ -258,6 +261,7 @@ __device__ __forceinline__ void taylor_thread_item(taylor_params const &p, std::
     std::uint32_t st_nodes = 0, st_far = 0, st_near = 0;
     unsigned const stride = blockDim.x;
     std::uint32_t *const stack = s_stack; // this thread's column; entries are blockDim.x apart
+    int const cap = p.thread_stack_cap > 0 && p.thread_stack_cap < Cap ? p.thread_stack_cap : Cap;
     int sp = 0;
     bool overflow = false;
 
@@ -324,7 +328,7 @@ __device__ __forceinline__ void taylor_thread_item(taylor_params const &p, std::
                 std::uint32_t const ref = __float_as_uint(b.w);
                 if ((ref & k_qref_leaf) == 0u) {
                     if (next != k_invalid_u32) {
-                        if (sp >= Cap) {
+                        if (sp >= cap) {
                             overflow = true;
                             break;
                         }
@@ -672,9 +676,13 @@ int launch_taylor_warp(taylor_params const &p, cudaStream_t s) {
     return GWNB_OK;
 }
 
+// Per-thread walk: each thread's stack column holds `cap` entries (the BVH's internal stack bound,
+// at most Cap): a 46-entry bound fits four blocks of 256 per SM where 64-entry columns fit three.
 template <int Order, int Cap, int Mode, bool Grad, bool Stats>
-int launch_taylor_cap(taylor_params const &p, int block, cudaStream_t s) {
-    std::size_t const smem = static_cast<std::size_t>(Cap) * block * sizeof(std::uint32_t);
+int launch_taylor_cap(taylor_params const &p_in, int block, int cap, cudaStream_t s) {
+    taylor_params p = p_in;
+    p.thread_stack_cap = cap > 0 && cap < Cap ? cap : Cap;
+    std::size_t const smem = static_cast<std::size_t>(p.thread_stack_cap) * block * sizeof(std::uint32_t);
     auto kern = k_taylor<Order, Cap, Mode, Grad, Stats>;
     if (smem > 48 * 1024)
         GWNB_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -692,12 +700,12 @@ int launch_taylor_mode(taylor_params const &p, int block, int cap, bool per_thre
     if (!per_thread && cap <= 64)
         return launch_taylor_warp<Order, 64, Mode, Grad, Stats>(p, s);
     if (cap <= 16)
-        return launch_taylor_cap<Order, 16, Mode, Grad, Stats>(p, block, s);
+        return launch_taylor_cap<Order, 16, Mode, Grad, Stats>(p, block, cap, s);
     if (cap <= 32)
-        return launch_taylor_cap<Order, 32, Mode, Grad, Stats>(p, block, s);
+        return launch_taylor_cap<Order, 32, Mode, Grad, Stats>(p, block, cap, s);
     if (cap <= 64)
-        return launch_taylor_cap<Order, 64, Mode, Grad, Stats>(p, block, s);
-    return launch_taylor_cap<Order, 128, Mode, Grad, Stats>(p, block, s);
+        return launch_taylor_cap<Order, 64, Mode, Grad, Stats>(p, block, cap, s);
+    return launch_taylor_cap<Order, 128, Mode, Grad, Stats>(p, block, cap, s);
 }
 
 template <int Order, bool Grad, bool Stats>
