@@ -1120,6 +1120,7 @@ int batch_query_prepare(taylor_request const *reqs, std::uint32_t n, batch_query
     std::uint64_t off = 0;
     for (std::uint32_t i = 0; i < n; ++i) {
         taylor_params p = make_taylor_params(reqs[i]);
+        p.thread_stack_cap = max_bound; // the per-thread kernel's stack columns (launch_batch_cap)
         unsorted[i] = p;
         if (reqs[i].n > 1 && reqs[i].root_bounds != nullptr) {
             GWNB_TRY(query_order(reqs[i].root_bounds, reqs[i].qx, reqs[i].qy, reqs[i].qz, reqs[i].n, st->orders + off, s,
@@ -1158,7 +1159,9 @@ int launch_batch_cap(batch_query_state const &st, batch_query_config const &c, c
     if (c.per_thread == 0) {
         note_launch(), k_batch_taylor_warp<Order, Cap, Mode><<<grid, block, 0, s>>>(meshes, st.warp_begin, st.mesh_count, st.warps);
     } else {
-        std::size_t const smem = static_cast<std::size_t>(Cap) * block * sizeof(std::uint32_t);
+        // stack columns of the batch's largest stack bound (every mesh's thread_stack_cap)
+        int const column = st.max_stack_bound > 0 && st.max_stack_bound < Cap ? st.max_stack_bound : Cap;
+        std::size_t const smem = static_cast<std::size_t>(column) * block * sizeof(std::uint32_t);
         auto kern = k_batch_taylor_thread<Order, Cap, Mode>;
         if (smem > 48 * 1024)
             GWNB_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
