@@ -1207,7 +1207,8 @@ def run_build_workload(args) -> None:
     def stage(ms_list, nbytes):
         ms = float(np.mean(ms_list))
         gbs = nbytes / (ms / 1e3) / 1e9
-        return {"ms": ms, "per_s": 1e3 / ms, "bytes": int(nbytes), "achieved_gbs": gbs, "frac": gbs / pk["hbm_gbs"]}
+        return {"ms": ms, "p50_ms": float(np.median(ms_list)), "max_ms": float(np.max(ms_list)), "per_s": 1e3 / ms,
+                "bytes": int(nbytes), "achieved_gbs": gbs, "frac": gbs / pk["hbm_gbs"]}
 
     stages = {"build_hploc": stage(t_hploc, b_build), "build_lbvh": stage(t_lbvh, b_build),
               "refit": stage(t_refit, b_build), "refit_async": stage(t_refit_async, b_build)}
