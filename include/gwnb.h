@@ -192,6 +192,14 @@ GWNB_API int gwnb_memory_stats(uint64_t *reserved, uint64_t *used);
  * Call it after the stream work that freed the memory has completed. */
 GWNB_API int gwnb_memory_trim(uint64_t keep_bytes);
 
+/* Failure injection on the host, for tests of the error paths: after `count` more device
+ * allocations of the library succeed, the next one fails as an out-of-memory allocation would
+ * (the call returns GWNB_CUDA_RUNTIME_ERROR, cudaErrorMemoryAllocation, "injected failure" in the
+ * message); the injection then disarms itself. A negative count disarms it. Process-wide (every
+ * thread's allocations count). Returns the count that was armed before this call: -1 when none
+ * was, or the injection has fired since. */
+GWNB_API int64_t gwnb_fail_allocation_after(int64_t count);
+
 /* ---- geometry (include/gwn/gwn_geometry.cuh:66-90) ---------------------------------------- */
 
 /* Replaces gwn::gwn_upload_geometry (include/gwn/gwn_geometry.cuh:66-72,

@@ -203,6 +203,7 @@ SIGNATURES: dict[str, tuple] = {
     "gwnb_cuda_runtime_version": (C.c_int, []),
     "gwnb_memory_stats": (C.c_int, [C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     "gwnb_memory_trim": (C.c_int, [C.c_uint64]),
+    "gwnb_fail_allocation_after": (C.c_int64, [C.c_int64]),
     "gwnb_launch_count": (C.c_uint64, []),
     "gwnb_fp32_fma_peak": (C.c_int, [C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_void_p]),
     "gwnb_set_wait_limit": (C.c_int, [C.c_int64]),

@@ -781,6 +781,13 @@ def fp32_fma_peak(iters: int = 16384, stream=None) -> tuple[float, float]:
     return float(tf.value), float(ms.value)
 
 
+def fail_allocation_after(count: int) -> int:
+    """Failure injection (gwnb_fail_allocation_after): the library's device allocation after the
+    next `count` fails as out of memory; a negative count disarms. Returns the previously armed
+    count (-1: none armed, or it has fired)."""
+    return int(_lib.load().gwnb_fail_allocation_after(int(count)))
+
+
 def memory_trim(keep_bytes: int = 0) -> gwn_status:
     """Return the pool's cached device memory to the driver down to keep_bytes (or what is in use)."""
     return _status(_lib.load().gwnb_memory_trim(int(keep_bytes)))

@@ -558,6 +558,8 @@ int build_scene_and_morton(gwnb_geometry_f32 const &g, int morton_bits, aabb *aa
                            cudaStream_t s) {
     std::uint64_t const nt = g.triangle_count;
     unsigned int *scene = nullptr;
+    scratch_guard guard(s);
+    guard.hold(scene);
     GWNB_TRY(alloc(&scene, 6, s));
     static unsigned int const init[6] = {0xffffffffu, 0xffffffffu, 0xffffffffu, 0u, 0u, 0u};
     GWNB_CUDA_TRY(cudaMemcpyAsync(scene, init, sizeof(init), cudaMemcpyHostToDevice, s));
@@ -585,9 +587,11 @@ int build_preprocess(gwnb_geometry_f32 const &g, int morton_bits, void *sorted_c
         return GWNB_OK;
     int const kb = morton_bits / 8;
     aabb *aabbs = nullptr;
-    void *codes = nullptr;
+    unsigned char *codes = nullptr;
+    scratch_guard guard(s);
+    guard.hold(aabbs, codes);
     GWNB_TRY(alloc(&aabbs, nt, s));
-    GWNB_TRY(alloc(reinterpret_cast<unsigned char **>(&codes), nt * kb, s));
+    GWNB_TRY(alloc(&codes, nt * kb, s));
     GWNB_TRY(build_scene_and_morton(g, morton_bits, aabbs, codes, s));
     GWNB_TRY(radix_sort_pairs(codes, sorted_codes, nullptr, sorted_ids, nt, kb, morton_bits, s, status));
     note_launch(), k_gather_aabbs<<<grid_for(nt), k_block, 0, s>>>(aabbs, sorted_ids, sorted_aabbs, nt);
@@ -606,6 +610,8 @@ int build_binary_lbvh(void const *sorted_codes, int morton_bits, std::uint64_t n
     std::uint32_t *leaf_parent = nullptr;
     aabb *pending = nullptr;
     unsigned int *arrivals = nullptr;
+    scratch_guard guard(s);
+    guard.hold(leaf_parent, pending, arrivals);
     GWNB_TRY(alloc(&leaf_parent, n, s));
     GWNB_TRY(alloc(&pending, 2 * ni, s));
     GWNB_TRY(alloc(&arrivals, ni, s));
@@ -659,6 +665,8 @@ int collapse_to_bvh4(binary_node const *binary, aabb const *binary_bounds, aabb 
     p.wait_limit = wait_limit();
     std::uint32_t *words = nullptr;
     std::size_t const nwords = 3 * (k_max_levels + 1) + 2;
+    scratch_guard guard(s);
+    guard.hold(p.lists[0], p.lists[1], words, p.tile_status);
     GWNB_TRY(alloc(&p.lists[0], ni, s));
     GWNB_TRY(alloc(&p.lists[1], ni, s));
     GWNB_TRY(alloc(&words, nwords, s));

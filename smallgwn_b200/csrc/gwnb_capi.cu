@@ -76,6 +76,18 @@ std::uint64_t reserve_revision() {
     }
 }
 
+// Allocations left before the injected failure (-1: none armed).
+static std::atomic<long long> g_alloc_failure_countdown{-1};
+
+bool injected_allocation_failure() {
+    long long c = g_alloc_failure_countdown.load(std::memory_order_relaxed);
+    while (c >= 0) {
+        if (g_alloc_failure_countdown.compare_exchange_weak(c, c - 1, std::memory_order_relaxed))
+            return c == 0;
+    }
+    return false;
+}
+
 int library_pool(cudaMemPool_t *pool) {
     constexpr int k_max_devices = 64;
     static std::mutex mutex;
@@ -224,6 +236,14 @@ struct build_readback {
     std::uint32_t pad;
 };
 
+// A failing CUDA call inside build_impl releases the staged tree and the temporaries (fail()).
+#define GWNB_BUILD_CUDA_TRY(expr)                                                                  \
+    do {                                                                                           \
+        cudaError_t const gwnb_e_ = (expr);                                                        \
+        if (gwnb_e_ != cudaSuccess)                                                                \
+            return fail(set_cuda_error(gwnb_e_, #expr));                                           \
+    } while (0)
+
 // The build enqueues every stage on the stream without a host round trip (the H-PLOC convergence
 // check, the collapse's depth and node count, the leaf-node list of the refit state all stay on
 // the device) and synchronizes once, to read the tree's sizes, bounds and error word.
@@ -268,7 +288,7 @@ int build_impl(gwnb_geometry_f32 const *g, int method, std::uint32_t radius, int
         return fail(rc);
     if ((rc = alloc(&rb, 1, s)) != GWNB_OK)
         return fail(rc);
-    GWNB_CUDA_TRY(cudaMemsetAsync(rb, 0, sizeof(build_readback), s));
+    GWNB_BUILD_CUDA_TRY(cudaMemsetAsync(rb, 0, sizeof(build_readback), s));
     if ((rc = nvtx_call("gwnb::build.morton_sort", [&] {
              return build_preprocess(*g, morton_bits, codes, b.primitive_indices, sorted_aabbs, s, status);
          })) != GWNB_OK)
@@ -276,7 +296,7 @@ int build_impl(gwnb_geometry_f32 const *g, int method, std::uint32_t radius, int
     std::uint64_t capacity = 0;
     std::uint32_t root_binary = 0;
     if (nt == 1) {
-        GWNB_CUDA_TRY(cudaMemcpyAsync(&rb->root_bounds, sorted_aabbs, sizeof(aabb), cudaMemcpyDeviceToDevice, s));
+        GWNB_BUILD_CUDA_TRY(cudaMemcpyAsync(&rb->root_bounds, sorted_aabbs, sizeof(aabb), cudaMemcpyDeviceToDevice, s));
         b.root.reference = make_ref(0, 1);
     } else {
         std::uint64_t const ni = nt - 1;
@@ -298,7 +318,7 @@ int build_impl(gwnb_geometry_f32 const *g, int method, std::uint32_t radius, int
         }
         if (rc != GWNB_OK)
             return fail(rc);
-        GWNB_CUDA_TRY(cudaMemcpyAsync(&rb->root_bounds, bin_bounds + root_binary, sizeof(aabb),
+        GWNB_BUILD_CUDA_TRY(cudaMemcpyAsync(&rb->root_bounds, bin_bounds + root_binary, sizeof(aabb),
                                       cudaMemcpyDeviceToDevice, s));
         if ((rc = alloc(reinterpret_cast<node4 **>(&b.nodes), ni, s)) != GWNB_OK)
             return fail(rc);
@@ -321,11 +341,11 @@ int build_impl(gwnb_geometry_f32 const *g, int method, std::uint32_t radius, int
                                                      reinterpret_cast<triangle *>(b.triangles), aux->tri48, s, status);
          })) != GWNB_OK)
         return fail(rc);
-    GWNB_CUDA_TRY(cudaMemcpyAsync(aux->root_bounds, &rb->root_bounds, sizeof(aabb), cudaMemcpyDeviceToDevice, s));
-    GWNB_CUDA_TRY(cudaMemcpyAsync(&rb->status, status, sizeof(unsigned int), cudaMemcpyDeviceToDevice, s));
+    GWNB_BUILD_CUDA_TRY(cudaMemcpyAsync(aux->root_bounds, &rb->root_bounds, sizeof(aabb), cudaMemcpyDeviceToDevice, s));
+    GWNB_BUILD_CUDA_TRY(cudaMemcpyAsync(&rb->status, status, sizeof(unsigned int), cudaMemcpyDeviceToDevice, s));
     build_readback host{};
-    GWNB_CUDA_TRY(cudaMemcpyAsync(&host, rb, sizeof(host), cudaMemcpyDeviceToHost, s));
-    GWNB_CUDA_TRY(cudaStreamSynchronize(s));
+    GWNB_BUILD_CUDA_TRY(cudaMemcpyAsync(&host, rb, sizeof(host), cudaMemcpyDeviceToHost, s));
+    GWNB_BUILD_CUDA_TRY(cudaStreamSynchronize(s));
     if (host.status == 0u && nt > 1 && host.collapse.pending != 0u) {
         // a tree deeper than the levels enqueued up front: collapse again level batch by level batch,
         // then derive the refit state again from the complete nodes
@@ -338,9 +358,9 @@ int build_impl(gwnb_geometry_f32 const *g, int method, std::uint32_t radius, int
         if ((rc = build_triangles(*g, b.primitive_indices, nt, reinterpret_cast<triangle *>(b.triangles), aux->tri48,
                                   s, status)) != GWNB_OK)
             return fail(rc);
-        GWNB_CUDA_TRY(cudaMemcpyAsync(&rb->status, status, sizeof(unsigned int), cudaMemcpyDeviceToDevice, s));
-        GWNB_CUDA_TRY(cudaMemcpyAsync(&host, rb, sizeof(host), cudaMemcpyDeviceToHost, s));
-        GWNB_CUDA_TRY(cudaStreamSynchronize(s));
+        GWNB_BUILD_CUDA_TRY(cudaMemcpyAsync(&rb->status, status, sizeof(unsigned int), cudaMemcpyDeviceToDevice, s));
+        GWNB_BUILD_CUDA_TRY(cudaMemcpyAsync(&host, rb, sizeof(host), cudaMemcpyDeviceToHost, s));
+        GWNB_BUILD_CUDA_TRY(cudaStreamSynchronize(s));
     }
     if (host.status != 0u) {
         if (host.status & k_err_index)
@@ -374,6 +394,7 @@ int build_impl(gwnb_geometry_f32 const *g, int method, std::uint32_t radius, int
     *out = b;
     return GWNB_OK;
 }
+#undef GWNB_BUILD_CUDA_TRY
 
 } // namespace
 } // namespace gwnb
@@ -436,6 +457,10 @@ int gwnb_wait_timeout_probe(int stage, gwnb_stream_t stream) try {
     return GWNB_OK;
 } catch (...) {
     return host_exception();
+}
+
+int64_t gwnb_fail_allocation_after(int64_t count) {
+    return g_alloc_failure_countdown.exchange(count >= 0 ? count : -1, std::memory_order_relaxed);
 }
 
 int gwnb_memory_trim(uint64_t keep_bytes) try {

@@ -275,11 +275,15 @@ int build_binary_hploc(void const *sorted_codes, int morton_bits, std::uint64_t 
     if (n > 0x7fffffffull)
         return set_error(GWNB_INVALID_ARGUMENT, "bvh.build.binary.hploc: too many primitives.");
     bool const deferred_check = counter != nullptr;
-    std::uint32_t *cluster = nullptr, *boundary = nullptr;
+    std::uint32_t *cluster = nullptr, *boundary = nullptr, *own_counter = nullptr;
+    scratch_guard guard(s);
+    guard.hold(cluster, boundary, own_counter);
     GWNB_TRY(alloc(&cluster, n, s));
     GWNB_TRY(alloc(&boundary, n, s));
-    if (!deferred_check)
-        GWNB_TRY(alloc(&counter, 1, s));
+    if (!deferred_check) {
+        GWNB_TRY(alloc(&own_counter, 1, s));
+        counter = own_counter;
+    }
     GWNB_CUDA_TRY(cudaMemsetAsync(boundary, 0xff, n * sizeof(std::uint32_t), s));
     GWNB_CUDA_TRY(cudaMemsetAsync(internal_parent, 0xff, (n - 1) * sizeof(std::uint32_t), s));
     std::uint32_t const n32 = static_cast<std::uint32_t>(n);
@@ -306,7 +310,7 @@ int build_binary_hploc(void const *sorted_codes, int morton_bits, std::uint64_t 
     GWNB_CUDA_TRY(cudaStreamSynchronize(s));
     release(cluster, s);
     release(boundary, s);
-    release(counter, s);
+    release(own_counter, s);
     if ((host_status & k_err_hploc) != 0u || host_count != 2 * n32 - 1)
         return set_error(GWNB_INTERNAL_ERROR,
                          "bvh.build.binary.hploc: H-PLOC builder did not converge to a complete binary hierarchy.");

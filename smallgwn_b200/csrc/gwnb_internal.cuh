@@ -268,10 +268,16 @@ __device__ __forceinline__ void fence_acq_rel_gpu() { asm volatile("fence.acq_re
 // cached memory on request.
 int library_pool(cudaMemPool_t *pool);
 
+// Host-side failure injection (gwnb_fail_allocation_after): true when this allocation is the one
+// armed to fail; it then reports cudaErrorMemoryAllocation without touching the device.
+bool injected_allocation_failure();
+
 template <class T> int alloc(T **ptr, std::size_t count, cudaStream_t s) {
     *ptr = nullptr;
     if (count == 0)
         return GWNB_OK;
+    if (injected_allocation_failure())
+        return set_cuda_error(cudaErrorMemoryAllocation, "cudaMallocFromPoolAsync (injected failure)");
     cudaMemPool_t pool = nullptr;
     GWNB_TRY(library_pool(&pool));
     void *p = nullptr;
@@ -286,6 +292,40 @@ template <class T> void release(T *&ptr, cudaStream_t s) {
         (void)cudaFreeAsync(ptr, s);
     ptr = nullptr;
 }
+
+// The device temporaries of one call: the pointer variables handed to hold() are released on the
+// stream when the guard goes out of scope -- on the success path and on every early error return
+// alike. A buffer released earlier (release() nulls its pointer) or handed on to an object (null
+// the variable) is skipped. Declare the guard after the variables it holds.
+class scratch_guard {
+public:
+    explicit scratch_guard(cudaStream_t s) : s_(s) {}
+    scratch_guard(scratch_guard const &) = delete;
+    scratch_guard &operator=(scratch_guard const &) = delete;
+    ~scratch_guard() {
+        for (int i = n_ - 1; i >= 0; --i)
+            slots_[i].free_fn(slots_[i].var, s_);
+    }
+    template <class T> void hold(T *&ptr) {
+        if (n_ < k_slots)
+            slots_[n_++] = slot{&ptr, &free_var<T>};
+    }
+    template <class T, class... R> void hold(T *&ptr, R *&...rest) {
+        hold(ptr);
+        hold(rest...);
+    }
+
+private:
+    static constexpr int k_slots = 24;
+    struct slot {
+        void *var;
+        void (*free_fn)(void *, cudaStream_t);
+    };
+    template <class T> static void free_var(void *var, cudaStream_t s) { release(*static_cast<T **>(var), s); }
+    slot slots_[k_slots];
+    int n_ = 0;
+    cudaStream_t s_;
+};
 
 // ---- cross-TU kernels / launchers ---------------------------------------------------------------
 int radix_sort_pairs(void const *keys_in, void *keys_out, std::uint32_t const *values_in,

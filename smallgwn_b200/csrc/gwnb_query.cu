@@ -759,6 +759,8 @@ int query_order(aabb const *root_bounds, float const *qx, float const *qy, float
     if (n == 0)
         return GWNB_OK;
     std::uint32_t *codes = nullptr, *sorted = nullptr;
+    scratch_guard guard(s);
+    guard.hold(codes, sorted);
     GWNB_TRY(alloc(&codes, n, s));
     GWNB_TRY(alloc(&sorted, n, s));
     note_launch(), k_query_codes<<<static_cast<unsigned>((n + 255) / 256), 256, 0, s>>>(qx, qy, qz, n, root_bounds, codes);
@@ -1024,6 +1026,8 @@ int taylor_batch(taylor_request const &r, cudaStream_t s) {
     taylor_params p = make_taylor_params(r);
     std::uint32_t *codes = nullptr, *sorted_codes = nullptr, *order = nullptr;
     float *gathered = nullptr;
+    scratch_guard guard(s);
+    guard.hold(codes, sorted_codes, order, gathered);
     bool const sorted = r.sort_queries != 0 && r.n > 1 && r.root_bounds != nullptr;
     if (sorted) {
         GWNB_NVTX("gwnb::taylor.order");
@@ -1130,12 +1134,14 @@ int batch_query_prepare(taylor_request const *reqs, std::uint32_t n, batch_query
         sorted[i] = p;
         off += reqs[i].n;
     }
+    // each buffer joins the state as soon as it exists, so batch_query_release frees it on any
+    // failure after this point
     taylor_params *ds = nullptr, *du = nullptr;
     GWNB_TRY(alloc(&ds, n, s));
-    GWNB_TRY(alloc(&du, n, s));
-    GWNB_TRY(alloc(&st->warp_begin, n + 1, s));
     st->meshes = ds;
+    GWNB_TRY(alloc(&du, n, s));
     st->meshes_unsorted = du;
+    GWNB_TRY(alloc(&st->warp_begin, n + 1, s));
     GWNB_CUDA_TRY(cudaMemcpyAsync(ds, sorted.data(), n * sizeof(taylor_params), cudaMemcpyHostToDevice, s));
     GWNB_CUDA_TRY(cudaMemcpyAsync(du, unsorted.data(), n * sizeof(taylor_params), cudaMemcpyHostToDevice, s));
     GWNB_CUDA_TRY(cudaMemcpyAsync(st->warp_begin, wb.data(), (n + 1) * sizeof(std::uint64_t), cudaMemcpyHostToDevice, s));

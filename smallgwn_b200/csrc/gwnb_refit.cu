@@ -904,14 +904,16 @@ int batch_refit_prepare(gwnb_geometry_f32 const *geoms, gwnb_bvh4_f32 *const *bv
     st->order = order;
     st->bounds_items = bb[n];
     st->moment_items = mb[n];
+    // each buffer joins the state as soon as it exists, so batch_refit_release frees it on any
+    // failure after this point
     batch_bounds_mesh *dbd = nullptr;
     moment_params *dmd = nullptr;
     GWNB_TRY(alloc(&dbd, n, s));
+    st->bounds_meshes = dbd;
     GWNB_TRY(alloc(&dmd, n, s));
+    st->moment_meshes = dmd;
     GWNB_TRY(alloc(&st->bounds_begin, n + 1, s));
     GWNB_TRY(alloc(&st->moment_begin, n + 1, s));
-    st->bounds_meshes = dbd;
-    st->moment_meshes = dmd;
     GWNB_CUDA_TRY(cudaMemcpyAsync(dbd, bd.data(), n * sizeof(batch_bounds_mesh), cudaMemcpyHostToDevice, s));
     GWNB_CUDA_TRY(cudaMemcpyAsync(dmd, md.data(), n * sizeof(moment_params), cudaMemcpyHostToDevice, s));
     GWNB_CUDA_TRY(cudaMemcpyAsync(st->bounds_begin, bb.data(), (n + 1) * sizeof(std::uint64_t), cudaMemcpyHostToDevice, s));

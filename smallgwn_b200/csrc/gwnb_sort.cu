@@ -263,6 +263,8 @@ int sort_impl(K const *keys_in, K *keys_out, std::uint32_t const *vals_in,
     std::uint32_t *vals_tmp = nullptr;
     std::uint32_t *words = nullptr; // hist (passes*256) | counters (passes) | status (passes*tiles*256)
     std::size_t const word_count = passes * 256 + passes + passes * tiles * 256;
+    scratch_guard guard(s);
+    guard.hold(keys_tmp, vals_tmp, words);
     GWNB_TRY(alloc(&keys_tmp, n, s));
     GWNB_TRY(alloc(&vals_tmp, n, s));
     GWNB_TRY(alloc(&words, word_count, s));
@@ -355,6 +357,8 @@ int onesweep_wait_probe(unsigned int *status, cudaStream_t s) {
     std::uint32_t *keys = nullptr, *out_keys = nullptr, *out_vals = nullptr, *words = nullptr;
     // words: histogram (256) | tile counter (1) | tile status (2 tiles x 256)
     std::size_t const word_count = 256 + 1 + 2 * 256;
+    scratch_guard guard(s);
+    guard.hold(keys, out_keys, out_vals, words);
     GWNB_TRY(alloc(&keys, n, s));
     GWNB_TRY(alloc(&out_keys, n, s));
     GWNB_TRY(alloc(&out_vals, n, s));

@@ -238,3 +238,14 @@ def test_spatial_python_mirror_rejects_span_mismatch():
 def test_status_mirror():
     assert api.gwn_status().is_ok()
     assert not api.gwn_status(api.gwn_error.internal_error, "x").is_ok()
+
+
+def test_allocation_failure_injection_arms_and_disarms():
+    """gwnb_fail_allocation_after returns the previously armed count and -1 once disarmed (host
+    only; the GPU sweep over every entry point is in test_gpu_alloc_failure.py)."""
+    lib = _lib.load()
+    assert lib.gwnb_fail_allocation_after(-1) == -1
+    assert lib.gwnb_fail_allocation_after(5) == -1
+    assert lib.gwnb_fail_allocation_after(2) == 5
+    assert lib.gwnb_fail_allocation_after(-7) == 2
+    assert lib.gwnb_fail_allocation_after(-1) == -1
