@@ -31,8 +31,10 @@ def sweep(cuda, op, after=None, limit=400) -> int:
     _, used0 = api.memory_stats()
     for k in range(limit):
         api.fail_allocation_after(k)
-        st = op()
-        armed = api.fail_allocation_after(-1)
+        try:
+            st = op()
+        finally:
+            armed = api.fail_allocation_after(-1)
         cuda.cuda.synchronize()
         if armed >= 0:  # the run needed no more than k allocations
             assert st.is_ok(), (k, st.message)
