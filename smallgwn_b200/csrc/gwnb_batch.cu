@@ -48,6 +48,7 @@ struct gwnb_batch {
     unsigned int **d_status = nullptr; // device copy of status_words
     unsigned int *d_flags = nullptr;   // OR of every mesh's status word
     cudaStream_t stream = nullptr;     // stream the batch's arrays were allocated on
+    bool ready = false;                // the device descriptors are complete (prepare_states succeeded)
 };
 
 namespace gwnb {
@@ -128,7 +129,7 @@ int tree_costs(gwnb_batch *b, std::vector<double> &cost, cudaStream_t s) {
 
 // The batch's device descriptors (refit items, traversal descriptors and Hilbert orders, status
 // words) from its meshes' current objects; replaces any previous ones.
-int prepare_states(gwnb_batch *b, cudaStream_t s) {
+int prepare_states_impl(gwnb_batch *b, cudaStream_t s) {
     batch_refit_release(b->refit, s);
     batch_query_release(b->query, s);
     b->refit = batch_refit_state{};
@@ -204,7 +205,26 @@ int check_current(gwnb_batch const *b) {
     return GWNB_OK;
 }
 
+// prepare_states_impl with the batch marked ready only when every descriptor is in place; on a
+// failure the partial descriptors are released and the frame entry points refuse the batch.
+int prepare_states(gwnb_batch *b, cudaStream_t s) {
+    b->ready = false;
+    int const rc = prepare_states_impl(b, s);
+    if (rc != GWNB_OK) {
+        batch_refit_release(b->refit, s);
+        batch_query_release(b->query, s);
+        b->refit = batch_refit_state{};
+        b->query = batch_query_state{};
+        return rc;
+    }
+    b->ready = true;
+    return GWNB_OK;
+}
+
 int run_stages(gwnb_batch *b, gwnb_batch_tuning const &t, unsigned stages, cudaStream_t s) {
+    if (!b->ready)
+        return set_error(GWNB_INTERNAL_ERROR, "batch: its device descriptors are incomplete after a failed rebuild; "
+                                              "call rebuild again or release the batch.");
     GWNB_TRY(check_current(b));
     bool const bounds = (stages & GWNB_BATCH_REFIT) != 0u, moments = (stages & GWNB_BATCH_MOMENTS) != 0u;
     if (bounds || moments)
@@ -341,8 +361,9 @@ int gwnb_batch_rebuild_f32(gwnb_batch *b, float threshold, int method, uint32_t 
         redo[i] = 1;
         ++count;
     }
-    if (count > 0) {
-        // the descriptors follow the replaced objects even when a later mesh failed
+    if (count > 0 || !b->ready) {
+        // the descriptors follow the replaced objects even when a later mesh failed (and are
+        // prepared again after an earlier rebuild could not finish them)
         int const prc = prepare_states(b, s);
         if (rc == GWNB_OK)
             rc = prc;
@@ -450,6 +471,9 @@ int gwnb_batch_tune_f32(gwnb_batch *b, int reps, gwnb_batch_tuning *chosen, gwnb
 int gwnb_batch_sync_f32(gwnb_batch *b, gwnb_stream_t stream) try {
     if (b == nullptr)
         return set_error(GWNB_INVALID_ARGUMENT, "batch: null handle.");
+    if (!b->ready) // the device copy of the status words may still name the replaced objects
+        return set_error(GWNB_INTERNAL_ERROR, "batch: its device descriptors are incomplete after a failed rebuild; "
+                                              "call rebuild again or release the batch.");
     GWNB_TRY(check_current(b));
     cudaStream_t const s = as_cuda(stream);
     GWNB_CUDA_TRY(cudaMemsetAsync(b->d_flags, 0, sizeof(unsigned int), s));

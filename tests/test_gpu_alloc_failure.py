@@ -194,3 +194,73 @@ def test_adjoint_and_batched_frames(cuda, scene):
     # signs cancel, so the bound is on the array's scale)
     for got, w in zip(dv + dq, want):
         np.testing.assert_allclose(got.cpu().numpy(), w, rtol=1e-4, atol=1e-4 * float(np.abs(w).max()))
+
+
+def test_scene_files_selection_diagnostics_and_batch_upkeep(cuda, scene, tmp_path):
+    mesh, geo, bvh, moms, q = scene
+    path = tmp_path / "scene.gwnb"
+    sweep(cuda, lambda: api.save_scene(path, geo, bvh, [moms[1], moms[2]]))
+    kept = {}
+
+    def load():
+        st, *kept["objects"] = api.load_scene(path)
+        return st
+
+    sweep(cuda, load)
+    sweep(cuda, lambda: api.select_taylor_form(geo, bvh, {1: moms[1], 2: moms[2]}, *q, 1e-3)[0])
+    counts = [cuda.empty(q[0].numel(), dtype=cuda.int32, device="cuda") for _ in range(3)]
+    sweep(cuda, lambda: api.taylor_traversal_stats(bvh, moms[2], *q, *counts))
+    sweep(cuda, lambda: api.spatial_traversal_stats(bvh, *q, *counts[:2]))
+    sweep(cuda, lambda: api.taylor_form_probe(bvh, moms[2], *q)[0])
+    out = cuda.empty_like(q[0])
+    b = api.gwn_batch([(geo, bvh, moms[1], *q, out)])
+    assert b.ok(), b.status.message
+    sweep(cuda, lambda: b.tune(1)[0])
+    b.release()
+
+
+def test_batch_rebuild_under_allocation_failure(cuda):
+    """A rebuild that fails part-way keeps what it finished (a mesh whose new tree and moments are
+    both in place has them), so device memory is not expected back; instead the batch must either
+    run frames or refuse them with an error until a later rebuild completes -- never launch over
+    incomplete descriptors."""
+    mesh = meshes.to_soa(*meshes.uv_sphere(40, 21, seed=6))
+    rng = np.random.default_rng(1)
+    moved = [(mesh[k] + rng.normal(0.0, 0.5, mesh[k].size)).astype(np.float32) for k in ("x", "y", "z")]
+    q = [cuda.from_numpy(v).cuda() for v in meshes.mixed_queries(mesh, 3000, seed=2)]
+    out = cuda.empty_like(q[0])
+    refused = 0
+    for k in range(400):
+        geo = g.gwn_geometry_object()
+        assert g.gwn_upload_geometry(geo, mesh["x"], mesh["y"], mesh["z"], mesh["i0"], mesh["i1"], mesh["i2"]).is_ok()
+        bvh = g.gwn_bvh4_object()
+        assert g.gwn_build_bvh(geo, bvh).is_ok()
+        mom = g.gwn_bvh4_moment_object(1)
+        assert g.gwn_refit_bvh_moment(1, bvh, mom).is_ok()
+        b = api.gwn_batch([(geo, bvh, mom, *q, out)])
+        assert b.ok(), b.status.message
+        # scrambled vertices push the refit tree's cost ratio past 1, so the mesh is rebuilt
+        assert g.gwn_update_geometry(geo, *moved).is_ok() and b.frame().is_ok()
+        api.fail_allocation_after(k)
+        try:
+            st, _ = b.rebuild(1.0)
+        finally:
+            armed = api.fail_allocation_after(-1)
+        cuda.cuda.synchronize()
+        if armed >= 0:  # the rebuild needed no more than k allocations
+            assert st.is_ok(), st.message
+            assert b.frame().is_ok() and b.sync().is_ok()
+            b.release()
+            assert k >= 5 and refused >= 1
+            return
+        assert st.error == g.gwn_error.cuda_runtime_error and "injected" in st.message, (k, st.message)
+        fr = b.frame()
+        if not fr.is_ok():
+            assert fr.error == g.gwn_error.internal_error and "incomplete" in fr.message, (k, fr.message)
+            refused += 1
+            st, _ = b.rebuild(1.0)  # finishes what the failed rebuild left
+            assert st.is_ok(), st.message
+            assert b.frame().is_ok()
+        cuda.cuda.synchronize()
+        b.release()
+    raise AssertionError("more allocations than the sweep limit")
