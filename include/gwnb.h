@@ -668,7 +668,9 @@ GWNB_API int gwnb_batch_quality_f32(gwnb_batch *batch, float *cost_ratio, gwnb_s
  * exceeds `threshold`, from its geometry's current positions, refits its moments, replaces the
  * caller's BVH and moment objects in place and re-derives the batch's descriptors (*rebuilt: how
  * many). Between frames: a CUDA graph captured before a rebuild that rebuilt anything refers to the
- * released arrays and must be captured again. Synchronizes. */
+ * released arrays and must be captured again. On failure the meshes rebuilt so far keep their new
+ * objects; if the descriptors could not be derived again, frames, stage runs, tuning and sync
+ * return GWNB_INTERNAL_ERROR ("incomplete") until a later rebuild call derives them. Synchronizes. */
 GWNB_API int gwnb_batch_rebuild_f32(gwnb_batch *batch, float threshold, int method, uint32_t radius,
                                     uint32_t *rebuilt, gwnb_stream_t stream);
 
