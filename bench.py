@@ -106,7 +106,8 @@ def run_profile(args) -> None:
         print("profile antipodal ok")
         return
     if args.profile in ("distance", "ray"):
-        # the traversal kernel twice (distance queries already in the batch's own order)
+        # the traversal kernel twice (distance queries already in Hilbert order, walked as the
+        # distance workload walks them: warp-cooperatively)
         ray = args.profile == "ray"
         mesh = meshes.sphere_mesh()
         inp = spatial_inputs(args.profile, mesh, args.queries)
@@ -128,7 +129,7 @@ def run_profile(args) -> None:
         else:
             out = torch.empty(args.queries, device="cuda")
             for _ in range(2):
-                assert g.gwn_compute_unsigned_distance_batch(bvh, *sin, out, sort_queries=False).is_ok()
+                assert g.gwn_compute_unsigned_distance_batch(bvh, *sin, out, sort_queries=True).is_ok()
         torch.cuda.synchronize()
         print(f"profile {args.profile} ok")
         return
@@ -1518,11 +1519,14 @@ def run_spatial_workload(args) -> None:
 
     # rays run in input order: the persistent ray kernel refills finished lanes, which beats
     # ordering the batch first (9.3 against 10.4 ms for 10M rays); distance queries are ordered
-    def call(xs, o, sort=not ray):
+    # (distance batches in Hilbert order are walked warp-cooperatively; traversal="thread" gives the
+    # per-thread walk, identical results)
+    def call(xs, o, sort=not ray, traversal="warp"):
         if ray:
             st = g.gwn_compute_ray_first_hit_batch(bvh, *xs, o, stream=stream, sort_queries=sort)
         else:
-            st = g.gwn_compute_unsigned_distance_batch(bvh, *xs, o, stream=stream, sort_queries=sort)
+            st = g.gwn_compute_unsigned_distance_batch(bvh, *xs, o, stream=stream, sort_queries=sort,
+                                                       traversal=traversal)
         assert st.is_ok(), st.message
 
     for _ in range(args.warmup):
@@ -1562,16 +1566,20 @@ def run_spatial_workload(args) -> None:
     e2e = timed_steps(e2e_step, max(3, min(args.steps, 10)), 1, stream, flush)
     e2e_value = world * n / (float(np.mean(e2e)) / 1e3)
 
-    # the traversal kernel alone (distance: over pre-ordered inputs; rays: the step is the
-    # traversal alone), and the bytes it touches
+    # the traversal kernel (rays: the step is the traversal alone; distance: the step over inputs
+    # already in Hilbert order, so that the batch's own ordering finds them sorted), the per-thread
+    # walk of the same batch, and the bytes the traversal touches
+    per_thread_ms = None
     if ray:
         sin = din
+        kt = timed_steps(lambda: call(sin, out, sort=False), 3, 1, stream, flush)
     else:
         order = torch.empty(n, dtype=torch.int32, device="cuda")
         assert api.query_order(bvh, *din, order, stream).is_ok()
         idx = order.long()
         sin = [d[idx].contiguous() for d in din]
-    kt = timed_steps(lambda: call(sin, out, sort=False), 3, 1, stream, flush)
+        kt = timed_steps(lambda: call(sin, out), 3, 1, stream, flush)
+        per_thread_ms = float(np.mean(timed_steps(lambda: call(din, out, traversal="thread"), 3, 1, stream, flush)))
     kernel_ms = float(np.mean(kt))
     sn = torch.empty(n, dtype=torch.int32, device="cuda")
     stri = torch.empty_like(sn)
@@ -1649,11 +1657,14 @@ def run_spatial_workload(args) -> None:
                        "l2": "flushed (256 MiB write) between timed steps", "parallelism": f"replicas x{world}",
                        "subset_mismatches_vs_oracle": mismatches, "parity_subset": int(sub.stop),
                        "mean_nodes_entered": nodes_entered / n, "mean_triangles_tested": tris_tested / n,
-                       "hit_fraction": hit_frac, "smallgwn_gpu_kernel_per_s": ref_gpu},
+                       "hit_fraction": hit_frac, "smallgwn_gpu_kernel_per_s": ref_gpu,
+                       "walk": None if ray else "warp-cooperative (32 neighbouring queries per warp)",
+                       "per_thread_walk_ms_per_step": per_thread_ms},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
                          "frac": achieved / pk["hbm_gbs"], "peak_source": pk["source"],
-                         "traffic": profiled_spatial_traffic(kind, n),
-                         "kernel": "k_ray (persistent, input order)" if ray else "k_distance (pre-ordered inputs)",
+                         "traffic": profiled_spatial_traffic("ray" if ray else "distance_warp", n),
+                         "kernel": "k_ray (persistent, input order)" if ray else
+                                   "k_distance_warp (inputs already in Hilbert order; the batch's ordering included)",
                          "kernel_ms": kernel_ms, "algorithmic_bytes": alg_bytes,
                          "bytes_model": f"{in_bytes} B in + {out_bytes} B out per query + 128 B per node entered + "
                                         "48 B per triangle tested"},

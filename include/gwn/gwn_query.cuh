@@ -197,7 +197,7 @@ template <gwn_query_batch_config Config = gwn_query_batch_config{}, int Width, g
             return gwn_status::invalid_argument("BVH object contains no queryable data.");
         GWN_RETURN_ON_ERROR(detail::check_batch_spans(qx, qy, qz, output.size()));
         gwnb_bvh4_f32 v = detail::query_view(bvh);
-        gwnb_spatial_options const o{Config.block_size, Config.stack_capacity, 0};
+        gwnb_spatial_options const o{Config.block_size, Config.stack_capacity, 0, GWNB_WALK_WARP};
         int const rc = gwnb_unsigned_distance_batch_f32(&v, qx.data(), qy.data(), qz.data(), output.data(),
                                                         output.size(), culling_band, &o, detail::gwnb_stream(stream));
         detail::store_aux(bvh, v);
@@ -231,7 +231,7 @@ template <gwn_query_batch_config Config = gwn_query_batch_config{}, int Width, g
             output.size() != n)
             return gwn_status::invalid_argument("ray first-hit: mismatched span sizes");
         gwnb_bvh4_f32 v = detail::query_view(bvh);
-        gwnb_spatial_options const o{Config.block_size, Config.stack_capacity, 0};
+        gwnb_spatial_options const o{Config.block_size, Config.stack_capacity, 0, GWNB_WALK_WARP};
         int const rc = gwnb_ray_first_hit_batch_f32(&v, ox.data(), oy.data(), oz.data(), dx.data(), dy.data(),
                                                     dz.data(), reinterpret_cast<gwnb_ray_hit_f32 *>(output.data()), n,
                                                     t_min, t_max, &o, detail::gwnb_stream(stream));
@@ -264,7 +264,7 @@ template <gwn_query_batch_config Config = gwn_query_batch_config{}, int Width, g
         gwnb_geometry_f32 g = detail::to_gwnb(geometry.accessor());
         gwnb_bvh4_f32 v = detail::query_view(bvh);
         gwnb_boundary_chain_u32 c = detail::to_gwnb(boundary_chain.accessor());
-        gwnb_spatial_options const o{Config.block_size, Config.stack_capacity, 0};
+        gwnb_spatial_options const o{Config.block_size, Config.stack_capacity, 0, GWNB_WALK_WARP};
         int const rc = gwnb_winding_antipodal_batch_f32(&g, &v, &c, qx.data(), qy.data(), qz.data(), output.data(),
                                                         output.size(), &o, detail::gwnb_stream(stream));
         detail::store_aux(bvh, v);

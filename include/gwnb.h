@@ -392,10 +392,13 @@ typedef struct gwnb_spatial_options {
     int block_size;     /* gwn_query_batch_config::block_size, multiple of 32 (0 = default 256)  */
     int stack_capacity; /* gwn_query_batch_config::stack_capacity (0 = default 64)               */
     int sort_queries;   /* 1: traverse in Hilbert order of the query points / ray origins        */
+    int per_thread;     /* distance batches in Hilbert order: GWNB_WALK_WARP (0, default),
+                         * GWNB_WALK_THREAD (1) or GWNB_WALK_TIMED (2); identical results           */
 } gwnb_spatial_options;
-/* Distance batches in Hilbert order run one query per thread; in input order, and every ray
- * batch, run persistently: a thread whose query has finished takes the next unclaimed one.
- * For the rays of the 1M-triangle benchmark, input order (sort_queries = 0) is the faster choice. */
+/* Distance batches in Hilbert order are walked warp-cooperatively (32 neighbouring queries walk one
+ * traversal, each lane pruning by its own bound) or one query per thread; in input order, and every
+ * ray batch, run persistently: a thread whose query has finished takes the next unclaimed one. For
+ * the rays of the 1M-triangle benchmark, input order (sort_queries = 0) is the faster choice. */
 
 /* gwn::gwn_ray_first_hit_status (include/gwn/gwn_query.cuh:63-68). */
 enum { GWNB_RAY_MISS = 0, GWNB_RAY_HIT = 1, GWNB_RAY_OVERFLOW = 2 };

@@ -152,6 +152,7 @@ class spatial_options(C.Structure):
         ("block_size", C.c_int),
         ("stack_capacity", C.c_int),
         ("sort_queries", C.c_int),
+        ("per_thread", C.c_int),
     ]
 
 

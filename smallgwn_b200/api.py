@@ -512,8 +512,9 @@ def _ray_rows(out) -> int:
     return n // RAY_HIT_WORDS
 
 
-def _spatial_options(config: gwn_query_batch_config, sort_queries: bool):
-    return _lib.spatial_options(int(config.block_size), int(config.stack_capacity), 1 if sort_queries else 0)
+def _spatial_options(config: gwn_query_batch_config, sort_queries: bool, traversal: str = "warp"):
+    return _lib.spatial_options(int(config.block_size), int(config.stack_capacity), 1 if sort_queries else 0,
+                                TRAVERSALS[traversal])
 
 
 class gwn_boundary_chain_object(_stream_mixin):
@@ -609,15 +610,20 @@ def gwn_compute_winding_gradient_antipodal_batch(geometry, boundary: gwn_boundar
 
 def gwn_compute_unsigned_distance_batch(bvh: gwn_bvh4_object, qx, qy, qz, out, culling_band: float = float("inf"),
                                         stream=None, config: gwn_query_batch_config = gwn_query_batch_config(),
-                                        sort_queries: bool = False) -> gwn_status:
+                                        sort_queries: bool = False, traversal: str = "warp") -> gwn_status:
     """Unsigned point-to-mesh distances of a device batch, at most ``culling_band`` (asynchronous).
-    ``sort_queries`` traverses in Hilbert order of the points (results stay at input positions)."""
+    ``sort_queries`` traverses in Hilbert order of the points (results stay at input positions);
+    such a batch is walked by ``traversal``: "warp" (32 neighbouring queries per warp walk one
+    traversal), "thread" (one walk per query) or "timed" (the faster of the two for calls of this
+    kind, from the timed first two); identical results."""
     if not bvh.has_data():
         return gwn_status(gwn_error.invalid_argument, "BVH object contains no queryable data.")
+    if traversal not in TRAVERSALS:
+        return gwn_status(gwn_error.invalid_argument, f"Unknown traversal {traversal!r}.")
     bad = _check_spans(qx, qy, qz, out)
     if bad is not None:
         return bad
-    opt = _spatial_options(config, sort_queries)
+    opt = _spatial_options(config, sort_queries, traversal)
     rc = _lib.load().gwnb_unsigned_distance_batch_f32(C.byref(bvh._view), _ptr(qx), _ptr(qy), _ptr(qz), _ptr(out),
                                                       _numel(out), float(culling_band), C.byref(opt), _stream(stream))
     return _status(rc)

@@ -17,6 +17,7 @@
 #include <atomic>
 #include <cstddef>
 #include <cstdint>
+#include <tuple>
 #include <string>
 
 #include "../../include/gwnb.h"
@@ -326,6 +327,28 @@ private:
     int n_ = 0;
     cudaStream_t s_;
 };
+
+// ---- timed walk choice (GWNB_WALK_TIMED) --------------------------------------------------------
+// The kind of a batch whose walks are timed against each other: its tree (the moment sidecar for
+// Taylor batches, the node array for distance batches), the batch family (0 Taylor, 1 distance),
+// and the parameters that change the walk's cost.
+struct walk_kind {
+    void const *tree;
+    int device, family, order, mode, grad, sorted, size_class;
+    std::uint32_t scale_bits; // accuracy scale (Taylor) or culling band (distance), as bits
+    bool operator<(walk_kind const &o) const {
+        return std::tie(tree, device, family, order, mode, grad, sorted, size_class, scale_bits) <
+               std::tie(o.tree, o.device, o.family, o.order, o.mode, o.grad, o.sorted, o.size_class, o.scale_bits);
+    }
+};
+struct walk_plan {
+    bool per_thread = false;
+    cudaEvent_t start = nullptr, stop = nullptr; // recorded around the traversal (null: untimed)
+};
+// The walk for the next call of kind k on stream s: the first call of a kind walks
+// warp-cooperatively and the second per thread, each between two events; later calls take the
+// faster once both timings have completed (polled, never waited for). Thread-safe.
+walk_plan plan_walk(walk_kind const &k, cudaStream_t s);
 
 // ---- cross-TU kernels / launchers ---------------------------------------------------------------
 int radix_sort_pairs(void const *keys_in, void *keys_out, std::uint32_t const *values_in,

@@ -909,25 +909,11 @@ int taylor_probe(taylor_request const &r, std::uint32_t const *order, cudaStream
 // decided walk, or the warp walk, and record nothing.
 namespace {
 
-struct walk_kind {
-    void const *qnodes;
-    int device, order, mode, grad, sorted, size_class;
-    std::uint32_t beta_bits;
-    bool operator<(walk_kind const &o) const {
-        return std::tie(qnodes, device, order, mode, grad, sorted, size_class, beta_bits) <
-               std::tie(o.qnodes, o.device, o.order, o.mode, o.grad, o.sorted, o.size_class, o.beta_bits);
-    }
-};
 struct walk_timing {
     int phase = 0; // 0: nothing timed; 1: warp walk timed; 2: both timed; 3: decided
     bool per_thread = false;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr}; // warp start / end, per-thread start / end
 };
-struct walk_plan {
-    bool per_thread = false;
-    cudaEvent_t start = nullptr, stop = nullptr; // recorded around the traversal (null: untimed)
-};
-
 constexpr std::size_t k_walk_kinds = 256; // the table is emptied when it holds this many kinds
 
 std::mutex &walk_mutex() {
@@ -955,6 +941,8 @@ cudaError_t poll(cudaEvent_t e) {
         (void)cudaGetLastError();
     return q;
 }
+
+} // namespace
 
 walk_plan plan_walk(walk_kind const &k, cudaStream_t s) {
     walk_plan plan;
@@ -1018,8 +1006,6 @@ walk_plan plan_walk(walk_kind const &k, cudaStream_t s) {
     return plan;
 }
 
-} // namespace
-
 int taylor_batch(taylor_request const &r, cudaStream_t s) {
     if (r.n == 0)
         return GWNB_OK;
@@ -1077,8 +1063,8 @@ int taylor_batch(taylor_request const &r, cudaStream_t s) {
         int size_class = 0;
         for (std::uint64_t v = r.n; v > 1; v >>= 1)
             ++size_class;
-        plan = plan_walk(walk_kind{r.qnodes, device, r.order, r.near_mode, grad ? 1 : 0, sorted ? 1 : 0, size_class,
-                                   beta_bits},
+        plan = plan_walk(walk_kind{r.qnodes, device, 0, r.order, r.near_mode, grad ? 1 : 0, sorted ? 1 : 0,
+                                   size_class, beta_bits},
                          s);
     }
     bool const per_thread = plan.per_thread;

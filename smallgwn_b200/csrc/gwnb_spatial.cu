@@ -19,6 +19,8 @@
 // device error bit instead of trapping.
 #include "gwnb_internal.cuh"
 
+#include <cstring>
+
 #include <cfloat>
 
 namespace gwnb {
@@ -700,6 +702,145 @@ template <bool Stats> __global__ void __launch_bounds__(256) k_distance(spatial_
     distance_finish<Stats>(p, L, overflow);
 }
 
+// Warp-cooperative distance walk for batches in Hilbert order: the 32 lanes of a warp (32
+// neighbouring queries) walk one traversal together. Every stack entry carries the mask of lanes
+// that still need the subtree; at a node each lane tests the four child boxes against its own
+// bound, the leaf children are evaluated by the lanes that need them (slot order) and the internal
+// ones are pushed far to near by the smallest box distance among the lanes that need them, the
+// nearest entered directly. A lane leaves a subtree when the child box is no nearer than its bound
+// and leaves the walk once a triangle touches it. Each lane's result is the minimum over the
+// triangles its own pruning lets through -- the same triangle set bound as the per-thread walk, so
+// the same minimum -- only the order of the visits differs (and with it how soon a bound tightens).
+// The stack lives in the lanes' registers (entry e in lane e & 31, bank e >> 5), as in the Taylor
+// warp walk; the union walk never holds more entries than the tree's internal stack bound.
+template <int Cap> __global__ void __launch_bounds__(256) k_distance_warp(spatial_params p) {
+    static_assert(Cap <= 64, "warp stack holds at most 64 entries");
+    unsigned const lane = threadIdx.x & 31u;
+    std::uint64_t const idx = static_cast<std::uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    bool const valid = idx < p.n;
+    if (__ballot_sync(0xffffffffu, valid) == 0u)
+        return;
+    distance_lane L{};
+    bool const walks = valid && distance_begin<false>(p, idx, L);
+    unsigned mask = __ballot_sync(0xffffffffu, walks);
+    bool overflow = false;
+    if (mask != 0u) {
+        std::uint32_t node = static_cast<std::uint32_t>(ref_offset(p.root_ref));
+        std::uint32_t st_node0 = 0, st_node1 = 0;
+        unsigned st_mask0 = 0, st_mask1 = 0;
+        int sp = 0;
+        for (;;) {
+            mask &= __ballot_sync(0xffffffffu, walks && !L.touched);
+            if (mask != 0u && node < p.node_count) {
+                bool const active = ((mask >> lane) & 1u) != 0u;
+                float4 const *nd = p.nodes + static_cast<std::uint64_t>(node) * 8;
+                // internal children that some lane needs: (warp-nearest box distance, node, lanes)
+                std::uint32_t key[4], child[4];
+                unsigned cm[4];
+                int ni = 0;
+#pragma unroll
+                for (int s = 0; s < 4; ++s) {
+                    key[s] = 0xffffffffu;
+                    child[s] = k_invalid_u32;
+                    cm[s] = 0u;
+                }
+#pragma unroll
+                for (int s = 0; s < 4; ++s) {
+                    float4 const A = __ldg(nd + 2 * s);
+                    float4 const B = __ldg(nd + 2 * s + 1);
+                    std::uint64_t const ref =
+                        (static_cast<std::uint64_t>(__float_as_uint(B.w)) << 32) | __float_as_uint(B.z);
+                    if (!ref_valid(ref))
+                        continue;
+                    float const d2 = active ? aabb_d2(L.q, A, B) : 0.0f;
+                    bool const want = active && d2 < L.best;
+                    unsigned const m = __ballot_sync(0xffffffffu, want);
+                    if (m == 0u)
+                        continue;
+                    if (ref_leaf(ref)) {
+                        if (want && !L.touched && d2 < L.best)
+                            distance_leaf<false>(p, L, ref);
+                    } else if (ref_offset(ref) < p.node_count) {
+                        // d2 >= 0, so its bits order like the value
+                        std::uint32_t const k = __reduce_min_sync(0xffffffffu, want ? __float_as_uint(d2) : 0xffffffffu);
+#pragma unroll
+                        for (int j = 0; j < 4; ++j)
+                            if (j == ni) {
+                                key[j] = k;
+                                child[j] = static_cast<std::uint32_t>(ref_offset(ref));
+                                cm[j] = m;
+                            }
+                        ++ni;
+                    }
+                }
+                // near first (the five-comparator network on the uniform keys)
+                auto cswap = [&](int l, int r) {
+                    if (key[l] > key[r]) {
+                        std::uint32_t const tk = key[l], tc = child[l];
+                        unsigned const tm = cm[l];
+                        key[l] = key[r];
+                        child[l] = child[r];
+                        cm[l] = cm[r];
+                        key[r] = tk;
+                        child[r] = tc;
+                        cm[r] = tm;
+                    }
+                };
+                cswap(0, 1);
+                cswap(2, 3);
+                cswap(0, 2);
+                cswap(1, 3);
+                cswap(1, 2);
+                std::uint32_t next = k_invalid_u32;
+                unsigned next_mask = 0u;
+#pragma unroll
+                for (int s = 3; s >= 0; --s) {
+                    if (child[s] == k_invalid_u32)
+                        continue;
+                    if (next != k_invalid_u32) {
+                        if (sp >= Cap || sp >= p.stack_cap) {
+                            overflow = true;
+                            break;
+                        }
+                        if (static_cast<unsigned>(sp & 31) == lane) {
+                            if (sp < 32) {
+                                st_node0 = next;
+                                st_mask0 = next_mask;
+                            } else {
+                                st_node1 = next;
+                                st_mask1 = next_mask;
+                            }
+                        }
+                        ++sp;
+                    }
+                    next = child[s];
+                    next_mask = cm[s];
+                }
+                if (overflow)
+                    break;
+                if (next != k_invalid_u32) {
+                    node = next;
+                    mask = next_mask;
+                    continue;
+                }
+            }
+            if (sp == 0)
+                break;
+            --sp;
+            int const src = sp & 31;
+            if (sp < 32) {
+                node = __shfl_sync(0xffffffffu, st_node0, src);
+                mask = __shfl_sync(0xffffffffu, st_mask0, src);
+            } else {
+                node = __shfl_sync(0xffffffffu, st_node1, src);
+                mask = __shfl_sync(0xffffffffu, st_mask1, src);
+            }
+        }
+    }
+    if (valid)
+        distance_finish<false>(p, L, walks && overflow);
+}
+
 template <bool Stats> __global__ void __launch_bounds__(256) k_distance_walk(spatial_params p) {
     extern __shared__ std::uint32_t s_stack[]; // [p.stack_cap][blockDim.x]
     walk<distance_walk, Stats>(p, s_stack + threadIdx.x);
@@ -793,9 +934,19 @@ template <class Kern> int launch_persistent(Kern kern, spatial_params p, int blo
     return GWNB_OK;
 }
 
-template <bool Ray, bool Stats> int launch_spatial(spatial_params const &p, int block, cudaStream_t s) {
+template <int Cap> int launch_distance_warp(spatial_params const &p, cudaStream_t s) {
+    unsigned const grid = static_cast<unsigned>((p.n + 255) / 256);
+    note_launch(), k_distance_warp<Cap><<<grid, 256, 0, s>>>(p);
+    GWNB_CUDA_TRY(cudaGetLastError());
+    return GWNB_OK;
+}
+
+// warp_walk: a distance batch in Hilbert order walked warp-cooperatively (k_distance_warp).
+template <bool Ray, bool Stats> int launch_spatial(spatial_params const &p, int block, bool warp_walk, cudaStream_t s) {
     if (Ray)
         return launch_persistent(k_ray<Stats>, p, block, s);
+    if (warp_walk)
+        return p.stack_cap <= 32 ? launch_distance_warp<32>(p, s) : launch_distance_warp<64>(p, s);
     return p.order != nullptr ? launch_per_query(k_distance<Stats>, p, block, s)
                               : launch_persistent(k_distance_walk<Stats>, p, block, s);
 }
@@ -873,20 +1024,42 @@ int spatial_batch(gwnb_bvh4_f32 *b, spatial_request const &r, cudaStream_t s) {
     if (p.stack_cap < 1)
         p.stack_cap = 1;
     bool const stats = r.stat_nodes != nullptr;
+    // the walk of a distance batch in Hilbert order (the statistics keep the per-thread walk, whose
+    // visit counts are the canonical traversal's)
+    walk_plan plan;
+    plan.per_thread = true;
+    if (!r.ray && !stats && p.order != nullptr && p.stack_cap <= 64) {
+        plan.per_thread = r.opt.per_thread == GWNB_WALK_THREAD;
+        if (r.opt.per_thread == GWNB_WALK_TIMED) {
+            int device = 0;
+            (void)cudaGetDevice(&device);
+            float const band = r.culling_band;
+            std::uint32_t band_bits = 0;
+            std::memcpy(&band_bits, &band, sizeof(band_bits));
+            int size_class = 0;
+            for (std::uint64_t v = r.n; v > 1; v >>= 1)
+                ++size_class;
+            plan = plan_walk(walk_kind{b->nodes, device, 1, 0, 0, 0, 1, size_class, band_bits}, s);
+        }
+    }
+    if (plan.start != nullptr)
+        (void)cudaEventRecord(plan.start, s);
+    int const block = query_launch_block(r.opt.block_size);
+    bool const warp = !plan.per_thread;
     int rc;
     if (r.ray)
-        rc = stats ? launch_spatial<true, true>(p, query_launch_block(r.opt.block_size), s)
-                   : launch_spatial<true, false>(p, query_launch_block(r.opt.block_size), s);
+        rc = stats ? launch_spatial<true, true>(p, block, false, s) : launch_spatial<true, false>(p, block, false, s);
     else
-        rc = stats ? launch_spatial<false, true>(p, query_launch_block(r.opt.block_size), s)
-                   : launch_spatial<false, false>(p, query_launch_block(r.opt.block_size), s);
+        rc = stats ? launch_spatial<false, true>(p, block, false, s) : launch_spatial<false, false>(p, block, warp, s);
+    if (plan.stop != nullptr)
+        (void)cudaEventRecord(plan.stop, s);
     release(order, s);
     return rc;
 }
 
 // Shared validation in smallgwn's order (include/gwn/gwn_query.cuh:149-170 and :232-248).
 int spatial_options(gwnb_bvh4_f32 const *b, gwnb_spatial_options const *in, gwnb_spatial_options &o) {
-    o = gwnb_spatial_options{256, 64, 0};
+    o = gwnb_spatial_options{256, 64, 0, GWNB_WALK_WARP};
     if (in != nullptr) {
         o = *in;
         if (o.block_size == 0)
@@ -898,6 +1071,8 @@ int spatial_options(gwnb_bvh4_f32 const *b, gwnb_spatial_options const *in, gwnb
         return set_error(GWNB_INVALID_ARGUMENT, "Query batch block size must be a multiple of 32 in [32, 1024].");
     if (o.stack_capacity <= 0)
         return set_error(GWNB_INVALID_ARGUMENT, "Traversal stack capacity must be positive.");
+    if (o.per_thread < GWNB_WALK_WARP || o.per_thread > GWNB_WALK_TIMED)
+        return set_error(GWNB_INVALID_ARGUMENT, "Unknown traversal (per_thread must be 0, 1 or 2).");
     if (ref_internal(b->root.reference) && b->internal_stack_bound > static_cast<std::uint32_t>(o.stack_capacity))
         return set_error(GWNB_INVALID_ARGUMENT, "Traversal stack capacity is below the BVH internal stack bound.");
     // the shared-memory stack holds the internal stack bound for every thread of a block

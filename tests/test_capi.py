@@ -197,6 +197,11 @@ def test_spatial_batches_reject_invalid_contracts_before_launch():
     assert lib.gwnb_ray_first_hit_batch_f32(C.byref(fake), None, None, None, None, None, None, None, 0, 0.0, 1.0,
                                             C.byref(one), None) == _lib.GWNB_INVALID_ARGUMENT
     assert "Traversal stack capacity" in _lib.last_error()
+    # an unknown distance walk is refused
+    walk = _lib.spatial_options(256, 64, 1, _lib.GWNB_WALK_TIMED + 1)
+    assert lib.gwnb_unsigned_distance_batch_f32(C.byref(fake), None, None, None, None, 0, 1.0, C.byref(walk),
+                                                None) == _lib.GWNB_INVALID_ARGUMENT
+    assert "Unknown traversal" in _lib.last_error()
     # empty batches with a valid capacity are accepted; t_max < t_min (or NaN) is not
     assert lib.gwnb_unsigned_distance_batch_f32(C.byref(fake), None, None, None, None, 0, 1.0, None, None) == 0
     assert lib.gwnb_ray_first_hit_batch_f32(C.byref(fake), None, None, None, None, None, None, None, 0, 0.0, 1.0,

@@ -3,7 +3,7 @@
 Against the oracle (the canonical traversal of detail/gwn_query_distance_impl.cuh:40-160 and
 detail/gwn_query_ray_impl.cuh:376-560 restated in C with the same fixed pattern of fused
 multiply-adds) on the tree the GPU built: distances, hit records and traversal statistics bit for bit, in input order and in
-Hilbert order. Against smallgwn's known answers (tests/unit_gwn_query_distance_ray.cu, restated in
+Hilbert order (distances under every walk of a Hilbert-ordered batch). Against smallgwn's known answers (tests/unit_gwn_query_distance_ray.cu, restated in
 spatial_cases.py), against FP64 closest points, and against smallgwn's own kernels (oracle/_ref,
 compiled with FMA contraction, so within a few ulps; equal-t hits may name either triangle there).
 """
@@ -98,7 +98,9 @@ def test_distance_bit_exact_with_oracle(cuda, name, method):
     for band in (float("inf"), 0.02, -1.0):
         ref, st = oracle.unsigned_distance(nodes, tris, root, *q, culling_band=band, stats=True)
         np.testing.assert_array_equal(gpu_distance(cuda, bvh, q, band), ref)
-        np.testing.assert_array_equal(gpu_distance(cuda, bvh, q, band, sort_queries=True), ref)
+        # Hilbert order: the warp-cooperative walk, the per-thread walk and the timed choice
+        for walk in ("warp", "thread", "timed", "timed", "timed"):
+            np.testing.assert_array_equal(gpu_distance(cuda, bvh, q, band, sort_queries=True, traversal=walk), ref)
     # traversal statistics (unbounded band) equal the oracle's counts
     ref, st = oracle.unsigned_distance(nodes, tris, root, *q, stats=True)
     dq = dev(cuda, *q)
