@@ -190,10 +190,13 @@ def test_adjoint_and_batched_frames(cuda, scene):
     b.release()
     assert api.gwn_winding_taylor_backward(saved["state"], geo, bvh, moms[1], upstream, *dv, *dq).is_ok()
     cuda.cuda.synchronize()
-    # dL/dV sums its per-triangle terms by atomics: equal up to the order of the sums (terms of both
-    # signs cancel, so the bound is on the array's scale)
-    for got, w in zip(dv + dq, want):
-        np.testing.assert_allclose(got.cpu().numpy(), w, rtol=1e-4, atol=1e-4 * float(np.abs(w).max()))
+    # dL/dV sums its per-triangle terms by atomics, in an order that changes from run to run, and
+    # the terms of both signs cancel: the check is on the array's scale (a state damaged by a failed
+    # call would be off by far more); dL/dq has no atomics
+    for got, w in zip(dv, want[:3]):
+        np.testing.assert_allclose(got.cpu().numpy(), w, rtol=1e-3, atol=1e-3 * float(np.abs(w).max()))
+    for got, w in zip(dq, want[3:]):
+        np.testing.assert_array_equal(got.cpu().numpy(), w)
 
 
 def test_scene_files_selection_diagnostics_and_batch_upkeep(cuda, scene, tmp_path):
